@@ -1,0 +1,318 @@
+"""ORACLE — CPU checkers for the genome-wide LD-score hot path (test infrastructure).
+
+Two CPU implementations live here, and only tests/, ``__graft_entry__.smoke()``
+and the CPU-baseline leg of ``bench.py`` may use them:
+
+* ``Oracle`` — our FP64 restatement (``oracle/lds_oracle.cpp``), built into
+  ``oracle/_build/liblds_oracle.so``;
+* ``Reference`` — the reference's own ``gwldcore.cpp``/``genotype.cpp``
+  compiled unchanged into ``oracle/_ref/libref_gwld.so`` (``oracle/Makefile``).
+
+``gw_ldscore`` restates the per-V-tile driver of
+``src/summit/ldscore/gw_ldscore.py:1753-2222`` (``GenomewideLDScore._compute_ldscore``)
+for the case without covariates: balanced V-tiles (``_bounded_vtile_sizes``
+:687-697), blocks of ``step_size`` SNPs (:1702-1703), residual variances fused
+into the first phase-1 pass (:1776-1787), phase 1 per block (:1959), zeroing of
+untouched bins (:2017-2019), phase 2 per block (:2096), division by the probe
+count (:2197) and the correlation null ``M_k / N_denom`` (:2220-2222).  It can
+drive either CPU implementation, so the restatement is checked against the
+reference end to end.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_SO = HERE / "_build" / "liblds_oracle.so"
+REF_SO = HERE / "_ref" / "libref_gwld.so"
+
+_p = C.c_void_p
+_i64 = C.c_int64
+_u64 = C.c_uint64
+_int = C.c_int
+_dbl = C.c_double
+_str = C.c_char_p
+
+DIST_CODES = {"rademacher": 0, "gaussian": 1, "normal": 1, "spherical": 2}
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(_p)
+
+
+def bounded_vtile_sizes(nvecs: int, vmax: int, granularity: int = 64) -> list[int]:
+    """Probe V-tile partition, gw_ldscore.py:687-697."""
+    width = min(nvecs, vmax)
+    if width >= granularity:
+        width = max(granularity, (width // granularity) * granularity)
+    return [min(width, nvecs - s) for s in range(0, nvecs, width)]
+
+
+def compute_blocks(nsnps: int, step: int) -> list[tuple[int, int]]:
+    """SNP blocks, gw_ldscore.py:1702-1703."""
+    return [(s, min(nsnps, s + step)) for s in range(0, nsnps, step)]
+
+
+class Oracle:
+    """ctypes view of oracle/_build/liblds_oracle.so (our FP64 restatement)."""
+
+    def __init__(self, path: Path = ORACLE_SO):
+        if not path.exists():
+            raise RuntimeError(f"oracle library missing: {path} (run `make -C oracle`)")
+        L = C.CDLL(str(path))
+        L.orc_last_error.restype = _str
+        L.orc_standardize_block.argtypes = [_p, _i64, _i64, _p, _i64, _int, _int, _int, _int,
+                                            _u64, _p, _p, _p]
+        L.orc_make_probes.argtypes = [_u64, _int, _int, _int, _int, _int, _int, _p]
+        L.orc_phase1_block.argtypes = [_p, _i64, _int, _p, _int, _p, _p, _int, _p, _p, _int]
+        L.orc_phase2_block.argtypes = [_p, _i64, _int, _int, _p, _int, _p, _i64, _p, _int, _int,
+                                       _p, _p, _dbl, _int]
+        L.orc_inv_resvar_block.argtypes = [_p, _i64, _int, _dbl, _p]
+        L.orc_int_products.argtypes = [_p, _i64, _i64, _int, _p, _i64, _p, _p]
+        self.lib = L
+
+    def standardize(self, bed_rows: np.ndarray, n_total: int, blk_start: int, blk_end: int,
+                    rows=None, ddof=1, impute="mean", impute_seed=0):
+        bed_rows = np.ascontiguousarray(bed_rows, dtype=np.uint8)
+        rows_a = None if rows is None else np.ascontiguousarray(rows, dtype=np.int64)
+        n = n_total if rows_a is None else rows_a.size
+        L = blk_end - blk_start
+        geno = np.empty((n, L), dtype=np.float64, order="F")
+        mean = np.empty(L)
+        inv = np.empty(L)
+        self.lib.orc_standardize_block(_ptr(bed_rows), bed_rows.shape[1], n_total, _ptr(rows_a),
+                                       n, blk_start, blk_end, ddof, int(impute == "hwe"),
+                                       impute_seed, _ptr(geno), _ptr(mean), _ptr(inv))
+        return geno, mean, inv
+
+    def probes(self, root, blk_start, v_start, L, V, dist="rademacher", as_float=False):
+        Z = np.empty((L, V), dtype=np.float64, order="F")
+        self.lib.orc_make_probes(root, blk_start, v_start, L, V, DIST_CODES[dist],
+                                 int(as_float), _ptr(Z))
+        return Z
+
+    def phase1_block(self, geno, annot, inv, Z, Xz, bin_init=None, as_float=False):
+        N, L = geno.shape
+        K = annot.shape[1]
+        V = Z.shape[1]
+        self.lib.orc_phase1_block(_ptr(geno), N, L, _ptr(np.ascontiguousarray(annot, np.float64)),
+                                  K, _ptr(np.ascontiguousarray(inv, np.float64)), _ptr(Z), V,
+                                  _ptr(Xz), _ptr(bin_init), int(as_float))
+
+    def phase2_block(self, geno, blk_start, inv, V, Xz, meansq, N_denom, mc_agg=None,
+                     mc_per_snp=None, extreme=1e10, drop_extreme=True):
+        N, L = geno.shape
+        rc = self.lib.orc_phase2_block(_ptr(geno), N, L, blk_start,
+                                       _ptr(np.ascontiguousarray(inv, np.float64)), V, _ptr(Xz),
+                                       Xz.shape[1], _ptr(meansq), meansq.shape[1], N_denom,
+                                       _ptr(mc_agg), _ptr(mc_per_snp), extreme, int(drop_extreme))
+        if rc:
+            raise RuntimeError(self.lib.orc_last_error().decode())
+
+    def inv_resvar(self, geno, eps=1e-10):
+        N, L = geno.shape
+        out = np.empty(L)
+        self.lib.orc_inv_resvar_block(_ptr(geno), N, L, eps, _ptr(out))
+        return out
+
+    def int_products(self, bed_rows, n, y_q):
+        """Exact int64 G^T y and O^T y for int8 columns y_q (N x Q, F-order)."""
+        bed_rows = np.ascontiguousarray(bed_rows, dtype=np.uint8)
+        y = np.asfortranarray(y_q, dtype=np.int8)
+        L = bed_rows.shape[0]
+        Q = y.shape[1]
+        out = np.empty((L, Q), dtype=np.int64)
+        obs = np.empty((L, Q), dtype=np.int64)
+        self.lib.orc_int_products(_ptr(bed_rows), bed_rows.shape[1], n, L, _ptr(y), Q,
+                                  _ptr(out), _ptr(obs))
+        return out, obs
+
+    # ------------------------------------------------------------------
+    def gw_ldscore(self, bed_rows, n, annot, nvecs, step, seed, dist="rademacher",
+                   vtile=None, ddof=1, impute="mean", impute_seed=0, as_float=False,
+                   with_mc=False, rows=None, eps=1e-10):
+        """Whole genome-wide estimator on our restatement (FP64 arithmetic).
+
+        Returns a dict with ``ldscore`` (M x K), ``meansq_accum``, ``inv`` and,
+        if requested, the MC fourth-moment sums.
+        """
+        m = bed_rows.shape[0]
+        annot = np.ascontiguousarray(annot, dtype=np.float64)
+        K = annot.shape[1]
+        nsel = n if rows is None else len(rows)
+        blocks = compute_blocks(m, step)
+        vt = bounded_vtile_sizes(nvecs, vtile or nvecs)
+        std = [self.standardize(bed_rows, n, s, e, rows, ddof, impute, impute_seed)[0]
+               for (s, e) in blocks]
+        inv = np.concatenate([self.inv_resvar(g, eps) for g in std])
+        if as_float:
+            inv = inv.astype(np.float32).astype(np.float64)
+        meansq = np.zeros((m, K))
+        mc_agg = np.zeros(K) if with_mc else None
+        mc_snp = np.zeros((m, K)) if with_mc else None
+        N_denom = nsel - ddof + 1
+        v0 = 0
+        for V in vt:
+            Xz = np.empty((nsel, K * V), order="F")
+            init = np.zeros(K, dtype=np.uint8)
+            for (s, e), g in zip(blocks, std):
+                Z = self.probes(seed, s, v0, e - s, V, dist, as_float)
+                self.phase1_block(g, annot[s:e], inv[s:e], Z, Xz, init, as_float)
+            for k in np.flatnonzero(init == 0):
+                Xz[:, k * V:(k + 1) * V] = 0.0
+            for (s, e), g in zip(blocks, std):
+                self.phase2_block(g, s, inv[s:e], V, Xz, meansq, N_denom, mc_agg, mc_snp)
+            v0 += V
+        ld = meansq / float(nvecs) - (annot.sum(axis=0) / float(nsel - ddof))[None, :]
+        return {"ldscore": ld, "meansq_accum": meansq, "inv": inv,
+                "mc_aggregate_sumsq": mc_agg, "mc_per_snp_sumsq": mc_snp}
+
+
+class Reference:
+    """ctypes view of the reference's own gwldcore.cpp, compiled unchanged."""
+
+    def __init__(self, path: Path = REF_SO):
+        if not path.exists():
+            raise RuntimeError(f"reference library missing: {path} (run `make -C oracle ref`)")
+        L = C.CDLL(str(path))
+        L.ref_last_error.restype = _str
+        L.ref_blas_config.restype = _str
+        for t in ("f32", "f64"):
+            getattr(L, f"ref_phase1_bed_{t}").argtypes = [
+                _str, _str, _int, _int, _p, _i64, _int, _p, _i64, _i64, _p, _int, _int, _int,
+                _str, _int, _u64, _p, _i64, _p, _str, _int, _u64, _p]
+            getattr(L, f"ref_phase2_bed_{t}").argtypes = [
+                _str, _str, _int, _int, _p, _i64, _int, _p, _i64, _int, _p, _i64, _i64, _p, _i64,
+                _int, _str, _int, _u64, _p, _p]
+            getattr(L, f"ref_phase2_geno_{t}").argtypes = [
+                _p, _i64, _i64, _int, _p, _int, _p, _i64, _p, _i64, _int, _p, _p]
+            getattr(L, f"ref_phase1_geno_{t}").argtypes = [
+                _p, _i64, _i64, _int, _p, _i64, _p, _int, _int, _int, _str, _int, _u64, _p, _p]
+            getattr(L, f"ref_resvar_bed_{t}").argtypes = [
+                _str, _str, _int, _int, _p, _i64, _int, _dbl, _str, _int, _u64, _p]
+            getattr(L, f"ref_phase1_bed_rowmajor_{t}").argtypes = [
+                _str, _str, _int, _int, _p, _i64, _int, _p, _i64, _i64, _p, _int, _int, _int,
+                _str, _int, _u64, _p, _i64, _str, _int, _u64]
+            getattr(L, f"ref_col_sums_rowmajor_{t}").argtypes = [_p, _i64, _i64, _p]
+            getattr(L, f"ref_phase2_mailman_rowmajor_{t}").argtypes = [
+                _str, _str, _int, _int, _p, _i64, _int, _p, _i64, _int, _p, _i64, _i64, _p, _i64,
+                _p, _int, _int, _u64, _p, _p]
+        L.ref_set_num_threads.argtypes = [_int]
+        self.lib = L
+
+    def _chk(self, rc):
+        if rc:
+            raise RuntimeError(self.lib.ref_last_error().decode())
+
+    def set_threads(self, n: int):
+        self.lib.ref_set_num_threads(int(n))
+
+    def blas_config(self) -> str:
+        return self.lib.ref_blas_config().decode()
+
+    def clear_caches(self):
+        self.lib.ref_clear_caches()
+
+    @staticmethod
+    def _t(dtype):
+        return "f32" if np.dtype(dtype) == np.float32 else "f64"
+
+    def phase1_bed(self, prefix, blk_start, blk_end, annot_blk, inv_right, v_start, v_count,
+                   kmax_hint, rand_dist, seed, Xz, bin_init_mask=None, rows=None, ddof=1,
+                   impute_mode="mean", impute_seed=None, inv_out=None):
+        dt = Xz.dtype
+        t = self._t(dt)
+        annot_blk = np.ascontiguousarray(annot_blk, dtype=dt)
+        inv_right = np.ascontiguousarray(inv_right, dtype=dt)
+        rows_a = None if rows is None else np.ascontiguousarray(rows, dtype=np.int64)
+        fn = getattr(self.lib, f"ref_phase1_bed_{t}")
+        self._chk(fn(f"{prefix}.bed".removesuffix(".bed").encode(), f"{prefix}.fam".encode(),
+                     blk_start, blk_end, _ptr(rows_a), 0 if rows_a is None else rows_a.size, ddof,
+                     _ptr(annot_blk), annot_blk.shape[0], annot_blk.shape[1], _ptr(inv_right),
+                     v_start, v_count, kmax_hint, rand_dist.encode(), int(seed is not None),
+                     0 if seed is None else seed, _ptr(Xz), Xz.shape[0], _ptr(bin_init_mask),
+                     impute_mode.encode(), int(impute_seed is not None),
+                     0 if impute_seed is None else impute_seed, _ptr(inv_out)))
+
+    def phase2_bed(self, prefix, blk_start, blk_end, inv_left, tile_nvecs, Xz, meansq,
+                   N_denom, rows=None, ddof=1, impute_mode="mean", impute_seed=None,
+                   mc_agg=None, mc_per_snp=None):
+        t = self._t(Xz.dtype)
+        inv_left = np.ascontiguousarray(inv_left, dtype=Xz.dtype)
+        rows_a = None if rows is None else np.ascontiguousarray(rows, dtype=np.int64)
+        fn = getattr(self.lib, f"ref_phase2_bed_{t}")
+        self._chk(fn(str(prefix).encode(), f"{prefix}.fam".encode(), blk_start, blk_end,
+                     _ptr(rows_a), 0 if rows_a is None else rows_a.size, ddof, _ptr(inv_left),
+                     inv_left.size, tile_nvecs, _ptr(Xz), Xz.shape[0], Xz.shape[1], _ptr(meansq),
+                     meansq.shape[0], N_denom, impute_mode.encode(), int(impute_seed is not None),
+                     0 if impute_seed is None else impute_seed, _ptr(mc_agg), _ptr(mc_per_snp)))
+
+    def phase2_geno(self, geno, blk_start, inv_left, tile_nvecs, Xz, meansq, N_denom,
+                    mc_agg=None, mc_per_snp=None):
+        t = self._t(Xz.dtype)
+        geno = np.asfortranarray(geno, dtype=Xz.dtype)
+        inv_left = np.ascontiguousarray(inv_left, dtype=Xz.dtype)
+        fn = getattr(self.lib, f"ref_phase2_geno_{t}")
+        self._chk(fn(_ptr(geno), geno.shape[0], geno.shape[1], blk_start, _ptr(inv_left),
+                     tile_nvecs, _ptr(Xz), Xz.shape[1], _ptr(meansq), meansq.shape[0], N_denom,
+                     _ptr(mc_agg), _ptr(mc_per_snp)))
+
+    def resvar_bed(self, prefix, nsnps, step, dtype=np.float64, rows=None, ddof=1, eps=1e-10,
+                   impute_mode="mean", impute_seed=None):
+        t = self._t(dtype)
+        out = np.empty(nsnps, dtype=dtype)
+        rows_a = None if rows is None else np.ascontiguousarray(rows, dtype=np.int64)
+        fn = getattr(self.lib, f"ref_resvar_bed_{t}")
+        self._chk(fn(str(prefix).encode(), f"{prefix}.fam".encode(), nsnps, step, _ptr(rows_a),
+                     0 if rows_a is None else rows_a.size, ddof, eps, impute_mode.encode(),
+                     int(impute_seed is not None), 0 if impute_seed is None else impute_seed,
+                     _ptr(out)))
+        return out
+
+    def gw_ldscore(self, prefix, n, m, annot, nvecs, step, seed, dist="rademacher", vtile=None,
+                   ddof=1, impute="mean", impute_seed=0, dtype=np.float64, with_mc=False,
+                   rows=None, eps=1e-10):
+        """The reference's per-block native calls in the order of
+        GenomewideLDScore._compute_ldscore (gw_ldscore.py:1753-2222)."""
+        annot = np.ascontiguousarray(annot, dtype=dtype)
+        K = annot.shape[1]
+        nsel = n if rows is None else len(rows)
+        blocks = compute_blocks(m, step)
+        vt = bounded_vtile_sizes(nvecs, vtile or nvecs)
+        inv = np.empty(m, dtype=dtype)
+        meansq = np.zeros((m, K), dtype=dtype)
+        mc_agg = np.zeros(K) if with_mc else None
+        mc_snp = np.zeros((m, K)) if with_mc else None
+        N_denom = nsel - ddof + 1
+        kmax = [int((annot[s:e] != 0).sum(axis=0).max()) for (s, e) in blocks]
+        Xz_chunk = np.empty((nsel, K * max(vt)), dtype=dtype, order="F")
+        init = np.empty(K, dtype=np.uint8)
+        # The phase-1 CSR cache is keyed by array addresses; the driver clears
+        # it around every run (gw_ldscore.py:1775, :2151).
+        self.clear_caches()
+        v0 = 0
+        for ti, V in enumerate(vt):
+            fuse = ti == 0
+            Xz = Xz_chunk[:, :K * V]
+            init.fill(0)
+            for bi, (s, e) in enumerate(blocks):
+                if kmax[bi] == 0 and not fuse:
+                    continue
+                self.phase1_bed(prefix, s, e, annot[s:e], inv[s:e], v0, V, kmax[bi], dist, seed,
+                                Xz, init, rows, ddof, impute, impute_seed,
+                                inv_out=inv[s:e] if fuse else None)
+            for k in np.flatnonzero(init == 0):
+                Xz[:, k * V:(k + 1) * V] = 0
+            for (s, e) in blocks:
+                self.phase2_bed(prefix, s, e, inv[s:e], V, Xz, meansq, N_denom, rows, ddof,
+                                impute, impute_seed, mc_agg, mc_snp)
+            v0 += V
+        self.clear_caches()
+        ms = (meansq / float(nvecs)).astype(dtype)
+        ld = ms - (annot.sum(axis=0, dtype=np.float64) / float(nsel - ddof)).astype(dtype)[None, :]
+        return {"ldscore": ld.astype(np.float64), "meansq_accum": meansq, "inv": inv,
+                "mc_aggregate_sumsq": mc_agg, "mc_per_snp_sumsq": mc_snp}

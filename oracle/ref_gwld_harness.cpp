@@ -1,0 +1,247 @@
+// Oracle harness: compiles the reference's gwldcore.cpp UNCHANGED (through the
+// nanobind-subset shim in oracle/nbshim) and exposes its implementation
+// functions through a plain C ABI so tests and the CPU-baseline leg of the
+// benchmark can call the reference's own code path.  Test infrastructure only.
+//
+// Built by oracle/Makefile into oracle/_ref/libref_gwld.so from the sources
+// where they lie in the reference tree (src/native/gwldcore.cpp,
+// src/native/common/genotype.cpp).
+#include "gwldcore.cpp"
+
+#include <cstdio>
+#include <string>
+
+namespace {
+
+thread_local std::string g_ref_err;
+
+template <typename T>
+nb::object arr(T* p, std::initializer_list<size_t> shape) {
+    if (!p) return nb::none();
+    return nb::object(nb::ndarray<T>(p, shape));
+}
+
+nb::object opt_u64(int has, uint64_t v) {
+    return has ? nb::object::from_uint(v) : nb::none();
+}
+
+nb::object rows_obj(const int64_t* rows, int64_t n) {
+    if (!rows) return nb::none();
+    return arr(const_cast<int64_t*>(rows), {(size_t)n});
+}
+
+template <typename F>
+int guarded(F&& f) {
+    try {
+        f();
+        return 0;
+    } catch (const std::exception& e) {
+        g_ref_err = e.what();
+        return -1;
+    }
+}
+
+template <typename T>
+int phase1_bed(const char* bed_prefix, const char* fam_path, int blk_start, int blk_end,
+               const int64_t* rows, int64_t n_rows, int ddof,
+               const T* annot, int64_t L, int64_t K, const T* inv_right,
+               int v_start, int v_count, int kmax_hint, const char* rand_dist,
+               int has_seed, uint64_t seed, T* Xz, int64_t N, uint8_t* bin_init_mask,
+               const char* impute_mode, int has_impute_seed, uint64_t impute_seed,
+               T* inv_out) {
+    return guarded([&] {
+        nb_mat2c_ro<T> ann(const_cast<T*>(annot), {(size_t)L, (size_t)K});
+        nb_mat2f_rw<T> xz(Xz, {(size_t)N, (size_t)(K * v_count)});
+        phase1_compute_Xz_bed_chunk_impl<T>(
+            bed_prefix, fam_path, blk_start, blk_end, rows_obj(rows, n_rows), ddof,
+            ann, arr(const_cast<T*>(inv_right), {(size_t)L}), v_start, v_count, kmax_hint,
+            rand_dist, opt_u64(has_seed, seed), xz,
+            bin_init_mask ? arr(bin_init_mask, {(size_t)K}) : nb::none(), false,
+            nb::none(), nb::none(), impute_mode, opt_u64(has_impute_seed, impute_seed),
+            nb::none(), inv_out ? arr(inv_out, {(size_t)L}) : nb::none(), 1e-10);
+    });
+}
+
+template <typename T>
+int phase1_geno(T* geno, int64_t N, int64_t L, int blk_start, const T* annot, int64_t K,
+                const T* inv_right, int v_start, int v_count, int kmax_hint,
+                const char* rand_dist, int has_seed, uint64_t seed, T* Xz,
+                uint8_t* bin_init_mask) {
+    return guarded([&] {
+        nb_mat2f_rw<T> g(geno, {(size_t)N, (size_t)L});
+        nb_mat2c_ro<T> ann(const_cast<T*>(annot), {(size_t)L, (size_t)K});
+        nb_mat2f_rw<T> xz(Xz, {(size_t)N, (size_t)(K * v_count)});
+        phase1_compute_Xz_geno_chunk_impl<T>(
+            g, blk_start, ann, arr(const_cast<T*>(inv_right), {(size_t)L}), v_start, v_count,
+            kmax_hint, rand_dist, opt_u64(has_seed, seed), xz,
+            bin_init_mask ? arr(bin_init_mask, {(size_t)K}) : nb::none(),
+            nb::none(), nb::none(), nb::none(), nb::none(), 1e-10);
+    });
+}
+
+template <typename T>
+int phase2_bed(const char* bed_prefix, const char* fam_path, int blk_start, int blk_end,
+               const int64_t* rows, int64_t n_rows, int ddof, const T* inv_left, int64_t L,
+               int tile_nvecs, const T* Xz, int64_t N, int64_t Q, T* meansq, int64_t M,
+               int N_denom, const char* impute_mode, int has_impute_seed, uint64_t impute_seed,
+               double* mc_agg, double* mc_per_snp) {
+    return guarded([&] {
+        const int64_t K = Q / tile_nvecs;
+        nb_mat2f_ro<T> xz(const_cast<T*>(Xz), {(size_t)N, (size_t)Q});
+        nb_mat2c_rw<T> ms(meansq, {(size_t)M, (size_t)K});
+        phase2_accum_XtXz_bed_impl<T>(
+            bed_prefix, fam_path, blk_start, blk_end, rows_obj(rows, n_rows), ddof,
+            nb_vec1_ro<T>(const_cast<T*>(inv_left), {(size_t)L}), tile_nvecs, xz, ms,
+            nb::none(), nb::none(), N_denom, impute_mode, opt_u64(has_impute_seed, impute_seed),
+            mc_agg ? arr(mc_agg, {(size_t)K}) : nb::none(),
+            mc_per_snp ? arr(mc_per_snp, {(size_t)M, (size_t)K}) : nb::none());
+    });
+}
+
+template <typename T>
+int phase2_geno(T* geno, int64_t N, int64_t L, int blk_start, const T* inv_left,
+                int tile_nvecs, const T* Xz, int64_t Q, T* meansq, int64_t M, int N_denom,
+                double* mc_agg, double* mc_per_snp) {
+    return guarded([&] {
+        const int64_t K = Q / tile_nvecs;
+        nb_mat2f_rw<T> g(geno, {(size_t)N, (size_t)L});
+        nb_mat2f_ro<T> xz(const_cast<T*>(Xz), {(size_t)N, (size_t)Q});
+        nb_mat2c_rw<T> ms(meansq, {(size_t)M, (size_t)K});
+        phase2_accum_XtXz_geno_impl<T>(
+            g, blk_start, nb_vec1_ro<T>(const_cast<T*>(inv_left), {(size_t)L}), tile_nvecs, xz,
+            ms, nb::none(), nb::none(), N_denom,
+            mc_agg ? arr(mc_agg, {(size_t)K}) : nb::none(),
+            mc_per_snp ? arr(mc_per_snp, {(size_t)M, (size_t)K}) : nb::none());
+    });
+}
+
+template <typename T>
+int resvar_bed(const char* bed_prefix, const char* fam_path, int nsnps, int step_size,
+               const int64_t* rows, int64_t n_rows, int ddof, double eps,
+               const char* impute_mode, int has_impute_seed, uint64_t impute_seed, T* inv_out) {
+    return guarded([&] {
+        nb::tuple t = precompute_residual_variances_bed_impl<T>(
+            bed_prefix, fam_path, nsnps, step_size, rows_obj(rows, n_rows), ddof, eps, false,
+            nb::none(), nb::none(), nb::none(), impute_mode,
+            opt_u64(has_impute_seed, impute_seed), nb::none());
+        const nb::object o = t[0];
+        std::memcpy(inv_out, o.a_.data, sizeof(T) * (size_t)nsnps);
+    });
+}
+
+template <typename T>
+int phase1_bed_rowmajor(const char* bed_prefix, const char* fam_path, int blk_start,
+                        int blk_end, const int64_t* rows, int64_t n_rows, int ddof,
+                        const T* annot, int64_t L, int64_t K, const T* inv_right, int v_start,
+                        int v_count, int kmax_hint, const char* rand_dist, int has_seed,
+                        uint64_t seed, T* Xz, int64_t N, const char* impute_mode,
+                        int has_impute_seed, uint64_t impute_seed) {
+    return guarded([&] {
+        nb_mat2c_ro<T> ann(const_cast<T*>(annot), {(size_t)L, (size_t)K});
+        nb_mat2c_rw<T> xz(Xz, {(size_t)N, (size_t)(K * v_count)});
+        phase1_compute_Xz_bed_chunk_rowmajor_impl<T>(
+            bed_prefix, fam_path, blk_start, blk_end, rows_obj(rows, n_rows), ddof, ann,
+            arr(const_cast<T*>(inv_right), {(size_t)L}), v_start, v_count, kmax_hint, rand_dist,
+            opt_u64(has_seed, seed), xz, false, nb::none(), nb::none(), impute_mode,
+            opt_u64(has_impute_seed, impute_seed), nb::none(), nb::none(), 1e-10);
+    });
+}
+
+template <typename T>
+int col_sums_rowmajor(const T* Xz, int64_t N, int64_t Q, double* out) {
+    return guarded([&] {
+        nb_mat2c_ro<T> xz(const_cast<T*>(Xz), {(size_t)N, (size_t)Q});
+        auto r = compute_col_sums_rowmajor_impl<T>(xz);
+        std::memcpy(out, r.data(), sizeof(double) * (size_t)Q);
+    });
+}
+
+template <typename T>
+int phase2_mailman_rowmajor(const char* bed_prefix, const char* fam_path, int blk_start,
+                            int blk_end, const int64_t* rows, int64_t n_rows, int ddof,
+                            const T* inv_left, int64_t L, int tile_nvecs, const T* Xz, int64_t N,
+                            int64_t Q, T* meansq, int64_t M, const double* sum_Xz, int N_denom,
+                            int has_impute_seed, uint64_t impute_seed, double* mc_agg,
+                            double* mc_per_snp) {
+    return guarded([&] {
+        const int64_t K = Q / tile_nvecs;
+        nb_mat2c_ro<T> xz(const_cast<T*>(Xz), {(size_t)N, (size_t)Q});
+        nb_mat2c_rw<T> ms(meansq, {(size_t)M, (size_t)K});
+        phase2_accum_XtXz_bed_mailman_rm_impl<T>(
+            bed_prefix, fam_path, blk_start, blk_end, rows_obj(rows, n_rows), ddof,
+            nb_vec1_ro<T>(const_cast<T*>(inv_left), {(size_t)L}), tile_nvecs, xz, ms,
+            nb_vec1_ro<double>(const_cast<double*>(sum_Xz), {(size_t)Q}), N_denom,
+            opt_u64(has_impute_seed, impute_seed),
+            mc_agg ? arr(mc_agg, {(size_t)K}) : nb::none(),
+            mc_per_snp ? arr(mc_per_snp, {(size_t)M, (size_t)K}) : nb::none());
+    });
+}
+
+}  // namespace
+
+#define REF_EXPORT extern "C" __attribute__((visibility("default")))
+
+REF_EXPORT const char* ref_last_error() { return g_ref_err.c_str(); }
+REF_EXPORT void ref_set_num_threads(int n) {
+    set_num_threads(n);
+    openblas_set_num_threads(n);
+}
+REF_EXPORT int ref_get_max_threads() { return get_max_threads(); }
+REF_EXPORT const char* ref_blas_config() { return openblas_get_config(); }
+REF_EXPORT void ref_clear_caches() {
+    clear_phase1_csr_cache();
+    clear_bed_mapping_cache();
+}
+
+#define REF_BOTH(NAME, SIG_F, CALL_F, SIG_D, CALL_D) \
+    REF_EXPORT int NAME##_f32 SIG_F { return CALL_F; } \
+    REF_EXPORT int NAME##_f64 SIG_D { return CALL_D; }
+
+#define P1_SIG(T) (const char* bp, const char* fam, int bs, int be, const int64_t* rows, \
+    int64_t nr, int ddof, const T* annot, int64_t L, int64_t K, const T* inv, int vs, int vc, \
+    int kmax, const char* rd, int hs, uint64_t seed, T* Xz, int64_t N, uint8_t* bim, \
+    const char* im, int his, uint64_t iseed, T* inv_out)
+#define P1_CALL(T) phase1_bed<T>(bp, fam, bs, be, rows, nr, ddof, annot, L, K, inv, vs, vc, \
+    kmax, rd, hs, seed, Xz, N, bim, im, his, iseed, inv_out)
+REF_BOTH(ref_phase1_bed, P1_SIG(float), P1_CALL(float), P1_SIG(double), P1_CALL(double))
+
+#define P1G_SIG(T) (T* g, int64_t N, int64_t L, int bs, const T* annot, int64_t K, const T* inv, \
+    int vs, int vc, int kmax, const char* rd, int hs, uint64_t seed, T* Xz, uint8_t* bim)
+#define P1G_CALL(T) phase1_geno<T>(g, N, L, bs, annot, K, inv, vs, vc, kmax, rd, hs, seed, Xz, bim)
+REF_BOTH(ref_phase1_geno, P1G_SIG(float), P1G_CALL(float), P1G_SIG(double), P1G_CALL(double))
+
+#define P2_SIG(T) (const char* bp, const char* fam, int bs, int be, const int64_t* rows, \
+    int64_t nr, int ddof, const T* inv, int64_t L, int tv, const T* Xz, int64_t N, int64_t Q, \
+    T* ms, int64_t M, int nd, const char* im, int his, uint64_t iseed, double* mca, double* mcp)
+#define P2_CALL(T) phase2_bed<T>(bp, fam, bs, be, rows, nr, ddof, inv, L, tv, Xz, N, Q, ms, M, \
+    nd, im, his, iseed, mca, mcp)
+REF_BOTH(ref_phase2_bed, P2_SIG(float), P2_CALL(float), P2_SIG(double), P2_CALL(double))
+
+#define P2G_SIG(T) (T* g, int64_t N, int64_t L, int bs, const T* inv, int tv, const T* Xz, \
+    int64_t Q, T* ms, int64_t M, int nd, double* mca, double* mcp)
+#define P2G_CALL(T) phase2_geno<T>(g, N, L, bs, inv, tv, Xz, Q, ms, M, nd, mca, mcp)
+REF_BOTH(ref_phase2_geno, P2G_SIG(float), P2G_CALL(float), P2G_SIG(double), P2G_CALL(double))
+
+#define RV_SIG(T) (const char* bp, const char* fam, int nsnps, int step, const int64_t* rows, \
+    int64_t nr, int ddof, double eps, const char* im, int his, uint64_t iseed, T* inv_out)
+#define RV_CALL(T) resvar_bed<T>(bp, fam, nsnps, step, rows, nr, ddof, eps, im, his, iseed, inv_out)
+REF_BOTH(ref_resvar_bed, RV_SIG(float), RV_CALL(float), RV_SIG(double), RV_CALL(double))
+
+#define P1R_SIG(T) (const char* bp, const char* fam, int bs, int be, const int64_t* rows, \
+    int64_t nr, int ddof, const T* annot, int64_t L, int64_t K, const T* inv, int vs, int vc, \
+    int kmax, const char* rd, int hs, uint64_t seed, T* Xz, int64_t N, const char* im, int his, \
+    uint64_t iseed)
+#define P1R_CALL(T) phase1_bed_rowmajor<T>(bp, fam, bs, be, rows, nr, ddof, annot, L, K, inv, vs, \
+    vc, kmax, rd, hs, seed, Xz, N, im, his, iseed)
+REF_BOTH(ref_phase1_bed_rowmajor, P1R_SIG(float), P1R_CALL(float), P1R_SIG(double), P1R_CALL(double))
+
+#define CS_SIG(T) (const T* Xz, int64_t N, int64_t Q, double* out)
+#define CS_CALL(T) col_sums_rowmajor<T>(Xz, N, Q, out)
+REF_BOTH(ref_col_sums_rowmajor, CS_SIG(float), CS_CALL(float), CS_SIG(double), CS_CALL(double))
+
+#define P2M_SIG(T) (const char* bp, const char* fam, int bs, int be, const int64_t* rows, \
+    int64_t nr, int ddof, const T* inv, int64_t L, int tv, const T* Xz, int64_t N, int64_t Q, \
+    T* ms, int64_t M, const double* sxz, int nd, int his, uint64_t iseed, double* mca, double* mcp)
+#define P2M_CALL(T) phase2_mailman_rowmajor<T>(bp, fam, bs, be, rows, nr, ddof, inv, L, tv, Xz, N, \
+    Q, ms, M, sxz, nd, his, iseed, mca, mcp)
+REF_BOTH(ref_phase2_mailman_rowmajor, P2M_SIG(float), P2M_CALL(float), P2M_SIG(double), P2M_CALL(double))
