@@ -1,0 +1,194 @@
+/*
+ * lds.h — C ABI of liblds.so, the B200 implementation of SUMMIT's genotype x
+ * probe hot path (BED decode, X.W and X^T.(X.W) over probe blocks with
+ * on-the-fly centering and scaling, and the LD-score reductions on top).
+ *
+ * The reference exposes this path as nanobind Python functions (module
+ * `gwldcore`, src/native/gwldcore.cpp:3656-3829).  Each entry point below is
+ * the plain-C counterpart of one of them: host pointers and sizes, no Python
+ * or torch types.  Arrays keep the reference's layouts:
+ *   - Xz2d / Geno / C / R: column-major (Fortran order);
+ *   - annot_blk, meansq_accum, mc_per_snp_sumsq: row-major (C order);
+ *   - `_f32` / `_f64` suffixes select float32 / float64 arrays, like the
+ *     nanobind overloads.
+ * Optional arrays are passed as NULL.  Optional integers (seed, impute_seed)
+ * come with a `has_` flag.  Every function returns 0 on success and a
+ * negative code on failure; lds_last_error() then holds the message, which
+ * the Python shim raises as RuntimeError (the reference raises
+ * std::runtime_error -> RuntimeError with the same wording where it has one).
+ *
+ * Computation runs on the current CUDA device.  There is no CPU fallback:
+ * without a usable device every compute entry returns LDS_ERR_CUDA.
+ */
+#ifndef LDS_H
+#define LDS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LDS_OK 0
+#define LDS_ERR_ARG -1
+#define LDS_ERR_CUDA -2
+#define LDS_ERR_IO -3
+#define LDS_ERR_INTERNAL -4
+
+/* Probe distributions (gwldcore.cpp:1693-1716). */
+#define LDS_DIST_RADEMACHER 0
+#define LDS_DIST_GAUSSIAN 1
+#define LDS_DIST_SPHERICAL 2
+
+/* Imputation modes (genotype.hpp:33-36, ImputeMode). */
+#define LDS_IMPUTE_MEAN 0
+#define LDS_IMPUTE_HWE 1
+
+/* Thread-local text of the last error. */
+const char* lds_last_error(void);
+
+/* Library build information ("liblds <version> sm_100a ..."). */
+const char* lds_version(void);
+
+/* Number of visible CUDA devices (0 when no driver/device). */
+int lds_device_count(void);
+
+/* Number of int8 digit slices used for floating operands (3..6, default 4).
+ * Higher = closer to FP64 at proportional tensor-core cost. */
+int lds_set_slices(int slices);
+int lds_get_slices(void);
+
+/* Counters of the library's own CUDA kernel launches since process start
+ * (all kernels) — used to report launches inside timed regions. */
+uint64_t lds_kernel_launches(void);
+
+/* Release cached device genotype images and workspaces
+ * (clear_gwld_native_scratch, gwldcore.cpp:194-200; _clear_bed_mapping_cache,
+ * :3668). */
+void lds_clear_device_cache(void);
+
+/* ---------------------------------------------------------------------
+ * Phase 1: Xz2d[:, k*v_count+c] (+)= sum_{j in bin k} x_j * z_jc * inv_j*sqrt(a_jk)
+ * for SNP block [blk_start, blk_end) of a PLINK BED fileset.
+ * Replaces gwldcore.phase1_compute_Xz_bed_chunk (gwldcore.cpp:3673-3688,
+ * implementation :1582-1894).  Xz2d is N x (K*v_count), column-major,
+ * updated in place; bin_init_mask (K bytes, may be NULL) selects beta = 0
+ * for a bin's first write and is set to 1 for bins written.  When inv_out is
+ * given, residual variances of the block are computed into it and used in
+ * place of inv_right (fused residual variance, :1659-1669).
+ * project_right / covariates are not supported by this entry (the caller
+ * projects Xz2d afterwards, as gw_ldscore.py does).
+ * ------------------------------------------------------------------- */
+int lds_phase1_compute_Xz_bed_chunk_f32(
+    const char* bed_prefix, const char* fam_path, int blk_start, int blk_end,
+    const int64_t* row_sel, int64_t n_row_sel, int ddof, const float* annot_blk,
+    int64_t annot_rows, int64_t K, const float* inv_right, int v_start, int v_count,
+    int kmax_hint, int rand_dist, int has_seed, uint64_t seed, float* Xz2d_chunk,
+    int64_t xz_rows, int64_t xz_cols, uint8_t* bin_init_mask, int impute_mode,
+    int has_impute_seed, uint64_t impute_seed, float* inv_out, double resvar_eps);
+int lds_phase1_compute_Xz_bed_chunk_f64(
+    const char* bed_prefix, const char* fam_path, int blk_start, int blk_end,
+    const int64_t* row_sel, int64_t n_row_sel, int ddof, const double* annot_blk,
+    int64_t annot_rows, int64_t K, const double* inv_right, int v_start, int v_count,
+    int kmax_hint, int rand_dist, int has_seed, uint64_t seed, double* Xz2d_chunk,
+    int64_t xz_rows, int64_t xz_cols, uint8_t* bin_init_mask, int impute_mode,
+    int has_impute_seed, uint64_t impute_seed, double* inv_out, double resvar_eps);
+
+/* ---------------------------------------------------------------------
+ * Phase 2: Work = X_blk^T Xz2d; meansq_accum[blk_start+j, k] +=
+ * max(0, sum_{c in bin k} Work_jc^2 * inv_j^2 / (N_denom-1)^2) with the
+ * reference's non-finite / extreme-update guards, and the optional
+ * fourth-moment sums.  Replaces gwldcore.phase2_accum_XtXz_bed
+ * (gwldcore.cpp:3759-3770, implementation :2329-2600).  Xz2d is N x Q
+ * column-major with Q = K*tile_nvecs; meansq_accum is M x K row-major;
+ * mc_aggregate_sumsq (K doubles) and mc_per_snp_sumsq (M x K doubles) may be
+ * NULL.
+ * ------------------------------------------------------------------- */
+int lds_phase2_accum_XtXz_bed_f32(
+    const char* bed_prefix, const char* fam_path, int blk_start, int blk_end,
+    const int64_t* row_sel, int64_t n_row_sel, int ddof, const float* inv_left, int64_t L,
+    int tile_nvecs, const float* Xz2d, int64_t xz_rows, int64_t xz_cols, float* meansq_accum,
+    int64_t M_rows, int64_t K, int N_denom, int impute_mode, int has_impute_seed,
+    uint64_t impute_seed, double* mc_aggregate_sumsq, double* mc_per_snp_sumsq);
+int lds_phase2_accum_XtXz_bed_f64(
+    const char* bed_prefix, const char* fam_path, int blk_start, int blk_end,
+    const int64_t* row_sel, int64_t n_row_sel, int ddof, const double* inv_left, int64_t L,
+    int tile_nvecs, const double* Xz2d, int64_t xz_rows, int64_t xz_cols,
+    double* meansq_accum, int64_t M_rows, int64_t K, int N_denom, int impute_mode,
+    int has_impute_seed, uint64_t impute_seed, double* mc_aggregate_sumsq,
+    double* mc_per_snp_sumsq);
+
+/* ---------------------------------------------------------------------
+ * Residual variances: inv[j] = 1/sqrt(max(eps, ||x_j||^2 / (N-1))) for all
+ * nsnps SNPs, without covariates.  Replaces
+ * gwldcore.precompute_residual_variances_bed (gwldcore.cpp:3748-3757,
+ * implementation :3335-3566) for C = R = None and compute_mu22 = False.
+ * ------------------------------------------------------------------- */
+int lds_precompute_residual_variances_bed_f32(
+    const char* bed_prefix, const char* fam_path, int nsnps, int step_size,
+    const int64_t* row_sel, int64_t n_row_sel, int ddof, double eps, int impute_mode,
+    int has_impute_seed, uint64_t impute_seed, float* inv_out);
+int lds_precompute_residual_variances_bed_f64(
+    const char* bed_prefix, const char* fam_path, int nsnps, int step_size,
+    const int64_t* row_sel, int64_t n_row_sel, int ddof, double eps, int impute_mode,
+    int has_impute_seed, uint64_t impute_seed, double* inv_out);
+
+/* ---------------------------------------------------------------------
+ * Whole genome-wide LD-score estimate in one call (all V-tiles, all SNP
+ * blocks, residual variances, phase 1, untouched-bin zeroing, phase 2,
+ * division by the probe count and the M_k/N_denom null), i.e. the native
+ * work of GenomewideLDScore._compute_ldscore (gw_ldscore.py:1753-2222)
+ * without covariates.  The genotype image stays on the device for the whole
+ * call; probes follow the reference's per-block mt19937_64 streams, so the
+ * result equals the reference's on the same seed, blocks and V-tiles.
+ *
+ * bed_rows: SNP-major packed BED rows (no 3-byte header), M rows of
+ *   bed_row_bytes >= ceil(n_total/4) bytes, host memory.
+ * annot: M x K row-major float64.  ldscore / meansq_accum: M x K float64
+ *   outputs.  inv_out (M, may be NULL).  mc_* may be NULL.
+ * as_float != 0 reproduces the float32 path's inputs (float probes and
+ *   float-rounded residual variances).
+ * ------------------------------------------------------------------- */
+int lds_gw_ldscore(
+    const uint8_t* bed_rows, int64_t bed_row_bytes, int64_t n_total, int64_t M,
+    const int64_t* row_sel, int64_t n_row_sel, const double* annot, int64_t K,
+    int nvecs, int step_size, int vtile, uint64_t seed, int rand_dist, int ddof,
+    int impute_mode, uint64_t impute_seed, double resvar_eps, int as_float,
+    double* ldscore, double* meansq_accum, double* inv_out,
+    double* mc_aggregate_sumsq, double* mc_per_snp_sumsq);
+
+/* Same as lds_gw_ldscore, reading the fileset `bed_prefix`.bed/.bim/.fam. */
+int lds_gw_ldscore_bed(
+    const char* bed_prefix, const char* fam_path, const int64_t* row_sel,
+    int64_t n_row_sel, const double* annot, int64_t K, int nvecs, int step_size, int vtile,
+    uint64_t seed, int rand_dist, int ddof, int impute_mode, uint64_t impute_seed,
+    double resvar_eps, int as_float, double* ldscore, double* meansq_accum,
+    double* inv_out, double* mc_aggregate_sumsq, double* mc_per_snp_sumsq);
+
+/* Device timing of the last lds_gw_ldscore call (milliseconds, CUDA events
+ * on the library stream): [0] upload+prepare, [1] phase 1 total, [2] phase 2
+ * total, [3] whole call. */
+int lds_last_timings(double* ms_out, int n);
+
+/* Verification entry: exact int64 products G^T y and O^T y of the int8
+ * columns y (n x Q, column-major) with the genotype rows of `bed_rows`
+ * (L SNP rows of bed_row_bytes bytes, n samples), computed by the same int8
+ * tensor-core phase-2 kernel as the LD-score path (one digit).  out_g/out_o:
+ * L x Q row-major.  No reference counterpart: it exposes the exact-integer
+ * core of the phase-2 product (gwldcore.cpp:2490 Geno^T.Xz) for testing. */
+int lds_debug_xt_products(const uint8_t* bed_rows, int64_t bed_row_bytes, int64_t n, int64_t L,
+                          const int8_t* y, int64_t Q, int64_t* out_g, int64_t* out_o);
+
+/* Synthetic genotype image generated on the device with the integer-exact
+ * generator (identical bytes to the numpy generator in bedfile.py):
+ * writes M rows of ceil(n/4) bytes to host memory `out`.  t0/t1 are the
+ * per-SNP integer latent thresholds. */
+int lds_synth_bed(int64_t n, int64_t M, uint64_t seed, const int64_t* t0, const int64_t* t1,
+                  int missing, uint8_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LDS_H */

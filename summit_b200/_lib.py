@@ -1,0 +1,85 @@
+"""ctypes binding of liblds.so (declarations in include/lds.h).
+
+The library is built in-tree by ``summit_b200.build`` (nvcc, sm_100a).  There is
+no fallback: if the shared object is missing, importing the compute API raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "liblds.so"
+
+LDS_DIST = {"rademacher": 0, "gaussian": 1, "normal": 1, "spherical": 2}
+LDS_IMPUTE = {"mean": 0, "hwe": 1}
+
+_p = C.c_void_p
+_i64 = C.c_int64
+_u64 = C.c_uint64
+_int = C.c_int
+_dbl = C.c_double
+_str = C.c_char_p
+
+# name -> (restype, argtypes); mirrors include/lds.h.
+SIGNATURES: dict[str, tuple] = {
+    "lds_last_error": (_str, []),
+    "lds_version": (_str, []),
+    "lds_device_count": (_int, []),
+    "lds_set_slices": (_int, [_int]),
+    "lds_get_slices": (_int, []),
+    "lds_kernel_launches": (_u64, []),
+    "lds_clear_device_cache": (None, []),
+    "lds_last_timings": (_int, [_p, _int]),
+    "lds_gw_ldscore": (_int, [_p, _i64, _i64, _i64, _p, _i64, _p, _i64, _int, _int, _int, _u64,
+                              _int, _int, _int, _u64, _dbl, _int, _p, _p, _p, _p, _p]),
+    "lds_gw_ldscore_bed": (_int, [_str, _str, _p, _i64, _p, _i64, _int, _int, _int, _u64, _int,
+                                  _int, _int, _u64, _dbl, _int, _p, _p, _p, _p, _p]),
+    "lds_debug_xt_products": (_int, [_p, _i64, _i64, _i64, _p, _i64, _p, _p]),
+    "lds_synth_bed": (_int, [_i64, _i64, _u64, _p, _p, _int, _p]),
+}
+for _t in ("f32", "f64"):
+    SIGNATURES[f"lds_phase1_compute_Xz_bed_chunk_{_t}"] = (
+        _int, [_str, _str, _int, _int, _p, _i64, _int, _p, _i64, _i64, _p, _int, _int, _int, _int,
+               _int, _u64, _p, _i64, _i64, _p, _int, _int, _u64, _p, _dbl])
+    SIGNATURES[f"lds_phase2_accum_XtXz_bed_{_t}"] = (
+        _int, [_str, _str, _int, _int, _p, _i64, _int, _p, _i64, _int, _p, _i64, _i64, _p, _i64,
+               _i64, _int, _int, _int, _u64, _p, _p])
+    SIGNATURES[f"lds_precompute_residual_variances_bed_{_t}"] = (
+        _int, [_str, _str, _int, _int, _p, _i64, _int, _dbl, _int, _int, _u64, _p])
+
+_LIB = None
+
+
+def load() -> C.CDLL:
+    """Load liblds.so (once).  Raises RuntimeError if it is not built."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not LIB_PATH.exists():
+        raise RuntimeError(
+            f"liblds.so not found at {LIB_PATH}; build it with `python -m summit_b200.build` "
+            "(there is no CPU fallback)")
+    lib = C.CDLL(str(LIB_PATH))
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = lib
+    return lib
+
+
+def check(rc: int) -> None:
+    if rc != 0:
+        raise RuntimeError(load().lds_last_error().decode(errors="replace"))
+
+
+def ptr(a):
+    return None if a is None else a.ctypes.data_as(_p)
+
+
+def enc(s) -> bytes:
+    return os.fsencode(str(s))

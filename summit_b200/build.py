@@ -1,0 +1,44 @@
+"""Build liblds.so in-tree for sm_100a (``python -m summit_b200.build``)."""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+CSRC = PKG / "csrc"
+OUT = PKG / "liblds.so"
+SOURCES = ["lds_kernels.cu", "lds_host.cu"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and Path(cand).exists():
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    deps = [CSRC / s for s in SOURCES] + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + [
+        PKG.parent / "include" / "lds.h"]
+    if OUT.exists() and not force:
+        newest = max(p.stat().st_mtime for p in deps if p.exists())
+        if OUT.stat().st_mtime >= newest:
+            return OUT
+    cmd = [nvcc(), *ARCH, "-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
+           "-Xcompiler", "-fvisibility=hidden", "-shared", "-cudart", "static",
+           *[str(CSRC / s) for s in SOURCES], "-o", str(OUT)]
+    if verbose:
+        print(" ".join(cmd))
+    tmp_out = OUT.with_suffix(".so.tmp")
+    cmd[-1] = str(tmp_out)
+    subprocess.run(cmd, check=True)
+    os.replace(tmp_out, OUT)
+    return OUT
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose=True))

@@ -1,0 +1,1103 @@
+// Host side of liblds.so: C ABI (include/lds.h), device genotype cache,
+// per-SNP statistics, probe streams, and the phase-1 / phase-2 orchestration.
+//
+// Floating-point statistics that must match the reference bit for bit
+// (means, inverse sds, residual variances, HWE thresholds) are computed on
+// the host from exact integer code counts produced on the device, with the
+// reference's formulas (genotype.cpp:629-689, gwldcore.cpp:3220-3333).
+#include <algorithm>
+#include <atomic>
+#include <cerrno>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <fcntl.h>
+#include <limits>
+#include <list>
+#include <memory>
+#include <mutex>
+#include <random>
+#include <stdexcept>
+#include <string>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <thread>
+#include <unistd.h>
+#include <vector>
+
+#include "../../include/lds.h"
+#include "lds_device.cuh"
+#include "lds_internal.h"
+
+namespace lds {
+
+static std::atomic<unsigned long long> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+namespace {
+
+thread_local std::string g_err;
+
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+[[noreturn]] void fail(int code, const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    throw Error(code, buf);
+}
+
+void ck(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) fail(LDS_ERR_CUDA, "CUDA error in %s: %s", what, cudaGetErrorString(e));
+}
+
+template <typename F>
+int guarded(F&& f) {
+    try {
+        f();
+        return LDS_OK;
+    } catch (const Error& e) {
+        g_err = e.what();
+        return e.code;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return LDS_ERR_INTERNAL;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Device buffers
+// ---------------------------------------------------------------------------
+struct DevBuf {
+    void* p = nullptr;
+    size_t n = 0;
+    void* get(size_t bytes) {
+        if (bytes <= n && p) return p;
+        release();
+        if (bytes == 0) bytes = 16;
+        ck(cudaMalloc(&p, bytes), "cudaMalloc");
+        n = bytes;
+        return p;
+    }
+    template <typename T>
+    T* as(size_t count) { return static_cast<T*>(get(count * sizeof(T))); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    ~DevBuf() { release(); }
+};
+
+template <typename T>
+void h2d(T* d, const T* h, size_t count, cudaStream_t st) {
+    if (count) ck(cudaMemcpyAsync(d, h, count * sizeof(T), cudaMemcpyHostToDevice, st), "H2D");
+}
+template <typename T>
+void d2h(T* h, const T* d, size_t count, cudaStream_t st) {
+    if (count) ck(cudaMemcpyAsync(h, d, count * sizeof(T), cudaMemcpyDeviceToHost, st), "D2H");
+}
+
+inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+// ---------------------------------------------------------------------------
+// Prepared genotype image + statistics
+// ---------------------------------------------------------------------------
+struct Prepared {
+    std::string key;
+    DevGeno g;
+    DevBuf codes;
+    std::vector<SnpCounts> counts;    // after imputation (HWE) or raw (mean)
+    std::vector<double> mean, sdinv;  // per SNP, the reference's formulas
+    int impute = LDS_IMPUTE_MEAN;
+    int ddof = 1;
+    DevBuf d_mean, d_sdinv;
+};
+
+struct Context {
+    std::mutex mu;
+    bool ready = false;
+    int device = -1;
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev[8];
+    std::list<std::unique_ptr<Prepared>> cache;  // most recent first
+    DevBuf raw, rows_dev, hwe_q0, hwe_q01, hwe_sb, counts_dev;
+    DevBuf y, yq, ycs, wq, wcs, z, rowind, sc, binoff, wqoff, accum, mc, guards, lscale, xin;
+    double timings[4] = {0, 0, 0, 0};
+    int slices = 4;
+};
+
+Context& ctx() {
+    static Context c;
+    return c;
+}
+
+void ensure_device(Context& c) {
+    if (c.ready) return;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0)
+        fail(LDS_ERR_CUDA, "no CUDA device available (liblds has no CPU fallback)");
+    ck(cudaGetDevice(&c.device), "cudaGetDevice");
+    ck(cudaStreamCreateWithFlags(&c.st, cudaStreamNonBlocking), "cudaStreamCreate");
+    for (auto& e : c.ev) ck(cudaEventCreate(&e), "cudaEventCreate");
+    c.ready = true;
+}
+
+// Mean and inverse sd over observed calls (genotype.cpp:651-689).
+void stats_observed(long long nobs, long long sum, long long sumsq, int ddof, double& mu,
+                    double& inv_sd) {
+    const double dn = (double)nobs;
+    const long long denom = nobs - (long long)ddof;
+    mu = (nobs > 0) ? ((double)sum / dn) : 0.0;
+    double m2 = 0.0;
+    if (nobs > 0) {
+        m2 = (double)sumsq - ((double)sum * (double)sum) / dn;
+        if (m2 < 0.0 && m2 > -1e-12) m2 = 0.0;
+    }
+    inv_sd = 1.0;
+    if (denom > 0 && m2 > 0.0) {
+        const double var = m2 / (double)denom;
+        if (var > 0.0) inv_sd = 1.0 / std::sqrt(var);
+    }
+}
+
+// Mean and inverse sd after completion (genotype.cpp:629-649).
+void stats_completed(long long sum, long long sumsq, int n, int ddof, double& mean,
+                     double& inv_std) {
+    mean = (n > 0) ? ((double)sum / (double)n) : 0.0;
+    inv_std = 1.0;
+    const long long denom = (long long)n - (long long)ddof;
+    if (n <= 0 || denom <= 0) return;
+    double m2 = (double)sumsq - ((double)sum * (double)sum) / (double)n;
+    if (m2 < 0.0 && m2 > -1e-12) m2 = 0.0;
+    if (m2 > 0.0) {
+        const double var = m2 / (double)denom;
+        if (var > 0.0 && std::isfinite(var)) inv_std = 1.0 / std::sqrt(var);
+    }
+}
+
+uint64_t hwe_seed_base(uint64_t impute_seed, int global_snp) {
+    uint64_t h = mix64(impute_seed);
+    h ^= mix64((uint64_t)(uint32_t)global_snp + 0x243f6a8885a308d3ULL);
+    return h;
+}
+
+uint64_t fnv1a(const void* data, size_t n, uint64_t h = 1469598103934665603ULL) {
+    const uint8_t* p = static_cast<const uint8_t*>(data);
+    for (size_t i = 0; i < n; ++i) {
+        h ^= p[i];
+        h *= 1099511628211ULL;
+    }
+    return h;
+}
+
+// Upload raw SNP-major rows, repack, count, impute, and compute statistics.
+// `global_snp0` is the genome index of the first row (HWE seeds use it).
+std::unique_ptr<Prepared> prepare(Context& c, const uint8_t* host_rows, int64_t row_bytes,
+                                  int64_t n_total, int64_t M, const int64_t* row_sel,
+                                  int64_t n_sel, int impute, uint64_t impute_seed, int ddof,
+                                  const std::string& key) {
+    auto P = std::make_unique<Prepared>();
+    P->key = key;
+    P->impute = impute;
+    P->ddof = ddof;
+    DevGeno& g = P->g;
+    g.N = row_sel ? n_sel : n_total;
+    if (g.N <= 0) fail(LDS_ERR_ARG, "no samples selected");
+    g.N_pad = round_up(g.N, kSamplePad);
+    g.nbp = g.N_pad / 4;
+    g.M = M;
+    g.M_pad = round_up(std::max<int64_t>(M, 1), kSnpPad) + kSnpPad;
+    g.codes = P->codes.as<uint8_t>((size_t)(g.M_pad * g.nbp));
+
+    std::vector<int32_t> rows32;
+    int32_t* d_rows = nullptr;
+    if (row_sel) {
+        rows32.resize((size_t)n_sel);
+        for (int64_t i = 0; i < n_sel; ++i) {
+            if (row_sel[i] < 0 || row_sel[i] >= n_total)
+                fail(LDS_ERR_ARG, "row_sel contains an out-of-range sample index");
+            rows32[(size_t)i] = (int32_t)row_sel[i];
+        }
+        d_rows = c.rows_dev.as<int32_t>(rows32.size());
+        h2d(d_rows, rows32.data(), rows32.size(), c.st);
+    }
+    // Upload in slabs to bound the staging buffer.
+    const int64_t slab_rows =
+        std::max<int64_t>(1, std::min<int64_t>(M, (int64_t)(1LL << 30) / std::max<int64_t>(row_bytes, 1)));
+    uint8_t* d_raw = c.raw.as<uint8_t>((size_t)(slab_rows * row_bytes));
+    for (int64_t j0 = 0; j0 < M; j0 += slab_rows) {
+        const int64_t nr = std::min(slab_rows, M - j0);
+        h2d(d_raw, host_rows + j0 * row_bytes, (size_t)(nr * row_bytes), c.st);
+        DevGeno sub = g;
+        sub.M = nr;
+        sub.M_pad = nr;
+        sub.codes = g.codes + j0 * g.nbp;
+        launch_repack(d_raw, row_bytes, n_total, d_rows, sub, c.st);
+    }
+    // Padding rows (all code 01).
+    if (g.M_pad > M)
+        ck(cudaMemsetAsync(g.codes + M * g.nbp, 0x55, (size_t)((g.M_pad - M) * g.nbp), c.st),
+           "memset pad rows");
+
+    SnpCounts* d_counts = c.counts_dev.as<SnpCounts>((size_t)std::max<int64_t>(M, 1));
+    P->counts.resize((size_t)M);
+    launch_counts(g, d_counts, c.st);
+    d2h(P->counts.data(), d_counts, (size_t)M, c.st);
+    ck(cudaStreamSynchronize(c.st), "counts");
+
+    P->mean.resize((size_t)M);
+    P->sdinv.resize((size_t)M);
+    if (impute == LDS_IMPUTE_HWE) {
+        std::vector<double> q0((size_t)M), q01((size_t)M);
+        std::vector<uint64_t> sb((size_t)M);
+        bool any_missing = false;
+        for (int64_t j = 0; j < M; ++j) {
+            const SnpCounts& k = P->counts[(size_t)j];
+            const long long nobs = (long long)k.n[0] + k.n[1] + k.n[2];
+            const long long sum = (long long)k.n[1] + 2LL * k.n[2];
+            double p = 0.0;
+            if (nobs > 0) {
+                p = (double)sum / (2.0 * (double)nobs);
+                if (p < 0.0) p = 0.0;
+                if (p > 1.0) p = 1.0;
+            }
+            q0[(size_t)j] = (1.0 - p) * (1.0 - p);
+            q01[(size_t)j] = q0[(size_t)j] + 2.0 * p * (1.0 - p);
+            sb[(size_t)j] = hwe_seed_base(impute_seed, (int)j);
+            any_missing |= k.n[3] > 0;
+        }
+        if (any_missing) {
+            double* dq0 = c.hwe_q0.as<double>((size_t)M);
+            double* dq01 = c.hwe_q01.as<double>((size_t)M);
+            uint64_t* dsb = c.hwe_sb.as<uint64_t>((size_t)M);
+            h2d(dq0, q0.data(), (size_t)M, c.st);
+            h2d(dq01, q01.data(), (size_t)M, c.st);
+            h2d(dsb, sb.data(), (size_t)M, c.st);
+            launch_hwe_impute(g, dq0, dq01, dsb, d_rows, c.st);
+            launch_counts(g, d_counts, c.st);
+            d2h(P->counts.data(), d_counts, (size_t)M, c.st);
+            ck(cudaStreamSynchronize(c.st), "hwe counts");
+        }
+        for (int64_t j = 0; j < M; ++j) {
+            const SnpCounts& k = P->counts[(size_t)j];
+            const long long sum = (long long)k.n[1] + 2LL * k.n[2];
+            const long long sumsq = (long long)k.n[1] + 4LL * k.n[2];
+            stats_completed(sum, sumsq, (int)g.N, ddof, P->mean[(size_t)j], P->sdinv[(size_t)j]);
+        }
+    } else {
+        for (int64_t j = 0; j < M; ++j) {
+            const SnpCounts& k = P->counts[(size_t)j];
+            const long long nobs = (long long)k.n[0] + k.n[1] + k.n[2];
+            const long long sum = (long long)k.n[1] + 2LL * k.n[2];
+            const long long sumsq = (long long)k.n[1] + 4LL * k.n[2];
+            stats_observed(nobs, sum, sumsq, ddof, P->mean[(size_t)j], P->sdinv[(size_t)j]);
+        }
+    }
+    double* dm = P->d_mean.as<double>((size_t)std::max<int64_t>(M, 1));
+    double* ds = P->d_sdinv.as<double>((size_t)std::max<int64_t>(M, 1));
+    h2d(dm, P->mean.data(), (size_t)M, c.st);
+    h2d(ds, P->sdinv.data(), (size_t)M, c.st);
+    ck(cudaStreamSynchronize(c.st), "prepare");
+    return P;
+}
+
+// Sum of squared standardized values of SNP j, from code counts; values are
+// rounded to T first like the reference's standardized block
+// (gwldcore.cpp:3275-3284 sums x^2 of the T-typed block).
+template <typename T>
+double sumsq_std(const Prepared& P, int64_t j) {
+    const SnpCounts& k = P.counts[(size_t)j];
+    const double mu = P.mean[(size_t)j], s = P.sdinv[(size_t)j];
+    double acc = 0.0;
+    for (int c = 0; c < 3; ++c) {
+        const double x = (double)(T)(((double)c - mu) * s);
+        acc += (double)k.n[c] * (x * x);
+    }
+    return acc;
+}
+
+// inv_j = 1/sqrt(max(eps, ||x_j||^2/(N-1))) (gwldcore.cpp:3320-3331).
+template <typename T>
+T inv_resvar(const Prepared& P, int64_t j, double eps) {
+    const double var = sumsq_std<T>(P, j) / (double)(P.g.N - 1);
+    const double safe = std::isnan(var) ? var : (var > eps ? var : eps);
+    return (T)(1.0 / std::sqrt(safe));
+}
+
+// ---------------------------------------------------------------------------
+// Probe streams: mt19937_64 seeded per (root, block start, V-tile start)
+// (gwldcore.cpp:452-458, :1691-1716).  Column-major L x V into Z (ld = z_ld).
+// ---------------------------------------------------------------------------
+template <typename T>
+void make_probes(uint64_t root, int blk_start, int v_start, int L, int V, int dist, double* Z,
+                 int64_t z_ld) {
+    uint64_t s = 0x1234abcdULL;
+    s ^= mix64(root);
+    s ^= mix64((uint64_t)blk_start + 0x9e37ULL);
+    s ^= mix64((uint64_t)v_start + 0x85ebULL);
+    std::mt19937_64 rng(s);
+    std::normal_distribution<T> gN(0, (T)1);
+    std::vector<T> col((size_t)L);
+    for (int c = 0; c < V; ++c) {
+        long double ss = 0.0L;
+        for (int r = 0; r < L; ++r) {
+            const T z = (dist == LDS_DIST_RADEMACHER) ? ((rng() & 1) ? T(1) : T(-1)) : gN(rng);
+            col[(size_t)r] = z;
+            if (dist == LDS_DIST_SPHERICAL) ss += (long double)z * (long double)z;
+        }
+        if (dist == LDS_DIST_SPHERICAL) {
+            const T zs = ss > 0.0L ? (T)std::sqrt((long double)L / ss) : T(1);
+            for (int r = 0; r < L; ++r) col[(size_t)r] *= zs;
+        }
+        for (int r = 0; r < L; ++r) Z[(int64_t)c * z_ld + r] = (double)col[(size_t)r];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Phase-1 CSR over annotation bins (build_phase1_csr, gwldcore.cpp:1002-1063).
+// annot: L x K row-major (values as T), inv: L (as T); SNP j = snp0 + i.
+// ---------------------------------------------------------------------------
+struct Csr {
+    std::vector<int64_t> bin_off;   // K+1, padded to kSnpStep
+    std::vector<int32_t> rowind;
+    std::vector<double> sc;
+    std::vector<int64_t> nnz;       // real members per bin
+    std::vector<int64_t> wq_off;    // K, bytes
+    int64_t wq_bytes = 0;
+};
+
+template <typename T>
+Csr build_csr(const T* annot, const T* inv, int64_t L, int64_t K, int64_t snp0, int Vp, int S) {
+    Csr c;
+    c.bin_off.assign((size_t)K + 1, 0);
+    c.nnz.assign((size_t)K, 0);
+    c.wq_off.assign((size_t)K, 0);
+    std::vector<std::vector<std::pair<int32_t, double>>> members((size_t)K);
+    for (int64_t k = 0; k < K; ++k) {
+        for (int64_t i = 0; i < L; ++i) {
+            const T a = annot[i * K + k];
+            if (a == T(0)) continue;
+            const double ad = (double)a;
+            if (!(ad > 0.0) || !std::isfinite(ad)) continue;
+            const double invd = (double)inv[i];
+            if (!std::isfinite(invd) || invd <= 0.0) continue;
+            const double s = invd * std::sqrt(ad);
+            if (!std::isfinite(s)) continue;
+            if (std::is_same<T, float>::value && s > (double)std::numeric_limits<float>::max())
+                continue;
+            members[(size_t)k].push_back({(int32_t)(snp0 + i), (double)(T)s});
+        }
+    }
+    int64_t off = 0, wq = 0;
+    for (int64_t k = 0; k < K; ++k) {
+        const int64_t n = (int64_t)members[(size_t)k].size();
+        const int64_t np = round_up(n, kSnpStep);
+        c.nnz[(size_t)k] = n;
+        c.bin_off[(size_t)k] = off;
+        c.wq_off[(size_t)k] = wq;
+        off += np;
+        wq += (int64_t)S * 2 * Vp * np;
+    }
+    c.bin_off[(size_t)K] = off;
+    c.wq_bytes = wq;
+    c.rowind.assign((size_t)off, (int32_t)snp0);
+    c.sc.assign((size_t)off, 0.0);
+    for (int64_t k = 0; k < K; ++k) {
+        int64_t p = c.bin_off[(size_t)k];
+        for (auto& m : members[(size_t)k]) {
+            c.rowind[(size_t)p] = m.first;
+            c.sc[(size_t)p] = m.second;
+            ++p;
+        }
+    }
+    return c;
+}
+
+// Run phase 1 for all bins of `csr` with probes Z (rows z_row0.., ld z_ld),
+// leaving Y (N_pad x K*V FP64) in c.y.
+void run_phase1(Context& c, Prepared& P, const Csr& csr, int64_t K, int V, const double* Z_host,
+                int64_t z_ld, int64_t z_rows, int64_t z_row0) {
+    const int S = c.slices;
+    const int Vp = (int)round_up(V, kColTile);
+    const int64_t nm = std::max<int64_t>((int64_t)csr.rowind.size(), 1);
+    int32_t* d_rowind = c.rowind.as<int32_t>((size_t)nm);
+    double* d_sc = c.sc.as<double>((size_t)nm);
+    int64_t* d_binoff = c.binoff.as<int64_t>(csr.bin_off.size());
+    int64_t* d_wqoff = c.wqoff.as<int64_t>(std::max<size_t>(csr.wq_off.size(), 1));
+    h2d(d_rowind, csr.rowind.data(), csr.rowind.size(), c.st);
+    h2d(d_sc, csr.sc.data(), csr.sc.size(), c.st);
+    h2d(d_binoff, csr.bin_off.data(), csr.bin_off.size(), c.st);
+    h2d(d_wqoff, csr.wq_off.data(), csr.wq_off.size(), c.st);
+    double* d_z = c.z.as<double>((size_t)std::max<int64_t>(z_ld * V, 1));
+    h2d(d_z, Z_host, (size_t)(z_ld * V), c.st);
+    (void)z_rows;
+
+    P1Weights w;
+    w.K = (int)K;
+    w.V = V;
+    w.Vp = Vp;
+    w.S = S;
+    w.rowind = d_rowind;
+    w.sc = d_sc;
+    w.bin_off = d_binoff;
+    w.wq_off = d_wqoff;
+    w.wq = c.wq.as<int8_t>((size_t)std::max<int64_t>(csr.wq_bytes, 16));
+    w.colscale = c.wcs.as<double>((size_t)(K * Vp));
+    launch_p1_weights(w, static_cast<double*>(P.d_mean.p), static_cast<double*>(P.d_sdinv.p), d_z,
+                      z_ld, z_row0, c.st);
+    double* Y = c.y.as<double>((size_t)(P.g.N_pad * K * V));
+    launch_p1(P.g, w, csr.bin_off.data(), Y, c.st);
+}
+
+// Quantize the device sketch in c.y (N_pad x K*V) into c.yq.
+void quantize_sketch(Context& c, Prepared& P, int64_t K, int V) {
+    const int S = c.slices;
+    const int Vp = (int)round_up(V, kColTile);
+    int8_t* yq = c.yq.as<int8_t>((size_t)(S * K * Vp * P.g.N_pad));
+    double* cs = c.ycs.as<double>((size_t)(K * Vp));
+    launch_quantize_y(static_cast<double*>(c.y.p), P.g.N, P.g.N_pad, (int)K, V, Vp, S, yq, cs,
+                      c.st);
+}
+
+// Phase 2 over SNPs [j0, j1) into device accumulators (out_row0 offset).
+void run_phase2(Context& c, Prepared& P, int64_t K, int V, int64_t j0, int64_t j1,
+                int64_t out_row0, double* d_accum, double* d_mc, const double* d_lscale) {
+    P2Args a;
+    a.K = (int)K;
+    a.V = V;
+    a.Vp = (int)round_up(V, kColTile);
+    a.S = c.slices;
+    a.j0 = j0;
+    a.j1 = j1;
+    a.out_row0 = out_row0;
+    a.Yq = static_cast<int8_t*>(c.yq.p);
+    a.colscale = static_cast<double*>(c.ycs.p);
+    a.mean = static_cast<double*>(P.d_mean.p);
+    a.sdinv = static_cast<double*>(P.d_sdinv.p);
+    a.left_scale = d_lscale;
+    a.accum = d_accum;
+    a.mc = d_mc;
+    a.guard_counts = c.guards.as<unsigned long long>(2);
+    static const double warn = [] {
+        const char* s = std::getenv("SUMMIT_P2_EXTREME_LD_WARN");
+        if (!s || !*s) s = std::getenv("SUMMIT_P2_ABS_LD_MAX");
+        double v = 1.0e10;
+        if (s && *s) {
+            char* end = nullptr;
+            const double x = std::strtod(s, &end);
+            if (end != s && std::isfinite(x)) v = x;
+        }
+        return v > 0.0 ? v : std::numeric_limits<double>::infinity();
+    }();
+    static const int drop = [] {
+        const char* s = std::getenv("SUMMIT_P2_DROP_EXTREME");
+        if (!s || !*s) return 1;
+        if (!strcmp(s, "0") || !strcmp(s, "false") || !strcmp(s, "FALSE") || !strcmp(s, "no") ||
+            !strcmp(s, "NO"))
+            return 0;
+        return 1;
+    }();
+    a.extreme_warn = warn;
+    a.drop_extreme = drop;
+    launch_p2(P.g, a, c.st);
+}
+
+void report_guards(Context& c, const char* label, int blk_start, int blk_end) {
+    unsigned long long h[2] = {0, 0};
+    d2h(h, static_cast<unsigned long long*>(c.guards.p), 2, c.st);
+    ck(cudaStreamSynchronize(c.st), "guards");
+    if (h[0])
+        std::fprintf(stderr,
+                     "[phase2-warning] %s block [%d:%d): dropped %llu non-finite LD-score updates.\n",
+                     label, blk_start, blk_end, h[0]);
+    if (h[1])
+        std::fprintf(stderr,
+                     "[phase2-warning] %s block [%d:%d): %llu finite updates exceeded the "
+                     "LD-score warning threshold. They were dropped unless "
+                     "SUMMIT_P2_DROP_EXTREME=0; inspect this run before using it.\n",
+                     label, blk_start, blk_end, h[1]);
+}
+
+// ---------------------------------------------------------------------------
+// Files: identity key, FAM/BIM line counts, mapped BED.
+// ---------------------------------------------------------------------------
+std::string file_identity(const std::string& path) {
+    struct stat s {};
+    if (::stat(path.c_str(), &s) != 0) fail(LDS_ERR_IO, "Failed to stat input path: %s", path.c_str());
+    char buf[512];
+    snprintf(buf, sizeof buf, "%s#%llu:%llu:%llu:%lld.%ld:%lld.%ld", path.c_str(),
+             (unsigned long long)s.st_dev, (unsigned long long)s.st_ino,
+             (unsigned long long)s.st_size, (long long)s.st_mtim.tv_sec, s.st_mtim.tv_nsec,
+             (long long)s.st_ctim.tv_sec, s.st_ctim.tv_nsec);
+    return buf;
+}
+
+int64_t count_lines(const std::string& path) {
+    FILE* f = std::fopen(path.c_str(), "r");
+    if (!f) fail(LDS_ERR_IO, "Failed to open file: %s", path.c_str());
+    int64_t n = 0;
+    char* line = nullptr;
+    size_t cap = 0;
+    ssize_t len;
+    while ((len = getline(&line, &cap, f)) != -1) {
+        if (len > 0 && line[0] == '#') continue;
+        ++n;
+    }
+    std::free(line);
+    std::fclose(f);
+    return n;
+}
+
+struct MappedBed {
+    int fd = -1;
+    size_t size = 0;
+    uint8_t* base = nullptr;
+    explicit MappedBed(const std::string& path) {
+        fd = ::open(path.c_str(), O_RDONLY | O_CLOEXEC);
+        if (fd < 0) fail(LDS_ERR_IO, "Failed to open bed: %s", path.c_str());
+        struct stat st {};
+        if (::fstat(fd, &st) != 0 || st.st_size < 3)
+            fail(LDS_ERR_IO, "stat failed or BED too small: %s", path.c_str());
+        size = (size_t)st.st_size;
+        void* p = ::mmap(nullptr, size, PROT_READ, MAP_PRIVATE, fd, 0);
+        if (p == MAP_FAILED) fail(LDS_ERR_IO, "mmap failed for: %s", path.c_str());
+        base = static_cast<uint8_t*>(p);
+        if (!(base[0] == 0x6C && base[1] == 0x1B && base[2] == 0x01))
+            fail(LDS_ERR_IO, "Invalid BED magic/mode (expected 6C 1B 01) for: %s", path.c_str());
+    }
+    ~MappedBed() {
+        if (base) ::munmap(base, size);
+        if (fd >= 0) ::close(fd);
+    }
+};
+
+std::string sel_key(const int64_t* rows, int64_t n) {
+    if (!rows) return "all";
+    char b[64];
+    snprintf(b, sizeof b, "%lld:%016llx", (long long)n,
+             (unsigned long long)fnv1a(rows, (size_t)n * sizeof(int64_t)));
+    return b;
+}
+
+// Device image of a BED fileset, cached by file identity, sample selection,
+// imputation mode/seed and ddof (like the reference's mapping cache,
+// genotype.cpp:350-410, keyed by file identity).
+Prepared& prepared_for_file(Context& c, const std::string& bed_prefix, const std::string& fam,
+                            const int64_t* rows, int64_t n_rows, int impute, uint64_t iseed,
+                            int ddof, int64_t* M_total_out) {
+    const std::string bed = bed_prefix + ".bed";
+    const std::string bim = bed_prefix + ".bim";
+    const int64_t n_total = count_lines(fam);
+    if (n_total <= 0) fail(LDS_ERR_IO, "FAM has zero rows: %s", fam.c_str());
+    const int64_t M = count_lines(bim);
+    if (M_total_out) *M_total_out = M;
+    char kb[128];
+    snprintf(kb, sizeof kb, "|%d|%llu|%d|%lld", impute,
+             (unsigned long long)(impute == LDS_IMPUTE_HWE ? iseed : 0ULL), ddof, (long long)n_total);
+    const std::string key = file_identity(bed) + "|" + sel_key(rows, n_rows) + kb;
+    for (auto it = c.cache.begin(); it != c.cache.end(); ++it) {
+        if ((*it)->key == key) {
+            c.cache.splice(c.cache.begin(), c.cache, it);
+            return *c.cache.front();
+        }
+    }
+    MappedBed mb(bed);
+    const int64_t nbytes = (n_total + 3) / 4;
+    if ((size_t)(3 + M * nbytes) > mb.size)
+        fail(LDS_ERR_IO, "BED file too small for requested block: %s", bed.c_str());
+    while (c.cache.size() >= 2) c.cache.pop_back();
+    auto P = prepare(c, mb.base + 3, nbytes, n_total, M, rows, n_rows, impute, iseed, ddof, key);
+    c.cache.push_front(std::move(P));
+    return *c.cache.front();
+}
+
+// ---------------------------------------------------------------------------
+// Entry-point implementations
+// ---------------------------------------------------------------------------
+template <typename T>
+void phase1_bed_impl(const char* bed_prefix, const char* fam_path, int blk_start, int blk_end,
+                     const int64_t* row_sel, int64_t n_row_sel, int ddof, const T* annot,
+                     int64_t annot_rows, int64_t K, const T* inv_right, int v_start, int v_count,
+                     int rand_dist, int has_seed, uint64_t seed, T* Xz, int64_t xz_rows,
+                     int64_t xz_cols, uint8_t* bin_init, int impute, int has_iseed,
+                     uint64_t iseed, T* inv_out, double resvar_eps) {
+    Context& c = ctx();
+    std::lock_guard<std::mutex> lk(c.mu);
+    ensure_device(c);
+    if (impute != LDS_IMPUTE_MEAN && impute != LDS_IMPUTE_HWE)
+        fail(LDS_ERR_ARG, "impute_mode must be 'mean' or 'hwe'");
+    int64_t M = 0;
+    Prepared& P = prepared_for_file(c, bed_prefix, fam_path, row_sel, n_row_sel, impute,
+                                    has_iseed ? iseed : 0ULL, ddof, &M);
+    if (blk_end > M) fail(LDS_ERR_ARG, "blk_end exceeds #SNPs in BIM");
+    if (blk_end <= blk_start) return;
+    const int64_t L = blk_end - blk_start;
+    if (annot_rows != L) fail(LDS_ERR_ARG, "L mismatch");
+    std::vector<T> inv((size_t)L);
+    if (inv_out) {
+        for (int64_t i = 0; i < L; ++i) inv[(size_t)i] = inv_resvar<T>(P, blk_start + i, resvar_eps);
+        std::memcpy(inv_out, inv.data(), sizeof(T) * (size_t)L);
+    } else {
+        if (!inv_right) fail(LDS_ERR_ARG, "inv_right shape mismatch in phase1");
+        std::memcpy(inv.data(), inv_right, sizeof(T) * (size_t)L);
+    }
+    if (xz_rows != P.g.N || xz_cols != K * v_count)
+        fail(LDS_ERR_ARG, "Xz2d_chunk shape must be (N, B*v_count)");
+    if (v_count <= 0) return;
+    const int S = c.slices;
+    const int Vp = (int)round_up(v_count, kColTile);
+    Csr csr = build_csr<T>(annot, inv.data(), L, K, blk_start, Vp, S);
+    const uint64_t root = has_seed ? seed : std::random_device{}();
+    std::vector<double> Z((size_t)(L * v_count));
+    make_probes<T>(root, blk_start, v_start, (int)L, v_count, rand_dist, Z.data(), L);
+    run_phase1(c, P, csr, K, v_count, Z.data(), L, L, blk_start);
+    // Download the block's contribution and merge with beta semantics.
+    const int64_t N = P.g.N;
+    std::vector<double> D((size_t)(N * K * v_count));
+    const double* Y = static_cast<double*>(c.y.p);
+    for (int64_t q = 0; q < K * v_count; ++q)
+        d2h(D.data() + q * N, Y + q * P.g.N_pad, (size_t)N, c.st);
+    ck(cudaStreamSynchronize(c.st), "phase1");
+    for (int64_t k = 0; k < K; ++k) {
+        if (csr.nnz[(size_t)k] == 0) continue;
+        bool beta1 = true;
+        if (bin_init) {
+            beta1 = bin_init[k] != 0;
+            bin_init[k] = 1;
+        }
+        for (int64_t cc = 0; cc < v_count; ++cc) {
+            T* dst = Xz + (k * v_count + cc) * N;
+            const double* src = D.data() + (k * v_count + cc) * N;
+            if (beta1)
+                for (int64_t n = 0; n < N; ++n) dst[n] = (T)((double)dst[n] + src[n]);
+            else
+                for (int64_t n = 0; n < N; ++n) dst[n] = (T)src[n];
+        }
+    }
+}
+
+template <typename T>
+void phase2_bed_impl(const char* bed_prefix, const char* fam_path, int blk_start, int blk_end,
+                     const int64_t* row_sel, int64_t n_row_sel, int ddof, const T* inv_left,
+                     int64_t L_in, int tile_nvecs, const T* Xz, int64_t xz_rows, int64_t xz_cols,
+                     T* meansq, int64_t M_rows, int64_t K_in, int N_denom, int impute,
+                     int has_iseed, uint64_t iseed, double* mc_agg, double* mc_snp) {
+    Context& c = ctx();
+    std::lock_guard<std::mutex> lk(c.mu);
+    ensure_device(c);
+    if (impute != LDS_IMPUTE_MEAN && impute != LDS_IMPUTE_HWE)
+        fail(LDS_ERR_ARG, "impute_mode must be 'mean' or 'hwe'");
+    int64_t M = 0;
+    Prepared& P = prepared_for_file(c, bed_prefix, fam_path, row_sel, n_row_sel, impute,
+                                    has_iseed ? iseed : 0ULL, ddof, &M);
+    if (blk_end > M) fail(LDS_ERR_ARG, "blk_end exceeds #SNPs in BIM");
+    if (blk_end <= blk_start) return;
+    const int64_t L = blk_end - blk_start;
+    if (L_in != L) fail(LDS_ERR_ARG, "inv_left shape mismatch in phase2_accum_XtXz_bed");
+    if (xz_rows != P.g.N) fail(LDS_ERR_ARG, "Xz2d shape mismatch in phase2_accum_XtXz_bed");
+    const int64_t Q = xz_cols;
+    if (tile_nvecs <= 0 || Q % tile_nvecs)
+        fail(LDS_ERR_ARG, "Xz2d col count must be a multiple of tile_nvecs");
+    const int64_t K = Q / tile_nvecs;
+    if (K_in != K) fail(LDS_ERR_ARG, "meansq_accum shape mismatch in phase2_accum_XtXz_bed");
+    if (blk_end > M_rows) fail(LDS_ERR_ARG, "meansq_accum rows smaller than SNP count");
+    if (K > 512) fail(LDS_ERR_ARG, "B too large for fixed seg buffers in phase2_accum_XtXz_bed");
+    const int64_t N = P.g.N, Np = P.g.N_pad;
+    // Sketch to device (FP64, padded rows zero).
+    std::vector<double> y((size_t)(Np * Q), 0.0);
+    for (int64_t q = 0; q < Q; ++q)
+        for (int64_t n = 0; n < N; ++n) y[(size_t)(q * Np + n)] = (double)Xz[q * N + n];
+    double* dY = c.y.as<double>((size_t)(Np * Q));
+    h2d(dY, y.data(), y.size(), c.st);
+    quantize_sketch(c, P, K, tile_nvecs);
+    // Left scales.
+    double denom = (double)N_denom - 1.0;
+    if (denom <= 0.0) denom = 1.0;
+    const double inv_denom2 = 1.0 / (denom * denom);
+    std::vector<double> ls((size_t)M, 0.0);
+    for (int64_t i = 0; i < L; ++i) {
+        const double v = (double)inv_left[i];
+        ls[(size_t)(blk_start + i)] = (std::isfinite(v) && v > 0.0) ? v * v * inv_denom2 : 0.0;
+    }
+    double* d_ls = c.lscale.as<double>((size_t)M);
+    h2d(d_ls, ls.data(), (size_t)M, c.st);
+    double* d_acc = c.accum.as<double>((size_t)(L * K));
+    ck(cudaMemsetAsync(d_acc, 0, sizeof(double) * (size_t)(L * K), c.st), "memset");
+    double* d_mc = nullptr;
+    if (mc_agg || mc_snp) {
+        d_mc = c.mc.as<double>((size_t)(L * K));
+        ck(cudaMemsetAsync(d_mc, 0, sizeof(double) * (size_t)(L * K), c.st), "memset");
+    }
+    ck(cudaMemsetAsync(c.guards.as<unsigned long long>(2), 0, 16, c.st), "memset");
+    run_phase2(c, P, K, tile_nvecs, blk_start, blk_end, blk_start, d_acc, d_mc, d_ls);
+    std::vector<double> upd((size_t)(L * K)), mcv;
+    d2h(upd.data(), d_acc, upd.size(), c.st);
+    if (d_mc) {
+        mcv.resize((size_t)(L * K));
+        d2h(mcv.data(), d_mc, mcv.size(), c.st);
+    }
+    ck(cudaStreamSynchronize(c.st), "phase2");
+    report_guards(c, "accum", blk_start, blk_end);
+    for (int64_t i = 0; i < L; ++i)
+        for (int64_t k = 0; k < K; ++k)
+            meansq[(blk_start + i) * K + k] += (T)upd[(size_t)(i * K + k)];
+    if (d_mc) {
+        for (int64_t k = 0; k < K; ++k) {
+            double agg = 0.0;
+            for (int64_t i = 0; i < L; ++i) {
+                const double s = mcv[(size_t)(i * K + k)];
+                agg += s;
+                if (mc_snp) mc_snp[(blk_start + i) * K + k] += s;
+            }
+            if (mc_agg) mc_agg[k] += agg;
+        }
+    }
+}
+
+template <typename T>
+void resvar_impl(const char* bed_prefix, const char* fam_path, int nsnps, const int64_t* row_sel,
+                 int64_t n_row_sel, int ddof, double eps, int impute, int has_iseed,
+                 uint64_t iseed, T* inv_out) {
+    Context& c = ctx();
+    std::lock_guard<std::mutex> lk(c.mu);
+    ensure_device(c);
+    int64_t M = 0;
+    Prepared& P = prepared_for_file(c, bed_prefix, fam_path, row_sel, n_row_sel, impute,
+                                    has_iseed ? iseed : 0ULL, ddof, &M);
+    if (nsnps > M) fail(LDS_ERR_ARG, "nsnps exceeds #SNPs in BIM");
+    if (P.g.N <= 1) fail(LDS_ERR_ARG, "Invalid block dimensions in compute_inv_resvar_from_geno_block");
+    for (int64_t j = 0; j < nsnps; ++j) inv_out[j] = inv_resvar<T>(P, j, eps);
+}
+
+// Whole-estimator session on an in-memory BED image.
+void gw_ldscore_impl(const uint8_t* bed_rows, int64_t row_bytes, int64_t n_total, int64_t M,
+                     const int64_t* row_sel, int64_t n_sel, const double* annot, int64_t K,
+                     int nvecs, int step, int vtile, uint64_t seed, int dist, int ddof,
+                     int impute, uint64_t iseed, double eps, int as_float, double* ldscore,
+                     double* meansq_out, double* inv_out, double* mc_agg, double* mc_snp) {
+    Context& c = ctx();
+    std::lock_guard<std::mutex> lk(c.mu);
+    ensure_device(c);
+    if (nvecs <= 0 || step <= 0 || K <= 0 || M <= 0) fail(LDS_ERR_ARG, "invalid sizes");
+    if (row_bytes < (n_total + 3) / 4) fail(LDS_ERR_ARG, "bed_row_bytes smaller than ceil(N/4)");
+    if (impute != LDS_IMPUTE_MEAN && impute != LDS_IMPUTE_HWE)
+        fail(LDS_ERR_ARG, "impute_mode must be 'mean' or 'hwe'");
+    ck(cudaEventRecord(c.ev[0], c.st), "event");
+    auto P = prepare(c, bed_rows, row_bytes, n_total, M, row_sel, n_sel, impute, iseed, ddof,
+                     "session");
+    ck(cudaEventRecord(c.ev[1], c.st), "event");
+    const int64_t N = P->g.N;
+    // Residual variances (fused into the first phase-1 pass in the reference;
+    // same values), rounded to the working type.
+    std::vector<double> inv((size_t)M);
+    for (int64_t j = 0; j < M; ++j)
+        inv[(size_t)j] = as_float ? (double)inv_resvar<float>(*P, j, eps) : inv_resvar<double>(*P, j, eps);
+    if (inv_out) std::memcpy(inv_out, inv.data(), sizeof(double) * (size_t)M);
+    // CSR over the whole genome: blocks only affect probe streams.
+    const int S = c.slices;
+    std::vector<int> vt;
+    {
+        int width = std::min(nvecs, vtile > 0 ? vtile : nvecs);
+        if (width >= 64) width = std::max(64, (width / 64) * 64);
+        for (int s = 0; s < nvecs; s += width) vt.push_back(std::min(width, nvecs - s));
+    }
+    const int vmax = *std::max_element(vt.begin(), vt.end());
+    Csr csr;
+    std::vector<float> annot_f, inv_f;
+    if (as_float) {
+        annot_f.assign(annot, annot + M * K);
+        inv_f.resize((size_t)M);
+        for (int64_t j = 0; j < M; ++j) inv_f[(size_t)j] = (float)inv[(size_t)j];
+    }
+    // Left scales (gwldcore.cpp:2436-2445).
+    const double denom = std::max(1.0, (double)(N - ddof + 1) - 1.0);
+    const double inv_denom2 = 1.0 / (denom * denom);
+    std::vector<double> ls((size_t)M);
+    for (int64_t j = 0; j < M; ++j) {
+        const double v = inv[(size_t)j];
+        ls[(size_t)j] = (std::isfinite(v) && v > 0.0) ? v * v * inv_denom2 : 0.0;
+    }
+    double* d_ls = c.lscale.as<double>((size_t)M);
+    h2d(d_ls, ls.data(), (size_t)M, c.st);
+    double* d_acc = c.accum.as<double>((size_t)(M * K));
+    ck(cudaMemsetAsync(d_acc, 0, sizeof(double) * (size_t)(M * K), c.st), "memset");
+    double* d_mc = nullptr;
+    if (mc_agg || mc_snp) {
+        d_mc = c.mc.as<double>((size_t)(M * K));
+        ck(cudaMemsetAsync(d_mc, 0, sizeof(double) * (size_t)(M * K), c.st), "memset");
+    }
+    ck(cudaMemsetAsync(c.guards.as<unsigned long long>(2), 0, 16, c.st), "memset");
+    std::vector<double> Z((size_t)(M * vmax));
+    const int nblk = (int)((M + step - 1) / step);
+    const unsigned hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    float p1_ms = 0.f, p2_ms = 0.f;
+    int v0 = 0;
+    for (int V : vt) {
+        const int Vp = (int)round_up(V, kColTile);
+        csr = as_float ? build_csr<float>(annot_f.data(), inv_f.data(), M, K, 0, Vp, S)
+                       : build_csr<double>(annot, inv.data(), M, K, 0, Vp, S);
+        // Probe streams per block, generated in parallel.
+        {
+            std::vector<std::thread> th;
+            std::atomic<int> next{0};
+            for (unsigned t = 0; t < hw; ++t)
+                th.emplace_back([&] {
+                    for (int b; (b = next.fetch_add(1)) < nblk;) {
+                        const int s = b * step;
+                        const int L = (int)std::min<int64_t>(step, M - s);
+                        // Column-major M x V with ld = M: block rows start at s.
+                        std::vector<double> blk((size_t)L * V);
+                        if (as_float) make_probes<float>(seed, s, v0, L, V, dist, blk.data(), L);
+                        else make_probes<double>(seed, s, v0, L, V, dist, blk.data(), L);
+                        for (int cc = 0; cc < V; ++cc)
+                            std::memcpy(&Z[(size_t)cc * M + s], &blk[(size_t)cc * L],
+                                        sizeof(double) * L);
+                    }
+                });
+            for (auto& t : th) t.join();
+        }
+        ck(cudaEventRecord(c.ev[2], c.st), "event");
+        run_phase1(c, *P, csr, K, V, Z.data(), M, M, 0);
+        quantize_sketch(c, *P, K, V);
+        ck(cudaEventRecord(c.ev[3], c.st), "event");
+        run_phase2(c, *P, K, V, 0, M, 0, d_acc, d_mc, d_ls);
+        ck(cudaEventRecord(c.ev[4], c.st), "event");
+        ck(cudaEventSynchronize(c.ev[4]), "sync");
+        float a = 0.f, b = 0.f;
+        cudaEventElapsedTime(&a, c.ev[2], c.ev[3]);
+        cudaEventElapsedTime(&b, c.ev[3], c.ev[4]);
+        p1_ms += a;
+        p2_ms += b;
+        v0 += V;
+    }
+    std::vector<double> acc((size_t)(M * K));
+    d2h(acc.data(), d_acc, acc.size(), c.st);
+    std::vector<double> mcv;
+    if (d_mc) {
+        mcv.resize((size_t)(M * K));
+        d2h(mcv.data(), d_mc, mcv.size(), c.st);
+    }
+    ck(cudaEventRecord(c.ev[5], c.st), "event");
+    ck(cudaStreamSynchronize(c.st), "session");
+    report_guards(c, "accum", 0, (int)M);
+    float up = 0.f, tot = 0.f;
+    cudaEventElapsedTime(&up, c.ev[0], c.ev[1]);
+    cudaEventElapsedTime(&tot, c.ev[0], c.ev[5]);
+    c.timings[0] = up;
+    c.timings[1] = p1_ms;
+    c.timings[2] = p2_ms;
+    c.timings[3] = tot;
+    if (meansq_out) std::memcpy(meansq_out, acc.data(), sizeof(double) * acc.size());
+    // Finalize: / nvecs, minus M_k / (N - ddof) (gw_ldscore.py:2197, :2220-2222).
+    std::vector<double> Mk((size_t)K, 0.0);
+    for (int64_t j = 0; j < M; ++j)
+        for (int64_t k = 0; k < K; ++k) Mk[(size_t)k] += annot[j * K + k];
+    const double nd = (double)(N - ddof);
+    for (int64_t j = 0; j < M; ++j)
+        for (int64_t k = 0; k < K; ++k)
+            ldscore[j * K + k] = acc[(size_t)(j * K + k)] / (double)nvecs - Mk[(size_t)k] / nd;
+    if (d_mc) {
+        for (int64_t k = 0; k < K; ++k) {
+            double agg = 0.0;
+            for (int64_t j = 0; j < M; ++j) agg += mcv[(size_t)(j * K + k)];
+            if (mc_agg) mc_agg[k] = agg;
+        }
+        if (mc_snp) std::memcpy(mc_snp, mcv.data(), sizeof(double) * mcv.size());
+    }
+}
+
+}  // namespace
+}  // namespace lds
+
+using namespace lds;
+
+#define LDS_API extern "C" __attribute__((visibility("default")))
+
+LDS_API const char* lds_last_error(void) { return g_err.c_str(); }
+
+LDS_API const char* lds_version(void) {
+    return "liblds 0.1 sm_100a (int8 digit-sliced exact products; mma.sync path)";
+}
+
+LDS_API int lds_device_count(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+    return n;
+}
+
+LDS_API int lds_set_slices(int s) {
+    if (s < 3 || s > kMaxSlices) {
+        g_err = "slices must be in [3, 6]";
+        return LDS_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    ctx().slices = s;
+    return LDS_OK;
+}
+
+LDS_API int lds_get_slices(void) { return ctx().slices; }
+
+LDS_API uint64_t lds_kernel_launches(void) { return g_launches.load(); }
+
+LDS_API void lds_clear_device_cache(void) {
+    Context& c = ctx();
+    std::lock_guard<std::mutex> lk(c.mu);
+    c.cache.clear();
+    for (DevBuf* b : {&c.raw, &c.rows_dev, &c.hwe_q0, &c.hwe_q01, &c.hwe_sb, &c.counts_dev, &c.y,
+                      &c.yq, &c.ycs, &c.wq, &c.wcs, &c.z, &c.rowind, &c.sc, &c.binoff, &c.wqoff,
+                      &c.accum, &c.mc, &c.guards, &c.lscale, &c.xin})
+        b->release();
+}
+
+#define P1_ARGS(T)                                                                              \
+    const char *bed_prefix, const char *fam_path, int blk_start, int blk_end,                   \
+        const int64_t *row_sel, int64_t n_row_sel, int ddof, const T *annot_blk,                \
+        int64_t annot_rows, int64_t K, const T *inv_right, int v_start, int v_count,            \
+        int kmax_hint, int rand_dist, int has_seed, uint64_t seed, T *Xz2d_chunk,                \
+        int64_t xz_rows, int64_t xz_cols, uint8_t *bin_init_mask, int impute_mode,              \
+        int has_impute_seed, uint64_t impute_seed, T *inv_out, double resvar_eps
+#define P1_CALL(T)                                                                              \
+    guarded([&] {                                                                               \
+        (void)kmax_hint;                                                                        \
+        phase1_bed_impl<T>(bed_prefix, fam_path, blk_start, blk_end, row_sel, n_row_sel, ddof,  \
+                           annot_blk, annot_rows, K, inv_right, v_start, v_count, rand_dist,    \
+                           has_seed, seed, Xz2d_chunk, xz_rows, xz_cols, bin_init_mask,         \
+                           impute_mode, has_impute_seed, impute_seed, inv_out, resvar_eps);     \
+    })
+LDS_API int lds_phase1_compute_Xz_bed_chunk_f32(P1_ARGS(float)) { return P1_CALL(float); }
+LDS_API int lds_phase1_compute_Xz_bed_chunk_f64(P1_ARGS(double)) { return P1_CALL(double); }
+
+#define P2_ARGS(T)                                                                              \
+    const char *bed_prefix, const char *fam_path, int blk_start, int blk_end,                   \
+        const int64_t *row_sel, int64_t n_row_sel, int ddof, const T *inv_left, int64_t L,      \
+        int tile_nvecs, const T *Xz2d, int64_t xz_rows, int64_t xz_cols, T *meansq_accum,       \
+        int64_t M_rows, int64_t K, int N_denom, int impute_mode, int has_impute_seed,           \
+        uint64_t impute_seed, double *mc_aggregate_sumsq, double *mc_per_snp_sumsq
+#define P2_CALL(T)                                                                              \
+    guarded([&] {                                                                               \
+        phase2_bed_impl<T>(bed_prefix, fam_path, blk_start, blk_end, row_sel, n_row_sel, ddof,  \
+                           inv_left, L, tile_nvecs, Xz2d, xz_rows, xz_cols, meansq_accum,       \
+                           M_rows, K, N_denom, impute_mode, has_impute_seed, impute_seed,       \
+                           mc_aggregate_sumsq, mc_per_snp_sumsq);                               \
+    })
+LDS_API int lds_phase2_accum_XtXz_bed_f32(P2_ARGS(float)) { return P2_CALL(float); }
+LDS_API int lds_phase2_accum_XtXz_bed_f64(P2_ARGS(double)) { return P2_CALL(double); }
+
+#define RV_ARGS(T)                                                                              \
+    const char *bed_prefix, const char *fam_path, int nsnps, int step_size,                     \
+        const int64_t *row_sel, int64_t n_row_sel, int ddof, double eps, int impute_mode,       \
+        int has_impute_seed, uint64_t impute_seed, T *inv_out
+#define RV_CALL(T)                                                                              \
+    guarded([&] {                                                                               \
+        (void)step_size;                                                                        \
+        resvar_impl<T>(bed_prefix, fam_path, nsnps, row_sel, n_row_sel, ddof, eps, impute_mode, \
+                       has_impute_seed, impute_seed, inv_out);                                  \
+    })
+LDS_API int lds_precompute_residual_variances_bed_f32(RV_ARGS(float)) { return RV_CALL(float); }
+LDS_API int lds_precompute_residual_variances_bed_f64(RV_ARGS(double)) { return RV_CALL(double); }
+
+LDS_API int lds_gw_ldscore(const uint8_t* bed_rows, int64_t bed_row_bytes, int64_t n_total,
+                           int64_t M, const int64_t* row_sel, int64_t n_row_sel,
+                           const double* annot, int64_t K, int nvecs, int step_size, int vtile,
+                           uint64_t seed, int rand_dist, int ddof, int impute_mode,
+                           uint64_t impute_seed, double resvar_eps, int as_float, double* ldscore,
+                           double* meansq_accum, double* inv_out, double* mc_aggregate_sumsq,
+                           double* mc_per_snp_sumsq) {
+    return guarded([&] {
+        gw_ldscore_impl(bed_rows, bed_row_bytes, n_total, M, row_sel, n_row_sel, annot, K, nvecs,
+                        step_size, vtile, seed, rand_dist, ddof, impute_mode, impute_seed,
+                        resvar_eps, as_float, ldscore, meansq_accum, inv_out, mc_aggregate_sumsq,
+                        mc_per_snp_sumsq);
+    });
+}
+
+LDS_API int lds_gw_ldscore_bed(const char* bed_prefix, const char* fam_path,
+                               const int64_t* row_sel, int64_t n_row_sel, const double* annot,
+                               int64_t K, int nvecs, int step_size, int vtile, uint64_t seed,
+                               int rand_dist, int ddof, int impute_mode, uint64_t impute_seed,
+                               double resvar_eps, int as_float, double* ldscore,
+                               double* meansq_accum, double* inv_out, double* mc_aggregate_sumsq,
+                               double* mc_per_snp_sumsq) {
+    return guarded([&] {
+        const std::string bed = std::string(bed_prefix) + ".bed";
+        const int64_t n_total = count_lines(fam_path);
+        const int64_t M = count_lines(std::string(bed_prefix) + ".bim");
+        MappedBed mb(bed);
+        const int64_t nbytes = (n_total + 3) / 4;
+        if ((size_t)(3 + M * nbytes) > mb.size) fail(LDS_ERR_IO, "BED file too small: %s", bed.c_str());
+        gw_ldscore_impl(mb.base + 3, nbytes, n_total, M, row_sel, n_row_sel, annot, K, nvecs,
+                        step_size, vtile, seed, rand_dist, ddof, impute_mode, impute_seed,
+                        resvar_eps, as_float, ldscore, meansq_accum, inv_out, mc_aggregate_sumsq,
+                        mc_per_snp_sumsq);
+    });
+}
+
+LDS_API int lds_debug_xt_products(const uint8_t* bed_rows, int64_t bed_row_bytes, int64_t n,
+                                  int64_t L, const int8_t* y, int64_t Q, int64_t* out_g,
+                                  int64_t* out_o) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        ensure_device(c);
+        if (L <= 0 || Q <= 0 || n <= 0) fail(LDS_ERR_ARG, "invalid sizes");
+        auto P = prepare(c, bed_rows, bed_row_bytes, n, L, nullptr, 0, LDS_IMPUTE_MEAN, 0, 1,
+                         "debug");
+        const int64_t Np = P->g.N_pad, Vp = round_up(Q, kColTile);
+        std::vector<int8_t> yq((size_t)(Vp * Np), 0);
+        for (int64_t q = 0; q < Q; ++q) std::memcpy(&yq[(size_t)(q * Np)], y + q * n, (size_t)n);
+        int8_t* d_yq = c.yq.as<int8_t>(yq.size());
+        h2d(d_yq, yq.data(), yq.size(), c.st);
+        DevBuf rg, ro;
+        long long* dg = rg.as<long long>((size_t)(L * Q));
+        long long* dO = ro.as<long long>((size_t)(L * Q));
+        P2Args a;
+        a.K = 1;
+        a.V = (int)Q;
+        a.Vp = (int)Vp;
+        a.S = 1;
+        a.j0 = 0;
+        a.j1 = L;
+        a.out_row0 = 0;
+        a.Yq = d_yq;
+        a.raw_g = dg;
+        a.raw_o = dO;
+        launch_p2(P->g, a, c.st);
+        ck(cudaGetLastError(), "launch");
+        d2h(reinterpret_cast<long long*>(out_g), dg, (size_t)(L * Q), c.st);
+        d2h(reinterpret_cast<long long*>(out_o), dO, (size_t)(L * Q), c.st);
+        ck(cudaStreamSynchronize(c.st), "debug products");
+    });
+}
+
+LDS_API int lds_last_timings(double* ms_out, int n) {
+    Context& c = ctx();
+    for (int i = 0; i < n && i < 4; ++i) ms_out[i] = c.timings[i];
+    return LDS_OK;
+}
+
+LDS_API int lds_synth_bed(int64_t n, int64_t M, uint64_t seed, const int64_t* t0,
+                          const int64_t* t1, int missing, uint8_t* out) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        ensure_device(c);
+        const int64_t nb = (n + 3) / 4;
+        DevBuf dt0, dt1, dout;
+        int64_t* a = dt0.as<int64_t>((size_t)M);
+        int64_t* b = dt1.as<int64_t>((size_t)M);
+        h2d(a, t0, (size_t)M, c.st);
+        h2d(b, t1, (size_t)M, c.st);
+        uint8_t* o = dout.as<uint8_t>((size_t)(nb * M));
+        launch_synth(n, M, seed, a, b, missing, o, c.st);
+        d2h(out, o, (size_t)(nb * M), c.st);
+        ck(cudaStreamSynchronize(c.st), "synth");
+    });
+}

@@ -1,0 +1,98 @@
+// Internal interfaces between the host orchestration (lds_host.cu) and the
+// kernels (lds_kernels.cu).  Not part of the C ABI.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace lds {
+
+// Padding rules of the device genotype image.
+constexpr int kSamplePad = 256;   // N_pad multiple (phase-2 K-steps, phase-1 sample tiles)
+constexpr int kSnpPad = 128;      // M_pad multiple (phase-2 SNP tiles)
+constexpr int kColTile = 16;      // probe columns per tile (bins padded to a multiple)
+constexpr int kSnpStep = 32;      // phase-1 K-step (SNPs); CSR lists padded to a multiple
+constexpr int kMaxSlices = 6;
+
+// Device-resident, padded genotype image: SNP-major 2-bit codes, row stride
+// nbp = N_pad/4 bytes, M_pad rows.  Padding samples and rows hold code 01
+// (missing), so they decode to g = 0, o = 0 and contribute nothing.
+struct DevGeno {
+    int64_t N = 0, N_pad = 0, nbp = 0, M = 0, M_pad = 0;
+    uint8_t* codes = nullptr;
+};
+
+// Per-SNP code counts produced by the stats kernel: n0, n1, n2, nmiss
+// (real samples only).
+struct SnpCounts {
+    int32_t n[4];
+};
+
+// ---- kernel launchers (all on `st`) ----
+// Repack raw BED rows (row stride src_bytes, n_total samples) into the padded
+// device layout, selecting `rows` (device int32, may be null = all).
+void launch_repack(const uint8_t* src, int64_t src_bytes, int64_t n_total, const int32_t* rows,
+                   const DevGeno& g, cudaStream_t st);
+void launch_counts(const DevGeno& g, SnpCounts* out, cudaStream_t st);
+// HWE imputation in place (genotype.cpp:146-184, :810-826): q0/q01/seed_base
+// per SNP (host-computed doubles), global row index per selected sample.
+void launch_hwe_impute(const DevGeno& g, const double* q0, const double* q01,
+                       const uint64_t* seed_base, const int32_t* global_rows, cudaStream_t st);
+
+// Phase-1 weights: for each bin k and probe v, W1[r] = s_j * sc_r * z_{j v}
+// and W2[r] = mu_j * W1[r] over the bin's CSR members (j = rowind[r]);
+// quantized per column into S signed int8 digits with a power-of-two scale.
+struct P1Weights {
+    int K = 0, V = 0, Vp = 0, S = 4;
+    const int32_t* rowind = nullptr;     // concatenated member lists (padded per bin)
+    const double* sc = nullptr;          // inv_j * sqrt(a_jk) per member (0 in padding)
+    const int64_t* bin_off = nullptr;    // K+1 offsets into rowind/sc (multiples of kSnpStep)
+    const int64_t* wq_off = nullptr;     // K offsets (bytes) into wq
+    int8_t* wq = nullptr;                // per bin: [S][2][Vp][nnzp]
+    double* colscale = nullptr;          // K*Vp
+};
+void launch_p1_weights(const P1Weights& w, const double* mean, const double* sdinv,
+                       const double* Z, int64_t z_ld, int64_t z_row0, cudaStream_t st);
+
+// Phase 1: Y[:, k*V+v] = sum_r x_{rowind[r]} * W[r, (k,v)], FP64 output
+// (N_pad rows, column stride N_pad, only real columns written).
+void launch_p1(const DevGeno& g, const P1Weights& w, const int64_t* h_bin_off, double* Y,
+               cudaStream_t st);
+
+// Quantize Y (N_pad x K*V, FP64) into S int8 digit planes Yq[S][K*Vp][N_pad]
+// with per-column power-of-two scales (padding columns -> 0).
+void launch_quantize_y(const double* Y, int64_t N, int64_t N_pad, int K, int V, int Vp, int S,
+                       int8_t* Yq, double* colscale, cudaStream_t st);
+
+// Phase 2 over SNP rows [j0, j1): Work = x_j^T Y, per bin k:
+// upd = sum_v Work^2 * left_scale_j with guards; accum[(j-j0_out)*K + k] += upd;
+// mc (may be null) += sum_v Work^4 * left_scale^2.  guard_counts[0..1] +=
+// dropped non-finite / extreme counts.
+struct P2Args {
+    int K = 0, V = 0, Vp = 0, S = 4;
+    int64_t j0 = 0, j1 = 0, out_row0 = 0;
+    const int8_t* Yq = nullptr;
+    const double* colscale = nullptr;
+    const double* mean = nullptr;
+    const double* sdinv = nullptr;
+    const double* left_scale = nullptr;
+    double* accum = nullptr;
+    double* mc = nullptr;
+    unsigned long long* guard_counts = nullptr;
+    double extreme_warn = 1e10;
+    int drop_extreme = 1;
+    // Verification mode (S must be 1): write exact int64 G^T y / O^T y of the
+    // single bin to raw_g / raw_o ((j - out_row0) * V + v) instead of reducing.
+    long long* raw_g = nullptr;
+    long long* raw_o = nullptr;
+};
+void launch_p2(const DevGeno& g, const P2Args& a, cudaStream_t st);
+
+// Synthetic generator (bedfile.py), writing n samples x M SNPs, row stride
+// ceil(n/4), into `out` (device).
+void launch_synth(int64_t n, int64_t M, uint64_t seed, const int64_t* t0, const int64_t* t1,
+                  int missing, uint8_t* out, cudaStream_t st);
+
+// Launch accounting.
+void count_launch();
+
+}  // namespace lds

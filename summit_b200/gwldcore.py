@@ -1,0 +1,282 @@
+"""Drop-in replacement for SUMMIT's native ``gwldcore`` module, backed by liblds.so.
+
+Function names, keyword arguments, defaults, array layouts and error messages
+follow the reference's nanobind bindings (``src/native/gwldcore.cpp:3656-3829``),
+so ``summit.ldscore.gw_ldscore`` can import this module in place of the native
+one.  The ``float32`` / ``float64`` overloads are selected from the dtype of the
+sketch array, as nanobind's overload resolution does.
+
+All genotype arithmetic runs on the GPU (sm_100a).  There is no CPU fallback:
+without liblds.so or a CUDA device every compute call raises RuntimeError.
+
+In addition to the reference's per-block functions, ``gw_ldscore`` computes a
+whole genome-wide estimate in one call with the genotype image resident on
+the device (same probes, blocks and V-tiles, hence the same result).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, enc, ptr
+
+_REQUIRED = object()
+_verbose = False
+
+
+def _need(name, value):
+    if value is _REQUIRED:
+        raise TypeError(f"missing required argument '{name}'")
+    return value
+
+
+def _tsuffix(arr) -> str:
+    if arr.dtype == np.float32:
+        return "f32"
+    if arr.dtype == np.float64:
+        return "f64"
+    raise TypeError("incompatible function arguments: arrays must be float32 or float64")
+
+
+def _rows(row_sel):
+    if row_sel is None:
+        return None, 0
+    r = np.asarray(row_sel)
+    if r.ndim != 1 or r.dtype not in (np.int32, np.int64):
+        raise RuntimeError("row_sel must be a 1D CPU array of int32 or int64 indices")
+    r = np.ascontiguousarray(r, dtype=np.int64)
+    return r, int(r.size)
+
+
+def _rw(arr, dtype, order, name):
+    """In-place arrays must already have the right dtype and layout."""
+    if not isinstance(arr, np.ndarray) or arr.dtype != dtype:
+        raise TypeError(f"incompatible function arguments: {name} must be a {np.dtype(dtype)} array")
+    ok = arr.flags.f_contiguous if order == "F" else arr.flags.c_contiguous
+    if not ok or not arr.flags.writeable:
+        raise TypeError(f"incompatible function arguments: {name} must be writable and "
+                        f"{'column' if order == 'F' else 'row'}-major contiguous")
+    return arr
+
+
+def _impute(mode: str) -> int:
+    if mode not in _lib.LDS_IMPUTE:
+        raise RuntimeError("impute_mode must be 'mean' or 'hwe'")
+    return _lib.LDS_IMPUTE[mode]
+
+
+def _dist(name: str) -> int:
+    # The reference treats any non-"rademacher" name as Gaussian, with
+    # "spherical" rescaled (gwldcore.cpp:1693-1716).
+    if name == "rademacher":
+        return 0
+    return 2 if name == "spherical" else 1
+
+
+# ---------------------------------------------------------------------------
+# Housekeeping (gwldcore.cpp:3659-3671, :3742-3746)
+# ---------------------------------------------------------------------------
+def set_verbose(enabled: bool) -> None:
+    global _verbose
+    _verbose = bool(enabled)
+
+
+def set_num_threads(n: int) -> None:
+    """Host threads are not used for genotype arithmetic; accepted for API parity."""
+
+
+def get_max_threads() -> int:
+    return 1
+
+
+def prefetch_bed_block(bed_prefix, fam_path, blk_start, blk_end, ahead_blocks=1) -> None:
+    """The genotype image is resident on the device after first use; nothing to prefetch."""
+
+
+def clear_gwld_native_scratch() -> None:
+    _lib.load().lds_clear_device_cache()
+
+
+clear_phase1_native_scratch = clear_gwld_native_scratch
+clear_phase2_native_scratch = clear_gwld_native_scratch
+clear_gwld_genotype_scratch = clear_gwld_native_scratch
+_clear_bed_mapping_cache = clear_gwld_native_scratch
+
+
+def clear_phase1_csr_cache() -> None:
+    """CSR lists are rebuilt per call from the arrays passed; nothing is cached."""
+
+
+def _bed_mapping_cache_info() -> dict:
+    return {"entries": 0, "capacity": 2, "hits": 0, "misses": 0, "evictions": 0}
+
+
+# ---------------------------------------------------------------------------
+# Phase 1 (gwldcore.cpp:3673-3688)
+# ---------------------------------------------------------------------------
+def phase1_compute_Xz_bed_chunk(bed_prefix, fam_path, blk_start, blk_end, row_sel=None, ddof=1,
+                                annot_blk=_REQUIRED, inv_right=_REQUIRED, v_start=_REQUIRED,
+                                v_count=_REQUIRED, kmax_hint=_REQUIRED, rand_dist="rademacher",
+                                seed=None, Xz2d_chunk=_REQUIRED, bin_init_mask=None,
+                                project_right=False, C=None, R=None, impute_mode="hwe",
+                                impute_seed=None, resvar_gram=None, inv_out=None,
+                                resvar_eps=1e-10):
+    Xz = _need("Xz2d_chunk", Xz2d_chunk)
+    t = _tsuffix(Xz)
+    dt = Xz.dtype
+    _rw(Xz, dt, "F", "Xz2d_chunk")
+    if Xz.ndim != 2:
+        raise RuntimeError("Xz2d_chunk shape must be (N, B*v_count)")
+    if (C is not None or R is not None) and (project_right or inv_out is not None):
+        raise RuntimeError("covariate projection inside phase 1 is not supported by the B200 "
+                           "backend; project Xz2d after phase 1 (project_colmajor_inplace)")
+    ann = np.ascontiguousarray(_need("annot_blk", annot_blk), dtype=dt)
+    if ann.ndim != 2:
+        raise RuntimeError("L mismatch")
+    inv_r = None
+    if inv_out is not None:
+        _rw(inv_out, dt, "C", "inv_out")
+        if inv_out.shape[0] != ann.shape[0]:
+            raise RuntimeError("inv_out shape mismatch in phase1 fused residual variance")
+    else:
+        inv_r = np.ascontiguousarray(_need("inv_right", inv_right), dtype=dt)
+        if inv_r.shape[0] != ann.shape[0]:
+            raise RuntimeError("inv_right shape mismatch in phase1")
+    if bin_init_mask is not None:
+        _rw(bin_init_mask, np.uint8, "C", "bin_init_mask")
+        if bin_init_mask.shape[0] != ann.shape[1]:
+            raise RuntimeError("bin_init_mask shape mismatch in phase1")
+    rows, nr = _rows(row_sel)
+    fn = getattr(_lib.load(), f"lds_phase1_compute_Xz_bed_chunk_{t}")
+    check(fn(enc(bed_prefix), enc(fam_path), int(blk_start), int(blk_end), ptr(rows), nr,
+             int(ddof), ptr(ann), ann.shape[0], ann.shape[1], ptr(inv_r), int(_need("v_start", v_start)),
+             int(_need("v_count", v_count)), int(_need("kmax_hint", kmax_hint)), _dist(rand_dist),
+             int(seed is not None), 0 if seed is None else int(seed) & (2**64 - 1), ptr(Xz),
+             Xz.shape[0], Xz.shape[1], ptr(bin_init_mask), _impute(impute_mode),
+             int(impute_seed is not None), 0 if impute_seed is None else int(impute_seed),
+             ptr(inv_out), float(resvar_eps)))
+
+
+# ---------------------------------------------------------------------------
+# Phase 2 (gwldcore.cpp:3759-3770)
+# ---------------------------------------------------------------------------
+def phase2_accum_XtXz_bed(bed_prefix, fam_path, blk_start, blk_end, row_sel=None, ddof=1,
+                          inv_left=_REQUIRED, tile_nvecs=_REQUIRED, Xz2d=_REQUIRED,
+                          meansq_accum=_REQUIRED, C=None, R=None, N_denom=0, impute_mode="hwe",
+                          impute_seed=None, mc_aggregate_sumsq=None, mc_per_snp_sumsq=None):
+    if C is not None and R is not None:
+        raise RuntimeError("covariate projection inside phase 2 is not supported by the B200 "
+                           "backend; pass the projected sketch with C=R=None as gw_ldscore.py does")
+    ms = _need("meansq_accum", meansq_accum)
+    t = _tsuffix(ms)
+    dt = ms.dtype
+    _rw(ms, dt, "C", "meansq_accum")
+    Xz = np.asfortranarray(_need("Xz2d", Xz2d), dtype=dt)
+    inv = np.ascontiguousarray(_need("inv_left", inv_left), dtype=dt)
+    if ms.ndim != 2:
+        raise RuntimeError("meansq_accum shape mismatch in phase2_accum_XtXz_bed")
+    if mc_aggregate_sumsq is not None:
+        _rw(mc_aggregate_sumsq, np.float64, "C", "mc_aggregate_sumsq")
+        if mc_aggregate_sumsq.shape[0] != ms.shape[1]:
+            raise RuntimeError("mc_aggregate_sumsq length must equal the annotation count")
+    if mc_per_snp_sumsq is not None:
+        _rw(mc_per_snp_sumsq, np.float64, "C", "mc_per_snp_sumsq")
+        if mc_per_snp_sumsq.shape != ms.shape:
+            raise RuntimeError("mc_per_snp_sumsq shape must match meansq_accum")
+    rows, nr = _rows(row_sel)
+    fn = getattr(_lib.load(), f"lds_phase2_accum_XtXz_bed_{t}")
+    check(fn(enc(bed_prefix), enc(fam_path), int(blk_start), int(blk_end), ptr(rows), nr,
+             int(ddof), ptr(inv), inv.shape[0], int(_need("tile_nvecs", tile_nvecs)), ptr(Xz),
+             Xz.shape[0], Xz.shape[1], ptr(ms), ms.shape[0], ms.shape[1], int(N_denom),
+             _impute(impute_mode), int(impute_seed is not None),
+             0 if impute_seed is None else int(impute_seed), ptr(mc_aggregate_sumsq),
+             ptr(mc_per_snp_sumsq)))
+
+
+# ---------------------------------------------------------------------------
+# Residual variances (gwldcore.cpp:3748-3757)
+# ---------------------------------------------------------------------------
+def precompute_residual_variances_bed(bed_prefix, fam_path, nsnps, step_size, row_sel=None,
+                                      ddof=1, eps=1e-10, compute_mu22=False, annot_all=None,
+                                      C=None, R=None, impute_mode="hwe", impute_seed=None,
+                                      snp_var_out=None, dtype=np.float64):
+    if C is not None or R is not None or compute_mu22 or snp_var_out is not None:
+        raise RuntimeError("covariates, mu22 and snp_var_out are not supported by the B200 "
+                           "residual-variance entry")
+    t = "f32" if np.dtype(dtype) == np.float32 else "f64"
+    out = np.empty(int(nsnps), dtype=np.float32 if t == "f32" else np.float64)
+    rows, nr = _rows(row_sel)
+    fn = getattr(_lib.load(), f"lds_precompute_residual_variances_bed_{t}")
+    check(fn(enc(bed_prefix), enc(fam_path), int(nsnps), int(step_size), ptr(rows), nr, int(ddof),
+             float(eps), _impute(impute_mode), int(impute_seed is not None),
+             0 if impute_seed is None else int(impute_seed), ptr(out)))
+    return out, None
+
+
+# ---------------------------------------------------------------------------
+# Whole-estimator entry (no reference counterpart as a single call; it fuses
+# the per-block loop of gw_ldscore.py:1753-2222).
+# ---------------------------------------------------------------------------
+def gw_ldscore(bed_rows, n_total, annot, nvecs, step_size, seed, rand_dist="rademacher",
+               vtile=None, ddof=1, impute_mode="mean", impute_seed=0, eps=1e-10,
+               dtype=np.float64, row_sel=None, with_mc=False):
+    """Genome-wide (partitioned) LD scores from an in-memory BED image.
+
+    ``bed_rows``: (M, row_bytes) uint8 SNP-major packed rows (no header).
+    ``annot``: (M, K) annotation matrix.  Returns a dict with ``ldscore``,
+    ``meansq_accum``, ``inv`` and, with ``with_mc``, the MC fourth-moment sums.
+    """
+    bed_rows = np.ascontiguousarray(bed_rows, dtype=np.uint8)
+    M, row_bytes = bed_rows.shape
+    annot = np.ascontiguousarray(annot, dtype=np.float64)
+    K = annot.shape[1]
+    ld = np.empty((M, K))
+    ms = np.empty((M, K))
+    inv = np.empty(M)
+    mca = np.empty(K) if with_mc else None
+    mcp = np.empty((M, K)) if with_mc else None
+    rows, nr = _rows(row_sel)
+    lib = _lib.load()
+    check(lib.lds_gw_ldscore(ptr(bed_rows), row_bytes, int(n_total), M, ptr(rows), nr, ptr(annot),
+                             K, int(nvecs), int(step_size), int(vtile or 0), int(seed),
+                             _dist(rand_dist), int(ddof), _impute(impute_mode), int(impute_seed),
+                             float(eps), int(np.dtype(dtype) == np.float32), ptr(ld), ptr(ms),
+                             ptr(inv), ptr(mca), ptr(mcp)))
+    return {"ldscore": ld, "meansq_accum": ms, "inv": inv, "mc_aggregate_sumsq": mca,
+            "mc_per_snp_sumsq": mcp}
+
+
+def last_timings() -> dict:
+    """Device times (ms) of the last gw_ldscore call."""
+    buf = np.zeros(4)
+    _lib.load().lds_last_timings(ptr(buf), 4)
+    return {"prepare_ms": buf[0], "phase1_ms": buf[1], "phase2_ms": buf[2], "total_ms": buf[3]}
+
+
+def debug_xt_products(bed_rows, n, y):
+    """Exact int64 (G^T y, O^T y) from the tensor-core kernel (verification)."""
+    bed_rows = np.ascontiguousarray(bed_rows, dtype=np.uint8)
+    y = np.asfortranarray(y, dtype=np.int8)
+    L = bed_rows.shape[0]
+    Q = y.shape[1]
+    g = np.empty((L, Q), dtype=np.int64)
+    o = np.empty((L, Q), dtype=np.int64)
+    check(_lib.load().lds_debug_xt_products(ptr(bed_rows), bed_rows.shape[1], int(n), L, ptr(y), Q,
+                                            ptr(g), ptr(o)))
+    return g, o
+
+
+def set_slices(s: int) -> None:
+    check(_lib.load().lds_set_slices(int(s)))
+
+
+def synth_bed_rows(n: int, m: int, seed: int, missing: bool = True) -> np.ndarray:
+    """Synthetic packed BED rows generated on the device (same bytes as bedfile.py)."""
+    from .bedfile import allele_freqs, hwe_thresholds
+
+    p = allele_freqs(seed, m)
+    t0, t1 = hwe_thresholds(p)
+    out = np.empty((m, (n + 3) // 4), dtype=np.uint8)
+    check(_lib.load().lds_synth_bed(int(n), int(m), int(seed), ptr(np.ascontiguousarray(t0)),
+                                    ptr(np.ascontiguousarray(t1)), int(missing), ptr(out)))
+    return out

@@ -1,0 +1,165 @@
+"""GPU parity tests for the genome-wide LD-score path (liblds.so through its C ABI).
+
+The checker is the oracle (our FP64 restatement, itself pinned to the
+reference's compiled code in test_oracle_pins.py) and, for the drop-in
+per-block functions, the reference's own compiled gwldcore.cpp.
+
+Tolerances: integer products are compared bit for bit.  LD scores carry the
+representation error of 4 int8 digits of the floating operands (28 bits), far
+below the 1e-6 relative bound asserted here.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+
+LD_RTOL = 1e-6
+
+
+@pytest.fixture(scope="module")
+def gw():
+    from summit_b200 import gwldcore
+
+    gwldcore.set_slices(4)
+    return gwldcore
+
+
+def test_tensor_core_products_are_exact(gw, oracle):
+    from summit_b200 import bedfile
+
+    rng = np.random.default_rng(5)
+    n, L, Q = 1000, 300, 37  # none of them a tile multiple
+    geno = bedfile.synth_genotypes(n, L, seed=99)
+    rows = bedfile.pack_bed_rows(geno)
+    y = np.asfortranarray(rng.integers(-127, 128, size=(n, Q), dtype=np.int8))
+    g_gpu, o_gpu = gw.debug_xt_products(rows, n, y)
+    g_ref, o_ref = oracle.int_products(rows, n, y)
+    np.testing.assert_array_equal(g_gpu, g_ref)
+    np.testing.assert_array_equal(o_gpu, o_ref)
+
+
+def test_device_synthetic_generator_matches_numpy(gw):
+    from summit_b200 import bedfile
+
+    n, m = 517, 64
+    dev = gw.synth_bed_rows(n, m, seed=31337)
+    host = bedfile.pack_bed_rows(bedfile.synth_genotypes(n, m, seed=31337))
+    np.testing.assert_array_equal(dev, host)
+
+
+@pytest.mark.parametrize("impute", ["mean", "hwe"])
+@pytest.mark.parametrize("dist", ["rademacher", "gaussian", "spherical"])
+def test_session_matches_oracle(gw, oracle, small_bed, impute, dist):
+    n, m, rows = small_bed["n"], small_bed["m"], small_bed["rows"]
+    rng = np.random.default_rng(3)
+    annot = np.ones((m, 3))
+    annot[:, 1] = rng.random(m) < 0.3
+    annot[:, 2] = rng.random(m) * (rng.random(m) < 0.5)  # continuous, some zeros
+    kw = dict(nvecs=40, seed=11, vtile=16, impute_seed=5)
+    gpu = gw.gw_ldscore(rows, n, annot, step_size=97, rand_dist=dist, impute_mode=impute,
+                        with_mc=True, **kw)
+    ora = oracle.gw_ldscore(rows, n, annot, step=97, dist=dist, impute=impute, with_mc=True, **kw)
+    # Residual variances are summed from code counts instead of sample by
+    # sample, so they agree to rounding (the sequential FP64 sum's order).
+    assert rel_err(gpu["inv"], ora["inv"]) < 1e-13
+    assert rel_err(gpu["meansq_accum"], ora["meansq_accum"]) < LD_RTOL
+    assert rel_err(gpu["ldscore"], ora["ldscore"]) < LD_RTOL
+    assert rel_err(gpu["mc_per_snp_sumsq"], ora["mc_per_snp_sumsq"]) < 10 * LD_RTOL
+    assert rel_err(gpu["mc_aggregate_sumsq"], ora["mc_aggregate_sumsq"]) < 10 * LD_RTOL
+
+
+def test_session_float_path_inputs(gw, oracle, small_bed):
+    n, m, rows = small_bed["n"], small_bed["m"], small_bed["rows"]
+    annot = np.ones((m, 1))
+    gpu = gw.gw_ldscore(rows, n, annot, 30, 64, 17, rand_dist="gaussian", dtype=np.float32)
+    ora = oracle.gw_ldscore(rows, n, annot, 30, 64, 17, dist="gaussian", as_float=True)
+    assert rel_err(gpu["ldscore"], ora["ldscore"]) < LD_RTOL
+
+
+def test_session_row_selection(gw, oracle, small_bed):
+    n, m, rows = small_bed["n"], small_bed["m"], small_bed["rows"]
+    sel = np.sort(np.random.default_rng(8).choice(n, size=201, replace=False)).astype(np.int64)
+    annot = np.ones((m, 1))
+    gpu = gw.gw_ldscore(rows, n, annot, 20, 50, 3, row_sel=sel, impute_mode="hwe", impute_seed=9)
+    ora = oracle.gw_ldscore(rows, n, annot, 20, 50, 3, rows=sel, impute="hwe", impute_seed=9)
+    assert rel_err(gpu["ldscore"], ora["ldscore"]) < LD_RTOL
+
+
+def test_session_is_deterministic(gw, small_bed):
+    n, m, rows = small_bed["n"], small_bed["m"], small_bed["rows"]
+    annot = np.ones((m, 2))
+    a = gw.gw_ldscore(rows, n, annot, 25, 64, 1, with_mc=True)
+    b = gw.gw_ldscore(rows, n, annot, 25, 64, 1)
+    np.testing.assert_array_equal(a["ldscore"], b["ldscore"])
+
+
+def _blockwise(mod, prefix, n, m, annot, nvecs, step, seed, dist, impute, dtype, vtile):
+    """The native call sequence of GenomewideLDScore._compute_ldscore
+    (gw_ldscore.py:1753-2222, no covariates) against module `mod`."""
+    from oracle.oracle import bounded_vtile_sizes, compute_blocks
+
+    annot = np.ascontiguousarray(annot, dtype=dtype)
+    K = annot.shape[1]
+    blocks = compute_blocks(m, step)
+    vt = bounded_vtile_sizes(nvecs, vtile)
+    inv = np.empty(m, dtype=dtype)
+    meansq = np.zeros((m, K), dtype=dtype)
+    mc_agg = np.zeros(K)
+    mc_snp = np.zeros((m, K))
+    kmax = [int((annot[s:e] != 0).sum(axis=0).max()) for (s, e) in blocks]
+    v0 = 0
+    for ti, V in enumerate(vt):
+        Xz = np.empty((n, K * V), dtype=dtype, order="F")
+        init = np.zeros(K, dtype=np.uint8)
+        for bi, (s, e) in enumerate(blocks):
+            mod.phase1_compute_Xz_bed_chunk(
+                bed_prefix=prefix, fam_path=prefix + ".fam", blk_start=s, blk_end=e,
+                row_sel=None, ddof=1, annot_blk=annot[s:e], inv_right=inv[s:e], v_start=v0,
+                v_count=V, kmax_hint=kmax[bi], rand_dist=dist, seed=seed, Xz2d_chunk=Xz,
+                bin_init_mask=init, impute_mode=impute, impute_seed=4,
+                inv_out=inv[s:e] if ti == 0 else None)
+        for k in np.flatnonzero(init == 0):
+            Xz[:, k * V:(k + 1) * V] = 0
+        for (s, e) in blocks:
+            mod.phase2_accum_XtXz_bed(
+                bed_prefix=prefix, fam_path=prefix + ".fam", blk_start=s, blk_end=e, row_sel=None,
+                ddof=1, inv_left=inv[s:e], tile_nvecs=V, Xz2d=Xz, meansq_accum=meansq,
+                mc_aggregate_sumsq=mc_agg, mc_per_snp_sumsq=mc_snp, C=None, R=None, N_denom=n,
+                impute_mode=impute, impute_seed=4)
+        v0 += V
+    return {"meansq": meansq, "inv": inv, "mc_agg": mc_agg, "mc_snp": mc_snp}
+
+
+@pytest.mark.parametrize("impute", ["mean", "hwe"])
+def test_dropin_blockwise_matches_reference(gw, reference, small_bed, impute):
+    """The per-block drop-in functions against the reference's own compiled
+    gwldcore.cpp, both driven by the reference driver's call sequence."""
+    prefix, n, m = small_bed["prefix"], small_bed["n"], small_bed["m"]
+    annot = np.ones((m, 2))
+    annot[1::2, 1] = 0
+    ours = _blockwise(gw, prefix, n, m, annot, 24, 100, 77, "rademacher", impute, np.float64, 16)
+    ref = reference.gw_ldscore(prefix, n, m, annot, 24, 100, 77, dist="rademacher", vtile=16,
+                               impute=impute, impute_seed=4, with_mc=True)
+    assert rel_err(ours["inv"], ref["inv"]) < 1e-13
+    assert rel_err(ours["meansq"], ref["meansq_accum"]) < LD_RTOL
+    assert rel_err(ours["mc_snp"], ref["mc_per_snp_sumsq"]) < 10 * LD_RTOL
+
+
+def test_dropin_float32_overload(gw, reference, small_bed):
+    prefix, n, m = small_bed["prefix"], small_bed["n"], small_bed["m"]
+    annot = np.ones((m, 1))
+    ours = _blockwise(gw, prefix, n, m, annot, 16, 128, 5, "spherical", "mean", np.float32, 16)
+    ref64 = reference.gw_ldscore(prefix, n, m, annot, 16, 128, 5, dist="spherical", vtile=16,
+                                 dtype=np.float64)
+    ref32 = reference.gw_ldscore(prefix, n, m, annot, 16, 128, 5, dist="spherical", vtile=16,
+                                 dtype=np.float32)
+    assert ours["meansq"].dtype == np.float32
+    # The float32 path draws float probes; its FP64-arithmetic counterpart is the
+    # oracle with float inputs.  Against the reference's own float32 run the
+    # difference is the reference's single-precision GEMM error.
+    assert rel_err(ours["meansq"], ref32["meansq_accum"]) < 1e-4
+    assert np.isfinite(ours["meansq"]).all() and rel_err(ref32["meansq_accum"], ref64["meansq_accum"]) < 1.0
