@@ -1,0 +1,390 @@
+#!/usr/bin/env python3
+"""Benchmark of the genotype x probe hot path: genome-wide partitioned LD scores.
+
+Workload (one "step" = one complete estimate over one synthetic BED batch):
+    N = 50,000 samples x M = 500,000 SNPs (HWE hard calls, AR(1) latent LD,
+    1% missing), K = 24 Bernoulli(0.1) annotations, B = 50 Rademacher probes,
+    SNP blocks of 1,000 (the reference's default --block-size), mean imputation.
+Metric: geno x probe TOPS = (2 N nnz(A) B  [phase 1]  +  2 N M K B  [phase 2]) / time,
+2 ops per multiply-accumulate.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+``value`` is device time of the estimate's kernels with the genotype image
+resident in HBM (CUDA events on the library stream, max over ranks); ``e2e``
+is the same estimate through the C ABI (lds_gw_ldscore) from pinned host
+buffers, host<->device copies included.  ``--impl reference`` times the
+reference's own native CPU code (compiled unchanged into oracle/_ref) on a
+bounded SNP sample of the same workload with all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+N_SAMPLES = 50_000
+M_SNPS = 500_000
+K_BINS = 24
+B_PROBES = 50
+BLOCK = 1_000
+DATA_SEED = 20260501
+ANNOT_SEED = 7
+PROBE_SEED = 12345
+METRIC = "geno x probe TOPS (genome-wide partitioned LD scores)"
+WORKLOAD = "gw_partitioned_ldscore_n50k_m500k_k24_b50_rademacher"
+
+
+def annotations(m: int, k: int = K_BINS) -> np.ndarray:
+    rng = np.random.default_rng(ANNOT_SEED)
+    return (rng.random((m, k)) < 0.1).astype(np.float64)
+
+
+def algorithmic_ops(n: int, annot: np.ndarray, b: int) -> tuple[float, float]:
+    """(phase-1 ops, phase-2 ops), 2 per multiply-accumulate."""
+    nnz = float((annot > 0).sum())
+    m, k = annot.shape
+    return 2.0 * n * nnz * b, 2.0 * n * m * k * b
+
+
+def env_int(name: str, default: int) -> int:
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+# ---------------------------------------------------------------------------
+# clocks sampler (nvidia-smi during the timed region)
+# ---------------------------------------------------------------------------
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except (OSError, ValueError):
+            self.p = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self) -> dict:
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        load = [s for s in sm if s > 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(load) if load else None,
+                "sm_max_mhz": mx or None, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU legs: the reference's own native code on a bounded SNP sample
+# ---------------------------------------------------------------------------
+def reference_sample(m_sample: int, tmpdir: str, packed=None) -> tuple[str, np.ndarray]:
+    """Write the first m_sample SNPs of the workload as a BED fileset.
+
+    ``packed`` (the workload's rows, when already generated) is sliced;
+    otherwise the rows come from the CPU copy of the generator in oracle/."""
+    from summit_b200 import bedfile
+
+    if packed is None:
+        from oracle.oracle import Oracle
+
+        packed = Oracle().synth_bed_rows(N_SAMPLES, m_sample, DATA_SEED)
+    prefix = bedfile.write_plink(Path(tmpdir) / f"sample{m_sample}", packed=packed[:m_sample],
+                                 n=N_SAMPLES)
+    return prefix, annotations(M_SNPS)[:m_sample]
+
+
+def run_reference(prefix: str, annot: np.ndarray, threads: int) -> float:
+    """One reference estimate (float32, the CLI default dtype); returns seconds.
+
+    The reference prints a per-block "[phase2-watch]" line on stderr; it is
+    silenced for the duration of the run."""
+    from oracle.oracle import Reference
+
+    ref = Reference()
+    ref.set_threads(threads)
+    m = annot.shape[0]
+    sys.stderr.flush()
+    saved = os.dup(2)
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 2)
+    try:
+        t0 = time.perf_counter()
+        ref.gw_ldscore(prefix, N_SAMPLES, m, annot, B_PROBES, BLOCK, PROBE_SEED,
+                       dist="rademacher", impute="mean", dtype=np.float32)
+        return time.perf_counter() - t0
+    finally:
+        os.dup2(saved, 2)
+        os.close(saved)
+        os.close(devnull)
+
+
+def cpu_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def calibrated_reference(target_s: float, tmpdir: str, threads: int, packed=None):
+    """Pick a SNP sample whose reference run takes about target_s seconds."""
+    m0 = 2000
+    prefix, annot = reference_sample(m0, tmpdir, packed)
+    t = run_reference(prefix, annot, threads)
+    m = int(min(M_SNPS, max(m0, round(m0 * target_s / max(t, 1e-3) / BLOCK) * BLOCK)))
+    if m != m0:
+        prefix, annot = reference_sample(m, tmpdir, packed)
+    return prefix, annot, m
+
+
+def reference_arm(args) -> None:
+    rank = env_int("RANK", 0)
+    if rank != 0:
+        return
+    threads = cpu_threads()
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    with tempfile.TemporaryDirectory() as td:
+        prefix, annot, m = calibrated_reference(float(os.environ.get("LDS_REF_STEP_S", "8")), td,
+                                                threads)
+        ops = sum(algorithmic_ops(N_SAMPLES, annot, B_PROBES))
+        for _ in range(args.warmup):
+            run_reference(prefix, annot, threads)
+        times = [run_reference(prefix, annot, threads) for _ in range(args.steps)]
+    from oracle.oracle import Reference
+
+    sec = float(np.mean(times))
+    value = ops / sec / 1e12
+    sample = (f"first {m} of {M_SNPS} SNPs, N={N_SAMPLES}, K={K_BINS}, B={B_PROBES}; "
+              "reference gwldcore.cpp+genotype.cpp compiled unchanged (float32 path), "
+              f"OpenMP+{Reference().blas_config().split()[0:2]}")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 6), "unit": "TOPS",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(sec * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample_snps": m, "l2": "inputs larger than L2"},
+        "cpu_baseline": {"value": round(value, 6), "unit": "TOPS", "cores": threads,
+                         "kind": "reference", "sample": sample},
+        "e2e": {"value": round(value, 6), "unit": "TOPS", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def read_traffic() -> dict | None:
+    """Per-launch DRAM bytes of the phase-2 kernel from the committed ncu summary."""
+    f = ROOT / "profiles" / "p2_kernel_gw_n50k_m500k.md"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return {"bytes": float(line.split(":", 1)[1].strip())}
+            except ValueError:
+                return None
+    return None
+
+
+def ours_arm(args) -> None:
+    import torch
+
+    rank = env_int("RANK", 0)
+    world = env_int("WORLD_SIZE", 1)
+    local = env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    from summit_b200 import _lib, gwldcore
+    from summit_b200.session import GwSession, set_stream
+
+    lib = _lib.load()
+    stream = torch.cuda.Stream()
+    set_stream(stream.cuda_stream)
+
+    n, m = N_SAMPLES, env_int("LDS_BENCH_M", M_SNPS)
+    seed = DATA_SEED + rank  # weak scaling: every rank estimates its own batch
+    bed = gwldcore.synth_bed_rows(n, m, seed)
+    pinned = torch.empty(bed.shape, dtype=torch.uint8, pin_memory=True)
+    pinned.numpy()[:] = bed
+    bed_host = pinned.numpy()
+    del bed
+    annot = annotations(m)
+    ops1, ops2 = algorithmic_ops(n, annot, B_PROBES)
+    ops = ops1 + ops2
+
+    sess = GwSession(bed_host, n, impute_mode="mean")
+    plan = sess.plan(annot, B_PROBES, BLOCK, PROBE_SEED, "rademacher")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        plan.execute()
+    torch.cuda.synchronize()
+    plan.kernel_ms()  # drop warm-up kernel times
+
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    launches0 = lib.lds_kernel_launches()
+    with Clocks(local) as clk:
+        barrier()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            plan.execute()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    launches = int(lib.lds_kernel_launches() - launches0)
+    ms = ev0.elapsed_time(ev1) / args.steps
+    kms = plan.kernel_ms()
+    res = plan.results()
+    assert np.isfinite(res["ldscore"]).all()
+
+    # End to end through the C ABI from pinned host buffers.
+    e2e_steps = max(1, min(args.steps, env_int("LDS_E2E_STEPS", 2)))
+    gwldcore.gw_ldscore(bed_host, n, annot, B_PROBES, BLOCK, PROBE_SEED)  # warm
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        out = gwldcore.gw_ldscore(bed_host, n, annot, B_PROBES, BLOCK, PROBE_SEED)
+    torch.cuda.synchronize()
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
+    barrier()
+    assert np.isfinite(out["ldscore"]).all()
+    nnz = int((annot > 0).sum())
+    h2d = int(bed_host.nbytes + m * B_PROBES * 8 + nnz * 12 + m * 8)
+    d2h = int(m * K_BINS * 8)
+
+    t = torch.tensor([ms, e2e_ms], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms, e2e_ms = float(t[0]), float(t[1])
+
+    if rank == 0:
+        peaks = {}
+        pf = ROOT / "MEASURED_PEAKS.json"
+        if pf.exists():
+            peaks = json.loads(pf.read_text())
+        peak = float(peaks.get("bf16_tflops", 1590.0))
+        p2_ms = kms["phase2"]
+        achieved = ops2 / (p2_ms * 1e-3) / 1e12 if p2_ms > 0 else None
+        tr = read_traffic()
+        clocks = clk.summary()
+        line = {
+            "metric": METRIC, "value": round(world * ops / (ms * 1e-3) / 1e12, 3), "unit": "TOPS",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int8-digit exact products, f64 epilogue",
+            "data": "synthetic (seeded HWE/AR(1) generator on device)",
+            "config": {"workload": WORKLOAD, "N": n, "M": m, "K": K_BINS, "B": B_PROBES,
+                       "block": BLOCK, "impute": "mean", "digits": lib.lds_get_slices(),
+                       "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (6.3 GB genotype image per step)"},
+            "kernel_ms": {k: round(v, 3) for k, v in kms.items()},
+            "roofline": {
+                "kernel": "p2_kernel (phase 2: X^T Y + LD epilogue)", "bound": "tensor",
+                "achieved": None if achieved is None else round(achieved, 3),
+                "peak": peak, "unit": "TFLOP/s",
+                "frac": None if achieved is None else round(achieved / peak, 4),
+                "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)" if peaks else "fallback",
+                "traffic": None if tr is None else tr["bytes"],
+                "algorithmic_ops_per_launch": ops2},
+            "e2e": {"value": round(world * ops / (e2e_ms * 1e-3) / 1e12, 3), "unit": "TOPS",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "ms_per_step": round(e2e_ms, 1)},
+            "gpu_launches": launches,
+            "clocks": clocks,
+        }
+        if world == 1 and not os.environ.get("LDS_SKIP_CPU_BASELINE"):
+            threads = cpu_threads()
+            with tempfile.TemporaryDirectory() as td:
+                prefix, ann_s, ms_snps = calibrated_reference(
+                    float(os.environ.get("LDS_CPU_BASELINE_S", "12")), td, threads, bed_host)
+                sec = run_reference(prefix, ann_s, threads)
+            cops = sum(algorithmic_ops(n, ann_s, B_PROBES))
+            line["cpu_baseline"] = {
+                "value": round(cops / sec / 1e12, 6), "unit": "TOPS", "cores": threads,
+                "kind": "reference",
+                "sample": f"first {ms_snps} SNPs of the workload (N={n}, K={K_BINS}, "
+                          f"B={B_PROBES}); reference gwldcore.cpp compiled unchanged, float32, "
+                          f"{sec:.1f} s"}
+        print(json.dumps(line), flush=True)
+
+    plan.close()
+    sess.close()
+    set_stream(None)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        ours_arm(args)
+
+
+if __name__ == "__main__":
+    main()

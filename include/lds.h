@@ -166,6 +166,35 @@ int lds_gw_ldscore_bed(
     double resvar_eps, int as_float, double* ldscore, double* meansq_accum,
     double* inv_out, double* mc_aggregate_sumsq, double* mc_per_snp_sumsq);
 
+/* ---------------------------------------------------------------------
+ * Resident form of lds_gw_ldscore for repeated runs and timing.
+ *   lds_geno_create: upload + repack + per-SNP statistics (+ HWE imputation)
+ *     of a BED image into device memory; returns a handle.
+ *   lds_gw_plan_create: residual variances, CSR lists, probe streams and all
+ *     other kernel inputs of one estimate, uploaded; returns a plan.
+ *   lds_gw_plan_execute: enqueue the estimate's kernels (phase 1 weights,
+ *     phase 1, sketch digits, phase 2) on the library stream; asynchronous.
+ *   lds_gw_plan_results: wait, then copy out and finalize like lds_gw_ldscore.
+ *   lds_gw_plan_kernel_ms: CUDA-event time per kernel kind of the last
+ *     execute: [weights, phase 1, sketch digits, phase 2] in ms (plans with at
+ *     most 3 V-tiles).
+ * No reference counterpart as single calls: together they perform the
+ * native work of gw_ldscore.py:1753-2222 like lds_gw_ldscore.
+ * ------------------------------------------------------------------- */
+int lds_set_stream(void* cuda_stream); /* NULL restores the library's own stream */
+int lds_geno_create(const uint8_t* bed_rows, int64_t bed_row_bytes, int64_t n_total, int64_t M,
+                    const int64_t* row_sel, int64_t n_row_sel, int impute_mode,
+                    uint64_t impute_seed, int ddof, int64_t* handle_out);
+int lds_geno_destroy(int64_t handle);
+int lds_gw_plan_create(int64_t geno, const double* annot, int64_t K, int nvecs, int step_size,
+                       int vtile, uint64_t seed, int rand_dist, double resvar_eps, int as_float,
+                       int with_mc, int64_t* plan_out);
+int lds_gw_plan_execute(int64_t plan);
+int lds_gw_plan_results(int64_t plan, double* ldscore, double* meansq_accum, double* inv_out,
+                        double* mc_aggregate_sumsq, double* mc_per_snp_sumsq);
+int lds_gw_plan_kernel_ms(int64_t plan, double* ms4);
+int lds_gw_plan_destroy(int64_t plan);
+
 /* Device timing of the last lds_gw_ldscore call (milliseconds, CUDA events
  * on the library stream): [0] upload+prepare, [1] phase 1 total, [2] phase 2
  * total, [3] whole call. */

@@ -348,6 +348,37 @@ ORC_EXPORT void orc_int_products(const uint8_t* bed, int64_t nbytes, int64_t N, 
     }
 }
 
+// The seeded synthetic genotype generator of summit_b200/bedfile.py, in C for
+// CPU-side sample generation (identical bytes): packed rows of ceil(n/4).
+ORC_EXPORT void orc_synth_bed(int64_t n, int64_t M, uint64_t seed, const int64_t* t0,
+                              const int64_t* t1, int missing, uint8_t* out) {
+    const uint64_t k2 = mix64(seed ^ mix64(2ULL));
+    const uint64_t k3 = mix64(seed ^ mix64(3ULL));
+    const int64_t nb = (n + 3) / 4;
+#pragma omp parallel for schedule(static)
+    for (int64_t b = 0; b < nb; ++b) {
+        long long u[4] = {0, 0, 0, 0};
+        for (int64_t j = 0; j < M; ++j) {
+            uint32_t byte = 0;
+            for (int t = 0; t < 4; ++t) {
+                const int64_t i = b * 4 + t;
+                if (i >= n) break;
+                const uint64_t r = mix64(k2 ^ mix64(((uint64_t)j << 32) | (uint64_t)i));
+                const long long e = (long long)(r & 0xFFFFULL) + (long long)((r >> 16) & 0xFFFFULL) +
+                                    (long long)((r >> 32) & 0xFFFFULL) + (long long)(r >> 48) -
+                                    131070LL;
+                u[t] = (j == 0) ? e : ((58982LL * u[t] + 28567LL * e) >> 16);
+                uint32_t code = (u[t] < t0[j]) ? 0u : (u[t] < t1[j]) ? 2u : 3u;
+                if (missing &&
+                    (mix64(k3 ^ mix64(((uint64_t)j << 32) | (uint64_t)i)) >> 32) < 42949673ULL)
+                    code = 1u;
+                byte |= code << (2 * t);
+            }
+            out[j * nb + b] = (uint8_t)byte;
+        }
+    }
+}
+
 ORC_EXPORT int orc_max_threads() {
 #ifdef _OPENMP
     return omp_get_max_threads();

@@ -73,7 +73,18 @@ class Oracle:
                                        _p, _p, _dbl, _int]
         L.orc_inv_resvar_block.argtypes = [_p, _i64, _int, _dbl, _p]
         L.orc_int_products.argtypes = [_p, _i64, _i64, _int, _p, _i64, _p, _p]
+        L.orc_synth_bed.argtypes = [_i64, _i64, _u64, _p, _p, _int, _p]
         self.lib = L
+
+    def synth_bed_rows(self, n: int, m: int, seed: int, missing: bool = True) -> np.ndarray:
+        """The synthetic generator of summit_b200/bedfile.py in C (same bytes)."""
+        from summit_b200.bedfile import allele_freqs, hwe_thresholds
+
+        t0, t1 = hwe_thresholds(allele_freqs(seed, m))
+        out = np.empty((m, (n + 3) // 4), dtype=np.uint8)
+        self.lib.orc_synth_bed(n, m, seed, _ptr(np.ascontiguousarray(t0)),
+                               _ptr(np.ascontiguousarray(t1)), int(missing), _ptr(out))
+        return out
 
     def standardize(self, bed_rows: np.ndarray, n_total: int, blk_start: int, blk_end: int,
                     rows=None, ddof=1, impute="mean", impute_seed=0):
@@ -202,14 +213,29 @@ class Reference:
                 _str, _str, _int, _int, _p, _i64, _int, _p, _i64, _int, _p, _i64, _i64, _p, _i64,
                 _p, _int, _int, _u64, _p, _p]
         L.ref_set_num_threads.argtypes = [_int]
+        L.ref_set_omp_threads.argtypes = [_int]
+        L.ref_set_blas_threads.argtypes = [_int]
         self.lib = L
+        self.threads = 0
 
     def _chk(self, rc):
         if rc:
             raise RuntimeError(self.lib.ref_last_error().decode())
 
     def set_threads(self, n: int):
+        self.threads = int(n)
         self.lib.ref_set_num_threads(int(n))
+
+    def _phase_threads(self, phase: int):
+        """OpenMP/BLAS split of the reference driver (gw_ldscore.py:1765-1771)."""
+        if self.threads <= 0:
+            return
+        if phase == 1:
+            self.lib.ref_set_omp_threads(self.threads)
+            self.lib.ref_set_blas_threads(1)
+        else:
+            self.lib.ref_set_omp_threads(1)
+            self.lib.ref_set_blas_threads(self.threads)
 
     def blas_config(self) -> str:
         return self.lib.ref_blas_config().decode()
@@ -299,6 +325,7 @@ class Reference:
             fuse = ti == 0
             Xz = Xz_chunk[:, :K * V]
             init.fill(0)
+            self._phase_threads(1)
             for bi, (s, e) in enumerate(blocks):
                 if kmax[bi] == 0 and not fuse:
                     continue
@@ -307,6 +334,7 @@ class Reference:
                                 inv_out=inv[s:e] if fuse else None)
             for k in np.flatnonzero(init == 0):
                 Xz[:, k * V:(k + 1) * V] = 0
+            self._phase_threads(2)
             for (s, e) in blocks:
                 self.phase2_bed(prefix, s, e, inv[s:e], V, Xz, meansq, N_denom, rows, ddof,
                                 impute, impute_seed, mc_agg, mc_snp)

@@ -187,6 +187,11 @@ REF_EXPORT void ref_set_num_threads(int n) {
     openblas_set_num_threads(n);
 }
 REF_EXPORT int ref_get_max_threads() { return get_max_threads(); }
+// The reference driver splits threads between OpenMP and BLAS per phase
+// (gw_ldscore.py:1765-1771, :2027, :2086): phase 1 runs one BLAS thread per
+// OpenMP member, phase 2 one OpenMP thread and a threaded BLAS.
+REF_EXPORT void ref_set_omp_threads(int n) { set_num_threads(n); }
+REF_EXPORT void ref_set_blas_threads(int n) { openblas_set_num_threads(n); }
 REF_EXPORT const char* ref_blas_config() { return openblas_get_config(); }
 REF_EXPORT void ref_clear_caches() {
     clear_phase1_csr_cache();

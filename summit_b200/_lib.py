@@ -40,6 +40,15 @@ SIGNATURES: dict[str, tuple] = {
                                   _int, _int, _u64, _dbl, _int, _p, _p, _p, _p, _p]),
     "lds_debug_xt_products": (_int, [_p, _i64, _i64, _i64, _p, _i64, _p, _p]),
     "lds_synth_bed": (_int, [_i64, _i64, _u64, _p, _p, _int, _p]),
+    "lds_set_stream": (_int, [_p]),
+    "lds_geno_create": (_int, [_p, _i64, _i64, _i64, _p, _i64, _int, _u64, _int, _p]),
+    "lds_geno_destroy": (_int, [_i64]),
+    "lds_gw_plan_create": (_int, [_i64, _p, _i64, _int, _int, _int, _u64, _int, _dbl, _int, _int,
+                                  _p]),
+    "lds_gw_plan_execute": (_int, [_i64]),
+    "lds_gw_plan_results": (_int, [_i64, _p, _p, _p, _p, _p]),
+    "lds_gw_plan_kernel_ms": (_int, [_i64, _p]),
+    "lds_gw_plan_destroy": (_int, [_i64]),
 }
 for _t in ("f32", "f64"):
     SIGNATURES[f"lds_phase1_compute_Xz_bed_chunk_{_t}"] = (

@@ -16,6 +16,7 @@
 #include <fcntl.h>
 #include <limits>
 #include <list>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <random>
@@ -468,6 +469,33 @@ void quantize_sketch(Context& c, Prepared& P, int64_t K, int V) {
 }
 
 // Phase 2 over SNPs [j0, j1) into device accumulators (out_row0 offset).
+double extreme_warn_env() {
+    static const double warn = [] {
+        const char* s = std::getenv("SUMMIT_P2_EXTREME_LD_WARN");
+        if (!s || !*s) s = std::getenv("SUMMIT_P2_ABS_LD_MAX");
+        double v = 1.0e10;
+        if (s && *s) {
+            char* end = nullptr;
+            const double x = std::strtod(s, &end);
+            if (end != s && std::isfinite(x)) v = x;
+        }
+        return v > 0.0 ? v : std::numeric_limits<double>::infinity();
+    }();
+    return warn;
+}
+
+int drop_extreme_env() {
+    static const int drop = [] {
+        const char* s = std::getenv("SUMMIT_P2_DROP_EXTREME");
+        if (!s || !*s) return 1;
+        if (!strcmp(s, "0") || !strcmp(s, "false") || !strcmp(s, "FALSE") || !strcmp(s, "no") ||
+            !strcmp(s, "NO"))
+            return 0;
+        return 1;
+    }();
+    return drop;
+}
+
 void run_phase2(Context& c, Prepared& P, int64_t K, int V, int64_t j0, int64_t j1,
                 int64_t out_row0, double* d_accum, double* d_mc, const double* d_lscale) {
     P2Args a;
@@ -486,27 +514,8 @@ void run_phase2(Context& c, Prepared& P, int64_t K, int V, int64_t j0, int64_t j
     a.accum = d_accum;
     a.mc = d_mc;
     a.guard_counts = c.guards.as<unsigned long long>(2);
-    static const double warn = [] {
-        const char* s = std::getenv("SUMMIT_P2_EXTREME_LD_WARN");
-        if (!s || !*s) s = std::getenv("SUMMIT_P2_ABS_LD_MAX");
-        double v = 1.0e10;
-        if (s && *s) {
-            char* end = nullptr;
-            const double x = std::strtod(s, &end);
-            if (end != s && std::isfinite(x)) v = x;
-        }
-        return v > 0.0 ? v : std::numeric_limits<double>::infinity();
-    }();
-    static const int drop = [] {
-        const char* s = std::getenv("SUMMIT_P2_DROP_EXTREME");
-        if (!s || !*s) return 1;
-        if (!strcmp(s, "0") || !strcmp(s, "false") || !strcmp(s, "FALSE") || !strcmp(s, "no") ||
-            !strcmp(s, "NO"))
-            return 0;
-        return 1;
-    }();
-    a.extreme_warn = warn;
-    a.drop_extreme = drop;
+    a.extreme_warn = extreme_warn_env();
+    a.drop_extreme = drop_extreme_env();
     launch_p2(P.g, a, c.st);
 }
 
@@ -777,7 +786,266 @@ void resvar_impl(const char* bed_prefix, const char* fam_path, int nsnps, const 
     for (int64_t j = 0; j < nsnps; ++j) inv_out[j] = inv_resvar<T>(P, j, eps);
 }
 
-// Whole-estimator session on an in-memory BED image.
+// ---------------------------------------------------------------------------
+// Genome-wide estimator as geno handle + plan + execute.  A plan holds every
+// device input of the kernels (CSR lists, probes, left scales), so execute()
+// is a pure sequence of asynchronous launches on the library stream — the
+// unit the benchmark times and that can be captured in a CUDA graph.
+// ---------------------------------------------------------------------------
+struct GwPlan {
+    std::shared_ptr<Prepared> P;
+    int64_t K = 0;
+    int nvecs = 0, S = 4, as_float = 0, with_mc = 0;
+    std::vector<int> vt;
+    std::vector<double> inv, Mk;
+    struct Tile {
+        int V = 0, Vp = 0;
+        Csr csr;
+        DevBuf rowind, sc, binoff, wqoff, z, wq, wcs;
+    };
+    std::vector<std::unique_ptr<Tile>> tiles;
+    DevBuf y, yq, ycs, accum, mc, lscale, guards;
+    // One set of events per execute (up to kMaxTimed executes between reads):
+    // a start event and one after each kernel of each V-tile.
+    static constexpr int kMaxTimed = 64;
+    std::vector<std::vector<cudaEvent_t>> evsets;
+    int pending = 0;
+    double kernel_ms[4] = {0, 0, 0, 0};  // weights, phase 1, sketch digits, phase 2
+    ~GwPlan() {
+        for (auto& s : evsets)
+            for (cudaEvent_t e : s) cudaEventDestroy(e);
+    }
+};
+
+std::map<int64_t, std::shared_ptr<Prepared>>& geno_table() {
+    static std::map<int64_t, std::shared_ptr<Prepared>> t;
+    return t;
+}
+std::map<int64_t, std::unique_ptr<GwPlan>>& plan_table() {
+    static std::map<int64_t, std::unique_ptr<GwPlan>> t;
+    return t;
+}
+int64_t next_handle() {
+    static int64_t h = 0;
+    return ++h;
+}
+
+std::unique_ptr<GwPlan> plan_create(Context& c, std::shared_ptr<Prepared> P, const double* annot,
+                                    int64_t K, int nvecs, int step, int vtile, uint64_t seed,
+                                    int dist, double eps, int as_float, int with_mc) {
+    const int64_t M = P->g.M, N = P->g.N;
+    if (nvecs <= 0 || step <= 0 || K <= 0 || M <= 0) fail(LDS_ERR_ARG, "invalid sizes");
+    if (K > 512) fail(LDS_ERR_ARG, "B too large for fixed seg buffers in phase2_accum_XtXz_bed");
+    auto pl = std::make_unique<GwPlan>();
+    pl->P = P;
+    pl->K = K;
+    pl->nvecs = nvecs;
+    pl->S = c.slices;
+    pl->as_float = as_float;
+    pl->with_mc = with_mc;
+    {
+        int width = std::min(nvecs, vtile > 0 ? vtile : nvecs);
+        if (width >= 64) width = std::max(64, (width / 64) * 64);
+        for (int s = 0; s < nvecs; s += width) pl->vt.push_back(std::min(width, nvecs - s));
+    }
+    // Residual variances (the reference fuses them into the first phase-1
+    // pass; same values), rounded to the working type.
+    pl->inv.resize((size_t)M);
+    for (int64_t j = 0; j < M; ++j)
+        pl->inv[(size_t)j] =
+            as_float ? (double)inv_resvar<float>(*P, j, eps) : inv_resvar<double>(*P, j, eps);
+    pl->Mk.assign((size_t)K, 0.0);
+    for (int64_t j = 0; j < M; ++j)
+        for (int64_t k = 0; k < K; ++k) pl->Mk[(size_t)k] += annot[j * K + k];
+    // Left scales (gwldcore.cpp:2436-2445) with N_denom = N - ddof + 1.
+    const double denom = std::max(1.0, (double)(N - P->ddof + 1) - 1.0);
+    const double inv_denom2 = 1.0 / (denom * denom);
+    std::vector<double> ls((size_t)M);
+    for (int64_t j = 0; j < M; ++j) {
+        const double v = pl->inv[(size_t)j];
+        ls[(size_t)j] = (std::isfinite(v) && v > 0.0) ? v * v * inv_denom2 : 0.0;
+    }
+    h2d(pl->lscale.as<double>((size_t)M), ls.data(), (size_t)M, c.st);
+    std::vector<float> annot_f, inv_f;
+    if (as_float) {
+        annot_f.assign(annot, annot + M * K);
+        inv_f.resize((size_t)M);
+        for (int64_t j = 0; j < M; ++j) inv_f[(size_t)j] = (float)pl->inv[(size_t)j];
+    }
+    const int nblk = (int)((M + step - 1) / step);
+    const unsigned hw = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+    int vmax = 0, v0 = 0;
+    for (int V : pl->vt) {
+        vmax = std::max(vmax, V);
+        auto t = std::make_unique<GwPlan::Tile>();
+        t->V = V;
+        t->Vp = (int)round_up(V, kColTile);
+        t->csr = as_float ? build_csr<float>(annot_f.data(), inv_f.data(), M, K, 0, t->Vp, pl->S)
+                          : build_csr<double>(annot, pl->inv.data(), M, K, 0, t->Vp, pl->S);
+        // Probe streams per SNP block (mt19937_64), generated in parallel.
+        std::vector<double> Z((size_t)(M * V));
+        std::vector<std::thread> th;
+        std::atomic<int> next{0};
+        for (unsigned w = 0; w < hw; ++w)
+            th.emplace_back([&] {
+                for (int b; (b = next.fetch_add(1)) < nblk;) {
+                    const int s = b * step;
+                    const int L = (int)std::min<int64_t>(step, M - s);
+                    std::vector<double> blk((size_t)L * V);
+                    if (as_float) make_probes<float>(seed, s, v0, L, V, dist, blk.data(), L);
+                    else make_probes<double>(seed, s, v0, L, V, dist, blk.data(), L);
+                    for (int cc = 0; cc < V; ++cc)
+                        std::memcpy(&Z[(size_t)cc * M + s], &blk[(size_t)cc * L], sizeof(double) * L);
+                }
+            });
+        for (auto& x : th) x.join();
+        const Csr& cs = t->csr;
+        const size_t nm = std::max<size_t>(cs.rowind.size(), 1);
+        h2d(t->rowind.as<int32_t>(nm), cs.rowind.data(), cs.rowind.size(), c.st);
+        h2d(t->sc.as<double>(nm), cs.sc.data(), cs.sc.size(), c.st);
+        h2d(t->binoff.as<int64_t>(cs.bin_off.size()), cs.bin_off.data(), cs.bin_off.size(), c.st);
+        h2d(t->wqoff.as<int64_t>(cs.wq_off.size()), cs.wq_off.data(), cs.wq_off.size(), c.st);
+        h2d(t->z.as<double>(Z.size()), Z.data(), Z.size(), c.st);
+        t->wq.as<int8_t>((size_t)std::max<int64_t>(cs.wq_bytes, 16));
+        t->wcs.as<double>((size_t)(K * t->Vp));
+        ck(cudaStreamSynchronize(c.st), "plan upload");  // Z is a stack temporary
+        pl->tiles.push_back(std::move(t));
+        v0 += V;
+    }
+    const int vpmax = (int)round_up(vmax, kColTile);
+    pl->y.as<double>((size_t)(P->g.N_pad * K * vmax));
+    pl->yq.as<int8_t>((size_t)(pl->S * K * vpmax * P->g.N_pad));
+    pl->ycs.as<double>((size_t)(K * vpmax));
+    pl->accum.as<double>((size_t)(M * K));
+    if (with_mc) pl->mc.as<double>((size_t)(M * K));
+    pl->guards.as<unsigned long long>(2);
+    ck(cudaStreamSynchronize(c.st), "plan");
+    return pl;
+}
+
+void plan_execute(Context& c, GwPlan& pl) {
+    Prepared& P = *pl.P;
+    const int64_t M = P.g.M, K = pl.K;
+    ck(cudaMemsetAsync(pl.accum.p, 0, sizeof(double) * (size_t)(M * K), c.st), "memset");
+    if (pl.with_mc) ck(cudaMemsetAsync(pl.mc.p, 0, sizeof(double) * (size_t)(M * K), c.st), "memset");
+    ck(cudaMemsetAsync(pl.guards.p, 0, 16, c.st), "memset");
+    const bool tm = pl.pending < GwPlan::kMaxTimed;
+    cudaEvent_t* ev = nullptr;
+    if (tm) {
+        if ((int)pl.evsets.size() <= pl.pending) {
+            std::vector<cudaEvent_t> set(1 + 4 * pl.tiles.size());
+            for (auto& x : set) ck(cudaEventCreate(&x), "event");
+            pl.evsets.push_back(std::move(set));
+        }
+        ev = pl.evsets[(size_t)pl.pending].data();
+    }
+    int e = 0;
+    if (tm) ck(cudaEventRecord(ev[e++], c.st), "event");
+    for (auto& tp : pl.tiles) {
+        GwPlan::Tile& t = *tp;
+        P1Weights w;
+        w.K = (int)K;
+        w.V = t.V;
+        w.Vp = t.Vp;
+        w.S = pl.S;
+        w.rowind = static_cast<int32_t*>(t.rowind.p);
+        w.sc = static_cast<double*>(t.sc.p);
+        w.bin_off = static_cast<int64_t*>(t.binoff.p);
+        w.wq_off = static_cast<int64_t*>(t.wqoff.p);
+        w.wq = static_cast<int8_t*>(t.wq.p);
+        w.colscale = static_cast<double*>(t.wcs.p);
+        launch_p1_weights(w, static_cast<double*>(P.d_mean.p), static_cast<double*>(P.d_sdinv.p),
+                          static_cast<double*>(t.z.p), M, 0, c.st);
+        if (tm) ck(cudaEventRecord(ev[e++], c.st), "event");
+        launch_p1(P.g, w, nullptr, static_cast<double*>(pl.y.p), c.st);
+        if (tm) ck(cudaEventRecord(ev[e++], c.st), "event");
+        launch_quantize_y(static_cast<double*>(pl.y.p), P.g.N, P.g.N_pad, (int)K, t.V, t.Vp, pl.S,
+                          static_cast<int8_t*>(pl.yq.p), static_cast<double*>(pl.ycs.p), c.st);
+        if (tm) ck(cudaEventRecord(ev[e++], c.st), "event");
+        P2Args a;
+        a.K = (int)K;
+        a.V = t.V;
+        a.Vp = t.Vp;
+        a.S = pl.S;
+        a.j0 = 0;
+        a.j1 = M;
+        a.out_row0 = 0;
+        a.Yq = static_cast<int8_t*>(pl.yq.p);
+        a.colscale = static_cast<double*>(pl.ycs.p);
+        a.mean = static_cast<double*>(P.d_mean.p);
+        a.sdinv = static_cast<double*>(P.d_sdinv.p);
+        a.left_scale = static_cast<double*>(pl.lscale.p);
+        a.accum = static_cast<double*>(pl.accum.p);
+        a.mc = pl.with_mc ? static_cast<double*>(pl.mc.p) : nullptr;
+        a.guard_counts = static_cast<unsigned long long*>(pl.guards.p);
+        a.extreme_warn = extreme_warn_env();
+        a.drop_extreme = drop_extreme_env();
+        launch_p2(P.g, a, c.st);
+        if (tm) ck(cudaEventRecord(ev[e++], c.st), "event");
+    }
+    if (tm) ++pl.pending;
+    ck(cudaGetLastError(), "launch");
+}
+
+// Mean per-execute kernel times over the executes since the last call.
+void plan_kernel_times(GwPlan& pl) {
+    if (pl.pending == 0) return;
+    for (double& x : pl.kernel_ms) x = 0.0;
+    const size_t nt = pl.tiles.size();
+    for (int p = 0; p < pl.pending; ++p) {
+        const std::vector<cudaEvent_t>& ev = pl.evsets[(size_t)p];
+        ck(cudaEventSynchronize(ev[4 * nt]), "event sync");
+        for (size_t t = 0; t < nt; ++t)
+            for (int k = 0; k < 4; ++k) {
+                float ms = 0.f;
+                ck(cudaEventElapsedTime(&ms, ev[4 * t + k], ev[4 * t + k + 1]), "elapsed");
+                pl.kernel_ms[k] += ms;
+            }
+    }
+    for (double& x : pl.kernel_ms) x /= (double)pl.pending;
+    pl.pending = 0;
+}
+
+void plan_results(Context& c, GwPlan& pl, double* ldscore, double* meansq_out, double* inv_out,
+                  double* mc_agg, double* mc_snp) {
+    const int64_t M = pl.P->g.M, K = pl.K, N = pl.P->g.N;
+    std::vector<double> acc((size_t)(M * K));
+    d2h(acc.data(), static_cast<double*>(pl.accum.p), acc.size(), c.st);
+    std::vector<double> mcv;
+    if (pl.with_mc) {
+        mcv.resize((size_t)(M * K));
+        d2h(mcv.data(), static_cast<double*>(pl.mc.p), mcv.size(), c.st);
+    }
+    ck(cudaStreamSynchronize(c.st), "results");
+    plan_kernel_times(pl);
+    {
+        unsigned long long h[2] = {0, 0};
+        d2h(h, static_cast<unsigned long long*>(pl.guards.p), 2, c.st);
+        ck(cudaStreamSynchronize(c.st), "guards");
+        if (h[0] || h[1])
+            std::fprintf(stderr,
+                         "[phase2-warning] accum: dropped %llu non-finite and %llu extreme "
+                         "LD-score updates; inspect this run before using it.\n", h[0], h[1]);
+    }
+    if (meansq_out) std::memcpy(meansq_out, acc.data(), sizeof(double) * acc.size());
+    if (inv_out) std::memcpy(inv_out, pl.inv.data(), sizeof(double) * (size_t)M);
+    // Finalize: / nvecs, minus M_k / (N - ddof) (gw_ldscore.py:2197, :2220-2222).
+    const double nd = (double)(N - pl.P->ddof);
+    if (ldscore)
+        for (int64_t j = 0; j < M; ++j)
+            for (int64_t k = 0; k < K; ++k)
+                ldscore[j * K + k] = acc[(size_t)(j * K + k)] / (double)pl.nvecs - pl.Mk[(size_t)k] / nd;
+    if (pl.with_mc) {
+        if (mc_agg)
+            for (int64_t k = 0; k < K; ++k) {
+                double agg = 0.0;
+                for (int64_t j = 0; j < M; ++j) agg += mcv[(size_t)(j * K + k)];
+                mc_agg[k] = agg;
+            }
+        if (mc_snp) std::memcpy(mc_snp, mcv.data(), sizeof(double) * mcv.size());
+    }
+}
+
 void gw_ldscore_impl(const uint8_t* bed_rows, int64_t row_bytes, int64_t n_total, int64_t M,
                      const int64_t* row_sel, int64_t n_sel, const double* annot, int64_t K,
                      int nvecs, int step, int vtile, uint64_t seed, int dist, int ddof,
@@ -786,132 +1054,26 @@ void gw_ldscore_impl(const uint8_t* bed_rows, int64_t row_bytes, int64_t n_total
     Context& c = ctx();
     std::lock_guard<std::mutex> lk(c.mu);
     ensure_device(c);
-    if (nvecs <= 0 || step <= 0 || K <= 0 || M <= 0) fail(LDS_ERR_ARG, "invalid sizes");
     if (row_bytes < (n_total + 3) / 4) fail(LDS_ERR_ARG, "bed_row_bytes smaller than ceil(N/4)");
     if (impute != LDS_IMPUTE_MEAN && impute != LDS_IMPUTE_HWE)
         fail(LDS_ERR_ARG, "impute_mode must be 'mean' or 'hwe'");
     ck(cudaEventRecord(c.ev[0], c.st), "event");
-    auto P = prepare(c, bed_rows, row_bytes, n_total, M, row_sel, n_sel, impute, iseed, ddof,
-                     "session");
+    std::shared_ptr<Prepared> P(prepare(c, bed_rows, row_bytes, n_total, M, row_sel, n_sel, impute,
+                                        iseed, ddof, "session"));
     ck(cudaEventRecord(c.ev[1], c.st), "event");
-    const int64_t N = P->g.N;
-    // Residual variances (fused into the first phase-1 pass in the reference;
-    // same values), rounded to the working type.
-    std::vector<double> inv((size_t)M);
-    for (int64_t j = 0; j < M; ++j)
-        inv[(size_t)j] = as_float ? (double)inv_resvar<float>(*P, j, eps) : inv_resvar<double>(*P, j, eps);
-    if (inv_out) std::memcpy(inv_out, inv.data(), sizeof(double) * (size_t)M);
-    // CSR over the whole genome: blocks only affect probe streams.
-    const int S = c.slices;
-    std::vector<int> vt;
-    {
-        int width = std::min(nvecs, vtile > 0 ? vtile : nvecs);
-        if (width >= 64) width = std::max(64, (width / 64) * 64);
-        for (int s = 0; s < nvecs; s += width) vt.push_back(std::min(width, nvecs - s));
-    }
-    const int vmax = *std::max_element(vt.begin(), vt.end());
-    Csr csr;
-    std::vector<float> annot_f, inv_f;
-    if (as_float) {
-        annot_f.assign(annot, annot + M * K);
-        inv_f.resize((size_t)M);
-        for (int64_t j = 0; j < M; ++j) inv_f[(size_t)j] = (float)inv[(size_t)j];
-    }
-    // Left scales (gwldcore.cpp:2436-2445).
-    const double denom = std::max(1.0, (double)(N - ddof + 1) - 1.0);
-    const double inv_denom2 = 1.0 / (denom * denom);
-    std::vector<double> ls((size_t)M);
-    for (int64_t j = 0; j < M; ++j) {
-        const double v = inv[(size_t)j];
-        ls[(size_t)j] = (std::isfinite(v) && v > 0.0) ? v * v * inv_denom2 : 0.0;
-    }
-    double* d_ls = c.lscale.as<double>((size_t)M);
-    h2d(d_ls, ls.data(), (size_t)M, c.st);
-    double* d_acc = c.accum.as<double>((size_t)(M * K));
-    ck(cudaMemsetAsync(d_acc, 0, sizeof(double) * (size_t)(M * K), c.st), "memset");
-    double* d_mc = nullptr;
-    if (mc_agg || mc_snp) {
-        d_mc = c.mc.as<double>((size_t)(M * K));
-        ck(cudaMemsetAsync(d_mc, 0, sizeof(double) * (size_t)(M * K), c.st), "memset");
-    }
-    ck(cudaMemsetAsync(c.guards.as<unsigned long long>(2), 0, 16, c.st), "memset");
-    std::vector<double> Z((size_t)(M * vmax));
-    const int nblk = (int)((M + step - 1) / step);
-    const unsigned hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
-    float p1_ms = 0.f, p2_ms = 0.f;
-    int v0 = 0;
-    for (int V : vt) {
-        const int Vp = (int)round_up(V, kColTile);
-        csr = as_float ? build_csr<float>(annot_f.data(), inv_f.data(), M, K, 0, Vp, S)
-                       : build_csr<double>(annot, inv.data(), M, K, 0, Vp, S);
-        // Probe streams per block, generated in parallel.
-        {
-            std::vector<std::thread> th;
-            std::atomic<int> next{0};
-            for (unsigned t = 0; t < hw; ++t)
-                th.emplace_back([&] {
-                    for (int b; (b = next.fetch_add(1)) < nblk;) {
-                        const int s = b * step;
-                        const int L = (int)std::min<int64_t>(step, M - s);
-                        // Column-major M x V with ld = M: block rows start at s.
-                        std::vector<double> blk((size_t)L * V);
-                        if (as_float) make_probes<float>(seed, s, v0, L, V, dist, blk.data(), L);
-                        else make_probes<double>(seed, s, v0, L, V, dist, blk.data(), L);
-                        for (int cc = 0; cc < V; ++cc)
-                            std::memcpy(&Z[(size_t)cc * M + s], &blk[(size_t)cc * L],
-                                        sizeof(double) * L);
-                    }
-                });
-            for (auto& t : th) t.join();
-        }
-        ck(cudaEventRecord(c.ev[2], c.st), "event");
-        run_phase1(c, *P, csr, K, V, Z.data(), M, M, 0);
-        quantize_sketch(c, *P, K, V);
-        ck(cudaEventRecord(c.ev[3], c.st), "event");
-        run_phase2(c, *P, K, V, 0, M, 0, d_acc, d_mc, d_ls);
-        ck(cudaEventRecord(c.ev[4], c.st), "event");
-        ck(cudaEventSynchronize(c.ev[4]), "sync");
-        float a = 0.f, b = 0.f;
-        cudaEventElapsedTime(&a, c.ev[2], c.ev[3]);
-        cudaEventElapsedTime(&b, c.ev[3], c.ev[4]);
-        p1_ms += a;
-        p2_ms += b;
-        v0 += V;
-    }
-    std::vector<double> acc((size_t)(M * K));
-    d2h(acc.data(), d_acc, acc.size(), c.st);
-    std::vector<double> mcv;
-    if (d_mc) {
-        mcv.resize((size_t)(M * K));
-        d2h(mcv.data(), d_mc, mcv.size(), c.st);
-    }
+    auto pl = plan_create(c, P, annot, K, nvecs, step, vtile, seed, dist, eps, as_float,
+                          (mc_agg || mc_snp) ? 1 : 0);
+    plan_execute(c, *pl);
+    plan_results(c, *pl, ldscore, meansq_out, inv_out, mc_agg, mc_snp);
     ck(cudaEventRecord(c.ev[5], c.st), "event");
-    ck(cudaStreamSynchronize(c.st), "session");
-    report_guards(c, "accum", 0, (int)M);
+    ck(cudaEventSynchronize(c.ev[5]), "sync");
     float up = 0.f, tot = 0.f;
     cudaEventElapsedTime(&up, c.ev[0], c.ev[1]);
     cudaEventElapsedTime(&tot, c.ev[0], c.ev[5]);
     c.timings[0] = up;
-    c.timings[1] = p1_ms;
-    c.timings[2] = p2_ms;
+    c.timings[1] = pl->kernel_ms[0] + pl->kernel_ms[1];
+    c.timings[2] = pl->kernel_ms[2] + pl->kernel_ms[3];
     c.timings[3] = tot;
-    if (meansq_out) std::memcpy(meansq_out, acc.data(), sizeof(double) * acc.size());
-    // Finalize: / nvecs, minus M_k / (N - ddof) (gw_ldscore.py:2197, :2220-2222).
-    std::vector<double> Mk((size_t)K, 0.0);
-    for (int64_t j = 0; j < M; ++j)
-        for (int64_t k = 0; k < K; ++k) Mk[(size_t)k] += annot[j * K + k];
-    const double nd = (double)(N - ddof);
-    for (int64_t j = 0; j < M; ++j)
-        for (int64_t k = 0; k < K; ++k)
-            ldscore[j * K + k] = acc[(size_t)(j * K + k)] / (double)nvecs - Mk[(size_t)k] / nd;
-    if (d_mc) {
-        for (int64_t k = 0; k < K; ++k) {
-            double agg = 0.0;
-            for (int64_t j = 0; j < M; ++j) agg += mcv[(size_t)(j * K + k)];
-            if (mc_agg) mc_agg[k] = agg;
-        }
-        if (mc_snp) std::memcpy(mc_snp, mcv.data(), sizeof(double) * mcv.size());
-    }
 }
 
 }  // namespace
@@ -1074,6 +1236,104 @@ LDS_API int lds_debug_xt_products(const uint8_t* bed_rows, int64_t bed_row_bytes
         d2h(reinterpret_cast<long long*>(out_g), dg, (size_t)(L * Q), c.st);
         d2h(reinterpret_cast<long long*>(out_o), dO, (size_t)(L * Q), c.st);
         ck(cudaStreamSynchronize(c.st), "debug products");
+    });
+}
+
+LDS_API int lds_set_stream(void* stream) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        ensure_device(c);
+        static cudaStream_t own = c.st;
+        c.st = stream ? static_cast<cudaStream_t>(stream) : own;
+    });
+}
+
+LDS_API int lds_geno_create(const uint8_t* bed_rows, int64_t bed_row_bytes, int64_t n_total,
+                            int64_t M, const int64_t* row_sel, int64_t n_row_sel, int impute_mode,
+                            uint64_t impute_seed, int ddof, int64_t* handle_out) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        ensure_device(c);
+        if (bed_row_bytes < (n_total + 3) / 4) fail(LDS_ERR_ARG, "bed_row_bytes smaller than ceil(N/4)");
+        if (impute_mode != LDS_IMPUTE_MEAN && impute_mode != LDS_IMPUTE_HWE)
+            fail(LDS_ERR_ARG, "impute_mode must be 'mean' or 'hwe'");
+        std::shared_ptr<Prepared> P(prepare(c, bed_rows, bed_row_bytes, n_total, M, row_sel,
+                                            n_row_sel, impute_mode, impute_seed, ddof, "handle"));
+        const int64_t h = next_handle();
+        geno_table()[h] = P;
+        *handle_out = h;
+    });
+}
+
+LDS_API int lds_geno_destroy(int64_t handle) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        geno_table().erase(handle);
+    });
+}
+
+LDS_API int lds_gw_plan_create(int64_t geno, const double* annot, int64_t K, int nvecs,
+                               int step_size, int vtile, uint64_t seed, int rand_dist,
+                               double resvar_eps, int as_float, int with_mc, int64_t* plan_out) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        ensure_device(c);
+        auto it = geno_table().find(geno);
+        if (it == geno_table().end()) fail(LDS_ERR_ARG, "unknown genotype handle");
+        auto pl = plan_create(c, it->second, annot, K, nvecs, step_size, vtile, seed, rand_dist,
+                              resvar_eps, as_float, with_mc);
+        const int64_t h = next_handle();
+        plan_table()[h] = std::move(pl);
+        *plan_out = h;
+    });
+}
+
+static GwPlan& plan_of(int64_t h) {
+    auto it = plan_table().find(h);
+    if (it == plan_table().end()) fail(LDS_ERR_ARG, "unknown plan handle");
+    return *it->second;
+}
+
+LDS_API int lds_gw_plan_execute(int64_t plan) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        plan_execute(c, plan_of(plan));
+    });
+}
+
+LDS_API int lds_gw_plan_results(int64_t plan, double* ldscore, double* meansq_accum,
+                                double* inv_out, double* mc_aggregate_sumsq,
+                                double* mc_per_snp_sumsq) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        plan_results(c, plan_of(plan), ldscore, meansq_accum, inv_out, mc_aggregate_sumsq,
+                     mc_per_snp_sumsq);
+    });
+}
+
+LDS_API int lds_gw_plan_kernel_ms(int64_t plan, double* ms4) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        GwPlan& pl = plan_of(plan);
+        ck(cudaStreamSynchronize(c.st), "sync");
+        plan_kernel_times(pl);
+        for (int i = 0; i < 4; ++i) ms4[i] = pl.kernel_ms[i];
+    });
+}
+
+LDS_API int lds_gw_plan_destroy(int64_t plan) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        if (c.ready) ck(cudaStreamSynchronize(c.st), "sync");
+        plan_table().erase(plan);
     });
 }
 
