@@ -209,6 +209,18 @@ int lds_last_timings(double* ms_out, int n);
 int lds_debug_xt_products(const uint8_t* bed_rows, int64_t bed_row_bytes, int64_t n, int64_t L,
                           const int8_t* y, int64_t Q, int64_t* out_g, int64_t* out_o);
 
+/* Same check through the tcgen05 phase-2 kernel: y is n x (4*V) int8,
+ * column 4 v + t = digit t of probe v; out_g/out_o (L x V row-major) receive
+ * the exact digit recombination ((d0*128 + d1)*128 + d2)*128 + d3 of the
+ * per-digit products.  No reference counterpart (test entry). */
+int lds_debug_xt_products_umma(const uint8_t* bed_rows, int64_t bed_row_bytes, int64_t n,
+                               int64_t L, const int8_t* y, int64_t V, int64_t* out_g,
+                               int64_t* out_o);
+
+/* Phase-2 kernel selection: 1 = tcgen05 (default), 0 = mma.sync.  Applies to
+ * plans created afterwards.  No reference counterpart. */
+int lds_set_p2_kernel(int impl);
+
 /* Synthetic genotype image generated on the device with the integer-exact
  * generator (identical bytes to the numpy generator in bedfile.py):
  * writes M rows of ceil(n/4) bytes to host memory `out`.  t0/t1 are the

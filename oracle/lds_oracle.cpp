@@ -242,7 +242,12 @@ ORC_EXPORT int orc_phase1_block(const double* geno, int64_t N, int L, const doub
                 const double* x = geno + (int64_t)idx[r] * N;
                 for (int64_t n = 0; n < N; ++n) acc[(size_t)n] += x[n] * w;
             }
-            for (int64_t n = 0; n < N; ++n) dst[n] = beta * dst[n] + acc[(size_t)n];
+            // beta = 0 must not read the destination (BLAS semantics: it may
+            // hold uninitialized memory, NaN included).
+            if (beta == 0.0)
+                for (int64_t n = 0; n < N; ++n) dst[n] = acc[(size_t)n];
+            else
+                for (int64_t n = 0; n < N; ++n) dst[n] += acc[(size_t)n];
         }
     }
     return 0;

@@ -28,9 +28,12 @@
 #include <unistd.h>
 #include <vector>
 
+#include <cudaTypedefs.h>
+
 #include "../../include/lds.h"
 #include "lds_device.cuh"
 #include "lds_internal.h"
+#include "lds_umma.h"
 
 namespace lds {
 
@@ -107,6 +110,40 @@ void d2h(T* h, const T* d, size_t count, cudaStream_t st) {
 }
 
 inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+// 2-D uint8 TMA descriptor over a row-major device buffer (no multicast use).
+CUtensorMap make_map_2d(void* base, uint64_t inner, uint64_t outer, uint64_t row_bytes,
+                        uint32_t box_inner, uint32_t box_outer, CUtensorMapSwizzle swz) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault,
+                                             &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !p)
+            p = nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }();
+    if (!encode) fail(LDS_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    CUtensorMap m;
+    const cuuint64_t dims[2] = {inner, outer};
+    const cuuint64_t strides[1] = {row_bytes};
+    const cuuint32_t box[2] = {box_inner, box_outer};
+    const cuuint32_t es[2] = {1, 1};
+    const CUresult r = encode(&m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, base, dims, strides, box, es,
+                              CU_TENSOR_MAP_INTERLEAVE_NONE, swz, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) fail(LDS_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return m;
+}
+
+// Phase-2 implementation: 1 = tcgen05 (default; needs 4 digits), 0 = mma.sync.
+int& p2_impl() {
+    static int v = [] {
+        const char* s = std::getenv("LDS_P2_KERNEL");
+        return (s && !strcmp(s, "mma")) ? 0 : 1;
+    }();
+    return v;
+}
 
 // ---------------------------------------------------------------------------
 // Prepared genotype image + statistics
@@ -804,7 +841,10 @@ struct GwPlan {
         DevBuf rowind, sc, binoff, wqoff, z, wq, wcs;
     };
     std::vector<std::unique_ptr<Tile>> tiles;
-    DevBuf y, yq, ycs, accum, mc, lscale, guards;
+    DevBuf y, yq, ycs, accum, mc, lscale, guards, status;
+    bool umma = false;
+    std::vector<CUtensorMap> tmB;    // per V-tile (sketch digit layout depends on V)
+    CUtensorMap tmA;
     // One set of events per execute (up to kMaxTimed executes between reads):
     // a start event and one after each kernel of each V-tile.
     static constexpr int kMaxTimed = 64;
@@ -913,9 +953,25 @@ std::unique_ptr<GwPlan> plan_create(Context& c, std::shared_ptr<Prepared> P, con
         v0 += V;
     }
     const int vpmax = (int)round_up(vmax, kColTile);
+    pl->umma = (p2_impl() == 1 && pl->S == 4);
     pl->y.as<double>((size_t)(P->g.N_pad * K * vmax));
-    pl->yq.as<int8_t>((size_t)(pl->S * K * vpmax * P->g.N_pad));
-    pl->ycs.as<double>((size_t)(K * vpmax));
+    if (pl->umma) {
+        const int ncolp = umma::ncolp_for(vmax);
+        int8_t* yq = pl->yq.as<int8_t>((size_t)(K * ncolp * P->g.N_pad));
+        pl->ycs.as<double>((size_t)(K * vmax));
+        pl->tmA = make_map_2d(P->g.codes, (uint64_t)P->g.nbp, (uint64_t)P->g.M_pad,
+                              (uint64_t)P->g.nbp, 32, 128, CU_TENSOR_MAP_SWIZZLE_NONE);
+        for (int V : pl->vt) {
+            const int nc = umma::ncolp_for(V);
+            pl->tmB.push_back(make_map_2d(yq, (uint64_t)P->g.N_pad, (uint64_t)(K * nc),
+                                          (uint64_t)P->g.N_pad, 128, (uint32_t)std::min(256, nc),
+                                          CU_TENSOR_MAP_SWIZZLE_128B));
+        }
+        ck(cudaMemsetAsync(pl->status.as<unsigned>(1), 0, 4, c.st), "memset");
+    } else {
+        pl->yq.as<int8_t>((size_t)(pl->S * K * vpmax * P->g.N_pad));
+        pl->ycs.as<double>((size_t)(K * vpmax));
+    }
     pl->accum.as<double>((size_t)(M * K));
     if (with_mc) pl->mc.as<double>((size_t)(M * K));
     pl->guards.as<unsigned long long>(2);
@@ -959,6 +1015,37 @@ void plan_execute(Context& c, GwPlan& pl) {
         if (tm) ck(cudaEventRecord(ev[e++], c.st), "event");
         launch_p1(P.g, w, nullptr, static_cast<double*>(pl.y.p), c.st);
         if (tm) ck(cudaEventRecord(ev[e++], c.st), "event");
+        if (pl.umma) {
+            const int nc = umma::ncolp_for(t.V);
+            umma::launch_quantize_y4(static_cast<double*>(pl.y.p), P.g.N, P.g.N_pad, (int)K, t.V, nc,
+                                     static_cast<int8_t*>(pl.yq.p), static_cast<double*>(pl.ycs.p),
+                                     c.st);
+            if (tm) ck(cudaEventRecord(ev[e++], c.st), "event");
+            umma::P2UArgs u;
+            u.K = (int)K;
+            u.V = t.V;
+            u.ncolp = nc;
+            u.ngroups = (nc + 255) / 256;
+            u.box_rows = std::min(256, nc);
+            u.nkt = (int)(P.g.N_pad / 128);
+            u.M = M;
+            u.j0 = 0;
+            u.j1 = M;
+            u.out_row0 = 0;
+            u.colscale = static_cast<double*>(pl.ycs.p);
+            u.mean = static_cast<double*>(P.d_mean.p);
+            u.sdinv = static_cast<double*>(P.d_sdinv.p);
+            u.left_scale = static_cast<double*>(pl.lscale.p);
+            u.accum = static_cast<double*>(pl.accum.p);
+            u.mc = pl.with_mc ? static_cast<double*>(pl.mc.p) : nullptr;
+            u.guard_counts = static_cast<unsigned long long*>(pl.guards.p);
+            u.extreme_warn = extreme_warn_env();
+            u.drop_extreme = drop_extreme_env();
+            u.status = static_cast<unsigned*>(pl.status.p);
+            umma::launch_p2_umma(pl.tmA, pl.tmB[(size_t)(&tp - &pl.tiles[0])], u, c.st);
+            if (tm) ck(cudaEventRecord(ev[e++], c.st), "event");
+            continue;
+        }
         launch_quantize_y(static_cast<double*>(pl.y.p), P.g.N, P.g.N_pad, (int)K, t.V, t.Vp, pl.S,
                           static_cast<int8_t*>(pl.yq.p), static_cast<double*>(pl.ycs.p), c.st);
         if (tm) ck(cudaEventRecord(ev[e++], c.st), "event");
@@ -1017,6 +1104,12 @@ void plan_results(Context& c, GwPlan& pl, double* ldscore, double* meansq_out, d
         d2h(mcv.data(), static_cast<double*>(pl.mc.p), mcv.size(), c.st);
     }
     ck(cudaStreamSynchronize(c.st), "results");
+    if (pl.umma) {
+        unsigned st = 0;
+        d2h(&st, static_cast<unsigned*>(pl.status.p), 1, c.st);
+        ck(cudaStreamSynchronize(c.st), "status");
+        if (st) fail(LDS_ERR_CUDA, "phase-2 tensor-core pipeline wait timed out (code %u)", st);
+    }
     plan_kernel_times(pl);
     {
         unsigned long long h[2] = {0, 0};
@@ -1335,6 +1428,67 @@ LDS_API int lds_gw_plan_destroy(int64_t plan) {
         if (c.ready) ck(cudaStreamSynchronize(c.st), "sync");
         plan_table().erase(plan);
     });
+}
+
+LDS_API int lds_debug_xt_products_umma(const uint8_t* bed_rows, int64_t bed_row_bytes,
+                                       int64_t n, int64_t L, const int8_t* y, int64_t V,
+                                       int64_t* out_g, int64_t* out_o) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        ensure_device(c);
+        if (L <= 0 || V <= 0 || n <= 0) fail(LDS_ERR_ARG, "invalid sizes");
+        auto P = prepare(c, bed_rows, bed_row_bytes, n, L, nullptr, 0, LDS_IMPUTE_MEAN, 0, 1,
+                         "debug");
+        const int64_t Np = P->g.N_pad;
+        const int nc = umma::ncolp_for((int)V);
+        std::vector<int8_t> yq((size_t)(nc * Np), 0);
+        for (int64_t q = 0; q < 4 * V; ++q) std::memcpy(&yq[(size_t)(q * Np)], y + q * n, (size_t)n);
+        DevBuf dyq, rg, ro, st;
+        int8_t* d_yq = dyq.as<int8_t>(yq.size());
+        h2d(d_yq, yq.data(), yq.size(), c.st);
+        long long* dg = rg.as<long long>((size_t)(L * V));
+        long long* dO = ro.as<long long>((size_t)(L * V));
+        unsigned* dst = st.as<unsigned>(1);
+        ck(cudaMemsetAsync(dst, 0, 4, c.st), "memset");
+        const CUtensorMap tA = make_map_2d(P->g.codes, (uint64_t)P->g.nbp, (uint64_t)P->g.M_pad,
+                                           (uint64_t)P->g.nbp, 32, 128, CU_TENSOR_MAP_SWIZZLE_NONE);
+        const CUtensorMap tB = make_map_2d(d_yq, (uint64_t)Np, (uint64_t)nc, (uint64_t)Np, 128,
+                                           (uint32_t)std::min(256, nc), CU_TENSOR_MAP_SWIZZLE_128B);
+        umma::P2UArgs u;
+        u.K = 1;
+        u.V = (int)V;
+        u.ncolp = nc;
+        u.ngroups = (nc + 255) / 256;
+        u.box_rows = std::min(256, nc);
+        u.nkt = (int)(Np / 128);
+        u.M = L;
+        u.j0 = 0;
+        u.j1 = L;
+        u.out_row0 = 0;
+        u.mean = static_cast<double*>(P->d_mean.p);
+        u.sdinv = static_cast<double*>(P->d_sdinv.p);
+        u.status = dst;
+        u.raw_g = dg;
+        u.raw_o = dO;
+        umma::launch_p2_umma(tA, tB, u, c.st);
+        ck(cudaGetLastError(), "launch");
+        unsigned stv = 0;
+        d2h(&stv, dst, 1, c.st);
+        d2h(reinterpret_cast<long long*>(out_g), dg, (size_t)(L * V), c.st);
+        d2h(reinterpret_cast<long long*>(out_o), dO, (size_t)(L * V), c.st);
+        ck(cudaStreamSynchronize(c.st), "debug umma products");
+        if (stv) fail(LDS_ERR_CUDA, "phase-2 tensor-core pipeline wait timed out (code %u)", stv);
+    });
+}
+
+LDS_API int lds_set_p2_kernel(int impl) {
+    if (impl != 0 && impl != 1) {
+        g_err = "p2 kernel must be 0 (mma.sync) or 1 (tcgen05)";
+        return LDS_ERR_ARG;
+    }
+    p2_impl() = impl;
+    return LDS_OK;
 }
 
 LDS_API int lds_last_timings(double* ms_out, int n) {

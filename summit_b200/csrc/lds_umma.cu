@@ -1,0 +1,415 @@
+// Phase 2 on 5th-generation tensor cores (tcgen05, sm_100a).
+//
+// Work[j, c] = x_j^T Y[:, c] for a tile of 128 SNPs and one annotation bin,
+// with the LD-score epilogue, as in p2_kernel (lds_kernels.cu) but with:
+//   * TMA (cp.async.bulk.tensor, no multicast) bringing the packed 2-bit
+//     genotype tile (128 SNPs x 128 samples = 4 KB) and the sketch digit tile
+//     (bin columns x 128 samples, SWIZZLE_128B) into a 3-stage smem ring;
+//   * 4 decoder warps expanding packed codes into the G (value) and O
+//     (observed) int8 operand tiles in the canonical K-major SWIZZLE_128B
+//     layout the UMMA descriptors expect;
+//   * one thread issuing tcgen05.mma.kind::i8 (M=128, N=bin columns, K=32)
+//     into two TMEM accumulators (G at column 0, O at column 256);
+//   * the decoder warps reading the accumulators back with tcgen05.ld for the
+//     exact digit recombination and the squared-sum epilogue.
+// Digits of each probe column sit next to each other (column = 4 v + t), so
+// one 32-column TMEM load holds 8 probes x 4 digits.
+//
+// Every wait on an mbarrier is bounded; on timeout the kernel records an
+// error code in `status`, stops issuing work and releases its TMEM.
+#include <cstdint>
+#include <cstdio>
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include "lds_device.cuh"
+#include "lds_internal.h"
+#include "lds_umma.h"
+
+namespace lds {
+namespace umma {
+
+constexpr int kStages = 3;
+constexpr int kBM = 128;              // SNP rows per CTA (UMMA M)
+constexpr int kBK = 128;              // samples per stage (bytes per operand row)
+constexpr int kPkBytes = kBM * 32;    // packed tile: 128 rows x 32 bytes
+constexpr int kATile = kBM * kBK;     // 16 KB
+constexpr int kBTileMax = 256 * kBK;  // 32 KB
+constexpr int kStageBytes = kPkBytes + 2 * kATile + kBTileMax;  // 69632
+constexpr int kThreads = 192;
+constexpr uint32_t kTmemCols = 512;
+constexpr uint32_t kOCol = 256;       // TMEM column of the O accumulator
+constexpr long long kWaitLimit = 1LL << 26;
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(
+        smem_u32(bar)));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile(
+        "{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(
+            smem_u32(bar)),
+        "r"(bytes));
+}
+// Bounded wait for the phase with the given parity.  Returns false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    const uint32_t addr = smem_u32(bar);
+    for (long long i = 0; i < kWaitLimit; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(addr), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y,
+                                            uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// UMMA shared-memory descriptor: K-major, SWIZZLE_128B, 8-row groups 1024 B
+// apart (SBO), version 1 (sm100), base offset 0 (tiles are 1024-aligned).
+__device__ __forceinline__ uint64_t sw128_desc(const void* smem) {
+    const uint64_t a = (uint64_t)((smem_u32(smem) >> 4) & 0x3FFF);
+    return a | (1ULL << 16) | ((uint64_t)(1024 >> 4) << 32) | (1ULL << 46) | (2ULL << 61);
+}
+
+// Instruction descriptor: kind::i8, D = s32, A = s8, B = s8, both K-major.
+__host__ __device__ constexpr uint32_t idesc_i8(int M, int N) {
+    return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
+           ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                        uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, int (&r)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+        "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+          "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+          "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+          "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+          "=r"(r[31])
+        : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_wait_ld() {
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+    p2_umma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                   P2UArgs a) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
+    uint64_t* full_tma = bars;                 // [kStages]
+    uint64_t* full_dec = bars + kStages;       // [kStages]
+    uint64_t* empty = bars + 2 * kStages;      // [kStages]
+    uint64_t* acc_full = bars + 3 * kStages;
+    uint64_t* acc_empty = bars + 3 * kStages + 1;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 3 * kStages + 2);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int k = blockIdx.y;
+    const int64_t jt0 = a.j0 + (int64_t)blockIdx.x * kBM;
+
+    if (tid == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(&full_tma[s], 1);
+            mbar_init(&full_dec[s], 128);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(acc_full, 1);
+        mbar_init(acc_empty, 128);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(tmem_slot)),
+                     "r"(kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    auto fail = [&](int code) {
+        atomicCAS(a.status, 0u, (unsigned)code);
+        *abort_flag = 1;
+    };
+
+    const int ngroups = a.ngroups;
+    if (warp == 0) {
+        // ---------------- TMA producer ----------------
+        if (lane == 0) {
+            int it = 0;
+            for (int g = 0; g < ngroups && !*abort_flag; ++g) {
+                for (int kt = 0; kt < a.nkt; ++kt, ++it) {
+                    const int s = it % kStages;
+                    const uint32_t ph = (uint32_t)(it / kStages) & 1u;
+                    if (it >= kStages && !mbar_wait(&empty[s], ph ^ 1u)) { fail(1); break; }
+                    if (*abort_flag) break;
+                    uint8_t* st = smem + s * kStageBytes;
+                    mbar_expect_tx(&full_tma[s], (uint32_t)(kPkBytes + a.box_rows * kBK));
+                    tma_load_2d(st, &tmA, kt * 32, (int)jt0, &full_tma[s]);
+                    tma_load_2d(st + kPkBytes + 2 * kATile, &tmB, kt * kBK,
+                                k * a.ncolp + g * 256, &full_tma[s]);
+                }
+            }
+        }
+    } else if (warp == 1) {
+        // ---------------- MMA issuer ----------------
+        if (lane == 0) {
+            int it = 0;
+            for (int g = 0; g < ngroups && !*abort_flag; ++g) {
+                const int ncols = min(256, a.ncolp - g * 256);
+                const uint32_t idesc = idesc_i8(kBM, ncols);
+                if (g > 0 && !mbar_wait(acc_empty, (uint32_t)(g - 1) & 1u)) { fail(2); break; }
+                tc_fence_after();
+                for (int kt = 0; kt < a.nkt; ++kt, ++it) {
+                    const int s = it % kStages;
+                    const uint32_t ph = (uint32_t)(it / kStages) & 1u;
+                    if (!mbar_wait(&full_dec[s], ph)) { fail(3); break; }
+                    if (*abort_flag) break;
+                    tc_fence_after();
+                    uint8_t* st = smem + s * kStageBytes;
+                    const uint64_t dG = sw128_desc(st + kPkBytes);
+                    const uint64_t dO = sw128_desc(st + kPkBytes + kATile);
+                    const uint64_t dB = sw128_desc(st + kPkBytes + 2 * kATile);
+#pragma unroll
+                    for (int kk = 0; kk < kBK / 32; ++kk) {
+                        const uint32_t acc = (kt | kk) ? 1u : 0u;
+                        umma_i8(tmem, dG + 2 * kk, dB + 2 * kk, idesc, acc);
+                        umma_i8(tmem + kOCol, dO + 2 * kk, dB + 2 * kk, idesc, acc);
+                    }
+                    umma_commit(&empty[s]);
+                }
+                umma_commit(acc_full);
+            }
+        }
+    } else {
+        // ---------------- decoders + epilogue (warps 2..5) ----------------
+        const int r = tid - 64;              // operand row this thread decodes
+        const int q = warp & 3;              // TMEM lane quadrant this warp may access
+        const int row = q * 32 + lane;       // accumulator row (SNP) of this thread
+        const int64_t j = jt0 + row;
+        const bool stats = (j < a.M) && a.mean && a.sdinv;
+        const double mu = stats ? a.mean[j] : 0.0;
+        const double sd = stats ? a.sdinv[j] : 0.0;
+        double run2 = 0.0, run4 = 0.0;
+        int it = 0;
+        for (int g = 0; g < ngroups; ++g) {
+            for (int kt = 0; kt < a.nkt; ++kt, ++it) {
+                const int s = it % kStages;
+                const uint32_t ph = (uint32_t)(it / kStages) & 1u;
+                if (!mbar_wait(&full_tma[s], ph)) { fail(4); break; }
+                if (*abort_flag) break;
+                uint8_t* st = smem + s * kStageBytes;
+                const uint4* pk = reinterpret_cast<const uint4*>(st + r * 32);
+                const uint4 p0 = pk[0], p1 = pk[1];
+                const uint32_t words[8] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w};
+                uint8_t* gRow = st + kPkBytes + (r >> 3) * 1024 + (r & 7) * 128;
+                uint8_t* oRow = gRow + kATile;
+#pragma unroll
+                for (int c = 0; c < 8; ++c) {  // 16-byte chunk c = samples 16c..16c+15
+                    uint32_t g0, g1, g2, g3, o0, o1, o2, o3;
+                    decode8(words[c] & 0xFFFFu, g0, g1, o0, o1);
+                    decode8(words[c] >> 16, g2, g3, o2, o3);
+                    const int off = ((c ^ (r & 7)) << 4);
+                    *reinterpret_cast<uint4*>(gRow + off) = make_uint4(g0, g1, g2, g3);
+                    *reinterpret_cast<uint4*>(oRow + off) = make_uint4(o0, o1, o2, o3);
+                }
+                fence_async_smem();
+                mbar_arrive(&full_dec[s]);
+            }
+            if (*abort_flag) break;
+            // Epilogue of column group g.
+            if (!mbar_wait(acc_full, (uint32_t)g & 1u)) { fail(5); break; }
+            tc_fence_after();
+            const int ncols = min(256, a.ncolp - g * 256);
+            const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16);
+            for (int c0 = 0; c0 < ncols; c0 += 32) {
+                int rg[32], ro[32];
+                tmem_ld32(tbase + (uint32_t)c0, rg);
+                tmem_ld32(tbase + kOCol + (uint32_t)c0, ro);
+                tmem_wait_ld();
+#pragma unroll
+                for (int p = 0; p < 8; ++p) {
+                    const int v = g * 64 + c0 / 4 + p;
+                    if (v >= a.V) continue;
+                    const long long TG =
+                        (((long long)rg[4 * p] * 128 + rg[4 * p + 1]) * 128 + rg[4 * p + 2]) * 128 +
+                        rg[4 * p + 3];
+                    const long long TO =
+                        (((long long)ro[4 * p] * 128 + ro[4 * p + 1]) * 128 + ro[4 * p + 2]) * 128 +
+                        ro[4 * p + 3];
+                    if (a.raw_g) {
+                        if (j < a.j1) {
+                            a.raw_g[(j - a.out_row0) * a.V + v] = TG;
+                            a.raw_o[(j - a.out_row0) * a.V + v] = TO;
+                        }
+                        continue;
+                    }
+                    const double wv = sd * a.colscale[(int64_t)k * a.V + v] *
+                                      ((double)TG - mu * (double)TO);
+                    const double w2 = wv * wv;
+                    run2 += w2;
+                    run4 += w2 * w2;
+                }
+            }
+            tc_fence_before();
+            mbar_arrive(acc_empty);
+        }
+        if (!*abort_flag && j < a.j1 && !a.raw_g) {
+            const double ls = a.left_scale[j];
+            double upd = run2 * ls;
+            const double seg = (double)a.V;
+            const bool nonfinite = !isfinite(upd);
+            const bool extreme = !nonfinite && isfinite(a.extreme_warn) && seg > 0.0 &&
+                                 upd > a.extreme_warn * seg;
+            if (a.guard_counts) {
+                if (nonfinite) atomicAdd(&a.guard_counts[0], 1ULL);
+                else if (extreme) atomicAdd(&a.guard_counts[1], 1ULL);
+            }
+            if (!(nonfinite || (extreme && a.drop_extreme))) {
+                if (upd < 0.0) upd = 0.0;
+                const int64_t o = (j - a.out_row0) * a.K + k;
+                a.accum[o] += upd;
+                if (a.mc) a.mc[o] += run4 * ls * ls;
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(kTmemCols));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Sketch digits in the layout of this kernel: per bin, column 4 v + t holds
+// digit t of probe v; ncolp columns per bin (padding columns zero).
+// ---------------------------------------------------------------------------
+__global__ void quantize_y4_kernel(const double* __restrict__ Y, int64_t N, int64_t N_pad, int K,
+                                   int V, int ncolp, int8_t* __restrict__ Yq,
+                                   double* __restrict__ colscale) {
+    __shared__ double red[32];
+    const int k = blockIdx.x / V, v = blockIdx.x - (blockIdx.x / V) * V;
+    const double* y = Y + ((int64_t)k * V + v) * N_pad;
+    double amax = 0.0;
+    for (int64_t i = threadIdx.x; i < N; i += blockDim.x) amax = fmax(amax, fabs(y[i]));
+    for (int o = 16; o; o >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = amax;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double x = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0.0;
+        for (int o = 16; o; o >>= 1) x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
+        if (threadIdx.x == 0) red[0] = x;
+    }
+    __syncthreads();
+    amax = red[0];
+    int e = 0;
+    if (amax > 0.0 && isfinite(amax)) {
+        e = ilogb(amax) + 1;
+        if (ldexp(amax, 7 - e) > 127.0) e += 1;
+    }
+    int8_t* base = Yq + ((int64_t)k * ncolp + 4 * v) * N_pad;
+    for (int64_t i = threadIdx.x; i < N_pad; i += blockDim.x) {
+        int8_t d[4] = {0, 0, 0, 0};
+        if (i < N) {
+            double t = ldexp(y[i], 7 - e);
+            double rr = rint(t);
+            d[0] = (int8_t)rr;
+            t -= rr;
+            for (int s = 1; s < 4; ++s) {
+                t *= 128.0;
+                rr = rint(t);
+                d[s] = (int8_t)rr;
+                t -= rr;
+            }
+        }
+        for (int s = 0; s < 4; ++s) base[(int64_t)s * N_pad + i] = d[s];
+    }
+    if (threadIdx.x == 0) colscale[(int64_t)k * V + v] = ldexp(1.0, e - 7 - 21);
+}
+
+__global__ void zero_pad_cols_kernel(int8_t* Yq, int64_t N_pad, int K, int V, int ncolp) {
+    const int k = blockIdx.y;
+    const int c = 4 * V + blockIdx.x;
+    if (c >= ncolp) return;
+    int8_t* base = Yq + ((int64_t)k * ncolp + c) * N_pad;
+    for (int64_t i = threadIdx.x; i < N_pad; i += blockDim.x) base[i] = 0;
+}
+
+void launch_quantize_y4(const double* Y, int64_t N, int64_t N_pad, int K, int V, int ncolp,
+                        int8_t* Yq, double* colscale, cudaStream_t st) {
+    quantize_y4_kernel<<<(unsigned)(K * V), 256, 0, st>>>(Y, N, N_pad, K, V, ncolp, Yq, colscale);
+    count_launch();
+    if (ncolp > 4 * V) {
+        zero_pad_cols_kernel<<<dim3((unsigned)(ncolp - 4 * V), (unsigned)K), 256, 0, st>>>(
+            Yq, N_pad, K, V, ncolp);
+        count_launch();
+    }
+}
+
+size_t p2_umma_smem_bytes() { return (size_t)kStages * kStageBytes + 1024 + 256; }
+
+void launch_p2_umma(const CUtensorMap& tmA, const CUtensorMap& tmB, const P2UArgs& a,
+                    cudaStream_t st) {
+    const int64_t rows = a.j1 - a.j0;
+    if (rows <= 0 || a.K <= 0) return;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(p2_umma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)p2_umma_smem_bytes());
+        attr = true;
+    }
+    dim3 grid((unsigned)((rows + kBM - 1) / kBM), (unsigned)a.K);
+    p2_umma_kernel<<<grid, kThreads, p2_umma_smem_bytes(), st>>>(tmA, tmB, a);
+    count_launch();
+}
+
+}  // namespace umma
+}  // namespace lds

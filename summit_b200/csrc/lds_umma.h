@@ -1,0 +1,41 @@
+// tcgen05 (UMMA) phase-2 kernel interface.
+#pragma once
+#include <cstdint>
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+namespace lds {
+namespace umma {
+
+// Arguments of p2_umma_kernel.  The sketch digits live in Yq with layout
+// [K bins][ncolp columns][N_pad samples], column 4 v + t = digit t of probe v.
+struct P2UArgs {
+    int K = 0, V = 0, ncolp = 0, ngroups = 1, box_rows = 0, nkt = 0;
+    int64_t M = 0, j0 = 0, j1 = 0, out_row0 = 0;
+    const double* colscale = nullptr;    // K*V
+    const double* mean = nullptr;
+    const double* sdinv = nullptr;
+    const double* left_scale = nullptr;
+    double* accum = nullptr;
+    double* mc = nullptr;
+    unsigned long long* guard_counts = nullptr;
+    double extreme_warn = 1e10;
+    int drop_extreme = 1;
+    unsigned int* status = nullptr;      // 0 = ok; nonzero = pipeline wait timed out
+    // Verification mode: write the exact recombined products G^T y and O^T y
+    // per (SNP, probe) to raw_g / raw_o ((j - out_row0) * V + v), no epilogue.
+    long long* raw_g = nullptr;
+    long long* raw_o = nullptr;
+};
+
+// Columns per bin (4 digits per probe, padded to a multiple of 16).
+inline int ncolp_for(int V) { return ((4 * V + 15) / 16) * 16; }
+
+void launch_quantize_y4(const double* Y, int64_t N, int64_t N_pad, int K, int V, int ncolp,
+                        int8_t* Yq, double* colscale, cudaStream_t st);
+size_t p2_umma_smem_bytes();
+void launch_p2_umma(const CUtensorMap& tmA, const CUtensorMap& tmB, const P2UArgs& a,
+                    cudaStream_t st);
+
+}  // namespace umma
+}  // namespace lds

@@ -266,6 +266,26 @@ def debug_xt_products(bed_rows, n, y):
     return g, o
 
 
+def debug_xt_products_umma(bed_rows, n, y4):
+    """Exact Horner-combined int64 products from the tcgen05 kernel (verification).
+
+    ``y4``: (n, 4*V) int8, column 4 v + t = digit t of probe v."""
+    bed_rows = np.ascontiguousarray(bed_rows, dtype=np.uint8)
+    y4 = np.asfortranarray(y4, dtype=np.int8)
+    L = bed_rows.shape[0]
+    V = y4.shape[1] // 4
+    g = np.empty((L, V), dtype=np.int64)
+    o = np.empty((L, V), dtype=np.int64)
+    check(_lib.load().lds_debug_xt_products_umma(ptr(bed_rows), bed_rows.shape[1], int(n), L,
+                                                 ptr(y4), V, ptr(g), ptr(o)))
+    return g, o
+
+
+def set_p2_kernel(impl: str) -> None:
+    """Phase-2 kernel for plans created afterwards: "tcgen05" (default) or "mma"."""
+    check(_lib.load().lds_set_p2_kernel({"mma": 0, "tcgen05": 1}[impl]))
+
+
 def set_slices(s: int) -> None:
     check(_lib.load().lds_set_slices(int(s)))
 

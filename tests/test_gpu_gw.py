@@ -42,6 +42,38 @@ def test_tensor_core_products_are_exact(gw, oracle):
     np.testing.assert_array_equal(o_gpu, o_ref)
 
 
+def test_tcgen05_products_are_exact(gw, oracle):
+    """The tcgen05 phase-2 kernel's integer core: per-digit int8 products
+    accumulated in TMEM, recombined exactly (Horner in int64)."""
+    from summit_b200 import bedfile
+
+    rng = np.random.default_rng(6)
+    n, L, V = 1000, 300, 50  # 200 digit columns -> N = 208 per MMA
+    geno = bedfile.synth_genotypes(n, L, seed=98)
+    rows = bedfile.pack_bed_rows(geno)
+    y4 = np.asfortranarray(rng.integers(-127, 128, size=(n, 4 * V), dtype=np.int8))
+    g_gpu, o_gpu = gw.debug_xt_products_umma(rows, n, y4)
+    g_ref, o_ref = oracle.int_products(rows, n, y4)
+    horner = lambda a: ((a[:, 0::4] * 128 + a[:, 1::4]) * 128 + a[:, 2::4]) * 128 + a[:, 3::4]
+    np.testing.assert_array_equal(g_gpu, horner(g_ref))
+    np.testing.assert_array_equal(o_gpu, horner(o_ref))
+
+
+@pytest.mark.parametrize("V", [8, 50, 64, 100])
+def test_tcgen05_and_mma_sync_paths_agree(gw, oracle, small_bed, V):
+    n, m, rows = small_bed["n"], small_bed["m"], small_bed["rows"]
+    annot = np.ones((m, 2))
+    annot[::2, 1] = 0
+    out = {}
+    for impl in ("tcgen05", "mma"):
+        gw.set_p2_kernel(impl)
+        out[impl] = gw.gw_ldscore(rows, n, annot, V, 128, 21, vtile=V, with_mc=True)
+    gw.set_p2_kernel("tcgen05")
+    ora = oracle.gw_ldscore(rows, n, annot, V, 128, 21, vtile=V, with_mc=True)
+    assert rel_err(out["tcgen05"]["meansq_accum"], out["mma"]["meansq_accum"]) < 1e-12
+    assert rel_err(out["tcgen05"]["ldscore"], ora["ldscore"]) < LD_RTOL
+
+
 def test_device_synthetic_generator_matches_numpy(gw):
     from summit_b200 import bedfile
 
