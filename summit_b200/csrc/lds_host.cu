@@ -413,7 +413,8 @@ struct Csr {
 };
 
 template <typename T>
-Csr build_csr(const T* annot, const T* inv, int64_t L, int64_t K, int64_t snp0, int Vp, int S) {
+Csr build_csr(const T* annot, const T* inv, int64_t L, int64_t K, int64_t snp0, int Vp, int S,
+              int64_t pad = kSnpStep) {
     Csr c;
     c.bin_off.assign((size_t)K + 1, 0);
     c.nnz.assign((size_t)K, 0);
@@ -437,7 +438,7 @@ Csr build_csr(const T* annot, const T* inv, int64_t L, int64_t K, int64_t snp0, 
     int64_t off = 0, wq = 0;
     for (int64_t k = 0; k < K; ++k) {
         const int64_t n = (int64_t)members[(size_t)k].size();
-        const int64_t np = round_up(n, kSnpStep);
+        const int64_t np = round_up(n, pad);
         c.nnz[(size_t)k] = n;
         c.bin_off[(size_t)k] = off;
         c.wq_off[(size_t)k] = wq;
@@ -839,6 +840,8 @@ struct GwPlan {
         int V = 0, Vp = 0;
         Csr csr;
         DevBuf rowind, sc, binoff, wqoff, z, wq, wcs;
+        int64_t lmax = 0;     // tcgen05 phase 1: padded member-list length
+        CUtensorMap tmW;      // tcgen05 phase 1: weight digits
     };
     std::vector<std::unique_ptr<Tile>> tiles;
     DevBuf y, yq, ycs, accum, mc, lscale, guards, status;
@@ -920,8 +923,10 @@ std::unique_ptr<GwPlan> plan_create(Context& c, std::shared_ptr<Prepared> P, con
         auto t = std::make_unique<GwPlan::Tile>();
         t->V = V;
         t->Vp = (int)round_up(V, kColTile);
-        t->csr = as_float ? build_csr<float>(annot_f.data(), inv_f.data(), M, K, 0, t->Vp, pl->S)
-                          : build_csr<double>(annot, pl->inv.data(), M, K, 0, t->Vp, pl->S);
+        const bool tc = (p2_impl() == 1 && pl->S == 4);
+        const int64_t pad = tc ? 128 : kSnpStep;
+        t->csr = as_float ? build_csr<float>(annot_f.data(), inv_f.data(), M, K, 0, t->Vp, pl->S, pad)
+                          : build_csr<double>(annot, pl->inv.data(), M, K, 0, t->Vp, pl->S, pad);
         // Probe streams per SNP block (mt19937_64), generated in parallel.
         std::vector<double> Z((size_t)(M * V));
         std::vector<std::thread> th;
@@ -946,8 +951,21 @@ std::unique_ptr<GwPlan> plan_create(Context& c, std::shared_ptr<Prepared> P, con
         h2d(t->binoff.as<int64_t>(cs.bin_off.size()), cs.bin_off.data(), cs.bin_off.size(), c.st);
         h2d(t->wqoff.as<int64_t>(cs.wq_off.size()), cs.wq_off.data(), cs.wq_off.size(), c.st);
         h2d(t->z.as<double>(Z.size()), Z.data(), Z.size(), c.st);
-        t->wq.as<int8_t>((size_t)std::max<int64_t>(cs.wq_bytes, 16));
-        t->wcs.as<double>((size_t)(K * t->Vp));
+        if (tc) {
+            for (int64_t kk = 0; kk < K; ++kk)
+                t->lmax = std::max(t->lmax, cs.bin_off[(size_t)kk + 1] - cs.bin_off[(size_t)kk]);
+            t->lmax = std::max<int64_t>(t->lmax, 128);
+            const int nc = umma::ncolp_for(V);
+            const size_t bytes = (size_t)(K * 2 * nc) * (size_t)t->lmax;
+            int8_t* wq = t->wq.as<int8_t>(bytes);
+            ck(cudaMemsetAsync(wq, 0, bytes, c.st), "memset weights");
+            t->wcs.as<double>((size_t)(K * V));
+            t->tmW = make_map_2d(wq, (uint64_t)t->lmax, (uint64_t)(K * 2 * nc), (uint64_t)t->lmax,
+                                 128, (uint32_t)std::min(256, nc), CU_TENSOR_MAP_SWIZZLE_128B);
+        } else {
+            t->wq.as<int8_t>((size_t)std::max<int64_t>(cs.wq_bytes, 16));
+            t->wcs.as<double>((size_t)(K * t->Vp));
+        }
         ck(cudaStreamSynchronize(c.st), "plan upload");  // Z is a stack temporary
         pl->tiles.push_back(std::move(t));
         v0 += V;
@@ -1010,10 +1028,44 @@ void plan_execute(Context& c, GwPlan& pl) {
         w.wq_off = static_cast<int64_t*>(t.wqoff.p);
         w.wq = static_cast<int8_t*>(t.wq.p);
         w.colscale = static_cast<double*>(t.wcs.p);
-        launch_p1_weights(w, static_cast<double*>(P.d_mean.p), static_cast<double*>(P.d_sdinv.p),
-                          static_cast<double*>(t.z.p), M, 0, c.st);
-        if (tm) ck(cudaEventRecord(ev[e++], c.st), "event");
-        launch_p1(P.g, w, nullptr, static_cast<double*>(pl.y.p), c.st);
+        if (pl.umma) {
+            const int nc = umma::ncolp_for(t.V);
+            umma::P1UWeights uw;
+            uw.K = (int)K;
+            uw.V = t.V;
+            uw.ncolp = nc;
+            uw.lmax = t.lmax;
+            uw.rowind = w.rowind;
+            uw.sc = w.sc;
+            uw.bin_off = w.bin_off;
+            uw.wq = w.wq;
+            uw.colscale = w.colscale;
+            umma::launch_p1_weights4(uw, static_cast<double*>(P.d_mean.p),
+                                     static_cast<double*>(P.d_sdinv.p), static_cast<double*>(t.z.p),
+                                     M, c.st);
+            if (tm) ck(cudaEventRecord(ev[e++], c.st), "event");
+            umma::P1UArgs pa;
+            pa.K = (int)K;
+            pa.V = t.V;
+            pa.ncolp = nc;
+            pa.ngroups = (nc + 255) / 256;
+            pa.box_rows = std::min(256, nc);
+            pa.nbp = P.g.nbp;
+            pa.N_pad = P.g.N_pad;
+            pa.bin_off = w.bin_off;
+            pa.rowind = w.rowind;
+            pa.codes = P.g.codes;
+            pa.colscale = w.colscale;
+            pa.Y = static_cast<double*>(pl.y.p);
+            pa.status = static_cast<unsigned*>(pl.status.p);
+            umma::launch_p1_umma(t.tmW, pa, P.g.N_pad, c.st);
+        } else {
+            launch_p1_weights(w, static_cast<double*>(P.d_mean.p),
+                              static_cast<double*>(P.d_sdinv.p), static_cast<double*>(t.z.p), M, 0,
+                              c.st);
+            if (tm) ck(cudaEventRecord(ev[e++], c.st), "event");
+            launch_p1(P.g, w, nullptr, static_cast<double*>(pl.y.p), c.st);
+        }
         if (tm) ck(cudaEventRecord(ev[e++], c.st), "event");
         if (pl.umma) {
             const int nc = umma::ncolp_for(t.V);

@@ -24,6 +24,7 @@
 
 #include "lds_device.cuh"
 #include "lds_internal.h"
+#include "lds_tc.cuh"
 #include "lds_umma.h"
 
 namespace lds {
@@ -39,99 +40,6 @@ constexpr int kStageBytes = kPkBytes + 2 * kATile + kBTileMax;  // 69632
 constexpr int kThreads = 192;
 constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kOCol = 256;       // TMEM column of the O accumulator
-constexpr long long kWaitLimit = 1LL << 26;
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(
-        smem_u32(bar)));
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-    asm volatile(
-        "{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(
-            smem_u32(bar)),
-        "r"(bytes));
-}
-// Bounded wait for the phase with the given parity.  Returns false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-    const uint32_t addr = smem_u32(bar);
-    for (long long i = 0; i < kWaitLimit; ++i) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(done)
-            : "r"(addr), "r"(parity)
-            : "memory");
-        if (done) return true;
-    }
-    return false;
-}
-
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y,
-                                            uint64_t* bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes "
-        "[%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
-        : "memory");
-}
-
-// UMMA shared-memory descriptor: K-major, SWIZZLE_128B, 8-row groups 1024 B
-// apart (SBO), version 1 (sm100), base offset 0 (tiles are 1024-aligned).
-__device__ __forceinline__ uint64_t sw128_desc(const void* smem) {
-    const uint64_t a = (uint64_t)((smem_u32(smem) >> 4) & 0x3FFF);
-    return a | (1ULL << 16) | ((uint64_t)(1024 >> 4) << 32) | (1ULL << 46) | (2ULL << 61);
-}
-
-// Instruction descriptor: kind::i8, D = s32, A = s8, B = s8, both K-major.
-__host__ __device__ constexpr uint32_t idesc_i8(int M, int N) {
-    return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
-           ((uint32_t)(M >> 4) << 24);
-}
-
-__device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
-                                        uint32_t idesc, uint32_t accumulate) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
-}
-
-__device__ __forceinline__ void umma_commit(uint64_t* bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                     smem_u32(bar))
-                 : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, int (&r)[32]) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
-        "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
-          "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
-          "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
-          "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
-          "=r"(r[31])
-        : "r"(taddr));
-}
-
-__device__ __forceinline__ void tmem_wait_ld() {
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_before() {
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_after() {
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void fence_async_smem() {
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
 __global__ void __launch_bounds__(kThreads, 1)
     p2_umma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                    P2UArgs a) {
@@ -246,19 +154,8 @@ __global__ void __launch_bounds__(kThreads, 1)
                 if (*abort_flag) break;
                 uint8_t* st = smem + s * kStageBytes;
                 const uint4* pk = reinterpret_cast<const uint4*>(st + r * 32);
-                const uint4 p0 = pk[0], p1 = pk[1];
-                const uint32_t words[8] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w};
                 uint8_t* gRow = st + kPkBytes + (r >> 3) * 1024 + (r & 7) * 128;
-                uint8_t* oRow = gRow + kATile;
-#pragma unroll
-                for (int c = 0; c < 8; ++c) {  // 16-byte chunk c = samples 16c..16c+15
-                    uint32_t g0, g1, g2, g3, o0, o1, o2, o3;
-                    decode8(words[c] & 0xFFFFu, g0, g1, o0, o1);
-                    decode8(words[c] >> 16, g2, g3, o2, o3);
-                    const int off = ((c ^ (r & 7)) << 4);
-                    *reinterpret_cast<uint4*>(gRow + off) = make_uint4(g0, g1, g2, g3);
-                    *reinterpret_cast<uint4*>(oRow + off) = make_uint4(o0, o1, o2, o3);
-                }
+                decode_row_sw128(pk[0], pk[1], gRow, gRow + kATile, r);
                 fence_async_smem();
                 mbar_arrive(&full_dec[s]);
             }

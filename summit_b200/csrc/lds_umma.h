@@ -28,6 +28,35 @@ struct P2UArgs {
     long long* raw_o = nullptr;
 };
 
+// Phase-1 tcgen05 kernel arguments.  Member lists of bin k occupy
+// rowind[bin_off[k] .. bin_off[k+1]) (multiples of 128, padding rows carry
+// zero weights); weight digits Wq[((k*2+part)*ncolp + 4v+t)*lmax + r].
+struct P1UArgs {
+    int K = 0, V = 0, ncolp = 0, ngroups = 1, box_rows = 0;
+    int64_t nbp = 0, N_pad = 0;
+    const int64_t* bin_off = nullptr;
+    const int32_t* rowind = nullptr;
+    const uint8_t* codes = nullptr;
+    const double* colscale = nullptr;   // K*V
+    double* Y = nullptr;                // N_pad x (K*V), column (k*V+v)
+    unsigned int* status = nullptr;
+};
+
+struct P1UWeights {
+    int K = 0, V = 0, ncolp = 0;
+    int64_t lmax = 0;
+    const int32_t* rowind = nullptr;
+    const double* sc = nullptr;
+    const int64_t* bin_off = nullptr;
+    int8_t* wq = nullptr;
+    double* colscale = nullptr;
+};
+
+void launch_p1_weights4(const P1UWeights& w, const double* mean, const double* sdinv,
+                        const double* Z, int64_t z_ld, cudaStream_t st);
+size_t p1_umma_smem_bytes();
+void launch_p1_umma(const CUtensorMap& tmW, const P1UArgs& a, int64_t N_pad, cudaStream_t st);
+
 // Columns per bin (4 digits per probe, padded to a multiple of 16).
 inline int ncolp_for(int V) { return ((4 * V + 15) / 16) * 16; }
 
