@@ -30,29 +30,47 @@
 namespace lds {
 namespace umma {
 
-constexpr int kStages = 3;
 constexpr int kBM = 128;              // SNP rows per CTA (UMMA M)
 constexpr int kBK = 128;              // samples per stage (bytes per operand row)
 constexpr int kPkBytes = kBM * 32;    // packed tile: 128 rows x 32 bytes
 constexpr int kATile = kBM * kBK;     // 16 KB
-constexpr int kBTileMax = 256 * kBK;  // 32 KB
-constexpr int kStageBytes = kPkBytes + 2 * kATile + kBTileMax;  // 69632
-constexpr int kThreads = 192;
+constexpr int kPkStages = 8;          // packed-code ring (HBM latency)
+constexpr int kAStages = 2;           // decoded G/O operand ring
+constexpr int kBStages = 4;           // sketch-digit ring (L2 latency)
+constexpr int kThreads = 224;
 constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kOCol = 256;       // TMEM column of the O accumulator
+
+struct Layout {
+    uint32_t b_slot;                  // bytes of one sketch tile (box_rows x 128, 1 KB multiple)
+    __host__ __device__ explicit Layout(int box_rows)
+        : b_slot((uint32_t)(((box_rows * kBK) + 1023) / 1024 * 1024)) {}
+    __host__ __device__ uint32_t a_off(int s) const { return (uint32_t)s * 2 * kATile; }
+    __host__ __device__ uint32_t b_off(int s) const { return kAStages * 2 * kATile + s * b_slot; }
+    __host__ __device__ uint32_t pk_off(int s) const {
+        return kAStages * 2 * kATile + kBStages * b_slot + s * kPkBytes;
+    }
+    __host__ __device__ uint32_t bar_off() const { return pk_off(kPkStages); }
+    __host__ __device__ uint32_t bytes() const { return bar_off() + 256; }
+};
+
 __global__ void __launch_bounds__(kThreads, 1)
     p2_umma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                    P2UArgs a) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
-    uint64_t* full_tma = bars;                 // [kStages]
-    uint64_t* full_dec = bars + kStages;       // [kStages]
-    uint64_t* empty = bars + 2 * kStages;      // [kStages]
-    uint64_t* acc_full = bars + 3 * kStages;
-    uint64_t* acc_empty = bars + 3 * kStages + 1;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 3 * kStages + 2);
+    const Layout lay(a.box_rows);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + lay.bar_off());
+    uint64_t* pk_full = bars;                          // [kPkStages]
+    uint64_t* pk_empty = pk_full + kPkStages;          // [kPkStages]
+    uint64_t* a_full = pk_empty + kPkStages;           // [kAStages]
+    uint64_t* a_empty = a_full + kAStages;             // [kAStages]
+    uint64_t* b_full = a_empty + kAStages;             // [kBStages]
+    uint64_t* b_empty = b_full + kBStages;             // [kBStages]
+    uint64_t* acc_full = b_empty + kBStages;
+    uint64_t* acc_empty = acc_full + 1;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_empty + 1);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -60,10 +78,17 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int64_t jt0 = a.j0 + (int64_t)blockIdx.x * kBM;
 
     if (tid == 0) {
-        for (int s = 0; s < kStages; ++s) {
-            mbar_init(&full_tma[s], 1);
-            mbar_init(&full_dec[s], 128);
-            mbar_init(&empty[s], 1);
+        for (int s = 0; s < kPkStages; ++s) {
+            mbar_init(&pk_full[s], 1);
+            mbar_init(&pk_empty[s], 128);
+        }
+        for (int s = 0; s < kAStages; ++s) {
+            mbar_init(&a_full[s], 128);
+            mbar_init(&a_empty[s], 1);
+        }
+        for (int s = 0; s < kBStages; ++s) {
+            mbar_init(&b_full[s], 1);
+            mbar_init(&b_empty[s], 1);
         }
         mbar_init(acc_full, 1);
         mbar_init(acc_empty, 128);
@@ -87,22 +112,30 @@ __global__ void __launch_bounds__(kThreads, 1)
     };
 
     const int ngroups = a.ngroups;
+    const int total = ngroups * a.nkt;
     if (warp == 0) {
-        // ---------------- TMA producer ----------------
+        // ---------------- packed-code producer (runs up to 8 stages ahead) ----------------
         if (lane == 0) {
-            int it = 0;
-            for (int g = 0; g < ngroups && !*abort_flag; ++g) {
-                for (int kt = 0; kt < a.nkt; ++kt, ++it) {
-                    const int s = it % kStages;
-                    const uint32_t ph = (uint32_t)(it / kStages) & 1u;
-                    if (it >= kStages && !mbar_wait(&empty[s], ph ^ 1u)) { fail(1); break; }
-                    if (*abort_flag) break;
-                    uint8_t* st = smem + s * kStageBytes;
-                    mbar_expect_tx(&full_tma[s], (uint32_t)(kPkBytes + a.box_rows * kBK));
-                    tma_load_2d(st, &tmA, kt * 32, (int)jt0, &full_tma[s]);
-                    tma_load_2d(st + kPkBytes + 2 * kATile, &tmB, kt * kBK,
-                                k * a.ncolp + g * 256, &full_tma[s]);
-                }
+            for (int it = 0; it < total; ++it) {
+                const int s = it % kPkStages;
+                if (it >= kPkStages &&
+                    !mbar_wait(&pk_empty[s], ((uint32_t)(it / kPkStages) & 1u) ^ 1u)) { fail(1); break; }
+                if (*abort_flag) break;
+                mbar_expect_tx(&pk_full[s], (uint32_t)kPkBytes);
+                tma_load_2d(smem + lay.pk_off(s), &tmA, (it % a.nkt) * 32, (int)jt0, &pk_full[s]);
+            }
+        }
+    } else if (warp == 2) {
+        // ---------------- sketch-digit producer ----------------
+        if (lane == 0) {
+            for (int it = 0; it < total; ++it) {
+                const int s = it % kBStages;
+                if (it >= kBStages &&
+                    !mbar_wait(&b_empty[s], ((uint32_t)(it / kBStages) & 1u) ^ 1u)) { fail(2); break; }
+                if (*abort_flag) break;
+                const int g = it / a.nkt, kt = it % a.nkt;
+                mbar_expect_tx(&b_full[s], (uint32_t)(a.box_rows * kBK));
+                tma_load_2d(smem + lay.b_off(s), &tmB, kt * kBK, k * a.ncolp + g * 256, &b_full[s]);
             }
         }
     } else if (warp == 1) {
@@ -112,32 +145,32 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (int g = 0; g < ngroups && !*abort_flag; ++g) {
                 const int ncols = min(256, a.ncolp - g * 256);
                 const uint32_t idesc = idesc_i8(kBM, ncols);
-                if (g > 0 && !mbar_wait(acc_empty, (uint32_t)(g - 1) & 1u)) { fail(2); break; }
+                if (g > 0 && !mbar_wait(acc_empty, (uint32_t)(g - 1) & 1u)) { fail(3); break; }
                 tc_fence_after();
                 for (int kt = 0; kt < a.nkt; ++kt, ++it) {
-                    const int s = it % kStages;
-                    const uint32_t ph = (uint32_t)(it / kStages) & 1u;
-                    if (!mbar_wait(&full_dec[s], ph)) { fail(3); break; }
+                    const int sa = it % kAStages, sb = it % kBStages;
+                    if (!mbar_wait(&a_full[sa], (uint32_t)(it / kAStages) & 1u) ||
+                        !mbar_wait(&b_full[sb], (uint32_t)(it / kBStages) & 1u)) { fail(4); break; }
                     if (*abort_flag) break;
                     tc_fence_after();
-                    uint8_t* st = smem + s * kStageBytes;
-                    const uint64_t dG = sw128_desc(st + kPkBytes);
-                    const uint64_t dO = sw128_desc(st + kPkBytes + kATile);
-                    const uint64_t dB = sw128_desc(st + kPkBytes + 2 * kATile);
+                    const uint64_t dG = sw128_desc(smem + lay.a_off(sa));
+                    const uint64_t dO = sw128_desc(smem + lay.a_off(sa) + kATile);
+                    const uint64_t dB = sw128_desc(smem + lay.b_off(sb));
 #pragma unroll
                     for (int kk = 0; kk < kBK / 32; ++kk) {
                         const uint32_t acc = (kt | kk) ? 1u : 0u;
                         umma_i8(tmem, dG + 2 * kk, dB + 2 * kk, idesc, acc);
                         umma_i8(tmem + kOCol, dO + 2 * kk, dB + 2 * kk, idesc, acc);
                     }
-                    umma_commit(&empty[s]);
+                    umma_commit(&a_empty[sa]);
+                    umma_commit(&b_empty[sb]);
                 }
                 umma_commit(acc_full);
             }
         }
     } else {
-        // ---------------- decoders + epilogue (warps 2..5) ----------------
-        const int r = tid - 64;              // operand row this thread decodes
+        // ---------------- decoders + epilogue (warps 3..6) ----------------
+        const int r = tid - 96;              // operand row this thread decodes
         const int q = warp & 3;              // TMEM lane quadrant this warp may access
         const int row = q * 32 + lane;       // accumulator row (SNP) of this thread
         const int64_t j = jt0 + row;
@@ -148,20 +181,22 @@ __global__ void __launch_bounds__(kThreads, 1)
         int it = 0;
         for (int g = 0; g < ngroups; ++g) {
             for (int kt = 0; kt < a.nkt; ++kt, ++it) {
-                const int s = it % kStages;
-                const uint32_t ph = (uint32_t)(it / kStages) & 1u;
-                if (!mbar_wait(&full_tma[s], ph)) { fail(4); break; }
+                const int sp = it % kPkStages, sa = it % kAStages;
+                if (!mbar_wait(&pk_full[sp], (uint32_t)(it / kPkStages) & 1u)) { fail(5); break; }
                 if (*abort_flag) break;
-                uint8_t* st = smem + s * kStageBytes;
-                const uint4* pk = reinterpret_cast<const uint4*>(st + r * 32);
-                uint8_t* gRow = st + kPkBytes + (r >> 3) * 1024 + (r & 7) * 128;
-                decode_row_sw128(pk[0], pk[1], gRow, gRow + kATile, r);
+                const uint4* pk = reinterpret_cast<const uint4*>(smem + lay.pk_off(sp) + r * 32);
+                const uint4 p0 = pk[0], p1 = pk[1];
+                mbar_arrive(&pk_empty[sp]);
+                if (it >= kAStages &&
+                    !mbar_wait(&a_empty[sa], ((uint32_t)(it / kAStages) & 1u) ^ 1u)) { fail(6); break; }
+                uint8_t* gRow = smem + lay.a_off(sa) + (r >> 3) * 1024 + (r & 7) * 128;
+                decode_row_sw128(p0, p1, gRow, gRow + kATile, r);
                 fence_async_smem();
-                mbar_arrive(&full_dec[s]);
+                mbar_arrive(&a_full[sa]);
             }
             if (*abort_flag) break;
             // Epilogue of column group g.
-            if (!mbar_wait(acc_full, (uint32_t)g & 1u)) { fail(5); break; }
+            if (!mbar_wait(acc_full, (uint32_t)g & 1u)) { fail(7); break; }
             tc_fence_after();
             const int ncols = min(256, a.ncolp - g * 256);
             const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16);
@@ -291,20 +326,21 @@ void launch_quantize_y4(const double* Y, int64_t N, int64_t N_pad, int K, int V,
     }
 }
 
-size_t p2_umma_smem_bytes() { return (size_t)kStages * kStageBytes + 1024 + 256; }
+size_t p2_umma_smem_bytes(int box_rows) { return (size_t)Layout(box_rows).bytes() + 1024; }
 
 void launch_p2_umma(const CUtensorMap& tmA, const CUtensorMap& tmB, const P2UArgs& a,
                     cudaStream_t st) {
     const int64_t rows = a.j1 - a.j0;
     if (rows <= 0 || a.K <= 0) return;
-    static bool attr = false;
-    if (!attr) {
+    const size_t smem = p2_umma_smem_bytes(a.box_rows);
+    static size_t attr = 0;
+    if (attr < smem) {
         cudaFuncSetAttribute(p2_umma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)p2_umma_smem_bytes());
-        attr = true;
+                             (int)p2_umma_smem_bytes(256));
+        attr = p2_umma_smem_bytes(256);
     }
     dim3 grid((unsigned)((rows + kBM - 1) / kBM), (unsigned)a.K);
-    p2_umma_kernel<<<grid, kThreads, p2_umma_smem_bytes(), st>>>(tmA, tmB, a);
+    p2_umma_kernel<<<grid, kThreads, smem, st>>>(tmA, tmB, a);
     count_launch();
 }
 

@@ -62,7 +62,7 @@ inline int ncolp_for(int V) { return ((4 * V + 15) / 16) * 16; }
 
 void launch_quantize_y4(const double* Y, int64_t N, int64_t N_pad, int K, int V, int ncolp,
                         int8_t* Yq, double* colscale, cudaStream_t st);
-size_t p2_umma_smem_bytes();
+size_t p2_umma_smem_bytes(int box_rows);
 void launch_p2_umma(const CUtensorMap& tmA, const CUtensorMap& tmB, const P2UArgs& a,
                     cudaStream_t st);
 
