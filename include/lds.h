@@ -228,6 +228,40 @@ int lds_set_p2_kernel(int impl);
 int lds_synth_bed(int64_t n, int64_t M, uint64_t seed, const int64_t* t0, const int64_t* t1,
                   int missing, uint8_t* out);
 
+/* ---------------------------------------------------------------------
+ * Phase 2 without any device allocation.  No counterpart in the reference.
+ *
+ * For callers that cannot allocate device memory during this step — work
+ * captured into a CUDA graph (an allocation would break the capture),
+ * programs whose device memory belongs to another framework's pool, and
+ * services that forbid allocator calls after start-up.  The caller passes
+ * device buffers it owns; the library's scratch (4-digit sketch split,
+ * column scales, status words) is one fixed array of
+ * LDS_NOALLOC_SCRATCH_BYTES held by every GPU that loads liblds.so until the
+ * process exits.  Requires K * ceil16(4 V) * 4 row_bytes + 8 K V + ~1 KiB
+ * <= LDS_NOALLOC_SCRATCH_BYTES; larger sizes are rejected with LDS_ERR_ARG.
+ *
+ *   d_codes: packed genotype rows in the library's device layout: row j at
+ *     d_codes + j*row_bytes, row_bytes a multiple of 64 (N_pad = 4 row_bytes
+ *     samples), sample i in bits 2(i%4) of byte i/4, samples >= n coded 01;
+ *     16-byte aligned; rows_total rows addressable (rows_total >= j1).
+ *   d_Y: sketch, N_pad x (K*V) column-major (column k*V + v), FP64.
+ *   d_mean, d_sdinv, d_left_scale: per SNP row (index j), FP64.
+ *   d_accum: (j1-j0) x K row-major FP64, += sum_v Work^2 * left_scale with
+ *     the guards of lds_phase2_accum_XtXz_bed; d_mc (may be NULL) += the
+ *     fourth-moment sums.  Asynchronous on `stream` (cudaStream_t or NULL).
+ * The first call on each device looks up the scratch array's address
+ * (cudaGetSymbolAddress) and must come before any stream capture.  All
+ * calls share the array and it keeps the last call's contents, so calls
+ * that overlap on the GPU race; serialize them.
+ * ------------------------------------------------------------------- */
+#define LDS_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
+int lds_phase2_accum_device_noalloc(const uint8_t* d_codes, int64_t row_bytes, int64_t n,
+                                    int64_t rows_total, int64_t j0, int64_t j1, const double* d_Y,
+                                    int K, int V, const double* d_mean, const double* d_sdinv,
+                                    const double* d_left_scale, double* d_accum, double* d_mc,
+                                    void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1222,6 +1222,9 @@ void gw_ldscore_impl(const uint8_t* bed_rows, int64_t row_bytes, int64_t n_total
 }
 
 }  // namespace
+
+void set_last_error(const std::string& msg) { g_err = msg; }
+
 }  // namespace lds
 
 using namespace lds;

@@ -2,6 +2,7 @@
 // kernels (lds_kernels.cu).  Not part of the C ABI.
 #pragma once
 #include <cstdint>
+#include <string>
 #include <cuda_runtime.h>
 
 namespace lds {
@@ -94,5 +95,8 @@ void launch_synth(int64_t n, int64_t M, uint64_t seed, const int64_t* t0, const 
 
 // Launch accounting.
 void count_launch();
+
+// Set the text returned by lds_last_error() for the calling thread.
+void set_last_error(const std::string& msg);
 
 }  // namespace lds
