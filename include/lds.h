@@ -195,6 +195,34 @@ int lds_gw_plan_results(int64_t plan, double* ldscore, double* meansq_accum, dou
 int lds_gw_plan_kernel_ms(int64_t plan, double* ms4);
 int lds_gw_plan_destroy(int64_t plan);
 
+/* ---------------------------------------------------------------------
+ * Windowed + partitioned LD scores (stochastic, probe based).  Windows are a
+ * contiguous partition of the SNPs: window w = [window_starts[w],
+ * window_starts[w+1]), window_starts[0] = 0, window_starts[n_windows] = M.
+ * For SNP j in window w and bin k the estimate is the genome-wide estimator
+ * restricted to window w: sum over probes of (x_j^T X_w D_k z)^2 scaled as in
+ * phase 2, divided by nvecs, minus M_{w,k}/(N - ddof).  Window w draws its
+ * own probes: root seed lds_window_seed(seed, w), SNP blocks of step_size
+ * counted from the window start — so window w's scores equal lds_gw_ldscore
+ * on the window's SNPs with that seed.  All windows run as batched phase-1
+ * super-bins and a tile-table phase 2; the first execute captures the whole
+ * estimate into one CUDA graph and later executes launch that graph.
+ * batch_gb bounds the FP64 sketch of one window batch (<= 0: 8 GB).
+ * No single reference counterpart: the reference's windowed scores are
+ * exact (winldcore.cpp:783-931); this is the probe estimator of
+ * gw_ldscore.py:1753-2222 applied per window.
+ * ------------------------------------------------------------------- */
+int lds_win_plan_create(int64_t geno, const double* annot, int64_t K,
+                        const int64_t* window_starts, int64_t n_windows, int nvecs,
+                        int step_size, int vtile, uint64_t seed, int rand_dist, double resvar_eps,
+                        int as_float, int with_mc, double batch_gb, int64_t* plan_out);
+int lds_win_plan_execute(int64_t plan);
+int lds_win_plan_results(int64_t plan, double* ldscore, double* meansq_accum, double* inv_out,
+                         double* mc_per_snp_sumsq);
+int lds_win_plan_kernel_ms(int64_t plan, double* ms4);
+int lds_win_plan_destroy(int64_t plan);
+uint64_t lds_window_seed(uint64_t root, int64_t w);
+
 /* Device timing of the last lds_gw_ldscore call (milliseconds, CUDA events
  * on the library stream): [0] upload+prepare, [1] phase 1 total, [2] phase 2
  * total, [3] whole call. */

@@ -145,19 +145,23 @@ class Oracle:
     # ------------------------------------------------------------------
     def gw_ldscore(self, bed_rows, n, annot, nvecs, step, seed, dist="rademacher",
                    vtile=None, ddof=1, impute="mean", impute_seed=0, as_float=False,
-                   with_mc=False, rows=None, eps=1e-10):
+                   with_mc=False, rows=None, eps=1e-10, snp0=None):
         """Whole genome-wide estimator on our restatement (FP64 arithmetic).
 
-        Returns a dict with ``ldscore`` (M x K), ``meansq_accum``, ``inv`` and,
-        if requested, the MC fourth-moment sums.
+        ``snp0`` (not None) runs the estimator on SNPs [snp0, snp0 + len(annot)) of the
+        full image ``bed_rows`` (blocks and probe seeds counted from snp0, HWE
+        imputation seeded by the SNP's index in the image) — one window of a
+        windowed estimate.  Returns a dict with ``ldscore`` (M x K),
+        ``meansq_accum``, ``inv`` and, if requested, the MC fourth-moment sums.
         """
-        m = bed_rows.shape[0]
+        m = bed_rows.shape[0] if snp0 is None else len(annot)
+        base = 0 if snp0 is None else int(snp0)
         annot = np.ascontiguousarray(annot, dtype=np.float64)
         K = annot.shape[1]
         nsel = n if rows is None else len(rows)
         blocks = compute_blocks(m, step)
         vt = bounded_vtile_sizes(nvecs, vtile or nvecs)
-        std = [self.standardize(bed_rows, n, s, e, rows, ddof, impute, impute_seed)[0]
+        std = [self.standardize(bed_rows, n, base + s, base + e, rows, ddof, impute, impute_seed)[0]
                for (s, e) in blocks]
         inv = np.concatenate([self.inv_resvar(g, eps) for g in std])
         if as_float:

@@ -79,9 +79,27 @@ int guarded(F&& f) {
 // ---------------------------------------------------------------------------
 // Device buffers
 // ---------------------------------------------------------------------------
+// Owning device allocation; move-only so containers never double-free.
 struct DevBuf {
     void* p = nullptr;
     size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) {
+        o.p = nullptr;
+        o.n = 0;
+    }
+    DevBuf& operator=(DevBuf&& o) noexcept {
+        if (this != &o) {
+            release();
+            p = o.p;
+            n = o.n;
+            o.p = nullptr;
+            o.n = 0;
+        }
+        return *this;
+    }
     void* get(size_t bytes) {
         if (bytes <= n && p) return p;
         release();
@@ -1191,6 +1209,346 @@ void plan_results(Context& c, GwPlan& pl, double* ldscore, double* meansq_out, d
     }
 }
 
+// ---------------------------------------------------------------------------
+// Windowed estimates: SNP windows (a contiguous partition, window w = SNPs
+// [ws[w], ws[w+1])) are independent genome-wide problems on their SNPs.  Each
+// window draws its own probes (root seed window_seed(root, w), blocks of
+// `step` SNPs counted from the window start), so window w's LD scores equal
+// the genome-wide estimate on the window's sub-fileset with that seed.
+// (window, bin) pairs become phase-1 super-bins; phase 2 runs over a tile
+// table covering all windows of a batch.  Batches bound the sketch memory.
+// ---------------------------------------------------------------------------
+uint64_t window_seed(uint64_t root, int64_t w) {
+    return mix64(root ^ mix64(0x77696e646f77ULL + (uint64_t)w));
+}
+
+struct WinPlan {
+    std::shared_ptr<Prepared> P;
+    int64_t K = 0, W = 0;
+    int nvecs = 0, with_mc = 0;
+    std::vector<int> vt;
+    std::vector<int64_t> ws;            // W+1 window starts
+    std::vector<int32_t> win_of;        // SNP -> window
+    std::vector<double> inv, Mkw;       // Mkw[w*K + k]
+    struct Batch {
+        int64_t w0 = 0, w1 = 0, ksup = 0, lmax = 0;
+        Csr csr;
+        DevBuf rowind, sc, binoff, tiles;
+        int64_t ntiles = 0;
+    };
+    std::vector<Batch> batches;
+    std::vector<DevBuf> z;              // per V-tile, M x V FP64 probes
+    DevBuf y, yq, ycs, wq, wcs, accum, mc, lscale, guards, status;
+    CUtensorMap tmA;
+    std::vector<cudaEvent_t> ev;        // start, after phase 1 of each launch group, end
+    double kernel_ms[4] = {0, 0, 0, 0};
+    int pending = 0;
+    cudaGraphExec_t graph = nullptr;
+    ~WinPlan() {
+        for (cudaEvent_t e : ev) cudaEventDestroy(e);
+        if (graph) cudaGraphExecDestroy(graph);
+    }
+};
+
+std::map<int64_t, std::unique_ptr<WinPlan>>& win_table() {
+    static std::map<int64_t, std::unique_ptr<WinPlan>> t;
+    return t;
+}
+
+std::unique_ptr<WinPlan> win_plan_create(Context& c, std::shared_ptr<Prepared> P,
+                                         const double* annot, int64_t K, const int64_t* ws,
+                                         int64_t W, int nvecs, int step, int vtile, uint64_t seed,
+                                         int dist, double eps, int as_float, int with_mc,
+                                         double batch_gb) {
+    const int64_t M = P->g.M, N = P->g.N, Np = P->g.N_pad;
+    if (nvecs <= 0 || step <= 0 || K <= 0 || W <= 0) fail(LDS_ERR_ARG, "invalid sizes");
+    if (ws[0] != 0 || ws[W] != M) fail(LDS_ERR_ARG, "windows must partition [0, M)");
+    for (int64_t w = 0; w < W; ++w)
+        if (ws[w + 1] <= ws[w]) fail(LDS_ERR_ARG, "window starts must increase");
+    if (c.slices != 4 || p2_impl() != 1)
+        fail(LDS_ERR_ARG, "windowed estimates need the tcgen05 kernels with 4 digits");
+    auto pl = std::make_unique<WinPlan>();
+    pl->P = P;
+    pl->K = K;
+    pl->W = W;
+    pl->nvecs = nvecs;
+    pl->with_mc = with_mc;
+    pl->ws.assign(ws, ws + W + 1);
+    pl->win_of.resize((size_t)M);
+    for (int64_t w = 0; w < W; ++w)
+        for (int64_t j = ws[w]; j < ws[w + 1]; ++j) pl->win_of[(size_t)j] = (int32_t)w;
+    {
+        int width = std::min(nvecs, vtile > 0 ? vtile : nvecs);
+        if (width >= 64) width = std::max(64, (width / 64) * 64);
+        for (int s = 0; s < nvecs; s += width) pl->vt.push_back(std::min(width, nvecs - s));
+    }
+    const int vmax = *std::max_element(pl->vt.begin(), pl->vt.end());
+    const int ncmax = umma::ncolp_for(vmax);
+    pl->inv.resize((size_t)M);
+    for (int64_t j = 0; j < M; ++j)
+        pl->inv[(size_t)j] =
+            as_float ? (double)inv_resvar<float>(*P, j, eps) : inv_resvar<double>(*P, j, eps);
+    pl->Mkw.assign((size_t)(W * K), 0.0);
+    for (int64_t j = 0; j < M; ++j)
+        for (int64_t k = 0; k < K; ++k)
+            pl->Mkw[(size_t)(pl->win_of[(size_t)j] * K + k)] += annot[j * K + k];
+    const double denom = std::max(1.0, (double)(N - P->ddof + 1) - 1.0);
+    const double inv_denom2 = 1.0 / (denom * denom);
+    std::vector<double> ls((size_t)M);
+    for (int64_t j = 0; j < M; ++j) {
+        const double v = pl->inv[(size_t)j];
+        ls[(size_t)j] = (std::isfinite(v) && v > 0.0) ? v * v * inv_denom2 : 0.0;
+    }
+    h2d(pl->lscale.as<double>((size_t)M), ls.data(), (size_t)M, c.st);
+    // Window batches: the FP64 sketch of a batch stays under batch_gb.
+    const double per_window = (double)Np * (double)K * vmax * 8.0;
+    const int64_t wb = std::max<int64_t>(1, (int64_t)(batch_gb * 1e9 / per_window));
+    std::vector<float> annot_f, inv_f;
+    if (as_float) {
+        annot_f.assign(annot, annot + M * K);
+        inv_f.resize((size_t)M);
+        for (int64_t j = 0; j < M; ++j) inv_f[(size_t)j] = (float)pl->inv[(size_t)j];
+    }
+    int64_t max_ksup = 0, max_wq = 0;
+    for (int64_t w0 = 0; w0 < W; w0 += wb) {
+        WinPlan::Batch b;
+        b.w0 = w0;
+        b.w1 = std::min(W, w0 + wb);
+        b.ksup = (b.w1 - b.w0) * K;
+        // Super-bin CSR: super-bin (w - w0)*K + k lists the window's members of bin k.
+        Csr cs;
+        cs.bin_off.assign((size_t)b.ksup + 1, 0);
+        cs.nnz.assign((size_t)b.ksup, 0);
+        std::vector<int32_t> ri;
+        std::vector<double> scv;
+        int64_t off = 0;
+        for (int64_t w = b.w0; w < b.w1; ++w) {
+            const int64_t a0 = ws[w], L = ws[w + 1] - ws[w];
+            Csr part = as_float
+                           ? build_csr<float>(annot_f.data() + a0 * K, inv_f.data() + a0, L, K, a0, 16, 4, 128)
+                           : build_csr<double>(annot + a0 * K, pl->inv.data() + a0, L, K, a0, 16, 4, 128);
+            for (int64_t k = 0; k < K; ++k) {
+                const int64_t sbk = (w - b.w0) * K + k;
+                cs.bin_off[(size_t)sbk] = off;
+                cs.nnz[(size_t)sbk] = part.nnz[(size_t)k];
+                const int64_t p0 = part.bin_off[(size_t)k], p1 = part.bin_off[(size_t)k + 1];
+                ri.insert(ri.end(), part.rowind.begin() + p0, part.rowind.begin() + p1);
+                scv.insert(scv.end(), part.sc.begin() + p0, part.sc.begin() + p1);
+                off += p1 - p0;
+                b.lmax = std::max(b.lmax, p1 - p0);
+            }
+        }
+        cs.bin_off[(size_t)b.ksup] = off;
+        b.lmax = std::max<int64_t>(b.lmax, 128);
+        const size_t nm = std::max<size_t>(ri.size(), 1);
+        h2d(b.rowind.as<int32_t>(nm), ri.data(), ri.size(), c.st);
+        h2d(b.sc.as<double>(nm), scv.data(), scv.size(), c.st);
+        h2d(b.binoff.as<int64_t>(cs.bin_off.size()), cs.bin_off.data(), cs.bin_off.size(), c.st);
+        std::vector<int4> tiles;
+        for (int64_t w = b.w0; w < b.w1; ++w)
+            for (int64_t j = ws[w]; j < ws[w + 1]; j += 128)
+                tiles.push_back(make_int4((int)j, (int)ws[w + 1], (int)((w - b.w0) * K), 0));
+        b.ntiles = (int64_t)tiles.size();
+        h2d(b.tiles.as<int4>(tiles.size()), tiles.data(), tiles.size(), c.st);
+        ck(cudaStreamSynchronize(c.st), "window batch upload");
+        max_ksup = std::max(max_ksup, b.ksup);
+        max_wq = std::max(max_wq, b.ksup * 2 * ncmax * b.lmax);
+        b.csr.nnz = cs.nnz;
+        pl->batches.push_back(std::move(b));
+    }
+    // Probes: per window, blocks counted from the window start.
+    const unsigned hw = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+    std::vector<std::pair<int64_t, int64_t>> units;  // (window, relative block start)
+    for (int64_t w = 0; w < W; ++w)
+        for (int64_t s = 0; s < ws[w + 1] - ws[w]; s += step) units.push_back({w, s});
+    int v0 = 0;
+    for (int V : pl->vt) {
+        std::vector<double> Z((size_t)(M * V));
+        std::vector<std::thread> th;
+        std::atomic<size_t> next{0};
+        for (unsigned t = 0; t < hw; ++t)
+            th.emplace_back([&] {
+                for (size_t u; (u = next.fetch_add(1)) < units.size();) {
+                    const int64_t w = units[u].first, s = units[u].second;
+                    const int64_t a0 = ws[w];
+                    const int L = (int)std::min<int64_t>(step, ws[w + 1] - a0 - s);
+                    const uint64_t rw = window_seed(seed, w);
+                    if (as_float) make_probes<float>(rw, (int)s, v0, L, V, dist, &Z[(size_t)(a0 + s)], M);
+                    else make_probes<double>(rw, (int)s, v0, L, V, dist, &Z[(size_t)(a0 + s)], M);
+                }
+            });
+        for (auto& x : th) x.join();
+        pl->z.emplace_back();
+        h2d(pl->z.back().as<double>(Z.size()), Z.data(), Z.size(), c.st);
+        ck(cudaStreamSynchronize(c.st), "probe upload");
+        v0 += V;
+    }
+    pl->y.as<double>((size_t)(Np * max_ksup * vmax));
+    pl->yq.as<int8_t>((size_t)(max_ksup * ncmax * Np));
+    pl->ycs.as<double>((size_t)(max_ksup * vmax));
+    int8_t* wq = pl->wq.as<int8_t>((size_t)std::max<int64_t>(max_wq, 16));
+    (void)wq;
+    pl->wcs.as<double>((size_t)(max_ksup * vmax));
+    pl->accum.as<double>((size_t)(M * K));
+    if (with_mc) pl->mc.as<double>((size_t)(M * K));
+    pl->guards.as<unsigned long long>(2);
+    ck(cudaMemsetAsync(pl->status.as<unsigned>(1), 0, 4, c.st), "memset");
+    pl->tmA = make_map_2d(P->g.codes, (uint64_t)P->g.nbp, (uint64_t)P->g.M_pad, (uint64_t)P->g.nbp,
+                          32, 128, CU_TENSOR_MAP_SWIZZLE_NONE);
+    pl->ev.resize(1 + 4 * pl->vt.size() * pl->batches.size());
+    for (auto& e : pl->ev) ck(cudaEventCreate(&e), "event");
+    umma::prepare_p1_umma();
+    umma::prepare_p2_umma();
+    ck(cudaStreamSynchronize(c.st), "window plan");
+    return pl;
+}
+
+// Enqueue one windowed estimate (all V-tiles, all batches).
+void win_enqueue(Context& c, WinPlan& pl) {
+    Prepared& P = *pl.P;
+    const int64_t M = P.g.M, K = pl.K, Np = P.g.N_pad;
+    ck(cudaMemsetAsync(pl.accum.p, 0, sizeof(double) * (size_t)(M * K), c.st), "memset");
+    if (pl.with_mc) ck(cudaMemsetAsync(pl.mc.p, 0, sizeof(double) * (size_t)(M * K), c.st), "memset");
+    ck(cudaMemsetAsync(pl.guards.p, 0, 16, c.st), "memset");
+    int e = 0;
+    ck(cudaEventRecordWithFlags(pl.ev[(size_t)e++], c.st, cudaEventRecordExternal), "event");
+    for (size_t ti = 0; ti < pl.vt.size(); ++ti) {
+        const int V = pl.vt[ti];
+        const int nc = umma::ncolp_for(V);
+        for (auto& b : pl.batches) {
+            umma::P1UWeights uw;
+            uw.K = (int)b.ksup;
+            uw.V = V;
+            uw.ncolp = nc;
+            uw.lmax = b.lmax;
+            uw.rowind = static_cast<int32_t*>(b.rowind.p);
+            uw.sc = static_cast<double*>(b.sc.p);
+            uw.bin_off = static_cast<int64_t*>(b.binoff.p);
+            uw.wq = static_cast<int8_t*>(pl.wq.p);
+            uw.colscale = static_cast<double*>(pl.wcs.p);
+            const size_t wbytes = (size_t)(b.ksup * 2 * nc) * (size_t)b.lmax;
+            ck(cudaMemsetAsync(pl.wq.p, 0, wbytes, c.st), "memset weights");
+            umma::launch_p1_weights4(uw, static_cast<double*>(P.d_mean.p),
+                                     static_cast<double*>(P.d_sdinv.p),
+                                     static_cast<double*>(pl.z[ti].p), M, c.st);
+            ck(cudaEventRecordWithFlags(pl.ev[(size_t)e++], c.st, cudaEventRecordExternal), "event");
+            const CUtensorMap tmW =
+                make_map_2d(pl.wq.p, (uint64_t)b.lmax, (uint64_t)(b.ksup * 2 * nc), (uint64_t)b.lmax,
+                            128, (uint32_t)std::min(256, nc), CU_TENSOR_MAP_SWIZZLE_128B);
+            umma::P1UArgs pa;
+            pa.K = (int)b.ksup;
+            pa.V = V;
+            pa.ncolp = nc;
+            pa.ngroups = (nc + 255) / 256;
+            pa.box_rows = std::min(256, nc);
+            pa.nbp = P.g.nbp;
+            pa.N_pad = Np;
+            pa.bin_off = uw.bin_off;
+            pa.rowind = uw.rowind;
+            pa.codes = P.g.codes;
+            pa.colscale = uw.colscale;
+            pa.Y = static_cast<double*>(pl.y.p);
+            pa.status = static_cast<unsigned*>(pl.status.p);
+            umma::launch_p1_umma(tmW, pa, Np, c.st);
+            ck(cudaEventRecordWithFlags(pl.ev[(size_t)e++], c.st, cudaEventRecordExternal), "event");
+            umma::launch_quantize_y4(static_cast<double*>(pl.y.p), P.g.N, Np, (int)b.ksup, V, nc,
+                                     static_cast<int8_t*>(pl.yq.p), static_cast<double*>(pl.ycs.p),
+                                     c.st);
+            ck(cudaEventRecordWithFlags(pl.ev[(size_t)e++], c.st, cudaEventRecordExternal), "event");
+            const CUtensorMap tmB =
+                make_map_2d(pl.yq.p, (uint64_t)Np, (uint64_t)(b.ksup * nc), (uint64_t)Np, 128,
+                            (uint32_t)std::min(256, nc), CU_TENSOR_MAP_SWIZZLE_128B);
+            umma::P2UArgs u;
+            u.K = (int)K;
+            u.V = V;
+            u.ncolp = nc;
+            u.ngroups = (nc + 255) / 256;
+            u.box_rows = std::min(256, nc);
+            u.nkt = (int)(Np / 128);
+            u.M = M;
+            u.j0 = 0;
+            u.j1 = b.ntiles;  // number of tiles (tile-table mode)
+            u.out_row0 = 0;
+            u.colscale = static_cast<double*>(pl.ycs.p);
+            u.mean = static_cast<double*>(P.d_mean.p);
+            u.sdinv = static_cast<double*>(P.d_sdinv.p);
+            u.left_scale = static_cast<double*>(pl.lscale.p);
+            u.accum = static_cast<double*>(pl.accum.p);
+            u.mc = pl.with_mc ? static_cast<double*>(pl.mc.p) : nullptr;
+            u.guard_counts = static_cast<unsigned long long*>(pl.guards.p);
+            u.extreme_warn = extreme_warn_env();
+            u.drop_extreme = drop_extreme_env();
+            u.status = static_cast<unsigned*>(pl.status.p);
+            u.tiles = static_cast<int4*>(b.tiles.p);
+            umma::launch_p2_umma(pl.tmA, tmB, u, c.st);
+            ck(cudaEventRecordWithFlags(pl.ev[(size_t)e++], c.st, cudaEventRecordExternal), "event");
+        }
+    }
+    ck(cudaGetLastError(), "launch");
+}
+
+// Execute: the first call runs eagerly (kernel attributes, tensor maps) and
+// then captures the whole estimate into a CUDA graph; later calls launch it.
+void win_execute(Context& c, WinPlan& pl) {
+    if (!pl.graph) {
+        cudaGraph_t g = nullptr;
+        ck(cudaStreamBeginCapture(c.st, cudaStreamCaptureModeThreadLocal), "capture");
+        try {
+            win_enqueue(c, pl);
+        } catch (...) {
+            cudaStreamEndCapture(c.st, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        ck(cudaStreamEndCapture(c.st, &g), "capture end");
+        ck(cudaGraphInstantiate(&pl.graph, g, 0), "graph instantiate");
+        cudaGraphDestroy(g);
+    }
+    ck(cudaGraphLaunch(pl.graph, c.st), "graph launch");
+    pl.pending = 1;
+}
+
+void win_times(WinPlan& pl) {
+    if (!pl.pending) return;
+    ck(cudaEventSynchronize(pl.ev.back()), "event sync");
+    for (double& x : pl.kernel_ms) x = 0.0;
+    for (size_t i = 0; i + 1 < pl.ev.size(); ++i) {
+        float ms = 0.f;
+        ck(cudaEventElapsedTime(&ms, pl.ev[i], pl.ev[i + 1]), "elapsed");
+        // event order per (V-tile, batch): weights, phase 1, digits, phase 2
+        pl.kernel_ms[i % 4] += ms;
+    }
+    pl.pending = 0;
+}
+
+void win_results(Context& c, WinPlan& pl, double* ldscore, double* meansq_out, double* inv_out,
+                 double* mc_snp) {
+    const int64_t M = pl.P->g.M, K = pl.K, N = pl.P->g.N;
+    std::vector<double> acc((size_t)(M * K));
+    d2h(acc.data(), static_cast<double*>(pl.accum.p), acc.size(), c.st);
+    std::vector<double> mcv;
+    if (pl.with_mc && mc_snp) {
+        mcv.resize((size_t)(M * K));
+        d2h(mcv.data(), static_cast<double*>(pl.mc.p), mcv.size(), c.st);
+    }
+    unsigned st = 0;
+    d2h(&st, static_cast<unsigned*>(pl.status.p), 1, c.st);
+    ck(cudaStreamSynchronize(c.st), "results");
+    if (st) fail(LDS_ERR_CUDA, "tensor-core pipeline wait timed out (code %u)", st);
+    win_times(pl);
+    if (meansq_out) std::memcpy(meansq_out, acc.data(), sizeof(double) * acc.size());
+    if (inv_out) std::memcpy(inv_out, pl.inv.data(), sizeof(double) * (size_t)M);
+    const double nd = (double)(N - pl.P->ddof);
+    if (ldscore)
+        for (int64_t j = 0; j < M; ++j) {
+            const int64_t w = pl.win_of[(size_t)j];
+            for (int64_t k = 0; k < K; ++k)
+                ldscore[j * K + k] =
+                    acc[(size_t)(j * K + k)] / (double)pl.nvecs - pl.Mkw[(size_t)(w * K + k)] / nd;
+        }
+    if (mc_snp && !mcv.empty()) std::memcpy(mc_snp, mcv.data(), sizeof(double) * mcv.size());
+}
+
 void gw_ldscore_impl(const uint8_t* bed_rows, int64_t row_bytes, int64_t n_total, int64_t M,
                      const int64_t* row_sel, int64_t n_sel, const double* annot, int64_t K,
                      int nvecs, int step, int vtile, uint64_t seed, int dist, int ddof,
@@ -1545,6 +1903,71 @@ LDS_API int lds_set_p2_kernel(int impl) {
     p2_impl() = impl;
     return LDS_OK;
 }
+
+LDS_API int lds_win_plan_create(int64_t geno, const double* annot, int64_t K,
+                                const int64_t* window_starts, int64_t n_windows, int nvecs,
+                                int step_size, int vtile, uint64_t seed, int rand_dist,
+                                double resvar_eps, int as_float, int with_mc, double batch_gb,
+                                int64_t* plan_out) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        ensure_device(c);
+        auto it = geno_table().find(geno);
+        if (it == geno_table().end()) fail(LDS_ERR_ARG, "unknown genotype handle");
+        auto pl = win_plan_create(c, it->second, annot, K, window_starts, n_windows, nvecs,
+                                  step_size, vtile, seed, rand_dist, resvar_eps, as_float, with_mc,
+                                  batch_gb > 0 ? batch_gb : 8.0);
+        const int64_t h = next_handle();
+        win_table()[h] = std::move(pl);
+        *plan_out = h;
+    });
+}
+
+static WinPlan& win_of_handle(int64_t h) {
+    auto it = win_table().find(h);
+    if (it == win_table().end()) fail(LDS_ERR_ARG, "unknown windowed plan handle");
+    return *it->second;
+}
+
+LDS_API int lds_win_plan_execute(int64_t plan) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        win_execute(c, win_of_handle(plan));
+    });
+}
+
+LDS_API int lds_win_plan_results(int64_t plan, double* ldscore, double* meansq_accum,
+                                 double* inv_out, double* mc_per_snp_sumsq) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        win_results(c, win_of_handle(plan), ldscore, meansq_accum, inv_out, mc_per_snp_sumsq);
+    });
+}
+
+LDS_API int lds_win_plan_kernel_ms(int64_t plan, double* ms4) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        WinPlan& pl = win_of_handle(plan);
+        ck(cudaStreamSynchronize(c.st), "sync");
+        win_times(pl);
+        for (int i = 0; i < 4; ++i) ms4[i] = pl.kernel_ms[i];
+    });
+}
+
+LDS_API int lds_win_plan_destroy(int64_t plan) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        if (c.ready) ck(cudaStreamSynchronize(c.st), "sync");
+        win_table().erase(plan);
+    });
+}
+
+LDS_API uint64_t lds_window_seed(uint64_t root, int64_t w) { return window_seed(root, w); }
 
 LDS_API int lds_last_timings(double* ms_out, int n) {
     Context& c = ctx();

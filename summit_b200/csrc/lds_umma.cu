@@ -75,7 +75,18 @@ __global__ void __launch_bounds__(kThreads, 1)
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int k = blockIdx.y;
-    const int64_t jt0 = a.j0 + (int64_t)blockIdx.x * kBM;
+    int64_t jt0, jend;
+    int sb = 0;  // super-bin base of this tile's window
+    if (a.tiles) {
+        const int4 t = a.tiles[blockIdx.x];
+        jt0 = t.x;
+        jend = t.y;
+        sb = t.z;
+    } else {
+        jt0 = a.j0 + (int64_t)blockIdx.x * kBM;
+        jend = a.j1;
+    }
+    const int kb = sb + k;  // super-bin of this CTA
 
     if (tid == 0) {
         for (int s = 0; s < kPkStages; ++s) {
@@ -135,7 +146,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 if (*abort_flag) break;
                 const int g = it / a.nkt, kt = it % a.nkt;
                 mbar_expect_tx(&b_full[s], (uint32_t)(a.box_rows * kBK));
-                tma_load_2d(smem + lay.b_off(s), &tmB, kt * kBK, k * a.ncolp + g * 256, &b_full[s]);
+                tma_load_2d(smem + lay.b_off(s), &tmB, kt * kBK, kb * a.ncolp + g * 256, &b_full[s]);
             }
         }
     } else if (warp == 1) {
@@ -216,13 +227,13 @@ __global__ void __launch_bounds__(kThreads, 1)
                         (((long long)ro[4 * p] * 128 + ro[4 * p + 1]) * 128 + ro[4 * p + 2]) * 128 +
                         ro[4 * p + 3];
                     if (a.raw_g) {
-                        if (j < a.j1) {
+                        if (j < jend) {
                             a.raw_g[(j - a.out_row0) * a.V + v] = TG;
                             a.raw_o[(j - a.out_row0) * a.V + v] = TO;
                         }
                         continue;
                     }
-                    const double wv = sd * a.colscale[(int64_t)k * a.V + v] *
+                    const double wv = sd * a.colscale[(int64_t)kb * a.V + v] *
                                       ((double)TG - mu * (double)TO);
                     const double w2 = wv * wv;
                     run2 += w2;
@@ -232,7 +243,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             tc_fence_before();
             mbar_arrive(acc_empty);
         }
-        if (!*abort_flag && j < a.j1 && !a.raw_g) {
+        if (!*abort_flag && j < jend && !a.raw_g) {
             const double ls = a.left_scale[j];
             double upd = run2 * ls;
             const double seg = (double)a.V;
@@ -328,10 +339,15 @@ void launch_quantize_y4(const double* Y, int64_t N, int64_t N_pad, int K, int V,
 
 size_t p2_umma_smem_bytes(int box_rows) { return (size_t)Layout(box_rows).bytes() + 1024; }
 
+void prepare_p2_umma() {
+    cudaFuncSetAttribute(p2_umma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)p2_umma_smem_bytes(256));
+}
+
 void launch_p2_umma(const CUtensorMap& tmA, const CUtensorMap& tmB, const P2UArgs& a,
                     cudaStream_t st) {
     const int64_t rows = a.j1 - a.j0;
-    if (rows <= 0 || a.K <= 0) return;
+    if ((!a.tiles && rows <= 0) || a.K <= 0) return;
     const size_t smem = p2_umma_smem_bytes(a.box_rows);
     static size_t attr = 0;
     if (attr < smem) {
@@ -339,7 +355,8 @@ void launch_p2_umma(const CUtensorMap& tmA, const CUtensorMap& tmB, const P2UArg
                              (int)p2_umma_smem_bytes(256));
         attr = p2_umma_smem_bytes(256);
     }
-    dim3 grid((unsigned)((rows + kBM - 1) / kBM), (unsigned)a.K);
+    // With a tile table, j0 is unused and j1 - j0 carries the number of tiles.
+    dim3 grid((unsigned)(a.tiles ? rows : (rows + kBM - 1) / kBM), (unsigned)a.K);
     p2_umma_kernel<<<grid, kThreads, smem, st>>>(tmA, tmB, a);
     count_launch();
 }

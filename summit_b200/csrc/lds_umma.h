@@ -26,6 +26,10 @@ struct P2UArgs {
     // per (SNP, probe) to raw_g / raw_o ((j - out_row0) * V + v), no epilogue.
     long long* raw_g = nullptr;
     long long* raw_o = nullptr;
+    // Optional tile table (windowed estimates): CTA x processes rows
+    // [tiles[x].x, min(tiles[x].x + 128, tiles[x].y)) against super-bins
+    // tiles[x].z + k (sketch columns and scales of that window).
+    const int4* tiles = nullptr;
 };
 
 // Phase-1 tcgen05 kernel arguments.  Member lists of bin k occupy
@@ -63,6 +67,9 @@ inline int ncolp_for(int V) { return ((4 * V + 15) / 16) * 16; }
 void launch_quantize_y4(const double* Y, int64_t N, int64_t N_pad, int K, int V, int ncolp,
                         int8_t* Yq, double* colscale, cudaStream_t st);
 size_t p2_umma_smem_bytes(int box_rows);
+// Set the kernels' shared-memory attributes ahead of any stream capture.
+void prepare_p2_umma();
+void prepare_p1_umma();
 void launch_p2_umma(const CUtensorMap& tmA, const CUtensorMap& tmB, const P2UArgs& a,
                     cudaStream_t st);
 

@@ -271,6 +271,11 @@ void launch_p1_weights4(const P1UWeights& w, const double* mean, const double* s
 
 size_t p1_umma_smem_bytes() { return (size_t)p1::kStages * p1::kStageBytes + 1024 + 256; }
 
+void prepare_p1_umma() {
+    cudaFuncSetAttribute(p1_umma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)p1_umma_smem_bytes());
+}
+
 void launch_p1_umma(const CUtensorMap& tmW, const P1UArgs& a, int64_t N_pad, cudaStream_t st) {
     static bool attr = false;
     if (!attr) {
