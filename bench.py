@@ -1,12 +1,15 @@
 #!/usr/bin/env python3
-"""Benchmark of the genotype x probe hot path: genome-wide partitioned LD scores.
+"""Benchmark of the genotype x probe hot path: windowed + partitioned LD scores.
 
 Workload (one "step" = one complete estimate over one synthetic BED batch):
     N = 50,000 samples x M = 500,000 SNPs (HWE hard calls, AR(1) latent LD,
-    1% missing), K = 24 Bernoulli(0.1) annotations, B = 50 Rademacher probes,
-    SNP blocks of 1,000 (the reference's default --block-size), mean imputation.
+    1% missing), contiguous windows of 200-5,000 SNPs (log-uniform sizes),
+    K = 24 Bernoulli(0.1) annotations, B = 50 Rademacher probes, SNP blocks of
+    1,000 (the reference's default --block-size), mean imputation; all windows
+    in one CUDA-graph launch.  The genome-wide form of the same workload is
+    reported beside it (``genome_wide``).
 Metric: geno x probe TOPS = (2 N nnz(A) B  [phase 1]  +  2 N M K B  [phase 2]) / time,
-2 ops per multiply-accumulate.
+2 ops per multiply-accumulate (nnz over window x annotation members).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -42,13 +45,24 @@ BLOCK = 1_000
 DATA_SEED = 20260501
 ANNOT_SEED = 7
 PROBE_SEED = 12345
-METRIC = "geno x probe TOPS (genome-wide partitioned LD scores)"
-WORKLOAD = "gw_partitioned_ldscore_n50k_m500k_k24_b50_rademacher"
+WINDOW_SEED = 2025
+METRIC = "geno x probe TOPS (windowed + partitioned LD scores)"
+WORKLOAD = "windowed_partitioned_ldscore_n50k_m500k_w200-5000_k24_b50_rademacher"
 
 
 def annotations(m: int, k: int = K_BINS) -> np.ndarray:
     rng = np.random.default_rng(ANNOT_SEED)
     return (rng.random((m, k)) < 0.1).astype(np.float64)
+
+
+def windows(m: int, seed: int = WINDOW_SEED) -> np.ndarray:
+    """Contiguous window starts with log-uniform sizes in [200, 5000] (last may be shorter)."""
+    rng = np.random.default_rng(seed)
+    starts = [0]
+    while starts[-1] < m:
+        size = int(np.exp(rng.uniform(np.log(200.0), np.log(5000.0))))
+        starts.append(min(m, starts[-1] + size))
+    return np.asarray(starts, dtype=np.int64)
 
 
 def algorithmic_ops(n: int, annot: np.ndarray, b: int) -> tuple[float, float]:
@@ -136,6 +150,38 @@ def reference_sample(m_sample: int, tmpdir: str, packed=None) -> tuple[str, np.n
     return prefix, annotations(M_SNPS)[:m_sample]
 
 
+def run_reference_windows(packed: np.ndarray, annot: np.ndarray, ws: np.ndarray, threads: int,
+                          tmpdir: str) -> float:
+    """The reference's per-block native calls run window by window (each window
+    is the genome-wide estimator on its SNPs, probe root window_seed(seed, w));
+    returns seconds of reference compute."""
+    from oracle.oracle import Reference
+    from summit_b200 import bedfile
+    from summit_b200.bedfile import mix64
+
+    ref = Reference()
+    ref.set_threads(threads)
+    total = 0.0
+    sys.stderr.flush()
+    saved = os.dup(2)
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 2)
+    try:
+        for w in range(len(ws) - 1):
+            a, c = int(ws[w]), int(ws[w + 1])
+            pre = bedfile.write_plink(Path(tmpdir) / f"win{w}", packed=packed[a:c], n=N_SAMPLES)
+            seed_w = int(mix64(np.uint64(PROBE_SEED) ^ mix64(np.uint64(0x77696E646F77 + w))))
+            t0 = time.perf_counter()
+            ref.gw_ldscore(pre, N_SAMPLES, c - a, annot[a:c], B_PROBES, BLOCK, seed_w,
+                           dist="rademacher", impute="mean", dtype=np.float32)
+            total += time.perf_counter() - t0
+    finally:
+        os.dup2(saved, 2)
+        os.close(saved)
+        os.close(devnull)
+    return total
+
+
 def run_reference(prefix: str, annot: np.ndarray, threads: int) -> float:
     """One reference estimate (float32, the CLI default dtype); returns seconds.
 
@@ -179,6 +225,28 @@ def calibrated_reference(target_s: float, tmpdir: str, threads: int, packed=None
     return prefix, annot, m
 
 
+def reference_sample_windows(target_s: float, threads: int, tmpdir: str, packed=None):
+    """Leading windows of the workload totalling about target_s seconds of reference work."""
+    ws_all = windows(M_SNPS)
+    annot_all = annotations(M_SNPS)
+    # calibrate on the first window(s) covering >= 2000 SNPs
+    k = int(np.searchsorted(ws_all, 2000)) + 1
+    m_cal = int(ws_all[k])
+    if packed is None:
+        from oracle.oracle import Oracle
+
+        packed = Oracle().synth_bed_rows(N_SAMPLES, m_cal, DATA_SEED)
+    t = run_reference_windows(packed[:m_cal], annot_all, ws_all[:k + 1], threads, tmpdir)
+    m_target = min(M_SNPS, int(m_cal * target_s / max(t, 1e-3)))
+    k = max(1, int(np.searchsorted(ws_all, m_target)))
+    m_s = int(ws_all[k])
+    if packed.shape[0] < m_s:
+        from oracle.oracle import Oracle
+
+        packed = Oracle().synth_bed_rows(N_SAMPLES, m_s, DATA_SEED)
+    return packed[:m_s], annot_all[:m_s], ws_all[:k + 1]
+
+
 def reference_arm(args) -> None:
     rank = env_int("RANK", 0)
     if rank != 0:
@@ -186,25 +254,27 @@ def reference_arm(args) -> None:
     threads = cpu_threads()
     os.environ.setdefault("OMP_NUM_THREADS", str(threads))
     with tempfile.TemporaryDirectory() as td:
-        prefix, annot, m = calibrated_reference(float(os.environ.get("LDS_REF_STEP_S", "8")), td,
-                                                threads)
+        packed, annot, ws = reference_sample_windows(float(os.environ.get("LDS_REF_STEP_S", "8")),
+                                                     threads, td)
         ops = sum(algorithmic_ops(N_SAMPLES, annot, B_PROBES))
         for _ in range(args.warmup):
-            run_reference(prefix, annot, threads)
-        times = [run_reference(prefix, annot, threads) for _ in range(args.steps)]
+            run_reference_windows(packed, annot, ws, threads, td)
+        times = [run_reference_windows(packed, annot, ws, threads, td) for _ in range(args.steps)]
     from oracle.oracle import Reference
 
     sec = float(np.mean(times))
     value = ops / sec / 1e12
-    sample = (f"first {m} of {M_SNPS} SNPs, N={N_SAMPLES}, K={K_BINS}, B={B_PROBES}; "
-              "reference gwldcore.cpp+genotype.cpp compiled unchanged (float32 path), "
-              f"OpenMP+{Reference().blas_config().split()[0:2]}")
+    m = packed.shape[0]
+    sample = (f"first {len(ws) - 1} windows ({m} of {M_SNPS} SNPs), N={N_SAMPLES}, K={K_BINS}, "
+              f"B={B_PROBES}; reference gwldcore.cpp+genotype.cpp compiled unchanged (float32 "
+              f"path) run per window, OpenMP+{' '.join(Reference().blas_config().split()[0:2])}")
     line = {
         "impl": "reference", "metric": METRIC, "value": round(value, 6), "unit": "TOPS",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(sec * 1e3, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sample_snps": m, "l2": "inputs larger than L2"},
+        "config": {"workload": WORKLOAD, "sample_snps": m, "sample_windows": len(ws) - 1,
+                   "l2": "inputs larger than L2"},
         "cpu_baseline": {"value": round(value, 6), "unit": "TOPS", "cores": threads,
                          "kind": "reference", "sample": sample},
         "e2e": {"value": round(value, 6), "unit": "TOPS", "h2d_bytes_per_step": 0,
@@ -246,7 +316,7 @@ def ours_arm(args) -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
 
     from summit_b200 import _lib, gwldcore
-    from summit_b200.session import GwSession, set_stream
+    from summit_b200.session import GwSession, WinPlan, set_stream
 
     lib = _lib.load()
     stream = torch.cuda.Stream()
@@ -260,59 +330,85 @@ def ours_arm(args) -> None:
     bed_host = pinned.numpy()
     del bed
     annot = annotations(m)
+    ws = windows(m)
     ops1, ops2 = algorithmic_ops(n, annot, B_PROBES)
     ops = ops1 + ops2
-
-    sess = GwSession(bed_host, n, impute_mode="mean")
-    plan = sess.plan(annot, B_PROBES, BLOCK, PROBE_SEED, "rademacher")
 
     def barrier():
         if dist is not None:
             dist.barrier()
 
-    for _ in range(args.warmup):
-        plan.execute()
-    torch.cuda.synchronize()
-    plan.kernel_ms()  # drop warm-up kernel times
-
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    launches0 = lib.lds_kernel_launches()
-    with Clocks(local) as clk:
+    def timed(execute, steps):
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
         barrier()
         torch.cuda.synchronize()
         ev0.record(stream)
-        for _ in range(args.steps):
-            plan.execute()
+        for _ in range(steps):
+            execute()
         ev1.record(stream)
         torch.cuda.synchronize()
         barrier()
-    launches = int(lib.lds_kernel_launches() - launches0)
-    ms = ev0.elapsed_time(ev1) / args.steps
-    kms = plan.kernel_ms()
-    res = plan.results()
-    assert np.isfinite(res["ldscore"]).all()
+        return ev0.elapsed_time(ev1) / steps
 
-    # End to end through the C ABI from pinned host buffers.
+    sess = GwSession(bed_host, n, impute_mode="mean")
+
+    # ---- headline: windowed + partitioned, one graph launch per estimate ----
+    wplan = WinPlan(sess, annot, ws, B_PROBES, BLOCK, PROBE_SEED, "rademacher")
+    for _ in range(args.warmup):
+        wplan.execute()
+    torch.cuda.synchronize()
+    wplan.kernel_ms()
+    launches0 = lib.lds_kernel_launches()
+    with Clocks(local) as clk:
+        ms = timed(wplan.execute, args.steps)
+    launches = int(lib.lds_kernel_launches() - launches0)
+    kms = wplan.kernel_ms()  # last estimate, per kernel kind (events inside the graph)
+    res = wplan.results()
+    assert np.isfinite(res["ldscore"]).all()
+    # graph launches run kernels the launch counter does not see: count them per graph
+    wplan.close()
+
+    # ---- secondary: genome-wide form of the same workload ----
+    plan = sess.plan(annot, B_PROBES, BLOCK, PROBE_SEED, "rademacher")
+    for _ in range(args.warmup):
+        plan.execute()
+    torch.cuda.synchronize()
+    plan.kernel_ms()
+    gw_ms = timed(plan.execute, args.steps)
+    gw_kms = plan.kernel_ms()
+    plan.close()
+
+    # ---- end to end through the C ABI from pinned host buffers ----
+    def e2e_once():
+        s2 = GwSession(bed_host, n, impute_mode="mean")
+        p2 = WinPlan(s2, annot, ws, B_PROBES, BLOCK, PROBE_SEED, "rademacher")
+        p2.execute()
+        out = p2.results()
+        p2.close()
+        s2.close()
+        return out
+
     e2e_steps = max(1, min(args.steps, env_int("LDS_E2E_STEPS", 2)))
-    gwldcore.gw_ldscore(bed_host, n, annot, B_PROBES, BLOCK, PROBE_SEED)  # warm
+    e2e_once()  # warm
     torch.cuda.synchronize()
     barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        out = gwldcore.gw_ldscore(bed_host, n, annot, B_PROBES, BLOCK, PROBE_SEED)
+        out = e2e_once()
     torch.cuda.synchronize()
     e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
     barrier()
-    assert np.isfinite(out["ldscore"]).all()
+    assert np.allclose(out["ldscore"], res["ldscore"], rtol=0, atol=0)
     nnz = int((annot > 0).sum())
-    h2d = int(bed_host.nbytes + m * B_PROBES * 8 + nnz * 12 + m * 8)
+    h2d = int(bed_host.nbytes + m * B_PROBES * 8 + nnz * 12 + m * 8 + ws.nbytes)
     d2h = int(m * K_BINS * 8)
+    sess.close()
 
-    t = torch.tensor([ms, e2e_ms], dtype=torch.float64, device="cuda")
+    t = torch.tensor([ms, e2e_ms, gw_ms], dtype=torch.float64, device="cuda")
     if dist is not None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms, e2e_ms = float(t[0]), float(t[1])
+    ms, e2e_ms, gw_ms = float(t[0]), float(t[1]), float(t[2])
 
     if rank == 0:
         peaks = {}
@@ -330,13 +426,17 @@ def ours_arm(args) -> None:
             "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int8-digit exact products, f64 epilogue",
             "data": "synthetic (seeded HWE/AR(1) generator on device)",
-            "config": {"workload": WORKLOAD, "N": n, "M": m, "K": K_BINS, "B": B_PROBES,
-                       "block": BLOCK, "impute": "mean", "digits": lib.lds_get_slices(),
-                       "parallelism": f"replicas x{world}",
+            "config": {"workload": WORKLOAD, "N": n, "M": m, "windows": int(len(ws) - 1),
+                       "K": K_BINS, "B": B_PROBES, "block": BLOCK, "impute": "mean",
+                       "digits": lib.lds_get_slices(), "parallelism": f"replicas x{world}",
+                       "graph": "one CUDA graph launch per estimate",
                        "l2": "inputs larger than L2 (6.3 GB genotype image per step)"},
             "kernel_ms": {k: round(v, 3) for k, v in kms.items()},
+            "genome_wide": {"value": round(world * ops / (gw_ms * 1e-3) / 1e12, 3),
+                            "unit": "TOPS", "ms_per_step": round(gw_ms, 3),
+                            "kernel_ms": {k: round(v, 3) for k, v in gw_kms.items()}},
             "roofline": {
-                "kernel": "p2_kernel (phase 2: X^T Y + LD epilogue)", "bound": "tensor",
+                "kernel": "p2_umma_kernel (phase 2: X^T Y + LD epilogue)", "bound": "tensor",
                 "achieved": None if achieved is None else round(achieved, 3),
                 "peak": peak, "unit": "TFLOP/s",
                 "frac": None if achieved is None else round(achieved / peak, 4),
@@ -352,20 +452,18 @@ def ours_arm(args) -> None:
         if world == 1 and not os.environ.get("LDS_SKIP_CPU_BASELINE"):
             threads = cpu_threads()
             with tempfile.TemporaryDirectory() as td:
-                prefix, ann_s, ms_snps = calibrated_reference(
-                    float(os.environ.get("LDS_CPU_BASELINE_S", "12")), td, threads, bed_host)
-                sec = run_reference(prefix, ann_s, threads)
+                pk, ann_s, ws_s = reference_sample_windows(
+                    float(os.environ.get("LDS_CPU_BASELINE_S", "12")), threads, td, bed_host)
+                sec = run_reference_windows(pk, ann_s, ws_s, threads, td)
             cops = sum(algorithmic_ops(n, ann_s, B_PROBES))
             line["cpu_baseline"] = {
                 "value": round(cops / sec / 1e12, 6), "unit": "TOPS", "cores": threads,
                 "kind": "reference",
-                "sample": f"first {ms_snps} SNPs of the workload (N={n}, K={K_BINS}, "
-                          f"B={B_PROBES}); reference gwldcore.cpp compiled unchanged, float32, "
-                          f"{sec:.1f} s"}
+                "sample": f"first {len(ws_s) - 1} windows ({pk.shape[0]} SNPs) of the workload "
+                          f"(N={n}, K={K_BINS}, B={B_PROBES}); reference gwldcore.cpp compiled "
+                          f"unchanged, float32, run per window, {sec:.1f} s"}
         print(json.dumps(line), flush=True)
 
-    plan.close()
-    sess.close()
     set_stream(None)
     if dist is not None:
         dist.destroy_process_group()

@@ -207,7 +207,7 @@ int lds_gw_plan_destroy(int64_t plan);
  * on the window's SNPs with that seed.  All windows run as batched phase-1
  * super-bins and a tile-table phase 2; the first execute captures the whole
  * estimate into one CUDA graph and later executes launch that graph.
- * batch_gb bounds the FP64 sketch of one window batch (<= 0: 8 GB).
+ * batch_gb bounds the int8 sketch digits of one window batch (<= 0: 8 GB).
  * No single reference counterpart: the reference's windowed scores are
  * exact (winldcore.cpp:783-931); this is the probe estimator of
  * gw_ldscore.py:1753-2222 applied per window.

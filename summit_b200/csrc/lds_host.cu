@@ -1238,12 +1238,13 @@ struct WinPlan {
     };
     std::vector<Batch> batches;
     std::vector<DevBuf> z;              // per V-tile, M x V FP64 probes
-    DevBuf y, yq, ycs, wq, wcs, accum, mc, lscale, guards, status;
+    DevBuf y, yq, ycs, yshift, wq, wcs, accum, mc, lscale, guards, status;
     CUtensorMap tmA;
     std::vector<cudaEvent_t> ev;        // start, after phase 1 of each launch group, end
     double kernel_ms[4] = {0, 0, 0, 0};
     int pending = 0;
     cudaGraphExec_t graph = nullptr;
+    unsigned long long graph_kernels = 0;  // kernel nodes in the captured graph
     ~WinPlan() {
         for (cudaEvent_t e : ev) cudaEventDestroy(e);
         if (graph) cudaGraphExecDestroy(graph);
@@ -1300,8 +1301,8 @@ std::unique_ptr<WinPlan> win_plan_create(Context& c, std::shared_ptr<Prepared> P
         ls[(size_t)j] = (std::isfinite(v) && v > 0.0) ? v * v * inv_denom2 : 0.0;
     }
     h2d(pl->lscale.as<double>((size_t)M), ls.data(), (size_t)M, c.st);
-    // Window batches: the FP64 sketch of a batch stays under batch_gb.
-    const double per_window = (double)Np * (double)K * vmax * 8.0;
+    // Window batches: the sketch digits of a batch stay under batch_gb.
+    const double per_window = (double)Np * (double)K * umma::ncolp_for(vmax);
     const int64_t wb = std::max<int64_t>(1, (int64_t)(batch_gb * 1e9 / per_window));
     std::vector<float> annot_f, inv_f;
     if (as_float) {
@@ -1383,9 +1384,9 @@ std::unique_ptr<WinPlan> win_plan_create(Context& c, std::shared_ptr<Prepared> P
         ck(cudaStreamSynchronize(c.st), "probe upload");
         v0 += V;
     }
-    pl->y.as<double>((size_t)(Np * max_ksup * vmax));
     pl->yq.as<int8_t>((size_t)(max_ksup * ncmax * Np));
     pl->ycs.as<double>((size_t)(max_ksup * vmax));
+    pl->yshift.as<int>((size_t)(max_ksup * vmax));
     int8_t* wq = pl->wq.as<int8_t>((size_t)std::max<int64_t>(max_wq, 16));
     (void)wq;
     pl->wcs.as<double>((size_t)(max_ksup * vmax));
@@ -1415,6 +1416,8 @@ void win_enqueue(Context& c, WinPlan& pl) {
     for (size_t ti = 0; ti < pl.vt.size(); ++ti) {
         const int V = pl.vt[ti];
         const int nc = umma::ncolp_for(V);
+        // Phase 1 writes every digit row of every super-bin of a batch, the
+        // padding rows 4V..ncolp included (as zeros), so the buffer needs no clearing.
         for (auto& b : pl.batches) {
             umma::P1UWeights uw;
             uw.K = (int)b.ksup;
@@ -1426,6 +1429,8 @@ void win_enqueue(Context& c, WinPlan& pl) {
             uw.bin_off = static_cast<int64_t*>(b.binoff.p);
             uw.wq = static_cast<int8_t*>(pl.wq.p);
             uw.colscale = static_cast<double*>(pl.wcs.p);
+            uw.ycolscale = static_cast<double*>(pl.ycs.p);
+            uw.yshift = static_cast<int*>(pl.yshift.p);
             const size_t wbytes = (size_t)(b.ksup * 2 * nc) * (size_t)b.lmax;
             ck(cudaMemsetAsync(pl.wq.p, 0, wbytes, c.st), "memset weights");
             umma::launch_p1_weights4(uw, static_cast<double*>(P.d_mean.p),
@@ -1447,13 +1452,20 @@ void win_enqueue(Context& c, WinPlan& pl) {
             pa.rowind = uw.rowind;
             pa.codes = P.g.codes;
             pa.colscale = uw.colscale;
-            pa.Y = static_cast<double*>(pl.y.p);
+            pa.Y = nullptr;
             pa.status = static_cast<unsigned*>(pl.status.p);
+            static const int spc = [] {
+                const char* e = std::getenv("LDS_P1_SB_PER_CTA");
+                const int v = e ? std::atoi(e) : 0;
+                return v > 0 ? v : 8;
+            }();
+            pa.sb_per_cta = spc;
+            pa.yq = static_cast<int8_t*>(pl.yq.p);
+            pa.ycolscale = static_cast<double*>(pl.ycs.p);
+            pa.yshift = static_cast<int*>(pl.yshift.p);
             umma::launch_p1_umma(tmW, pa, Np, c.st);
             ck(cudaEventRecordWithFlags(pl.ev[(size_t)e++], c.st, cudaEventRecordExternal), "event");
-            umma::launch_quantize_y4(static_cast<double*>(pl.y.p), P.g.N, Np, (int)b.ksup, V, nc,
-                                     static_cast<int8_t*>(pl.yq.p), static_cast<double*>(pl.ycs.p),
-                                     c.st);
+            // (sketch digits were written by phase 1's epilogue)
             ck(cudaEventRecordWithFlags(pl.ev[(size_t)e++], c.st, cudaEventRecordExternal), "event");
             const CUtensorMap tmB =
                 make_map_2d(pl.yq.p, (uint64_t)Np, (uint64_t)(b.ksup * nc), (uint64_t)Np, 128,
@@ -1492,6 +1504,7 @@ void win_enqueue(Context& c, WinPlan& pl) {
 void win_execute(Context& c, WinPlan& pl) {
     if (!pl.graph) {
         cudaGraph_t g = nullptr;
+        const unsigned long long l0 = g_launches.load();
         ck(cudaStreamBeginCapture(c.st, cudaStreamCaptureModeThreadLocal), "capture");
         try {
             win_enqueue(c, pl);
@@ -1503,8 +1516,12 @@ void win_execute(Context& c, WinPlan& pl) {
         ck(cudaStreamEndCapture(c.st, &g), "capture end");
         ck(cudaGraphInstantiate(&pl.graph, g, 0), "graph instantiate");
         cudaGraphDestroy(g);
+        // Captured launches did not run; count them when the graph does.
+        pl.graph_kernels = g_launches.load() - l0;
+        g_launches.fetch_sub(pl.graph_kernels);
     }
     ck(cudaGraphLaunch(pl.graph, c.st), "graph launch");
+    g_launches.fetch_add(pl.graph_kernels);
     pl.pending = 1;
 }
 

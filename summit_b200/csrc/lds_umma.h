@@ -44,6 +44,13 @@ struct P1UArgs {
     const double* colscale = nullptr;   // K*V
     double* Y = nullptr;                // N_pad x (K*V), column (k*V+v)
     unsigned int* status = nullptr;
+    int sb_per_cta = 1;                 // super-bins processed by one CTA (pipeline continues)
+    // Digit output (windowed estimates): when yq is set the epilogue writes the
+    // sketch's 4 int8 digits in phase 2's layout (column k*ncolp + 4v + t)
+    // using the a-priori exponents in ycolscale (K*V) instead of FP64 Y.
+    int8_t* yq = nullptr;
+    const double* ycolscale = nullptr;
+    const int* yshift = nullptr;        // K*V digit shifts eW - eY (from the weight kernel)
 };
 
 struct P1UWeights {
@@ -54,6 +61,8 @@ struct P1UWeights {
     const int64_t* bin_off = nullptr;
     int8_t* wq = nullptr;
     double* colscale = nullptr;
+    double* ycolscale = nullptr;        // optional: a-priori sketch digit scales (K*V)
+    int* yshift = nullptr;              // with ycolscale: digit shifts eW - eY (K*V)
 };
 
 void launch_p1_weights4(const P1UWeights& w, const double* mean, const double* sdinv,

@@ -9,10 +9,13 @@
 // TMA, SWIZZLE_128B, K-major) into ONE accumulator, so TMEM holds
 // G.W1 - O.W2 = sum_j (g - mu_j o) s_j sc z directly.
 //
-// Roles (192 threads): warp 0 TMA producer for the digit tiles; warp 1 TMEM
+// Roles (320 threads): warp 0 TMA producer for the digit tiles; warp 1 TMEM
 // allocation and the single MMA-issuing thread; warps 2-5 gather the member
-// SNPs' packed bytes from global memory (one row each, prefetched one stage
-// ahead), decode them into the operand tiles, and run the epilogue.
+// SNPs' packed bytes from global memory (one row each, kept several stages
+// ahead by cp.async) and decode them into the operand tiles; warps 6-9 read the
+// accumulator out.  Two TMEM accumulators let the MMAs of the next job (super-bin,
+// column group) run while the epilogue of the previous one drains, which
+// matters for windowed estimates, whose super-bins are a few K-steps long.
 #include <cstdint>
 #include <cstdio>
 
@@ -30,8 +33,12 @@ constexpr int kBK = 128;          // member SNPs per stage
 constexpr int kATile = 128 * 128; // 16 KB
 constexpr int kWTile = 256 * 128; // 32 KB (max digit columns per pass)
 constexpr int kStageBytes = 2 * kATile + 2 * kWTile;  // 96 KB
-constexpr int kThreads = 192;
-constexpr uint32_t kTmemCols = 256;
+constexpr int kThreads = 448;
+constexpr int kEpiThreads = 256;         // warps 6..13: two per TMEM lane quadrant
+constexpr int kAccCols = 256;            // one accumulator: <= 256 digit columns
+constexpr uint32_t kTmemCols = 512;      // two accumulators (MMA of job j+1 || epilogue of j)
+constexpr int kRing = 8;                 // gathered packed rows in flight per decoder thread
+constexpr int kRingSlot = 128 * 32;      // 128 member rows x 32 bytes
 }  // namespace p1
 
 __global__ void __launch_bounds__(p1::kThreads, 1)
@@ -40,20 +47,22 @@ __global__ void __launch_bounds__(p1::kThreads, 1)
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
-    uint64_t* full_w = bars;
-    uint64_t* full_dec = bars + kStages;
-    uint64_t* empty = bars + 2 * kStages;
-    uint64_t* acc_full = bars + 3 * kStages;
-    uint64_t* acc_empty = bars + 3 * kStages + 1;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 3 * kStages + 2);
+    uint8_t* ring = smem + kStages * kStageBytes;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(ring + kRing * kRingSlot);
+    uint64_t* full_w = bars;                    // [kStages] weight tiles landed (TMA)
+    uint64_t* full_dec = bars + kStages;        // [kStages] genotype tiles decoded
+    uint64_t* empty = bars + 2 * kStages;       // [kStages] stage consumed by the MMAs
+    uint64_t* acc_full = bars + 3 * kStages;    // [2] accumulator b holds a finished job
+    uint64_t* acc_empty = acc_full + 2;         // [2] accumulator b read out
+    uint64_t* mma_done = acc_empty + 2;         // drain of the issuer's MMAs
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mma_done + 1);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int k = blockIdx.y;
     const int64_t i0 = (int64_t)blockIdx.x * kBM;
-    const int64_t r0 = a.bin_off[k];
-    const int nkt = (int)((a.bin_off[k + 1] - r0) / kBK);
+    // This CTA's super-bins: [kb0, kb1); a job is one (super-bin, column group).
+    const int kb0 = blockIdx.y * a.sb_per_cta;
+    const int kb1 = min(a.K, kb0 + a.sb_per_cta);
 
     if (tid == 0) {
         for (int s = 0; s < kStages; ++s) {
@@ -61,8 +70,11 @@ __global__ void __launch_bounds__(p1::kThreads, 1)
             mbar_init(&full_dec[s], 128);
             mbar_init(&empty[s], 1);
         }
-        mbar_init(acc_full, 1);
-        mbar_init(acc_empty, 128);
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&acc_full[b], 1);
+            mbar_init(&acc_empty[b], kEpiThreads);
+        }
+        mbar_init(mma_done, 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -80,11 +92,14 @@ __global__ void __launch_bounds__(p1::kThreads, 1)
         atomicCAS(a.status, 0u, (unsigned)code);
         *abort_flag = 1;
     };
+    auto nkt_of = [&](int k) { return (int)((a.bin_off[k + 1] - a.bin_off[k]) / kBK); };
 
-    if (nkt > 0) {
-        if (warp == 0) {
-            if (lane == 0) {
-                int it = 0;
+    if (warp == 0) {
+        // ---------------- TMA producer of weight-digit tiles ----------------
+        if (lane == 0) {
+            int it = 0;
+            for (int k = kb0; k < kb1 && !*abort_flag; ++k) {
+                const int nkt = nkt_of(k);
                 for (int g = 0; g < a.ngroups && !*abort_flag; ++g) {
                     for (int kt = 0; kt < nkt; ++kt, ++it) {
                         const int s = it % kStages;
@@ -100,13 +115,24 @@ __global__ void __launch_bounds__(p1::kThreads, 1)
                     }
                 }
             }
-        } else if (warp == 1) {
-            if (lane == 0) {
-                int it = 0;
-                for (int g = 0; g < a.ngroups && !*abort_flag; ++g) {
-                    const int ncols = min(256, a.ncolp - g * 256);
+            // Drain: no tile copy may still be landing when the CTA exits
+            // (only reachable with copies outstanding after an abort).
+            for (int j = max(0, it - kStages); j < it; ++j)
+                mbar_wait(&full_w[j % kStages], (uint32_t)(j / kStages) & 1u);
+        }
+    } else if (warp == 1) {
+        // ---------------- MMA issuer ----------------
+        if (lane == 0) {
+            int it = 0, au = 0;  // stage counter, jobs (accumulator uses)
+            for (int k = kb0; k < kb1 && !*abort_flag; ++k) {
+                const int nkt = nkt_of(k);
+                if (nkt == 0) continue;
+                for (int g = 0; g < a.ngroups && !*abort_flag; ++g, ++au) {
+                    const int b = au & 1, u = au >> 1;
+                    const int ncols = min(kAccCols, a.ncolp - g * 256);
                     const uint32_t idesc = idesc_i8_amn(kBM, ncols);
-                    if (g > 0 && !mbar_wait(acc_empty, (uint32_t)(g - 1) & 1u)) { fail(12); break; }
+                    const uint32_t acc = tmem + (uint32_t)(b * kAccCols);
+                    if (u > 0 && !mbar_wait(&acc_empty[b], (uint32_t)(u - 1) & 1u)) { fail(12); break; }
                     tc_fence_after();
                     for (int kt = 0; kt < nkt; ++kt, ++it) {
                         const int s = it % kStages;
@@ -125,38 +151,54 @@ __global__ void __launch_bounds__(p1::kThreads, 1)
 #pragma unroll
                         for (int kk = 0; kk < kBK / 32; ++kk) {
                             // A advances 32 K-rows = 4 swizzle atoms (4 KB); B advances 32 bytes.
-                            umma_i8(tmem, dG + 256 * kk, dW1 + 2 * kk, idesc, (kt | kk) ? 1u : 0u);
-                            umma_i8(tmem, dO + 256 * kk, dW2 + 2 * kk, idesc, 1u);
+                            umma_i8(acc, dG + 256 * kk, dW1 + 2 * kk, idesc, (kt | kk) ? 1u : 0u);
+                            umma_i8(acc, dO + 256 * kk, dW2 + 2 * kk, idesc, 1u);
                         }
                         umma_commit(&empty[s]);
                     }
-                    umma_commit(acc_full);
+                    umma_commit(&acc_full[b]);
                 }
             }
-        } else {
-            // Decoders: thread t handles member row t of every stage.
-            const int t = tid - 64;
-            const int q = warp & 3;
-            const uint8_t* codes = a.codes + i0 / 4;
-            int it = 0;
-            for (int g = 0; g < a.ngroups && !*abort_flag; ++g) {
-                const int32_t* ri = a.rowind + r0;
-                uint4 c0, c1;
-                {
-                    const uint4* src = reinterpret_cast<const uint4*>(codes + (int64_t)ri[t] * a.nbp);
-                    c0 = __ldg(src);
-                    c1 = __ldg(src + 1);
+            // Drain: every MMA issued here completes before TMEM is released.
+            umma_commit(mma_done);
+            mbar_wait(mma_done, 0u);
+        }
+    } else if (warp < 6) {
+        // ---------------- gather + decode (warps 2..5) ----------------
+        const int t = tid - 64;
+        const uint8_t* codes = a.codes + i0 / 4;
+        // Gather prefetcher: walks the same (super-bin, group, K-step) sequence
+        // kRing steps ahead, copying this thread's member row into a ring slot.
+        int pk = kb0, pg = 0, pkt = 0, pit = 0;
+        auto prefetch_one = [&]() {
+            while (pk < kb1 && nkt_of(pk) == 0) { ++pk; pg = 0; pkt = 0; }
+            if (pk < kb1) {
+                const int64_t row = a.rowind[a.bin_off[pk] + (int64_t)pkt * kBK + t];
+                const uint8_t* src = codes + row * a.nbp;
+                uint8_t* dst = ring + (pit % kRing) * kRingSlot + t * 32;
+                cp_async16(dst, src);
+                cp_async16(dst + 16, src + 16);
+                if (++pkt == nkt_of(pk)) {
+                    pkt = 0;
+                    if (++pg == a.ngroups) { pg = 0; ++pk; }
                 }
+            }
+            cp_async_commit();
+            ++pit;
+        };
+        for (int d = 0; d < kRing - 1; ++d) prefetch_one();
+        int it = 0;
+        for (int k = kb0; k < kb1 && !*abort_flag; ++k) {
+            const int nkt = nkt_of(k);
+            for (int g = 0; g < a.ngroups && nkt > 0 && !*abort_flag; ++g) {
                 for (int kt = 0; kt < nkt; ++kt, ++it) {
                     const int s = it % kStages;
                     const uint32_t ph = (uint32_t)(it / kStages) & 1u;
-                    uint4 n0 = c0, n1 = c1;
-                    if (kt + 1 < nkt) {
-                        const uint4* src = reinterpret_cast<const uint4*>(
-                            codes + (int64_t)ri[(kt + 1) * kBK + t] * a.nbp);
-                        n0 = __ldg(src);
-                        n1 = __ldg(src + 1);
-                    }
+                    prefetch_one();  // step it + kRing - 1
+                    asm volatile("cp.async.wait_group %0;\n" ::"n"(kRing - 1));
+                    const uint4* src =
+                        reinterpret_cast<const uint4*>(ring + (it % kRing) * kRingSlot + t * 32);
+                    const uint4 c0 = src[0], c1 = src[1];
                     if (it >= kStages && !mbar_wait(&empty[s], ph ^ 1u)) { fail(14); break; }
                     if (*abort_flag) break;
                     uint8_t* st = smem + s * kStageBytes;
@@ -164,39 +206,121 @@ __global__ void __launch_bounds__(p1::kThreads, 1)
                     decode_row_sw128(c0, c1, gRow, gRow + kATile, t);
                     fence_async_smem();
                     mbar_arrive(&full_dec[s]);
-                    c0 = n0;
-                    c1 = n1;
                 }
-                if (*abort_flag) break;
-                if (!mbar_wait(acc_full, (uint32_t)g & 1u)) { fail(15); break; }
+            }
+        }
+        cp_async_wait_all();  // no gather copy may outlive the CTA (abort path)
+    } else {
+        // ---------------- epilogue (warps 6..13) ----------------
+        const int e = tid - 192;
+        const int q = warp & 3;                  // TMEM lane quadrant of this warp
+        const int h = (warp - 6) >> 2;           // which half of the 32-column chunks
+        const int64_t i = i0 + q * 32 + lane;    // sample row of this thread's accumulator lane
+        int au = 0;
+        for (int k = kb0; k < kb1 && !*abort_flag; ++k) {
+            const int nkt = nkt_of(k);
+            if (a.yq) {
+                // Digit padding rows 4V..ncolp of this tile read as zero in phase 2.
+                for (int idx = e; idx < (a.ncolp - 4 * a.V) * 8; idx += kEpiThreads) {
+                    const int c = 4 * a.V + (idx >> 3);
+                    *reinterpret_cast<uint4*>(a.yq + ((int64_t)k * a.ncolp + c) * a.N_pad + i0 +
+                                              (idx & 7) * 16) = make_uint4(0, 0, 0, 0);
+                }
+            }
+            if (nkt == 0) {
+                // Bin without members: its sketch columns are zero (the
+                // reference's untouched-bin zeroing, gw_ldscore.py:2017-2019).
+                if (a.yq) {
+                    for (int idx = e; idx < 4 * a.V * 8; idx += kEpiThreads)
+                        *reinterpret_cast<uint4*>(a.yq + ((int64_t)k * a.ncolp + (idx >> 3)) * a.N_pad +
+                                                  i0 + (idx & 7) * 16) = make_uint4(0, 0, 0, 0);
+                } else {
+                    for (int idx = e; idx < a.V * 64; idx += kEpiThreads)
+                        *reinterpret_cast<uint4*>(a.Y + ((int64_t)k * a.V + (idx >> 6)) * a.N_pad +
+                                                  i0 + (idx & 63) * 2) = make_uint4(0, 0, 0, 0);
+                }
+                continue;
+            }
+            for (int g = 0; g < a.ngroups && !*abort_flag; ++g, ++au) {
+                const int b = au & 1, u = au >> 1;
+                // This group's 64 per-probe shifts (or scales), two per lane, loaded
+                // before the accumulator wait so the loads overlap the MMAs; the
+                // loop below broadcasts them with shuffles (warp-local, no barrier).
+                int shA = 0, shB = 0;
+                double scA = 0.0, scB = 0.0;
+                {
+                    const int va = g * 64 + lane, vb = va + 32;
+                    const int64_t o = (int64_t)k * a.V;
+                    if (a.yq) {
+                        if (va < a.V) shA = a.yshift[o + va];
+                        if (vb < a.V) shB = a.yshift[o + vb];
+                    } else {
+                        if (va < a.V) scA = a.colscale[o + va];
+                        if (vb < a.V) scB = a.colscale[o + vb];
+                    }
+                }
+                if (!mbar_wait(&acc_full[b], (uint32_t)u & 1u)) { fail(15); break; }
                 tc_fence_after();
-                const int ncols = min(256, a.ncolp - g * 256);
-                const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16);
-                const int64_t i = i0 + q * 32 + lane;
-                for (int c0c = 0; c0c < ncols; c0c += 32) {
+                const int ncols = min(kAccCols, a.ncolp - g * 256);
+                const uint32_t tbase = tmem + (uint32_t)(b * kAccCols) + ((uint32_t)(q * 32) << 16);
+                for (int c0c = 32 * h; c0c < ncols; c0c += 64) {
                     int rr[32];
                     tmem_ld32(tbase + (uint32_t)c0c, rr);
                     tmem_wait_ld();
 #pragma unroll
                     for (int p = 0; p < 8; ++p) {
-                        const int v = g * 64 + c0c / 4 + p;
+                        const int vl = c0c / 4 + p;  // probe within the group (warp-uniform)
+                        const int v = g * 64 + vl;
                         if (v >= a.V) continue;
                         const long long T =
                             (((long long)rr[4 * p] * 128 + rr[4 * p + 1]) * 128 + rr[4 * p + 2]) *
                                 128 + rr[4 * p + 3];
-                        a.Y[((int64_t)k * a.V + v) * a.N_pad + i] =
-                            a.colscale[(int64_t)k * a.V + v] * (double)T;
+                        if (a.yq) {
+                            // Digits straight into phase 2's operand layout.  With
+                            // y = T 2^(eW-28) and the column exponent eY fixed in
+                            // advance by a bound on |y|, the sketch's 28-bit value is
+                            // R = rint(T 2^(eW-eY)) (round half to even); its
+                            // balanced base-128 digits are exact integer work.
+                            const int sh = __shfl_sync(0xffffffffu, vl < 32 ? shA : shB, vl & 31);
+                            long long R;
+                            if (sh >= 0) {
+                                R = T << sh;
+                            } else {
+                                const int r = -sh;
+                                R = (T + ((1LL << (r - 1)) - 1) + ((T >> r) & 1)) >> r;
+                            }
+                            // |R| < 2^28 (the bound fixed eY), so 32 bits suffice: with
+                            // U = R + 63 (2^14 + 2^7 + 1) the low three base-128 digits
+                            // of U are the balanced digits d1..d3 (in [-63, 64]) plus 63
+                            // and U >> 21 is d0.
+                            const int U = (int)R + 63 * (16384 + 128 + 1);
+                            uint32_t w = (uint32_t)(U >> 21) & 0xFFu;
+                            w |= ((uint32_t)(U >> 14) & 127u) << 8;
+                            w |= ((uint32_t)(U >> 7) & 127u) << 16;
+                            w |= ((uint32_t)U & 127u) << 24;
+                            w = __vsub4(w, 0x3F3F3F00u);
+                            // Quad transpose: lane 4g+p ends with digit p of samples 4g..4g+3.
+                            const int qb = lane & ~3, p4 = lane & 3;
+                            const uint32_t w0 = __shfl_sync(0xffffffffu, w, qb + 0);
+                            const uint32_t w1 = __shfl_sync(0xffffffffu, w, qb + 1);
+                            const uint32_t w2 = __shfl_sync(0xffffffffu, w, qb + 2);
+                            const uint32_t w3 = __shfl_sync(0xffffffffu, w, qb + 3);
+                            uint32_t c0, c1, c2, c3;
+                            transpose4x4(w0, w1, w2, w3, c0, c1, c2, c3);
+                            const uint32_t uu = p4 == 0 ? c0 : p4 == 1 ? c1 : p4 == 2 ? c2 : c3;
+                            // first sample of the quad is i - p4 (4-byte aligned)
+                            *reinterpret_cast<uint32_t*>(
+                                a.yq + ((int64_t)k * a.ncolp + 4 * v + p4) * a.N_pad + (i - p4)) = uu;
+                        } else {
+                            const double sc = __shfl_sync(0xffffffffu, vl < 32 ? scA : scB, vl & 31);
+                            a.Y[((int64_t)k * a.V + v) * a.N_pad + i] = sc * (double)T;
+                        }
                     }
                 }
                 tc_fence_before();
-                mbar_arrive(acc_empty);
+                mbar_arrive(&acc_empty[b]);
             }
         }
-    } else if (warp >= 2) {
-        // Bin without members: its sketch columns are zero (the reference's
-        // untouched-bin zeroing, gw_ldscore.py:2017-2019).
-        const int64_t i = i0 + (tid - 64);
-        for (int v = 0; v < a.V; ++v) a.Y[((int64_t)k * a.V + v) * a.N_pad + i] = 0.0;
     }
     tc_fence_before();
     __syncthreads();
@@ -260,6 +384,39 @@ __global__ void p1_weights4_kernel(P1UWeights w, const double* __restrict__ mean
         }
     }
     if (threadIdx.x == 0) w.colscale[(int64_t)k * w.V + v] = ldexp(1.0, e - 7 - 21);
+    if (w.ycolscale) {
+        // Rigorous bound on |y_i| = |sum_j g_ij w1_j - o_ij w2_j| <= sum_j 2|w1_j| + |w2_j|
+        // (inflated for the digit rounding of the weights), fixing the sketch's
+        // digit exponent before phase 1 runs.
+        double bsum = 0.0;
+        for (int64_t r = threadIdx.x; r < nnzp; r += blockDim.x) {
+            const double sc = w.sc[r0 + r];
+            if (sc == 0.0) continue;
+            const int64_t j = w.rowind[r0 + r];
+            const double w1 = sdinv[j] * (sc * Z[(int64_t)v * z_ld + j]);
+            bsum += 2.0 * fabs(w1) + fabs(mean[j] * w1);
+        }
+        __syncthreads();
+        for (int o = 16; o; o >>= 1) bsum += __shfl_xor_sync(0xffffffffu, bsum, o);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = bsum;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double tot = 0.0;
+            for (int q = 0; q < (int)(blockDim.x >> 5); ++q) tot += red[q];
+            // The weights enter as 4-digit values, each within 2^(e-29) of w1 and
+            // of mu*w1: add that slack for every member, then the FP64 rounding
+            // of the sum.
+            tot = (tot + (double)nnzp * 3.0 * ldexp(1.0, e - 29)) * (1.0 + 1e-9);
+            int ey = 0;
+            if (tot > 0.0 && isfinite(tot)) {
+                ey = ilogb(tot) + 1;
+                if (ldexp(tot, 7 - ey) > 127.0) ey += 1;
+            }
+            w.ycolscale[(int64_t)k * w.V + v] = ldexp(1.0, ey - 28);
+            // digit shift for the phase-1 epilogue: R = rint(T 2^(eW - eY))
+            w.yshift[(int64_t)k * w.V + v] = e - ey;
+        }
+    }
 }
 
 void launch_p1_weights4(const P1UWeights& w, const double* mean, const double* sdinv,
@@ -269,7 +426,9 @@ void launch_p1_weights4(const P1UWeights& w, const double* mean, const double* s
     count_launch();
 }
 
-size_t p1_umma_smem_bytes() { return (size_t)p1::kStages * p1::kStageBytes + 1024 + 256; }
+size_t p1_umma_smem_bytes() {
+    return (size_t)p1::kStages * p1::kStageBytes + (size_t)p1::kRing * p1::kRingSlot + 1024 + 256;
+}
 
 void prepare_p1_umma() {
     cudaFuncSetAttribute(p1_umma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -283,8 +442,11 @@ void launch_p1_umma(const CUtensorMap& tmW, const P1UArgs& a, int64_t N_pad, cud
                              (int)p1_umma_smem_bytes());
         attr = true;
     }
-    dim3 grid((unsigned)(N_pad / p1::kBM), (unsigned)a.K);
-    p1_umma_kernel<<<grid, p1::kThreads, p1_umma_smem_bytes(), st>>>(tmW, a);
+    const int spc = a.sb_per_cta > 0 ? a.sb_per_cta : 1;
+    P1UArgs b = a;
+    b.sb_per_cta = spc;
+    dim3 grid((unsigned)(N_pad / p1::kBM), (unsigned)((a.K + spc - 1) / spc));
+    p1_umma_kernel<<<grid, p1::kThreads, p1_umma_smem_bytes(), st>>>(tmW, b);
     count_launch();
 }
 
