@@ -221,6 +221,28 @@ int lds_win_plan_results(int64_t plan, double* ldscore, double* meansq_accum, do
                          double* mc_per_snp_sumsq);
 int lds_win_plan_kernel_ms(int64_t plan, double* ms4);
 int lds_win_plan_destroy(int64_t plan);
+
+/* Control-variate outputs of a windowed plan (no counterpart in the reference;
+ * they serve the learned control variate).  Call lds_win_plan_set_cv before the
+ * plan's first execute.  split_tiles != 0 keeps one meansq slice per V-tile
+ * (independent probe sets, so their spread estimates the Monte-Carlo noise);
+ * band_D in {4, 8, 15} also computes, per (SNP j, bin k),
+ *   mu[j K + k] = sum_{|i-j| <= D, same window} c_ji^2 annot_ik^2   (exact) and
+ *   C[t][j K + k] = sum_v (sum_{same i} c_ji annot_ik z_iv)^2         (V-tile t),
+ * c_ji = (x_j . x_i) sqrt(left scale_j) from lds_nn_band's exact products, so
+ * that meansq - C + V mu is an unbiased near-field control-variate estimate
+ * of meansq.  band_D = 0 disables it.  annot: M x K row-major (as at create). */
+int lds_win_plan_set_cv(int64_t plan, const double* annot, int split_tiles, int band_D);
+/* Number of V-tiles and their probe counts (tile_sizes may be NULL). */
+int lds_win_plan_tiles(int64_t plan, int* n_tiles, int* tile_sizes);
+/* After execute: copy the outputs (host pointers, or device pointers when
+ * device_ptrs != 0; any may be NULL).  meansq_tiles and C_tiles hold
+ * n_out x M x K values (n_out = n_tiles with split_tiles, else 1); mu M x K;
+ * xx M x (band_D+1).  Waits for the plan's work. */
+int lds_win_plan_cv_outputs(int64_t plan, int device_ptrs, double* meansq_tiles,
+                            double* C_tiles, double* mu, double* xx);
+/* Device time (ms) of the control-variate kernels of the last execute. */
+int lds_win_plan_cv_ms(int64_t plan, double* ms);
 uint64_t lds_window_seed(uint64_t root, int64_t w);
 
 /* Device timing of the last lds_gw_ldscore call (milliseconds, CUDA events
@@ -255,6 +277,51 @@ int lds_set_p2_kernel(int impl);
  * per-SNP integer latent thresholds. */
 int lds_synth_bed(int64_t n, int64_t M, uint64_t seed, const int64_t* t0, const int64_t* t1,
                   int missing, uint8_t* out);
+
+/* ---------------------------------------------------------------------
+ * Exact products of each SNP with its D nearest right-hand neighbours on a
+ * resident genotype image (lds_geno_create):
+ *   xx_out[j*(D+1) + d] = x_j . x_{j+d}   (0 when j+d >= M),
+ * x_ij = s_j (g_ij - mu_j) o_ij with the image's imputation, mean and sd (the
+ * standardization of the stochastic estimators).  r^2 to a neighbour is
+ * xx[j][d]^2 / (xx[j][0] xx[j+d][0]).  counts_out (may be NULL) receives the
+ * exact integer sums GG, GO, OG, OO per (j, d), 4 int32 each.  These are the
+ * near-diagonal entries of X^T X that the exact windowed LD scores
+ * (compute_windowed_ld_chr_impl, winldcore.cpp:783, via syrk panels) sum in
+ * full; here they feed the control variate.  0 <= D <= LDS_NN_BAND_MAX.
+ * Synchronous.
+ * ------------------------------------------------------------------- */
+#define LDS_NN_BAND_MAX 15
+/* Per-SNP mean (2 x allele frequency) and inverse sd of a resident image, as
+ * used by its standardization (M values each; either pointer may be NULL). */
+int lds_geno_stats(int64_t geno, double* mean_out, double* sdinv_out);
+int lds_nn_band(int64_t geno, int D, double* xx_out, int32_t* counts_out);
+
+/* ---------------------------------------------------------------------
+ * Surrogate network of the learned control variate (no counterpart in the
+ * reference): in_dim -> 128 -> 128 -> 128 -> out_dim, GELU (erf form) after the
+ * hidden layers, FP32 master parameters, BF16 weights and activations in the
+ * products with FP32 accumulation.  Parameters are one FP32 array of
+ * lds_mlp_param_count floats: W1 [128][in], b1 [128], W2 [128][128], b2,
+ * W3 [128][128], b3, W4 [out][128], b4 [out] (row-major).  All pointers are
+ * device pointers owned by the caller; x is n x in_dim, targets and outputs
+ * n x out_dim (row-major FP32).  The loss is the mean over rows and outputs of
+ * the squared error.  Calls are synchronous.
+ * ------------------------------------------------------------------- */
+#define LDS_MLP_MAX_IN 128
+#define LDS_MLP_MAX_OUT 64
+int64_t lds_mlp_param_count(int in_dim, int out_dim);
+int lds_mlp_forward(const float* d_params, int in_dim, int out_dim, const float* d_x, int64_t n,
+                    float* d_out);
+/* d_grad (param_count floats) = gradient of the loss over all n rows; loss_out (host). */
+int lds_mlp_loss_grad(const float* d_params, int in_dim, int out_dim, const float* d_x,
+                      const float* d_t, int64_t n, float* d_grad, double* loss_out);
+/* Adam (beta 0.9 / 0.999, eps 1e-8, rate lr) over shuffled mini-batches of
+ * `batch` rows for `epochs` passes, in place on d_params; loss_per_epoch (host,
+ * may be NULL) receives each epoch's mean mini-batch loss. */
+int lds_mlp_train(float* d_params, int in_dim, int out_dim, const float* d_x, const float* d_t,
+                  int64_t n, int epochs, int batch, float lr, uint64_t seed,
+                  double* loss_per_epoch);
 
 /* ---------------------------------------------------------------------
  * Phase 2 without any device allocation.  No counterpart in the reference.

@@ -52,6 +52,22 @@ def bounded_vtile_sizes(nvecs: int, vmax: int, granularity: int = 64) -> list[in
     return [min(width, nvecs - s) for s in range(0, nvecs, width)]
 
 
+def band_counts(geno: np.ndarray, D: int) -> np.ndarray:
+    """Integer sums GG, GO, OG, OO of SNP pairs (j, j+d), d = 0..D, from hard calls
+    (M x N, missing < 0): the exact counts behind lds_nn_band (numpy, int64)."""
+    g = np.where(geno >= 0, geno, 0).astype(np.int64)
+    o = (geno >= 0).astype(np.int64)
+    m = g.shape[0]
+    out = np.zeros((m, D + 1, 4), dtype=np.int64)
+    for d in range(D + 1):
+        a, b = slice(0, m - d), slice(d, m)
+        out[: m - d, d, 0] = (g[a] * g[b]).sum(1)
+        out[: m - d, d, 1] = (g[a] * o[b]).sum(1)
+        out[: m - d, d, 2] = (o[a] * g[b]).sum(1)
+        out[: m - d, d, 3] = (o[a] * o[b]).sum(1)
+    return out
+
+
 def compute_blocks(nsnps: int, step: int) -> list[tuple[int, int]]:
     """SNP blocks, gw_ldscore.py:1702-1703."""
     return [(s, min(nsnps, s + step)) for s in range(0, nsnps, step)]
@@ -99,6 +115,16 @@ class Oracle:
                                        n, blk_start, blk_end, ddof, int(impute == "hwe"),
                                        impute_seed, _ptr(geno), _ptr(mean), _ptr(inv))
         return geno, mean, inv
+
+    def band_products(self, bed_rows, n_total, D, rows=None, ddof=1, impute="mean", impute_seed=0):
+        """x_j . x_{j+d} for d = 0..D (0 past the last SNP) from the standardized
+        genotypes of ``standardize`` (FP64)."""
+        m = bed_rows.shape[0]
+        X = self.standardize(bed_rows, n_total, 0, m, rows, ddof, impute, impute_seed)[0]
+        xx = np.zeros((m, D + 1))
+        for d in range(D + 1):
+            xx[: m - d, d] = np.einsum("ij,ij->j", X[:, : m - d], X[:, d:])
+        return xx
 
     def probes(self, root, blk_start, v_start, L, V, dist="rademacher", as_float=False):
         Z = np.empty((L, V), dtype=np.float64, order="F")

@@ -49,11 +49,21 @@ SIGNATURES: dict[str, tuple] = {
     "lds_win_plan_results": (_int, [_i64, _p, _p, _p, _p]),
     "lds_win_plan_kernel_ms": (_int, [_i64, _p]),
     "lds_win_plan_destroy": (_int, [_i64]),
+    "lds_win_plan_set_cv": (_int, [_i64, _p, _int, _int]),
+    "lds_win_plan_tiles": (_int, [_i64, _p, _p]),
+    "lds_win_plan_cv_outputs": (_int, [_i64, _int, _p, _p, _p, _p]),
+    "lds_win_plan_cv_ms": (_int, [_i64, _p]),
+    "lds_mlp_param_count": (_i64, [_int, _int]),
+    "lds_mlp_forward": (_int, [_p, _int, _int, _p, _i64, _p]),
+    "lds_mlp_loss_grad": (_int, [_p, _int, _int, _p, _p, _i64, _p, _p]),
+    "lds_mlp_train": (_int, [_p, _int, _int, _p, _p, _i64, _int, _int, C.c_float, _u64, _p]),
     "lds_window_seed": (_u64, [_u64, _i64]),
     "lds_phase2_accum_device_noalloc": (_int, [_p, _i64, _i64, _i64, _i64, _i64, _p, _int, _int,
                                                _p, _p, _p, _p, _p, _p]),
     "lds_geno_create": (_int, [_p, _i64, _i64, _i64, _p, _i64, _int, _u64, _int, _p]),
     "lds_geno_destroy": (_int, [_i64]),
+    "lds_nn_band": (_int, [_i64, _int, _p, _p]),
+    "lds_geno_stats": (_int, [_i64, _p, _p]),
     "lds_gw_plan_create": (_int, [_i64, _p, _i64, _int, _int, _int, _u64, _int, _dbl, _int, _int,
                                   _p]),
     "lds_gw_plan_execute": (_int, [_i64]),

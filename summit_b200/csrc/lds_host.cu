@@ -1239,14 +1239,23 @@ struct WinPlan {
     std::vector<Batch> batches;
     std::vector<DevBuf> z;              // per V-tile, M x V FP64 probes
     DevBuf y, yq, ycs, yshift, wq, wcs, accum, mc, lscale, guards, status;
+    // Optional outputs for the control variate (lds_win_plan_set_cv): per-V-tile
+    // meansq slices, near-field sums C and known means mu, neighbour products.
+    int split = 0, cv_D = 0;
+    DevBuf annot_d, winof_d, sqrt_ls, xx, band_cnt, cvC, cvMu;
+    cudaEvent_t cv_ev[2] = {nullptr, nullptr};
+    double cv_ms = 0.0;
     CUtensorMap tmA;
     std::vector<cudaEvent_t> ev;        // start, after phase 1 of each launch group, end
     double kernel_ms[4] = {0, 0, 0, 0};
     int pending = 0;
     cudaGraphExec_t graph = nullptr;
     unsigned long long graph_kernels = 0;  // kernel nodes in the captured graph
+    int ntiles_out() const { return split ? (int)vt.size() : 1; }
     ~WinPlan() {
         for (cudaEvent_t e : ev) cudaEventDestroy(e);
+        for (cudaEvent_t e : cv_ev)
+            if (e) cudaEventDestroy(e);
         if (graph) cudaGraphExecDestroy(graph);
     }
 };
@@ -1408,9 +1417,32 @@ std::unique_ptr<WinPlan> win_plan_create(Context& c, std::shared_ptr<Prepared> P
 void win_enqueue(Context& c, WinPlan& pl) {
     Prepared& P = *pl.P;
     const int64_t M = P.g.M, K = pl.K, Np = P.g.N_pad;
-    ck(cudaMemsetAsync(pl.accum.p, 0, sizeof(double) * (size_t)(M * K), c.st), "memset");
-    if (pl.with_mc) ck(cudaMemsetAsync(pl.mc.p, 0, sizeof(double) * (size_t)(M * K), c.st), "memset");
+    const size_t MK = (size_t)(M * K), nout = MK * (size_t)pl.ntiles_out();
+    ck(cudaMemsetAsync(pl.accum.p, 0, sizeof(double) * nout, c.st), "memset");
+    if (pl.with_mc) ck(cudaMemsetAsync(pl.mc.p, 0, sizeof(double) * MK, c.st), "memset");
     ck(cudaMemsetAsync(pl.guards.p, 0, 16, c.st), "memset");
+    if (pl.cv_D > 0) {
+        // Near-field control variate sums: inputs are static (probes, products),
+        // so they run first, timed by their own event pair.
+        ck(cudaEventRecordWithFlags(pl.cv_ev[0], c.st, cudaEventRecordExternal), "event");
+        ck(cudaMemsetAsync(pl.cvC.p, 0, sizeof(double) * nout, c.st), "memset");
+        for (size_t ti = 0; ti < pl.vt.size(); ++ti) {
+            CvNearArgs a;
+            a.M = M;
+            a.K = (int)K;
+            a.V = pl.vt[ti];
+            a.z = static_cast<double*>(pl.z[ti].p);
+            a.z_ld = M;
+            a.annot = static_cast<double*>(pl.annot_d.p);
+            a.win_of = static_cast<int32_t*>(pl.winof_d.p);
+            a.sqrt_ls = static_cast<double*>(pl.sqrt_ls.p);
+            a.xx = static_cast<double*>(pl.xx.p);
+            a.C = static_cast<double*>(pl.cvC.p) + (pl.split ? ti * MK : 0);
+            a.mu = ti == 0 ? static_cast<double*>(pl.cvMu.p) : nullptr;
+            launch_cv_near(a, pl.cv_D, c.st);
+        }
+        ck(cudaEventRecordWithFlags(pl.cv_ev[1], c.st, cudaEventRecordExternal), "event");
+    }
     int e = 0;
     ck(cudaEventRecordWithFlags(pl.ev[(size_t)e++], c.st, cudaEventRecordExternal), "event");
     for (size_t ti = 0; ti < pl.vt.size(); ++ti) {
@@ -1485,7 +1517,7 @@ void win_enqueue(Context& c, WinPlan& pl) {
             u.mean = static_cast<double*>(P.d_mean.p);
             u.sdinv = static_cast<double*>(P.d_sdinv.p);
             u.left_scale = static_cast<double*>(pl.lscale.p);
-            u.accum = static_cast<double*>(pl.accum.p);
+            u.accum = static_cast<double*>(pl.accum.p) + (pl.split ? ti * MK : 0);
             u.mc = pl.with_mc ? static_cast<double*>(pl.mc.p) : nullptr;
             u.guard_counts = static_cast<unsigned long long*>(pl.guards.p);
             u.extreme_warn = extreme_warn_env();
@@ -1529,6 +1561,11 @@ void win_times(WinPlan& pl) {
     if (!pl.pending) return;
     ck(cudaEventSynchronize(pl.ev.back()), "event sync");
     for (double& x : pl.kernel_ms) x = 0.0;
+    if (pl.cv_D > 0) {
+        float ms = 0.f;
+        ck(cudaEventElapsedTime(&ms, pl.cv_ev[0], pl.cv_ev[1]), "elapsed");
+        pl.cv_ms = ms;
+    }
     for (size_t i = 0; i + 1 < pl.ev.size(); ++i) {
         float ms = 0.f;
         ck(cudaEventElapsedTime(&ms, pl.ev[i], pl.ev[i + 1]), "elapsed");
@@ -1541,7 +1578,7 @@ void win_times(WinPlan& pl) {
 void win_results(Context& c, WinPlan& pl, double* ldscore, double* meansq_out, double* inv_out,
                  double* mc_snp) {
     const int64_t M = pl.P->g.M, K = pl.K, N = pl.P->g.N;
-    std::vector<double> acc((size_t)(M * K));
+    std::vector<double> acc((size_t)(M * K) * (size_t)pl.ntiles_out());
     d2h(acc.data(), static_cast<double*>(pl.accum.p), acc.size(), c.st);
     std::vector<double> mcv;
     if (pl.with_mc && mc_snp) {
@@ -1553,6 +1590,10 @@ void win_results(Context& c, WinPlan& pl, double* ldscore, double* meansq_out, d
     ck(cudaStreamSynchronize(c.st), "results");
     if (st) fail(LDS_ERR_CUDA, "tensor-core pipeline wait timed out (code %u)", st);
     win_times(pl);
+    // Per-V-tile slices (control-variate plans) add up to the plain sums.
+    for (int t = 1; t < pl.ntiles_out(); ++t)
+        for (size_t x = 0; x < (size_t)(M * K); ++x) acc[x] += acc[(size_t)t * (size_t)(M * K) + x];
+    acc.resize((size_t)(M * K));
     if (meansq_out) std::memcpy(meansq_out, acc.data(), sizeof(double) * acc.size());
     if (inv_out) std::memcpy(inv_out, pl.inv.data(), sizeof(double) * (size_t)M);
     const double nd = (double)(N - pl.P->ddof);
@@ -1564,6 +1605,37 @@ void win_results(Context& c, WinPlan& pl, double* ldscore, double* meansq_out, d
                     acc[(size_t)(j * K + k)] / (double)pl.nvecs - pl.Mkw[(size_t)(w * K + k)] / nd;
         }
     if (mc_snp && !mcv.empty()) std::memcpy(mc_snp, mcv.data(), sizeof(double) * mcv.size());
+}
+
+// Control-variate outputs of a windowed plan; call before its first execute.
+void win_set_cv(Context& c, WinPlan& pl, const double* annot, int split, int D) {
+    if (pl.graph) fail(LDS_ERR_ARG, "set the control-variate outputs before the first execute");
+    if (D != 0 && D != 4 && D != 8 && D != 15) fail(LDS_ERR_ARG, "band width D must be 0, 4, 8 or 15");
+    const int64_t M = pl.P->g.M, K = pl.K;
+    pl.split = split ? 1 : 0;
+    pl.cv_D = D;
+    const size_t MK = (size_t)(M * K), nout = MK * (size_t)pl.ntiles_out();
+    pl.accum.as<double>(nout);
+    if (D > 0) {
+        h2d(pl.annot_d.as<double>(MK), annot, MK, c.st);
+        h2d(pl.winof_d.as<int32_t>((size_t)M), pl.win_of.data(), (size_t)M, c.st);
+        std::vector<double> ls((size_t)M);
+        d2h(ls.data(), static_cast<double*>(pl.lscale.p), (size_t)M, c.st);
+        ck(cudaStreamSynchronize(c.st), "cv setup");
+        for (double& v : ls) v = std::sqrt(v);
+        h2d(pl.sqrt_ls.as<double>((size_t)M), ls.data(), (size_t)M, c.st);
+        int32_t* cnt = pl.band_cnt.as<int32_t>((size_t)(M * (D + 1) * 4));
+        double* xx = pl.xx.as<double>((size_t)(M * (D + 1)));
+        launch_nn_band(pl.P->g, D, cnt, c.st);
+        launch_nn_band_finish(M, D, cnt, static_cast<double*>(pl.P->d_mean.p),
+                              static_cast<double*>(pl.P->d_sdinv.p), xx, c.st);
+        pl.cvC.as<double>(nout);
+        pl.cvMu.as<double>(MK);
+        for (auto& e : pl.cv_ev)
+            if (!e) ck(cudaEventCreate(&e), "event");
+        ck(cudaGetLastError(), "launch");
+        ck(cudaStreamSynchronize(c.st), "cv setup");
+    }
 }
 
 void gw_ldscore_impl(const uint8_t* bed_rows, int64_t row_bytes, int64_t n_total, int64_t M,
@@ -1798,6 +1870,41 @@ LDS_API int lds_geno_destroy(int64_t handle) {
     });
 }
 
+LDS_API int lds_geno_stats(int64_t geno, double* mean_out, double* sdinv_out) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        auto it = geno_table().find(geno);
+        if (it == geno_table().end()) fail(LDS_ERR_ARG, "unknown genotype handle");
+        const Prepared& P = *it->second;
+        if (mean_out) std::memcpy(mean_out, P.mean.data(), sizeof(double) * P.mean.size());
+        if (sdinv_out) std::memcpy(sdinv_out, P.sdinv.data(), sizeof(double) * P.sdinv.size());
+    });
+}
+
+LDS_API int lds_nn_band(int64_t geno, int D, double* xx_out, int32_t* counts_out) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        ensure_device(c);
+        auto it = geno_table().find(geno);
+        if (it == geno_table().end()) fail(LDS_ERR_ARG, "unknown genotype handle");
+        if (D < 0 || D > LDS_NN_BAND_MAX) fail(LDS_ERR_ARG, "band width D must be in [0, 15]");
+        Prepared& P = *it->second;
+        const int64_t M = P.g.M, n = M * (D + 1);
+        DevBuf dc, dx;
+        int32_t* cnt = dc.as<int32_t>((size_t)(n * 4));
+        double* xx = dx.as<double>((size_t)n);
+        launch_nn_band(P.g, D, cnt, c.st);
+        launch_nn_band_finish(M, D, cnt, static_cast<double*>(P.d_mean.p),
+                              static_cast<double*>(P.d_sdinv.p), xx, c.st);
+        ck(cudaGetLastError(), "launch");
+        if (xx_out) d2h(xx_out, xx, (size_t)n, c.st);
+        if (counts_out) d2h(counts_out, cnt, (size_t)(n * 4), c.st);
+        ck(cudaStreamSynchronize(c.st), "band sync");
+    });
+}
+
 LDS_API int lds_gw_plan_create(int64_t geno, const double* annot, int64_t K, int nvecs,
                                int step_size, int vtile, uint64_t seed, int rand_dist,
                                double resvar_eps, int as_float, int with_mc, int64_t* plan_out) {
@@ -1972,6 +2079,181 @@ LDS_API int lds_win_plan_kernel_ms(int64_t plan, double* ms4) {
         ck(cudaStreamSynchronize(c.st), "sync");
         win_times(pl);
         for (int i = 0; i < 4; ++i) ms4[i] = pl.kernel_ms[i];
+    });
+}
+
+LDS_API int lds_win_plan_set_cv(int64_t plan, const double* annot, int split_tiles, int band_D) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        win_set_cv(c, win_of_handle(plan), annot, split_tiles, band_D);
+    });
+}
+
+LDS_API int lds_win_plan_tiles(int64_t plan, int* n_tiles, int* tile_sizes) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        WinPlan& pl = win_of_handle(plan);
+        *n_tiles = (int)pl.vt.size();
+        if (tile_sizes)
+            for (size_t t = 0; t < pl.vt.size(); ++t) tile_sizes[t] = pl.vt[t];
+    });
+}
+
+LDS_API int lds_win_plan_cv_outputs(int64_t plan, int device_ptrs, double* meansq_tiles,
+                                    double* C_tiles, double* mu, double* xx) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        WinPlan& pl = win_of_handle(plan);
+        const int64_t M = pl.P->g.M, K = pl.K;
+        const size_t nout = (size_t)(M * K) * (size_t)pl.ntiles_out();
+        const cudaMemcpyKind kind = device_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+        auto cp = [&](double* dst, const DevBuf& src, size_t n) {
+            if (dst && n) ck(cudaMemcpyAsync(dst, src.p, n * sizeof(double), kind, c.st), "copy");
+        };
+        unsigned st = 0;
+        d2h(&st, static_cast<unsigned*>(pl.status.p), 1, c.st);
+        cp(meansq_tiles, pl.accum, nout);
+        if (pl.cv_D > 0) {
+            cp(C_tiles, pl.cvC, nout);
+            cp(mu, pl.cvMu, (size_t)(M * K));
+            cp(xx, pl.xx, (size_t)(M * (pl.cv_D + 1)));
+        } else if (C_tiles || mu || xx) {
+            fail(LDS_ERR_ARG, "plan has no control-variate outputs (lds_win_plan_set_cv)");
+        }
+        ck(cudaStreamSynchronize(c.st), "cv outputs");
+        if (st) fail(LDS_ERR_CUDA, "tensor-core pipeline wait timed out (code %u)", st);
+        win_times(pl);
+    });
+}
+
+LDS_API int lds_win_plan_cv_ms(int64_t plan, double* ms) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        WinPlan& pl = win_of_handle(plan);
+        ck(cudaStreamSynchronize(c.st), "sync");
+        win_times(pl);
+        *ms = pl.cv_ms;
+    });
+}
+
+// ---------------------------------------------------------------------------
+// Surrogate network (learned control variate); device pointers owned by the caller.
+// ---------------------------------------------------------------------------
+static void check_mlp_dims(int in_dim, int out_dim) {
+    if (in_dim < 1 || in_dim > LDS_MLP_MAX_IN || out_dim < 1 || out_dim > LDS_MLP_MAX_OUT)
+        fail(LDS_ERR_ARG, "network input width must be in [1, 128] and output width in [1, 64]");
+}
+
+LDS_API int64_t lds_mlp_param_count(int in_dim, int out_dim) {
+    return mlp_layout(in_dim, out_dim).total;
+}
+
+LDS_API int lds_mlp_forward(const float* d_params, int in_dim, int out_dim, const float* d_x,
+                            int64_t n, float* d_out) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        ensure_device(c);
+        check_mlp_dims(in_dim, out_dim);
+        MlpArgs a;
+        a.params = d_params;
+        a.in = in_dim;
+        a.out = out_dim;
+        launch_mlp_forward(a, d_x, nullptr, n, nullptr, d_out, nullptr, nullptr, nullptr, 0.f, c.st);
+        ck(cudaGetLastError(), "launch");
+        ck(cudaStreamSynchronize(c.st), "mlp forward");
+    });
+}
+
+LDS_API int lds_mlp_loss_grad(const float* d_params, int in_dim, int out_dim, const float* d_x,
+                              const float* d_t, int64_t n, float* d_grad, double* loss_out) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        ensure_device(c);
+        check_mlp_dims(in_dim, out_dim);
+        if (n <= 0) fail(LDS_ERR_ARG, "n must be positive");
+        MlpArgs a;
+        a.params = d_params;
+        a.in = in_dim;
+        a.out = out_dim;
+        const int op = mlp_out_pad(out_dim);
+        const int64_t P = mlp_layout(in_dim, out_dim).total;
+        DevBuf zs, dzs, dout, ls;
+        float* z = zs.as<float>((size_t)(n * 3 * kMlpHidden));
+        float* dz = dzs.as<float>((size_t)(n * 3 * kMlpHidden));
+        float* d = dout.as<float>((size_t)(n * op));
+        double* l = ls.as<double>(1);
+        ck(cudaMemsetAsync(l, 0, sizeof(double), c.st), "memset");
+        ck(cudaMemsetAsync(d_grad, 0, sizeof(float) * (size_t)P, c.st), "memset");
+        launch_mlp_forward(a, d_x, nullptr, n, d_t, nullptr, z, d, l, 1.0f / (float)(n * out_dim), c.st);
+        launch_mlp_backward(a, d_x, nullptr, n, z, d, dz, d_grad, c.st);
+        ck(cudaGetLastError(), "launch");
+        if (loss_out) d2h(loss_out, l, 1, c.st);
+        ck(cudaStreamSynchronize(c.st), "mlp grad");
+    });
+}
+
+LDS_API int lds_mlp_train(float* d_params, int in_dim, int out_dim, const float* d_x,
+                          const float* d_t, int64_t n, int epochs, int batch, float lr,
+                          uint64_t seed, double* loss_per_epoch) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        ensure_device(c);
+        check_mlp_dims(in_dim, out_dim);
+        if (n <= 0 || epochs < 0 || batch <= 0) fail(LDS_ERR_ARG, "invalid training sizes");
+        MlpArgs a;
+        a.params = d_params;
+        a.in = in_dim;
+        a.out = out_dim;
+        const int op = mlp_out_pad(out_dim);
+        const int64_t P = mlp_layout(in_dim, out_dim).total;
+        const int64_t B = std::min<int64_t>(batch, n);
+        DevBuf m, v, g, zs, dzs, dout, rows, ls;
+        float* dm = m.as<float>((size_t)P);
+        float* dv = v.as<float>((size_t)P);
+        float* dg = g.as<float>((size_t)P);
+        float* z = zs.as<float>((size_t)(B * 3 * kMlpHidden));
+        float* dz = dzs.as<float>((size_t)(B * 3 * kMlpHidden));
+        float* d = dout.as<float>((size_t)(B * op));
+        int32_t* r = rows.as<int32_t>((size_t)n);
+        double* l = ls.as<double>((size_t)std::max(epochs, 1));
+        ck(cudaMemsetAsync(dm, 0, sizeof(float) * (size_t)P, c.st), "memset");
+        ck(cudaMemsetAsync(dv, 0, sizeof(float) * (size_t)P, c.st), "memset");
+        ck(cudaMemsetAsync(l, 0, sizeof(double) * (size_t)std::max(epochs, 1), c.st), "memset");
+        const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+        std::vector<int32_t> perm((size_t)n);
+        std::mt19937_64 rng(seed);
+        int64_t step = 0;
+        const int64_t nsteps = (n + B - 1) / B;
+        for (int e = 0; e < epochs; ++e) {
+            for (int64_t i = 0; i < n; ++i) perm[(size_t)i] = (int32_t)i;
+            std::shuffle(perm.begin(), perm.end(), rng);
+            ck(cudaStreamSynchronize(c.st), "mlp epoch");  // perm buffer reuse
+            h2d(r, perm.data(), (size_t)n, c.st);
+            for (int64_t s = 0; s < nsteps; ++s) {
+                const int64_t nb = std::min<int64_t>(B, n - s * B);
+                ck(cudaMemsetAsync(dg, 0, sizeof(float) * (size_t)P, c.st), "memset");
+                launch_mlp_forward(a, d_x, r + s * B, nb, d_t, nullptr, z, d, l + e,
+                                   1.0f / (float)(nb * out_dim * nsteps), c.st);
+                launch_mlp_backward(a, d_x, r + s * B, nb, z, d, dz, dg, c.st);
+                ++step;
+                // The loss scale folds 1/nsteps into the gradient (so the epoch's
+                // loss sums to its mean); Adam is invariant to that scale except
+                // through eps, which is scaled alike.
+                launch_mlp_adam(d_params, dm, dv, dg, P, lr, b1, b2, eps * (float)(1.0 / nsteps),
+                                1.0f - std::pow(b1, (float)step), 1.0f - std::pow(b2, (float)step),
+                                c.st);
+            }
+        }
+        ck(cudaGetLastError(), "launch");
+        if (loss_per_epoch && epochs > 0) d2h(loss_per_epoch, l, (size_t)epochs, c.st);
+        ck(cudaStreamSynchronize(c.st), "mlp train");
     });
 }
 

@@ -93,6 +93,66 @@ void launch_p2(const DevGeno& g, const P2Args& a, cudaStream_t st);
 void launch_synth(int64_t n, int64_t M, uint64_t seed, const int64_t* t0, const int64_t* t1,
                   int missing, uint8_t* out, cudaStream_t st);
 
+// Exact products with the D nearest right-hand neighbours (lds_band.cu):
+// counts[(j (D+1) + d) 4 + {0..3}] = GG, GO, OG, OO integer sums of SNPs j, j+d;
+// xx[j (D+1) + d] = x_j . x_{j+d} in FP64 from them.
+void launch_nn_band(const DevGeno& g, int D, int32_t* counts, cudaStream_t st);
+void launch_nn_band_finish(int64_t M, int D, const int32_t* counts, const double* mean,
+                           const double* sdinv, double* xx, cudaStream_t st);
+
+// Near-field control variate sums (lds_cv.cu): C[j K + k] += sum_v a_jkv^2 and,
+// if mu is set, mu[j K + k] = E[a_jk^2]; D in {4, 8, 15}.
+struct CvNearArgs {
+    int64_t M = 0;
+    int K = 0, V = 0;
+    const double* z = nullptr;      // probes, z[v z_ld + i]
+    int64_t z_ld = 0;
+    const double* annot = nullptr;  // M x K row-major
+    const int32_t* win_of = nullptr;
+    const double* sqrt_ls = nullptr;
+    const double* xx = nullptr;     // M x (D+1) neighbour products
+    double* C = nullptr;
+    double* mu = nullptr;
+};
+void launch_cv_near(const CvNearArgs& a, int D, cudaStream_t st);
+
+// Surrogate network of the learned control variate (lds_mlp.cu): in -> 128 ->
+// 128 -> 128 -> out, GELU, FP32 master parameters laid out as below.
+constexpr int kMlpHidden = 128;
+struct MlpLayout {
+    int64_t W1, b1, W2, b2, W3, b3, W4, b4, total;
+};
+__host__ __device__ inline MlpLayout mlp_layout(int in, int out) {
+    MlpLayout L;
+    L.W1 = 0;
+    L.b1 = L.W1 + (int64_t)kMlpHidden * in;
+    L.W2 = L.b1 + kMlpHidden;
+    L.b2 = L.W2 + (int64_t)kMlpHidden * kMlpHidden;
+    L.W3 = L.b2 + kMlpHidden;
+    L.b3 = L.W3 + (int64_t)kMlpHidden * kMlpHidden;
+    L.W4 = L.b3 + kMlpHidden;
+    L.b4 = L.W4 + (int64_t)out * kMlpHidden;
+    L.total = L.b4 + out;
+    return L;
+}
+__host__ __device__ inline int mlp_out_pad(int out) { return (out + 3) & ~3; }
+struct MlpArgs {
+    const float* params = nullptr;
+    int in = 0, out = 0;
+};
+// Forward over n rows (x rows gathered through `rows` if set): out (n x out,
+// may be null); with `target`, dout (n x out_pad) = 2 (o - t) gscale and
+// loss += gscale sum (o - t)^2; zs (n x 3 x 128, may be null) keeps z1..z3.
+void launch_mlp_forward(const MlpArgs& a, const float* x, const int32_t* rows, int64_t n,
+                        const float* target, float* out, float* zs, float* dout, double* loss,
+                        float gscale, cudaStream_t st);
+// Backward: grad (zeroed by the caller) += d loss / d params.
+void launch_mlp_backward(const MlpArgs& a, const float* x, const int32_t* rows, int64_t n,
+                         const float* zs, const float* dout, float* dzs, float* grad,
+                         cudaStream_t st);
+void launch_mlp_adam(float* p, float* m, float* v, const float* g, int64_t P, float lr, float b1,
+                     float b2, float eps, float bc1, float bc2, cudaStream_t st);
+
 // Launch accounting.
 void count_launch();
 

@@ -9,11 +9,11 @@
 // TMA, SWIZZLE_128B, K-major) into ONE accumulator, so TMEM holds
 // G.W1 - O.W2 = sum_j (g - mu_j o) s_j sc z directly.
 //
-// Roles (320 threads): warp 0 TMA producer for the digit tiles; warp 1 TMEM
+// Roles (704 threads): warp 0 TMA producer for the digit tiles; warp 1 TMEM
 // allocation and the single MMA-issuing thread; warps 2-5 gather the member
 // SNPs' packed bytes from global memory (one row each, kept several stages
-// ahead by cp.async) and decode them into the operand tiles; warps 6-9 read the
-// accumulator out.  Two TMEM accumulators let the MMAs of the next job (super-bin,
+// ahead by cp.async) and decode them into the operand tiles; warps 6-21 (four
+// per TMEM lane quadrant) read the accumulator out and split it into digits.  Two TMEM accumulators let the MMAs of the next job (super-bin,
 // column group) run while the epilogue of the previous one drains, which
 // matters for windowed estimates, whose super-bins are a few K-steps long.
 #include <cstdint>
@@ -33,8 +33,8 @@ constexpr int kBK = 128;          // member SNPs per stage
 constexpr int kATile = 128 * 128; // 16 KB
 constexpr int kWTile = 256 * 128; // 32 KB (max digit columns per pass)
 constexpr int kStageBytes = 2 * kATile + 2 * kWTile;  // 96 KB
-constexpr int kThreads = 448;
-constexpr int kEpiThreads = 256;         // warps 6..13: two per TMEM lane quadrant
+constexpr int kThreads = 704;
+constexpr int kEpiThreads = 512;         // warps 6..21: four per TMEM lane quadrant
 constexpr int kAccCols = 256;            // one accumulator: <= 256 digit columns
 constexpr uint32_t kTmemCols = 512;      // two accumulators (MMA of job j+1 || epilogue of j)
 constexpr int kRing = 8;                 // gathered packed rows in flight per decoder thread
@@ -211,10 +211,10 @@ __global__ void __launch_bounds__(p1::kThreads, 1)
         }
         cp_async_wait_all();  // no gather copy may outlive the CTA (abort path)
     } else {
-        // ---------------- epilogue (warps 6..13) ----------------
+        // ---------------- epilogue (warps 6..21) ----------------
         const int e = tid - 192;
         const int q = warp & 3;                  // TMEM lane quadrant of this warp
-        const int h = (warp - 6) >> 2;           // which half of the 32-column chunks
+        const int h = (warp - 6) >> 2;           // which quarter of the 16-column chunks
         const int64_t i = i0 + q * 32 + lane;    // sample row of this thread's accumulator lane
         int au = 0;
         for (int k = kb0; k < kb1 && !*abort_flag; ++k) {
@@ -263,12 +263,12 @@ __global__ void __launch_bounds__(p1::kThreads, 1)
                 tc_fence_after();
                 const int ncols = min(kAccCols, a.ncolp - g * 256);
                 const uint32_t tbase = tmem + (uint32_t)(b * kAccCols) + ((uint32_t)(q * 32) << 16);
-                for (int c0c = 32 * h; c0c < ncols; c0c += 64) {
-                    int rr[32];
-                    tmem_ld32(tbase + (uint32_t)c0c, rr);
+                for (int c0c = 16 * h; c0c < ncols; c0c += 64) {
+                    int rr[16];
+                    tmem_ld16(tbase + (uint32_t)c0c, rr);
                     tmem_wait_ld();
 #pragma unroll
-                    for (int p = 0; p < 8; ++p) {
+                    for (int p = 0; p < 4; ++p) {
                         const int vl = c0c / 4 + p;  // probe within the group (warp-uniform)
                         const int v = g * 64 + vl;
                         if (v >= a.V) continue;

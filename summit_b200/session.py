@@ -83,6 +83,21 @@ class GwSession:
                                              int(with_mc), C.byref(h)))
         return GwPlan(self, h.value, self.M, annot.shape[1], with_mc)
 
+    def stats(self) -> dict:
+        """Per-SNP mean (2 x allele frequency) and inverse sd of the standardization."""
+        mean, sdinv = np.empty(self.M), np.empty(self.M)
+        check(_lib.load().lds_geno_stats(self.handle, ptr(mean), ptr(sdinv)))
+        return {"mean": mean, "sdinv": sdinv}
+
+    def nn_band(self, D: int = 8, with_counts: bool = False):
+        """Exact products x_j . x_{j+d}, d = 0..D, of the standardized genotypes
+        (M x (D+1)); with ``with_counts`` also the integer sums GG, GO, OG, OO
+        (M x (D+1) x 4)."""
+        xx = np.empty((self.M, D + 1))
+        cnt = np.empty((self.M, D + 1, 4), dtype=np.int32) if with_counts else None
+        check(_lib.load().lds_nn_band(self.handle, int(D), ptr(xx), ptr(cnt)))
+        return (xx, cnt) if with_counts else xx
+
     def close(self) -> None:
         if self.handle:
             _lib.load().lds_geno_destroy(self.handle)
@@ -136,6 +151,43 @@ class WinPlan:
         buf = np.zeros(4)
         check(_lib.load().lds_win_plan_kernel_ms(self.handle, ptr(buf)))
         return {"weights": buf[0], "phase1": buf[1], "digits": buf[2], "phase2": buf[3]}
+
+    # ---- control-variate outputs (see lds_win_plan_set_cv) ----
+    def set_cv(self, annot, split_tiles: bool = True, band: int = 8) -> None:
+        annot = np.ascontiguousarray(annot, dtype=np.float64)
+        check(_lib.load().lds_win_plan_set_cv(self.handle, ptr(annot), int(split_tiles), int(band)))
+        self.split, self.band = bool(split_tiles), int(band)
+
+    def tiles(self) -> list[int]:
+        n = C.c_int(0)
+        sizes = np.zeros(4096, dtype=np.int32)
+        check(_lib.load().lds_win_plan_tiles(self.handle, C.byref(n), ptr(sizes)))
+        return [int(x) for x in sizes[: n.value]]
+
+    def cv_outputs(self) -> dict:
+        """Host copies: meansq per V-tile slice, near-field sums C per slice, mu, xx."""
+        T = len(self.tiles()) if getattr(self, "split", False) else 1
+        M, K = self.M, self.K
+        out = {"meansq": np.empty((T, M, K)), "C": None, "mu": None, "xx": None}
+        if getattr(self, "band", 0):
+            out["C"] = np.empty((T, M, K))
+            out["mu"] = np.empty((M, K))
+            out["xx"] = np.empty((M, self.band + 1))
+        check(_lib.load().lds_win_plan_cv_outputs(self.handle, 0, ptr(out["meansq"]), ptr(out["C"]),
+                                                  ptr(out["mu"]), ptr(out["xx"])))
+        return out
+
+    def cv_outputs_device(self, meansq, C_tiles=None, mu=None, xx=None) -> None:
+        """Copy the outputs into caller-owned device buffers (integer addresses,
+        e.g. torch tensors' data_ptr())."""
+        vp = lambda a: None if a is None else C.c_void_p(int(a))
+        check(_lib.load().lds_win_plan_cv_outputs(self.handle, 1, vp(meansq), vp(C_tiles), vp(mu),
+                                                  vp(xx)))
+
+    def cv_ms(self) -> float:
+        x = C.c_double(0.0)
+        check(_lib.load().lds_win_plan_cv_ms(self.handle, C.byref(x)))
+        return x.value
 
     def close(self) -> None:
         if self.handle:
