@@ -224,11 +224,12 @@ int lds_win_plan_destroy(int64_t plan);
 
 /* Control-variate outputs of a windowed plan (no counterpart in the reference;
  * they serve the learned control variate).  Call lds_win_plan_set_cv before the
- * plan's first execute.  split_tiles != 0 keeps one meansq slice per V-tile
- * (independent probe sets, so their spread estimates the Monte-Carlo noise);
+ * plan's first execute.  split_tiles != 0 keeps two meansq slices, probes
+ * [0, h) and [h, nvecs) with h = ceil(nvecs / 2) (independent probe sets, so
+ * their spread estimates the Monte-Carlo noise);
  * band_D in {4, 8, 15} also computes, per (SNP j, bin k),
  *   mu[j K + k] = sum_{|i-j| <= D, same window} c_ji^2 annot_ik^2   (exact) and
- *   C[t][j K + k] = sum_v (sum_{same i} c_ji annot_ik z_iv)^2         (V-tile t),
+ *   C[t][j K + k] = sum_v (sum_{same i} c_ji annot_ik z_iv)^2   (probes of slice t),
  * c_ji = (x_j . x_i) sqrt(left scale_j) from lds_nn_band's exact products, so
  * that meansq - C + V mu is an unbiased near-field control-variate estimate
  * of meansq.  band_D = 0 disables it.  annot: M x K row-major (as at create). */
@@ -237,7 +238,7 @@ int lds_win_plan_set_cv(int64_t plan, const double* annot, int split_tiles, int 
 int lds_win_plan_tiles(int64_t plan, int* n_tiles, int* tile_sizes);
 /* After execute: copy the outputs (host pointers, or device pointers when
  * device_ptrs != 0; any may be NULL).  meansq_tiles and C_tiles hold
- * n_out x M x K values (n_out = n_tiles with split_tiles, else 1); mu M x K;
+ * n_out x M x K values (n_out = 2 with split_tiles, else 1); mu M x K;
  * xx M x (band_D+1).  Waits for the plan's work. */
 int lds_win_plan_cv_outputs(int64_t plan, int device_ptrs, double* meansq_tiles,
                             double* C_tiles, double* mu, double* xx);

@@ -39,16 +39,18 @@ __global__ void cv_near_kernel(CvNearArgs a) {
         w[t] = c;
         mu += c * c;
     }
-    double acc = 0.0;
+    double acc = 0.0, acc2 = 0.0;
     for (int v = 0; v < a.V; ++v) {
         const double* z = a.z + (int64_t)v * a.z_ld;
         double s = 0.0;
 #pragma unroll
         for (int t = 0; t < 2 * D + 1; ++t)
             if (w[t] != 0.0) s += w[t] * z[j + t - D];
-        acc += s * s;
+        if (a.C2 && v >= a.split_v) acc2 += s * s;
+        else acc += s * s;
     }
     a.C[j * a.K + k] += acc;
+    if (a.C2) a.C2[j * a.K + k] += acc2;
     if (a.mu) a.mu[j * a.K + k] = mu;
 }
 

@@ -186,6 +186,9 @@ struct Context {
     std::list<std::unique_ptr<Prepared>> cache;  // most recent first
     DevBuf raw, rows_dev, hwe_q0, hwe_q01, hwe_sb, counts_dev;
     DevBuf y, yq, ycs, wq, wcs, z, rowind, sc, binoff, wqoff, accum, mc, guards, lscale, xin;
+    // Surrogate-network workspace, grow-only so that repeated training and
+    // inference calls make no device allocations (cudaFree synchronizes).
+    DevBuf mlp_m, mlp_v, mlp_g, mlp_zs, mlp_dzs, mlp_dout, mlp_rows, mlp_loss, mlp_pack;
     double timings[4] = {0, 0, 0, 0};
     int slices = 4;
 };
@@ -999,8 +1002,10 @@ std::unique_ptr<GwPlan> plan_create(Context& c, std::shared_ptr<Prepared> P, con
                               (uint64_t)P->g.nbp, 32, 128, CU_TENSOR_MAP_SWIZZLE_NONE);
         for (int V : pl->vt) {
             const int nc = umma::ncolp_for(V);
+            const int nb = umma::p2_bins_per_cta(nc, (int)K);
             pl->tmB.push_back(make_map_2d(yq, (uint64_t)P->g.N_pad, (uint64_t)(K * nc),
-                                          (uint64_t)P->g.N_pad, 128, (uint32_t)std::min(256, nc),
+                                          (uint64_t)P->g.N_pad, 128,
+                                          (uint32_t)std::min(256, nb * nc),
                                           CU_TENSOR_MAP_SWIZZLE_128B));
         }
         ck(cudaMemsetAsync(pl->status.as<unsigned>(1), 0, 4, c.st), "memset");
@@ -1095,8 +1100,9 @@ void plan_execute(Context& c, GwPlan& pl) {
             u.K = (int)K;
             u.V = t.V;
             u.ncolp = nc;
-            u.ngroups = (nc + 255) / 256;
-            u.box_rows = std::min(256, nc);
+            u.bins_per_cta = umma::p2_bins_per_cta(nc, (int)K);
+            u.ngroups = (u.bins_per_cta * nc + 255) / 256;
+            u.box_rows = std::min(256, u.bins_per_cta * nc);
             u.nkt = (int)(P.g.N_pad / 128);
             u.M = M;
             u.j0 = 0;
@@ -1251,7 +1257,17 @@ struct WinPlan {
     int pending = 0;
     cudaGraphExec_t graph = nullptr;
     unsigned long long graph_kernels = 0;  // kernel nodes in the captured graph
-    int ntiles_out() const { return split ? (int)vt.size() : 1; }
+    // Output slices: with `split`, probes [0, half) and [half, nvecs) of every
+    // (SNP, bin) sum go to two slices (two independent halves of the probes).
+    int ntiles_out() const { return split ? 2 : 1; }
+    int half() const { return (nvecs + 1) / 2; }
+    // Probe range of V-tile ti: [voff(ti), voff(ti) + vt[ti]).
+    int voff(size_t ti) const {
+        int o = 0;
+        for (size_t u = 0; u < ti; ++u) o += vt[u];
+        return o;
+    }
+    int split_local(size_t ti) const { return std::min(std::max(half() - voff(ti), 0), vt[ti]); }
     ~WinPlan() {
         for (cudaEvent_t e : ev) cudaEventDestroy(e);
         for (cudaEvent_t e : cv_ev)
@@ -1437,8 +1453,12 @@ void win_enqueue(Context& c, WinPlan& pl) {
             a.win_of = static_cast<int32_t*>(pl.winof_d.p);
             a.sqrt_ls = static_cast<double*>(pl.sqrt_ls.p);
             a.xx = static_cast<double*>(pl.xx.p);
-            a.C = static_cast<double*>(pl.cvC.p) + (pl.split ? ti * MK : 0);
+            a.C = static_cast<double*>(pl.cvC.p);
             a.mu = ti == 0 ? static_cast<double*>(pl.cvMu.p) : nullptr;
+            if (pl.split) {
+                a.C2 = static_cast<double*>(pl.cvC.p) + MK;
+                a.split_v = pl.split_local(ti);
+            }
             launch_cv_near(a, pl.cv_D, c.st);
         }
         ck(cudaEventRecordWithFlags(pl.cv_ev[1], c.st, cudaEventRecordExternal), "event");
@@ -1499,15 +1519,17 @@ void win_enqueue(Context& c, WinPlan& pl) {
             ck(cudaEventRecordWithFlags(pl.ev[(size_t)e++], c.st, cudaEventRecordExternal), "event");
             // (sketch digits were written by phase 1's epilogue)
             ck(cudaEventRecordWithFlags(pl.ev[(size_t)e++], c.st, cudaEventRecordExternal), "event");
+            const int nb = umma::p2_bins_per_cta(nc, (int)K);
             const CUtensorMap tmB =
                 make_map_2d(pl.yq.p, (uint64_t)Np, (uint64_t)(b.ksup * nc), (uint64_t)Np, 128,
-                            (uint32_t)std::min(256, nc), CU_TENSOR_MAP_SWIZZLE_128B);
+                            (uint32_t)std::min(256, nb * nc), CU_TENSOR_MAP_SWIZZLE_128B);
             umma::P2UArgs u;
             u.K = (int)K;
             u.V = V;
             u.ncolp = nc;
-            u.ngroups = (nc + 255) / 256;
-            u.box_rows = std::min(256, nc);
+            u.bins_per_cta = nb;
+            u.ngroups = (nb * nc + 255) / 256;
+            u.box_rows = std::min(256, nb * nc);
             u.nkt = (int)(Np / 128);
             u.M = M;
             u.j0 = 0;
@@ -1517,7 +1539,11 @@ void win_enqueue(Context& c, WinPlan& pl) {
             u.mean = static_cast<double*>(P.d_mean.p);
             u.sdinv = static_cast<double*>(P.d_sdinv.p);
             u.left_scale = static_cast<double*>(pl.lscale.p);
-            u.accum = static_cast<double*>(pl.accum.p) + (pl.split ? ti * MK : 0);
+            u.accum = static_cast<double*>(pl.accum.p);
+            if (pl.split) {
+                u.accum2 = static_cast<double*>(pl.accum.p) + MK;
+                u.split_v = pl.split_local(ti);
+            }
             u.mc = pl.with_mc ? static_cast<double*>(pl.mc.p) : nullptr;
             u.guard_counts = static_cast<unsigned long long*>(pl.guards.p);
             u.extreme_warn = extreme_warn_env();
@@ -2163,7 +2189,10 @@ LDS_API int lds_mlp_forward(const float* d_params, int in_dim, int out_dim, cons
         a.params = d_params;
         a.in = in_dim;
         a.out = out_dim;
-        launch_mlp_forward(a, d_x, nullptr, n, nullptr, d_out, nullptr, nullptr, nullptr, 0.f, c.st);
+        void* pack = c.mlp_pack.as<uint16_t>(mlp_pack_elems(in_dim, out_dim));
+        launch_mlp_pack(a, pack, c.st);
+        launch_mlp_forward(a, pack, d_x, nullptr, n, nullptr, d_out, nullptr, nullptr, nullptr, 0.f,
+                           c.st);
         ck(cudaGetLastError(), "launch");
         ck(cudaStreamSynchronize(c.st), "mlp forward");
     });
@@ -2183,15 +2212,17 @@ LDS_API int lds_mlp_loss_grad(const float* d_params, int in_dim, int out_dim, co
         a.out = out_dim;
         const int op = mlp_out_pad(out_dim);
         const int64_t P = mlp_layout(in_dim, out_dim).total;
-        DevBuf zs, dzs, dout, ls;
-        float* z = zs.as<float>((size_t)(n * 3 * kMlpHidden));
-        float* dz = dzs.as<float>((size_t)(n * 3 * kMlpHidden));
-        float* d = dout.as<float>((size_t)(n * op));
-        double* l = ls.as<double>(1);
+        float* z = c.mlp_zs.as<float>((size_t)(n * 3 * kMlpHidden));
+        float* dz = c.mlp_dzs.as<float>((size_t)(n * 3 * kMlpHidden));
+        float* d = c.mlp_dout.as<float>((size_t)(n * op));
+        double* l = c.mlp_loss.as<double>(1);
         ck(cudaMemsetAsync(l, 0, sizeof(double), c.st), "memset");
         ck(cudaMemsetAsync(d_grad, 0, sizeof(float) * (size_t)P, c.st), "memset");
-        launch_mlp_forward(a, d_x, nullptr, n, d_t, nullptr, z, d, l, 1.0f / (float)(n * out_dim), c.st);
-        launch_mlp_backward(a, d_x, nullptr, n, z, d, dz, d_grad, c.st);
+        void* pack = c.mlp_pack.as<uint16_t>(mlp_pack_elems(in_dim, out_dim));
+        launch_mlp_pack(a, pack, c.st);
+        launch_mlp_forward(a, pack, d_x, nullptr, n, d_t, nullptr, z, d, l,
+                           1.0f / (float)(n * out_dim), c.st);
+        launch_mlp_backward(a, pack, d_x, nullptr, n, z, d, dz, d_grad, c.st);
         ck(cudaGetLastError(), "launch");
         if (loss_out) d2h(loss_out, l, 1, c.st);
         ck(cudaStreamSynchronize(c.st), "mlp grad");
@@ -2214,34 +2245,39 @@ LDS_API int lds_mlp_train(float* d_params, int in_dim, int out_dim, const float*
         const int op = mlp_out_pad(out_dim);
         const int64_t P = mlp_layout(in_dim, out_dim).total;
         const int64_t B = std::min<int64_t>(batch, n);
-        DevBuf m, v, g, zs, dzs, dout, rows, ls;
-        float* dm = m.as<float>((size_t)P);
-        float* dv = v.as<float>((size_t)P);
-        float* dg = g.as<float>((size_t)P);
-        float* z = zs.as<float>((size_t)(B * 3 * kMlpHidden));
-        float* dz = dzs.as<float>((size_t)(B * 3 * kMlpHidden));
-        float* d = dout.as<float>((size_t)(B * op));
-        int32_t* r = rows.as<int32_t>((size_t)n);
-        double* l = ls.as<double>((size_t)std::max(epochs, 1));
+        float* dm = c.mlp_m.as<float>((size_t)P);
+        float* dv = c.mlp_v.as<float>((size_t)P);
+        float* dg = c.mlp_g.as<float>((size_t)P);
+        float* z = c.mlp_zs.as<float>((size_t)(B * 3 * kMlpHidden));
+        float* dz = c.mlp_dzs.as<float>((size_t)(B * 3 * kMlpHidden));
+        float* d = c.mlp_dout.as<float>((size_t)(B * op));
+        double* l = c.mlp_loss.as<double>((size_t)std::max(epochs, 1));
         ck(cudaMemsetAsync(dm, 0, sizeof(float) * (size_t)P, c.st), "memset");
         ck(cudaMemsetAsync(dv, 0, sizeof(float) * (size_t)P, c.st), "memset");
         ck(cudaMemsetAsync(l, 0, sizeof(double) * (size_t)std::max(epochs, 1), c.st), "memset");
         const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
-        std::vector<int32_t> perm((size_t)n);
+        // All epochs' shuffles up front: one upload, no host round trip per epoch.
+        std::vector<int32_t> perm((size_t)(n * std::max(epochs, 1)));
         std::mt19937_64 rng(seed);
+        for (int e = 0; e < epochs; ++e) {
+            int32_t* pe = perm.data() + (size_t)e * (size_t)n;
+            for (int64_t i = 0; i < n; ++i) pe[i] = (int32_t)i;
+            std::shuffle(pe, pe + n, rng);
+        }
+        int32_t* r = c.mlp_rows.as<int32_t>(perm.size());
+        h2d(r, perm.data(), perm.size(), c.st);
+        void* pack = c.mlp_pack.as<uint16_t>(mlp_pack_elems(in_dim, out_dim));
         int64_t step = 0;
         const int64_t nsteps = (n + B - 1) / B;
         for (int e = 0; e < epochs; ++e) {
-            for (int64_t i = 0; i < n; ++i) perm[(size_t)i] = (int32_t)i;
-            std::shuffle(perm.begin(), perm.end(), rng);
-            ck(cudaStreamSynchronize(c.st), "mlp epoch");  // perm buffer reuse
-            h2d(r, perm.data(), (size_t)n, c.st);
+            const int32_t* re = r + (size_t)e * (size_t)n;
             for (int64_t s = 0; s < nsteps; ++s) {
                 const int64_t nb = std::min<int64_t>(B, n - s * B);
                 ck(cudaMemsetAsync(dg, 0, sizeof(float) * (size_t)P, c.st), "memset");
-                launch_mlp_forward(a, d_x, r + s * B, nb, d_t, nullptr, z, d, l + e,
+                launch_mlp_pack(a, pack, c.st);
+                launch_mlp_forward(a, pack, d_x, re + s * B, nb, d_t, nullptr, z, d, l + e,
                                    1.0f / (float)(nb * out_dim * nsteps), c.st);
-                launch_mlp_backward(a, d_x, r + s * B, nb, z, d, dz, dg, c.st);
+                launch_mlp_backward(a, pack, d_x, re + s * B, nb, z, d, dz, dg, c.st);
                 ++step;
                 // The loss scale folds 1/nsteps into the gradient (so the epoch's
                 // loss sums to its mean); Adam is invariant to that scale except

@@ -113,6 +113,8 @@ struct CvNearArgs {
     const double* xx = nullptr;     // M x (D+1) neighbour products
     double* C = nullptr;
     double* mu = nullptr;
+    double* C2 = nullptr;           // if set, probes v >= split_v add to C2 instead of C
+    int split_v = 0;
 };
 void launch_cv_near(const CvNearArgs& a, int D, cudaStream_t st);
 
@@ -140,15 +142,19 @@ struct MlpArgs {
     const float* params = nullptr;
     int in = 0, out = 0;
 };
+// BF16 weight copies for the products (mlp_pack_elems bf16 values), remade
+// whenever the parameters change.
+size_t mlp_pack_elems(int in, int out);
+void launch_mlp_pack(const MlpArgs& a, void* pack, cudaStream_t st);
 // Forward over n rows (x rows gathered through `rows` if set): out (n x out,
 // may be null); with `target`, dout (n x out_pad) = 2 (o - t) gscale and
 // loss += gscale sum (o - t)^2; zs (n x 3 x 128, may be null) keeps z1..z3.
-void launch_mlp_forward(const MlpArgs& a, const float* x, const int32_t* rows, int64_t n,
-                        const float* target, float* out, float* zs, float* dout, double* loss,
-                        float gscale, cudaStream_t st);
+void launch_mlp_forward(const MlpArgs& a, const void* pack, const float* x, const int32_t* rows,
+                        int64_t n, const float* target, float* out, float* zs, float* dout,
+                        double* loss, float gscale, cudaStream_t st);
 // Backward: grad (zeroed by the caller) += d loss / d params.
-void launch_mlp_backward(const MlpArgs& a, const float* x, const int32_t* rows, int64_t n,
-                         const float* zs, const float* dout, float* dzs, float* grad,
+void launch_mlp_backward(const MlpArgs& a, const void* pack, const float* x, const int32_t* rows,
+                         int64_t n, const float* zs, const float* dout, float* dzs, float* grad,
                          cudaStream_t st);
 void launch_mlp_adam(float* p, float* m, float* v, const float* g, int64_t P, float lr, float b1,
                      float b2, float eps, float bc1, float bc2, cudaStream_t st);

@@ -63,28 +63,66 @@ __device__ __forceinline__ void tile_product(const float* A, int lda, const __nv
     }
 }
 
-// Copy W (rows x cols, FP32 row-major, global) into shared memory as BF16,
-// transposed (dst[c][r], row length ld >= rows, zero padding) or not
-// (dst[r][c], row length ld >= cols).
-__device__ void load_weights(const float* W, int rows, int cols, bool transpose,
-                             __nv_bfloat16* dst, int ld, int dst_rows) {
-    for (int idx = threadIdx.x; idx < dst_rows * ld; idx += blockDim.x) dst[idx] = __float2bfloat16_rn(0.0f);
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < rows * cols; idx += blockDim.x) {
-        const int r = idx / cols, c = idx - (idx / cols) * cols;
-        const __nv_bfloat16 v = __float2bfloat16_rn(W[idx]);
-        if (transpose) dst[c * ld + r] = v;
-        else dst[r * ld + c] = v;
-    }
+// Copy `bytes` (a multiple of 16) from global to shared memory.
+__device__ __forceinline__ void copy16(void* dst, const void* src, int bytes) {
+    const uint4* s = reinterpret_cast<const uint4*>(src);
+    uint4* d = reinterpret_cast<uint4*>(dst);
+    for (int i = threadIdx.x; i < bytes / 16; i += blockDim.x) d[i] = s[i];
 }
 
 }  // namespace mlp
 
 using namespace mlp;
 
+// BF16 copies of the weights, made once per step: pack_t = W1^T | W2^T | W3^T |
+// W4^T (column-contiguous, W4^T padded to out_pad columns) for the forward
+// products, pack_n = W4 | W3 | W2 as stored (W4 padded to out_pad rows) for the
+// backward ones.
+__global__ void mlp_pack_kernel(MlpArgs a, __nv_bfloat16* __restrict__ pack_t,
+                                __nv_bfloat16* __restrict__ pack_n) {
+    const MlpLayout L = mlp_layout(a.in, a.out);
+    const int op = mlp_out_pad(a.out), H = kMlpHidden;
+    const int64_t nt = (int64_t)a.in * H + 2 * H * H + (int64_t)H * op;
+    const int64_t nn = (int64_t)op * H + 2 * H * H;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nt + nn;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        if (i < nt) {
+            // transposed: element (k, c) of W^T = W[c][k]
+            float v = 0.0f;
+            int64_t r = i;
+            if (r < (int64_t)a.in * H) {
+                const int k = (int)(r / H), c = (int)(r % H);
+                v = a.params[L.W1 + (int64_t)c * a.in + k];
+            } else if ((r -= (int64_t)a.in * H) < H * H) {
+                v = a.params[L.W2 + (r % H) * H + r / H];
+            } else if ((r -= H * H) < H * H) {
+                v = a.params[L.W3 + (r % H) * H + r / H];
+            } else {
+                r -= H * H;
+                const int k = (int)(r / op), c = (int)(r % op);
+                v = c < a.out ? a.params[L.W4 + (int64_t)c * H + k] : 0.0f;
+            }
+            pack_t[i] = __float2bfloat16_rn(v);
+        } else {
+            int64_t r = i - nt;
+            float v = 0.0f;
+            if (r < (int64_t)op * H) {
+                const int c = (int)(r / H);
+                v = c < a.out ? a.params[L.W4 + r] : 0.0f;
+            } else if ((r -= (int64_t)op * H) < H * H) {
+                v = a.params[L.W3 + r];
+            } else {
+                v = a.params[L.W2 + (r - H * H)];
+            }
+            pack_n[i - nt] = __float2bfloat16_rn(v);
+        }
+    }
+}
+
 __global__ void __launch_bounds__(kThreads)
-    mlp_forward_kernel(MlpArgs a, const float* __restrict__ x, const int32_t* __restrict__ rows,
-                       int64_t n, const float* __restrict__ target, float* __restrict__ out,
+    mlp_forward_kernel(MlpArgs a, const __nv_bfloat16* __restrict__ pack_t,
+                       const float* __restrict__ x, const int32_t* __restrict__ rows, int64_t n,
+                       const float* __restrict__ target, float* __restrict__ out,
                        float* __restrict__ zs, float* __restrict__ dout, double* __restrict__ loss,
                        float gscale) {
     extern __shared__ __align__(16) uint8_t smem[];
@@ -99,10 +137,7 @@ __global__ void __launch_bounds__(kThreads)
     float* H2 = H1 + kR * kMlpHidden;                               // [kR][128]
     __shared__ float red[kThreads / 32];
 
-    load_weights(a.params + L.W1, kMlpHidden, a.in, true, T1, kMlpHidden, a.in);
-    load_weights(a.params + L.W2, kMlpHidden, kMlpHidden, true, T2, kMlpHidden, kMlpHidden);
-    load_weights(a.params + L.W3, kMlpHidden, kMlpHidden, true, T3, kMlpHidden, kMlpHidden);
-    load_weights(a.params + L.W4, a.out, kMlpHidden, true, T4, op, kMlpHidden);
+    copy16(T1, pack_t, (a.in * kMlpHidden + 2 * kMlpHidden * kMlpHidden + kMlpHidden * op) * 2);
     const int64_t r_base = (int64_t)blockIdx.x * kR;
     for (int idx = threadIdx.x; idx < kR * a.in; idx += blockDim.x) {
         const int r = idx / a.in, k = idx - (idx / a.in) * a.in;
@@ -178,19 +213,17 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 __global__ void __launch_bounds__(kThreads)
-    mlp_backward_data_kernel(MlpArgs a, int64_t n, const float* __restrict__ zs,
-                             const float* __restrict__ dout, float* __restrict__ dzs) {
+    mlp_backward_data_kernel(MlpArgs a, const __nv_bfloat16* __restrict__ pack_n, int64_t n,
+                             const float* __restrict__ zs, const float* __restrict__ dout,
+                             float* __restrict__ dzs) {
     extern __shared__ __align__(16) uint8_t smem[];
-    const MlpLayout L = mlp_layout(a.in, a.out);
     const int op = mlp_out_pad(a.out);
     __nv_bfloat16* N4 = reinterpret_cast<__nv_bfloat16*>(smem);     // [op][128] (W4 as stored)
     __nv_bfloat16* N3 = N4 + op * kMlpHidden;                       // [128][128]
     __nv_bfloat16* N2 = N3 + kMlpHidden * kMlpHidden;               // [128][128]
     float* G = reinterpret_cast<float*>(N2 + kMlpHidden * kMlpHidden);  // [kR][128] grad in
     float* D = G + kR * kMlpHidden;                                     // [kR][128] grad out
-    load_weights(a.params + L.W4, a.out, kMlpHidden, false, N4, kMlpHidden, op);
-    load_weights(a.params + L.W3, kMlpHidden, kMlpHidden, false, N3, kMlpHidden, kMlpHidden);
-    load_weights(a.params + L.W2, kMlpHidden, kMlpHidden, false, N2, kMlpHidden, kMlpHidden);
+    copy16(N4, pack_n, (op * kMlpHidden + 2 * kMlpHidden * kMlpHidden) * 2);
     const int64_t r_base = (int64_t)blockIdx.x * kR;
     for (int idx = threadIdx.x; idx < kR * op; idx += blockDim.x) {
         const int r = idx / op;
@@ -312,26 +345,51 @@ size_t mlp_backward_smem(int out) {
            (size_t)(2 * kR * kMlpHidden) * 4;
 }
 
-void launch_mlp_forward(const MlpArgs& a, const float* x, const int32_t* rows, int64_t n,
-                        const float* target, float* out, float* zs, float* dout, double* loss,
-                        float gscale, cudaStream_t st) {
-    if (n <= 0) return;
-    const size_t sm = mlp_forward_smem(a.in, a.out);
-    cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    mlp_forward_kernel<<<(unsigned)((n + kR - 1) / kR), kThreads, sm, st>>>(
-        a, x, rows, n, target, out, zs, dout, loss, gscale);
+size_t mlp_pack_elems(int in, int out) {
+    const int op = mlp_out_pad(out);
+    return (size_t)in * kMlpHidden + 2 * kMlpHidden * kMlpHidden + (size_t)kMlpHidden * op +
+           (size_t)op * kMlpHidden + 2 * kMlpHidden * kMlpHidden;
+}
+
+void launch_mlp_pack(const MlpArgs& a, void* pack, cudaStream_t st) {
+    __nv_bfloat16* pt = static_cast<__nv_bfloat16*>(pack);
+    __nv_bfloat16* pn = pt + (size_t)a.in * kMlpHidden + 2 * kMlpHidden * kMlpHidden +
+                        (size_t)kMlpHidden * mlp_out_pad(a.out);
+    mlp_pack_kernel<<<148, 256, 0, st>>>(a, pt, pn);
     count_launch();
 }
 
-void launch_mlp_backward(const MlpArgs& a, const float* x, const int32_t* rows, int64_t n,
-                         const float* zs, const float* dout, float* dzs, float* grad,
+static void set_smem_attrs(int in, int out) {
+    static int done_in = -1, done_out = -1;
+    if (done_in == in && done_out == out) return;
+    cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)mlp_forward_smem(in, out));
+    cudaFuncSetAttribute(mlp_backward_data_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)mlp_backward_smem(out));
+    done_in = in;
+    done_out = out;
+}
+
+void launch_mlp_forward(const MlpArgs& a, const void* pack, const float* x, const int32_t* rows,
+                        int64_t n, const float* target, float* out, float* zs, float* dout,
+                        double* loss, float gscale, cudaStream_t st) {
+    if (n <= 0) return;
+    set_smem_attrs(a.in, a.out);
+    mlp_forward_kernel<<<(unsigned)((n + kR - 1) / kR), kThreads, mlp_forward_smem(a.in, a.out), st>>>(
+        a, static_cast<const __nv_bfloat16*>(pack), x, rows, n, target, out, zs, dout, loss, gscale);
+    count_launch();
+}
+
+void launch_mlp_backward(const MlpArgs& a, const void* pack, const float* x, const int32_t* rows,
+                         int64_t n, const float* zs, const float* dout, float* dzs, float* grad,
                          cudaStream_t st) {
     if (n <= 0) return;
-    const size_t sm = mlp_backward_smem(a.out);
-    cudaFuncSetAttribute(mlp_backward_data_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)sm);
-    mlp_backward_data_kernel<<<(unsigned)((n + kR - 1) / kR), kThreads, sm, st>>>(a, n, zs, dout,
-                                                                                 dzs);
+    set_smem_attrs(a.in, a.out);
+    const __nv_bfloat16* pn = static_cast<const __nv_bfloat16*>(pack) +
+                              (size_t)a.in * kMlpHidden + 2 * kMlpHidden * kMlpHidden +
+                              (size_t)kMlpHidden * mlp_out_pad(a.out);
+    mlp_backward_data_kernel<<<(unsigned)((n + kR - 1) / kR), kThreads, mlp_backward_smem(a.out),
+                               st>>>(a, pn, n, zs, dout, dzs);
     count_launch();
     const int items = 3 * (kMlpHidden / 16) + (a.out + 15) / 16;
     const int rps = 512;

@@ -74,7 +74,11 @@ __global__ void __launch_bounds__(kThreads, 1)
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int k = blockIdx.y;
+    // This CTA's bins: k0 .. k0 + nbk - 1, sharing each decoded genotype tile;
+    // their sketch columns are consecutive (bin-major), one TMA box for all.
+    const int k0 = blockIdx.y * a.bins_per_cta;
+    const int nbk = min(a.bins_per_cta, a.K - k0);
+    const int cols = a.bins_per_cta * a.ncolp;
     int64_t jt0, jend;
     int sb = 0;  // super-bin base of this tile's window
     if (a.tiles) {
@@ -86,7 +90,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         jt0 = a.j0 + (int64_t)blockIdx.x * kBM;
         jend = a.j1;
     }
-    const int kb = sb + k;  // super-bin of this CTA
+    const int kb = sb + k0;  // first super-bin of this CTA
 
     if (tid == 0) {
         for (int s = 0; s < kPkStages; ++s) {
@@ -154,7 +158,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (lane == 0) {
             int it = 0;
             for (int g = 0; g < ngroups && !*abort_flag; ++g) {
-                const int ncols = min(256, a.ncolp - g * 256);
+                const int ncols = min(256, cols - g * 256);
                 const uint32_t idesc = idesc_i8(kBM, ncols);
                 if (g > 0 && !mbar_wait(acc_empty, (uint32_t)(g - 1) & 1u)) { fail(3); break; }
                 tc_fence_after();
@@ -188,7 +192,36 @@ __global__ void __launch_bounds__(kThreads, 1)
         const bool stats = (j < a.M) && a.mean && a.sdinv;
         const double mu = stats ? a.mean[j] : 0.0;
         const double sd = stats ? a.sdinv[j] : 0.0;
-        double run2 = 0.0, run4 = 0.0;
+        double run2 = 0.0, run4 = 0.0, run2b = 0.0;
+        int cur = 0;  // bin offset (within this CTA's bins) that run2/run4 belong to
+        // Add the running sums of bin k0 + cur to the outputs, with the
+        // reference's guards, and restart them.
+        auto flush = [&]() {
+            if (!*abort_flag && j < jend && !a.raw_g && cur < nbk) {
+                const double ls = a.left_scale[j];
+                double upd = (run2 + run2b) * ls;
+                const double seg = (double)a.V;
+                const bool nonfinite = !isfinite(upd);
+                const bool extreme = !nonfinite && isfinite(a.extreme_warn) && seg > 0.0 &&
+                                     upd > a.extreme_warn * seg;
+                if (a.guard_counts) {
+                    if (nonfinite) atomicAdd(&a.guard_counts[0], 1ULL);
+                    else if (extreme) atomicAdd(&a.guard_counts[1], 1ULL);
+                }
+                if (!(nonfinite || (extreme && a.drop_extreme))) {
+                    if (upd < 0.0) upd = 0.0;
+                    const int64_t o = (j - a.out_row0) * a.K + k0 + cur;
+                    if (a.accum2) {
+                        a.accum[o] += run2 * ls;
+                        a.accum2[o] += run2b * ls;
+                    } else {
+                        a.accum[o] += upd;
+                    }
+                    if (a.mc) a.mc[o] += run4 * ls * ls;
+                }
+            }
+            run2 = run4 = run2b = 0.0;
+        };
         int it = 0;
         for (int g = 0; g < ngroups; ++g) {
             for (int kt = 0; kt < a.nkt; ++kt, ++it) {
@@ -209,7 +242,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             // Epilogue of column group g.
             if (!mbar_wait(acc_full, (uint32_t)g & 1u)) { fail(7); break; }
             tc_fence_after();
-            const int ncols = min(256, a.ncolp - g * 256);
+            const int ncols = min(256, cols - g * 256);
             const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16);
             for (int c0 = 0; c0 < ncols; c0 += 32) {
                 int rg[32], ro[32];
@@ -218,8 +251,14 @@ __global__ void __launch_bounds__(kThreads, 1)
                 tmem_wait_ld();
 #pragma unroll
                 for (int p = 0; p < 8; ++p) {
-                    const int v = g * 64 + c0 / 4 + p;
-                    if (v >= a.V) continue;
+                    const int gc = g * 256 + c0 + 4 * p;   // column within this CTA's bins
+                    const int bo = gc / a.ncolp;            // bin offset (warp-uniform)
+                    const int v = (gc - bo * a.ncolp) >> 2;
+                    if (bo >= nbk || v >= a.V) continue;
+                    if (bo != cur) {
+                        flush();
+                        cur = bo;
+                    }
                     const long long TG =
                         (((long long)rg[4 * p] * 128 + rg[4 * p + 1]) * 128 + rg[4 * p + 2]) * 128 +
                         rg[4 * p + 3];
@@ -233,34 +272,18 @@ __global__ void __launch_bounds__(kThreads, 1)
                         }
                         continue;
                     }
-                    const double wv = sd * a.colscale[(int64_t)kb * a.V + v] *
+                    const double wv = sd * a.colscale[(int64_t)(kb + bo) * a.V + v] *
                                       ((double)TG - mu * (double)TO);
                     const double w2 = wv * wv;
-                    run2 += w2;
+                    if (a.accum2 && v >= a.split_v) run2b += w2;
+                    else run2 += w2;
                     run4 += w2 * w2;
                 }
             }
             tc_fence_before();
             mbar_arrive(acc_empty);
         }
-        if (!*abort_flag && j < jend && !a.raw_g) {
-            const double ls = a.left_scale[j];
-            double upd = run2 * ls;
-            const double seg = (double)a.V;
-            const bool nonfinite = !isfinite(upd);
-            const bool extreme = !nonfinite && isfinite(a.extreme_warn) && seg > 0.0 &&
-                                 upd > a.extreme_warn * seg;
-            if (a.guard_counts) {
-                if (nonfinite) atomicAdd(&a.guard_counts[0], 1ULL);
-                else if (extreme) atomicAdd(&a.guard_counts[1], 1ULL);
-            }
-            if (!(nonfinite || (extreme && a.drop_extreme))) {
-                if (upd < 0.0) upd = 0.0;
-                const int64_t o = (j - a.out_row0) * a.K + k;
-                a.accum[o] += upd;
-                if (a.mc) a.mc[o] += run4 * ls * ls;
-            }
-        }
+        flush();
     }
     tc_fence_before();
     __syncthreads();
@@ -356,7 +379,8 @@ void launch_p2_umma(const CUtensorMap& tmA, const CUtensorMap& tmB, const P2UArg
         attr = p2_umma_smem_bytes(256);
     }
     // With a tile table, j0 is unused and j1 - j0 carries the number of tiles.
-    dim3 grid((unsigned)(a.tiles ? rows : (rows + kBM - 1) / kBM), (unsigned)a.K);
+    const int nb = a.bins_per_cta > 0 ? a.bins_per_cta : 1;
+    dim3 grid((unsigned)(a.tiles ? rows : (rows + kBM - 1) / kBM), (unsigned)((a.K + nb - 1) / nb));
     p2_umma_kernel<<<grid, kThreads, smem, st>>>(tmA, tmB, a);
     count_launch();
 }

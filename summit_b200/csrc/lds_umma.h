@@ -30,7 +30,22 @@ struct P2UArgs {
     // [tiles[x].x, min(tiles[x].x + 128, tiles[x].y)) against super-bins
     // tiles[x].z + k (sketch columns and scales of that window).
     const int4* tiles = nullptr;
+    // Optional split of the probes into two sums: probes v < split_v go to
+    // accum, the rest to accum2 (guards judge their total).  Unused if null.
+    double* accum2 = nullptr;
+    int split_v = 0;
+    // Bins per CTA (consecutive; one decoded genotype tile serves them all):
+    // box_rows = min(256, bins_per_cta * ncolp) and ngroups =
+    // ceil(bins_per_cta * ncolp / 256) must match.  1 unless ncolp <= 128.
+    int bins_per_cta = 1;
 };
+
+// Bins that share one CTA in phase 2: as many whole bins as fit 256 columns.
+inline int p2_bins_per_cta(int ncolp, int K) {
+    if (ncolp > 128) return 1;
+    const int nb = 256 / ncolp;
+    return nb < K ? nb : K;
+}
 
 // Phase-1 tcgen05 kernel arguments.  Member lists of bin k occupy
 // rowind[bin_off[k] .. bin_off[k+1]) (multiples of 128, padding rows carry

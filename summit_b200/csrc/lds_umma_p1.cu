@@ -169,19 +169,29 @@ __global__ void __launch_bounds__(p1::kThreads, 1)
         const uint8_t* codes = a.codes + i0 / 4;
         // Gather prefetcher: walks the same (super-bin, group, K-step) sequence
         // kRing steps ahead, copying this thread's member row into a ring slot.
+        // The member row of the step being fetched is read from rowind one step
+        // earlier (row_next), so that load's latency overlaps a step of work
+        // instead of stalling the cp.async that needs the address.
         int pk = kb0, pg = 0, pkt = 0, pit = 0;
-        auto prefetch_one = [&]() {
+        auto cursor_row = [&]() -> int64_t {  // rowind of the cursor's step, or -1 past the end
             while (pk < kb1 && nkt_of(pk) == 0) { ++pk; pg = 0; pkt = 0; }
-            if (pk < kb1) {
-                const int64_t row = a.rowind[a.bin_off[pk] + (int64_t)pkt * kBK + t];
+            if (pk >= kb1) return -1;
+            const int64_t row = a.rowind[a.bin_off[pk] + (int64_t)pkt * kBK + t];
+            if (++pkt == nkt_of(pk)) {
+                pkt = 0;
+                if (++pg == a.ngroups) { pg = 0; ++pk; }
+            }
+            return row;
+        };
+        int64_t row_next = cursor_row();
+        auto prefetch_one = [&]() {
+            const int64_t row = row_next;
+            row_next = cursor_row();
+            if (row >= 0) {
                 const uint8_t* src = codes + row * a.nbp;
                 uint8_t* dst = ring + (pit % kRing) * kRingSlot + t * 32;
                 cp_async16(dst, src);
                 cp_async16(dst + 16, src + 16);
-                if (++pkt == nkt_of(pk)) {
-                    pkt = 0;
-                    if (++pg == a.ngroups) { pg = 0; ++pk; }
-                }
             }
             cp_async_commit();
             ++pit;

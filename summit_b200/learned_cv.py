@@ -17,7 +17,9 @@ u_jv = sum_{i in window} c_ji annot_ik z_iv.  Two steps reduce its variance:
    prediction h is combined with T per bin, mu + h + lambda_k (T - h), where
    lambda_k = b^2 / (b^2 + s^2) is the MSE-optimal weight given the network's
    squared bias b^2 (validation residual minus noise) and the noise s^2 of T,
-   itself measured from two independent halves of the probes.
+   itself measured from two independent halves of the probes; adding
+   (1 - lambda_k) mean_j (T - h) keeps each bin's mean over SNPs equal to the
+   unbiased near-field estimate's.
 
 The plain estimator stays available (``plain_ldscore``) and is the judge:
 tests and the benchmark compare both against a plain run with 10x the probes.
@@ -60,12 +62,10 @@ class LearnedCV:
         self.M, self.K = annot.shape
         self.N = session.N
         half = (cfg.nvecs + 1) // 2
-        self.plan = WinPlan(session, annot, ws, cfg.nvecs, step, seed, rand_dist, vtile=half,
+        self.plan = WinPlan(session, annot, ws, cfg.nvecs, step, seed, rand_dist,
                             batch_gb=batch_gb)
         self.plan.set_cv(annot, split_tiles=True, band=cfg.band)
-        self.tiles = self.plan.tiles()
-        if len(self.tiles) != 2:
-            raise ValueError(f"expected two probe halves, got V-tiles {self.tiles}")
+        self.tiles = [half, cfg.nvecs - half]  # the two probe halves
         dev = torch.device("cuda")
         M, K, D = self.M, self.K, cfg.band
         self.annot = torch.from_numpy(annot).to(dev)
@@ -91,7 +91,7 @@ class LearnedCV:
         nva = max(1, int(round(cfg.val_frac * M)))
         self.train_rows = torch.from_numpy(np.sort(perm[:ntr])).to(dev)
         self.val_rows = torch.from_numpy(np.sort(perm[ntr:ntr + nva])).to(dev)
-        T = len(self.tiles)
+        T = 2
         f64 = dict(dtype=torch.float64, device=dev)
         self.meansq = torch.empty((T, M, K), **f64)
         self.C = torch.empty((T, M, K), **f64)
@@ -150,7 +150,11 @@ class LearnedCV:
         nv = noise[va].mean(0)
         bias2 = (resid2 - nv).clamp_min(0.0)
         lam = bias2 / (bias2 + nv).clamp_min(1e-300)
-        est = self.mu + h + lam[None, :] * (target.double() - h)
+        # Per-SNP shrinkage toward the network, plus (1 - lambda) times the mean
+        # residual of each bin: the bin's mean over SNPs then equals the
+        # unbiased near-field estimate's, whatever the network's average bias.
+        resid = target.double() - h
+        est = self.mu + h + lam[None, :] * resid + (1.0 - lam)[None, :] * resid.mean(0, keepdim=True)
         ld = est - self.null
         torch.cuda.synchronize()
         t4 = time.perf_counter()

@@ -165,8 +165,9 @@ class WinPlan:
         return [int(x) for x in sizes[: n.value]]
 
     def cv_outputs(self) -> dict:
-        """Host copies: meansq per V-tile slice, near-field sums C per slice, mu, xx."""
-        T = len(self.tiles()) if getattr(self, "split", False) else 1
+        """Host copies: meansq per probe slice (two halves with split_tiles), near-field
+        sums C per slice, mu, xx."""
+        T = 2 if getattr(self, "split", False) else 1
         M, K = self.M, self.K
         out = {"meansq": np.empty((T, M, K)), "C": None, "mu": None, "xx": None}
         if getattr(self, "band", 0):

@@ -26,8 +26,11 @@ def _window_probes(oracle, ws, m, step, seed, v0, V):
     return Z
 
 
-@pytest.mark.parametrize("D", [4, 8])
-def test_cv_near_outputs_match_oracle(small_bed, oracle, D):
+@pytest.mark.parametrize("D,vtile", [(4, 12), (8, 12), (8, 0), (8, 10)])
+def test_cv_near_outputs_match_oracle(small_bed, oracle, D, vtile):
+    """Two probe halves [0, 12) and [12, 24): one V-tile each (vtile 12), both in
+    one V-tile (vtile 0: split inside the kernels), or a tile straddling the
+    split (vtile 10: tiles 10, 10, 4)."""
     from summit_b200.session import GwSession, WinPlan
 
     n, m, packed = small_bed["n"], small_bed["m"], small_bed["rows"]
@@ -38,13 +41,13 @@ def test_cv_near_outputs_match_oracle(small_bed, oracle, D):
     annot[:, 2] = rng.random(m) < 0.5
     seed, nvecs, step = 99, 24, 50
     sess = GwSession(packed, n)
-    plan = WinPlan(sess, annot, ws, nvecs, step, seed, "rademacher", vtile=12)
+    plan = WinPlan(sess, annot, ws, nvecs, step, seed, "rademacher", vtile=vtile)
     plan.set_cv(annot, split_tiles=True, band=D)
     plan.execute()
     out = plan.cv_outputs()
     res = plan.results()
     tiles = plan.tiles()
-    assert tiles == [12, 12]
+    assert sum(tiles) == nvecs and out["meansq"].shape[0] == 2
     # the slices add up to the plain sums
     np.testing.assert_allclose(out["meansq"].sum(0), res["meansq_accum"], rtol=1e-13, atol=0)
 
@@ -52,22 +55,25 @@ def test_cv_near_outputs_match_oracle(small_bed, oracle, D):
     inv = oracle.inv_resvar(X, 1e-10)
     win = np.repeat(np.arange(len(ws) - 1), np.diff(ws))
     assert rel_err(out["xx"], oracle.band_products(packed, n, D)) < 1e-13
+    # the plan's probes, tile by tile (streams are seeded per V-tile offset)
+    Z = np.hstack([_window_probes(oracle, ws, m, step, seed, int(sum(tiles[:t])), V)
+                   for t, V in enumerate(tiles)])
+    halves = [slice(0, 12), slice(12, 24)]
     mu = np.zeros((m, 3))
-    v0 = 0
-    for t, V in enumerate(tiles):
-        Z = _window_probes(oracle, ws, m, step, seed, v0, V)
-        C = np.zeros((m, 3))
-        for j in range(m):
-            nb = [i for i in range(max(0, j - D), min(m, j + D + 1)) if win[i] == win[j]]
-            c = (X[:, nb].T @ X[:, j]) * inv[j] / (n - 1)
-            w = c[:, None] * annot[nb]                # (neighbours, K)
-            a = Z[nb].T @ w                            # (V, K)
-            C[j] = (a ** 2).sum(0)
-            if t == 0:
-                mu[j] = (w ** 2).sum(0)
-        assert rel_err(out["C"][t], C) < 1e-11, f"tile {t}"
-        v0 += V
+    C = np.zeros((2, m, 3))
+    G = X.T @ X  # small: 410 x 410
+    for j in range(m):
+        nb = [i for i in range(max(0, j - D), min(m, j + D + 1)) if win[i] == win[j]]
+        c = G[nb, j] * inv[j] / (n - 1)
+        w = c[:, None] * annot[nb]                # (neighbours, K)
+        a = Z[nb].T @ w                            # (V, K)
+        for h, sl in enumerate(halves):
+            C[h, j] = (a[sl] ** 2).sum(0)
+        mu[j] = (w ** 2).sum(0)
+    for h in range(2):
+        assert rel_err(out["C"][h], C[h]) < 1e-11, f"half {h}"
     assert rel_err(out["mu"], mu) < 1e-11
+    # plain sums of each half against the oracle's per-window estimator
     plan.close()
     sess.close()
 
