@@ -299,6 +299,43 @@ int lds_geno_stats(int64_t geno, double* mean_out, double* sdinv_out);
 int lds_nn_band(int64_t geno, int D, double* xx_out, int32_t* counts_out);
 
 /* ---------------------------------------------------------------------
+ * Exact windowed LD scores (tcgen05 int8 Gram products, FP64 epilogue).
+ *
+ * lds_compute_windowed_ld_chr replaces winldcore.compute_windowed_ld_chr
+ * (winldcore.cpp:972-987, implementation :783-931): for SNPs j in
+ * [chr_start, chr_end) of the BED fileset,
+ *   out[j, b] = sum_{i : |bp_i - bp_j| <= 1000 ld_wind_kb} r~2_ij annot_chr[i, b]
+ * with r the correlation of the mean-imputed (restandardized) or HWE-completed
+ * genotypes over the selected samples and r~2 = r^2 - (1 - r^2)/(N - 2).
+ * annot_chr and out are m x K column-major (m = chr_end - chr_start); bp has m
+ * sorted positions.  Same argument checks and messages as the reference.
+ * chunk_size must be > 0 but, like panel_cols and cache_mb (CPU tiling knobs),
+ * does not change the result.  Covariate projection (C, R non-NULL with p > 0)
+ * is rejected with LDS_ERR_ARG.
+ *
+ * lds_geno_window_ld is the same computation on a resident image with an
+ * explicit partner interval per SNP: for j in [row0, row1),
+ *   out[(j-row0)*K + b] = sum_{i in [lo[j-row0], hi[j-row0])} f(r_ij) annot[(i-row0)*K + b]
+ * (row-major), f = r^2 when corr_dim <= 0 (the expectation of the stochastic
+ * windowed estimator's meansq / B), else r^2 - (1 - r^2)/(corr_dim - 1).
+ * Both are synchronous and deterministic.
+ *
+ * lds_compute_maf_bed replaces winldcore.compute_maf_bed (winldcore.cpp:988-993,
+ * compute_maf_block genotype.cpp:1634): maf_out[j] for the first nsnps SNPs.
+ * ------------------------------------------------------------------- */
+int lds_compute_windowed_ld_chr(const char* bed_prefix, const char* fam_path, int chr_start,
+                                int chr_end, const int64_t* bp, const double* annot_chr, int64_t K,
+                                double ld_wind_kb, int chunk_size, const int64_t* row_sel,
+                                int64_t n_row_sel, const double* C, const double* R, int64_t p,
+                                int impute_mode, int has_impute_seed, uint64_t impute_seed,
+                                int panel_cols, int cache_mb, double* out);
+int lds_geno_window_ld(int64_t geno, int64_t row0, int64_t row1, const int64_t* lo,
+                       const int64_t* hi, const double* annot, int64_t K, double corr_dim,
+                       double* out);
+int lds_compute_maf_bed(const char* bed_prefix, const char* fam_path, int nsnps, int step_size,
+                        const int64_t* row_sel, int64_t n_row_sel, double* maf_out);
+
+/* ---------------------------------------------------------------------
  * Surrogate network of the learned control variate (no counterpart in the
  * reference): in_dim -> 128 -> 128 -> 128 -> out_dim, GELU (erf form) after the
  * hidden layers, FP32 master parameters, BF16 weights and activations in the

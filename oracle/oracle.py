@@ -29,6 +29,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ORACLE_SO = HERE / "_build" / "liblds_oracle.so"
 REF_SO = HERE / "_ref" / "libref_gwld.so"
+REF_WIN_SO = HERE / "_ref" / "libref_winld.so"
 
 _p = C.c_void_p
 _i64 = C.c_int64
@@ -66,6 +67,53 @@ def band_counts(geno: np.ndarray, D: int) -> np.ndarray:
         out[: m - d, d, 2] = (o[a] * g[b]).sum(1)
         out[: m - d, d, 3] = (o[a] * o[b]).sum(1)
     return out
+
+
+def bp_window_bounds(bp: np.ndarray, ld_wind_kb: float) -> tuple[np.ndarray, np.ndarray]:
+    """Per SNP j the partner interval [lo_j, hi_j) of |bp_i - bp_j| <= W
+    (W = 1000 ld_wind_kb), as winldcore.cpp:434-442 (outside_bp_window) and
+    :596-606 (compute_block_left) define the window on sorted positions."""
+    bp = np.asarray(bp, dtype=np.int64)
+    w = float(ld_wind_kb) * 1000.0
+    lo = np.searchsorted(bp.astype(np.float64), bp - w, side="left")
+    hi = np.searchsorted(bp.astype(np.float64), bp + w, side="right")
+    return lo.astype(np.int64), hi.astype(np.int64)
+
+
+def windowed_ld_exact(X: np.ndarray, annot: np.ndarray, lo: np.ndarray, hi: np.ndarray,
+                      restandardize: bool, corr_dim: int | None) -> np.ndarray:
+    """Exact windowed LD scores (FP64, dense; small inputs only).
+
+    X: N x m standardized genotypes.  With ``restandardize`` each column is
+    recentred and rescaled to unit variance over the N rows (ddof 0), as
+    restandardize_cols_inplace (winldcore.cpp:215-267) does for mean
+    imputation; r = X^T X / N (accum_self_panel / accum_cross_panels,
+    :480-594); with ``corr_dim`` the unbiased r^2 - (1 - r^2)/(corr_dim - 1)
+    (:409-432), else plain r^2; pairs outside [lo_j, hi_j) are zeroed after
+    that (:434-478); LD = (f(r) o mask) annot."""
+    X = np.array(X, dtype=np.float64, order="F", copy=True)
+    n, m = X.shape
+    if restandardize:
+        for j in range(m):
+            col = X[:, j]
+            s, ss = col.sum(), (col * col).sum()
+            mean = s / n
+            v = ss - s * s / n
+            if -1e-12 < v < 0.0:
+                v = 0.0
+            inv = 1.0
+            if v > 0.0 and np.isfinite(v):
+                var = v / n
+                if var > 0.0 and np.isfinite(var):
+                    inv = 1.0 / np.sqrt(var)
+            X[:, j] = (col - mean) * inv
+    r = (X.T @ X) / n
+    f = r * r
+    if corr_dim is not None:
+        f = f - (1.0 - f) / float(corr_dim - 1)
+    idx = np.arange(m)
+    mask = (idx[None, :] >= lo[:, None]) & (idx[None, :] < hi[:, None])
+    return np.where(mask, f, 0.0) @ np.asarray(annot, dtype=np.float64)
 
 
 def compute_blocks(nsnps: int, step: int) -> list[tuple[int, int]]:
@@ -374,3 +422,54 @@ class Reference:
         ld = ms - (annot.sum(axis=0, dtype=np.float64) / float(nsel - ddof)).astype(dtype)[None, :]
         return {"ldscore": ld.astype(np.float64), "meansq_accum": meansq, "inv": inv,
                 "mc_aggregate_sumsq": mc_agg, "mc_per_snp_sumsq": mc_snp}
+
+
+class ReferenceWindowed:
+    """ctypes view of the reference's own winldcore.cpp, compiled unchanged."""
+
+    def __init__(self, path: Path = REF_WIN_SO):
+        if not path.exists():
+            raise RuntimeError(f"reference library missing: {path} (run `make -C oracle ref`)")
+        L = C.CDLL(str(path))
+        L.refw_last_error.restype = _str
+        L.refw_set_num_threads.argtypes = [_int]
+        L.refw_compute_windowed_ld_chr.argtypes = [
+            _str, _str, _int, _int, _p, _p, _i64, _dbl, _int, _p, _i64, _p, _p, _i64, _i64,
+            _str, _int, _u64, _int, _int, _p]
+        L.refw_compute_maf_bed.argtypes = [_str, _str, _int, _int, _p, _i64, _p]
+        self.lib = L
+
+    def _chk(self, rc):
+        if rc:
+            raise RuntimeError(self.lib.refw_last_error().decode())
+
+    def set_threads(self, n: int):
+        self.lib.refw_set_num_threads(int(n))
+
+    def compute_windowed_ld_chr(self, prefix, chr_start, chr_end, bp, annot, ld_wind_kb,
+                                chunk_size, row_sel=None, C=None, R=None, impute_mode="mean",
+                                impute_seed=None, panel_cols=0, cache_mb=-1):
+        m = chr_end - chr_start
+        bp = np.ascontiguousarray(bp, dtype=np.int64)
+        annot = np.asfortranarray(annot, dtype=np.float64)
+        rows = None if row_sel is None else np.ascontiguousarray(row_sel, dtype=np.int64)
+        Cf = None if C is None else np.asfortranarray(C, dtype=np.float64)
+        Rf = None if R is None else np.asfortranarray(R, dtype=np.float64)
+        out = np.empty((m, annot.shape[1]), dtype=np.float64, order="F")
+        self._chk(self.lib.refw_compute_windowed_ld_chr(
+            str(prefix).encode(), f"{prefix}.fam".encode(), chr_start, chr_end, _ptr(bp),
+            _ptr(annot), annot.shape[1], float(ld_wind_kb), int(chunk_size), _ptr(rows),
+            0 if rows is None else rows.size, _ptr(Cf), _ptr(Rf),
+            0 if Cf is None else Cf.shape[0], 0 if Cf is None else Cf.shape[1],
+            impute_mode.encode(), int(impute_seed is not None),
+            0 if impute_seed is None else int(impute_seed), int(panel_cols), int(cache_mb),
+            _ptr(out)))
+        return out
+
+    def compute_maf_bed(self, prefix, nsnps, step_size, row_sel=None):
+        rows = None if row_sel is None else np.ascontiguousarray(row_sel, dtype=np.int64)
+        out = np.empty(nsnps)
+        self._chk(self.lib.refw_compute_maf_bed(str(prefix).encode(), f"{prefix}.fam".encode(),
+                                                nsnps, step_size, _ptr(rows),
+                                                0 if rows is None else rows.size, _ptr(out)))
+        return out

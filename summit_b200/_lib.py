@@ -64,6 +64,10 @@ SIGNATURES: dict[str, tuple] = {
     "lds_geno_destroy": (_int, [_i64]),
     "lds_nn_band": (_int, [_i64, _int, _p, _p]),
     "lds_geno_stats": (_int, [_i64, _p, _p]),
+    "lds_geno_window_ld": (_int, [_i64, _i64, _i64, _p, _p, _p, _i64, _dbl, _p]),
+    "lds_compute_windowed_ld_chr": (_int, [_str, _str, _int, _int, _p, _p, _i64, _dbl, _int, _p,
+                                           _i64, _p, _p, _i64, _int, _int, _u64, _int, _int, _p]),
+    "lds_compute_maf_bed": (_int, [_str, _str, _int, _int, _p, _i64, _p]),
     "lds_gw_plan_create": (_int, [_i64, _p, _i64, _int, _int, _int, _u64, _int, _dbl, _int, _int,
                                   _p]),
     "lds_gw_plan_execute": (_int, [_i64]),

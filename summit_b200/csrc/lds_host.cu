@@ -1908,6 +1908,236 @@ LDS_API int lds_geno_stats(int64_t geno, double* mean_out, double* sdinv_out) {
     });
 }
 
+// ---------------------------------------------------------------------------
+// Exact windowed LD scores (compute_windowed_ld_chr_impl, winldcore.cpp:783-931)
+// ---------------------------------------------------------------------------
+// Per SNP the centering mean and rs = 1/sqrt(c_jj), c_jj = sum_obs (g - mu)^2,
+// from the exact code counts (after HWE completion when that mode is used).
+// The numerator Q nobs - S^2 is an exact integer.
+void pearson_stats(const Prepared& P, int64_t j0, int64_t j1, std::vector<double>& mu,
+                   std::vector<double>& rs) {
+    mu.assign((size_t)P.g.M, 0.0);
+    rs.assign((size_t)P.g.M, 0.0);
+    for (int64_t j = j0; j < j1; ++j) {
+        const SnpCounts& k = P.counts[(size_t)j];
+        const long long nobs = (long long)k.n[0] + k.n[1] + k.n[2];
+        const long long S = (long long)k.n[1] + 2LL * k.n[2];
+        const long long Q = (long long)k.n[1] + 4LL * k.n[2];
+        if (nobs <= 0) continue;
+        mu[(size_t)j] = (double)S / (double)nobs;
+        const long long num = Q * nobs - S * S;
+        if (num > 0) rs[(size_t)j] = 1.0 / std::sqrt((double)num / (double)nobs);
+    }
+}
+
+// LD[j, b] = sum_{i in [lo_j, hi_j)} f(r_ij) annot[i, b] for j in [row0, row1);
+// lo/hi are SNP indices (clamped to the range), annot row-major (j - row0) K + b,
+// f = r^2 (corr_dim <= 0) or the unbiased r^2 - (1 - r^2)/(corr_dim - 1).
+// Output out[(j - row0) ld_row + b ld_col] (host).
+void window_ld_impl(Context& c, const Prepared& P, int64_t row0, int64_t row1, const int64_t* lo,
+                    const int64_t* hi, const double* annot, int64_t K, double corr_dim,
+                    double* out, int64_t ld_row, int64_t ld_col) {
+    const int64_t m = row1 - row0;
+    if (row0 < 0 || row1 > P.g.M || m <= 0) fail(LDS_ERR_ARG, "SNP range outside the genotype image");
+    if (K <= 0) fail(LDS_ERR_ARG, "annot_chr must have at least one column");
+    if (corr_dim > 0.0 && corr_dim <= 1.0)
+        fail(LDS_ERR_ARG, "Too few residual dimensions for unbiased windowed r^2 correction");
+    std::vector<double> mu, rs;
+    pearson_stats(P, row0, row1, mu, rs);
+    std::vector<int32_t> lo32((size_t)m), hi32((size_t)m);
+    for (int64_t r = 0; r < m; ++r) {
+        lo32[(size_t)r] = (int32_t)std::min(row1, std::max(row0, lo[r]));
+        hi32[(size_t)r] = (int32_t)std::min(row1, std::max(row0, hi[r]));
+    }
+    constexpr int64_t TB = 128;
+    const int64_t nT = (m + TB - 1) / TB;
+    // Partner tiles of each row tile, on the same 128-grid from row0.
+    std::vector<std::pair<int64_t, int64_t>> span((size_t)nT, {0, 0});
+    int64_t pairs = 0;
+    for (int64_t T = 0; T < nT; ++T) {
+        const int64_t a0 = T * TB, a1 = std::min(m, a0 + TB);
+        int64_t lmin = row1, hmax = row0;
+        for (int64_t r = a0; r < a1; ++r) {
+            if (hi32[(size_t)r] <= lo32[(size_t)r]) continue;
+            lmin = std::min<int64_t>(lmin, lo32[(size_t)r]);
+            hmax = std::max<int64_t>(hmax, hi32[(size_t)r]);
+        }
+        if (hmax > lmin) {
+            span[(size_t)T] = {(lmin - row0) / TB, (hmax - 1 - row0) / TB + 1};
+            pairs += span[(size_t)T].second - span[(size_t)T].first;
+        }
+    }
+    const int64_t per_cta = std::max<int64_t>(1, std::min<int64_t>(8, pairs / (148 * 4)));
+    std::vector<int4> items;
+    std::vector<int32_t> slot_beg((size_t)nT + 1, 0);
+    for (int64_t T = 0; T < nT; ++T) {
+        for (int64_t u = span[(size_t)T].first; u < span[(size_t)T].second; u += per_cta)
+            items.push_back(make_int4((int)(row0 + T * TB), (int)(row0 + u * TB),
+                                      (int)std::min(per_cta, span[(size_t)T].second - u),
+                                      (int)items.size()));
+        slot_beg[(size_t)T + 1] = (int32_t)items.size();
+    }
+    DevBuf d_items, d_beg, d_lo, d_hi, d_mu, d_rs, d_annot, d_part, d_out, d_st;
+    const size_t nit = std::max<size_t>(items.size(), 1);
+    int4* di = d_items.as<int4>(nit);
+    h2d(di, items.data(), items.size(), c.st);
+    int32_t* db = d_beg.as<int32_t>(slot_beg.size());
+    h2d(db, slot_beg.data(), slot_beg.size(), c.st);
+    int32_t* dlo = d_lo.as<int32_t>((size_t)m);
+    int32_t* dhi = d_hi.as<int32_t>((size_t)m);
+    h2d(dlo, lo32.data(), (size_t)m, c.st);
+    h2d(dhi, hi32.data(), (size_t)m, c.st);
+    double* dmu = d_mu.as<double>(mu.size());
+    double* drs = d_rs.as<double>(rs.size());
+    h2d(dmu, mu.data(), mu.size(), c.st);
+    h2d(drs, rs.data(), rs.size(), c.st);
+    double* dan = d_annot.as<double>((size_t)(m * K));
+    h2d(dan, annot, (size_t)(m * K), c.st);
+    const size_t npart = nit * (size_t)TB * (size_t)K;
+    double* dpart = d_part.as<double>(npart);
+    ck(cudaMemsetAsync(dpart, 0, npart * sizeof(double), c.st), "memset partial");
+    double* dout = d_out.as<double>((size_t)(m * K));
+    unsigned* dst = d_st.as<unsigned>(1);
+    ck(cudaMemsetAsync(dst, 0, 4, c.st), "memset");
+    GramArgs ga;
+    ga.nkt = (int)(P.g.N_pad / 128);
+    ga.K = (int)K;
+    ga.row0 = row0;
+    ga.row1 = row1;
+    ga.items = di;
+    ga.lo = dlo;
+    ga.hi = dhi;
+    ga.mean = dmu;
+    ga.rs = drs;
+    ga.annot = dan;
+    ga.corr_den = corr_dim > 0.0 ? 1.0 / (corr_dim - 1.0) : 0.0;
+    ga.partial = dpart;
+    ga.status = dst;
+    const CUtensorMap tmC = make_map_2d(P.g.codes, (uint64_t)P.g.nbp, (uint64_t)P.g.M_pad,
+                                        (uint64_t)P.g.nbp, 32, 128, CU_TENSOR_MAP_SWIZZLE_NONE);
+    ck(cudaEventRecord(c.ev[0], c.st), "event");
+    launch_gram_ld(tmC, ga, (int)items.size(), c.st);
+    launch_gram_reduce(dpart, db, row0, row1, (int)K, dout, K, 1, c.st);
+    ck(cudaEventRecord(c.ev[1], c.st), "event");
+    ck(cudaGetLastError(), "launch");
+    std::vector<double> h((size_t)(m * K));
+    d2h(h.data(), dout, h.size(), c.st);
+    unsigned stv = 0;
+    d2h(&stv, dst, 1, c.st);
+    ck(cudaStreamSynchronize(c.st), "windowed LD");
+    if (stv) fail(LDS_ERR_CUDA, "windowed LD tensor-core pipeline wait timed out (code %u)", stv);
+    float ms = 0.f;
+    ck(cudaEventElapsedTime(&ms, c.ev[0], c.ev[1]), "elapsed");
+    c.timings[0] = ms;
+    for (int64_t r = 0; r < m; ++r)
+        for (int64_t b = 0; b < K; ++b) out[r * ld_row + b * ld_col] = h[(size_t)(r * K + b)];
+}
+
+LDS_API int lds_geno_window_ld(int64_t geno, int64_t row0, int64_t row1, const int64_t* lo,
+                               const int64_t* hi, const double* annot, int64_t K,
+                               double corr_dim, double* out) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        ensure_device(c);
+        auto it = geno_table().find(geno);
+        if (it == geno_table().end()) fail(LDS_ERR_ARG, "unknown genotype handle");
+        if (!lo || !hi || !annot || !out) fail(LDS_ERR_ARG, "null argument");
+        window_ld_impl(c, *it->second, row0, row1, lo, hi, annot, K, corr_dim, out, K, 1);
+    });
+}
+
+LDS_API int lds_compute_windowed_ld_chr(const char* bed_prefix, const char* fam_path,
+                                        int chr_start, int chr_end, const int64_t* bp,
+                                        const double* annot_chr, int64_t K, double ld_wind_kb,
+                                        int chunk_size, const int64_t* row_sel, int64_t n_row_sel,
+                                        const double* C, const double* R, int64_t p,
+                                        int impute_mode, int has_impute_seed,
+                                        uint64_t impute_seed, int panel_cols, int cache_mb,
+                                        double* out) {
+    return guarded([&] {
+        (void)panel_cols;  // CPU panel/cache tiling knobs: the result does not depend on them
+        (void)cache_mb;
+        if (chr_end < chr_start) fail(LDS_ERR_ARG, "chr_end must be >= chr_start");
+        const int64_t m = (int64_t)chr_end - chr_start;
+        if (m <= 0) fail(LDS_ERR_ARG, "Chromosome slice is empty");
+        if (chunk_size <= 0) fail(LDS_ERR_ARG, "chunk_size must be > 0");
+        const double window_bp = ld_wind_kb * 1000.0;
+        if (!std::isfinite(window_bp) || window_bp <= 0.0)
+            fail(LDS_ERR_ARG, "ld_wind_kb must define a finite positive BP window");
+        if (!bp || !annot_chr || !out) fail(LDS_ERR_ARG, "null argument");
+        for (int64_t i = 1; i < m; ++i)
+            if (bp[i] < bp[i - 1])
+                fail(LDS_ERR_ARG, "BP not sorted within chromosome block. Sort your .bim by CHR+BP.");
+        if (K <= 0) fail(LDS_ERR_ARG, "annot_chr must have at least one column");
+        if (impute_mode != LDS_IMPUTE_MEAN && impute_mode != LDS_IMPUTE_HWE)
+            fail(LDS_ERR_ARG, "impute_mode must be 'mean' or 'hwe'");
+        if ((C != nullptr) != (R != nullptr)) fail(LDS_ERR_ARG, "C and R must be given together");
+        if (C && p > 0)
+            fail(LDS_ERR_ARG, "covariate projection (C, R) is not supported by the GPU windowed path");
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        ensure_device(c);
+        int64_t M_total = 0;
+        Prepared& P = prepared_for_file(c, bed_prefix, fam_path, row_sel, n_row_sel, impute_mode,
+                                        has_impute_seed ? impute_seed : 0ULL, 0, &M_total);
+        if (chr_start < 0 || chr_end > P.g.M)
+            fail(LDS_ERR_IO, "BED file too small for requested block: %s.bed", bed_prefix);
+        if (P.g.N <= 2) fail(LDS_ERR_ARG, "Too few rows for windowed LD score computation");
+        const double corr_dim = (double)(P.g.N - 1);
+        if (corr_dim <= 1.0)
+            fail(LDS_ERR_ARG, "Too few residual dimensions for unbiased windowed r^2 correction");
+        // Partner interval of SNP j: |bp_i - bp_j| <= W (winldcore.cpp:434-442), a
+        // contiguous run of the sorted positions.
+        std::vector<int64_t> lo((size_t)m), hi((size_t)m);
+        int64_t a = 0, b = 0;
+        for (int64_t j = 0; j < m; ++j) {
+            while (a < j && std::fabs((long double)bp[j] - (long double)bp[a]) > (long double)window_bp) ++a;
+            if (b < j + 1) b = j + 1;
+            while (b < m && std::fabs((long double)bp[b] - (long double)bp[j]) <= (long double)window_bp) ++b;
+            lo[(size_t)j] = chr_start + a;
+            hi[(size_t)j] = chr_start + b;
+        }
+        std::vector<double> ann((size_t)(m * K));
+        for (int64_t j = 0; j < m; ++j)
+            for (int64_t k = 0; k < K; ++k) ann[(size_t)(j * K + k)] = annot_chr[k * m + j];
+        window_ld_impl(c, P, chr_start, chr_end, lo.data(), hi.data(), ann.data(), K, corr_dim, out,
+                       1, m);
+    });
+}
+
+// Minor allele frequency per SNP over the selected samples (compute_maf_block,
+// genotype.cpp:1634-1730): p = sum / (2 nobs) clipped to [0, 1], maf = min(p, 1 - p).
+LDS_API int lds_compute_maf_bed(const char* bed_prefix, const char* fam_path, int nsnps,
+                                int step_size, const int64_t* row_sel, int64_t n_row_sel,
+                                double* maf_out) {
+    return guarded([&] {
+        if (nsnps < 0) fail(LDS_ERR_ARG, "nsnps must be >= 0");
+        if (step_size <= 0) fail(LDS_ERR_ARG, "step_size must be > 0");
+        if (row_sel && n_row_sel <= 0) fail(LDS_ERR_ARG, "No rows selected in compute_maf_bed");
+        if (nsnps == 0) return;
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        ensure_device(c);
+        Prepared& P = prepared_for_file(c, bed_prefix, fam_path, row_sel, n_row_sel,
+                                        LDS_IMPUTE_MEAN, 0ULL, 1, nullptr);
+        if (nsnps > P.g.M)
+            fail(LDS_ERR_IO, "BED file too small for requested block: %s.bed", bed_prefix);
+        for (int64_t j = 0; j < nsnps; ++j) {
+            const SnpCounts& k = P.counts[(size_t)j];
+            const long long nobs = (long long)k.n[0] + k.n[1] + k.n[2];
+            const long long sum = (long long)k.n[1] + 2LL * k.n[2];
+            double pp = 0.0;
+            if (nobs > 0) {
+                pp = (double)sum / (2.0 * (double)nobs);
+                if (pp < 0.0) pp = 0.0;
+                if (pp > 1.0) pp = 1.0;
+            }
+            maf_out[j] = std::min(pp, 1.0 - pp);
+        }
+    });
+}
+
 LDS_API int lds_nn_band(int64_t geno, int D, double* xx_out, int32_t* counts_out) {
     return guarded([&] {
         Context& c = ctx();

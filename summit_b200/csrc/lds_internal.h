@@ -3,6 +3,7 @@
 #pragma once
 #include <cstdint>
 #include <string>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 namespace lds {
@@ -99,6 +100,31 @@ void launch_synth(int64_t n, int64_t M, uint64_t seed, const int64_t* t0, const 
 void launch_nn_band(const DevGeno& g, int D, int32_t* counts, cudaStream_t st);
 void launch_nn_band_finish(int64_t M, int D, const int32_t* counts, const double* mean,
                            const double* sdinv, double* xx, cudaStream_t st);
+
+// Exact windowed LD scores (lds_gram.cu).  Work item x: tile J = SNPs
+// [x.x, x.x + 128), partner tiles I = [x.y + 128 t, +128) for t < x.z, sums
+// into partial slot x.w.  lo/hi: partner interval of SNP j at (j - row0);
+// mean/rs (1/sqrt(c_jj), 0 for a constant SNP) indexed by SNP; annot row-major
+// ((i - row0) K + b); corr_den = 1/(corr_dim - 1) for the unbiased r^2, 0 for r^2.
+struct GramArgs {
+    int nkt = 0, K = 0;
+    int64_t row0 = 0, row1 = 0;
+    const int4* items = nullptr;
+    const int32_t* lo = nullptr;
+    const int32_t* hi = nullptr;
+    const double* mean = nullptr;
+    const double* rs = nullptr;
+    const double* annot = nullptr;
+    double corr_den = 0.0;
+    double* partial = nullptr;      // (slot 128 + jl) K + b, zeroed by the caller
+    unsigned* status = nullptr;
+};
+size_t gram_ld_smem_bytes();
+void launch_gram_ld(const CUtensorMap& tmC, const GramArgs& a, int n_items, cudaStream_t st);
+// out[(j - row0) ld_row + b ld_col] = sum of tile (j - row0)/128's slots
+// [slot_beg[T], slot_beg[T+1]) in order.
+void launch_gram_reduce(const double* partial, const int32_t* slot_beg, int64_t row0, int64_t row1,
+                        int K, double* out, int64_t ld_row, int64_t ld_col, cudaStream_t st);
 
 // Near-field control variate sums (lds_cv.cu): C[j K + k] += sum_v a_jkv^2 and,
 // if mu is set, mu[j K + k] = E[a_jk^2]; D in {4, 8, 15}.

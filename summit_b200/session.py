@@ -98,6 +98,40 @@ class GwSession:
         check(_lib.load().lds_nn_band(self.handle, int(D), ptr(xx), ptr(cnt)))
         return (xx, cnt) if with_counts else xx
 
+    def window_ld(self, lo, hi, annot, corr_dim: float | None = None, row0: int = 0,
+                  row1: int | None = None) -> np.ndarray:
+        """Exact windowed LD scores of SNPs [row0, row1): row j sums f(r_ij) annot[i]
+        over i in [lo[j - row0], hi[j - row0]), f = r^2, or with ``corr_dim`` the
+        unbiased r^2 - (1 - r^2)/(corr_dim - 1).  annot has one row per SNP of the
+        range; returns (row1 - row0) x K."""
+        row1 = self.M if row1 is None else int(row1)
+        m = row1 - int(row0)
+        lo = np.ascontiguousarray(lo, dtype=np.int64)
+        hi = np.ascontiguousarray(hi, dtype=np.int64)
+        annot = np.ascontiguousarray(annot, dtype=np.float64)
+        if annot.ndim == 1:
+            annot = annot[:, None]
+        if lo.shape != (m,) or hi.shape != (m,) or annot.shape[0] != m:
+            raise ValueError("lo, hi and annot must have one row per SNP of [row0, row1)")
+        out = np.empty((m, annot.shape[1]))
+        check(_lib.load().lds_geno_window_ld(self.handle, int(row0), row1, ptr(lo), ptr(hi),
+                                             ptr(annot), annot.shape[1],
+                                             float(corr_dim or 0.0), ptr(out)))
+        return out
+
+    def partition_ld_expectation(self, annot, window_starts) -> np.ndarray:
+        """Exact expectation of the windowed stochastic estimator (WinPlan) on
+        this image: per SNP j of window w, sum_{i in w} r_ij^2 annot[i] minus the
+        correlation null M_k(w) / (N - 1)."""
+        ws = np.ascontiguousarray(window_starts, dtype=np.int64)
+        annot = np.ascontiguousarray(annot, dtype=np.float64)
+        win = np.repeat(np.arange(ws.size - 1), np.diff(ws))
+        lo, hi = ws[win], ws[win + 1]
+        ld = self.window_ld(lo, hi, annot)
+        mkw = np.zeros((ws.size - 1, annot.shape[1]))
+        np.add.at(mkw, win, annot)
+        return ld - mkw[win] / float(self.N - 1)
+
     def close(self) -> None:
         if self.handle:
             _lib.load().lds_geno_destroy(self.handle)

@@ -11,6 +11,10 @@ Fixtures:
   float64 path, plus the residual variances.
 * synth_gw.npz — a 97 x 131 synthetic fileset (bedfile.py generator, seed 5),
   two annotation bins, Gaussian and spherical probes, with MC fourth moments.
+* hardcalls_winld.npz — exact windowed LD scores of the same hard calls from
+  the reference's winldcore.cpp (oracle/_ref/libref_winld.so): mean and HWE
+  imputation, 0.15 kb and 1 Mb windows over positions 100 bp apart, two
+  annotation columns.
 """
 from __future__ import annotations
 
@@ -23,7 +27,7 @@ import numpy as np
 ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
 
-from oracle.oracle import Reference  # noqa: E402
+from oracle.oracle import Reference, ReferenceWindowed  # noqa: E402
 from summit_b200 import bedfile  # noqa: E402
 
 HERE = Path(__file__).resolve().parent
@@ -81,6 +85,24 @@ def main() -> None:
         out["packed"] = bedfile.pack_bed_rows(g)
         out["annot"] = annot
         np.savez(HERE / "synth_gw.npz", **out)
+
+        refw = ReferenceWindowed()
+        refw.set_threads(1)
+        out = {}
+        g = hardcalls()
+        prefix = bedfile.write_plink(Path(td) / "hcw", g)
+        m, n = g.shape
+        bp = np.arange(1, m + 1, dtype=np.int64) * 100
+        annot = np.column_stack([np.ones(m), np.arange(m) % 2 == 0]).astype(np.float64)
+        for impute in ("mean", "hwe"):
+            for kb in (0.15, 1000.0):
+                key = f"{impute}_{'narrow' if kb < 1 else 'wide'}"
+                out[key] = refw.compute_windowed_ld_chr(prefix, 0, m, bp, annot, kb, 4,
+                                                        impute_mode=impute, impute_seed=17)
+        out["packed"] = bedfile.pack_bed_rows(g)
+        out["bp"] = bp
+        out["annot"] = annot
+        np.savez(HERE / "hardcalls_winld.npz", **out)
     print("wrote", sorted(p.name for p in HERE.glob("*.npz")))
 
 
