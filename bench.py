@@ -300,6 +300,99 @@ def read_traffic() -> dict | None:
     return None
 
 
+def ld_errors(est, truth) -> dict:
+    """Relative error of each bin's mean LD score (max over bins; the
+    reference's accuracy metric, manuscript/scripts/ld/numvec_error.py:86) and
+    the per-SNP relative RMSE (mean over bins)."""
+    est, truth = np.asarray(est, dtype=np.float64), np.asarray(truth, dtype=np.float64)
+    mean_rel = np.abs(est.mean(0) - truth.mean(0)) / np.abs(truth.mean(0))
+    rr = np.sqrt(((est - truth) ** 2).mean(0)) / np.sqrt((truth ** 2).mean(0))
+    return {"mean_ld_rel_err": round(float(mean_rel.max()), 6),
+            "snp_rel_rmse": round(float(rr.mean()), 5)}
+
+
+def learned_vs_plain(sess, annot, ws, stream) -> dict:
+    """LD-score time and error of the plain windowed estimator and of the
+    learned control variate (B = 10) on the same resident image, judged
+    against the exact expectation of the estimator (exact windowed Gram
+    kernel) and against the plain estimator at B = 1,000.  Wall times are
+    from the resident image to host results (plan set-up, probe streams and
+    any training included); device times are one steady-state execute."""
+    import math
+
+    import torch
+
+    from summit_b200 import _lib
+    from summit_b200.learned_cv import CvConfig, LearnedCV
+    from summit_b200.session import WinPlan
+
+    lib = _lib.load()
+    out = {}
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    truth = sess.partition_ld_expectation(annot, ws)
+    wall = time.perf_counter() - t0
+    buf = np.zeros(4)
+    lib.lds_last_timings(_lib.ptr(buf), 4)
+    out["exact"] = {"wall_ms": round(wall * 1e3, 1), "device_ms": round(float(buf[0]), 2),
+                    "mean_ld_rel_err": 0.0, "snp_rel_rmse": 0.0,
+                    "method": "exact expectation of the estimator (int8 Gram tensor-core kernel)"}
+
+    def plain(B, device=True):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        p = WinPlan(sess, annot, ws, B, BLOCK, PROBE_SEED, "rademacher")
+        p.execute()
+        ld = p.results()["ldscore"]
+        wall = time.perf_counter() - t0
+        dev = None
+        if device:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            p.execute()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            dev = e0.elapsed_time(e1)
+        p.close()
+        rec = {"B": B, "wall_ms": round(wall * 1e3, 1), **ld_errors(ld, truth)}
+        if dev is not None:
+            rec["device_ms"] = round(dev, 2)
+        return ld, rec
+
+    _, out["plain_b10"] = plain(10)
+    p100, out["plain_b100"] = plain(100)
+    p1000, out["plain_b1000"] = plain(1000, device=False)
+    cfg = CvConfig(nvecs=10)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    cv = LearnedCV(sess, annot, ws, BLOCK, PROBE_SEED + 1, cfg=cfg)
+    res = cv.run()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    res = cv.run()  # steady state (graph captured, workspace allocated)
+    cv.close()
+    ld = res["ldscore"].double().cpu().numpy()
+    near = res["nearcv_ldscore"].double().cpu().numpy()
+    out["learned_b10"] = {"B": 10, "wall_ms": round(wall * 1e3, 1),
+                          "device_ms": round(res["timings"]["total_ms"], 2),
+                          "stages_ms": {k: round(v, 2) for k, v in res["timings"].items()},
+                          **ld_errors(ld, truth),
+                          "near_field_only": ld_errors(near, truth)}
+    # Plain probes needed for the learned estimator's per-SNP error (error ~ B^-1/2).
+    ratio = out["plain_b100"]["snp_rel_rmse"] / max(out["learned_b10"]["snp_rel_rmse"], 1e-12)
+    b_eq = int(math.ceil(100.0 * ratio * ratio / 10.0) * 10)
+    if b_eq <= 2000:
+        _, out["plain_matched"] = plain(b_eq)
+        out["speedup_at_matched_snp_error"] = {
+            "wall": round(out["plain_matched"]["wall_ms"] / out["learned_b10"]["wall_ms"], 2),
+            "device": round(out["plain_matched"]["device_ms"] / out["learned_b10"]["device_ms"], 2)}
+    out["judge_plain_b1000"] = {"learned_b10": ld_errors(ld, p1000),
+                                "plain_b100": ld_errors(p100, p1000)}
+    out["error_metric"] = ("mean_ld_rel_err: max over bins of |mean est - mean truth| / |mean truth|; "
+                           "snp_rel_rmse: per-SNP RMS error / RMS truth, mean over bins")
+    return out
+
+
 def ours_arm(args) -> None:
     import torch
 
@@ -379,6 +472,11 @@ def ours_arm(args) -> None:
     gw_kms = plan.kernel_ms()
     plan.close()
 
+    # ---- learned control variate vs plain (config-2 shape, B = 10 vs 100) ----
+    lvp = None
+    if rank == 0 and not os.environ.get("LDS_SKIP_LEARNED"):
+        lvp = learned_vs_plain(sess, annot, ws, stream)
+
     # ---- end to end through the C ABI from pinned host buffers ----
     def e2e_once():
         s2 = GwSession(bed_host, n, impute_mode="mean")
@@ -449,6 +547,8 @@ def ours_arm(args) -> None:
             "gpu_launches": launches,
             "clocks": clocks,
         }
+        if lvp is not None:
+            line["learned_vs_plain"] = lvp
         if world == 1 and not os.environ.get("LDS_SKIP_CPU_BASELINE"):
             threads = cpu_threads()
             with tempfile.TemporaryDirectory() as td:

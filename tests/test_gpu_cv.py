@@ -94,3 +94,53 @@ def test_cv_plan_results_unchanged(small_bed):
     b.execute()
     np.testing.assert_array_equal(a.results()["ldscore"], b.results()["ldscore"])
     assert b.cv_ms() >= 0.0
+
+
+def _config_like(n, m, K=24, seed=11):
+    """Scaled-down config-2 inputs: Bernoulli(0.1) annotations, contiguous
+    windows with log-uniform sizes in [200, 5000]."""
+    from summit_b200 import gwldcore
+
+    bed = gwldcore.synth_bed_rows(n, m, seed)
+    rng = np.random.default_rng(seed)
+    annot = (rng.random((m, K)) < 0.1).astype(np.float64)
+    starts = [0]
+    while starts[-1] < m:
+        starts.append(min(m, starts[-1] + int(np.exp(rng.uniform(np.log(200.0), np.log(5000.0))))))
+    return bed, annot, np.asarray(starts, dtype=np.int64)
+
+
+def _snp_rrmse(est, truth):
+    est, truth = np.asarray(est), np.asarray(truth)
+    return float(np.mean(np.sqrt(((est - truth) ** 2).mean(0)) / np.sqrt((truth ** 2).mean(0))))
+
+
+def test_learned_network_gains_over_the_estimator_without_it():
+    """Judged against the exact expectation of the windowed estimator: with 10
+    probes, the trained network cuts the per-SNP error of the near-field
+    control variate it is added to, and beats the plain estimator with 10x the
+    probes; the combine keeps each bin's mean of the near-field estimate."""
+    from summit_b200.learned_cv import CvConfig, LearnedCV
+    from summit_b200.session import GwSession, WinPlan
+
+    n, m = 3000, 30000
+    bed, annot, ws = _config_like(n, m)
+    sess = GwSession(bed, n)
+    truth = sess.partition_ld_expectation(annot, ws)
+    cv = LearnedCV(sess, annot, ws, 1000, 2024, cfg=CvConfig(nvecs=10))
+    res = cv.run()
+    cv.close()
+    learned = res["ldscore"].cpu().numpy()
+    near = res["nearcv_ldscore"].cpu().numpy()
+    plain10 = res["plain_ldscore"].cpu().numpy()
+    p100 = WinPlan(sess, annot, ws, 100, 1000, 2024, "rademacher")
+    p100.execute()
+    plain100 = p100.results()["ldscore"]
+    p100.close()
+    sess.close()
+    e_learned, e_near = _snp_rrmse(learned, truth), _snp_rrmse(near, truth)
+    e_plain10, e_plain100 = _snp_rrmse(plain10, truth), _snp_rrmse(plain100, truth)
+    assert e_near < 0.85 * e_plain10, (e_near, e_plain10)
+    assert e_learned < 0.6 * e_near, (e_learned, e_near)
+    assert e_learned < e_plain100, (e_learned, e_plain100)
+    np.testing.assert_allclose(learned.mean(0), near.mean(0), rtol=1e-9, atol=1e-12)
