@@ -66,4 +66,31 @@ void launch_cv_near(const CvNearArgs& a, int D, cudaStream_t st) {
     count_launch();
 }
 
+// Finalize of a windowed estimate: meansq = sum of the probe slices and
+// ld = meansq / nvecs - Mkw[window(j), k] / nd (gw_ldscore.py:2197, :2220-2222
+// applied per window).
+__global__ void win_finalize_kernel(const double* __restrict__ acc, int slices, int64_t MK, int K,
+                                    double nvecs, double nd, const int32_t* __restrict__ win_of,
+                                    const double* __restrict__ mkw, double* __restrict__ ld,
+                                    double* __restrict__ meansq) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= MK) return;
+    double s = acc[t];
+    for (int q = 1; q < slices; ++q) s += acc[(int64_t)q * MK + t];
+    const int64_t j = t / K;
+    const int k = (int)(t - j * K);
+    meansq[t] = s;
+    ld[t] = s / nvecs - mkw[(int64_t)win_of[j] * K + k] / nd;
+}
+
+void launch_win_finalize(const double* acc, int slices, int64_t M, int K, double nvecs, double nd,
+                         const int32_t* win_of, const double* mkw, double* ld, double* meansq,
+                         cudaStream_t st) {
+    const int64_t MK = M * K;
+    if (MK == 0) return;
+    win_finalize_kernel<<<(unsigned)((MK + 255) / 256), 256, 0, st>>>(acc, slices, MK, K, nvecs, nd,
+                                                                      win_of, mkw, ld, meansq);
+    count_launch();
+}
+
 }  // namespace lds

@@ -189,6 +189,10 @@ struct Context {
     // Surrogate-network workspace, grow-only so that repeated training and
     // inference calls make no device allocations (cudaFree synchronizes).
     DevBuf mlp_m, mlp_v, mlp_g, mlp_zs, mlp_dzs, mlp_dout, mlp_rows, mlp_loss, mlp_pack;
+    // Sketch-digit (0) and weight-digit (1) workspaces shared by windowed plans:
+    // grow-only, and each plan keeps the buffer its graph captured alive, so
+    // creating and destroying plans does not allocate and free gigabytes.
+    std::shared_ptr<DevBuf> ws[2];
     double timings[4] = {0, 0, 0, 0};
     int slices = 4;
 };
@@ -1244,11 +1248,13 @@ struct WinPlan {
     };
     std::vector<Batch> batches;
     std::vector<DevBuf> z;              // per V-tile, M x V FP64 probes
-    DevBuf y, yq, ycs, yshift, wq, wcs, accum, mc, lscale, guards, status;
+    DevBuf y, ycs, yshift, wcs, accum, mc, lscale, guards, status;
+    std::shared_ptr<DevBuf> yq, wq;     // shared context workspaces (Context::ws)
     // Optional outputs for the control variate (lds_win_plan_set_cv): per-V-tile
     // meansq slices, near-field sums C and known means mu, neighbour products.
     int split = 0, cv_D = 0;
     DevBuf annot_d, winof_d, sqrt_ls, xx, band_cnt, cvC, cvMu;
+    DevBuf mkw_d, ld_d, ms_d;           // finalize inputs and outputs
     cudaEvent_t cv_ev[2] = {nullptr, nullptr};
     double cv_ms = 0.0;
     CUtensorMap tmA;
@@ -1275,6 +1281,17 @@ struct WinPlan {
         if (graph) cudaGraphExecDestroy(graph);
     }
 };
+
+// A context workspace of at least `bytes` (slot 0 sketch digits, 1 weight digits).
+std::shared_ptr<DevBuf> shared_workspace(Context& c, int slot, size_t bytes) {
+    std::shared_ptr<DevBuf>& w = c.ws[slot];
+    if (!w || w->n < bytes) {
+        w.reset();  // plans that captured the old buffer keep it alive
+        w = std::make_shared<DevBuf>();
+        w->get(bytes);
+    }
+    return w;
+}
 
 std::map<int64_t, std::unique_ptr<WinPlan>>& win_table() {
     static std::map<int64_t, std::unique_ptr<WinPlan>> t;
@@ -1326,6 +1343,8 @@ std::unique_ptr<WinPlan> win_plan_create(Context& c, std::shared_ptr<Prepared> P
         ls[(size_t)j] = (std::isfinite(v) && v > 0.0) ? v * v * inv_denom2 : 0.0;
     }
     h2d(pl->lscale.as<double>((size_t)M), ls.data(), (size_t)M, c.st);
+    h2d(pl->winof_d.as<int32_t>((size_t)M), pl->win_of.data(), (size_t)M, c.st);
+    h2d(pl->mkw_d.as<double>(pl->Mkw.size()), pl->Mkw.data(), pl->Mkw.size(), c.st);
     // Window batches: the sketch digits of a batch stay under batch_gb.
     const double per_window = (double)Np * (double)K * umma::ncolp_for(vmax);
     const int64_t wb = std::max<int64_t>(1, (int64_t)(batch_gb * 1e9 / per_window));
@@ -1409,11 +1428,10 @@ std::unique_ptr<WinPlan> win_plan_create(Context& c, std::shared_ptr<Prepared> P
         ck(cudaStreamSynchronize(c.st), "probe upload");
         v0 += V;
     }
-    pl->yq.as<int8_t>((size_t)(max_ksup * ncmax * Np));
+    pl->yq = shared_workspace(c, 0, (size_t)(max_ksup * ncmax * Np));
     pl->ycs.as<double>((size_t)(max_ksup * vmax));
     pl->yshift.as<int>((size_t)(max_ksup * vmax));
-    int8_t* wq = pl->wq.as<int8_t>((size_t)std::max<int64_t>(max_wq, 16));
-    (void)wq;
+    pl->wq = shared_workspace(c, 1, (size_t)std::max<int64_t>(max_wq, 16));
     pl->wcs.as<double>((size_t)(max_ksup * vmax));
     pl->accum.as<double>((size_t)(M * K));
     if (with_mc) pl->mc.as<double>((size_t)(M * K));
@@ -1479,18 +1497,18 @@ void win_enqueue(Context& c, WinPlan& pl) {
             uw.rowind = static_cast<int32_t*>(b.rowind.p);
             uw.sc = static_cast<double*>(b.sc.p);
             uw.bin_off = static_cast<int64_t*>(b.binoff.p);
-            uw.wq = static_cast<int8_t*>(pl.wq.p);
+            uw.wq = static_cast<int8_t*>(pl.wq->p);
             uw.colscale = static_cast<double*>(pl.wcs.p);
             uw.ycolscale = static_cast<double*>(pl.ycs.p);
             uw.yshift = static_cast<int*>(pl.yshift.p);
             const size_t wbytes = (size_t)(b.ksup * 2 * nc) * (size_t)b.lmax;
-            ck(cudaMemsetAsync(pl.wq.p, 0, wbytes, c.st), "memset weights");
+            ck(cudaMemsetAsync(pl.wq->p, 0, wbytes, c.st), "memset weights");
             umma::launch_p1_weights4(uw, static_cast<double*>(P.d_mean.p),
                                      static_cast<double*>(P.d_sdinv.p),
                                      static_cast<double*>(pl.z[ti].p), M, c.st);
             ck(cudaEventRecordWithFlags(pl.ev[(size_t)e++], c.st, cudaEventRecordExternal), "event");
             const CUtensorMap tmW =
-                make_map_2d(pl.wq.p, (uint64_t)b.lmax, (uint64_t)(b.ksup * 2 * nc), (uint64_t)b.lmax,
+                make_map_2d(pl.wq->p, (uint64_t)b.lmax, (uint64_t)(b.ksup * 2 * nc), (uint64_t)b.lmax,
                             128, (uint32_t)std::min(256, nc), CU_TENSOR_MAP_SWIZZLE_128B);
             umma::P1UArgs pa;
             pa.K = (int)b.ksup;
@@ -1512,7 +1530,7 @@ void win_enqueue(Context& c, WinPlan& pl) {
                 return v > 0 ? v : 8;
             }();
             pa.sb_per_cta = spc;
-            pa.yq = static_cast<int8_t*>(pl.yq.p);
+            pa.yq = static_cast<int8_t*>(pl.yq->p);
             pa.ycolscale = static_cast<double*>(pl.ycs.p);
             pa.yshift = static_cast<int*>(pl.yshift.p);
             umma::launch_p1_umma(tmW, pa, Np, c.st);
@@ -1521,7 +1539,7 @@ void win_enqueue(Context& c, WinPlan& pl) {
             ck(cudaEventRecordWithFlags(pl.ev[(size_t)e++], c.st, cudaEventRecordExternal), "event");
             const int nb = umma::p2_bins_per_cta(nc, (int)K);
             const CUtensorMap tmB =
-                make_map_2d(pl.yq.p, (uint64_t)Np, (uint64_t)(b.ksup * nc), (uint64_t)Np, 128,
+                make_map_2d(pl.yq->p, (uint64_t)Np, (uint64_t)(b.ksup * nc), (uint64_t)Np, 128,
                             (uint32_t)std::min(256, nb * nc), CU_TENSOR_MAP_SWIZZLE_128B);
             umma::P2UArgs u;
             u.K = (int)K;
@@ -1604,33 +1622,26 @@ void win_times(WinPlan& pl) {
 void win_results(Context& c, WinPlan& pl, double* ldscore, double* meansq_out, double* inv_out,
                  double* mc_snp) {
     const int64_t M = pl.P->g.M, K = pl.K, N = pl.P->g.N;
-    std::vector<double> acc((size_t)(M * K) * (size_t)pl.ntiles_out());
-    d2h(acc.data(), static_cast<double*>(pl.accum.p), acc.size(), c.st);
-    std::vector<double> mcv;
-    if (pl.with_mc && mc_snp) {
-        mcv.resize((size_t)(M * K));
-        d2h(mcv.data(), static_cast<double*>(pl.mc.p), mcv.size(), c.st);
-    }
+    const size_t MK = (size_t)(M * K);
+    // Per-V-tile slices (control-variate plans) add up to the plain sums; the
+    // finalize runs on the device and the outputs go straight to the caller.
+    const double nd = (double)(N - pl.P->ddof);
+    double* dld = pl.ld_d.as<double>(MK);
+    double* dms = pl.ms_d.as<double>(MK);
+    launch_win_finalize(static_cast<double*>(pl.accum.p), pl.ntiles_out(), M, (int)K,
+                        (double)pl.nvecs, nd, static_cast<int32_t*>(pl.winof_d.p),
+                        static_cast<double*>(pl.mkw_d.p), dld, dms, c.st);
+    ck(cudaGetLastError(), "finalize");
     unsigned st = 0;
     d2h(&st, static_cast<unsigned*>(pl.status.p), 1, c.st);
     ck(cudaStreamSynchronize(c.st), "results");
     if (st) fail(LDS_ERR_CUDA, "tensor-core pipeline wait timed out (code %u)", st);
     win_times(pl);
-    // Per-V-tile slices (control-variate plans) add up to the plain sums.
-    for (int t = 1; t < pl.ntiles_out(); ++t)
-        for (size_t x = 0; x < (size_t)(M * K); ++x) acc[x] += acc[(size_t)t * (size_t)(M * K) + x];
-    acc.resize((size_t)(M * K));
-    if (meansq_out) std::memcpy(meansq_out, acc.data(), sizeof(double) * acc.size());
+    if (ldscore) d2h(ldscore, dld, MK, c.st);
+    if (meansq_out) d2h(meansq_out, dms, MK, c.st);
+    if (pl.with_mc && mc_snp) d2h(mc_snp, static_cast<double*>(pl.mc.p), MK, c.st);
+    ck(cudaStreamSynchronize(c.st), "results copy");
     if (inv_out) std::memcpy(inv_out, pl.inv.data(), sizeof(double) * (size_t)M);
-    const double nd = (double)(N - pl.P->ddof);
-    if (ldscore)
-        for (int64_t j = 0; j < M; ++j) {
-            const int64_t w = pl.win_of[(size_t)j];
-            for (int64_t k = 0; k < K; ++k)
-                ldscore[j * K + k] =
-                    acc[(size_t)(j * K + k)] / (double)pl.nvecs - pl.Mkw[(size_t)(w * K + k)] / nd;
-        }
-    if (mc_snp && !mcv.empty()) std::memcpy(mc_snp, mcv.data(), sizeof(double) * mcv.size());
 }
 
 // Control-variate outputs of a windowed plan; call before its first execute.
@@ -1644,7 +1655,6 @@ void win_set_cv(Context& c, WinPlan& pl, const double* annot, int split, int D) 
     pl.accum.as<double>(nout);
     if (D > 0) {
         h2d(pl.annot_d.as<double>(MK), annot, MK, c.st);
-        h2d(pl.winof_d.as<int32_t>((size_t)M), pl.win_of.data(), (size_t)M, c.st);
         std::vector<double> ls((size_t)M);
         d2h(ls.data(), static_cast<double*>(pl.lscale.p), (size_t)M, c.st);
         ck(cudaStreamSynchronize(c.st), "cv setup");
@@ -1734,6 +1744,7 @@ LDS_API void lds_clear_device_cache(void) {
     Context& c = ctx();
     std::lock_guard<std::mutex> lk(c.mu);
     c.cache.clear();
+    for (auto& w : c.ws) w.reset();
     for (DevBuf* b : {&c.raw, &c.rows_dev, &c.hwe_q0, &c.hwe_q01, &c.hwe_sb, &c.counts_dev, &c.y,
                       &c.yq, &c.ycs, &c.wq, &c.wcs, &c.z, &c.rowind, &c.sc, &c.binoff, &c.wqoff,
                       &c.accum, &c.mc, &c.guards, &c.lscale, &c.xin})

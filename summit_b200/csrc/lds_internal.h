@@ -143,6 +143,11 @@ struct CvNearArgs {
     int split_v = 0;
 };
 void launch_cv_near(const CvNearArgs& a, int D, cudaStream_t st);
+// Windowed finalize: meansq = sum of `slices` slices of acc (each M*K), and
+// ld = meansq / nvecs - mkw[win_of[j] K + k] / nd.
+void launch_win_finalize(const double* acc, int slices, int64_t M, int K, double nvecs, double nd,
+                         const int32_t* win_of, const double* mkw, double* ld, double* meansq,
+                         cudaStream_t st);
 
 // Surrogate network of the learned control variate (lds_mlp.cu): in -> 128 ->
 // 128 -> 128 -> out, GELU, FP32 master parameters laid out as below.
