@@ -336,6 +336,63 @@ int lds_compute_maf_bed(const char* bed_prefix, const char* fam_path, int nsnps,
                         const int64_t* row_sel, int64_t n_row_sel, double* maf_out);
 
 /* ---------------------------------------------------------------------
+ * SUMMIT-GxE multi-environment products on a resident genotype image
+ * (replacing gxeldcore.MultiEnvironmentKernel, gxeldcore.cpp:10281-12557,
+ * bindings :16420-16474).  N = samples of the image, E environments, K
+ * annotation bins, B probes, T environments in a tile starting at env_start.
+ * Arrays are column-major unless stated; accumulators are (E * total_variants)
+ * x K row-major.  With device_ptrs = 0 every array argument is host memory
+ * (copied per call); with 1 every array is a device pointer.
+ *
+ * lds_gxe_create: the kernel's constructor inputs (environments N x E, common
+ *   basis N x r, directions N x E, feature basis N x F with power_indices /
+ *   power_offsets (4E+1) / ranks (E)) — the power-0 range of environment e
+ *   names its fixed-effect basis, on which projection leakage is measured.
+ * lds_gxe_source_block (source_block, :11008-11240): target (N x T 2 K B)
+ *   += X_[j0,j1) [sqrt(a) z s_x] (additive halves) and
+ *   phi_e o X_[j0,j1) [sqrt(a) z s_w] (interaction halves); probes L x B,
+ *   annotation L x K (square roots if annotation_is_sqrt), scales L x T.
+ * lds_gxe_project_sources (project_sources, :11583-11729): in place; leakages
+ *   receives one value per environment of the tile; leakage > 1e-9 is an error.
+ * lds_gxe_pair_create (prepare_protected_row_weighted_pair, :9808): seals
+ *   [right, w o right] (right N x C, row_weights N x G, column c weighted by
+ *   w[:, c / (C / G)]) on the device.
+ * lds_gxe_target_score_block (target_score_block, :11731-11936): out =
+ *   X_[j0,j1)^T [S, w o S]; accumulates sum_b (s out)^2 / (N - rank_e)^2.
+ * lds_gxe_normalize_scores (normalize_scores, :12490-12557): divides by B.
+ * lds_philox_rademacher (numpy_philox_rademacher_block, :10070-10113): out
+ *   rows x P of +-1 from NumPy Philox keys (P x 2 uint64), bit-identical to
+ *   Generator(Philox).integers(0, 2, dtype=int8) * 2 - 1.
+ * ------------------------------------------------------------------- */
+int lds_gxe_create(int64_t geno, int64_t E, const double* environments, int64_t r,
+                   const double* common_basis, const double* directions, int64_t F,
+                   const double* feature_basis, const int64_t* power_indices,
+                   const int64_t* power_offsets, const int32_t* ranks, int annotation_bins,
+                   int64_t* handle_out);
+int lds_gxe_destroy(int64_t gxe);
+int lds_gxe_source_block(int64_t gxe, int64_t j0, int64_t j1, const double* probes, int64_t B,
+                         const double* annotation, int annotation_is_sqrt, const double* scale_x,
+                         const double* scale_w, int64_t T, int environment_start, double* target,
+                         int device_ptrs);
+int lds_gxe_project_sources(int64_t gxe, double* panel, int64_t columns,
+                            int columns_per_environment, int environment_start, double* leakages,
+                            int device_ptrs);
+int lds_gxe_pair_create(int64_t gxe, const double* right, int64_t columns,
+                        const double* row_weights, int64_t groups, int device_ptrs,
+                        int64_t* pair_out);
+int lds_gxe_pair_destroy(int64_t pair);
+int lds_gxe_target_score_block(int64_t gxe, int64_t j0, int64_t j1, int64_t pair,
+                               const double* scale_x, const double* scale_w, int64_t T,
+                               double* accum_xx, double* accum_xw, double* accum_wx,
+                               double* accum_ww, int64_t block_start, int64_t total_variants,
+                               int probe_count, int environment_start, int device_ptrs);
+int lds_gxe_normalize_scores(double* accum_xx, double* accum_xw, double* accum_wx,
+                             double* accum_ww, int64_t rows, int64_t K, int probe_count,
+                             int device_ptrs);
+int lds_philox_rademacher(const uint64_t* keys, int64_t probes, int64_t rows, double* out,
+                          int device_ptrs);
+
+/* ---------------------------------------------------------------------
  * Surrogate network of the learned control variate (no counterpart in the
  * reference): in_dim -> 128 -> 128 -> 128 -> out_dim, GELU (erf form) after the
  * hidden layers, FP32 master parameters, BF16 weights and activations in the

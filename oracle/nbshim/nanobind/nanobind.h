@@ -95,6 +95,11 @@ public:
 
     ndarray() = default;
     explicit ndarray(const array_desc& desc) : d(desc) {}
+    template <typename P, typename O>
+    ndarray(P* ptr, std::initializer_list<size_t> shp, const O& owner_object)
+        : ndarray(ptr, shp, capsule()) {
+        (void)owner_object;  // caller keeps the owning object alive
+    }
     template <typename P>
     ndarray(P* ptr, std::initializer_list<size_t> shp, capsule owner = capsule()) {
         d.data = (void*)ptr;
@@ -116,7 +121,31 @@ public:
     }
     template <typename U, typename... Rest>
     ndarray_view1<U> view() const { return ndarray_view1<U>{static_cast<U*>(d.data)}; }
+    // Element strides of a dense array: column-major when the type says
+    // f_contig, row-major otherwise.
+    int64_t stride(size_t i) const {
+        int64_t st = 1;
+        if (is_f_order()) {
+            for (size_t k = 0; k < i; ++k) st *= (int64_t)d.shape[k];
+        } else {
+            for (size_t k = i + 1; k < d.ndim; ++k) st *= (int64_t)d.shape[k];
+        }
+        return st;
+    }
+    template <typename... I, typename S = Scalar>
+    S& operator()(I... idx) const {
+        const size_t ix[] = {(size_t)idx...};
+        size_t off = 0;
+        for (size_t k = 0; k < sizeof...(I); ++k) off += ix[k] * (size_t)stride(k);
+        return data()[off];
+    }
+    static constexpr bool is_f_order() { return (std::is_same_v<Args, struct f_contig> || ...); }
 };
+
+template <typename T>
+struct is_ndarray : std::false_type {};
+template <typename... A>
+struct is_ndarray<ndarray<A...>> : std::true_type {};
 
 class object {
 public:
@@ -128,6 +157,19 @@ public:
     static object from_array(const array_desc& a) { object o; o.kind_ = Kind::Array; o.a_ = a; return o; }
     template <typename... A>
     object(const ndarray<A...>& arr) : kind_(Kind::Array), a_(arr.d) {}
+    template <typename V, std::enable_if_t<std::is_integral_v<V>, int> = 0>
+    object(V v) : i_((int64_t)v), u_((uint64_t)v), kind_(Kind::Int) {}
+    template <typename V, std::enable_if_t<std::is_floating_point_v<V>, int> = 0>
+    object(V v) : f_((double)v), kind_(Kind::Float) {}
+    template <typename V, std::enable_if_t<std::is_class_v<std::decay_t<V>> &&
+                                             !is_ndarray<std::decay_t<V>>::value &&
+                                             !std::is_same_v<std::decay_t<V>, object> &&
+                                             !std::is_same_v<std::decay_t<V>, std::string>, int> = 0>
+    object(V&&) : kind_(Kind::None) {}  // list / dict / tuple results are not inspected
+    object(const char*) : kind_(Kind::Str) {}
+    object(const std::string&) : kind_(Kind::Str) {}
+    object attr(const char*) const { return object(); }
+    template <typename... A> object operator()(A&&...) const { return object(); }
 
     bool is_none() const { return kind_ == Kind::None; }
     Kind kind() const { return kind_; }
@@ -146,10 +188,6 @@ public:
     python_error() : std::runtime_error("interrupted") {}
 };
 
-template <typename T>
-struct is_ndarray : std::false_type {};
-template <typename... A>
-struct is_ndarray<ndarray<A...>> : std::true_type {};
 
 template <typename T>
 T cast(const object& o) {
@@ -175,6 +213,19 @@ T cast(const object& o) {
     }
 }
 
+enum class rv_policy { automatic, automatic_reference, take_ownership, copy, move, reference,
+                       reference_internal, none };
+
+// C++ value -> object (the inverse direction of cast<T>(object)).
+template <typename V>
+object cast(V&& v, rv_policy = rv_policy::automatic) {
+    if constexpr (is_ndarray<std::decay_t<V>>::value) return object(v);
+    else if constexpr (std::is_arithmetic_v<std::decay_t<V>>) return object(v);
+    else return object();
+}
+
+template <typename T> size_t len(const T& v) { return v.size(); }
+
 class tuple {
 public:
     std::vector<object> items;
@@ -192,10 +243,28 @@ tuple make_tuple(A&&... a) {
 class dict {
 public:
     struct proxy {
+        object value;
         template <typename V> proxy& operator=(V&&) { return *this; }
+        operator const object&() const { return value; }
     };
     proxy operator[](const char*) { return proxy{}; }
+    proxy operator[](const char*) const { return proxy{}; }
+    proxy operator[](const std::string&) const { return proxy{}; }
+    bool contains(const char*) const { return false; }
+    size_t size() const { return 0; }
 };
+
+class list {
+public:
+    std::vector<object> items;
+    list() = default;
+    template <typename V> void append(V&& v) { items.push_back(object(std::forward<V>(v))); }
+    size_t size() const { return items.size(); }
+    object operator[](size_t i) const { return items.at(i); }
+};
+
+template <typename... A> struct init {};
+struct kw_only {};
 
 struct gil_scoped_acquire {};
 struct gil_scoped_release {};
@@ -203,17 +272,35 @@ struct gil_scoped_release {};
 struct arg {
     explicit arg(const char*) {}
     template <typename V> arg& operator=(V&&) { return *this; }
+    arg& noconvert(bool = true) { return *this; }
+    arg& none(bool = true) { return *this; }
 };
 
 class module_ {
 public:
     std::string& doc() { return doc_; }
     template <typename... A> module_& def(A&&...) { return *this; }
+    object attr(const char*) const { return object(); }
+    static module_ import_(const char*) { return module_(); }
 private:
     std::string doc_;
 };
 
+// Class registration is parsed but never run (NB_MODULE bodies are templates).
+template <typename T, typename... Extra>
+class class_ {
+public:
+    template <typename... A> class_(A&&...) {}
+    template <typename... A> class_& def(A&&...) { return *this; }
+    template <typename... A> class_& def_prop_ro(A&&...) { return *this; }
+    template <typename... A> class_& def_static(A&&...) { return *this; }
+    template <typename... A> class_& def_ro(A&&...) { return *this; }
+};
+
 }  // namespace nanobind
 
+// The module body is a template that is never instantiated: it is parsed, but
+// registration calls on the dependent module object are not resolved.
 #define NB_MODULE(name, m) \
-    [[maybe_unused]] static void nbshim_module_init_##name(::nanobind::module_& m)
+    template <typename NbShimModuleT> \
+    [[maybe_unused]] static void nbshim_module_init_##name(NbShimModuleT& m)

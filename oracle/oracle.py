@@ -473,3 +473,114 @@ class ReferenceWindowed:
                                                 nsnps, step_size, _ptr(rows),
                                                 0 if rows is None else rows.size, _ptr(out)))
         return out
+
+
+REF_GXE_SO = HERE / "_ref" / "libref_gxe.so"
+
+
+class ReferenceGxe:
+    """ctypes view of the reference's own gxeldcore.cpp (MultiEnvironmentKernel,
+    protected right pair, NumPy-Philox probes), compiled unchanged."""
+
+    def __init__(self, path: Path = REF_GXE_SO):
+        if not path.exists():
+            raise RuntimeError(f"reference library missing: {path} (run `make -C oracle ref`)")
+        L = C.CDLL(str(path))
+        L.refg_last_error.restype = _str
+        L.refg_kernel_create.argtypes = [_i64, _i64, _p, _i64, _p, _p, _i64, _p, _p, _p, _i64, _p,
+                                         _p, _i64, _p, _p, _int, _int, _int, C.POINTER(_p)]
+        L.refg_kernel_destroy.argtypes = [_p]
+        L.refg_source_block.argtypes = [_p, _p, _i64, _i64, _p, _i64, _p, _i64, _p, _i64, _p, _p,
+                                        _i64, _int, _int]
+        L.refg_project_sources.argtypes = [_p, _p, _i64, _i64, _int, _int, _p]
+        L.refg_prepare_pair.argtypes = [_p, _i64, _i64, _p, _i64, _int, C.POINTER(_p)]
+        L.refg_pair_destroy.argtypes = [_p]
+        L.refg_target_score_block.argtypes = [_p, _p, _i64, _i64, _p, _p, _p, _i64, _p, _p, _p, _p,
+                                              _i64, _i64, _int, _int, _int, _int]
+        L.refg_normalize_scores.argtypes = [_p, _p, _p, _p, _p, _i64, _i64, _int]
+        L.refg_philox_rademacher.argtypes = [_p, _i64, _int, _int, _p]
+        self.lib = L
+
+    def _chk(self, rc):
+        if rc:
+            raise RuntimeError(self.lib.refg_last_error().decode())
+
+    def kernel(self, environments, feature_basis, power_indices, power_offsets, ranks,
+               gram_values, gram_offsets, e2_gram_values, common_basis, directions, ddof,
+               annotation_bins, threads=1):
+        return _RefGxeKernel(self, environments, feature_basis, power_indices, power_offsets,
+                             ranks, gram_values, gram_offsets, e2_gram_values, common_basis,
+                             directions, ddof, annotation_bins, threads)
+
+    def philox_rademacher(self, keys, rows, threads=1):
+        keys = np.ascontiguousarray(keys, dtype=np.uint64)
+        out = np.empty((rows, keys.shape[0]), dtype=np.float64, order="F")
+        self._chk(self.lib.refg_philox_rademacher(_ptr(keys), keys.shape[0], int(rows),
+                                                   int(threads), _ptr(out)))
+        return out
+
+
+class _RefGxeKernel:
+    def __init__(self, ref, env, fb, pidx, poff, ranks, gv, goff, e2, common, dirs, ddof, bins,
+                 threads):
+        self.ref = ref
+        F = lambda a: np.asfortranarray(a, dtype=np.float64)
+        self.keep = [F(env), F(fb), np.ascontiguousarray(pidx, np.int64),
+                     np.ascontiguousarray(poff, np.int64), np.ascontiguousarray(ranks, np.int32),
+                     np.ascontiguousarray(gv, np.float64), np.ascontiguousarray(goff, np.int64),
+                     np.ascontiguousarray(e2, np.float64), F(common), F(dirs)]
+        env, fb, pidx, poff, ranks, gv, goff, e2, common, dirs = self.keep
+        self.N, self.E = env.shape
+        h = _p()
+        ref._chk(ref.lib.refg_kernel_create(
+            self.N, self.E, _ptr(env), fb.shape[1], _ptr(fb), _ptr(pidx), pidx.size, _ptr(poff),
+            _ptr(ranks), _ptr(gv), gv.size, _ptr(goff), _ptr(e2), common.shape[1], _ptr(common),
+            _ptr(dirs), int(ddof), int(bins), int(threads), C.byref(h)))
+        self.h = h
+
+    def source_block(self, target, genotype, probes, annotation, scale_x, scale_w,
+                     environment_start, annotation_is_sqrt=False):
+        F = lambda a: np.asfortranarray(a, dtype=np.float64)
+        g, z, a, sx, sw = F(genotype), F(probes), F(annotation), F(scale_x), F(scale_w)
+        self.ref._chk(self.ref.lib.refg_source_block(
+            self.h, _ptr(target), target.shape[0], target.shape[1], _ptr(g), g.shape[1], _ptr(z),
+            z.shape[1], _ptr(a), a.shape[1], _ptr(sx), _ptr(sw), sx.shape[1],
+            int(environment_start), int(bool(annotation_is_sqrt))))
+
+    def project_sources(self, panel, columns_per_environment, environment_start):
+        tile = panel.shape[1] // (2 * columns_per_environment)
+        leak = np.empty(max(tile, 1))
+        self.ref._chk(self.ref.lib.refg_project_sources(
+            self.h, _ptr(panel), panel.shape[0], panel.shape[1], int(columns_per_environment),
+            int(environment_start), _ptr(leak)))
+        return leak[:tile]
+
+    def pair(self, right, row_weights, threads=1):
+        right = np.asfortranarray(right, dtype=np.float64)
+        w = np.asfortranarray(row_weights, dtype=np.float64)
+        h = _p()
+        self.ref._chk(self.ref.lib.refg_prepare_pair(_ptr(right), right.shape[0], right.shape[1],
+                                                     _ptr(w), w.shape[1], int(threads), C.byref(h)))
+        return h
+
+    def target_score_block(self, genotype, pair, scale_x, scale_w, accs, block_start,
+                           total_variants, probe_count, environment_start):
+        F = lambda a: np.asfortranarray(a, dtype=np.float64)
+        g, sx, sw = F(genotype), F(scale_x), F(scale_w)
+        xx, xw, wx, ww = accs
+        self.ref._chk(self.ref.lib.refg_target_score_block(
+            self.h, _ptr(g), g.shape[0], g.shape[1], pair, _ptr(sx), _ptr(sw), sx.shape[1],
+            _ptr(xx), _ptr(xw), _ptr(wx), _ptr(ww), xx.shape[0], xx.shape[1], int(block_start),
+            int(total_variants), int(probe_count), int(environment_start)))
+
+    def normalize_scores(self, accs, probe_count):
+        xx, xw, wx, ww = accs
+        self.ref._chk(self.ref.lib.refg_normalize_scores(
+            self.h, _ptr(xx), _ptr(xw), _ptr(wx), _ptr(ww), xx.shape[0], xx.shape[1],
+            int(probe_count)))
+
+    def __del__(self):
+        try:
+            self.ref.lib.refg_kernel_destroy(self.h)
+        except Exception:
+            pass

@@ -1674,6 +1674,342 @@ void win_set_cv(Context& c, WinPlan& pl, const double* annot, int split, int D) 
     }
 }
 
+// ---------------------------------------------------------------------------
+// SUMMIT-GxE multi-environment products (MultiEnvironmentKernel,
+// gxeldcore.cpp:10281-12557) on a resident genotype image.  The image's
+// standardization (mean imputation, its ddof) is the genotype block the
+// reference's driver passes (GenomewideEnvLDScore._read_genotype_block).
+// ---------------------------------------------------------------------------
+struct GxeCtx {
+    std::shared_ptr<Prepared> P;
+    int64_t N = 0, E = 0, r = 0;
+    int K = 0;
+    std::vector<int32_t> ranks;
+    DevBuf env, common, dirs_ones, ranks_d, ones_M;
+    std::vector<DevBuf> basis0;          // per environment: N x rank fixed-effect basis
+    // workspaces (grow-only)
+    DevBuf probes, annot, sx, sw, panel, y, wq, wcs, rowind, sc, binoff, coef, coef2, denom;
+    DevBuf sacc, acc4, guards, status, flag;
+};
+
+struct GxePair {
+    int64_t N = 0, C = 0, G = 0;
+    DevBuf ypair;                        // N_pad x 2C FP64, rows N..N_pad zero
+    int B = 0;                           // probe count the digits were made for
+    DevBuf yq, ycs;
+    CUtensorMap tmB;
+};
+
+std::map<int64_t, std::unique_ptr<GxeCtx>>& gxe_table() {
+    static std::map<int64_t, std::unique_ptr<GxeCtx>> t;
+    return t;
+}
+std::map<int64_t, std::unique_ptr<GxePair>>& gxe_pair_table() {
+    static std::map<int64_t, std::unique_ptr<GxePair>> t;
+    return t;
+}
+
+// Device view of a caller array: the pointer itself, or a copy in `buf`.
+template <typename T>
+const T* dev_in(Context& c, DevBuf& buf, const T* p, size_t n, int device_ptrs) {
+    if (device_ptrs || !p) return p;
+    T* d = buf.as<T>(std::max<size_t>(n, 1));
+    h2d(d, p, n, c.st);
+    return d;
+}
+
+// source_block: target (N x T 2 K B, column-major) += the contribution of SNPs
+// [j0, j1) (gxeldcore.cpp:11008-11240).
+void gxe_source_impl(Context& c, GxeCtx& g, int64_t j0, int64_t j1, const double* probes, int64_t B,
+                     const double* annot, int is_sqrt, const double* sx, const double* sw, int64_t T,
+                     int env_start, double* target, int device_ptrs) {
+    const Prepared& P = *g.P;
+    const int64_t L = j1 - j0, N = P.g.N, Np = P.g.N_pad, K = g.K;
+    if (B <= 0 || T <= 0 || env_start < 0 || env_start + T > g.E || L <= 0 || j0 < 0 || j1 > P.g.M)
+        fail(LDS_ERR_ARG, "Multi-environment native source inputs have incompatible dimensions");
+    const int64_t G = T * 2 * K, C = G * B;
+    const double* dz = dev_in(c, g.probes, probes, (size_t)(L * B), device_ptrs);
+    const double* da = dev_in(c, g.annot, annot, (size_t)(L * K), device_ptrs);
+    const double* dsx = dev_in(c, g.sx, sx, (size_t)(L * T), device_ptrs);
+    const double* dsw = dev_in(c, g.sw, sw, (size_t)(L * T), device_ptrs);
+    unsigned* flag = g.flag.as<unsigned>(1);
+    ck(cudaMemsetAsync(flag, 0, 4, c.st), "memset");
+    launch_gxe_check(dz, L * B, dsx, dsw, L * T, da, is_sqrt ? 0 : L * K, flag, c.st);
+    // Member lists need the annotation and scales on the host.
+    std::vector<double> ha((size_t)(L * K)), hx((size_t)(L * T)), hw((size_t)(L * T));
+    d2h(ha.data(), da, ha.size(), c.st);
+    d2h(hx.data(), dsx, hx.size(), c.st);
+    d2h(hw.data(), dsw, hw.size(), c.st);
+    unsigned fv = 0;
+    d2h(&fv, flag, 1, c.st);
+    ck(cudaStreamSynchronize(c.st), "gxe inputs");
+    if (fv) fail(LDS_ERR_ARG, "Multi-environment native source inputs contain invalid values");
+    double* dtarget = device_ptrs ? target : g.panel.as<double>((size_t)(N * C));
+    if (!device_ptrs) h2d(dtarget, target, (size_t)(N * C), c.st);
+    const int nc = umma::ncolp_for((int)B);
+    // SNP chunks bound the weight-digit buffer (G x 2 x ncolp x chunk bytes).
+    const int64_t cap = (int64_t)1 << 30;
+    int64_t Lb = std::max<int64_t>(128, cap / std::max<int64_t>(1, G * 2 * nc) / 128 * 128);
+    Lb = std::min(Lb, round_up(L, 128));
+    double* Y = g.y.as<double>((size_t)(Np * C));
+    for (int64_t a = 0; a < L; a += Lb) {
+        const int64_t b = std::min(L, a + Lb), Lc = b - a;
+        // Super-bin (e, h, k): members with sqrt(a_jk) > 0, scale sqrt(a_jk) s_h,e[j].
+        std::vector<int64_t> off((size_t)G + 1, 0);
+        std::vector<int32_t> ri;
+        std::vector<double> scv;
+        int64_t lmax = 128;
+        for (int64_t e = 0; e < T; ++e)
+            for (int h = 0; h < 2; ++h)
+                for (int64_t k = 0; k < K; ++k) {
+                    const int64_t gi = (e * 2 + h) * K + k;
+                    off[(size_t)gi] = (int64_t)ri.size();
+                    const double* s = (h == 0 ? hx.data() : hw.data()) + e * L;
+                    for (int64_t j = a; j < b; ++j) {
+                        const double av = ha[(size_t)(k * L + j)];
+                        const double sa = is_sqrt ? av : std::sqrt(std::max(0.0, av));
+                        if (!(sa > 0.0)) continue;
+                        ri.push_back((int32_t)(j - a));
+                        scv.push_back(sa * s[j]);
+                    }
+                    const int64_t n = (int64_t)ri.size() - off[(size_t)gi];
+                    const int64_t np = round_up(n, 128);
+                    for (int64_t q = n; q < np; ++q) {
+                        ri.push_back(0);
+                        scv.push_back(0.0);
+                    }
+                    lmax = std::max(lmax, np);
+                }
+        off[(size_t)G] = (int64_t)ri.size();
+        const size_t nm = std::max<size_t>(ri.size(), 1);
+        h2d(g.rowind.as<int32_t>(nm), ri.data(), ri.size(), c.st);
+        h2d(g.sc.as<double>(nm), scv.data(), scv.size(), c.st);
+        h2d(g.binoff.as<int64_t>(off.size()), off.data(), off.size(), c.st);
+        const size_t wbytes = (size_t)(G * 2 * nc) * (size_t)lmax;
+        int8_t* wq = g.wq.as<int8_t>(wbytes);
+        ck(cudaMemsetAsync(wq, 0, wbytes, c.st), "memset weights");
+        umma::P1UWeights uw;
+        uw.K = (int)G;
+        uw.V = (int)B;
+        uw.ncolp = nc;
+        uw.lmax = lmax;
+        uw.rowind = static_cast<int32_t*>(g.rowind.p);
+        uw.sc = static_cast<double*>(g.sc.p);
+        uw.bin_off = static_cast<int64_t*>(g.binoff.p);
+        uw.wq = wq;
+        uw.colscale = g.wcs.as<double>((size_t)(G * B));
+        const double* mean = static_cast<const double*>(P.d_mean.p) + j0 + a;
+        const double* sdinv = static_cast<const double*>(P.d_sdinv.p) + j0 + a;
+        umma::launch_p1_weights4(uw, mean, sdinv, dz + a, L, c.st);
+        const CUtensorMap tmW = make_map_2d(wq, (uint64_t)lmax, (uint64_t)(G * 2 * nc), (uint64_t)lmax,
+                                            128, (uint32_t)std::min(256, nc),
+                                            CU_TENSOR_MAP_SWIZZLE_128B);
+        umma::P1UArgs pa;
+        pa.K = (int)G;
+        pa.V = (int)B;
+        pa.ncolp = nc;
+        pa.ngroups = (nc + 255) / 256;
+        pa.box_rows = std::min(256, nc);
+        pa.nbp = P.g.nbp;
+        pa.N_pad = Np;
+        pa.bin_off = uw.bin_off;
+        pa.rowind = uw.rowind;
+        pa.codes = P.g.codes + (j0 + a) * P.g.nbp;
+        pa.colscale = uw.colscale;
+        pa.Y = Y;
+        pa.status = g.status.as<unsigned>(1);
+        ck(cudaMemsetAsync(pa.status, 0, 4, c.st), "memset");
+        umma::launch_p1_umma(tmW, pa, Np, c.st);
+        launch_gxe_source_finalize(Y, N, Np, C, (int)(K * B), static_cast<double*>(g.env.p), N,
+                                   env_start, dtarget, N, c.st);
+        unsigned stv = 0;
+        d2h(&stv, pa.status, 1, c.st);
+        ck(cudaStreamSynchronize(c.st), "gxe source");
+        if (stv) fail(LDS_ERR_CUDA, "GxE source tensor-core pipeline wait timed out (code %u)", stv);
+        (void)Lc;
+    }
+    if (!device_ptrs) {
+        d2h(target, dtarget, (size_t)(N * C), c.st);
+        ck(cudaStreamSynchronize(c.st), "gxe source copy");
+    }
+}
+
+// project_sources (gxeldcore.cpp:11583-11729); leakages[e] for the tile.
+void gxe_project_impl(Context& c, GxeCtx& g, double* panel, int64_t cols, int cpe, int env_start,
+                      int device_ptrs, double* leakages) {
+    const int64_t N = g.N;
+    if (cpe <= 0 || cols % (2 * (int64_t)cpe) != 0)
+        fail(LDS_ERR_ARG, "Multi-environment native projection panel is mis-sized");
+    const int64_t T = cols / (2 * (int64_t)cpe);
+    if (T <= 0 || env_start < 0 || env_start + T > g.E)
+        fail(LDS_ERR_ARG, "Multi-environment native projection tile is outside the environment axis");
+    double* dp = device_ptrs ? panel : g.panel.as<double>((size_t)(N * cols));
+    if (!device_ptrs) h2d(dp, panel, (size_t)(N * cols), c.st);
+    const int mb = col_dots_max_basis();
+    // P <- P - U (U^T P), basis in chunks of mb columns
+    for (int64_t a0 = 0; a0 < g.r; a0 += mb) {
+        const int nb = (int)std::min<int64_t>(mb, g.r - a0);
+        double* coef = g.coef.as<double>((size_t)(cols * nb));
+        const double* U = static_cast<const double*>(g.common.p) + a0 * N;
+        launch_col_dots(dp, N, N, cols, U, N, nb, 0, coef, c.st);
+        launch_sub_lowrank(dp, N, N, cols, U, N, nb, coef, 0, 1.0, c.st);
+    }
+    // direction and mean from the same values: basis [d_e, 1]
+    const int64_t seg = 2 * (int64_t)cpe;
+    double* coef2 = g.coef2.as<double>((size_t)(seg * 2));
+    for (int64_t e = 0; e < T; ++e) {
+        double* v = dp + e * seg * N;
+        const double* D = static_cast<const double*>(g.dirs_ones.p) + (env_start + e) * 2 * N;
+        launch_col_dots(v, N, N, seg, D, N, 2, 0, coef2, c.st);
+        launch_sub_lowrank(v, N, N, seg, D, N, 2, coef2, 1, 1.0 / (double)N, c.st);
+    }
+    // leakage onto each environment's fixed-effect basis
+    std::vector<double> den((size_t)seg), co;
+    for (int64_t e = 0; e < T; ++e) {
+        const int env = (int)(env_start + e);
+        const int rank = g.ranks[(size_t)env];
+        double* v = dp + e * seg * N;
+        double* dd = g.denom.as<double>((size_t)seg);
+        launch_col_dots(v, N, N, seg, nullptr, N, 1, 1, dd, c.st);
+        std::vector<double> leaked((size_t)seg, 0.0);
+        d2h(den.data(), dd, (size_t)seg, c.st);
+        for (int a0 = 0; a0 < rank; a0 += mb) {
+            const int nb = std::min(mb, rank - a0);
+            double* coef = g.coef.as<double>((size_t)(seg * nb));
+            const double* B0 = static_cast<const double*>(g.basis0[(size_t)env].p) + (int64_t)a0 * N;
+            launch_col_dots(v, N, N, seg, B0, N, nb, 0, coef, c.st);
+            co.resize((size_t)(seg * nb));
+            d2h(co.data(), coef, co.size(), c.st);
+            ck(cudaStreamSynchronize(c.st), "gxe leakage");
+            for (int64_t q = 0; q < seg; ++q)
+                for (int a = 0; a < nb; ++a) leaked[(size_t)q] += co[(size_t)(q * nb + a)] * co[(size_t)(q * nb + a)];
+        }
+        ck(cudaStreamSynchronize(c.st), "gxe leakage");
+        double maximum = 0.0;
+        for (int64_t q = 0; q < seg; ++q) {
+            const double rel = den[(size_t)q] > 0.0 ? std::sqrt(leaked[(size_t)q] / den[(size_t)q])
+                                                    : std::numeric_limits<double>::infinity();
+            if (!std::isfinite(rel)) fail(LDS_ERR_ARG, "Multi-environment native source leakage is non-finite");
+            maximum = std::max(maximum, rel);
+        }
+        if (maximum > 1.0e-9)
+            fail(LDS_ERR_ARG, "Multi-environment native source projection has excessive leakage");
+        if (leakages) leakages[e] = maximum;
+    }
+    if (!device_ptrs) d2h(panel, dp, (size_t)(N * cols), c.st);
+    ck(cudaStreamSynchronize(c.st), "gxe project");
+}
+
+// [right, w o right] sealed on the device (prepare_protected_row_weighted_pair,
+// gxeldcore.cpp:9808); column c uses weight column c / (C / G).
+std::unique_ptr<GxePair> gxe_pair_impl(Context& c, const Prepared& P, const double* right, int64_t N,
+                                       int64_t C, const double* w, int64_t G, int device_ptrs) {
+    if (N != P.g.N || C <= 0 || G <= 0 || C % G != 0)
+        fail(LDS_ERR_ARG, "Protected GxE right-pair inputs have incompatible dimensions");
+    auto pr = std::make_unique<GxePair>();
+    pr->N = N;
+    pr->C = C;
+    pr->G = G;
+    DevBuf tr, tw;
+    const double* dr = dev_in(c, tr, right, (size_t)(N * C), device_ptrs);
+    const double* dw = dev_in(c, tw, w, (size_t)(N * G), device_ptrs);
+    double* yp = pr->ypair.as<double>((size_t)(P.g.N_pad * 2 * C));
+    launch_gxe_pair(dr, N, N, P.g.N_pad, C, C / G, dw, N, 0, yp, c.st);
+    ck(cudaGetLastError(), "launch");
+    ck(cudaStreamSynchronize(c.st), "gxe pair");
+    return pr;
+}
+
+// target_score_block (gxeldcore.cpp:11731-11936).
+void gxe_target_impl(Context& c, GxeCtx& g, int64_t j0, int64_t j1, GxePair& pr, const double* sx,
+                     const double* sw, int64_t T, double* axx, double* axw, double* awx, double* aww,
+                     int64_t block_start, int64_t total, int probe_count, int env_start,
+                     int device_ptrs) {
+    const Prepared& P = *g.P;
+    const int64_t L = j1 - j0, N = P.g.N, Np = P.g.N_pad, K = g.K;
+    if (block_start < 0 || total <= 0 || block_start + L > total || probe_count <= 0 || T <= 0 ||
+        env_start < 0 || env_start + T > g.E || L <= 0 || j0 < 0 || j1 > P.g.M)
+        fail(LDS_ERR_ARG, "Multi-environment native target scale/block metadata is invalid");
+    const int64_t B = probe_count, pair_cols = T * 2 * K * B;
+    if (pr.N != N || pr.C != pair_cols)
+        fail(LDS_ERR_ARG, "Multi-environment native target pair is incompatible with the tile");
+    const int64_t Kp = 2 * T * 2 * K;
+    const int nc = umma::ncolp_for((int)B);
+    if (pr.B != (int)B) {
+        int8_t* yq = pr.yq.as<int8_t>((size_t)(Kp * nc * Np));
+        umma::launch_quantize_y4(static_cast<double*>(pr.ypair.p), N, Np, (int)Kp, (int)B, nc, yq,
+                                 pr.ycs.as<double>((size_t)(Kp * B)), c.st);
+        const int nb = umma::p2_bins_per_cta(nc, (int)Kp);
+        pr.tmB = make_map_2d(yq, (uint64_t)Np, (uint64_t)(Kp * nc), (uint64_t)Np, 128,
+                             (uint32_t)std::min(256, nb * nc), CU_TENSOR_MAP_SWIZZLE_128B);
+        pr.B = (int)B;
+    }
+    const double* dsx = dev_in(c, g.sx, sx, (size_t)(L * T), device_ptrs);
+    const double* dsw = dev_in(c, g.sw, sw, (size_t)(L * T), device_ptrs);
+    unsigned* flag = g.flag.as<unsigned>(1);
+    ck(cudaMemsetAsync(flag, 0, 4, c.st), "memset");
+    launch_gxe_check(dsx, 0, dsx, dsw, L * T, dsx, 0, flag, c.st);
+    unsigned fv = 0;
+    d2h(&fv, flag, 1, c.st);
+    ck(cudaStreamSynchronize(c.st), "gxe scales");
+    if (fv) fail(LDS_ERR_ARG, "Multi-environment native target scales contain invalid values");
+    double* S = g.sacc.as<double>((size_t)(L * Kp));
+    ck(cudaMemsetAsync(S, 0, sizeof(double) * (size_t)(L * Kp), c.st), "memset");
+    const int nb = umma::p2_bins_per_cta(nc, (int)Kp);
+    umma::P2UArgs u;
+    u.K = (int)Kp;
+    u.V = (int)B;
+    u.ncolp = nc;
+    u.bins_per_cta = nb;
+    u.ngroups = (nb * nc + 255) / 256;
+    u.box_rows = std::min(256, nb * nc);
+    u.nkt = (int)(Np / 128);
+    u.M = P.g.M;
+    u.j0 = j0;
+    u.j1 = j1;
+    u.out_row0 = j0;
+    u.colscale = static_cast<double*>(pr.ycs.p);
+    u.mean = static_cast<double*>(P.d_mean.p);
+    u.sdinv = static_cast<double*>(P.d_sdinv.p);
+    u.left_scale = static_cast<double*>(g.ones_M.p);
+    u.accum = S;
+    u.guard_counts = g.guards.as<unsigned long long>(2);
+    u.extreme_warn = std::numeric_limits<double>::infinity();
+    u.drop_extreme = 0;
+    u.status = g.status.as<unsigned>(1);
+    ck(cudaMemsetAsync(u.status, 0, 4, c.st), "memset");
+    const CUtensorMap tmA = make_map_2d(P.g.codes, (uint64_t)P.g.nbp, (uint64_t)P.g.M_pad,
+                                        (uint64_t)P.g.nbp, 32, 128, CU_TENSOR_MAP_SWIZZLE_NONE);
+    umma::launch_p2_umma(tmA, pr.tmB, u, c.st);
+    const size_t nacc = (size_t)(g.E * total * K);
+    double* A[4];
+    if (device_ptrs) {
+        A[0] = axx;
+        A[1] = axw;
+        A[2] = awx;
+        A[3] = aww;
+    } else {
+        double* base = g.acc4.as<double>(4 * nacc);
+        const double* hs[4] = {axx, axw, awx, aww};
+        for (int q = 0; q < 4; ++q) {
+            A[q] = base + (size_t)q * nacc;
+            h2d(A[q], hs[q], nacc, c.st);
+        }
+    }
+    launch_gxe_target_finalize(S, L, (int)Kp, (int)K, (int)T, dsx, dsw, L,
+                               static_cast<int32_t*>(g.ranks_d.p), N, env_start, total, block_start,
+                               A[0], A[1], A[2], A[3], c.st);
+    ck(cudaGetLastError(), "launch");
+    unsigned stv = 0;
+    d2h(&stv, u.status, 1, c.st);
+    if (!device_ptrs) {
+        double* hs[4] = {axx, axw, awx, aww};
+        for (int q = 0; q < 4; ++q) d2h(hs[q], A[q], nacc, c.st);
+    }
+    ck(cudaStreamSynchronize(c.st), "gxe target");
+    if (stv) fail(LDS_ERR_CUDA, "GxE target tensor-core pipeline wait timed out (code %u)", stv);
+}
+
 void gw_ldscore_impl(const uint8_t* bed_rows, int64_t row_bytes, int64_t n_total, int64_t M,
                      const int64_t* row_sel, int64_t n_sel, const double* annot, int64_t K,
                      int nvecs, int step, int vtile, uint64_t seed, int dist, int ddof,
@@ -2567,5 +2903,214 @@ LDS_API int lds_synth_bed(int64_t n, int64_t M, uint64_t seed, const int64_t* t0
         launch_synth(n, M, seed, a, b, missing, o, c.st);
         d2h(out, o, (size_t)(nb * M), c.st);
         ck(cudaStreamSynchronize(c.st), "synth");
+    });
+}
+
+
+// ---------------------------------------------------------------------------
+// SUMMIT-GxE C ABI (include/lds.h)
+// ---------------------------------------------------------------------------
+static GxeCtx& gxe_of(int64_t h) {
+    auto it = gxe_table().find(h);
+    if (it == gxe_table().end()) fail(LDS_ERR_ARG, "unknown GxE kernel handle");
+    return *it->second;
+}
+static GxePair& gxe_pair_of(int64_t h) {
+    auto it = gxe_pair_table().find(h);
+    if (it == gxe_pair_table().end()) fail(LDS_ERR_ARG, "unknown GxE right-pair handle");
+    return *it->second;
+}
+
+LDS_API int lds_gxe_create(int64_t geno, int64_t E, const double* environments, int64_t r,
+                           const double* common_basis, const double* directions, int64_t F,
+                           const double* feature_basis, const int64_t* power_indices,
+                           const int64_t* power_offsets, const int32_t* ranks, int annotation_bins,
+                           int64_t* handle_out) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        ensure_device(c);
+        auto it = geno_table().find(geno);
+        if (it == geno_table().end()) fail(LDS_ERR_ARG, "unknown genotype handle");
+        const int64_t N = it->second->g.N;
+        if (N <= 2 || E <= 0 || F <= 0 || r < 0 || annotation_bins <= 0 || !environments ||
+            !directions || !feature_basis || !power_indices || !power_offsets || !ranks ||
+            (r > 0 && !common_basis))
+            fail(LDS_ERR_ARG, "Multi-environment native kernel inputs have incompatible dimensions");
+        if (power_offsets[0] != 0)
+            fail(LDS_ERR_ARG, "Multi-environment native feature offsets do not span their buffers");
+        auto g = std::make_unique<GxeCtx>();
+        g->P = it->second;
+        g->N = N;
+        g->E = E;
+        g->r = r;
+        g->K = annotation_bins;
+        g->ranks.assign(ranks, ranks + E);
+        for (int64_t e = 0; e < E; ++e) {
+            const int rk = ranks[e];
+            if (rk <= 0 || rk >= N) fail(LDS_ERR_ARG, "Multi-environment native feature rank is invalid");
+            for (int pw = 0; pw < 4; ++pw)
+                if (power_offsets[4 * e + pw + 1] - power_offsets[4 * e + pw] != rk)
+                    fail(LDS_ERR_ARG, "Multi-environment native power-index ranges are malformed");
+        }
+        h2d(g->env.as<double>((size_t)(N * E)), environments, (size_t)(N * E), c.st);
+        if (r > 0) h2d(g->common.as<double>((size_t)(N * r)), common_basis, (size_t)(N * r), c.st);
+        // [d_e, 1] per environment for the direction and mean projection
+        std::vector<double> dones((size_t)(2 * N * E), 1.0);
+        for (int64_t e = 0; e < E; ++e)
+            std::memcpy(&dones[(size_t)(2 * e * N)], directions + e * N, sizeof(double) * (size_t)N);
+        h2d(g->dirs_ones.as<double>(dones.size()), dones.data(), dones.size(), c.st);
+        h2d(g->ranks_d.as<int32_t>((size_t)E), ranks, (size_t)E, c.st);
+        std::vector<double> ones((size_t)std::max<int64_t>(it->second->g.M, 1), 1.0);
+        h2d(g->ones_M.as<double>(ones.size()), ones.data(), ones.size(), c.st);
+        g->basis0.resize((size_t)E);
+        for (int64_t e = 0; e < E; ++e) {
+            const int rk = ranks[e];
+            std::vector<double> b((size_t)(N * rk));
+            for (int a = 0; a < rk; ++a) {
+                const int64_t col = power_indices[power_offsets[4 * e] + a];
+                if (col < 0 || col >= F) fail(LDS_ERR_ARG, "Multi-environment native power index is out of range");
+                std::memcpy(&b[(size_t)(a * N)], feature_basis + col * N, sizeof(double) * (size_t)N);
+            }
+            h2d(g->basis0[(size_t)e].as<double>(b.size()), b.data(), b.size(), c.st);
+            ck(cudaStreamSynchronize(c.st), "gxe create");
+        }
+        ck(cudaStreamSynchronize(c.st), "gxe create");
+        const int64_t h = next_handle();
+        gxe_table()[h] = std::move(g);
+        *handle_out = h;
+    });
+}
+
+LDS_API int lds_gxe_destroy(int64_t gxe) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        if (c.ready) ck(cudaStreamSynchronize(c.st), "sync");
+        gxe_table().erase(gxe);
+    });
+}
+
+LDS_API int lds_gxe_source_block(int64_t gxe, int64_t j0, int64_t j1, const double* probes,
+                                 int64_t B, const double* annotation, int annotation_is_sqrt,
+                                 const double* scale_x, const double* scale_w, int64_t T,
+                                 int environment_start, double* target, int device_ptrs) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        if (!probes || !annotation || !scale_x || !scale_w || !target) fail(LDS_ERR_ARG, "null argument");
+        gxe_source_impl(c, gxe_of(gxe), j0, j1, probes, B, annotation, annotation_is_sqrt, scale_x,
+                        scale_w, T, environment_start, target, device_ptrs);
+    });
+}
+
+LDS_API int lds_gxe_project_sources(int64_t gxe, double* panel, int64_t columns,
+                                    int columns_per_environment, int environment_start,
+                                    double* leakages, int device_ptrs) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        if (!panel) fail(LDS_ERR_ARG, "null argument");
+        gxe_project_impl(c, gxe_of(gxe), panel, columns, columns_per_environment, environment_start,
+                         device_ptrs, leakages);
+    });
+}
+
+LDS_API int lds_gxe_pair_create(int64_t gxe, const double* right, int64_t columns,
+                                const double* row_weights, int64_t groups, int device_ptrs,
+                                int64_t* pair_out) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        if (!right || !row_weights) fail(LDS_ERR_ARG, "null argument");
+        GxeCtx& g = gxe_of(gxe);
+        auto pr = gxe_pair_impl(c, *g.P, right, g.N, columns, row_weights, groups, device_ptrs);
+        const int64_t h = next_handle();
+        gxe_pair_table()[h] = std::move(pr);
+        *pair_out = h;
+    });
+}
+
+LDS_API int lds_gxe_pair_destroy(int64_t pair) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        if (c.ready) ck(cudaStreamSynchronize(c.st), "sync");
+        gxe_pair_table().erase(pair);
+    });
+}
+
+LDS_API int lds_gxe_target_score_block(int64_t gxe, int64_t j0, int64_t j1, int64_t pair,
+                                       const double* scale_x, const double* scale_w, int64_t T,
+                                       double* accum_xx, double* accum_xw, double* accum_wx,
+                                       double* accum_ww, int64_t block_start, int64_t total_variants,
+                                       int probe_count, int environment_start, int device_ptrs) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        if (!scale_x || !scale_w || !accum_xx || !accum_xw || !accum_wx || !accum_ww)
+            fail(LDS_ERR_ARG, "null argument");
+        gxe_target_impl(c, gxe_of(gxe), j0, j1, gxe_pair_of(pair), scale_x, scale_w, T, accum_xx,
+                        accum_xw, accum_wx, accum_ww, block_start, total_variants, probe_count,
+                        environment_start, device_ptrs);
+    });
+}
+
+LDS_API int lds_gxe_normalize_scores(double* accum_xx, double* accum_xw, double* accum_wx,
+                                     double* accum_ww, int64_t rows, int64_t K, int probe_count,
+                                     int device_ptrs) {
+    return guarded([&] {
+        if (probe_count <= 0)
+            fail(LDS_ERR_ARG, "Multi-environment native score normalization requires probes");
+        if (rows <= 0 || K <= 0) fail(LDS_ERR_ARG, "Multi-environment native score normalization shape is invalid");
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        ensure_device(c);
+        const size_t n = (size_t)(rows * K);
+        double* hs[4] = {accum_xx, accum_xw, accum_wx, accum_ww};
+        DevBuf tmp;
+        double* base = device_ptrs ? nullptr : tmp.as<double>(4 * n);
+        for (int q = 0; q < 4; ++q) {
+            double* d = device_ptrs ? hs[q] : base + (size_t)q * n;
+            if (!device_ptrs) h2d(d, hs[q], n, c.st);
+            launch_scale(d, (int64_t)n, 1.0 / (double)probe_count, c.st);
+        }
+        // non-finite check (gxeldcore.cpp:12540-12550)
+        DevBuf fl;
+        unsigned* flag = fl.as<unsigned>(1);
+        ck(cudaMemsetAsync(flag, 0, 4, c.st), "memset");
+        for (int q = 0; q < 4; ++q) {
+            double* d = device_ptrs ? hs[q] : base + (size_t)q * n;
+            launch_gxe_check(d, (int64_t)n, d, d, 0, d, 0, flag, c.st);
+            if (!device_ptrs) d2h(hs[q], d, n, c.st);
+        }
+        unsigned fv = 0;
+        d2h(&fv, flag, 1, c.st);
+        ck(cudaStreamSynchronize(c.st), "normalize");
+        if (fv) fail(LDS_ERR_ARG, "Multi-environment native normalized scores are non-finite");
+    });
+}
+
+LDS_API int lds_philox_rademacher(const uint64_t* keys, int64_t probes, int64_t rows, double* out,
+                                  int device_ptrs) {
+    return guarded([&] {
+        if (!keys || !out || rows <= 0 || probes <= 0)
+            fail(LDS_ERR_ARG, "Native Philox Rademacher inputs are invalid");
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        ensure_device(c);
+        DevBuf k, o;
+        const uint64_t* dk = keys;
+        double* dout = out;
+        if (!device_ptrs) {
+            uint64_t* kk = k.as<uint64_t>((size_t)(2 * probes));
+            h2d(kk, keys, (size_t)(2 * probes), c.st);
+            dk = kk;
+            dout = o.as<double>((size_t)(rows * probes));
+        }
+        launch_philox_rademacher(dk, probes, rows, dout, c.st);
+        ck(cudaGetLastError(), "launch");
+        if (!device_ptrs) d2h(out, dout, (size_t)(rows * probes), c.st);
+        ck(cudaStreamSynchronize(c.st), "philox");
     });
 }

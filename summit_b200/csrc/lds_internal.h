@@ -126,6 +126,33 @@ void launch_gram_ld(const CUtensorMap& tmC, const GramArgs& a, int n_items, cuda
 void launch_gram_reduce(const double* partial, const int32_t* slot_beg, int64_t row0, int64_t row1,
                         int K, double* out, int64_t ld_row, int64_t ld_col, cudaStream_t st);
 
+// GxE (lds_gxe.cu): see the file header for the column layouts.
+void launch_gxe_source_finalize(const double* Y, int64_t N, int64_t N_pad, int64_t C, int cols_half,
+                                const double* env, int64_t env_ld, int env_start, double* target,
+                                int64_t t_ld, cudaStream_t st);
+// out[c nb + a] = basis_a . panel_c (basis null: column sums, nb = 1); with
+// `squares` out[c] = panel_c . panel_c.  nb <= col_dots_max_basis().
+void launch_col_dots(const double* panel, int64_t p_ld, int64_t N, int64_t C, const double* basis,
+                     int64_t b_ld, int nb, int squares, double* out, cudaStream_t st);
+int col_dots_max_basis();
+// panel_c -= sum_a basis_a coef[c nb + a] (the last basis column is all ones,
+// scaled by last_scale, when ones_last).
+void launch_sub_lowrank(double* panel, int64_t ld, int64_t N, int64_t C, const double* basis,
+                        int64_t b_ld, int nb, const double* coef, int ones_last, double last_scale,
+                        cudaStream_t st);
+void launch_gxe_pair(const double* S, int64_t s_ld, int64_t N, int64_t N_pad, int64_t C,
+                     int64_t cols_per_group, const double* w, int64_t w_ld, int w_first,
+                     double* Ypair, cudaStream_t st);
+void launch_gxe_target_finalize(const double* S, int64_t L, int Kp, int K, int T, const double* sx,
+                                const double* sw, int64_t s_ld, const int32_t* ranks, int64_t N,
+                                int env_start, int64_t total, int64_t block_start, double* a0,
+                                double* a1, double* a2, double* a3, cudaStream_t st);
+void launch_scale(double* x, int64_t n, double s, cudaStream_t st);
+void launch_gxe_check(const double* probes, int64_t np, const double* sx, const double* sw,
+                      int64_t ns, const double* annot, int64_t na, unsigned* flag, cudaStream_t st);
+void launch_philox_rademacher(const uint64_t* keys, int64_t P, int64_t rows, double* out,
+                              cudaStream_t st);
+
 // Near-field control variate sums (lds_cv.cu): C[j K + k] += sum_v a_jkv^2 and,
 // if mu is set, mu[j K + k] = E[a_jk^2]; D in {4, 8, 15}.
 struct CvNearArgs {

@@ -98,6 +98,13 @@ class GwSession:
         check(_lib.load().lds_nn_band(self.handle, int(D), ptr(xx), ptr(cnt)))
         return (xx, cnt) if with_counts else xx
 
+    def block(self, start: int, stop: int):
+        """SNPs [start, stop) of this image as a genotype block argument of the
+        GxE kernel (summit_b200.gxeldcore)."""
+        from .gxeldcore import GenotypeBlock
+
+        return GenotypeBlock(self, start, stop)
+
     def window_ld(self, lo, hi, annot, corr_dim: float | None = None, row0: int = 0,
                   row1: int | None = None) -> np.ndarray:
         """Exact windowed LD scores of SNPs [row0, row1): row j sums f(r_ij) annot[i]
