@@ -569,16 +569,161 @@ def ours_arm(args) -> None:
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------------------
+# SUMMIT-GxE workload (config-3 shape): N = 100,000 x M = 1,000,000, 8 exposures
+# (6 continuous N(0,1) with pairwise correlation 0.2, 2 categorical with 3 and 5
+# levels, level-coded and standardized), K = 1 bin, B = 100 Gaussian probes.
+# One step = one whole reference build: source panel, projection, sealed pair,
+# target scores, normalization.
+# ---------------------------------------------------------------------------
+GXE_N, GXE_M, GXE_E, GXE_B = 100_000, 1_000_000, 8, 100
+GXE_METRIC = "geno x probe TOPS (SUMMIT-GxE multi-environment reference)"
+GXE_WORKLOAD = "gxe_reference_n100k_m1m_e8_k1_b100_gaussian"
+
+
+def gxe_ops(n: int, m: int, E: int, K: int, B: int) -> float:
+    """2 N M C (source) + 2 N M 2C (target pair), C = E 2 K B columns."""
+    C = E * 2 * K * B
+    return 2.0 * n * m * C + 2.0 * n * m * 2 * C
+
+
+def gxe_reference_sample(n: int, snps: int, threads: int, seed: int = DATA_SEED) -> tuple[float, str]:
+    """The reference's gxeldcore.cpp (compiled unchanged) on the first `snps`
+    SNPs: source_block + project_sources + target_score_block, dense FP64
+    genotypes from the reference's standardization; returns seconds."""
+    from oracle.gxe_oracle import design
+    from oracle.oracle import Oracle, ReferenceGxe
+
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    ora = Oracle()
+    rows = ora.synth_bed_rows(n, snps, seed)
+    X = ora.standardize(rows, n, 0, snps)[0]
+    d = design(n, GXE_E, seed=3, categorical=2)
+    ref = ReferenceGxe()
+    ker = ref.kernel(d["environments"], d["feature_basis"], d["power_indices"], d["power_offsets"],
+                     d["ranks"], d["gram_values"], d["gram_offsets"], d["e2_gram_values"],
+                     d["common_basis"], d["directions"], 1, 1, threads)
+    rng = np.random.default_rng(5)
+    z = np.asfortranarray(rng.normal(size=(snps, GXE_B)))
+    ones = np.ones((snps, GXE_E), order="F")
+    cols = GXE_E * 2 * GXE_B
+    t0 = time.perf_counter()
+    target = np.zeros((n, cols), order="F")
+    ker.source_block(target, X, z, np.ones((snps, 1)), ones, ones, 0)
+    ker.project_sources(target, GXE_B, 0)
+    pair = ker.pair(target, d["environments"])
+    accs = [np.zeros((GXE_E * snps, 1)) for _ in range(4)]
+    ker.target_score_block(X, pair, ones, ones, accs, 0, snps, GXE_B, 0)
+    ker.normalize_scores(accs, GXE_B)
+    sec = time.perf_counter() - t0
+    ref.lib.refg_pair_destroy(pair)
+    return sec, (f"first {snps} SNPs of the workload (N={n}, E={GXE_E}, B={GXE_B}); reference "
+                 f"gxeldcore.cpp MultiEnvironmentKernel compiled unchanged, FP64 OpenBLAS, "
+                 f"{threads} threads, {sec:.1f} s")
+
+
+def gxe_arm(args) -> None:
+    import torch
+
+    rank = env_int("RANK", 0)
+    world = env_int("WORLD_SIZE", 1)
+    local = env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    from summit_b200 import _lib, gwldcore
+    from summit_b200.gxe import GxeReference, synthetic_design
+    from summit_b200.session import GwSession
+
+    n, m = env_int("LDS_GXE_N", GXE_N), env_int("LDS_GXE_M", GXE_M)
+    E, B, K = GXE_E, GXE_B, 1
+    bed = gwldcore.synth_bed_rows(n, m, DATA_SEED + rank)
+    d = synthetic_design(n, E, seed=3, categorical=2)
+    dev = torch.device("cuda")
+    g = torch.Generator(device=dev)
+    g.manual_seed(1234 + rank)
+    probes = torch.randn((B, m), generator=g, dtype=torch.float64, device=dev).T
+    annot = torch.ones((K, m), dtype=torch.float64, device=dev).T
+    scale = torch.ones((E, m), dtype=torch.float64, device=dev).T
+    lib = _lib.load()
+    keys = ("environments", "feature_basis", "power_indices", "power_offsets", "ranks",
+            "gram_values", "gram_offsets", "e2_gram_values", "common_basis", "directions")
+
+    def build(sess):
+        gx = GxeReference(sess, *[d[k] for k in keys], annotation_bins=K)
+        return gx, gx.run(probes, annot, scale, scale)
+
+    t0 = time.perf_counter()
+    sess = GwSession(bed, n)
+    torch.cuda.synchronize()
+    upload_s = time.perf_counter() - t0
+    gx, res = build(sess)  # warm-up
+    launches0 = lib.lds_kernel_launches()
+    with Clocks(local) as clk:
+        times = []
+        for _ in range(args.steps):
+            res = gx.run(probes, annot, scale, scale)
+            times.append(res["timings"]["total"])
+    launches = int(lib.lds_kernel_launches() - launches0) // max(args.steps, 1)
+    ms = float(np.mean(times))
+    ops = gxe_ops(n, m, E, K, B)
+    # end to end: host BED rows -> resident image -> scores back on the host
+    t0 = time.perf_counter()
+    sess2 = GwSession(bed, n)
+    gx2, res2 = build(sess2)
+    host = {k: res2[k].cpu().numpy() for k in ("accum_xx", "accum_xw", "accum_wx", "accum_ww")}
+    e2e_s = time.perf_counter() - t0
+    sess2.close()
+    for k, v in host.items():
+        assert np.isfinite(v).all(), k
+    line = {
+        "metric": GXE_METRIC, "value": round(world * ops / (ms * 1e-3) / 1e12, 3), "unit": "TOPS",
+        "n_gpus": world, "steps": args.steps, "warmup": 1, "ms_per_step": round(ms, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int8-digit exact products, f64 projection and reductions",
+        "data": "synthetic (seeded HWE/AR(1) generator; Gaussian probes on device)",
+        "config": {"workload": GXE_WORKLOAD, "N": n, "M": m, "E": E, "K": K, "B": B,
+                   "columns": E * 2 * K * B, "scales": "ones (unscaled kernel mode)",
+                   "l2": "inputs larger than L2 (genotype image %.1f GB)" % (bed.nbytes / 1e9)},
+        "stage_ms": {k: round(v, 1) for k, v in res["timings"].items()},
+        "max_leakage": float(np.max(res["leakages"])),
+        "e2e": {"value": round(world * ops / e2e_s / 1e12, 3), "unit": "TOPS",
+                "h2d_bytes_per_step": int(bed.nbytes), "d2h_bytes_per_step": int(4 * E * m * K * 8),
+                "ms_per_step": round(e2e_s * 1e3, 1), "upload_ms": round(upload_s * 1e3, 1)},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not os.environ.get("LDS_SKIP_CPU_BASELINE"):
+        threads = cpu_threads()
+        snps = env_int("LDS_GXE_CPU_SNPS", 400)
+        sec, sample = gxe_reference_sample(n, snps, threads)
+        line["cpu_baseline"] = {"value": round(gxe_ops(n, snps, E, K, B) / sec / 1e12, 6),
+                                "unit": "TOPS", "cores": threads, "kind": "reference",
+                                "sample": sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["windowed", "gxe"], default="windowed")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.workload == "gxe":
+        if args.impl == "reference":
+            sec, sample = gxe_reference_sample(GXE_N, env_int("LDS_GXE_CPU_SNPS", 400),
+                                               cpu_threads())
+            v = gxe_ops(GXE_N, env_int("LDS_GXE_CPU_SNPS", 400), GXE_E, 1, GXE_B) / sec / 1e12
+            print(json.dumps({"impl": "reference", "metric": GXE_METRIC, "value": round(v, 6),
+                              "unit": "TOPS", "cpu_baseline": {"value": round(v, 6), "unit": "TOPS",
+                                                               "cores": cpu_threads(),
+                                                               "kind": "reference", "sample": sample}}))
+        else:
+            gxe_arm(args)
+    elif args.impl == "reference":
         reference_arm(args)
     else:
         ours_arm(args)

@@ -9,8 +9,8 @@ Follows MultiEnvironmentKernel in src/native/gxeldcore.cpp:
 * normalize_scores    :12490-12557
 and the probe streams of src/summit/ldscore/gwe_ldscore.py:524-530
 (_make_seed) and :2484-2505 (_generate_random_block, NumPy Philox).
-``design`` builds a self-consistent set of kernel inputs (environments, common
-basis, directions, fixed-effect feature bases) for tests and the benchmark.
+``design`` returns the package's synthetic kernel inputs
+(summit_b200.gxe.synthetic_design).
 """
 from __future__ import annotations
 
@@ -128,39 +128,7 @@ def normalize_scores(accs, probe_count):
 
 
 def design(n: int, E: int, seed: int = 0, n_cov: int = 1, categorical: int = 0):
-    """Self-consistent kernel inputs: environments (E - categorical continuous
-    N(0,1) with pairwise correlation 0.2, then ``categorical`` level-coded
-    exposures with 3, 5, ... levels, each standardized), a common basis of the
-    intercept and ``n_cov`` covariates, unit directions of the environments
-    orthogonal to it, and per environment the fixed-effect basis [U, d_e]
-    (feature power ranges all point at it; Grams are identities)."""
-    rng = np.random.default_rng(seed)
-    Ec = E - categorical
-    cov = np.full((Ec, Ec), 0.2) + 0.8 * np.eye(Ec)
-    envs = [rng.multivariate_normal(np.zeros(Ec), cov, size=n)] if Ec else []
-    for c in range(categorical):
-        levels = 3 + 2 * c
-        x = rng.integers(0, levels, size=n).astype(np.float64)
-        envs.append(((x - x.mean()) / x.std())[:, None])
-    env = np.asfortranarray(np.hstack(envs))
-    Xc = np.column_stack([np.ones(n)] + [rng.normal(size=n) for _ in range(n_cov)])
-    U = np.linalg.qr(Xc)[0]
-    D = env - U @ (U.T @ env)
-    D /= np.linalg.norm(D, axis=0)
-    r = U.shape[1]
-    feature_basis = np.asfortranarray(np.hstack([U, D]))
-    rank = r + 1
-    pidx, poff = [], [0]
-    for e in range(E):
-        cols = list(range(r)) + [r + e]
-        for _ in range(4):
-            pidx += cols
-            poff.append(len(pidx))
-    gram = np.concatenate([np.eye(rank).ravel() for _ in range(E)])
-    goff = np.arange(E + 1, dtype=np.int64) * rank * rank
-    fixed = [np.hstack([U, D[:, [e]]]) for e in range(E)]
-    return {"environments": env, "feature_basis": feature_basis,
-            "power_indices": np.asarray(pidx, np.int64), "power_offsets": np.asarray(poff, np.int64),
-            "ranks": np.full(E, rank, np.int32), "gram_values": gram, "gram_offsets": goff,
-            "e2_gram_values": gram.copy(), "common_basis": np.asfortranarray(U),
-            "directions": np.asfortranarray(D), "fixed_bases": fixed}
+    """Synthetic kernel inputs (summit_b200.gxe.synthetic_design)."""
+    from summit_b200.gxe import synthetic_design
+
+    return synthetic_design(n, E, seed, n_cov, categorical)
