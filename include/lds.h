@@ -299,6 +299,71 @@ int lds_geno_stats(int64_t geno, double* mean_out, double* sdinv_out);
 int lds_nn_band(int64_t geno, int D, double* xx_out, int32_t* counts_out);
 
 /* ---------------------------------------------------------------------
+ * Further gwldcore entry points (gwldcore.cpp:3656-3829), float and double:
+ *
+ * lds_phase1_compute_Xz_bed_chunk_rowmajor_*  (:3703-3718, impl :1925-2130):
+ *   as the column-major phase 1, but Xz2d_chunk is N x K*v_count row-major and
+ *   always accumulates (no bin_init_mask).
+ * lds_phase2_accum_XtXz_bed_mailman_* (:3785-3794, impl :2651-2917) and
+ *   lds_phase2_accum_XtXz_bed_mailman_rowmajor_* (:3796-3805, impl :2919-3119):
+ *   phase 2 on HWE-completed genotypes (the Mailman path's imputation); the
+ *   row-major form takes Xz2d row-major and the sketch's column sums sum_Xz
+ *   (n_sum = Q), which are recomputed exactly on the device.
+ * lds_compute_col_sums_rowmajor_* (:3720, impl :3121-3132): FP64 column sums
+ *   of a row-major N x Q sketch (same summation order as the reference).
+ * lds_project_rowmajor_inplace_and_col_sums_* (:3722-3725) and
+ *   lds_project_colmajor_inplace_* (:3726-3729): X <- (I - C R) X with C N x p
+ *   and R p x N column-major (no-op when either is NULL or p = 0); the
+ *   row-major form also returns the column sums.
+ * lds_standardize_dosage_inplace_* (:3664-3669, impl :1511-1580): per
+ *   column (x - mean) / sd over calls in [0, 2] (ddof), missing and invalid
+ *   calls set to 0; missing_out receives the count of missing calls;
+ *   out-of-range non-missing calls are an error (after the update, as in the
+ *   reference).
+ * ------------------------------------------------------------------- */
+#define LDS_P1R_ARGS(T)                                                                       \
+    const char *bed_prefix, const char *fam_path, int blk_start, int blk_end,                 \
+        const int64_t *row_sel, int64_t n_row_sel, int ddof, const T *annot_blk,              \
+        int64_t annot_rows, int64_t K, const T *inv_right, int v_start, int v_count,          \
+        int kmax_hint, int rand_dist, int has_seed, uint64_t seed, T *Xz2d_chunk,              \
+        int64_t xz_rows, int64_t xz_cols, int impute_mode, int has_impute_seed,               \
+        uint64_t impute_seed, T *inv_out, double resvar_eps
+int lds_phase1_compute_Xz_bed_chunk_rowmajor_f32(LDS_P1R_ARGS(float));
+int lds_phase1_compute_Xz_bed_chunk_rowmajor_f64(LDS_P1R_ARGS(double));
+#define LDS_P2M_ARGS(T)                                                                       \
+    const char *bed_prefix, const char *fam_path, int blk_start, int blk_end,                 \
+        const int64_t *row_sel, int64_t n_row_sel, int ddof, const T *inv_left, int64_t L,    \
+        int tile_nvecs, const T *Xz2d, int64_t xz_rows, int64_t xz_cols, T *meansq_accum,     \
+        int64_t M_rows, int64_t K, int N_denom, int has_impute_seed, uint64_t impute_seed,    \
+        double *mc_aggregate_sumsq, double *mc_per_snp_sumsq
+int lds_phase2_accum_XtXz_bed_mailman_f32(LDS_P2M_ARGS(float));
+int lds_phase2_accum_XtXz_bed_mailman_f64(LDS_P2M_ARGS(double));
+#define LDS_P2MR_ARGS(T)                                                                      \
+    const char *bed_prefix, const char *fam_path, int blk_start, int blk_end,                 \
+        const int64_t *row_sel, int64_t n_row_sel, int ddof, const T *inv_left, int64_t L,    \
+        int tile_nvecs, const T *Xz2d, int64_t xz_rows, int64_t xz_cols, T *meansq_accum,     \
+        int64_t M_rows, int64_t K, const double *sum_Xz, int64_t n_sum, int N_denom,          \
+        int has_impute_seed, uint64_t impute_seed, double *mc_aggregate_sumsq,                \
+        double *mc_per_snp_sumsq
+int lds_phase2_accum_XtXz_bed_mailman_rowmajor_f32(LDS_P2MR_ARGS(float));
+int lds_phase2_accum_XtXz_bed_mailman_rowmajor_f64(LDS_P2MR_ARGS(double));
+int lds_compute_col_sums_rowmajor_f32(const float* X, int64_t N, int64_t Q, double* out);
+int lds_compute_col_sums_rowmajor_f64(const double* X, int64_t N, int64_t Q, double* out);
+int lds_project_rowmajor_inplace_and_col_sums_f32(float* X, int64_t N, int64_t Q, const float* C,
+                                                  const float* R, int64_t p, double* sums);
+int lds_project_rowmajor_inplace_and_col_sums_f64(double* X, int64_t N, int64_t Q,
+                                                  const double* C, const double* R, int64_t p,
+                                                  double* sums);
+int lds_project_colmajor_inplace_f32(float* X, int64_t N, int64_t Q, const float* C,
+                                     const float* R, int64_t p);
+int lds_project_colmajor_inplace_f64(double* X, int64_t N, int64_t Q, const double* C,
+                                     const double* R, int64_t p);
+int lds_standardize_dosage_inplace_f32(float* G, int64_t N, int64_t L, int ddof,
+                                       double missing_value, int64_t* missing_out);
+int lds_standardize_dosage_inplace_f64(double* G, int64_t N, int64_t L, int ddof,
+                                       double missing_value, int64_t* missing_out);
+
+/* ---------------------------------------------------------------------
  * Exact windowed LD scores (tcgen05 int8 Gram products, FP64 epilogue).
  *
  * lds_compute_windowed_ld_chr replaces winldcore.compute_windowed_ld_chr

@@ -287,6 +287,9 @@ class Reference:
                 _str, _str, _int, _int, _p, _i64, _int, _p, _i64, _i64, _p, _int, _int, _int,
                 _str, _int, _u64, _p, _i64, _str, _int, _u64]
             getattr(L, f"ref_col_sums_rowmajor_{t}").argtypes = [_p, _i64, _i64, _p]
+            getattr(L, f"ref_project_rowmajor_{t}").argtypes = [_p, _i64, _i64, _p, _p, _i64, _p]
+            getattr(L, f"ref_project_colmajor_{t}").argtypes = [_p, _i64, _i64, _p, _p, _i64]
+            getattr(L, f"ref_standardize_dosage_{t}").argtypes = [_p, _i64, _i64, _int, _dbl, _p]
             getattr(L, f"ref_phase2_mailman_rowmajor_{t}").argtypes = [
                 _str, _str, _int, _int, _p, _i64, _int, _p, _i64, _int, _p, _i64, _i64, _p, _i64,
                 _p, _int, _int, _u64, _p, _p]
@@ -364,6 +367,65 @@ class Reference:
         self._chk(fn(_ptr(geno), geno.shape[0], geno.shape[1], blk_start, _ptr(inv_left),
                      tile_nvecs, _ptr(Xz), Xz.shape[1], _ptr(meansq), meansq.shape[0], N_denom,
                      _ptr(mc_agg), _ptr(mc_per_snp)))
+
+    def phase1_bed_rowmajor(self, prefix, blk_start, blk_end, annot_blk, inv_right, v_start,
+                            v_count, kmax_hint, rand_dist, seed, Xz, rows=None, ddof=1,
+                            impute_mode="hwe", impute_seed=None):
+        t = self._t(Xz.dtype)
+        annot_blk = np.ascontiguousarray(annot_blk, dtype=Xz.dtype)
+        inv_right = np.ascontiguousarray(inv_right, dtype=Xz.dtype)
+        rows_a = None if rows is None else np.ascontiguousarray(rows, dtype=np.int64)
+        fn = getattr(self.lib, f"ref_phase1_bed_rowmajor_{t}")
+        self._chk(fn(str(prefix).encode(), f"{prefix}.fam".encode(), blk_start, blk_end,
+                     _ptr(rows_a), 0 if rows_a is None else rows_a.size, ddof, _ptr(annot_blk),
+                     annot_blk.shape[0], annot_blk.shape[1], _ptr(inv_right), v_start, v_count,
+                     kmax_hint, rand_dist.encode(), int(seed is not None),
+                     0 if seed is None else seed, _ptr(Xz), Xz.shape[0], impute_mode.encode(),
+                     int(impute_seed is not None), 0 if impute_seed is None else impute_seed))
+
+    def col_sums_rowmajor(self, Xz):
+        out = np.empty(Xz.shape[1])
+        self._chk(getattr(self.lib, f"ref_col_sums_rowmajor_{self._t(Xz.dtype)}")(
+            _ptr(Xz), Xz.shape[0], Xz.shape[1], _ptr(out)))
+        return out
+
+    def phase2_mailman_rowmajor(self, prefix, blk_start, blk_end, inv_left, tile_nvecs, Xz,
+                                meansq, sum_Xz, N_denom, rows=None, ddof=1, impute_seed=None,
+                                mc_agg=None, mc_per_snp=None):
+        t = self._t(Xz.dtype)
+        inv_left = np.ascontiguousarray(inv_left, dtype=Xz.dtype)
+        rows_a = None if rows is None else np.ascontiguousarray(rows, dtype=np.int64)
+        sum_Xz = np.ascontiguousarray(sum_Xz, dtype=np.float64)
+        fn = getattr(self.lib, f"ref_phase2_mailman_rowmajor_{t}")
+        self._chk(fn(str(prefix).encode(), f"{prefix}.fam".encode(), blk_start, blk_end,
+                     _ptr(rows_a), 0 if rows_a is None else rows_a.size, ddof, _ptr(inv_left),
+                     inv_left.size, tile_nvecs, _ptr(Xz), Xz.shape[0], Xz.shape[1], _ptr(meansq),
+                     meansq.shape[0], _ptr(sum_Xz), N_denom, int(impute_seed is not None),
+                     0 if impute_seed is None else impute_seed, _ptr(mc_agg), _ptr(mc_per_snp)))
+
+    def project_rowmajor(self, Xz, C=None, R=None):
+        t = self._t(Xz.dtype)
+        Cf = None if C is None else np.asfortranarray(C, dtype=Xz.dtype)
+        Rf = None if R is None else np.asfortranarray(R, dtype=Xz.dtype)
+        sums = np.empty(Xz.shape[1])
+        self._chk(getattr(self.lib, f"ref_project_rowmajor_{t}")(
+            _ptr(Xz), Xz.shape[0], Xz.shape[1], _ptr(Cf), _ptr(Rf),
+            0 if Cf is None else Cf.shape[1], _ptr(sums)))
+        return sums
+
+    def project_colmajor(self, Xz, C=None, R=None):
+        t = self._t(Xz.dtype)
+        Cf = None if C is None else np.asfortranarray(C, dtype=Xz.dtype)
+        Rf = None if R is None else np.asfortranarray(R, dtype=Xz.dtype)
+        self._chk(getattr(self.lib, f"ref_project_colmajor_{t}")(
+            _ptr(Xz), Xz.shape[0], Xz.shape[1], _ptr(Cf), _ptr(Rf),
+            0 if Cf is None else Cf.shape[1]))
+
+    def standardize_dosage(self, G, ddof=1, missing_value=-9.0):
+        n = np.zeros(1, dtype=np.int64)
+        self._chk(getattr(self.lib, f"ref_standardize_dosage_{self._t(G.dtype)}")(
+            _ptr(G), G.shape[0], G.shape[1], int(ddof), float(missing_value), _ptr(n)))
+        return int(n[0])
 
     def resvar_bed(self, prefix, nsnps, step, dtype=np.float64, rows=None, ddof=1, eps=1e-10,
                    impute_mode="mean", impute_seed=None):

@@ -177,6 +177,36 @@ int phase2_mailman_rowmajor(const char* bed_prefix, const char* fam_path, int bl
     });
 }
 
+template <typename T>
+int project_rowmajor(T* Xz, int64_t N, int64_t Q, const T* C, const T* R, int64_t p,
+                     double* sums) {
+    return guarded([&] {
+        nb_mat2c_rw<T> xz(Xz, {(size_t)N, (size_t)Q});
+        nb::object Co = C ? nb::object(nb::ndarray<const T>(C, {(size_t)N, (size_t)p})) : nb::none();
+        nb::object Ro = R ? nb::object(nb::ndarray<const T>(R, {(size_t)p, (size_t)N})) : nb::none();
+        auto r = project_rowmajor_inplace_and_col_sums_impl<T>(xz, Co, Ro);
+        std::memcpy(sums, r.data(), sizeof(double) * (size_t)Q);
+    });
+}
+
+template <typename T>
+int project_colmajor(T* Xz, int64_t N, int64_t Q, const T* C, const T* R, int64_t p) {
+    return guarded([&] {
+        nb_mat2f_rw<T> xz(Xz, {(size_t)N, (size_t)Q});
+        nb::object Co = C ? nb::object(nb::ndarray<const T>(C, {(size_t)N, (size_t)p})) : nb::none();
+        nb::object Ro = R ? nb::object(nb::ndarray<const T>(R, {(size_t)p, (size_t)N})) : nb::none();
+        project_colmajor_inplace_impl<T>(xz, Co, Ro);
+    });
+}
+
+template <typename T>
+int standardize_dosage(T* G, int64_t N, int64_t L, int ddof, double missing, int64_t* nmiss) {
+    return guarded([&] {
+        nb_mat2f_rw<T> g(G, {(size_t)N, (size_t)L});
+        *nmiss = standardize_dosage_inplace_impl<T>(g, ddof, missing, 1);
+    });
+}
+
 }  // namespace
 
 #define REF_EXPORT extern "C" __attribute__((visibility("default")))
@@ -250,3 +280,15 @@ REF_BOTH(ref_col_sums_rowmajor, CS_SIG(float), CS_CALL(float), CS_SIG(double), C
 #define P2M_CALL(T) phase2_mailman_rowmajor<T>(bp, fam, bs, be, rows, nr, ddof, inv, L, tv, Xz, N, \
     Q, ms, M, sxz, nd, his, iseed, mca, mcp)
 REF_BOTH(ref_phase2_mailman_rowmajor, P2M_SIG(float), P2M_CALL(float), P2M_SIG(double), P2M_CALL(double))
+
+#define PRM_SIG(T) (T* X, int64_t N, int64_t Q, const T* C, const T* R, int64_t p, double* sums)
+#define PRM_CALL(T) project_rowmajor<T>(X, N, Q, C, R, p, sums)
+REF_BOTH(ref_project_rowmajor, PRM_SIG(float), PRM_CALL(float), PRM_SIG(double), PRM_CALL(double))
+
+#define PCM_SIG(T) (T* X, int64_t N, int64_t Q, const T* C, const T* R, int64_t p)
+#define PCM_CALL(T) project_colmajor<T>(X, N, Q, C, R, p)
+REF_BOTH(ref_project_colmajor, PCM_SIG(float), PCM_CALL(float), PCM_SIG(double), PCM_CALL(double))
+
+#define SDI_SIG(T) (T* G, int64_t N, int64_t L, int ddof, double missing, int64_t* nmiss)
+#define SDI_CALL(T) standardize_dosage<T>(G, N, L, ddof, missing, nmiss)
+REF_BOTH(ref_standardize_dosage, SDI_SIG(float), SDI_CALL(float), SDI_SIG(double), SDI_CALL(double))

@@ -1674,6 +1674,147 @@ void win_set_cv(Context& c, WinPlan& pl, const double* annot, int split, int D) 
     }
 }
 
+// Row-major phase 1 (phase1_compute_Xz_bed_chunk_rowmajor_impl,
+// gwldcore.cpp:1925-2130): Xz2d (N x K*v, row-major) += the block's
+// contribution; bins without members are left as they are.
+template <typename T>
+void phase1_bed_rowmajor_impl(const char* bed_prefix, const char* fam_path, int blk_start,
+                              int blk_end, const int64_t* row_sel, int64_t n_row_sel, int ddof,
+                              const T* annot, int64_t annot_rows, int64_t K, const T* inv_right,
+                              int v_start, int v_count, int rand_dist, int has_seed, uint64_t seed,
+                              T* Xz, int64_t xz_rows, int64_t xz_cols, int impute, int has_iseed,
+                              uint64_t iseed, T* inv_out, double resvar_eps) {
+    if (xz_cols != K * v_count) fail(LDS_ERR_ARG, "Xz2d_chunk shape must be (N, B*v_count)");
+    std::vector<T> tmp((size_t)(xz_rows * xz_cols), T(0));
+    phase1_bed_impl<T>(bed_prefix, fam_path, blk_start, blk_end, row_sel, n_row_sel, ddof, annot,
+                       annot_rows, K, inv_right, v_start, v_count, rand_dist, has_seed, seed,
+                       tmp.data(), xz_rows, xz_cols, nullptr, impute, has_iseed, iseed, inv_out,
+                       resvar_eps);
+    for (int64_t n = 0; n < xz_rows; ++n)
+        for (int64_t q = 0; q < xz_cols; ++q) Xz[n * xz_cols + q] += tmp[(size_t)(q * xz_rows + n)];
+}
+
+// C, R (N x p and p x N, column-major) projection of a device panel X (N x Q,
+// column-major FP64): X <- X - C (R X) (project_panel_inplace,
+// gwldcore.cpp:1119-1132).
+template <typename T>
+void project_device(Context& c, double* X, int64_t N, int64_t Q, const T* Cm, const T* Rm,
+                    int64_t p) {
+    if (p <= 0 || N <= 0 || Q <= 0) return;
+    std::vector<double> Cd((size_t)(N * p)), Rt((size_t)(N * p));
+    for (int64_t a = 0; a < p; ++a)
+        for (int64_t i = 0; i < N; ++i) {
+            Cd[(size_t)(a * N + i)] = (double)Cm[a * N + i];
+            Rt[(size_t)(a * N + i)] = (double)Rm[i * p + a];
+        }
+    DevBuf dC, dR, dcoef;
+    double* c_ = dC.as<double>(Cd.size());
+    double* r_ = dR.as<double>(Rt.size());
+    h2d(c_, Cd.data(), Cd.size(), c.st);
+    h2d(r_, Rt.data(), Rt.size(), c.st);
+    const int mb = col_dots_max_basis();
+    const int64_t nch = (p + mb - 1) / mb;
+    double* coef = dcoef.as<double>((size_t)(Q * mb * nch));
+    // all coefficients from the unprojected panel first, then the update
+    for (int64_t ch = 0; ch < nch; ++ch) {
+        const int nb = (int)std::min<int64_t>(mb, p - ch * mb);
+        launch_col_dots(X, N, N, Q, r_ + ch * mb * N, N, nb, 0, coef + ch * Q * mb, c.st);
+    }
+    for (int64_t ch = 0; ch < nch; ++ch) {
+        const int nb = (int)std::min<int64_t>(mb, p - ch * mb);
+        launch_sub_lowrank(X, N, N, Q, c_ + ch * mb * N, N, nb, coef + ch * Q * mb, 0, 1.0, c.st);
+    }
+    ck(cudaGetLastError(), "launch");
+    ck(cudaStreamSynchronize(c.st), "projection");
+}
+
+template <typename T>
+void col_sums_rowmajor_impl(const T* X, int64_t N, int64_t Q, double* out) {
+    Context& c = ctx();
+    std::lock_guard<std::mutex> lk(c.mu);
+    ensure_device(c);
+    if (N <= 0 || Q <= 0) {
+        for (int64_t q = 0; q < Q; ++q) out[q] = 0.0;
+        return;
+    }
+    DevBuf dx, ds;
+    T* x = dx.as<T>((size_t)(N * Q));
+    h2d(x, X, (size_t)(N * Q), c.st);
+    double* s = ds.as<double>((size_t)Q);
+    launch_col_sums_rowmajor<T>(x, N, Q, s, c.st);
+    ck(cudaGetLastError(), "launch");
+    d2h(out, s, (size_t)Q, c.st);
+    ck(cudaStreamSynchronize(c.st), "col sums");
+}
+
+template <typename T>
+void project_rowmajor_impl(T* X, int64_t N, int64_t Q, const T* Cm, const T* Rm, int64_t p,
+                           double* sums) {
+    Context& c = ctx();
+    std::lock_guard<std::mutex> lk(c.mu);
+    ensure_device(c);
+    if (N <= 0 || Q <= 0) {
+        for (int64_t q = 0; q < Q; ++q) sums[q] = 0.0;
+        return;
+    }
+    DevBuf dx, dcol, ds;
+    T* x = dx.as<T>((size_t)(N * Q));
+    h2d(x, X, (size_t)(N * Q), c.st);
+    if (p > 0 && Cm && Rm) {
+        double* col = dcol.as<double>((size_t)(N * Q));
+        launch_rowmajor_to_colmajor<T>(x, N, Q, col, c.st);
+        project_device<T>(c, col, N, Q, Cm, Rm, p);
+        launch_colmajor_to_rowmajor<T>(col, N, Q, x, c.st);
+        d2h(X, x, (size_t)(N * Q), c.st);
+    }
+    double* s = ds.as<double>((size_t)Q);
+    launch_col_sums_rowmajor<T>(x, N, Q, s, c.st);
+    ck(cudaGetLastError(), "launch");
+    d2h(sums, s, (size_t)Q, c.st);
+    ck(cudaStreamSynchronize(c.st), "projection");
+}
+
+template <typename T>
+void project_colmajor_impl(T* X, int64_t N, int64_t Q, const T* Cm, const T* Rm, int64_t p) {
+    if (N <= 0 || Q <= 0 || p <= 0 || !Cm || !Rm) return;
+    Context& c = ctx();
+    std::lock_guard<std::mutex> lk(c.mu);
+    ensure_device(c);
+    DevBuf dx, dcol;
+    T* x = dx.as<T>((size_t)(N * Q));
+    h2d(x, X, (size_t)(N * Q), c.st);
+    double* col = dcol.as<double>((size_t)(N * Q));
+    launch_convert<T>(x, N * Q, col, c.st);
+    project_device<T>(c, col, N, Q, Cm, Rm, p);
+    launch_convert_back<T>(col, N * Q, x, c.st);
+    ck(cudaGetLastError(), "launch");
+    d2h(X, x, (size_t)(N * Q), c.st);
+    ck(cudaStreamSynchronize(c.st), "projection");
+}
+
+template <typename T>
+int64_t standardize_dosage_impl(T* G, int64_t N, int64_t L, int ddof, double missing) {
+    if (N <= 0) fail(LDS_ERR_ARG, "Dosage matrix must have at least one sample");
+    if (L < 0) fail(LDS_ERR_ARG, "Invalid dosage matrix column count");
+    if (L == 0) return 0;
+    Context& c = ctx();
+    std::lock_guard<std::mutex> lk(c.mu);
+    ensure_device(c);
+    DevBuf dg, dc;
+    T* g = dg.as<T>((size_t)(N * L));
+    h2d(g, G, (size_t)(N * L), c.st);
+    unsigned long long* cnt = dc.as<unsigned long long>(2);
+    ck(cudaMemsetAsync(cnt, 0, 16, c.st), "memset");
+    launch_standardize_dosage<T>(g, N, L, ddof, missing, cnt, c.st);
+    ck(cudaGetLastError(), "launch");
+    unsigned long long hc[2] = {0, 0};
+    d2h(G, g, (size_t)(N * L), c.st);
+    d2h(hc, cnt, 2, c.st);
+    ck(cudaStreamSynchronize(c.st), "standardize");
+    if (hc[1]) fail(LDS_ERR_ARG, "Dosage matrix contains nonfinite or out-of-range nonmissing values");
+    return (int64_t)hc[0];
+}
+
 // ---------------------------------------------------------------------------
 // SUMMIT-GxE multi-environment products (MultiEnvironmentKernel,
 // gxeldcore.cpp:10281-12557) on a resident genotype image.  The image's
@@ -2120,6 +2261,107 @@ LDS_API int lds_phase1_compute_Xz_bed_chunk_f64(P1_ARGS(double)) { return P1_CAL
     })
 LDS_API int lds_phase2_accum_XtXz_bed_f32(P2_ARGS(float)) { return P2_CALL(float); }
 LDS_API int lds_phase2_accum_XtXz_bed_f64(P2_ARGS(double)) { return P2_CALL(double); }
+
+#define P1R_ARGS(T)                                                                             \
+    const char *bed_prefix, const char *fam_path, int blk_start, int blk_end,                   \
+        const int64_t *row_sel, int64_t n_row_sel, int ddof, const T *annot_blk,                \
+        int64_t annot_rows, int64_t K, const T *inv_right, int v_start, int v_count,            \
+        int kmax_hint, int rand_dist, int has_seed, uint64_t seed, T *Xz2d_chunk,                \
+        int64_t xz_rows, int64_t xz_cols, int impute_mode, int has_impute_seed,                 \
+        uint64_t impute_seed, T *inv_out, double resvar_eps
+#define P1R_CALL(T)                                                                             \
+    guarded([&] {                                                                               \
+        (void)kmax_hint;                                                                        \
+        phase1_bed_rowmajor_impl<T>(bed_prefix, fam_path, blk_start, blk_end, row_sel,          \
+                                    n_row_sel, ddof, annot_blk, annot_rows, K, inv_right,       \
+                                    v_start, v_count, rand_dist, has_seed, seed, Xz2d_chunk,    \
+                                    xz_rows, xz_cols, impute_mode, has_impute_seed, impute_seed, \
+                                    inv_out, resvar_eps);                                       \
+    })
+LDS_API int lds_phase1_compute_Xz_bed_chunk_rowmajor_f32(P1R_ARGS(float)) { return P1R_CALL(float); }
+LDS_API int lds_phase1_compute_Xz_bed_chunk_rowmajor_f64(P1R_ARGS(double)) { return P1R_CALL(double); }
+
+// Mailman phase 2 (gwldcore.cpp:2651-3119): HWE-completed genotypes, the same
+// centered products on the tensor cores.
+#define P2M_ARGS(T)                                                                             \
+    const char *bed_prefix, const char *fam_path, int blk_start, int blk_end,                   \
+        const int64_t *row_sel, int64_t n_row_sel, int ddof, const T *inv_left, int64_t L,      \
+        int tile_nvecs, const T *Xz2d, int64_t xz_rows, int64_t xz_cols, T *meansq_accum,       \
+        int64_t M_rows, int64_t K, int N_denom, int has_impute_seed, uint64_t impute_seed,      \
+        double *mc_aggregate_sumsq, double *mc_per_snp_sumsq
+#define P2M_CALL(T)                                                                             \
+    guarded([&] {                                                                               \
+        phase2_bed_impl<T>(bed_prefix, fam_path, blk_start, blk_end, row_sel, n_row_sel, ddof,  \
+                           inv_left, L, tile_nvecs, Xz2d, xz_rows, xz_cols, meansq_accum,       \
+                           M_rows, K, N_denom, LDS_IMPUTE_HWE, has_impute_seed, impute_seed,    \
+                           mc_aggregate_sumsq, mc_per_snp_sumsq);                               \
+    })
+LDS_API int lds_phase2_accum_XtXz_bed_mailman_f32(P2M_ARGS(float)) { return P2M_CALL(float); }
+LDS_API int lds_phase2_accum_XtXz_bed_mailman_f64(P2M_ARGS(double)) { return P2M_CALL(double); }
+
+// Row-major sketch with its column sums (gwldcore.cpp:2919-3119); the sums are
+// recomputed exactly on the device, sum_Xz is checked for shape only.
+#define P2MR_ARGS(T)                                                                            \
+    const char *bed_prefix, const char *fam_path, int blk_start, int blk_end,                   \
+        const int64_t *row_sel, int64_t n_row_sel, int ddof, const T *inv_left, int64_t L,      \
+        int tile_nvecs, const T *Xz2d, int64_t xz_rows, int64_t xz_cols, T *meansq_accum,       \
+        int64_t M_rows, int64_t K, const double *sum_Xz, int64_t n_sum, int N_denom,            \
+        int has_impute_seed, uint64_t impute_seed, double *mc_aggregate_sumsq,                  \
+        double *mc_per_snp_sumsq
+#define P2MR_CALL(T)                                                                            \
+    guarded([&] {                                                                               \
+        if (!sum_Xz || n_sum != xz_cols)                                                        \
+            fail(LDS_ERR_ARG, "sum_Xz length must equal the Xz2d column count");                \
+        std::vector<T> f((size_t)(xz_rows * xz_cols));                                          \
+        for (int64_t n = 0; n < xz_rows; ++n)                                                   \
+            for (int64_t q = 0; q < xz_cols; ++q)                                               \
+                f[(size_t)(q * xz_rows + n)] = Xz2d[n * xz_cols + q];                          \
+        phase2_bed_impl<T>(bed_prefix, fam_path, blk_start, blk_end, row_sel, n_row_sel, ddof,  \
+                           inv_left, L, tile_nvecs, f.data(), xz_rows, xz_cols, meansq_accum,   \
+                           M_rows, K, N_denom, LDS_IMPUTE_HWE, has_impute_seed, impute_seed,    \
+                           mc_aggregate_sumsq, mc_per_snp_sumsq);                               \
+    })
+LDS_API int lds_phase2_accum_XtXz_bed_mailman_rowmajor_f32(P2MR_ARGS(float)) { return P2MR_CALL(float); }
+LDS_API int lds_phase2_accum_XtXz_bed_mailman_rowmajor_f64(P2MR_ARGS(double)) { return P2MR_CALL(double); }
+
+LDS_API int lds_compute_col_sums_rowmajor_f32(const float* X, int64_t N, int64_t Q, double* out) {
+    return guarded([&] { col_sums_rowmajor_impl<float>(X, N, Q, out); });
+}
+LDS_API int lds_compute_col_sums_rowmajor_f64(const double* X, int64_t N, int64_t Q, double* out) {
+    return guarded([&] { col_sums_rowmajor_impl<double>(X, N, Q, out); });
+}
+LDS_API int lds_project_rowmajor_inplace_and_col_sums_f32(float* X, int64_t N, int64_t Q,
+                                                          const float* C, const float* R,
+                                                          int64_t p, double* sums) {
+    return guarded([&] { project_rowmajor_impl<float>(X, N, Q, C, R, p, sums); });
+}
+LDS_API int lds_project_rowmajor_inplace_and_col_sums_f64(double* X, int64_t N, int64_t Q,
+                                                          const double* C, const double* R,
+                                                          int64_t p, double* sums) {
+    return guarded([&] { project_rowmajor_impl<double>(X, N, Q, C, R, p, sums); });
+}
+LDS_API int lds_project_colmajor_inplace_f32(float* X, int64_t N, int64_t Q, const float* C,
+                                             const float* R, int64_t p) {
+    return guarded([&] { project_colmajor_impl<float>(X, N, Q, C, R, p); });
+}
+LDS_API int lds_project_colmajor_inplace_f64(double* X, int64_t N, int64_t Q, const double* C,
+                                             const double* R, int64_t p) {
+    return guarded([&] { project_colmajor_impl<double>(X, N, Q, C, R, p); });
+}
+LDS_API int lds_standardize_dosage_inplace_f32(float* G, int64_t N, int64_t L, int ddof,
+                                               double missing_value, int64_t* missing_out) {
+    return guarded([&] {
+        const int64_t mt = standardize_dosage_impl<float>(G, N, L, ddof, missing_value);
+        if (missing_out) *missing_out = mt;
+    });
+}
+LDS_API int lds_standardize_dosage_inplace_f64(double* G, int64_t N, int64_t L, int ddof,
+                                               double missing_value, int64_t* missing_out) {
+    return guarded([&] {
+        const int64_t mt = standardize_dosage_impl<double>(G, N, L, ddof, missing_value);
+        if (missing_out) *missing_out = mt;
+    });
+}
 
 #define RV_ARGS(T)                                                                              \
     const char *bed_prefix, const char *fam_path, int nsnps, int step_size,                     \

@@ -153,6 +153,20 @@ void launch_gxe_check(const double* probes, int64_t np, const double* sx, const 
 void launch_philox_rademacher(const uint64_t* keys, int64_t P, int64_t rows, double* out,
                               cudaStream_t st);
 
+// Sketch-panel utilities (lds_proj.cu), T = float or double.
+template <typename T> void launch_col_sums_rowmajor(const T* X, int64_t N, int64_t Q, double* out,
+                                                    cudaStream_t st);
+template <typename T> void launch_rowmajor_to_colmajor(const T* in, int64_t N, int64_t Q,
+                                                       double* out, cudaStream_t st);
+template <typename T> void launch_colmajor_to_rowmajor(const double* in, int64_t N, int64_t Q,
+                                                       T* out, cudaStream_t st);
+template <typename T> void launch_convert(const T* in, int64_t n, double* out, cudaStream_t st);
+template <typename T> void launch_convert_back(const double* in, int64_t n, T* out,
+                                               cudaStream_t st);
+template <typename T> void launch_standardize_dosage(T* G, int64_t N, int64_t L, int ddof,
+                                                     double missing, unsigned long long* counts,
+                                                     cudaStream_t st);
+
 // Near-field control variate sums (lds_cv.cu): C[j K + k] += sum_v a_jkv^2 and,
 // if mu is set, mu[j K + k] = E[a_jk^2]; D in {4, 8, 15}.
 struct CvNearArgs {

@@ -194,6 +194,151 @@ def phase2_accum_XtXz_bed(bed_prefix, fam_path, blk_start, blk_end, row_sel=None
 
 
 # ---------------------------------------------------------------------------
+# Row-major phase 1, Mailman phase 2, sketch sums and projections
+# (gwldcore.cpp:3703-3729, :3785-3805)
+# ---------------------------------------------------------------------------
+def phase1_compute_Xz_bed_chunk_rowmajor(bed_prefix, fam_path, blk_start, blk_end, row_sel=None,
+                                         ddof=1, annot_blk=_REQUIRED, inv_right=_REQUIRED,
+                                         v_start=_REQUIRED, v_count=_REQUIRED,
+                                         kmax_hint=_REQUIRED, rand_dist="rademacher", seed=None,
+                                         Xz2d_chunk=_REQUIRED, project_right=False, C=None, R=None,
+                                         impute_mode="hwe", impute_seed=None, resvar_gram=None,
+                                         inv_out=None, resvar_eps=1e-10):
+    Xz = _need("Xz2d_chunk", Xz2d_chunk)
+    t = _tsuffix(Xz)
+    dt = Xz.dtype
+    _rw(Xz, dt, "C", "Xz2d_chunk")
+    if Xz.ndim != 2:
+        raise RuntimeError("Xz2d_chunk shape must be (N, B*v_count)")
+    if (C is not None or R is not None) and (project_right or inv_out is not None):
+        raise RuntimeError("covariate projection inside phase 1 is not supported by the B200 "
+                           "backend; project Xz2d after phase 1 (project_rowmajor_inplace_and_col_sums)")
+    ann = np.ascontiguousarray(_need("annot_blk", annot_blk), dtype=dt)
+    inv_r = None
+    if inv_out is not None:
+        _rw(inv_out, dt, "C", "inv_out")
+    else:
+        inv_r = np.ascontiguousarray(_need("inv_right", inv_right), dtype=dt)
+        if inv_r.shape[0] != ann.shape[0]:
+            raise RuntimeError("inv_right shape mismatch in phase1")
+    rows, nr = _rows(row_sel)
+    fn = getattr(_lib.load(), f"lds_phase1_compute_Xz_bed_chunk_rowmajor_{t}")
+    check(fn(enc(bed_prefix), enc(fam_path), int(blk_start), int(blk_end), ptr(rows), nr,
+             int(ddof), ptr(ann), ann.shape[0], ann.shape[1], ptr(inv_r),
+             int(_need("v_start", v_start)), int(_need("v_count", v_count)),
+             int(_need("kmax_hint", kmax_hint)), _dist(rand_dist), int(seed is not None),
+             0 if seed is None else int(seed) & (2**64 - 1), ptr(Xz), Xz.shape[0], Xz.shape[1],
+             _impute(impute_mode), int(impute_seed is not None),
+             0 if impute_seed is None else int(impute_seed), ptr(inv_out), float(resvar_eps)))
+
+
+def _mailman_common(meansq_accum, Xz2d, order, inv_left, mc_aggregate_sumsq, mc_per_snp_sumsq,
+                    name):
+    ms = _need("meansq_accum", meansq_accum)
+    t = _tsuffix(ms)
+    dt = ms.dtype
+    _rw(ms, dt, "C", "meansq_accum")
+    Xz = _need("Xz2d", Xz2d)
+    Xz = np.asfortranarray(Xz, dtype=dt) if order == "F" else np.ascontiguousarray(Xz, dtype=dt)
+    inv = np.ascontiguousarray(_need("inv_left", inv_left), dtype=dt)
+    if mc_aggregate_sumsq is not None:
+        _rw(mc_aggregate_sumsq, np.float64, "C", "mc_aggregate_sumsq")
+    if mc_per_snp_sumsq is not None:
+        _rw(mc_per_snp_sumsq, np.float64, "C", "mc_per_snp_sumsq")
+        if mc_per_snp_sumsq.shape != ms.shape:
+            raise RuntimeError(f"mc_per_snp_sumsq shape must match meansq_accum in {name}")
+    return t, ms, Xz, inv
+
+
+def phase2_accum_XtXz_bed_mailman(bed_prefix, fam_path, blk_start, blk_end, row_sel=None, ddof=1,
+                                  inv_left=_REQUIRED, tile_nvecs=_REQUIRED, Xz2d=_REQUIRED,
+                                  meansq_accum=_REQUIRED, C=None, R=None, N_denom=0,
+                                  impute_seed=None, mc_aggregate_sumsq=None,
+                                  mc_per_snp_sumsq=None):
+    if C is not None and R is not None:
+        raise RuntimeError("covariate projection inside phase 2 is not supported by the B200 "
+                           "backend; pass the projected sketch with C=R=None")
+    t, ms, Xz, inv = _mailman_common(meansq_accum, Xz2d, "F", inv_left, mc_aggregate_sumsq,
+                                     mc_per_snp_sumsq, "phase2_accum_XtXz_bed_mailman")
+    rows, nr = _rows(row_sel)
+    fn = getattr(_lib.load(), f"lds_phase2_accum_XtXz_bed_mailman_{t}")
+    check(fn(enc(bed_prefix), enc(fam_path), int(blk_start), int(blk_end), ptr(rows), nr,
+             int(ddof), ptr(inv), inv.shape[0], int(_need("tile_nvecs", tile_nvecs)), ptr(Xz),
+             Xz.shape[0], Xz.shape[1], ptr(ms), ms.shape[0], ms.shape[1], int(N_denom),
+             int(impute_seed is not None), 0 if impute_seed is None else int(impute_seed),
+             ptr(mc_aggregate_sumsq), ptr(mc_per_snp_sumsq)))
+
+
+def phase2_accum_XtXz_bed_mailman_rowmajor(bed_prefix, fam_path, blk_start, blk_end,
+                                           row_sel=None, ddof=1, inv_left=_REQUIRED,
+                                           tile_nvecs=_REQUIRED, Xz2d=_REQUIRED,
+                                           meansq_accum=_REQUIRED, sum_Xz=_REQUIRED, N_denom=0,
+                                           impute_seed=None, mc_aggregate_sumsq=None,
+                                           mc_per_snp_sumsq=None):
+    t, ms, Xz, inv = _mailman_common(meansq_accum, Xz2d, "C", inv_left, mc_aggregate_sumsq,
+                                     mc_per_snp_sumsq, "phase2_accum_XtXz_bed_mailman_rowmajor")
+    sx = np.ascontiguousarray(_need("sum_Xz", sum_Xz), dtype=np.float64)
+    rows, nr = _rows(row_sel)
+    fn = getattr(_lib.load(), f"lds_phase2_accum_XtXz_bed_mailman_rowmajor_{t}")
+    check(fn(enc(bed_prefix), enc(fam_path), int(blk_start), int(blk_end), ptr(rows), nr,
+             int(ddof), ptr(inv), inv.shape[0], int(_need("tile_nvecs", tile_nvecs)), ptr(Xz),
+             Xz.shape[0], Xz.shape[1], ptr(ms), ms.shape[0], ms.shape[1], ptr(sx), sx.size,
+             int(N_denom), int(impute_seed is not None),
+             0 if impute_seed is None else int(impute_seed), ptr(mc_aggregate_sumsq),
+             ptr(mc_per_snp_sumsq)))
+
+
+def compute_col_sums_rowmajor(Xz2d) -> np.ndarray:
+    X = np.asarray(Xz2d)
+    t = _tsuffix(X)
+    X = np.ascontiguousarray(X)
+    out = np.empty(X.shape[1])
+    check(getattr(_lib.load(), f"lds_compute_col_sums_rowmajor_{t}")(ptr(X), X.shape[0],
+                                                                       X.shape[1], ptr(out)))
+    return out
+
+
+def _cr(C, R, dt, N, name):
+    if C is None or R is None:
+        return None, None, 0
+    Cf = np.asfortranarray(C, dtype=dt)
+    Rf = np.asfortranarray(R, dtype=dt)
+    p = Cf.shape[1]
+    if Cf.shape[0] != N or Rf.shape != (p, N):
+        raise RuntimeError(f"C/R shape mismatch in {name}")
+    return Cf, Rf, p
+
+
+def project_rowmajor_inplace_and_col_sums(Xz2d, C=None, R=None) -> np.ndarray:
+    t = _tsuffix(Xz2d)
+    X = _rw(Xz2d, Xz2d.dtype, "C", "Xz2d")
+    Cf, Rf, p = _cr(C, R, X.dtype, X.shape[0], "project_rowmajor_inplace_and_col_sums")
+    sums = np.empty(X.shape[1])
+    check(getattr(_lib.load(), f"lds_project_rowmajor_inplace_and_col_sums_{t}")(
+        ptr(X), X.shape[0], X.shape[1], ptr(Cf), ptr(Rf), p, ptr(sums)))
+    return sums
+
+
+def project_colmajor_inplace(Xz2d, C=None, R=None) -> None:
+    t = _tsuffix(Xz2d)
+    X = _rw(Xz2d, Xz2d.dtype, "F", "Xz2d")
+    Cf, Rf, p = _cr(C, R, X.dtype, X.shape[0], "project_colmajor_inplace")
+    if p == 0:
+        return
+    check(getattr(_lib.load(), f"lds_project_colmajor_inplace_{t}")(
+        ptr(X), X.shape[0], X.shape[1], ptr(Cf), ptr(Rf), p))
+
+
+def standardize_dosage_inplace(Geno, ddof=1, missing_value=-9.0, num_threads=0) -> int:
+    t = _tsuffix(Geno)
+    G = _rw(Geno, Geno.dtype, "F", "Geno")
+    n = np.zeros(1, dtype=np.int64)
+    check(getattr(_lib.load(), f"lds_standardize_dosage_inplace_{t}")(
+        ptr(G), G.shape[0], G.shape[1], int(ddof), float(missing_value), ptr(n)))
+    return int(n[0])
+
+
+# ---------------------------------------------------------------------------
 # Residual variances (gwldcore.cpp:3748-3757)
 # ---------------------------------------------------------------------------
 def precompute_residual_variances_bed(bed_prefix, fam_path, nsnps, step_size, row_sel=None,
