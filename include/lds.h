@@ -77,8 +77,12 @@ void lds_clear_device_cache(void);
  * for a bin's first write and is set to 1 for bins written.  When inv_out is
  * given, residual variances of the block are computed into it and used in
  * place of inv_right (fused residual variance, :1659-1669).
- * project_right / covariates are not supported by this entry (the caller
- * projects Xz2d afterwards, as gw_ldscore.py does).
+ * Covariates enter only the fused residual variances, as in the reference's
+ * driver (gw_ldscore.py:1929-1956): with C (N x p) and R (p x N, both
+ * column-major) and optional resvar_gram (p x p row-major), inv_out[j] =
+ * 1/sqrt(max(eps, (||x_j||^2 + q - 2h)/(N - p - 1))) with h = ||R x_j||^2 and
+ * q = (R x_j)^T gram (R x_j) (or h) (compute_inv_resvar_from_geno_block,
+ * :3220-3333).  The caller projects Xz2d afterwards (project_*).
  * ------------------------------------------------------------------- */
 int lds_phase1_compute_Xz_bed_chunk_f32(
     const char* bed_prefix, const char* fam_path, int blk_start, int blk_end,
@@ -86,14 +90,16 @@ int lds_phase1_compute_Xz_bed_chunk_f32(
     int64_t annot_rows, int64_t K, const float* inv_right, int v_start, int v_count,
     int kmax_hint, int rand_dist, int has_seed, uint64_t seed, float* Xz2d_chunk,
     int64_t xz_rows, int64_t xz_cols, uint8_t* bin_init_mask, int impute_mode,
-    int has_impute_seed, uint64_t impute_seed, float* inv_out, double resvar_eps);
+    int has_impute_seed, uint64_t impute_seed, float* inv_out, double resvar_eps,
+    const float* C, const float* R, int64_t p, const float* resvar_gram);
 int lds_phase1_compute_Xz_bed_chunk_f64(
     const char* bed_prefix, const char* fam_path, int blk_start, int blk_end,
     const int64_t* row_sel, int64_t n_row_sel, int ddof, const double* annot_blk,
     int64_t annot_rows, int64_t K, const double* inv_right, int v_start, int v_count,
     int kmax_hint, int rand_dist, int has_seed, uint64_t seed, double* Xz2d_chunk,
     int64_t xz_rows, int64_t xz_cols, uint8_t* bin_init_mask, int impute_mode,
-    int has_impute_seed, uint64_t impute_seed, double* inv_out, double resvar_eps);
+    int has_impute_seed, uint64_t impute_seed, double* inv_out, double resvar_eps,
+    const double* C, const double* R, int64_t p, const double* resvar_gram);
 
 /* ---------------------------------------------------------------------
  * Phase 2: Work = X_blk^T Xz2d; meansq_accum[blk_start+j, k] +=
@@ -121,18 +127,22 @@ int lds_phase2_accum_XtXz_bed_f64(
 
 /* ---------------------------------------------------------------------
  * Residual variances: inv[j] = 1/sqrt(max(eps, ||x_j||^2 / (N-1))) for all
- * nsnps SNPs, without covariates.  Replaces
+ * nsnps SNPs, or with covariates (C N x p, R p x N column-major)
+ * inv[j] = 1/sqrt(max(eps, ||(I - C R) x_j||^2 / (N - p - 1))); snp_var_out
+ * (may be NULL) receives min(1, ||(I - C R) x_j||^2 / ||x_j||^2).  Replaces
  * gwldcore.precompute_residual_variances_bed (gwldcore.cpp:3748-3757,
- * implementation :3335-3566) for C = R = None and compute_mu22 = False.
+ * implementation :3335-3566) for compute_mu22 = False.
  * ------------------------------------------------------------------- */
 int lds_precompute_residual_variances_bed_f32(
     const char* bed_prefix, const char* fam_path, int nsnps, int step_size,
     const int64_t* row_sel, int64_t n_row_sel, int ddof, double eps, int impute_mode,
-    int has_impute_seed, uint64_t impute_seed, float* inv_out);
+    int has_impute_seed, uint64_t impute_seed, float* inv_out, const float* C, const float* R,
+    int64_t p, double* snp_var_out);
 int lds_precompute_residual_variances_bed_f64(
     const char* bed_prefix, const char* fam_path, int nsnps, int step_size,
     const int64_t* row_sel, int64_t n_row_sel, int ddof, double eps, int impute_mode,
-    int has_impute_seed, uint64_t impute_seed, double* inv_out);
+    int has_impute_seed, uint64_t impute_seed, double* inv_out, const double* C,
+    const double* R, int64_t p, double* snp_var_out);
 
 /* ---------------------------------------------------------------------
  * Whole genome-wide LD-score estimate in one call (all V-tiles, all SNP
@@ -327,7 +337,8 @@ int lds_nn_band(int64_t geno, int D, double* xx_out, int32_t* counts_out);
         int64_t annot_rows, int64_t K, const T *inv_right, int v_start, int v_count,          \
         int kmax_hint, int rand_dist, int has_seed, uint64_t seed, T *Xz2d_chunk,              \
         int64_t xz_rows, int64_t xz_cols, int impute_mode, int has_impute_seed,               \
-        uint64_t impute_seed, T *inv_out, double resvar_eps
+        uint64_t impute_seed, T *inv_out, double resvar_eps, const T *C, const T *R,          \
+        int64_t p, const T *resvar_gram
 int lds_phase1_compute_Xz_bed_chunk_rowmajor_f32(LDS_P1R_ARGS(float));
 int lds_phase1_compute_Xz_bed_chunk_rowmajor_f64(LDS_P1R_ARGS(double));
 #define LDS_P2M_ARGS(T)                                                                       \

@@ -288,6 +288,12 @@ class Reference:
                 _str, _int, _u64, _p, _i64, _str, _int, _u64]
             getattr(L, f"ref_col_sums_rowmajor_{t}").argtypes = [_p, _i64, _i64, _p]
             getattr(L, f"ref_project_rowmajor_{t}").argtypes = [_p, _i64, _i64, _p, _p, _i64, _p]
+            getattr(L, f"ref_resvar_bed_cov_{t}").argtypes = [
+                _str, _str, _int, _int, _p, _i64, _int, _dbl, _str, _int, _u64, _p, _p, _i64, _i64,
+                _p, _p]
+            getattr(L, f"ref_phase1_bed_cov_{t}").argtypes = [
+                _str, _str, _int, _int, _p, _i64, _int, _p, _i64, _i64, _int, _int, _str, _u64, _p,
+                _i64, _str, _p, _p, _i64, _p, _p]
             getattr(L, f"ref_project_colmajor_{t}").argtypes = [_p, _i64, _i64, _p, _p, _i64]
             getattr(L, f"ref_standardize_dosage_{t}").argtypes = [_p, _i64, _i64, _int, _dbl, _p]
             getattr(L, f"ref_phase2_mailman_rowmajor_{t}").argtypes = [
@@ -402,6 +408,34 @@ class Reference:
                      inv_left.size, tile_nvecs, _ptr(Xz), Xz.shape[0], Xz.shape[1], _ptr(meansq),
                      meansq.shape[0], _ptr(sum_Xz), N_denom, int(impute_seed is not None),
                      0 if impute_seed is None else impute_seed, _ptr(mc_agg), _ptr(mc_per_snp)))
+
+    def resvar_bed_cov(self, prefix, nsnps, step, C, R, dtype=np.float64, ddof=1, eps=1e-10,
+                       impute_mode="mean", snp_var=None):
+        t = self._t(dtype)
+        Cf = np.asfortranarray(C, dtype=dtype)
+        Rf = np.asfortranarray(R, dtype=dtype)
+        out = np.empty(nsnps, dtype=dtype)
+        self._chk(getattr(self.lib, f"ref_resvar_bed_cov_{t}")(
+            str(prefix).encode(), f"{prefix}.fam".encode(), nsnps, step, None, 0, ddof, eps,
+            impute_mode.encode(), 0, 0, _ptr(Cf), _ptr(Rf), Cf.shape[0], Cf.shape[1],
+            _ptr(snp_var), _ptr(out)))
+        return out
+
+    def phase1_bed_cov(self, prefix, blk_start, blk_end, annot_blk, v_start, v_count, seed, Xz,
+                       C, R, gram=None, ddof=1, impute_mode="mean"):
+        t = self._t(Xz.dtype)
+        dt = Xz.dtype
+        ann = np.ascontiguousarray(annot_blk, dtype=dt)
+        Cf = np.asfortranarray(C, dtype=dt)
+        Rf = np.asfortranarray(R, dtype=dt)
+        G = None if gram is None else np.ascontiguousarray(gram, dtype=dt)
+        inv = np.empty(ann.shape[0], dtype=dt)
+        self._chk(getattr(self.lib, f"ref_phase1_bed_cov_{t}")(
+            str(prefix).encode(), f"{prefix}.fam".encode(), blk_start, blk_end, None, 0, ddof,
+            _ptr(ann), ann.shape[0], ann.shape[1], v_start, v_count, b"rademacher", seed,
+            _ptr(Xz), Xz.shape[0], impute_mode.encode(), _ptr(Cf), _ptr(Rf), Cf.shape[1],
+            _ptr(G), _ptr(inv)))
+        return inv
 
     def project_rowmajor(self, Xz, C=None, R=None):
         t = self._t(Xz.dtype)

@@ -207,6 +207,48 @@ int standardize_dosage(T* G, int64_t N, int64_t L, int ddof, double missing, int
     });
 }
 
+template <typename T>
+nb::object matf(const T* p, int64_t r, int64_t c) {
+    if (!p) return nb::none();
+    return nb::object(nb::ndarray<const T>(p, {(size_t)r, (size_t)c}));
+}
+
+// precompute_residual_variances_bed with covariates and snp_var_out.
+template <typename T>
+int resvar_bed_cov(const char* bed_prefix, const char* fam_path, int nsnps, int step_size,
+                   const int64_t* rows, int64_t n_rows, int ddof, double eps,
+                   const char* impute_mode, int has_impute_seed, uint64_t impute_seed,
+                   const T* C, const T* R, int64_t N, int64_t p, double* snp_var, T* inv_out) {
+    return guarded([&] {
+        nb::object sv = snp_var ? nb::object(nb::ndarray<double>(snp_var, {(size_t)nsnps})) : nb::none();
+        nb::tuple t = precompute_residual_variances_bed_impl<T>(
+            bed_prefix, fam_path, nsnps, step_size, rows_obj(rows, n_rows), ddof, eps, false,
+            nb::none(), matf(C, N, p), matf(R, p, N), impute_mode,
+            opt_u64(has_impute_seed, impute_seed), sv);
+        const nb::object o = t[0];
+        std::memcpy(inv_out, o.a_.data, sizeof(T) * (size_t)nsnps);
+    });
+}
+
+// phase1_compute_Xz_bed_chunk with the fused residual variances under covariates.
+template <typename T>
+int phase1_bed_cov(const char* bed_prefix, const char* fam_path, int blk_start, int blk_end,
+                   const int64_t* rows, int64_t n_rows, int ddof, const T* annot, int64_t L,
+                   int64_t K, int v_start, int v_count, const char* rand_dist, uint64_t seed,
+                   T* Xz, int64_t N, const char* impute_mode, const T* C, const T* R, int64_t p,
+                   const T* gram, T* inv_out) {
+    return guarded([&] {
+        nb_mat2c_ro<T> ann(const_cast<T*>(annot), {(size_t)L, (size_t)K});
+        nb_mat2f_rw<T> xz(Xz, {(size_t)N, (size_t)(K * v_count)});
+        nb::object g = gram ? nb::object(nb::ndarray<const T>(gram, {(size_t)p, (size_t)p})) : nb::none();
+        phase1_compute_Xz_bed_chunk_impl<T>(
+            bed_prefix, fam_path, blk_start, blk_end, rows_obj(rows, n_rows), ddof, ann,
+            nb::none(), v_start, v_count, 1, rand_dist, nb::object::from_uint(seed), xz,
+            nb::none(), false, matf(C, N, p), matf(R, p, N), impute_mode, nb::none(), g,
+            arr(inv_out, {(size_t)L}), 1e-10);
+    });
+}
+
 }  // namespace
 
 #define REF_EXPORT extern "C" __attribute__((visibility("default")))
@@ -292,3 +334,18 @@ REF_BOTH(ref_project_colmajor, PCM_SIG(float), PCM_CALL(float), PCM_SIG(double),
 #define SDI_SIG(T) (T* G, int64_t N, int64_t L, int ddof, double missing, int64_t* nmiss)
 #define SDI_CALL(T) standardize_dosage<T>(G, N, L, ddof, missing, nmiss)
 REF_BOTH(ref_standardize_dosage, SDI_SIG(float), SDI_CALL(float), SDI_SIG(double), SDI_CALL(double))
+
+#define RVC_SIG(T) (const char* bp, const char* fam, int nsnps, int step, const int64_t* rows, \
+    int64_t nr, int ddof, double eps, const char* im, int his, uint64_t iseed, const T* C, \
+    const T* R, int64_t N, int64_t p, double* sv, T* inv_out)
+#define RVC_CALL(T) resvar_bed_cov<T>(bp, fam, nsnps, step, rows, nr, ddof, eps, im, his, iseed, \
+    C, R, N, p, sv, inv_out)
+REF_BOTH(ref_resvar_bed_cov, RVC_SIG(float), RVC_CALL(float), RVC_SIG(double), RVC_CALL(double))
+
+#define P1C_SIG(T) (const char* bp, const char* fam, int bs, int be, const int64_t* rows, \
+    int64_t nr, int ddof, const T* annot, int64_t L, int64_t K, int vs, int vc, const char* rd, \
+    uint64_t seed, T* Xz, int64_t N, const char* im, const T* C, const T* R, int64_t p, \
+    const T* gram, T* inv_out)
+#define P1C_CALL(T) phase1_bed_cov<T>(bp, fam, bs, be, rows, nr, ddof, annot, L, K, vs, vc, rd, \
+    seed, Xz, N, im, C, R, p, gram, inv_out)
+REF_BOTH(ref_phase1_bed_cov, P1C_SIG(float), P1C_CALL(float), P1C_SIG(double), P1C_CALL(double))

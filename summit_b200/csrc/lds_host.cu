@@ -691,6 +691,158 @@ Prepared& prepared_for_file(Context& c, const std::string& bed_prefix, const std
     return *c.cache.front();
 }
 
+// Exact-digit products x_j . y_v of the standardized genotypes of SNPs [j0, j1)
+// with the columns of a dense N x V matrix Y (column-major, FP64): the phase-2
+// tensor-core kernel in its raw-product mode (G^T y and O^T y per digit set,
+// recombined exactly), then x_j . y = s_j colscale_v (G^T y - mu_j O^T y).
+// Returns (j1 - j0) x V row-major.
+std::vector<double> snp_products(Context& c, const Prepared& P, int64_t j0, int64_t j1,
+                                 const std::vector<double>& Y, int64_t V) {
+    const int64_t L = j1 - j0, N = P.g.N, Np = P.g.N_pad;
+    std::vector<double> out((size_t)(L * V), 0.0);
+    if (L <= 0 || V <= 0) return out;
+    if (c.slices != 4 || p2_impl() != 1)
+        fail(LDS_ERR_ARG, "covariate products need the tcgen05 kernels with 4 digits");
+    std::vector<double> y((size_t)(Np * V), 0.0);
+    for (int64_t v = 0; v < V; ++v)
+        std::memcpy(&y[(size_t)(v * Np)], &Y[(size_t)(v * N)], sizeof(double) * (size_t)N);
+    DevBuf dy, dyq, dcs, rg, ro, st;
+    double* d_y = dy.as<double>(y.size());
+    h2d(d_y, y.data(), y.size(), c.st);
+    const int nc = umma::ncolp_for((int)V);
+    int8_t* yq = dyq.as<int8_t>((size_t)(nc * Np));
+    double* cs = dcs.as<double>((size_t)V);
+    umma::launch_quantize_y4(d_y, N, Np, 1, (int)V, nc, yq, cs, c.st);
+    long long* dg = rg.as<long long>((size_t)(L * V));
+    long long* dO = ro.as<long long>((size_t)(L * V));
+    unsigned* dst = st.as<unsigned>(1);
+    ck(cudaMemsetAsync(dst, 0, 4, c.st), "memset");
+    const CUtensorMap tA = make_map_2d(P.g.codes, (uint64_t)P.g.nbp, (uint64_t)P.g.M_pad,
+                                       (uint64_t)P.g.nbp, 32, 128, CU_TENSOR_MAP_SWIZZLE_NONE);
+    const CUtensorMap tB = make_map_2d(yq, (uint64_t)Np, (uint64_t)nc, (uint64_t)Np, 128,
+                                       (uint32_t)std::min(256, nc), CU_TENSOR_MAP_SWIZZLE_128B);
+    umma::P2UArgs u;
+    u.K = 1;
+    u.V = (int)V;
+    u.ncolp = nc;
+    u.ngroups = (nc + 255) / 256;
+    u.box_rows = std::min(256, nc);
+    u.nkt = (int)(Np / 128);
+    u.M = P.g.M;
+    u.j0 = j0;
+    u.j1 = j1;
+    u.out_row0 = j0;
+    u.colscale = cs;
+    u.mean = static_cast<double*>(P.d_mean.p);
+    u.sdinv = static_cast<double*>(P.d_sdinv.p);
+    u.status = dst;
+    u.raw_g = dg;
+    u.raw_o = dO;
+    umma::launch_p2_umma(tA, tB, u, c.st);
+    ck(cudaGetLastError(), "launch");
+    std::vector<long long> hg((size_t)(L * V)), ho((size_t)(L * V));
+    std::vector<double> hcs((size_t)V);
+    unsigned stv = 0;
+    d2h(hg.data(), dg, hg.size(), c.st);
+    d2h(ho.data(), dO, ho.size(), c.st);
+    d2h(hcs.data(), cs, hcs.size(), c.st);
+    d2h(&stv, dst, 1, c.st);
+    ck(cudaStreamSynchronize(c.st), "snp products");
+    if (stv) fail(LDS_ERR_CUDA, "phase-2 tensor-core pipeline wait timed out (code %u)", stv);
+    for (int64_t j = 0; j < L; ++j) {
+        const double mu = P.mean[(size_t)(j0 + j)], sd = P.sdinv[(size_t)(j0 + j)];
+        for (int64_t v = 0; v < V; ++v) {
+            const size_t q = (size_t)(j * V + v);
+            out[q] = sd * hcs[(size_t)v] * ((double)hg[q] - mu * (double)ho[q]);
+        }
+    }
+    return out;
+}
+
+// Residual variances with covariates, fused form (compute_inv_resvar_from_geno_block,
+// gwldcore.cpp:3220-3333): ss_j = ||x_j||^2 + q - 2h with proj = R x_j,
+// h = ||proj||^2, q = proj^T G proj (G = resvar_gram, row-major p x p) or h;
+// df = N - p - 1.
+template <typename T>
+void inv_resvar_fused_cov(Context& c, const Prepared& P, int64_t j0, int64_t L, const T* Cm,
+                          const T* Rm, int64_t p, const T* gram, double eps, T* inv_out) {
+    const int64_t N = P.g.N;
+    if ((Cm != nullptr) != (Rm != nullptr))
+        fail(LDS_ERR_ARG, "C and R must be provided together for fused residual variances");
+    if (N - p <= 1) fail(LDS_ERR_ARG, "N_eff must be > 1 in fused residual variances");
+    const double df = (double)(N - p - 1);
+    std::vector<double> Rt((size_t)(N * p));
+    for (int64_t a = 0; a < p; ++a)
+        for (int64_t i = 0; i < N; ++i) Rt[(size_t)(a * N + i)] = (double)Rm[a + i * p];
+    const std::vector<double> proj = snp_products(c, P, j0, j0 + L, Rt, p);
+    for (int64_t j = 0; j < L; ++j) {
+        const double* pr = &proj[(size_t)(j * p)];
+        double h = 0.0;
+        for (int64_t a = 0; a < p; ++a) h += (double)(T)pr[a] * (double)(T)pr[a];
+        double q = h;
+        if (gram) {
+            q = 0.0;
+            for (int64_t a = 0; a < p; ++a) {
+                double gy = 0.0;
+                for (int64_t b = 0; b < p; ++b) gy += (double)gram[a * p + b] * (double)(T)pr[b];
+                q += (double)(T)pr[a] * gy;
+            }
+        }
+        const double ss = sumsq_std<T>(P, j0 + j) + q - 2.0 * h;
+        const double var = ss / df;
+        const double safe = std::isnan(var) ? var : (var > eps ? var : eps);
+        inv_out[j] = (T)(1.0 / std::sqrt(safe));
+    }
+}
+
+// Residual variances with covariates, block-projection form
+// (precompute_residual_variances_bed_impl, gwldcore.cpp:3335-3566):
+// ss_j = ||(I - C R) x_j||^2 = ||x||^2 - 2 (C^T x).(R x) + (R x)^T (C^T C) (R x),
+// df = N - p - 1; snp_var[j] = min(1, ss / ||x||^2) when requested.
+template <typename T>
+void inv_resvar_projected_cov(Context& c, const Prepared& P, int64_t nsnps, const T* Cm,
+                              const T* Rm, int64_t p, double eps, T* inv_out, double* snp_var) {
+    const int64_t N = P.g.N;
+    const double df = (double)(N - p - 1);
+    if (df <= 0.0) fail(LDS_ERR_ARG, "Projected residual df must be > 0 in precompute_residual_variances_bed");
+    std::vector<double> Y((size_t)(N * 2 * p));
+    for (int64_t a = 0; a < p; ++a)
+        for (int64_t i = 0; i < N; ++i) {
+            Y[(size_t)(a * N + i)] = (double)Rm[a + i * p];            // R rows
+            Y[(size_t)((p + a) * N + i)] = (double)Cm[a * N + i];      // C columns
+        }
+    std::vector<double> CtC((size_t)(p * p), 0.0);
+    for (int64_t a = 0; a < p; ++a)
+        for (int64_t b = 0; b < p; ++b) {
+            double s = 0.0;
+            for (int64_t i = 0; i < N; ++i) s += (double)Cm[a * N + i] * (double)Cm[b * N + i];
+            CtC[(size_t)(a * p + b)] = s;
+        }
+    const int64_t chunk = 1 << 16;
+    for (int64_t j0 = 0; j0 < nsnps; j0 += chunk) {
+        const int64_t j1 = std::min(nsnps, j0 + chunk);
+        const std::vector<double> pr = snp_products(c, P, j0, j1, Y, 2 * p);
+        for (int64_t j = j0; j < j1; ++j) {
+            const double* rx = &pr[(size_t)((j - j0) * 2 * p)];
+            const double* cx = rx + p;
+            double cross = 0.0, quad = 0.0;
+            for (int64_t a = 0; a < p; ++a) {
+                cross += cx[a] * rx[a];
+                double gy = 0.0;
+                for (int64_t b = 0; b < p; ++b) gy += CtC[(size_t)(a * p + b)] * rx[b];
+                quad += rx[a] * gy;
+            }
+            const double raw = sumsq_std<T>(P, j);
+            double ss = raw - 2.0 * cross + quad;
+            if (ss < 0.0) ss = 0.0;
+            const double var = ss / df;
+            const double safe = std::isnan(var) ? var : (var > eps ? var : eps);
+            inv_out[j] = (T)(1.0 / std::sqrt(safe));
+            if (snp_var) snp_var[j] = (raw > 0.0 && std::isfinite(ss)) ? std::min(1.0, ss / raw) : 0.0;
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Entry-point implementations
 // ---------------------------------------------------------------------------
@@ -700,7 +852,8 @@ void phase1_bed_impl(const char* bed_prefix, const char* fam_path, int blk_start
                      int64_t annot_rows, int64_t K, const T* inv_right, int v_start, int v_count,
                      int rand_dist, int has_seed, uint64_t seed, T* Xz, int64_t xz_rows,
                      int64_t xz_cols, uint8_t* bin_init, int impute, int has_iseed,
-                     uint64_t iseed, T* inv_out, double resvar_eps) {
+                     uint64_t iseed, T* inv_out, double resvar_eps, const T* Cm = nullptr,
+                     const T* Rm = nullptr, int64_t p = 0, const T* gram = nullptr) {
     Context& c = ctx();
     std::lock_guard<std::mutex> lk(c.mu);
     ensure_device(c);
@@ -715,7 +868,10 @@ void phase1_bed_impl(const char* bed_prefix, const char* fam_path, int blk_start
     if (annot_rows != L) fail(LDS_ERR_ARG, "L mismatch");
     std::vector<T> inv((size_t)L);
     if (inv_out) {
-        for (int64_t i = 0; i < L; ++i) inv[(size_t)i] = inv_resvar<T>(P, blk_start + i, resvar_eps);
+        if (Cm && Rm && p > 0)
+            inv_resvar_fused_cov<T>(c, P, blk_start, L, Cm, Rm, p, gram, resvar_eps, inv.data());
+        else
+            for (int64_t i = 0; i < L; ++i) inv[(size_t)i] = inv_resvar<T>(P, blk_start + i, resvar_eps);
         std::memcpy(inv_out, inv.data(), sizeof(T) * (size_t)L);
     } else {
         if (!inv_right) fail(LDS_ERR_ARG, "inv_right shape mismatch in phase1");
@@ -837,7 +993,8 @@ void phase2_bed_impl(const char* bed_prefix, const char* fam_path, int blk_start
 template <typename T>
 void resvar_impl(const char* bed_prefix, const char* fam_path, int nsnps, const int64_t* row_sel,
                  int64_t n_row_sel, int ddof, double eps, int impute, int has_iseed,
-                 uint64_t iseed, T* inv_out) {
+                 uint64_t iseed, T* inv_out, const T* Cm = nullptr, const T* Rm = nullptr,
+                 int64_t p = 0, double* snp_var = nullptr) {
     Context& c = ctx();
     std::lock_guard<std::mutex> lk(c.mu);
     ensure_device(c);
@@ -846,7 +1003,15 @@ void resvar_impl(const char* bed_prefix, const char* fam_path, int nsnps, const 
                                     has_iseed ? iseed : 0ULL, ddof, &M);
     if (nsnps > M) fail(LDS_ERR_ARG, "nsnps exceeds #SNPs in BIM");
     if (P.g.N <= 1) fail(LDS_ERR_ARG, "Invalid block dimensions in compute_inv_resvar_from_geno_block");
-    for (int64_t j = 0; j < nsnps; ++j) inv_out[j] = inv_resvar<T>(P, j, eps);
+    if ((Cm != nullptr) != (Rm != nullptr)) fail(LDS_ERR_ARG, "C and R must be provided together");
+    if (Cm && Rm && p > 0) {
+        inv_resvar_projected_cov<T>(c, P, nsnps, Cm, Rm, p, eps, inv_out, snp_var);
+        return;
+    }
+    for (int64_t j = 0; j < nsnps; ++j) {
+        inv_out[j] = inv_resvar<T>(P, j, eps);
+        if (snp_var) snp_var[j] = sumsq_std<T>(P, j) > 0.0 ? 1.0 : 0.0;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1683,13 +1848,14 @@ void phase1_bed_rowmajor_impl(const char* bed_prefix, const char* fam_path, int 
                               const T* annot, int64_t annot_rows, int64_t K, const T* inv_right,
                               int v_start, int v_count, int rand_dist, int has_seed, uint64_t seed,
                               T* Xz, int64_t xz_rows, int64_t xz_cols, int impute, int has_iseed,
-                              uint64_t iseed, T* inv_out, double resvar_eps) {
+                              uint64_t iseed, T* inv_out, double resvar_eps, const T* Cm,
+                              const T* Rm, int64_t p, const T* gram) {
     if (xz_cols != K * v_count) fail(LDS_ERR_ARG, "Xz2d_chunk shape must be (N, B*v_count)");
     std::vector<T> tmp((size_t)(xz_rows * xz_cols), T(0));
     phase1_bed_impl<T>(bed_prefix, fam_path, blk_start, blk_end, row_sel, n_row_sel, ddof, annot,
                        annot_rows, K, inv_right, v_start, v_count, rand_dist, has_seed, seed,
                        tmp.data(), xz_rows, xz_cols, nullptr, impute, has_iseed, iseed, inv_out,
-                       resvar_eps);
+                       resvar_eps, Cm, Rm, p, gram);
     for (int64_t n = 0; n < xz_rows; ++n)
         for (int64_t q = 0; q < xz_cols; ++q) Xz[n * xz_cols + q] += tmp[(size_t)(q * xz_rows + n)];
 }
@@ -2234,14 +2400,16 @@ LDS_API void lds_clear_device_cache(void) {
         int64_t annot_rows, int64_t K, const T *inv_right, int v_start, int v_count,            \
         int kmax_hint, int rand_dist, int has_seed, uint64_t seed, T *Xz2d_chunk,                \
         int64_t xz_rows, int64_t xz_cols, uint8_t *bin_init_mask, int impute_mode,              \
-        int has_impute_seed, uint64_t impute_seed, T *inv_out, double resvar_eps
+        int has_impute_seed, uint64_t impute_seed, T *inv_out, double resvar_eps, const T *C,   \
+        const T *R, int64_t p, const T *resvar_gram
 #define P1_CALL(T)                                                                              \
     guarded([&] {                                                                               \
         (void)kmax_hint;                                                                        \
         phase1_bed_impl<T>(bed_prefix, fam_path, blk_start, blk_end, row_sel, n_row_sel, ddof,  \
                            annot_blk, annot_rows, K, inv_right, v_start, v_count, rand_dist,    \
                            has_seed, seed, Xz2d_chunk, xz_rows, xz_cols, bin_init_mask,         \
-                           impute_mode, has_impute_seed, impute_seed, inv_out, resvar_eps);     \
+                           impute_mode, has_impute_seed, impute_seed, inv_out, resvar_eps, C,   \
+                           R, p, resvar_gram);                                                  \
     })
 LDS_API int lds_phase1_compute_Xz_bed_chunk_f32(P1_ARGS(float)) { return P1_CALL(float); }
 LDS_API int lds_phase1_compute_Xz_bed_chunk_f64(P1_ARGS(double)) { return P1_CALL(double); }
@@ -2268,7 +2436,8 @@ LDS_API int lds_phase2_accum_XtXz_bed_f64(P2_ARGS(double)) { return P2_CALL(doub
         int64_t annot_rows, int64_t K, const T *inv_right, int v_start, int v_count,            \
         int kmax_hint, int rand_dist, int has_seed, uint64_t seed, T *Xz2d_chunk,                \
         int64_t xz_rows, int64_t xz_cols, int impute_mode, int has_impute_seed,                 \
-        uint64_t impute_seed, T *inv_out, double resvar_eps
+        uint64_t impute_seed, T *inv_out, double resvar_eps, const T *C, const T *R, int64_t p, \
+        const T *resvar_gram
 #define P1R_CALL(T)                                                                             \
     guarded([&] {                                                                               \
         (void)kmax_hint;                                                                        \
@@ -2276,7 +2445,7 @@ LDS_API int lds_phase2_accum_XtXz_bed_f64(P2_ARGS(double)) { return P2_CALL(doub
                                     n_row_sel, ddof, annot_blk, annot_rows, K, inv_right,       \
                                     v_start, v_count, rand_dist, has_seed, seed, Xz2d_chunk,    \
                                     xz_rows, xz_cols, impute_mode, has_impute_seed, impute_seed, \
-                                    inv_out, resvar_eps);                                       \
+                                    inv_out, resvar_eps, C, R, p, resvar_gram);                 \
     })
 LDS_API int lds_phase1_compute_Xz_bed_chunk_rowmajor_f32(P1R_ARGS(float)) { return P1R_CALL(float); }
 LDS_API int lds_phase1_compute_Xz_bed_chunk_rowmajor_f64(P1R_ARGS(double)) { return P1R_CALL(double); }
@@ -2366,12 +2535,13 @@ LDS_API int lds_standardize_dosage_inplace_f64(double* G, int64_t N, int64_t L, 
 #define RV_ARGS(T)                                                                              \
     const char *bed_prefix, const char *fam_path, int nsnps, int step_size,                     \
         const int64_t *row_sel, int64_t n_row_sel, int ddof, double eps, int impute_mode,       \
-        int has_impute_seed, uint64_t impute_seed, T *inv_out
+        int has_impute_seed, uint64_t impute_seed, T *inv_out, const T *C, const T *R,          \
+        int64_t p, double *snp_var_out
 #define RV_CALL(T)                                                                              \
     guarded([&] {                                                                               \
         (void)step_size;                                                                        \
         resvar_impl<T>(bed_prefix, fam_path, nsnps, row_sel, n_row_sel, ddof, eps, impute_mode, \
-                       has_impute_seed, impute_seed, inv_out);                                  \
+                       has_impute_seed, impute_seed, inv_out, C, R, p, snp_var_out);            \
     })
 LDS_API int lds_precompute_residual_variances_bed_f32(RV_ARGS(float)) { return RV_CALL(float); }
 LDS_API int lds_precompute_residual_variances_bed_f64(RV_ARGS(double)) { return RV_CALL(double); }

@@ -59,6 +59,25 @@ def _rw(arr, dtype, order, name):
     return arr
 
 
+def _cov(C, R, dt, gram=None):
+    """Covariate basis C (N x p) and R (p x N) as column-major arrays of dtype dt."""
+    if C is None or R is None:
+        if (C is None) != (R is None):
+            raise RuntimeError("C and R must be provided together for fused residual variances")
+        return None, None, 0, None
+    Cf = np.asfortranarray(C, dtype=dt)
+    Rf = np.asfortranarray(R, dtype=dt)
+    p = Cf.shape[1]
+    if Rf.shape != (p, Cf.shape[0]):
+        raise RuntimeError("C/R shape mismatch in fused residual variances")
+    G = None
+    if gram is not None:
+        G = np.ascontiguousarray(gram, dtype=dt)
+        if G.shape != (p, p):
+            raise RuntimeError("covariate Gram shape mismatch in fused residual variances")
+    return Cf, Rf, p, G
+
+
 def _impute(mode: str) -> int:
     if mode not in _lib.LDS_IMPUTE:
         raise RuntimeError("impute_mode must be 'mean' or 'hwe'")
@@ -127,9 +146,10 @@ def phase1_compute_Xz_bed_chunk(bed_prefix, fam_path, blk_start, blk_end, row_se
     _rw(Xz, dt, "F", "Xz2d_chunk")
     if Xz.ndim != 2:
         raise RuntimeError("Xz2d_chunk shape must be (N, B*v_count)")
-    if (C is not None or R is not None) and (project_right or inv_out is not None):
-        raise RuntimeError("covariate projection inside phase 1 is not supported by the B200 "
-                           "backend; project Xz2d after phase 1 (project_colmajor_inplace)")
+    if project_right:
+        raise RuntimeError("project_right is not supported by the B200 backend; project Xz2d "
+                           "after phase 1 (project_colmajor_inplace), as gw_ldscore.py does")
+    Cf, Rf, p, G = _cov(C, R, dt, resvar_gram) if inv_out is not None else (None, None, 0, None)
     ann = np.ascontiguousarray(_need("annot_blk", annot_blk), dtype=dt)
     if ann.ndim != 2:
         raise RuntimeError("L mismatch")
@@ -154,7 +174,7 @@ def phase1_compute_Xz_bed_chunk(bed_prefix, fam_path, blk_start, blk_end, row_se
              int(seed is not None), 0 if seed is None else int(seed) & (2**64 - 1), ptr(Xz),
              Xz.shape[0], Xz.shape[1], ptr(bin_init_mask), _impute(impute_mode),
              int(impute_seed is not None), 0 if impute_seed is None else int(impute_seed),
-             ptr(inv_out), float(resvar_eps)))
+             ptr(inv_out), float(resvar_eps), ptr(Cf), ptr(Rf), p, ptr(G)))
 
 
 # ---------------------------------------------------------------------------
@@ -210,9 +230,10 @@ def phase1_compute_Xz_bed_chunk_rowmajor(bed_prefix, fam_path, blk_start, blk_en
     _rw(Xz, dt, "C", "Xz2d_chunk")
     if Xz.ndim != 2:
         raise RuntimeError("Xz2d_chunk shape must be (N, B*v_count)")
-    if (C is not None or R is not None) and (project_right or inv_out is not None):
-        raise RuntimeError("covariate projection inside phase 1 is not supported by the B200 "
-                           "backend; project Xz2d after phase 1 (project_rowmajor_inplace_and_col_sums)")
+    if project_right:
+        raise RuntimeError("project_right is not supported by the B200 backend; project Xz2d "
+                           "after phase 1 (project_rowmajor_inplace_and_col_sums)")
+    Cf, Rf, p, G = _cov(C, R, dt, resvar_gram) if inv_out is not None else (None, None, 0, None)
     ann = np.ascontiguousarray(_need("annot_blk", annot_blk), dtype=dt)
     inv_r = None
     if inv_out is not None:
@@ -229,7 +250,8 @@ def phase1_compute_Xz_bed_chunk_rowmajor(bed_prefix, fam_path, blk_start, blk_en
              int(_need("kmax_hint", kmax_hint)), _dist(rand_dist), int(seed is not None),
              0 if seed is None else int(seed) & (2**64 - 1), ptr(Xz), Xz.shape[0], Xz.shape[1],
              _impute(impute_mode), int(impute_seed is not None),
-             0 if impute_seed is None else int(impute_seed), ptr(inv_out), float(resvar_eps)))
+             0 if impute_seed is None else int(impute_seed), ptr(inv_out), float(resvar_eps),
+             ptr(Cf), ptr(Rf), p, ptr(G)))
 
 
 def _mailman_common(meansq_accum, Xz2d, order, inv_left, mc_aggregate_sumsq, mc_per_snp_sumsq,
@@ -345,16 +367,30 @@ def precompute_residual_variances_bed(bed_prefix, fam_path, nsnps, step_size, ro
                                       ddof=1, eps=1e-10, compute_mu22=False, annot_all=None,
                                       C=None, R=None, impute_mode="hwe", impute_seed=None,
                                       snp_var_out=None, dtype=np.float64):
-    if C is not None or R is not None or compute_mu22 or snp_var_out is not None:
-        raise RuntimeError("covariates, mu22 and snp_var_out are not supported by the B200 "
-                           "residual-variance entry")
+    if compute_mu22:
+        raise RuntimeError("compute_mu22 is not supported by the B200 residual-variance entry")
     t = "f32" if np.dtype(dtype) == np.float32 else "f64"
-    out = np.empty(int(nsnps), dtype=np.float32 if t == "f32" else np.float64)
+    dt = np.float32 if t == "f32" else np.float64
+    out = np.empty(int(nsnps), dtype=dt)
+    if C is not None and R is not None:
+        Cf = np.asfortranarray(C, dtype=dt)
+        Rf = np.asfortranarray(R, dtype=dt)
+        p = Cf.shape[1]
+        if Rf.shape != (p, Cf.shape[0]):
+            raise RuntimeError("C/R shape mismatch in precompute_residual_variances_bed")
+    else:
+        Cf = Rf = None
+        p = 0
+    if snp_var_out is not None:
+        _rw(snp_var_out, np.float64, "C", "snp_var_out")
+        if snp_var_out.shape[0] != int(nsnps):
+            raise RuntimeError("snp_var_out shape mismatch in precompute_residual_variances_bed")
     rows, nr = _rows(row_sel)
     fn = getattr(_lib.load(), f"lds_precompute_residual_variances_bed_{t}")
     check(fn(enc(bed_prefix), enc(fam_path), int(nsnps), int(step_size), ptr(rows), nr, int(ddof),
              float(eps), _impute(impute_mode), int(impute_seed is not None),
-             0 if impute_seed is None else int(impute_seed), ptr(out)))
+             0 if impute_seed is None else int(impute_seed), ptr(out), ptr(Cf), ptr(Rf), p,
+             ptr(snp_var_out)))
     return out, None
 
 

@@ -112,3 +112,41 @@ def test_standardize_dosage_matches_reference(reference, dt):
     bad[0, 0] = 3.5
     with pytest.raises(RuntimeError, match="out-of-range"):
         gwldcore.standardize_dosage_inplace(bad)
+
+
+def _covariates(n, p=3, seed=12):
+    rng = np.random.default_rng(seed)
+    C = np.linalg.qr(np.column_stack([np.ones(n)] + [rng.normal(size=n) for _ in range(p - 1)]))[0]
+    return np.asfortranarray(C), np.asfortranarray(C.T)
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.float32])
+def test_residual_variances_with_covariates_match_reference(small_bed, reference, dt):
+    """precompute_residual_variances_bed with C, R and snp_var_out, and the
+    phase-1 fused residual variances with C, R and the covariate Gram."""
+    from summit_b200 import gwldcore
+
+    n, m, prefix = small_bed["n"], small_bed["m"], small_bed["prefix"]
+    C, R = _covariates(n)
+    sv_r, sv_g = np.zeros(m), np.zeros(m)
+    inv_r = reference.resvar_bed_cov(prefix, m, 100, C, R, dtype=dt, snp_var=sv_r)
+    inv_g, mu22 = gwldcore.precompute_residual_variances_bed(
+        prefix, prefix + ".fam", m, 100, C=C, R=R, impute_mode="mean", snp_var_out=sv_g, dtype=dt)
+    assert mu22 is None
+    tol = 1e-6 if dt == np.float32 else 1e-9
+    assert rel_err(inv_g, inv_r) < tol
+    assert np.max(np.abs(sv_g - sv_r)) < tol
+    a, b, V, K = 30, 230, 8, 2
+    annot = np.ones((b - a, K), dtype=dt)
+    gram = (C.T @ C).astype(dt)
+    for g in (None, gram):
+        Xr = np.zeros((n, K * V), dtype=dt, order="F")
+        Xg = np.zeros((n, K * V), dtype=dt, order="F")
+        fr = reference.phase1_bed_cov(prefix, a, b, annot, 0, V, 31, Xr, C, R, g)
+        fg = np.empty(b - a, dtype=dt)
+        gwldcore.phase1_compute_Xz_bed_chunk(prefix, prefix + ".fam", a, b, annot_blk=annot,
+                                             inv_right=None, v_start=0, v_count=V, kmax_hint=1,
+                                             seed=31, Xz2d_chunk=Xg, C=C, R=R, impute_mode="mean",
+                                             resvar_gram=g, inv_out=fg)
+        assert rel_err(fg, fr) < tol
+        assert rel_err(Xg, Xr) < (1e-6 if dt == np.float32 else 1e-7)
