@@ -469,6 +469,32 @@ int lds_philox_rademacher(const uint64_t* keys, int64_t probes, int64_t rows, do
                           int device_ptrs);
 
 /* ---------------------------------------------------------------------
+ * SNP-block jackknife and normal-equation solves in FP64 on the device
+ * (inference/jackknife.py:109-214, context/fit.py:435-525, replicate SE of
+ * inference/gxe.py:2052-2057).
+ *
+ * lds_block_boundaries: contiguous jackknife blocks of M SNPs; mass == NULL
+ *   gives equal-count blocks (_equal_count_block_boundaries), otherwise
+ *   weighted blocks (_weighted_contiguous_block_boundaries, min_snps per block).
+ * lds_sym_solve: nsys systems laid out as (K*K row-major matrix, K rhs);
+ *   symmetrize, eigendecompose, keep |lambda| > max(100 eps scale,
+ *   rtol max|lambda|), x = sum_kept v (v^T b)/(v^T A v); rank and ascending
+ *   eigenvalues per system (either may be NULL).  Asymmetry above 2e-10 scale,
+ *   non-finite input, or (require_full_rank) rank < K is an error.  K <= 96.
+ * lds_jackknife_normal_equations: terms is M x (K*K + K) per-SNP contributions
+ *   [vec(A_j), b_j]; blocks [starts[b], ends[b]); theta = solve(sum A, sum b),
+ *   replicates[b] = delete-block-b solutions, se = sqrt((B-1)/B sum (r - mean)^2),
+ *   cov the matching covariance (rank-revealing solves, rtol).
+ * ------------------------------------------------------------------- */
+int lds_block_boundaries(int64_t M, int B, const double* mass, int min_snps, int64_t* starts,
+                         int64_t* ends);
+int lds_sym_solve(const double* systems, int64_t nsys, int K, double rtol, int require_full_rank,
+                  double* x, int* rank, double* eigenvalues, int device_ptrs);
+int lds_jackknife_normal_equations(const double* terms, int64_t M, int K, const int64_t* starts,
+                                   const int64_t* ends, int64_t B, double rtol, double* theta,
+                                   double* replicates, double* se, double* cov, int device_ptrs);
+
+/* ---------------------------------------------------------------------
  * Surrogate network of the learned control variate (no counterpart in the
  * reference): in_dim -> 128 -> 128 -> 128 -> out_dim, GELU (erf form) after the
  * hidden layers, FP32 master parameters, BF16 weights and activations in the

@@ -79,6 +79,10 @@ SIGNATURES: dict[str, tuple] = {
                                           _i64, _i64, _int, _int, _int]),
     "lds_gxe_normalize_scores": (_int, [_p, _p, _p, _p, _i64, _i64, _int, _int]),
     "lds_philox_rademacher": (_int, [_p, _i64, _i64, _p, _int]),
+    "lds_block_boundaries": (_int, [_i64, _int, _p, _int, _p, _p]),
+    "lds_sym_solve": (_int, [_p, _i64, _int, _dbl, _int, _p, _p, _p, _int]),
+    "lds_jackknife_normal_equations": (_int, [_p, _i64, _int, _p, _p, _i64, _dbl, _p, _p, _p, _p,
+                                              _int]),
     "lds_gw_plan_create": (_int, [_i64, _p, _i64, _int, _int, _int, _u64, _int, _dbl, _int, _int,
                                   _p]),
     "lds_gw_plan_execute": (_int, [_i64]),

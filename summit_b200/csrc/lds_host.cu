@@ -3526,3 +3526,193 @@ LDS_API int lds_philox_rademacher(const uint64_t* keys, int64_t probes, int64_t 
         ck(cudaStreamSynchronize(c.st), "philox");
     });
 }
+
+
+// ---------------------------------------------------------------------------
+// SNP-block jackknife and normal-equation solves (include/lds.h)
+// ---------------------------------------------------------------------------
+namespace {
+// NumPy's pairwise summation of float64 (the algorithm behind np.sum): blocks
+// of 8 partial sums up to 128 elements, halves (rounded to a multiple of 8)
+// above that.
+double pairwise_sum(const double* a, int64_t n) {
+    if (n < 8) {
+        double r = 0.0;
+        for (int64_t i = 0; i < n; ++i) r += a[i];
+        return r;
+    }
+    if (n <= 128) {
+        double r[8];
+        for (int k = 0; k < 8; ++k) r[k] = a[k];
+        int64_t i = 8;
+        for (; i < n - (n % 8); i += 8)
+            for (int k = 0; k < 8; ++k) r[k] += a[i + k];
+        double res = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + (r[6] + r[7]));
+        for (; i < n; ++i) res += a[i];
+        return res;
+    }
+    int64_t n2 = n / 2;
+    n2 -= n2 % 8;
+    return pairwise_sum(a, n2) + pairwise_sum(a + n2, n - n2);
+}
+}  // namespace
+
+LDS_API int lds_block_boundaries(int64_t M, int B, const double* mass, int min_snps,
+                                 int64_t* starts, int64_t* ends) {
+    return guarded([&] {
+        if (!(1 <= B && B <= M)) fail(LDS_ERR_ARG, "Need 1 <= nblocks <= nsnps, got B=%d, M=%lld", B, (long long)M);
+        auto equal = [&] {
+            // edges = floor(linspace(0, M, B + 1)), last edge M (jackknife.py:109-118)
+            const double step = (double)M / (double)B;
+            std::vector<int64_t> e((size_t)B + 1);
+            for (int i = 0; i < B; ++i) e[(size_t)i] = (int64_t)std::floor((double)i * step);
+            e[(size_t)B] = M;
+            for (int i = 0; i < B; ++i) {
+                starts[i] = e[(size_t)i];
+                ends[i] = e[(size_t)i + 1];
+                if (ends[i] <= starts[i]) fail(LDS_ERR_INTERNAL, "Equal-count partition produced an empty block.");
+            }
+        };
+        if (!mass) {
+            equal();
+            return;
+        }
+        // weighted contiguous boundaries (jackknife.py:156-211)
+        if (min_snps <= 0) fail(LDS_ERR_ARG, "min_snps must be >= 1");
+        if ((int64_t)min_snps * B > M)
+            fail(LDS_ERR_ARG, "min_snps * nblocks exceeds nsnps: %d * %d > %lld", min_snps, B, (long long)M);
+        std::vector<double> m((size_t)M);
+        for (int64_t j = 0; j < M; ++j)
+            m[(size_t)j] = (std::isfinite(mass[j]) && mass[j] > 0.0) ? mass[j] : 0.0;
+        const double total = pairwise_sum(m.data(), M);
+        if (!(std::isfinite(total) && total > 0.0)) {
+            equal();
+            return;
+        }
+        std::vector<double> cs((size_t)M);
+        double acc = 0.0;
+        for (int64_t j = 0; j < M; ++j) cs[(size_t)j] = (acc += m[(size_t)j]);
+        int64_t st = 0;
+        for (int b = 0; b < B; ++b) {
+            starts[b] = st;
+            const int rem = B - b - 1;
+            int64_t e;
+            if (rem == 0) {
+                e = M;
+            } else {
+                const int64_t low = st + min_snps, high = M - (int64_t)rem * min_snps;
+                const double target = (double)(b + 1) * total / (double)B;
+                e = (int64_t)(std::lower_bound(cs.begin(), cs.end(), target) - cs.begin()) + 1;
+                if (e < low) e = low;
+                if (e > high) e = high;
+            }
+            ends[b] = e;
+            st = e;
+        }
+        if (starts[0] != 0 || ends[B - 1] != M)
+            fail(LDS_ERR_INTERNAL, "Weighted contiguous partition produced invalid block boundaries.");
+        for (int b = 0; b < B; ++b)
+            if (ends[b] <= starts[b])
+                fail(LDS_ERR_INTERNAL, "Weighted contiguous partition produced invalid block boundaries.");
+    });
+}
+
+// Systems laid out as nsys x (K*K row-major matrix, K rhs).
+static void sym_solve_impl(Context& c, const double* dsys, int64_t nsys, int K, double rtol,
+                           int require_full_rank, double* x, int* rank, double* eig,
+                           int device_ptrs) {
+    if (K <= 0 || K > sym_solve_max_k()) fail(LDS_ERR_ARG, "system size must be in [1, %d]", sym_solve_max_k());
+    if (!std::isfinite(rtol) || rtol <= 0.0) fail(LDS_ERR_ARG, "rtol must be finite and positive.");
+    DevBuf dx, dr, de, dstat;
+    // The kernel writes x, rank and eigenvalues of every system: each gets a
+    // device buffer of its own unless the caller passed a device pointer.
+    double* xo = (device_ptrs && x) ? x : dx.as<double>((size_t)(nsys * K));
+    int* ro = (device_ptrs && rank) ? rank : dr.as<int>((size_t)nsys);
+    double* eo = (device_ptrs && eig) ? eig : de.as<double>((size_t)(nsys * K));
+    int* so = dstat.as<int>((size_t)nsys);
+    launch_sym_solve(dsys, nsys, K, rtol, require_full_rank, xo, ro, eo, so, c.st);
+    ck(cudaGetLastError(), "launch");
+    std::vector<int> st((size_t)nsys), rk((size_t)nsys);
+    d2h(st.data(), so, st.size(), c.st);
+    d2h(rk.data(), ro, rk.size(), c.st);
+    if (!device_ptrs) {
+        if (x) d2h(x, xo, (size_t)(nsys * K), c.st);
+        if (rank) d2h(rank, ro, (size_t)nsys, c.st);
+        if (eig) d2h(eig, eo, (size_t)(nsys * K), c.st);
+    }
+    ck(cudaStreamSynchronize(c.st), "solve");
+    for (int64_t q = 0; q < nsys; ++q) {
+        if (st[(size_t)q] & 4) fail(LDS_ERR_ARG, "normal matrix contains non-finite values.");
+        if (st[(size_t)q] & 1) fail(LDS_ERR_ARG, "Normal matrix has material asymmetry.");
+        if (st[(size_t)q] & 2)
+            fail(LDS_ERR_ARG, "Contextual normal system is not identifiable: rank %d of %d.",
+                 rk[(size_t)q], K);
+    }
+}
+
+LDS_API int lds_sym_solve(const double* systems, int64_t nsys, int K, double rtol,
+                          int require_full_rank, double* x, int* rank, double* eigenvalues,
+                          int device_ptrs) {
+    return guarded([&] {
+        if (!systems || nsys <= 0) fail(LDS_ERR_ARG, "no systems");
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        ensure_device(c);
+        DevBuf ds;
+        const double* d = systems;
+        if (!device_ptrs) {
+            double* t = ds.as<double>((size_t)(nsys * (K * K + K)));
+            h2d(t, systems, (size_t)(nsys * (K * K + K)), c.st);
+            d = t;
+        }
+        sym_solve_impl(c, d, nsys, K, rtol, require_full_rank, x, rank, eigenvalues, device_ptrs);
+    });
+}
+
+LDS_API int lds_jackknife_normal_equations(const double* terms, int64_t M, int K,
+                                           const int64_t* starts, const int64_t* ends, int64_t B,
+                                           double rtol, double* theta, double* replicates,
+                                           double* se, double* cov, int device_ptrs) {
+    return guarded([&] {
+        if (!terms || !starts || !ends || M <= 0 || B <= 1) fail(LDS_ERR_ARG, "invalid jackknife inputs");
+        for (int64_t b = 0; b < B; ++b)
+            if (starts[b] < 0 || ends[b] > M || ends[b] <= starts[b])
+                fail(LDS_ERR_ARG, "invalid jackknife block boundaries");
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        ensure_device(c);
+        const int64_t P = (int64_t)K * K + K;
+        DevBuf dt, dst, den, dblk, dsys, dx, dr, de, dmean, dse, dcov;
+        const double* t = terms;
+        if (!device_ptrs) {
+            double* p = dt.as<double>((size_t)(M * P));
+            h2d(p, terms, (size_t)(M * P), c.st);
+            t = p;
+        }
+        int64_t* s_ = dst.as<int64_t>((size_t)B);
+        int64_t* e_ = den.as<int64_t>((size_t)B);
+        h2d(s_, starts, (size_t)B, c.st);
+        h2d(e_, ends, (size_t)B, c.st);
+        double* blk = dblk.as<double>((size_t)(B * P));
+        launch_block_sums(t, P, s_, e_, B, blk, c.st);
+        double* sys = dsys.as<double>((size_t)((B + 1) * P));
+        launch_delete_one(blk, B, P, sys, c.st);
+        double* xs = dx.as<double>((size_t)((B + 1) * K));
+        sym_solve_impl(c, sys, B + 1, K, rtol, 0, xs, nullptr, nullptr, 1);
+        double* mean = dmean.as<double>((size_t)K);
+        double* sed = dse.as<double>((size_t)K);
+        double* cv = dcov.as<double>((size_t)(K * K));
+        launch_jackknife_stats(xs + K, B, K, mean, sed, cv, c.st);
+        ck(cudaGetLastError(), "launch");
+        auto out = [&](double* dst_, const double* src, size_t n) {
+            if (!dst_) return;
+            if (device_ptrs) ck(cudaMemcpyAsync(dst_, src, n * sizeof(double), cudaMemcpyDeviceToDevice, c.st), "copy");
+            else d2h(dst_, src, n, c.st);
+        };
+        out(theta, xs, (size_t)K);
+        out(replicates, xs + K, (size_t)(B * K));
+        out(se, sed, (size_t)K);
+        out(cov, cv, (size_t)(K * K));
+        ck(cudaStreamSynchronize(c.st), "jackknife");
+    });
+}

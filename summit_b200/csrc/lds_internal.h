@@ -167,6 +167,16 @@ template <typename T> void launch_standardize_dosage(T* G, int64_t N, int64_t L,
                                                      double missing, unsigned long long* counts,
                                                      cudaStream_t st);
 
+// Jackknife and normal-equation solves (lds_jack.cu).
+int sym_solve_max_k();
+void launch_block_sums(const double* X, int64_t P, const int64_t* starts, const int64_t* ends,
+                       int64_t B, double* out, cudaStream_t st);
+void launch_delete_one(const double* blocks, int64_t B, int64_t P, double* sys, cudaStream_t st);
+void launch_sym_solve(const double* sys, int64_t nsys, int K, double rtol, int require_full_rank,
+                      double* x, int* rank, double* eig, int* status, cudaStream_t st);
+void launch_jackknife_stats(const double* reps, int64_t R, int K, double* mean, double* se,
+                            double* cov, cudaStream_t st);
+
 // Near-field control variate sums (lds_cv.cu): C[j K + k] += sum_v a_jkv^2 and,
 // if mu is set, mu[j K + k] = E[a_jk^2]; D in {4, 8, 15}.
 struct CvNearArgs {
