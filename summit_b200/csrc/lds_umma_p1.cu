@@ -269,6 +269,7 @@ __global__ void __launch_bounds__(p1::kThreads, 1)
                         if (vb < a.V) scB = a.colscale[o + vb];
                     }
                 }
+                int8_t* const yrow = a.yq ? a.yq + (int64_t)k * a.ncolp * a.N_pad + i : nullptr;
                 if (!mbar_wait(&acc_full[b], (uint32_t)u & 1u)) { fail(15); break; }
                 tc_fence_after();
                 const int ncols = min(kAccCols, a.ncolp - g * 256);
@@ -309,18 +310,14 @@ __global__ void __launch_bounds__(p1::kThreads, 1)
                             w |= ((uint32_t)(U >> 7) & 127u) << 16;
                             w |= ((uint32_t)U & 127u) << 24;
                             w = __vsub4(w, 0x3F3F3F00u);
-                            // Quad transpose: lane 4g+p ends with digit p of samples 4g..4g+3.
-                            const int qb = lane & ~3, p4 = lane & 3;
-                            const uint32_t w0 = __shfl_sync(0xffffffffu, w, qb + 0);
-                            const uint32_t w1 = __shfl_sync(0xffffffffu, w, qb + 1);
-                            const uint32_t w2 = __shfl_sync(0xffffffffu, w, qb + 2);
-                            const uint32_t w3 = __shfl_sync(0xffffffffu, w, qb + 3);
-                            uint32_t c0, c1, c2, c3;
-                            transpose4x4(w0, w1, w2, w3, c0, c1, c2, c3);
-                            const uint32_t uu = p4 == 0 ? c0 : p4 == 1 ? c1 : p4 == 2 ? c2 : c3;
-                            // first sample of the quad is i - p4 (4-byte aligned)
-                            *reinterpret_cast<uint32_t*>(
-                                a.yq + ((int64_t)k * a.ncolp + 4 * v + p4) * a.N_pad + (i - p4)) = uu;
+                            // Digit t of probe v for this lane's sample: one byte
+                            // store per digit row; the warp's 32 lanes write 32
+                            // consecutive samples, one full sector per store.
+                            int8_t* dst = yrow + (int64_t)(4 * v) * a.N_pad;
+                            dst[0] = (int8_t)(w & 0xFFu);
+                            dst[a.N_pad] = (int8_t)((w >> 8) & 0xFFu);
+                            dst[2 * a.N_pad] = (int8_t)((w >> 16) & 0xFFu);
+                            dst[3 * a.N_pad] = (int8_t)(w >> 24);
                         } else {
                             const double sc = __shfl_sync(0xffffffffu, vl < 32 ? scA : scB, vl & 31);
                             a.Y[((int64_t)k * a.V + v) * a.N_pad + i] = sc * (double)T;
