@@ -570,6 +570,89 @@ def ours_arm(args) -> None:
 
 
 # ---------------------------------------------------------------------------
+# Exact windowed LD scores (winldcore form) over the config-2 windows: unbiased
+# r^2 within each window (the partition is expressed as base-pair positions 1e9
+# apart between windows and a 5 kb window), tensor-core Gram products.
+# Value: 2 N sum_w L_w^2 / time (the reference's FP64 SYRK/GEMM work).
+# ---------------------------------------------------------------------------
+EXACT_METRIC = "pair-product TOPS (exact windowed LD scores, unbiased r^2)"
+
+
+def partition_positions(ws: np.ndarray) -> np.ndarray:
+    win = np.repeat(np.arange(ws.size - 1), np.diff(ws))
+    return (win.astype(np.int64) * 1_000_000_000 + (np.arange(ws[-1]) - ws[win]) + 1).astype(np.int64)
+
+
+def exact_arm(args) -> None:
+    import torch
+
+    from summit_b200 import _lib, gwldcore
+    from summit_b200.session import GwSession
+
+    torch.cuda.set_device(env_int("LOCAL_RANK", 0))
+    n, m = N_SAMPLES, env_int("LDS_BENCH_M", M_SNPS)
+    bed = gwldcore.synth_bed_rows(n, m, DATA_SEED)
+    annot = annotations(m)
+    ws = windows(m)
+    win = np.repeat(np.arange(ws.size - 1), np.diff(ws))
+    lo, hi = ws[win], ws[win + 1]
+    ops = 2.0 * n * float((np.diff(ws).astype(np.float64) ** 2).sum())
+    lib = _lib.load()
+    sess = GwSession(bed, n)
+    buf = np.zeros(4)
+    for _ in range(args.warmup):
+        sess.window_ld(lo, hi, annot, corr_dim=n - 1)
+    times = []
+    launches0 = lib.lds_kernel_launches()
+    with Clocks(env_int("LOCAL_RANK", 0)) as clk:
+        for _ in range(args.steps):
+            out = sess.window_ld(lo, hi, annot, corr_dim=n - 1)
+            lib.lds_last_timings(buf.ctypes.data_as(__import__("ctypes").c_void_p), 4)
+            times.append(float(buf[0]))
+    launches = int(lib.lds_kernel_launches() - launches0) // max(args.steps, 1)
+    ms = float(np.mean(times))
+    t0 = time.perf_counter()
+    s2 = GwSession(bed, n)
+    out2 = s2.window_ld(lo, hi, annot, corr_dim=n - 1)
+    e2e_s = time.perf_counter() - t0
+    s2.close()
+    assert np.array_equal(out, out2)
+    line = {"metric": EXACT_METRIC, "value": round(ops / (ms * 1e-3) / 1e12, 3), "unit": "TOPS",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 2),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "int8 exact Gram sums, f64 r and sums", "data": "synthetic",
+            "config": {"workload": "exact_windowed_ld_n50k_m500k_w200-5000_k24", "N": n, "M": m,
+                       "windows": int(ws.size - 1), "K": K_BINS,
+                       "snp_pairs": float((np.diff(ws).astype(np.float64) ** 2).sum())},
+            "e2e": {"value": round(ops / e2e_s / 1e12, 3), "unit": "TOPS",
+                    "h2d_bytes_per_step": int(bed.nbytes + annot.nbytes + lo.nbytes + hi.nbytes),
+                    "d2h_bytes_per_step": int(out.nbytes), "ms_per_step": round(e2e_s * 1e3, 1)},
+            "gpu_launches": launches, "clocks": clk.summary()}
+    if not os.environ.get("LDS_SKIP_CPU_BASELINE"):
+        from oracle.oracle import ReferenceWindowed
+        from summit_b200 import bedfile
+
+        threads = cpu_threads()
+        ref = ReferenceWindowed()
+        ref.set_threads(threads)
+        k = int(np.searchsorted(ws, env_int("LDS_EXACT_CPU_SNPS", 6000))) + 1
+        k = min(k, ws.size - 1)
+        ms_ = int(ws[k])
+        with tempfile.TemporaryDirectory() as td:
+            pre = bedfile.write_plink(Path(td) / "exact", packed=bed[:ms_], n=n)
+            bp = partition_positions(ws[:k + 1])
+            t0 = time.perf_counter()
+            ref.compute_windowed_ld_chr(pre, 0, ms_, bp, annot[:ms_], 5.0, 1000)
+            sec = time.perf_counter() - t0
+        cops = 2.0 * n * float((np.diff(ws[:k + 1]).astype(np.float64) ** 2).sum())
+        line["cpu_baseline"] = {"value": round(cops / sec / 1e12, 6), "unit": "TOPS", "cores": threads,
+                                "kind": "reference",
+                                "sample": f"first {k} windows ({ms_} SNPs); reference winldcore.cpp "
+                                          f"compiled unchanged, FP64 OpenBLAS, {sec:.1f} s"}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
 # SUMMIT-GxE workload (config-3 shape): N = 100,000 x M = 1,000,000, 8 exposures
 # (6 continuous N(0,1) with pairwise correlation 0.2, 2 categorical with 3 and 5
 # levels, level-coded and standardized), K = 1 bin, B = 100 Gaussian probes.
@@ -708,11 +791,13 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["windowed", "gxe"], default="windowed")
+    ap.add_argument("--workload", choices=["windowed", "gxe", "exact"], default="windowed")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.workload == "gxe":
+    if args.workload == "exact":
+        exact_arm(args)
+    elif args.workload == "gxe":
         if args.impl == "reference":
             sec, sample = gxe_reference_sample(GXE_N, env_int("LDS_GXE_CPU_SNPS", 400),
                                                cpu_threads())
