@@ -602,15 +602,27 @@ def exact_arm(args) -> None:
     buf = np.zeros(4)
     for _ in range(args.warmup):
         sess.window_ld(lo, hi, annot, corr_dim=n - 1)
-    times = []
+    times, gram = [], []
     launches0 = lib.lds_kernel_launches()
     with Clocks(env_int("LOCAL_RANK", 0)) as clk:
         for _ in range(args.steps):
             out = sess.window_ld(lo, hi, annot, corr_dim=n - 1)
             lib.lds_last_timings(buf.ctypes.data_as(__import__("ctypes").c_void_p), 4)
             times.append(float(buf[0]))
+            gram.append(float(buf[1]))
     launches = int(lib.lds_kernel_launches() - launches0) // max(args.steps, 1)
     ms = float(np.mean(times))
+    gram_ms = float(np.mean(gram))
+    pf = ROOT / "MEASURED_PEAKS.json"
+    peaks = json.loads(pf.read_text()) if pf.exists() else {}
+    peak = float(peaks.get("bf16_tflops", 1590.0))
+    # Tensor-core work the Gram kernel issues: 4 int8 planes (GG, GO, OG, OO)
+    # over every 128 x 128 tile pair of the band, 2 N_pad ops per product.
+    tiles = 0
+    for w in range(ws.size - 1):
+        t = -(-int(ws[w + 1] - ws[w]) // 128)
+        tiles += t * t
+    issued = 4.0 * 2.0 * 128 * 128 * (-(-n // 256) * 256) * tiles
     t0 = time.perf_counter()
     s2 = GwSession(bed, n)
     out2 = s2.window_ld(lo, hi, annot, corr_dim=n - 1)
@@ -627,6 +639,15 @@ def exact_arm(args) -> None:
             "e2e": {"value": round(ops / e2e_s / 1e12, 3), "unit": "TOPS",
                     "h2d_bytes_per_step": int(bed.nbytes + annot.nbytes + lo.nbytes + hi.nbytes),
                     "d2h_bytes_per_step": int(out.nbytes), "ms_per_step": round(e2e_s * 1e3, 1)},
+            "kernel_ms": {"gram_ld": round(gram_ms, 3), "total": round(ms, 3)},
+            "roofline": {"kernel": "gram_ld_kernel (int8 GG/GO/OG/OO tile products + LD epilogue)",
+                         "bound": "tensor", "achieved": round(ops / (gram_ms * 1e-3) / 1e12, 3),
+                         "peak": peak, "unit": "TFLOP/s",
+                         "frac": round(ops / (gram_ms * 1e-3) / 1e12 / peak, 4),
+                         "issued_int8_tops": round(issued / (gram_ms * 1e-3) / 1e12, 3),
+                         "peak_source": ("MEASURED_PEAKS.json bf16_tflops (burst)" if peaks
+                                         else "fallback"),
+                         "traffic": None, "algorithmic_ops_per_launch": ops},
             "gpu_launches": launches, "clocks": clk.summary()}
     if not os.environ.get("LDS_SKIP_CPU_BASELINE"):
         from oracle.oracle import ReferenceWindowed

@@ -2776,6 +2776,7 @@ void window_ld_impl(Context& c, const Prepared& P, int64_t row0, int64_t row1, c
                                         (uint64_t)P.g.nbp, 32, 128, CU_TENSOR_MAP_SWIZZLE_NONE);
     ck(cudaEventRecord(c.ev[0], c.st), "event");
     launch_gram_ld(tmC, ga, (int)items.size(), c.st);
+    ck(cudaEventRecord(c.ev[2], c.st), "event");
     launch_gram_reduce(dpart, db, row0, row1, (int)K, dout, K, 1, c.st);
     ck(cudaEventRecord(c.ev[1], c.st), "event");
     ck(cudaGetLastError(), "launch");
@@ -2788,6 +2789,8 @@ void window_ld_impl(Context& c, const Prepared& P, int64_t row0, int64_t row1, c
     float ms = 0.f;
     ck(cudaEventElapsedTime(&ms, c.ev[0], c.ev[1]), "elapsed");
     c.timings[0] = ms;
+    ck(cudaEventElapsedTime(&ms, c.ev[0], c.ev[2]), "elapsed");
+    c.timings[1] = ms;  // Gram kernel alone
     for (int64_t r = 0; r < m; ++r)
         for (int64_t b = 0; b < K; ++b) out[r * ld_row + b * ld_col] = h[(size_t)(r * K + b)];
 }
