@@ -526,7 +526,7 @@ def ours_arm(args) -> None:
             "data": "synthetic (seeded HWE/AR(1) generator on device)",
             "config": {"workload": WORKLOAD, "N": n, "M": m, "windows": int(len(ws) - 1),
                        "K": K_BINS, "B": B_PROBES, "block": BLOCK, "impute": "mean",
-                       "digits": lib.lds_get_slices(), "parallelism": f"replicas x{world}",
+                       "digits": lib.lds_get_slices(), "parallelism": f"partition x{world} (each rank its own chromosome; no collective)",
                        "graph": "one CUDA graph launch per estimate",
                        "l2": "inputs larger than L2 (6.3 GB genotype image per step)"},
             "kernel_ms": {k: round(v, 3) for k, v in kms.items()},

@@ -206,6 +206,41 @@ int lds_gw_plan_kernel_ms(int64_t plan, double* ms4);
 int lds_gw_plan_destroy(int64_t plan);
 
 /* ---------------------------------------------------------------------
+ * SNP shards across GPUs (one process per GPU).  Phase 1 is a sum over SNP
+ * blocks, so each rank holds a contiguous SNP shard as its own genotype
+ * image, computes the partial sketch of its SNPs, and the ranks sum the
+ * sketches (one all-reduce per V-tile); phase 2 is then independent per
+ * shard.  The caller owns the exchange (e.g. an NCCL all-reduce on the
+ * stream set with lds_set_stream).  No single reference counterpart: the
+ * reference runs the same sum over SNP blocks in one process
+ * (gw_ldscore.py:1934-2019 phase-1 loop, :2060-2160 phase-2 loop).
+ *   lds_gw_plan_create_shard: lds_gw_plan_create for a genotype image that
+ *     holds SNPs [snp_offset, snp_offset + M) of the fileset; snp_offset is
+ *     a multiple of step_size, so the shard's blocks and their probe streams
+ *     (keyed by the block's start in the fileset) are the unsharded ones.
+ *     Mean imputation only (HWE draws are keyed by the fileset SNP index).
+ *   lds_gw_plan_tiles: number of V-tiles, their probe counts (tile_sizes
+ *     may be NULL) and the sketch's row count N_pad (may be NULL).
+ *   lds_gw_plan_phase1: enqueue phase 1 of V-tile `tile` into the caller's
+ *     device buffer d_sketch (N_pad x K*V FP64, column-major, column k*V+v;
+ *     every element written).  Tile 0 also zeroes the plan's accumulators.
+ *   lds_gw_plan_phase2: enqueue phase 2 of V-tile `tile` from d_sketch (the
+ *     all-reduced sketch) into the plan's accumulators.
+ *   lds_gw_plan_set_bin_totals / lds_gw_plan_bin_totals: the per-bin
+ *     annotation totals M_k used by lds_gw_plan_results' finalize (default:
+ *     the shard's own; set them to the sum over shards).
+ * ------------------------------------------------------------------- */
+int lds_gw_plan_create_shard(int64_t geno, const double* annot, int64_t K, int nvecs,
+                             int step_size, int vtile, uint64_t seed, int rand_dist,
+                             double resvar_eps, int as_float, int with_mc, int64_t snp_offset,
+                             int64_t* plan_out);
+int lds_gw_plan_tiles(int64_t plan, int* n_tiles, int* tile_sizes, int64_t* sketch_rows);
+int lds_gw_plan_phase1(int64_t plan, int tile, double* d_sketch);
+int lds_gw_plan_phase2(int64_t plan, int tile, const double* d_sketch);
+int lds_gw_plan_set_bin_totals(int64_t plan, const double* Mk);
+int lds_gw_plan_bin_totals(int64_t plan, double* Mk);
+
+/* ---------------------------------------------------------------------
  * Windowed + partitioned LD scores (stochastic, probe based).  Windows are a
  * contiguous partition of the SNPs: window w = [window_starts[w],
  * window_starts[w+1]), window_starts[0] = 0, window_starts[n_windows] = M.

@@ -89,6 +89,13 @@ SIGNATURES: dict[str, tuple] = {
     "lds_gw_plan_results": (_int, [_i64, _p, _p, _p, _p, _p]),
     "lds_gw_plan_kernel_ms": (_int, [_i64, _p]),
     "lds_gw_plan_destroy": (_int, [_i64]),
+    "lds_gw_plan_create_shard": (_int, [_i64, _p, _i64, _int, _int, _int, _u64, _int, _dbl, _int,
+                                        _int, _i64, _p]),
+    "lds_gw_plan_tiles": (_int, [_i64, _p, _p, _p]),
+    "lds_gw_plan_phase1": (_int, [_i64, _int, _p]),
+    "lds_gw_plan_phase2": (_int, [_i64, _int, _p]),
+    "lds_gw_plan_set_bin_totals": (_int, [_i64, _p]),
+    "lds_gw_plan_bin_totals": (_int, [_i64, _p]),
 }
 for _t in ("f32", "f64"):
     SIGNATURES[f"lds_phase1_compute_Xz_bed_chunk_{_t}"] = (

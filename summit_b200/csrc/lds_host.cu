@@ -1044,6 +1044,7 @@ struct GwPlan {
     std::vector<std::vector<cudaEvent_t>> evsets;
     int pending = 0;
     double kernel_ms[4] = {0, 0, 0, 0};  // weights, phase 1, sketch digits, phase 2
+    int64_t snp_offset = 0;  // index of SNP 0 of this image in the whole fileset (SNP shards)
     ~GwPlan() {
         for (auto& s : evsets)
             for (cudaEvent_t e : s) cudaEventDestroy(e);
@@ -1065,9 +1066,12 @@ int64_t next_handle() {
 
 std::unique_ptr<GwPlan> plan_create(Context& c, std::shared_ptr<Prepared> P, const double* annot,
                                     int64_t K, int nvecs, int step, int vtile, uint64_t seed,
-                                    int dist, double eps, int as_float, int with_mc) {
+                                    int dist, double eps, int as_float, int with_mc,
+                                    int64_t snp_offset = 0) {
     const int64_t M = P->g.M, N = P->g.N;
     if (nvecs <= 0 || step <= 0 || K <= 0 || M <= 0) fail(LDS_ERR_ARG, "invalid sizes");
+    if (snp_offset < 0 || snp_offset % step != 0)
+        fail(LDS_ERR_ARG, "a SNP shard must start on a block boundary (a multiple of step_size)");
     if (K > 512) fail(LDS_ERR_ARG, "B too large for fixed seg buffers in phase2_accum_XtXz_bed");
     auto pl = std::make_unique<GwPlan>();
     pl->P = P;
@@ -1076,6 +1080,7 @@ std::unique_ptr<GwPlan> plan_create(Context& c, std::shared_ptr<Prepared> P, con
     pl->S = c.slices;
     pl->as_float = as_float;
     pl->with_mc = with_mc;
+    pl->snp_offset = snp_offset;
     {
         int width = std::min(nvecs, vtile > 0 ? vtile : nvecs);
         if (width >= 64) width = std::max(64, (width / 64) * 64);
@@ -1127,8 +1132,11 @@ std::unique_ptr<GwPlan> plan_create(Context& c, std::shared_ptr<Prepared> P, con
                     const int s = b * step;
                     const int L = (int)std::min<int64_t>(step, M - s);
                     std::vector<double> blk((size_t)L * V);
-                    if (as_float) make_probes<float>(seed, s, v0, L, V, dist, blk.data(), L);
-                    else make_probes<double>(seed, s, v0, L, V, dist, blk.data(), L);
+                    // Probe streams are keyed by the block's start in the whole
+                    // fileset (make_seed, gwldcore.cpp:452-458).
+                    const int gs = (int)(snp_offset + s);
+                    if (as_float) make_probes<float>(seed, gs, v0, L, V, dist, blk.data(), L);
+                    else make_probes<double>(seed, gs, v0, L, V, dist, blk.data(), L);
                     for (int cc = 0; cc < V; ++cc)
                         std::memcpy(&Z[(size_t)cc * M + s], &blk[(size_t)cc * L], sizeof(double) * L);
                 }
@@ -1189,12 +1197,138 @@ std::unique_ptr<GwPlan> plan_create(Context& c, std::shared_ptr<Prepared> P, con
     return pl;
 }
 
-void plan_execute(Context& c, GwPlan& pl) {
-    Prepared& P = *pl.P;
-    const int64_t M = P.g.M, K = pl.K;
+// Zero the plan's accumulators before the first V-tile of an estimate.
+void plan_zero(Context& c, GwPlan& pl) {
+    const int64_t M = pl.P->g.M, K = pl.K;
     ck(cudaMemsetAsync(pl.accum.p, 0, sizeof(double) * (size_t)(M * K), c.st), "memset");
     if (pl.with_mc) ck(cudaMemsetAsync(pl.mc.p, 0, sizeof(double) * (size_t)(M * K), c.st), "memset");
     ck(cudaMemsetAsync(pl.guards.p, 0, 16, c.st), "memset");
+}
+
+// Phase 1 of V-tile ti: the weights, then the sketch y (N_pad x K*V,
+// column-major, column k*V + v) over this image's SNPs.  ev (may be NULL)
+// receives one event after each kernel.
+void plan_enqueue_phase1(Context& c, GwPlan& pl, size_t ti, double* y, cudaEvent_t* ev, int& e) {
+    Prepared& P = *pl.P;
+    const int64_t M = P.g.M, K = pl.K;
+    GwPlan::Tile& t = *pl.tiles[ti];
+    P1Weights w;
+    w.K = (int)K;
+    w.V = t.V;
+    w.Vp = t.Vp;
+    w.S = pl.S;
+    w.rowind = static_cast<int32_t*>(t.rowind.p);
+    w.sc = static_cast<double*>(t.sc.p);
+    w.bin_off = static_cast<int64_t*>(t.binoff.p);
+    w.wq_off = static_cast<int64_t*>(t.wqoff.p);
+    w.wq = static_cast<int8_t*>(t.wq.p);
+    w.colscale = static_cast<double*>(t.wcs.p);
+    if (pl.umma) {
+        const int nc = umma::ncolp_for(t.V);
+        umma::P1UWeights uw;
+        uw.K = (int)K;
+        uw.V = t.V;
+        uw.ncolp = nc;
+        uw.lmax = t.lmax;
+        uw.rowind = w.rowind;
+        uw.sc = w.sc;
+        uw.bin_off = w.bin_off;
+        uw.wq = w.wq;
+        uw.colscale = w.colscale;
+        umma::launch_p1_weights4(uw, static_cast<double*>(P.d_mean.p),
+                                 static_cast<double*>(P.d_sdinv.p), static_cast<double*>(t.z.p), M,
+                                 c.st);
+        if (ev) ck(cudaEventRecord(ev[e++], c.st), "event");
+        umma::P1UArgs pa;
+        pa.K = (int)K;
+        pa.V = t.V;
+        pa.ncolp = nc;
+        pa.ngroups = (nc + 255) / 256;
+        pa.box_rows = std::min(256, nc);
+        pa.nbp = P.g.nbp;
+        pa.N_pad = P.g.N_pad;
+        pa.bin_off = w.bin_off;
+        pa.rowind = w.rowind;
+        pa.codes = P.g.codes;
+        pa.colscale = w.colscale;
+        pa.Y = y;
+        pa.status = static_cast<unsigned*>(pl.status.p);
+        umma::launch_p1_umma(t.tmW, pa, P.g.N_pad, c.st);
+    } else {
+        launch_p1_weights(w, static_cast<double*>(P.d_mean.p), static_cast<double*>(P.d_sdinv.p),
+                          static_cast<double*>(t.z.p), M, 0, c.st);
+        if (ev) ck(cudaEventRecord(ev[e++], c.st), "event");
+        launch_p1(P.g, w, nullptr, y, c.st);
+    }
+    if (ev) ck(cudaEventRecord(ev[e++], c.st), "event");
+}
+
+// Phase 2 of V-tile ti from the sketch y: its digits, then
+// accum += the guarded per-SNP updates over this image's SNPs.
+void plan_enqueue_phase2(Context& c, GwPlan& pl, size_t ti, const double* y, cudaEvent_t* ev,
+                         int& e) {
+    Prepared& P = *pl.P;
+    const int64_t M = P.g.M, K = pl.K;
+    GwPlan::Tile& t = *pl.tiles[ti];
+    if (pl.umma) {
+        const int nc = umma::ncolp_for(t.V);
+        umma::launch_quantize_y4(y, P.g.N, P.g.N_pad, (int)K, t.V, nc,
+                                 static_cast<int8_t*>(pl.yq.p), static_cast<double*>(pl.ycs.p),
+                                 c.st);
+        if (ev) ck(cudaEventRecord(ev[e++], c.st), "event");
+        umma::P2UArgs u;
+        u.K = (int)K;
+        u.V = t.V;
+        u.ncolp = nc;
+        u.bins_per_cta = umma::p2_bins_per_cta(nc, (int)K);
+        u.ngroups = (u.bins_per_cta * nc + 255) / 256;
+        u.box_rows = std::min(256, u.bins_per_cta * nc);
+        u.nkt = (int)(P.g.N_pad / 128);
+        u.M = M;
+        u.j0 = 0;
+        u.j1 = M;
+        u.out_row0 = 0;
+        u.colscale = static_cast<double*>(pl.ycs.p);
+        u.mean = static_cast<double*>(P.d_mean.p);
+        u.sdinv = static_cast<double*>(P.d_sdinv.p);
+        u.left_scale = static_cast<double*>(pl.lscale.p);
+        u.accum = static_cast<double*>(pl.accum.p);
+        u.mc = pl.with_mc ? static_cast<double*>(pl.mc.p) : nullptr;
+        u.guard_counts = static_cast<unsigned long long*>(pl.guards.p);
+        u.extreme_warn = extreme_warn_env();
+        u.drop_extreme = drop_extreme_env();
+        u.status = static_cast<unsigned*>(pl.status.p);
+        umma::launch_p2_umma(pl.tmA, pl.tmB[ti], u, c.st);
+        if (ev) ck(cudaEventRecord(ev[e++], c.st), "event");
+        return;
+    }
+    launch_quantize_y(y, P.g.N, P.g.N_pad, (int)K, t.V, t.Vp, pl.S, static_cast<int8_t*>(pl.yq.p),
+                      static_cast<double*>(pl.ycs.p), c.st);
+    if (ev) ck(cudaEventRecord(ev[e++], c.st), "event");
+    P2Args a;
+    a.K = (int)K;
+    a.V = t.V;
+    a.Vp = t.Vp;
+    a.S = pl.S;
+    a.j0 = 0;
+    a.j1 = M;
+    a.out_row0 = 0;
+    a.Yq = static_cast<int8_t*>(pl.yq.p);
+    a.colscale = static_cast<double*>(pl.ycs.p);
+    a.mean = static_cast<double*>(P.d_mean.p);
+    a.sdinv = static_cast<double*>(P.d_sdinv.p);
+    a.left_scale = static_cast<double*>(pl.lscale.p);
+    a.accum = static_cast<double*>(pl.accum.p);
+    a.mc = pl.with_mc ? static_cast<double*>(pl.mc.p) : nullptr;
+    a.guard_counts = static_cast<unsigned long long*>(pl.guards.p);
+    a.extreme_warn = extreme_warn_env();
+    a.drop_extreme = drop_extreme_env();
+    launch_p2(P.g, a, c.st);
+    if (ev) ck(cudaEventRecord(ev[e++], c.st), "event");
+}
+
+void plan_execute(Context& c, GwPlan& pl) {
+    plan_zero(c, pl);
     const bool tm = pl.pending < GwPlan::kMaxTimed;
     cudaEvent_t* ev = nullptr;
     if (tm) {
@@ -1207,113 +1341,10 @@ void plan_execute(Context& c, GwPlan& pl) {
     }
     int e = 0;
     if (tm) ck(cudaEventRecord(ev[e++], c.st), "event");
-    for (auto& tp : pl.tiles) {
-        GwPlan::Tile& t = *tp;
-        P1Weights w;
-        w.K = (int)K;
-        w.V = t.V;
-        w.Vp = t.Vp;
-        w.S = pl.S;
-        w.rowind = static_cast<int32_t*>(t.rowind.p);
-        w.sc = static_cast<double*>(t.sc.p);
-        w.bin_off = static_cast<int64_t*>(t.binoff.p);
-        w.wq_off = static_cast<int64_t*>(t.wqoff.p);
-        w.wq = static_cast<int8_t*>(t.wq.p);
-        w.colscale = static_cast<double*>(t.wcs.p);
-        if (pl.umma) {
-            const int nc = umma::ncolp_for(t.V);
-            umma::P1UWeights uw;
-            uw.K = (int)K;
-            uw.V = t.V;
-            uw.ncolp = nc;
-            uw.lmax = t.lmax;
-            uw.rowind = w.rowind;
-            uw.sc = w.sc;
-            uw.bin_off = w.bin_off;
-            uw.wq = w.wq;
-            uw.colscale = w.colscale;
-            umma::launch_p1_weights4(uw, static_cast<double*>(P.d_mean.p),
-                                     static_cast<double*>(P.d_sdinv.p), static_cast<double*>(t.z.p),
-                                     M, c.st);
-            if (tm) ck(cudaEventRecord(ev[e++], c.st), "event");
-            umma::P1UArgs pa;
-            pa.K = (int)K;
-            pa.V = t.V;
-            pa.ncolp = nc;
-            pa.ngroups = (nc + 255) / 256;
-            pa.box_rows = std::min(256, nc);
-            pa.nbp = P.g.nbp;
-            pa.N_pad = P.g.N_pad;
-            pa.bin_off = w.bin_off;
-            pa.rowind = w.rowind;
-            pa.codes = P.g.codes;
-            pa.colscale = w.colscale;
-            pa.Y = static_cast<double*>(pl.y.p);
-            pa.status = static_cast<unsigned*>(pl.status.p);
-            umma::launch_p1_umma(t.tmW, pa, P.g.N_pad, c.st);
-        } else {
-            launch_p1_weights(w, static_cast<double*>(P.d_mean.p),
-                              static_cast<double*>(P.d_sdinv.p), static_cast<double*>(t.z.p), M, 0,
-                              c.st);
-            if (tm) ck(cudaEventRecord(ev[e++], c.st), "event");
-            launch_p1(P.g, w, nullptr, static_cast<double*>(pl.y.p), c.st);
-        }
-        if (tm) ck(cudaEventRecord(ev[e++], c.st), "event");
-        if (pl.umma) {
-            const int nc = umma::ncolp_for(t.V);
-            umma::launch_quantize_y4(static_cast<double*>(pl.y.p), P.g.N, P.g.N_pad, (int)K, t.V, nc,
-                                     static_cast<int8_t*>(pl.yq.p), static_cast<double*>(pl.ycs.p),
-                                     c.st);
-            if (tm) ck(cudaEventRecord(ev[e++], c.st), "event");
-            umma::P2UArgs u;
-            u.K = (int)K;
-            u.V = t.V;
-            u.ncolp = nc;
-            u.bins_per_cta = umma::p2_bins_per_cta(nc, (int)K);
-            u.ngroups = (u.bins_per_cta * nc + 255) / 256;
-            u.box_rows = std::min(256, u.bins_per_cta * nc);
-            u.nkt = (int)(P.g.N_pad / 128);
-            u.M = M;
-            u.j0 = 0;
-            u.j1 = M;
-            u.out_row0 = 0;
-            u.colscale = static_cast<double*>(pl.ycs.p);
-            u.mean = static_cast<double*>(P.d_mean.p);
-            u.sdinv = static_cast<double*>(P.d_sdinv.p);
-            u.left_scale = static_cast<double*>(pl.lscale.p);
-            u.accum = static_cast<double*>(pl.accum.p);
-            u.mc = pl.with_mc ? static_cast<double*>(pl.mc.p) : nullptr;
-            u.guard_counts = static_cast<unsigned long long*>(pl.guards.p);
-            u.extreme_warn = extreme_warn_env();
-            u.drop_extreme = drop_extreme_env();
-            u.status = static_cast<unsigned*>(pl.status.p);
-            umma::launch_p2_umma(pl.tmA, pl.tmB[(size_t)(&tp - &pl.tiles[0])], u, c.st);
-            if (tm) ck(cudaEventRecord(ev[e++], c.st), "event");
-            continue;
-        }
-        launch_quantize_y(static_cast<double*>(pl.y.p), P.g.N, P.g.N_pad, (int)K, t.V, t.Vp, pl.S,
-                          static_cast<int8_t*>(pl.yq.p), static_cast<double*>(pl.ycs.p), c.st);
-        if (tm) ck(cudaEventRecord(ev[e++], c.st), "event");
-        P2Args a;
-        a.K = (int)K;
-        a.V = t.V;
-        a.Vp = t.Vp;
-        a.S = pl.S;
-        a.j0 = 0;
-        a.j1 = M;
-        a.out_row0 = 0;
-        a.Yq = static_cast<int8_t*>(pl.yq.p);
-        a.colscale = static_cast<double*>(pl.ycs.p);
-        a.mean = static_cast<double*>(P.d_mean.p);
-        a.sdinv = static_cast<double*>(P.d_sdinv.p);
-        a.left_scale = static_cast<double*>(pl.lscale.p);
-        a.accum = static_cast<double*>(pl.accum.p);
-        a.mc = pl.with_mc ? static_cast<double*>(pl.mc.p) : nullptr;
-        a.guard_counts = static_cast<unsigned long long*>(pl.guards.p);
-        a.extreme_warn = extreme_warn_env();
-        a.drop_extreme = drop_extreme_env();
-        launch_p2(P.g, a, c.st);
-        if (tm) ck(cudaEventRecord(ev[e++], c.st), "event");
+    double* y = static_cast<double*>(pl.y.p);
+    for (size_t ti = 0; ti < pl.tiles.size(); ++ti) {
+        plan_enqueue_phase1(c, pl, ti, y, ev, e);
+        plan_enqueue_phase2(c, pl, ti, y, ev, e);
     }
     if (tm) ++pl.pending;
     ck(cudaGetLastError(), "launch");
@@ -2944,6 +2975,84 @@ static GwPlan& plan_of(int64_t h) {
     auto it = plan_table().find(h);
     if (it == plan_table().end()) fail(LDS_ERR_ARG, "unknown plan handle");
     return *it->second;
+}
+
+LDS_API int lds_gw_plan_create_shard(int64_t geno, const double* annot, int64_t K, int nvecs,
+                                     int step_size, int vtile, uint64_t seed, int rand_dist,
+                                     double resvar_eps, int as_float, int with_mc,
+                                     int64_t snp_offset, int64_t* plan_out) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        ensure_device(c);
+        auto it = geno_table().find(geno);
+        if (it == geno_table().end()) fail(LDS_ERR_ARG, "unknown genotype handle");
+        if (snp_offset != 0 && it->second->impute == LDS_IMPUTE_HWE)
+            fail(LDS_ERR_ARG, "HWE imputation seeds by the SNP's index in the fileset; build SNP "
+                              "shards with impute_mode 'mean'");
+        auto pl = plan_create(c, it->second, annot, K, nvecs, step_size, vtile, seed, rand_dist,
+                              resvar_eps, as_float, with_mc, snp_offset);
+        const int64_t h = next_handle();
+        plan_table()[h] = std::move(pl);
+        *plan_out = h;
+    });
+}
+
+LDS_API int lds_gw_plan_tiles(int64_t plan, int* n_tiles, int* tile_sizes, int64_t* sketch_rows) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        GwPlan& pl = plan_of(plan);
+        if (n_tiles) *n_tiles = (int)pl.tiles.size();
+        if (tile_sizes)
+            for (size_t t = 0; t < pl.tiles.size(); ++t) tile_sizes[t] = pl.tiles[t]->V;
+        if (sketch_rows) *sketch_rows = pl.P->g.N_pad;
+    });
+}
+
+LDS_API int lds_gw_plan_phase1(int64_t plan, int tile, double* d_sketch) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        GwPlan& pl = plan_of(plan);
+        if (tile < 0 || tile >= (int)pl.tiles.size()) fail(LDS_ERR_ARG, "V-tile index out of range");
+        if (!d_sketch) fail(LDS_ERR_ARG, "sketch buffer is NULL");
+        if (tile == 0) plan_zero(c, pl);
+        int e = 0;
+        plan_enqueue_phase1(c, pl, (size_t)tile, d_sketch, nullptr, e);
+        ck(cudaGetLastError(), "launch");
+    });
+}
+
+LDS_API int lds_gw_plan_phase2(int64_t plan, int tile, const double* d_sketch) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        GwPlan& pl = plan_of(plan);
+        if (tile < 0 || tile >= (int)pl.tiles.size()) fail(LDS_ERR_ARG, "V-tile index out of range");
+        if (!d_sketch) fail(LDS_ERR_ARG, "sketch buffer is NULL");
+        int e = 0;
+        plan_enqueue_phase2(c, pl, (size_t)tile, d_sketch, nullptr, e);
+        ck(cudaGetLastError(), "launch");
+    });
+}
+
+LDS_API int lds_gw_plan_set_bin_totals(int64_t plan, const double* Mk) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        GwPlan& pl = plan_of(plan);
+        for (int64_t k = 0; k < pl.K; ++k) pl.Mk[(size_t)k] = Mk[k];
+    });
+}
+
+LDS_API int lds_gw_plan_bin_totals(int64_t plan, double* Mk) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        GwPlan& pl = plan_of(plan);
+        for (int64_t k = 0; k < pl.K; ++k) Mk[k] = pl.Mk[(size_t)k];
+    });
 }
 
 LDS_API int lds_gw_plan_execute(int64_t plan) {

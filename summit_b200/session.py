@@ -44,6 +44,37 @@ class GwPlan:
         check(_lib.load().lds_gw_plan_kernel_ms(self.handle, ptr(buf)))
         return {"weights": buf[0], "phase1": buf[1], "digits": buf[2], "phase2": buf[3]}
 
+    # -- the two halves of an estimate, for callers that exchange the sketch --
+    def tiles(self) -> tuple[list[int], int]:
+        """Probe counts of the V-tiles and the sketch's row count N_pad."""
+        n = C.c_int(0)
+        rows = C.c_int64(0)
+        lib = _lib.load()
+        check(lib.lds_gw_plan_tiles(self.handle, C.byref(n), None, C.byref(rows)))
+        sizes = np.zeros(max(n.value, 1), dtype=np.int32)
+        check(lib.lds_gw_plan_tiles(self.handle, None, ptr(sizes), None))
+        return [int(v) for v in sizes[:n.value]], int(rows.value)
+
+    def phase1(self, tile: int, sketch_ptr: int) -> None:
+        """Enqueue phase 1 of V-tile ``tile`` into the device buffer at
+        ``sketch_ptr`` (N_pad x K*V FP64, column-major)."""
+        check(_lib.load().lds_gw_plan_phase1(self.handle, int(tile), C.c_void_p(int(sketch_ptr))))
+
+    def phase2(self, tile: int, sketch_ptr: int) -> None:
+        """Enqueue phase 2 of V-tile ``tile`` from the (all-reduced) sketch."""
+        check(_lib.load().lds_gw_plan_phase2(self.handle, int(tile), C.c_void_p(int(sketch_ptr))))
+
+    def bin_totals(self) -> np.ndarray:
+        out = np.empty(self.K)
+        check(_lib.load().lds_gw_plan_bin_totals(self.handle, ptr(out)))
+        return out
+
+    def set_bin_totals(self, Mk) -> None:
+        Mk = np.ascontiguousarray(Mk, dtype=np.float64)
+        if Mk.shape != (self.K,):
+            raise ValueError("bin totals must have one value per annotation bin")
+        check(_lib.load().lds_gw_plan_set_bin_totals(self.handle, ptr(Mk)))
+
     def close(self) -> None:
         if self.handle:
             _lib.load().lds_gw_plan_destroy(self.handle)
@@ -81,6 +112,21 @@ class GwSession:
                                              int(step_size), int(vtile or 0), int(seed),
                                              _dist(rand_dist), float(eps), int(as_float),
                                              int(with_mc), C.byref(h)))
+        return GwPlan(self, h.value, self.M, annot.shape[1], with_mc)
+
+    def shard_plan(self, annot, nvecs: int, step_size: int, seed: int, snp_offset: int,
+                   rand_dist: str = "rademacher", vtile: int | None = None, eps: float = 1e-10,
+                   as_float: bool = False, with_mc: bool = False) -> GwPlan:
+        """``plan`` for an image that holds SNPs [snp_offset, snp_offset + M) of
+        the fileset (one SNP shard); snp_offset is a multiple of step_size."""
+        annot = np.ascontiguousarray(annot, dtype=np.float64)
+        if annot.shape[0] != self.M:
+            raise ValueError("annot must have one row per SNP")
+        h = C.c_int64(0)
+        check(_lib.load().lds_gw_plan_create_shard(
+            self.handle, ptr(annot), annot.shape[1], int(nvecs), int(step_size), int(vtile or 0),
+            int(seed), _dist(rand_dist), float(eps), int(as_float), int(with_mc),
+            int(snp_offset), C.byref(h)))
         return GwPlan(self, h.value, self.M, annot.shape[1], with_mc)
 
     def stats(self) -> dict:

@@ -1,0 +1,166 @@
+"""SNP-sharded genome-wide LD scores: one process per GPU, one SNP shard each.
+
+The reference runs the estimator in one process: phase 1 sums the sketch
+Xz = sum over SNP blocks of X_blk W_blk (gw_ldscore.py:1934-2019, kernel
+gwldcore.cpp:1582-1894), then phase 2 scores every SNP against the finished
+sketch (gw_ldscore.py:2060-2160, kernel gwldcore.cpp:2329-2600).  Phase 1 is a
+sum over blocks, so the SNPs split into contiguous shards on block boundaries:
+rank r holds only its shard's genotype image, computes the partial sketch of
+its SNPs, the ranks sum the partial sketches (one all-reduce per V-tile), and
+phase 2 then runs independently per shard.  Each block keeps its probe stream
+(keyed by the block's start in the fileset), so the sharded estimate is the
+unsharded one up to the order of the final FP64 sums.  The annotation totals
+M_k of the finalize and the Monte-Carlo aggregate sums are all-reduced too.
+
+``ShardedGw.run`` is the driver; the shard's work comes from an engine:
+``DeviceShard`` runs it on liblds's kernels (sketch buffers in device memory,
+the library on torch's current stream so the NCCL all-reduce orders after
+phase 1 and before phase 2).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+
+def shard_bounds(M: int, world: int, step: int) -> list[tuple[int, int]]:
+    """Contiguous SNP shards [start, stop) for `world` ranks, on multiples of
+    `step` (the SNP-block size), with block counts differing by at most one."""
+    if M < 0 or world <= 0 or step <= 0:
+        raise ValueError("shard_bounds needs M >= 0, world > 0 and step > 0")
+    nblk = -(-M // step)
+    out = []
+    for r in range(world):
+        b0, b1 = r * nblk // world, (r + 1) * nblk // world
+        out.append((min(M, b0 * step), min(M, b1 * step)))
+    return out
+
+
+class DeviceShard:
+    """One rank's SNP shard on liblds: a resident genotype image of the shard's
+    BED rows and a shard plan (probe streams keyed by the fileset position)."""
+
+    def __init__(self, bed_rows: np.ndarray, n_total: int, snp_offset: int, annot, nvecs: int,
+                 step_size: int, seed: int, rand_dist: str = "rademacher",
+                 vtile: int | None = None, eps: float = 1e-10, as_float: bool = False,
+                 with_mc: bool = False, ddof: int = 1, row_sel=None):
+        import torch
+
+        from .session import GwSession, set_stream
+
+        self.torch = torch
+        self.device = torch.device("cuda", torch.cuda.current_device())
+        set_stream(torch.cuda.current_stream().cuda_stream)
+        self.session = GwSession(bed_rows, n_total, "mean", 0, ddof, row_sel)
+        self.plan = self.session.shard_plan(annot, nvecs, step_size, seed, snp_offset, rand_dist,
+                                            vtile, eps, as_float, with_mc)
+        self.K = self.plan.K
+        self.M = self.session.M
+        self.N = self.session.N
+        self.ddof = ddof
+        self._sizes, self._rows = self.plan.tiles()
+
+    def tile_sizes(self) -> list[int]:
+        return list(self._sizes)
+
+    def new_sketch(self, tile: int):
+        # N_pad x K*V column-major == a contiguous (K*V, N_pad) tensor
+        return self.torch.empty((self.K * self._sizes[tile], self._rows), dtype=self.torch.float64,
+                                device=self.device)
+
+    def phase1(self, tile: int, sketch) -> None:
+        self.plan.phase1(tile, sketch.data_ptr())
+
+    def phase2(self, tile: int, sketch) -> None:
+        self.plan.phase2(tile, sketch.data_ptr())
+
+    def bin_totals(self) -> np.ndarray:
+        return self.plan.bin_totals()
+
+    def set_bin_totals(self, Mk) -> None:
+        self.plan.set_bin_totals(Mk)
+
+    def results(self) -> dict:
+        return self.plan.results()
+
+    def close(self) -> None:
+        from .session import set_stream
+
+        self.plan.close()
+        self.session.close()
+        set_stream(None)
+
+
+@dataclass
+class ShardedResult:
+    bounds: list          # (start, stop) of every rank's shard
+    local: dict           # this rank's rows: ldscore, meansq_accum, inv, mc_per_snp_sumsq
+    ldscore: np.ndarray | None          # all SNPs (M x K), when gathered
+    mc_aggregate_sumsq: np.ndarray | None
+
+
+class ShardedGw:
+    """Driver of the sharded estimate.  `group` is a torch.distributed process
+    group (None: the default group; a run without torch.distributed is one
+    shard)."""
+
+    def __init__(self, engine, bounds: list[tuple[int, int]], group=None):
+        self.engine = engine
+        self.bounds = [tuple(map(int, b)) for b in bounds]
+        self.group = group
+
+    def _dist(self):
+        import torch.distributed as dist
+
+        if dist.is_available() and dist.is_initialized():
+            return dist
+        return None
+
+    def _allreduce_np(self, x: np.ndarray) -> np.ndarray:
+        dist = self._dist()
+        if dist is None:
+            return x
+        import torch
+
+        t = torch.from_numpy(np.ascontiguousarray(x, dtype=np.float64)).to(self.engine.device)
+        dist.all_reduce(t, group=self.group)
+        return t.cpu().numpy()
+
+    def run(self, gather: bool = True) -> ShardedResult:
+        dist = self._dist()
+        world = 1 if dist is None else dist.get_world_size(self.group)
+        rank = 0 if dist is None else dist.get_rank(self.group)
+        if len(self.bounds) != world:
+            raise ValueError(f"{len(self.bounds)} shard bounds for {world} ranks")
+        b0, b1 = self.bounds[rank]
+        if b1 - b0 != self.engine.M:
+            raise ValueError(f"rank {rank} holds {self.engine.M} SNPs, its shard is [{b0}, {b1})")
+        eng = self.engine
+        # every rank takes the same collective steps in the same order
+        eng.set_bin_totals(self._allreduce_np(eng.bin_totals()))
+        for t in range(len(eng.tile_sizes())):
+            y = eng.new_sketch(t)
+            eng.phase1(t, y)
+            if dist is not None and world > 1:
+                dist.all_reduce(y, group=self.group)
+            eng.phase2(t, y)
+        loc = eng.results()
+        mca = loc.get("mc_aggregate_sumsq")
+        if mca is not None:
+            mca = self._allreduce_np(mca)
+        ld = None
+        if gather:
+            ld = loc["ldscore"]
+            if dist is not None and world > 1:
+                import torch
+
+                mmax = max(e - s for s, e in self.bounds)
+                K = ld.shape[1]
+                buf = torch.zeros((mmax, K), dtype=torch.float64, device=eng.device)
+                buf[: ld.shape[0]] = torch.from_numpy(ld).to(eng.device)
+                parts = [torch.empty_like(buf) for _ in range(world)]
+                dist.all_gather(parts, buf, group=self.group)
+                ld = np.concatenate([parts[r][: e - s].cpu().numpy()
+                                     for r, (s, e) in enumerate(self.bounds)])
+        return ShardedResult(self.bounds, loc, ld, mca)
