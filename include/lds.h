@@ -82,7 +82,9 @@ void lds_clear_device_cache(void);
  * column-major) and optional resvar_gram (p x p row-major), inv_out[j] =
  * 1/sqrt(max(eps, (||x_j||^2 + q - 2h)/(N - p - 1))) with h = ||R x_j||^2 and
  * q = (R x_j)^T gram (R x_j) (or h) (compute_inv_resvar_from_geno_block,
- * :3220-3333).  The caller projects Xz2d afterwards (project_*).
+ * :3220-3333).  project_right != 0 with C and R projects the block's
+ * genotypes, X <- (I - C R) X, before the products (:1633-1650; an error
+ * together with inv_out, as in the reference).
  * ------------------------------------------------------------------- */
 int lds_phase1_compute_Xz_bed_chunk_f32(
     const char* bed_prefix, const char* fam_path, int blk_start, int blk_end,
@@ -91,7 +93,7 @@ int lds_phase1_compute_Xz_bed_chunk_f32(
     int kmax_hint, int rand_dist, int has_seed, uint64_t seed, float* Xz2d_chunk,
     int64_t xz_rows, int64_t xz_cols, uint8_t* bin_init_mask, int impute_mode,
     int has_impute_seed, uint64_t impute_seed, float* inv_out, double resvar_eps,
-    const float* C, const float* R, int64_t p, const float* resvar_gram);
+    const float* C, const float* R, int64_t p, const float* resvar_gram, int project_right);
 int lds_phase1_compute_Xz_bed_chunk_f64(
     const char* bed_prefix, const char* fam_path, int blk_start, int blk_end,
     const int64_t* row_sel, int64_t n_row_sel, int ddof, const double* annot_blk,
@@ -99,7 +101,7 @@ int lds_phase1_compute_Xz_bed_chunk_f64(
     int kmax_hint, int rand_dist, int has_seed, uint64_t seed, double* Xz2d_chunk,
     int64_t xz_rows, int64_t xz_cols, uint8_t* bin_init_mask, int impute_mode,
     int has_impute_seed, uint64_t impute_seed, double* inv_out, double resvar_eps,
-    const double* C, const double* R, int64_t p, const double* resvar_gram);
+    const double* C, const double* R, int64_t p, const double* resvar_gram, int project_right);
 
 /* ---------------------------------------------------------------------
  * Phase 2: Work = X_blk^T Xz2d; meansq_accum[blk_start+j, k] +=
@@ -109,21 +111,24 @@ int lds_phase1_compute_Xz_bed_chunk_f64(
  * (gwldcore.cpp:3759-3770, implementation :2329-2600).  Xz2d is N x Q
  * column-major with Q = K*tile_nvecs; meansq_accum is M x K row-major;
  * mc_aggregate_sumsq (K doubles) and mc_per_snp_sumsq (M x K doubles) may be
- * NULL.
+ * NULL.  With C and R (p > 0) the products use the projected genotypes,
+ * Work = ((I - C R) X)^T Xz2d (:2376-2390).
  * ------------------------------------------------------------------- */
 int lds_phase2_accum_XtXz_bed_f32(
     const char* bed_prefix, const char* fam_path, int blk_start, int blk_end,
     const int64_t* row_sel, int64_t n_row_sel, int ddof, const float* inv_left, int64_t L,
     int tile_nvecs, const float* Xz2d, int64_t xz_rows, int64_t xz_cols, float* meansq_accum,
     int64_t M_rows, int64_t K, int N_denom, int impute_mode, int has_impute_seed,
-    uint64_t impute_seed, double* mc_aggregate_sumsq, double* mc_per_snp_sumsq);
+    uint64_t impute_seed, double* mc_aggregate_sumsq, double* mc_per_snp_sumsq, const float* C,
+    const float* R, int64_t p);
 int lds_phase2_accum_XtXz_bed_f64(
     const char* bed_prefix, const char* fam_path, int blk_start, int blk_end,
     const int64_t* row_sel, int64_t n_row_sel, int ddof, const double* inv_left, int64_t L,
     int tile_nvecs, const double* Xz2d, int64_t xz_rows, int64_t xz_cols,
     double* meansq_accum, int64_t M_rows, int64_t K, int N_denom, int impute_mode,
     int has_impute_seed, uint64_t impute_seed, double* mc_aggregate_sumsq,
-    double* mc_per_snp_sumsq);
+    double* mc_per_snp_sumsq, const double* C,
+    const double* R, int64_t p);
 
 /* ---------------------------------------------------------------------
  * Residual variances: inv[j] = 1/sqrt(max(eps, ||x_j||^2 / (N-1))) for all
@@ -131,18 +136,24 @@ int lds_phase2_accum_XtXz_bed_f64(
  * inv[j] = 1/sqrt(max(eps, ||(I - C R) x_j||^2 / (N - p - 1))); snp_var_out
  * (may be NULL) receives min(1, ||(I - C R) x_j||^2 / ||x_j||^2).  Replaces
  * gwldcore.precompute_residual_variances_bed (gwldcore.cpp:3748-3757,
- * implementation :3335-3566) for compute_mu22 = False.
+ * implementation :3335-3566).  compute_mu22 != 0 also writes mu22_out
+ * (B x B row-major): with S = sum_j (x'_j o x'_j) annot_all[j, k] inv_j^2
+ * (x' the projected standardized genotypes; annot_all nsnps x B row-major),
+ * mu22[a][b] = (S^T S)[a][b] / (N Msum_a Msum_b), 0 where the denominator is
+ * 0 or the value not finite (:3421-3563).
  * ------------------------------------------------------------------- */
 int lds_precompute_residual_variances_bed_f32(
     const char* bed_prefix, const char* fam_path, int nsnps, int step_size,
     const int64_t* row_sel, int64_t n_row_sel, int ddof, double eps, int impute_mode,
     int has_impute_seed, uint64_t impute_seed, float* inv_out, const float* C, const float* R,
-    int64_t p, double* snp_var_out);
+    int64_t p, double* snp_var_out, int compute_mu22, const float* annot_all,
+    int64_t annot_rows, int64_t B, double* mu22_out);
 int lds_precompute_residual_variances_bed_f64(
     const char* bed_prefix, const char* fam_path, int nsnps, int step_size,
     const int64_t* row_sel, int64_t n_row_sel, int ddof, double eps, int impute_mode,
     int has_impute_seed, uint64_t impute_seed, double* inv_out, const double* C,
-    const double* R, int64_t p, double* snp_var_out);
+    const double* R, int64_t p, double* snp_var_out, int compute_mu22, const double* annot_all,
+    int64_t annot_rows, int64_t B, double* mu22_out);
 
 /* ---------------------------------------------------------------------
  * Whole genome-wide LD-score estimate in one call (all V-tiles, all SNP
@@ -223,7 +234,8 @@ int lds_gw_plan_destroy(int64_t plan);
  *     may be NULL) and the sketch's row count N_pad (may be NULL).
  *   lds_gw_plan_phase1: enqueue phase 1 of V-tile `tile` into the caller's
  *     device buffer d_sketch (N_pad x K*V FP64, column-major, column k*V+v;
- *     every element written).  Tile 0 also zeroes the plan's accumulators.
+ *     every element written; rows >= N are finite and ignored by phase 2).
+ *     Tile 0 also zeroes the plan's accumulators.
  *   lds_gw_plan_phase2: enqueue phase 2 of V-tile `tile` from d_sketch (the
  *     all-reduced sketch) into the plan's accumulators.
  *   lds_gw_plan_set_bin_totals / lds_gw_plan_bin_totals: the per-bin
@@ -381,7 +393,7 @@ int lds_phase1_compute_Xz_bed_chunk_rowmajor_f64(LDS_P1R_ARGS(double));
         const int64_t *row_sel, int64_t n_row_sel, int ddof, const T *inv_left, int64_t L,    \
         int tile_nvecs, const T *Xz2d, int64_t xz_rows, int64_t xz_cols, T *meansq_accum,     \
         int64_t M_rows, int64_t K, int N_denom, int has_impute_seed, uint64_t impute_seed,    \
-        double *mc_aggregate_sumsq, double *mc_per_snp_sumsq
+        double *mc_aggregate_sumsq, double *mc_per_snp_sumsq, const T *C, const T *R, int64_t p
 int lds_phase2_accum_XtXz_bed_mailman_f32(LDS_P2M_ARGS(float));
 int lds_phase2_accum_XtXz_bed_mailman_f64(LDS_P2M_ARGS(double));
 #define LDS_P2MR_ARGS(T)                                                                      \
@@ -408,6 +420,80 @@ int lds_standardize_dosage_inplace_f32(float* G, int64_t N, int64_t L, int ddof,
                                        double missing_value, int64_t* missing_out);
 int lds_standardize_dosage_inplace_f64(double* G, int64_t N, int64_t L, int ddof,
                                        double missing_value, int64_t* missing_out);
+
+/* ---------------------------------------------------------------------
+ * Dense genotype blocks (PGEN dosages and other callers that standardize
+ * themselves): geno is N x L column-major, already standardized.
+ * lds_phase1_compute_Xz_geno_chunk_* replaces phase1_compute_Xz_geno_chunk
+ * (gwldcore.cpp:3690-3701, impl :1896-1923): the phase-1 update of the BED
+ * form with the block's SNPs blk_start.. (probe streams keyed by blk_start),
+ * inv_out / C / R / resvar_gram as there (no project_right).
+ * lds_phase2_accum_XtXz_geno_* replaces phase2_accum_XtXz_geno
+ * (:3772-3783, impl :2624-2649); with C and R the block is projected in
+ * place, geno <- (I - C R) geno, as the reference does to the caller's array.
+ * The FP64 products run on the device (dense, no digit split).
+ * ------------------------------------------------------------------- */
+#define LDS_P1G_ARGS(T)                                                                       \
+    const T *geno, int64_t N, int64_t L, int blk_start, const T *annot_blk, int64_t annot_rows, \
+        int64_t K, const T *inv_right, int v_start, int v_count, int kmax_hint, int rand_dist, \
+        int has_seed, uint64_t seed, T *Xz2d_chunk, int64_t xz_rows, int64_t xz_cols,           \
+        uint8_t *bin_init_mask, const T *C, const T *R, int64_t p, const T *resvar_gram,        \
+        T *inv_out, double resvar_eps
+int lds_phase1_compute_Xz_geno_chunk_f32(LDS_P1G_ARGS(float));
+int lds_phase1_compute_Xz_geno_chunk_f64(LDS_P1G_ARGS(double));
+#define LDS_P2G_ARGS(T)                                                                       \
+    T *geno, int64_t N, int64_t L, int blk_start, const T *inv_left, int64_t L_in,             \
+        int tile_nvecs, const T *Xz2d, int64_t xz_rows, int64_t xz_cols, T *meansq_accum,      \
+        int64_t M_rows, int64_t K, const T *C, const T *R, int64_t p, int N_denom,             \
+        double *mc_aggregate_sumsq, double *mc_per_snp_sumsq
+int lds_phase2_accum_XtXz_geno_f32(LDS_P2G_ARGS(float));
+int lds_phase2_accum_XtXz_geno_f64(LDS_P2G_ARGS(double));
+
+/* Legacy direct phase 2, replaces phase2_compute_XtXz_bed (gwldcore.cpp:
+ * 3731-3740, impl :2132-2327): meansq += max(0, sum_c Work^2 inv^2 /
+ * (nvecs (N_denom - 1)^2)) with the guards, Xz2d N x K*nvecs. */
+#define LDS_P2L_ARGS(T)                                                                       \
+    const char *bed_prefix, const char *fam_path, int blk_start, int blk_end,                 \
+        const int64_t *row_sel, int64_t n_row_sel, int ddof, const T *inv_left, int64_t L,    \
+        int nvecs, const T *Xz2d, int64_t xz_rows, int64_t xz_cols, T *meansq, int64_t M_rows, \
+        int64_t K, const T *C, const T *R, int64_t p, int N_denom, int impute_mode,           \
+        int has_impute_seed, uint64_t impute_seed
+int lds_phase2_compute_XtXz_bed_f32(LDS_P2L_ARGS(float));
+int lds_phase2_compute_XtXz_bed_f64(LDS_P2L_ARGS(double));
+
+/* GRM panel products, replaces apply_grm_bed_panel / _mailman
+ * (gwldcore.cpp:3812-3828, impl :1134-1497): panel_out = P X D X^T P panel_in
+ * over SNPs [0, nsnps), D = diag(inv_all_j^2 / nsnps) (0 where not finite or
+ * <= 0), P = I - C R when C and R are given; panels N x Q column-major.  The
+ * Mailman form uses HWE-completed genotypes (impute_seed).  X^T V runs on the
+ * tensor-core phase-2 kernel's exact raw-product mode, X (D coef) on the
+ * phase-1 kernel. */
+#define LDS_GRM_ARGS(T)                                                                       \
+    const char *bed_prefix, const char *fam_path, int nsnps, int step_size,                   \
+        const int64_t *row_sel, int64_t n_row_sel, int ddof, const T *inv_all, int64_t n_inv, \
+        const T *panel_in, T *panel_out, int64_t rows, int64_t Q, const T *C, const T *R,     \
+        int64_t p, int impute_mode, int has_impute_seed, uint64_t impute_seed
+int lds_apply_grm_bed_panel_f32(LDS_GRM_ARGS(float));
+int lds_apply_grm_bed_panel_f64(LDS_GRM_ARGS(double));
+#define LDS_GRMM_ARGS(T)                                                                      \
+    const char *bed_prefix, const char *fam_path, int nsnps, int step_size,                   \
+        const int64_t *row_sel, int64_t n_row_sel, int ddof, const T *inv_all, int64_t n_inv, \
+        const T *panel_in, T *panel_out, int64_t rows, int64_t Q, const T *C, const T *R,     \
+        int64_t p, int has_impute_seed, uint64_t impute_seed
+int lds_apply_grm_bed_panel_mailman_f32(LDS_GRMM_ARGS(float));
+int lds_apply_grm_bed_panel_mailman_f64(LDS_GRMM_ARGS(double));
+
+/* Block corrections of binary annotations, replaces
+ * compute_block_corrections_binary (gwldcore.cpp:3807-3810, impl :3569-3627):
+ * M_a = #{i: annot_ia != 0}, S_ab = sum_{i: annot_ia != 0} meansq_raw[i, b],
+ * R2 = S / (M_a M_b), rho2 = (d^2 R2 - N mu22) / (N (N - 1)),
+ * bias = S - M_a M_b rho2, delta = mu22 - (1 + 2 rho2) (0 where M_a, M_b or
+ * S is 0); outputs B x B row-major.  annot_all is float32 or float64. */
+#define LDS_BCB_ARGS(T)                                                                       \
+    const double *meansq_raw, int64_t M, int64_t B, const double *mu22, const T *annot_all,   \
+        int N, double d, double *R2, double *rho2, double *bias, double *delta
+int lds_compute_block_corrections_binary_f32(LDS_BCB_ARGS(float));
+int lds_compute_block_corrections_binary_f64(LDS_BCB_ARGS(double));
 
 /* ---------------------------------------------------------------------
  * Exact windowed LD scores (tcgen05 int8 Gram products, FP64 epilogue).

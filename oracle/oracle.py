@@ -299,6 +299,27 @@ class Reference:
             getattr(L, f"ref_phase2_mailman_rowmajor_{t}").argtypes = [
                 _str, _str, _int, _int, _p, _i64, _int, _p, _i64, _int, _p, _i64, _i64, _p, _i64,
                 _p, _int, _int, _u64, _p, _p]
+            getattr(L, f"ref_phase1_geno_cov_{t}").argtypes = [
+                _p, _i64, _i64, _int, _p, _i64, _p, _int, _int, _str, _u64, _p, _p, _p, _p, _i64,
+                _p, _p]
+            getattr(L, f"ref_phase2_geno_cov_{t}").argtypes = [
+                _p, _i64, _i64, _int, _p, _int, _p, _i64, _p, _i64, _p, _p, _i64, _int, _p, _p]
+            getattr(L, f"ref_phase2_bed_cov_{t}").argtypes = [
+                _str, _str, _int, _int, _p, _i64, _int, _p, _i64, _int, _p, _i64, _i64, _p, _i64,
+                _int, _str, _p, _p, _i64, _int, _p, _p]
+            getattr(L, f"ref_phase1_bed_projright_{t}").argtypes = [
+                _str, _str, _int, _int, _int, _p, _i64, _i64, _p, _int, _int, _str, _u64, _p, _i64,
+                _p, _str, _p, _p, _i64]
+            getattr(L, f"ref_phase2_legacy_{t}").argtypes = [
+                _str, _str, _int, _int, _int, _p, _i64, _int, _p, _i64, _i64, _p, _i64, _int, _str,
+                _p, _p, _i64]
+            getattr(L, f"ref_apply_grm_{t}").argtypes = [
+                _str, _str, _int, _int, _int, _p, _p, _p, _i64, _i64, _p, _p, _i64, _str, _int,
+                _u64, _int]
+            getattr(L, f"ref_resvar_mu22_{t}").argtypes = [
+                _str, _str, _int, _int, _int, _str, _p, _i64, _p, _p, _i64, _i64, _p, _p]
+            getattr(L, f"ref_block_corrections_{t}").argtypes = [
+                _p, _i64, _i64, _p, _p, _int, _dbl, _p]
         L.ref_set_num_threads.argtypes = [_int]
         L.ref_set_omp_threads.argtypes = [_int]
         L.ref_set_blas_threads.argtypes = [_int]
@@ -436,6 +457,107 @@ class Reference:
             _ptr(Xz), Xz.shape[0], impute_mode.encode(), _ptr(Cf), _ptr(Rf), Cf.shape[1],
             _ptr(G), _ptr(inv)))
         return inv
+
+    # -- dense blocks, covariates inside the phases, GRM, mu22, corrections --
+    @staticmethod
+    def _cr(C, R, dt):
+        if C is None or R is None:
+            return None, None, 0
+        Cf = np.asfortranarray(C, dtype=dt)
+        return Cf, np.asfortranarray(R, dtype=dt), Cf.shape[1]
+
+    def phase1_geno_cov(self, geno, blk_start, annot, inv_right, v_start, v_count, seed, Xz,
+                        bin_init=None, C=None, R=None, gram=None, inv_out=None,
+                        rand_dist="rademacher"):
+        dt = Xz.dtype
+        ann = np.ascontiguousarray(annot, dtype=dt)
+        Cf, Rf, p = self._cr(C, R, dt)
+        G = None if gram is None else np.ascontiguousarray(gram, dtype=dt)
+        inv = None if inv_right is None else np.ascontiguousarray(inv_right, dtype=dt)
+        self._chk(getattr(self.lib, f"ref_phase1_geno_cov_{self._t(dt)}")(
+            _ptr(geno), geno.shape[0], geno.shape[1], blk_start, _ptr(ann), ann.shape[1],
+            _ptr(inv), v_start, v_count, rand_dist.encode(), seed, _ptr(Xz), _ptr(bin_init),
+            _ptr(Cf), _ptr(Rf), p, _ptr(G), _ptr(inv_out)))
+
+    def phase2_geno_cov(self, geno, blk_start, inv_left, tile_nvecs, Xz, meansq, N_denom,
+                        C=None, R=None, mc_agg=None, mc_per_snp=None):
+        dt = meansq.dtype
+        Cf, Rf, p = self._cr(C, R, dt)
+        inv = np.ascontiguousarray(inv_left, dtype=dt)
+        self._chk(getattr(self.lib, f"ref_phase2_geno_cov_{self._t(dt)}")(
+            _ptr(geno), geno.shape[0], geno.shape[1], blk_start, _ptr(inv), tile_nvecs, _ptr(Xz),
+            Xz.shape[1], _ptr(meansq), meansq.shape[0], _ptr(Cf), _ptr(Rf), p, N_denom,
+            _ptr(mc_agg), _ptr(mc_per_snp)))
+
+    def phase2_bed_cov(self, prefix, blk_start, blk_end, inv_left, tile_nvecs, Xz, meansq,
+                       N_denom, C, R, mailman=False, impute_mode="mean", ddof=1, mc_agg=None,
+                       mc_per_snp=None):
+        dt = meansq.dtype
+        Cf, Rf, p = self._cr(C, R, dt)
+        inv = np.ascontiguousarray(inv_left, dtype=dt)
+        self._chk(getattr(self.lib, f"ref_phase2_bed_cov_{self._t(dt)}")(
+            str(prefix).encode(), f"{prefix}.fam".encode(), blk_start, blk_end, None, 0, ddof,
+            _ptr(inv), inv.size, tile_nvecs, _ptr(Xz), Xz.shape[0], Xz.shape[1], _ptr(meansq),
+            meansq.shape[0], N_denom, impute_mode.encode(), _ptr(Cf), _ptr(Rf), p, int(mailman),
+            _ptr(mc_agg), _ptr(mc_per_snp)))
+
+    def phase1_bed_projright(self, prefix, blk_start, blk_end, annot, inv_right, v_start,
+                             v_count, seed, Xz, C, R, bin_init=None, impute_mode="mean", ddof=1):
+        dt = Xz.dtype
+        ann = np.ascontiguousarray(annot, dtype=dt)
+        inv = np.ascontiguousarray(inv_right, dtype=dt)
+        Cf, Rf, p = self._cr(C, R, dt)
+        self._chk(getattr(self.lib, f"ref_phase1_bed_projright_{self._t(dt)}")(
+            str(prefix).encode(), f"{prefix}.fam".encode(), blk_start, blk_end, ddof, _ptr(ann),
+            ann.shape[0], ann.shape[1], _ptr(inv), v_start, v_count, b"rademacher", seed,
+            _ptr(Xz), Xz.shape[0], _ptr(bin_init), impute_mode.encode(), _ptr(Cf), _ptr(Rf), p))
+
+    def phase2_legacy(self, prefix, blk_start, blk_end, inv_left, nvecs, Xz, meansq, N_denom,
+                      C=None, R=None, impute_mode="mean", ddof=1):
+        dt = meansq.dtype
+        Cf, Rf, p = self._cr(C, R, dt)
+        inv = np.ascontiguousarray(inv_left, dtype=dt)
+        self._chk(getattr(self.lib, f"ref_phase2_legacy_{self._t(dt)}")(
+            str(prefix).encode(), f"{prefix}.fam".encode(), blk_start, blk_end, ddof, _ptr(inv),
+            inv.size, nvecs, _ptr(Xz), Xz.shape[0], Xz.shape[1], _ptr(meansq), meansq.shape[0],
+            N_denom, impute_mode.encode(), _ptr(Cf), _ptr(Rf), p))
+
+    def apply_grm(self, prefix, nsnps, step, inv_all, panel_in, C=None, R=None,
+                  impute_mode="mean", impute_seed=None, mailman=False, ddof=1):
+        dt = panel_in.dtype
+        Cf, Rf, p = self._cr(C, R, dt)
+        pin = np.asfortranarray(panel_in)
+        out = np.zeros(pin.shape, dtype=dt, order="F")
+        inv = np.ascontiguousarray(inv_all, dtype=dt)
+        self._chk(getattr(self.lib, f"ref_apply_grm_{self._t(dt)}")(
+            str(prefix).encode(), f"{prefix}.fam".encode(), nsnps, step, ddof, _ptr(inv),
+            _ptr(pin), _ptr(out), pin.shape[0], pin.shape[1], _ptr(Cf), _ptr(Rf), p,
+            impute_mode.encode(), int(impute_seed is not None),
+            0 if impute_seed is None else impute_seed, int(mailman)))
+        return out
+
+    def resvar_mu22(self, prefix, nsnps, step, annot, C=None, R=None, dtype=np.float64,
+                    impute_mode="mean", ddof=1):
+        t = self._t(dtype)
+        ann = np.ascontiguousarray(annot, dtype=dtype)
+        Cf, Rf, p = self._cr(C, R, dtype)
+        inv = np.empty(nsnps, dtype=dtype)
+        mu22 = np.empty((ann.shape[1], ann.shape[1]))
+        N = 0 if Cf is None else Cf.shape[0]
+        self._chk(getattr(self.lib, f"ref_resvar_mu22_{t}")(
+            str(prefix).encode(), f"{prefix}.fam".encode(), nsnps, step, ddof,
+            impute_mode.encode(), _ptr(ann), ann.shape[1], _ptr(Cf), _ptr(Rf), N, p, _ptr(inv),
+            _ptr(mu22)))
+        return inv, mu22
+
+    def block_corrections(self, meansq_raw, mu22, annot, N, d):
+        m = np.ascontiguousarray(meansq_raw, dtype=np.float64)
+        u = np.ascontiguousarray(mu22, dtype=np.float64)
+        a = np.ascontiguousarray(annot)
+        out = np.empty((4, m.shape[1], m.shape[1]))
+        self._chk(getattr(self.lib, f"ref_block_corrections_{self._t(a.dtype)}")(
+            _ptr(m), m.shape[0], m.shape[1], _ptr(u), _ptr(a), int(N), float(d), _ptr(out)))
+        return tuple(out)
 
     def project_rowmajor(self, Xz, C=None, R=None):
         t = self._t(Xz.dtype)

@@ -100,16 +100,16 @@ SIGNATURES: dict[str, tuple] = {
 for _t in ("f32", "f64"):
     SIGNATURES[f"lds_phase1_compute_Xz_bed_chunk_{_t}"] = (
         _int, [_str, _str, _int, _int, _p, _i64, _int, _p, _i64, _i64, _p, _int, _int, _int, _int,
-               _int, _u64, _p, _i64, _i64, _p, _int, _int, _u64, _p, _dbl, _p, _p, _i64, _p])
+               _int, _u64, _p, _i64, _i64, _p, _int, _int, _u64, _p, _dbl, _p, _p, _i64, _p, _int])
     SIGNATURES[f"lds_phase2_accum_XtXz_bed_{_t}"] = (
         _int, [_str, _str, _int, _int, _p, _i64, _int, _p, _i64, _int, _p, _i64, _i64, _p, _i64,
-               _i64, _int, _int, _int, _u64, _p, _p])
+               _i64, _int, _int, _int, _u64, _p, _p, _p, _p, _i64])
     SIGNATURES[f"lds_phase1_compute_Xz_bed_chunk_rowmajor_{_t}"] = (
         _int, [_str, _str, _int, _int, _p, _i64, _int, _p, _i64, _i64, _p, _int, _int, _int, _int,
                _int, _u64, _p, _i64, _i64, _int, _int, _u64, _p, _dbl, _p, _p, _i64, _p])
     SIGNATURES[f"lds_phase2_accum_XtXz_bed_mailman_{_t}"] = (
         _int, [_str, _str, _int, _int, _p, _i64, _int, _p, _i64, _int, _p, _i64, _i64, _p, _i64,
-               _i64, _int, _int, _u64, _p, _p])
+               _i64, _int, _int, _u64, _p, _p, _p, _p, _i64])
     SIGNATURES[f"lds_phase2_accum_XtXz_bed_mailman_rowmajor_{_t}"] = (
         _int, [_str, _str, _int, _int, _p, _i64, _int, _p, _i64, _int, _p, _i64, _i64, _p, _i64,
                _i64, _p, _i64, _int, _int, _u64, _p, _p])
@@ -120,7 +120,24 @@ for _t in ("f32", "f64"):
     SIGNATURES[f"lds_standardize_dosage_inplace_{_t}"] = (_int, [_p, _i64, _i64, _int, _dbl, _p])
     SIGNATURES[f"lds_precompute_residual_variances_bed_{_t}"] = (
         _int, [_str, _str, _int, _int, _p, _i64, _int, _dbl, _int, _int, _u64, _p, _p, _p, _i64,
-               _p])
+               _p, _int, _p, _i64, _i64, _p])
+    SIGNATURES[f"lds_phase1_compute_Xz_geno_chunk_{_t}"] = (
+        _int, [_p, _i64, _i64, _int, _p, _i64, _i64, _p, _int, _int, _int, _int, _int, _u64, _p,
+               _i64, _i64, _p, _p, _p, _i64, _p, _p, _dbl])
+    SIGNATURES[f"lds_phase2_accum_XtXz_geno_{_t}"] = (
+        _int, [_p, _i64, _i64, _int, _p, _i64, _int, _p, _i64, _i64, _p, _i64, _i64, _p, _p,
+               _i64, _int, _p, _p])
+    SIGNATURES[f"lds_phase2_compute_XtXz_bed_{_t}"] = (
+        _int, [_str, _str, _int, _int, _p, _i64, _int, _p, _i64, _int, _p, _i64, _i64, _p, _i64,
+               _i64, _p, _p, _i64, _int, _int, _int, _u64])
+    SIGNATURES[f"lds_apply_grm_bed_panel_{_t}"] = (
+        _int, [_str, _str, _int, _int, _p, _i64, _int, _p, _i64, _p, _p, _i64, _i64, _p, _p,
+               _i64, _int, _int, _u64])
+    SIGNATURES[f"lds_apply_grm_bed_panel_mailman_{_t}"] = (
+        _int, [_str, _str, _int, _int, _p, _i64, _int, _p, _i64, _p, _p, _i64, _i64, _p, _p,
+               _i64, _int, _u64])
+    SIGNATURES[f"lds_compute_block_corrections_binary_{_t}"] = (
+        _int, [_p, _i64, _i64, _p, _p, _int, _dbl, _p, _p, _p, _p])
 
 _LIB = None
 

@@ -846,6 +846,514 @@ void inv_resvar_projected_cov(Context& c, const Prepared& P, int64_t nsnps, cons
 // ---------------------------------------------------------------------------
 // Entry-point implementations
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// Dense genotype blocks, covariate projections inside phase 1 / phase 2, GRM
+// panel products, mu22 moments and block corrections
+// (gwldcore.cpp:1896-1923, :2602-2649, :2132-2327, :1134-1497, :3335-3627).
+// ---------------------------------------------------------------------------
+struct DevCov {
+    DevBuf C, R;  // FP64, column-major N x p and p x N
+    int64_t N = 0, p = 0;
+    bool on() const { return p > 0; }
+};
+
+template <typename T>
+void upload_cov(Context& c, DevCov& d, const T* Cm, const T* Rm, int64_t N, int64_t p) {
+    d.N = N;
+    d.p = (Cm && Rm) ? p : 0;
+    if (!d.on()) return;
+    std::vector<double> h((size_t)(N * p));
+    for (size_t i = 0; i < h.size(); ++i) h[i] = (double)Cm[i];
+    h2d(d.C.as<double>(h.size()), h.data(), h.size(), c.st);
+    for (size_t i = 0; i < h.size(); ++i) h[i] = (double)Rm[i];
+    h2d(d.R.as<double>(h.size()), h.data(), h.size(), c.st);
+    ck(cudaStreamSynchronize(c.st), "covariates");
+}
+
+// X (N rows of an ld-strided column-major panel, L columns) <- X - C (R X),
+// or with `transpose` X <- X - R^T (C^T X) (the same projection applied from
+// the other side).  tmp: p x L scratch.
+void project_cols(Context& c, double* X, int64_t ld, int64_t L, const DevCov& cv, bool transpose,
+                  DevBuf& tmp) {
+    if (!cv.on() || L <= 0) return;
+    const int64_t N = cv.N, p = cv.p;
+    double* t = tmp.as<double>((size_t)(p * L));
+    DGemmArgs a;
+    a.M = p;
+    a.N = L;
+    a.K = N;
+    if (transpose) {
+        a.A = static_cast<const double*>(cv.C.p);  // C^T: (a, n) -> C[n + a N]
+        a.a_ms = N;
+        a.a_ks = 1;
+    } else {
+        a.A = static_cast<const double*>(cv.R.p);  // R: (a, n) -> R[a + n p]
+        a.a_ms = 1;
+        a.a_ks = p;
+    }
+    a.B = X;
+    a.b_ks = 1;
+    a.b_ns = ld;
+    a.C = t;
+    a.c_ms = 1;
+    a.c_ns = p;
+    launch_dgemm(a, c.st);
+    DGemmArgs b;
+    b.M = N;
+    b.N = L;
+    b.K = p;
+    if (transpose) {
+        b.A = static_cast<const double*>(cv.R.p);  // R^T: (n, a) -> R[a + n p]
+        b.a_ms = p;
+        b.a_ks = 1;
+    } else {
+        b.A = static_cast<const double*>(cv.C.p);  // C: (n, a) -> C[n + a N]
+        b.a_ms = 1;
+        b.a_ks = N;
+    }
+    b.B = t;
+    b.b_ks = 1;
+    b.b_ns = p;
+    b.C = X;
+    b.c_ms = 1;
+    b.c_ns = ld;
+    b.alpha = -1.0;
+    b.beta = 1.0;
+    launch_dgemm(b, c.st);
+    ck(cudaGetLastError(), "projection");
+}
+
+// Dense T matrix (rows x cols, column-major) to a device FP64 buffer with
+// leading dimension ld (padding rows zero).
+template <typename T>
+double* upload_dense(Context& c, DevBuf& buf, const T* h, int64_t rows, int64_t cols, int64_t ld) {
+    std::vector<double> tmp((size_t)(ld * cols), 0.0);
+    for (int64_t q = 0; q < cols; ++q)
+        for (int64_t i = 0; i < rows; ++i) tmp[(size_t)(q * ld + i)] = (double)h[q * rows + i];
+    double* d = buf.as<double>(std::max<size_t>(tmp.size(), 1));
+    h2d(d, tmp.data(), tmp.size(), c.st);
+    return d;
+}
+
+template <typename T>
+void download_dense(Context& c, T* h, const double* d, int64_t rows, int64_t cols, int64_t ld) {
+    std::vector<double> tmp((size_t)(ld * cols));
+    d2h(tmp.data(), d, tmp.size(), c.st);
+    ck(cudaStreamSynchronize(c.st), "download");
+    for (int64_t q = 0; q < cols; ++q)
+        for (int64_t i = 0; i < rows; ++i) h[q * rows + i] = (T)tmp[(size_t)(q * ld + i)];
+}
+
+// inv_j = 1/sqrt(max(eps, ss_j / df)) from ||x_j||^2 and (with covariates)
+// proj = R x_j: ss_j + q - 2h (compute_inv_resvar_from_geno_block,
+// gwldcore.cpp:3220-3333).
+template <typename T>
+void inv_from_sumsq(const double* ss, const double* proj, int64_t L, int64_t p, const T* gram,
+                    double df, double eps, T* inv_out) {
+    for (int64_t j = 0; j < L; ++j) {
+        double s2 = ss[j];
+        if (proj && p > 0) {
+            const double* t = proj + j * p;
+            double h = 0.0;
+            for (int64_t k = 0; k < p; ++k) h += t[k] * t[k];
+            double q = h;
+            if (gram) {
+                q = 0.0;
+                for (int64_t a = 0; a < p; ++a) {
+                    double gy = 0.0;
+                    for (int64_t b = 0; b < p; ++b) gy += (double)gram[a * p + b] * t[b];
+                    q += t[a] * gy;
+                }
+            }
+            s2 += q - 2.0 * h;
+        }
+        const double var = s2 / df;
+        const double safe = std::isnan(var) ? var : (var > eps ? var : eps);
+        inv_out[j] = (T)(1.0 / std::sqrt(safe));
+    }
+}
+
+template <typename T>
+void phase1_geno_impl(const T* geno, int64_t N, int64_t L, int blk_start, const T* annot,
+                      int64_t annot_rows, int64_t K, const T* inv_right, int v_start, int v_count,
+                      int rand_dist, int has_seed, uint64_t seed, T* Xz, int64_t xz_rows,
+                      int64_t xz_cols, uint8_t* bin_init, T* inv_out, double eps, const T* Cm,
+                      const T* Rm, int64_t p, const T* gram) {
+    Context& c = ctx();
+    std::lock_guard<std::mutex> lk(c.mu);
+    ensure_device(c);
+    if (N <= 0 || L < 0) fail(LDS_ERR_ARG, "Invalid external genotype block dimensions in phase1");
+    if (L == 0) return;
+    if (annot_rows != L) fail(LDS_ERR_ARG, "L mismatch");
+    DevBuf dx, dtmp, dp;
+    double* X = upload_dense<T>(c, dx, geno, N, L, N);
+    std::vector<T> inv((size_t)L);
+    if (inv_out) {
+        if ((Cm != nullptr) != (Rm != nullptr))
+            fail(LDS_ERR_ARG, "C and R must be provided together for fused residual variances");
+        if (N <= 1) fail(LDS_ERR_ARG, "Invalid block dimensions in compute_inv_resvar_from_geno_block");
+        const bool cov = Cm && Rm && p > 0;
+        if (cov && N - p <= 1) fail(LDS_ERR_ARG, "N_eff must be > 1 in fused residual variances");
+        const double df = cov ? (double)(N - p - 1) : (double)(N - 1);
+        std::vector<double> ss((size_t)L), proj;
+        double* dss = dtmp.as<double>((size_t)L);
+        launch_col_sumsq(X, N, N, L, dss, c.st);
+        d2h(ss.data(), dss, ss.size(), c.st);
+        if (cov) {
+            DevCov cv;
+            upload_cov<T>(c, cv, Cm, Rm, N, p);
+            double* pr = dp.as<double>((size_t)(p * L));
+            DGemmArgs a;
+            a.M = p;
+            a.N = L;
+            a.K = N;
+            a.A = static_cast<const double*>(cv.R.p);
+            a.a_ms = 1;
+            a.a_ks = p;
+            a.B = X;
+            a.b_ks = 1;
+            a.b_ns = N;
+            a.C = pr;
+            a.c_ms = 1;
+            a.c_ns = p;
+            launch_dgemm(a, c.st);
+            proj.resize((size_t)(p * L));
+            d2h(proj.data(), pr, proj.size(), c.st);
+        }
+        ck(cudaStreamSynchronize(c.st), "resvar");
+        inv_from_sumsq<T>(ss.data(), cov ? proj.data() : nullptr, L, p, gram, df, eps, inv.data());
+        std::memcpy(inv_out, inv.data(), sizeof(T) * (size_t)L);
+    } else {
+        if (!inv_right) fail(LDS_ERR_ARG, "inv_right shape mismatch in phase1");
+        std::memcpy(inv.data(), inv_right, sizeof(T) * (size_t)L);
+    }
+    if (xz_rows != N || xz_cols != K * v_count)
+        fail(LDS_ERR_ARG, "Xz2d_chunk shape must be (N, B*v_count)");
+    if (v_count <= 0) return;
+    const int V = v_count;
+    const uint64_t root = has_seed ? seed : std::random_device{}();
+    std::vector<double> Z((size_t)(L * V));
+    make_probes<T>(root, blk_start, v_start, (int)L, V, rand_dist, Z.data(), L);
+    const Csr cs = build_csr<T>(annot, inv.data(), L, K, 0, 1, 1, 1);
+    DevBuf dxz, db, di;
+    double* Y = upload_dense<T>(c, dxz, Xz, N, K * V, N);
+    std::vector<char> touched((size_t)K, 0);
+    for (int64_t k = 0; k < K; ++k) {
+        const int64_t n = cs.nnz[(size_t)k];
+        if (n == 0) continue;
+        const int64_t o = cs.bin_off[(size_t)k];
+        std::vector<double> Bk((size_t)(n * V));
+        for (int64_t cc = 0; cc < V; ++cc)
+            for (int64_t r = 0; r < n; ++r)
+                Bk[(size_t)(cc * n + r)] =
+                    (double)(T)(Z[(size_t)(cc * L + cs.rowind[(size_t)(o + r)])] * cs.sc[(size_t)(o + r)]);
+        double* dB = db.as<double>(Bk.size());
+        h2d(dB, Bk.data(), Bk.size(), c.st);
+        int32_t* dI = di.as<int32_t>((size_t)n);
+        h2d(dI, cs.rowind.data() + o, (size_t)n, c.st);
+        bool beta1 = true;
+        if (bin_init) {
+            beta1 = bin_init[k] != 0;
+            bin_init[k] = 1;
+        }
+        DGemmArgs a;
+        a.M = N;
+        a.N = V;
+        a.K = n;
+        a.A = X;
+        a.a_ms = 1;
+        a.a_ks = N;
+        a.a_kidx = dI;
+        a.B = dB;
+        a.b_ks = 1;
+        a.b_ns = n;
+        a.C = Y + k * V * N;
+        a.c_ms = 1;
+        a.c_ns = N;
+        a.beta = beta1 ? 1.0 : 0.0;
+        launch_dgemm(a, c.st);
+        ck(cudaStreamSynchronize(c.st), "phase1 dense");  // Bk and the index are reused
+        touched[(size_t)k] = 1;
+    }
+    ck(cudaGetLastError(), "phase1 dense");
+    std::vector<double> out((size_t)(N * K * V));
+    d2h(out.data(), Y, out.size(), c.st);
+    ck(cudaStreamSynchronize(c.st), "phase1 dense");
+    for (int64_t k = 0; k < K; ++k) {
+        if (!touched[(size_t)k]) continue;
+        for (int64_t q = k * V; q < (k + 1) * V; ++q)
+            for (int64_t i = 0; i < N; ++i) Xz[q * N + i] = (T)out[(size_t)(q * N + i)];
+    }
+}
+
+// Left scales, device accumulators and the guarded reduction of a product
+// panel W (L x Q on the device), merged into the caller's outputs like
+// phase2_bed_impl.
+template <typename T>
+void dense_p2_finish(Context& c, const double* W, int64_t L, int64_t K, int V, const T* inv_left,
+                     int N_denom, T* meansq, int blk_start, double* mc_agg, double* mc_snp,
+                     const char* label) {
+    double denom = (double)N_denom - 1.0;
+    if (denom <= 0.0) denom = 1.0;
+    const double inv_denom2 = 1.0 / (denom * denom);
+    std::vector<double> ls((size_t)L);
+    for (int64_t i = 0; i < L; ++i) {
+        const double v = (double)inv_left[i];
+        ls[(size_t)i] = (std::isfinite(v) && v > 0.0) ? v * v * inv_denom2 : 0.0;
+    }
+    DevBuf dls, dacc, dmc;
+    double* d_ls = dls.as<double>((size_t)L);
+    h2d(d_ls, ls.data(), ls.size(), c.st);
+    double* d_acc = dacc.as<double>((size_t)(L * K));
+    ck(cudaMemsetAsync(d_acc, 0, sizeof(double) * (size_t)(L * K), c.st), "memset");
+    double* d_mc = nullptr;
+    if (mc_agg || mc_snp) {
+        d_mc = dmc.as<double>((size_t)(L * K));
+        ck(cudaMemsetAsync(d_mc, 0, sizeof(double) * (size_t)(L * K), c.st), "memset");
+    }
+    unsigned long long* g = c.guards.as<unsigned long long>(2);
+    ck(cudaMemsetAsync(g, 0, 16, c.st), "memset");
+    launch_dense_p2_epilogue(W, L, (int)K, V, d_ls, d_acc, d_mc, g, extreme_warn_env(),
+                             drop_extreme_env(), c.st);
+    ck(cudaGetLastError(), "launch");
+    std::vector<double> upd((size_t)(L * K)), mcv;
+    d2h(upd.data(), d_acc, upd.size(), c.st);
+    if (d_mc) {
+        mcv.resize((size_t)(L * K));
+        d2h(mcv.data(), d_mc, mcv.size(), c.st);
+    }
+    ck(cudaStreamSynchronize(c.st), "phase2 dense");
+    report_guards(c, label, blk_start, (int)(blk_start + L));
+    for (int64_t i = 0; i < L; ++i)
+        for (int64_t k = 0; k < K; ++k)
+            meansq[(blk_start + i) * K + k] += (T)upd[(size_t)(i * K + k)];
+    if (d_mc) {
+        for (int64_t k = 0; k < K; ++k) {
+            double agg = 0.0;
+            for (int64_t i = 0; i < L; ++i) {
+                const double sv = mcv[(size_t)(i * K + k)];
+                agg += sv;
+                if (mc_snp) mc_snp[(blk_start + i) * K + k] += sv;
+            }
+            if (mc_agg) mc_agg[k] += agg;
+        }
+    }
+}
+
+template <typename T>
+void phase2_geno_impl(T* geno, int64_t N, int64_t L, int blk_start, const T* inv_left,
+                      int64_t L_in, int tile_nvecs, const T* Xz, int64_t xz_rows, int64_t xz_cols,
+                      T* meansq, int64_t M_rows, int64_t K_in, const T* Cm, const T* Rm, int64_t p,
+                      int N_denom, double* mc_agg, double* mc_snp) {
+    Context& c = ctx();
+    std::lock_guard<std::mutex> lk(c.mu);
+    ensure_device(c);
+    if (N <= 0 || L < 0) fail(LDS_ERR_ARG, "Invalid external genotype block dimensions in phase2");
+    if (L == 0) return;
+    DevBuf dx, dtmp, dxz, dw;
+    double* X = upload_dense<T>(c, dx, geno, N, L, N);
+    if (Cm && Rm && p > 0) {
+        // the reference projects the caller's genotype block in place
+        DevCov cv;
+        upload_cov<T>(c, cv, Cm, Rm, N, p);
+        project_cols(c, X, N, L, cv, false, dtmp);
+        download_dense<T>(c, geno, X, N, L, N);
+    }
+    if (L_in != L) fail(LDS_ERR_ARG, "inv_left shape mismatch in phase2_accum_XtXz_bed");
+    if (xz_rows != N) fail(LDS_ERR_ARG, "Xz2d shape mismatch in phase2_accum_XtXz_bed");
+    const int64_t Q = xz_cols;
+    if (tile_nvecs <= 0 || Q % tile_nvecs)
+        fail(LDS_ERR_ARG, "Xz2d col count must be a multiple of tile_nvecs");
+    const int64_t K = Q / tile_nvecs;
+    if (K_in != K) fail(LDS_ERR_ARG, "meansq_accum shape mismatch in phase2_accum_XtXz_bed");
+    if (blk_start + L > M_rows) fail(LDS_ERR_ARG, "meansq_accum rows smaller than SNP count");
+    if (K > 512) fail(LDS_ERR_ARG, "B too large for fixed seg buffers in phase2_accum_XtXz_bed");
+    double* Y = upload_dense<T>(c, dxz, Xz, N, Q, N);
+    double* W = dw.as<double>((size_t)(L * Q));
+    DGemmArgs a;
+    a.M = L;
+    a.N = Q;
+    a.K = N;
+    a.A = X;  // X^T: (j, n) -> X[n + j N]
+    a.a_ms = N;
+    a.a_ks = 1;
+    a.B = Y;
+    a.b_ks = 1;
+    a.b_ns = N;
+    a.C = W;
+    a.c_ms = 1;
+    a.c_ns = L;
+    launch_dgemm(a, c.st);
+    dense_p2_finish<T>(c, W, L, K, tile_nvecs, inv_left, N_denom, meansq, blk_start, mc_agg,
+                       mc_snp, "accum");
+}
+
+// GRM panel products (apply_grm_bed_panel_impl, gwldcore.cpp:1134-1254, and
+// its Mailman form :1256-1497): out = P X D X^T P V with D = diag(inv_j^2 / M)
+// over SNPs [0, nsnps) and P = I - C R when covariates are given.  X^T V runs
+// on the phase-2 tensor-core kernel's exact raw-product mode and X (D coef) on
+// the phase-1 kernel.
+template <typename T>
+void apply_grm_impl(const char* bed_prefix, const char* fam_path, int nsnps, int step_size,
+                    const int64_t* row_sel, int64_t n_row_sel, int ddof, const T* inv_all,
+                    int64_t n_inv, const T* panel_in, T* panel_out, int64_t rows, int64_t Q,
+                    const T* Cm, const T* Rm, int64_t p, int impute, int has_iseed, uint64_t iseed,
+                    const char* name) {
+    Context& c = ctx();
+    std::lock_guard<std::mutex> lk(c.mu);
+    ensure_device(c);
+    int64_t M = 0;
+    Prepared& P = prepared_for_file(c, bed_prefix, fam_path, row_sel, n_row_sel, impute,
+                                    has_iseed ? iseed : 0ULL, ddof, &M);
+    if (nsnps < 0 || nsnps > M) fail(LDS_ERR_ARG, "nsnps is out of range in %s", name);
+    if (step_size <= 0) fail(LDS_ERR_ARG, "step_size must be > 0 in %s", name);
+    const int64_t N = P.g.N, Np = P.g.N_pad;
+    if (N <= 0) fail(LDS_ERR_ARG, "No rows selected in %s", name);
+    if (n_inv < nsnps) fail(LDS_ERR_ARG, "inv_all shape mismatch in %s", name);
+    if (rows != N) fail(LDS_ERR_ARG, "panel row mismatch in %s", name);
+    for (int64_t i = 0; i < N * Q; ++i) panel_out[i] = T(0);
+    if (Q == 0 || nsnps == 0) return;
+    DevCov cv;
+    upload_cov<T>(c, cv, Cm, Rm, N, p);
+    DevBuf dv, dtmp;
+    double* V = upload_dense<T>(c, dv, panel_in, N, Q, Np);
+    project_cols(c, V, Np, Q, cv, false, dtmp);
+    std::vector<double> Vh((size_t)(N * Q));
+    for (int64_t q = 0; q < Q; ++q)
+        d2h(Vh.data() + q * N, V + q * Np, (size_t)N, c.st);
+    ck(cudaStreamSynchronize(c.st), "grm panel");
+    const std::vector<double> coef = snp_products(c, P, 0, nsnps, Vh, Q);  // nsnps x Q row-major
+    const double invM = 1.0 / (double)nsnps;
+    std::vector<T> w((size_t)nsnps), ones((size_t)nsnps, T(1));
+    for (int64_t j = 0; j < nsnps; ++j) {
+        const double ij = (double)inv_all[j];
+        double x = ij * ij * invM;
+        if (!std::isfinite(x) || x <= 0.0) x = 0.0;
+        w[(size_t)j] = (T)x;
+    }
+    std::vector<double> Z((size_t)(nsnps * Q));
+    for (int64_t j = 0; j < nsnps; ++j)
+        for (int64_t q = 0; q < Q; ++q) Z[(size_t)(q * nsnps + j)] = (double)(T)coef[(size_t)(j * Q + q)];
+    const int Vp = (int)round_up(Q, kColTile);
+    const Csr cs = build_csr<T>(ones.data(), w.data(), nsnps, 1, 0, Vp, c.slices);
+    if (cs.nnz[0] == 0) return;
+    run_phase1(c, P, cs, 1, (int)Q, Z.data(), nsnps, nsnps, 0);
+    double* Y = static_cast<double*>(c.y.p);
+    project_cols(c, Y, Np, Q, cv, false, dtmp);
+    std::vector<double> out((size_t)(Np * Q));
+    d2h(out.data(), Y, out.size(), c.st);
+    ck(cudaStreamSynchronize(c.st), "grm panel");
+    for (int64_t q = 0; q < Q; ++q)
+        for (int64_t i = 0; i < N; ++i) panel_out[q * N + i] = (T)out[(size_t)(q * Np + i)];
+}
+
+// mu22 (precompute_residual_variances_bed_impl, gwldcore.cpp:3421-3563):
+// S = sum_j (x_j o x_j) a_jk inv_j^2 over the (projected) standardized
+// genotypes, mu22[a][b] = (S^T S)[a][b] / (N Msum_a Msum_b).
+template <typename T>
+void mu22_impl(Context& c, const Prepared& P, int64_t nsnps, const T* inv, const T* annot,
+               int64_t B, const T* Cm, const T* Rm, int64_t p, double* mu22) {
+    const int64_t N = P.g.N;
+    std::vector<double> Msum((size_t)B, 0.0);
+    for (int64_t j = 0; j < nsnps; ++j)
+        for (int64_t k = 0; k < B; ++k) Msum[(size_t)k] += (double)annot[j * B + k];
+    DevCov cv;
+    upload_cov<T>(c, cv, Cm, Rm, N, p);
+    const int64_t Lb = std::max<int64_t>(1, std::min<int64_t>(std::max<int64_t>(nsnps, 1),
+                                                              (int64_t)(256u << 20) / (8 * N)));
+    DevBuf dx, dtmp, dwt, ds, dss;
+    double* X = dx.as<double>((size_t)(N * Lb));
+    double* S = ds.as<double>((size_t)(N * B));
+    ck(cudaMemsetAsync(S, 0, sizeof(double) * (size_t)(N * B), c.st), "memset");
+    double* Wd = dwt.as<double>((size_t)(Lb * B));
+    std::vector<double> Wh((size_t)(Lb * B));
+    for (int64_t j0 = 0; j0 < nsnps; j0 += Lb) {
+        const int64_t L = std::min(Lb, nsnps - j0);
+        launch_decode_standardized(P.g, j0, L, static_cast<const double*>(P.d_mean.p),
+                                   static_cast<const double*>(P.d_sdinv.p), X, N, c.st);
+        project_cols(c, X, N, L, cv, false, dtmp);
+        for (int64_t k = 0; k < B; ++k)
+            for (int64_t j = 0; j < L; ++j) {
+                const double iv = (double)inv[j0 + j];
+                Wh[(size_t)(k * L + j)] = (double)annot[(j0 + j) * B + k] * (iv * iv);
+            }
+        ck(cudaStreamSynchronize(c.st), "mu22");  // Wd is rewritten
+        h2d(Wd, Wh.data(), (size_t)(L * B), c.st);
+        DGemmArgs a;
+        a.M = N;
+        a.N = B;
+        a.K = L;
+        a.A = X;
+        a.a_ms = 1;
+        a.a_ks = N;
+        a.a_square = 1;
+        a.B = Wd;
+        a.b_ks = 1;
+        a.b_ns = L;
+        a.C = S;
+        a.c_ms = 1;
+        a.c_ns = N;
+        a.beta = 1.0;
+        launch_dgemm(a, c.st);
+    }
+    double* SS = dss.as<double>((size_t)(B * B));
+    DGemmArgs g;
+    g.M = B;
+    g.N = B;
+    g.K = N;
+    g.A = S;
+    g.a_ms = N;
+    g.a_ks = 1;
+    g.B = S;
+    g.b_ks = 1;
+    g.b_ns = N;
+    g.C = SS;
+    g.c_ms = 1;
+    g.c_ns = B;
+    launch_dgemm(g, c.st);
+    ck(cudaGetLastError(), "mu22");
+    std::vector<double> h((size_t)(B * B));
+    d2h(h.data(), SS, h.size(), c.st);
+    ck(cudaStreamSynchronize(c.st), "mu22");
+    for (int64_t a = 0; a < B; ++a)
+        for (int64_t b = 0; b < B; ++b) {
+            const double den = (double)N * Msum[(size_t)a] * Msum[(size_t)b];
+            double v = 0.0;
+            if (den != 0.0) {
+                v = h[(size_t)(a + b * B)] / den;
+                if (!std::isfinite(v)) v = 0.0;
+            }
+            mu22[a * B + b] = v;
+        }
+}
+
+template <typename Tann>
+void block_corrections_impl(const double* meansq, const double* mu22, const Tann* annot,
+                            int64_t M, int64_t B, int N, double d, double* R2, double* rho2,
+                            double* bias, double* delta) {
+    Context& c = ctx();
+    std::lock_guard<std::mutex> lk(c.mu);
+    ensure_device(c);
+    if (N <= 1) fail(LDS_ERR_ARG, "N must be > 1 in compute_block_corrections_binary");
+    if (B <= 0) return;
+    DevBuf dm, du, da, dout;
+    double* m = dm.as<double>((size_t)std::max<int64_t>(M * B, 1));
+    h2d(m, meansq, (size_t)(M * B), c.st);
+    double* u = du.as<double>((size_t)(B * B));
+    h2d(u, mu22, (size_t)(B * B), c.st);
+    Tann* an = da.as<Tann>((size_t)std::max<int64_t>(M * B, 1));
+    h2d(an, annot, (size_t)(M * B), c.st);
+    double* o = dout.as<double>((size_t)(4 * B * B));
+    launch_block_corrections<Tann>(m, u, an, M, (int)B, (double)N, d, o, o + B * B, o + 2 * B * B,
+                                   o + 3 * B * B, c.st);
+    ck(cudaGetLastError(), "launch");
+    d2h(R2, o, (size_t)(B * B), c.st);
+    d2h(rho2, o + B * B, (size_t)(B * B), c.st);
+    d2h(bias, o + 2 * B * B, (size_t)(B * B), c.st);
+    d2h(delta, o + 3 * B * B, (size_t)(B * B), c.st);
+    ck(cudaStreamSynchronize(c.st), "block corrections");
+}
+
 template <typename T>
 void phase1_bed_impl(const char* bed_prefix, const char* fam_path, int blk_start, int blk_end,
                      const int64_t* row_sel, int64_t n_row_sel, int ddof, const T* annot,
@@ -853,7 +1361,8 @@ void phase1_bed_impl(const char* bed_prefix, const char* fam_path, int blk_start
                      int rand_dist, int has_seed, uint64_t seed, T* Xz, int64_t xz_rows,
                      int64_t xz_cols, uint8_t* bin_init, int impute, int has_iseed,
                      uint64_t iseed, T* inv_out, double resvar_eps, const T* Cm = nullptr,
-                     const T* Rm = nullptr, int64_t p = 0, const T* gram = nullptr) {
+                     const T* Rm = nullptr, int64_t p = 0, const T* gram = nullptr,
+                     int project_right = 0) {
     Context& c = ctx();
     std::lock_guard<std::mutex> lk(c.mu);
     ensure_device(c);
@@ -865,6 +1374,12 @@ void phase1_bed_impl(const char* bed_prefix, const char* fam_path, int blk_start
     if (blk_end > M) fail(LDS_ERR_ARG, "blk_end exceeds #SNPs in BIM");
     if (blk_end <= blk_start) return;
     const int64_t L = blk_end - blk_start;
+    // project_right (gwldcore.cpp:1633-1650): the block's genotypes are
+    // projected, X <- (I - C R) X, before the products; by linearity the
+    // block's contribution to the sketch is projected instead.
+    const bool proj = project_right && Cm && Rm && p > 0;
+    if (proj && inv_out)
+        fail(LDS_ERR_ARG, "Fused residual variance is incompatible with project_right=True");
     if (annot_rows != L) fail(LDS_ERR_ARG, "L mismatch");
     std::vector<T> inv((size_t)L);
     if (inv_out) {
@@ -887,8 +1402,14 @@ void phase1_bed_impl(const char* bed_prefix, const char* fam_path, int blk_start
     std::vector<double> Z((size_t)(L * v_count));
     make_probes<T>(root, blk_start, v_start, (int)L, v_count, rand_dist, Z.data(), L);
     run_phase1(c, P, csr, K, v_count, Z.data(), L, L, blk_start);
-    // Download the block's contribution and merge with beta semantics.
     const int64_t N = P.g.N;
+    if (proj) {
+        DevCov cv;
+        upload_cov<T>(c, cv, Cm, Rm, N, p);
+        DevBuf tmp;
+        project_cols(c, static_cast<double*>(c.y.p), P.g.N_pad, K * v_count, cv, false, tmp);
+    }
+    // Download the block's contribution and merge with beta semantics.
     std::vector<double> D((size_t)(N * K * v_count));
     const double* Y = static_cast<double*>(c.y.p);
     for (int64_t q = 0; q < K * v_count; ++q)
@@ -917,7 +1438,9 @@ void phase2_bed_impl(const char* bed_prefix, const char* fam_path, int blk_start
                      const int64_t* row_sel, int64_t n_row_sel, int ddof, const T* inv_left,
                      int64_t L_in, int tile_nvecs, const T* Xz, int64_t xz_rows, int64_t xz_cols,
                      T* meansq, int64_t M_rows, int64_t K_in, int N_denom, int impute,
-                     int has_iseed, uint64_t iseed, double* mc_agg, double* mc_snp) {
+                     int has_iseed, uint64_t iseed, double* mc_agg, double* mc_snp,
+                     const T* Cm = nullptr, const T* Rm = nullptr, int64_t p = 0,
+                     int proj_sketch = 0, double post_scale = 1.0, const char* label = "accum") {
     Context& c = ctx();
     std::lock_guard<std::mutex> lk(c.mu);
     ensure_device(c);
@@ -945,6 +1468,15 @@ void phase2_bed_impl(const char* bed_prefix, const char* fam_path, int blk_start
         for (int64_t n = 0; n < N; ++n) y[(size_t)(q * Np + n)] = (double)Xz[q * N + n];
     double* dY = c.y.as<double>((size_t)(Np * Q));
     h2d(dY, y.data(), y.size(), c.st);
+    if (Cm && Rm && p > 0) {
+        // Work = ((I - C R) X)^T Xz = X^T (I - C R)^T Xz for the dense form
+        // (gwldcore.cpp:2376-2390); the Mailman form projects the sketch,
+        // Xz <- (I - C R) Xz (:615-638).
+        DevCov cv;
+        upload_cov<T>(c, cv, Cm, Rm, N, p);
+        DevBuf tmp;
+        project_cols(c, dY, Np, Q, cv, proj_sketch == 0, tmp);
+    }
     quantize_sketch(c, P, K, tile_nvecs);
     // Left scales.
     double denom = (double)N_denom - 1.0;
@@ -973,10 +1505,10 @@ void phase2_bed_impl(const char* bed_prefix, const char* fam_path, int blk_start
         d2h(mcv.data(), d_mc, mcv.size(), c.st);
     }
     ck(cudaStreamSynchronize(c.st), "phase2");
-    report_guards(c, "accum", blk_start, blk_end);
+    report_guards(c, label, blk_start, blk_end);
     for (int64_t i = 0; i < L; ++i)
         for (int64_t k = 0; k < K; ++k)
-            meansq[(blk_start + i) * K + k] += (T)upd[(size_t)(i * K + k)];
+            meansq[(blk_start + i) * K + k] += (T)(upd[(size_t)(i * K + k)] * post_scale);
     if (d_mc) {
         for (int64_t k = 0; k < K; ++k) {
             double agg = 0.0;
@@ -994,7 +1526,8 @@ template <typename T>
 void resvar_impl(const char* bed_prefix, const char* fam_path, int nsnps, const int64_t* row_sel,
                  int64_t n_row_sel, int ddof, double eps, int impute, int has_iseed,
                  uint64_t iseed, T* inv_out, const T* Cm = nullptr, const T* Rm = nullptr,
-                 int64_t p = 0, double* snp_var = nullptr) {
+                 int64_t p = 0, double* snp_var = nullptr, const T* annot_all = nullptr,
+                 int64_t annot_rows = 0, int64_t B = 0, double* mu22 = nullptr) {
     Context& c = ctx();
     std::lock_guard<std::mutex> lk(c.mu);
     ensure_device(c);
@@ -1004,14 +1537,21 @@ void resvar_impl(const char* bed_prefix, const char* fam_path, int nsnps, const 
     if (nsnps > M) fail(LDS_ERR_ARG, "nsnps exceeds #SNPs in BIM");
     if (P.g.N <= 1) fail(LDS_ERR_ARG, "Invalid block dimensions in compute_inv_resvar_from_geno_block");
     if ((Cm != nullptr) != (Rm != nullptr)) fail(LDS_ERR_ARG, "C and R must be provided together");
+    if (mu22) {
+        if (!annot_all) fail(LDS_ERR_ARG, "annot_all must be provided when compute_mu22=True");
+        if (annot_rows != nsnps)
+            fail(LDS_ERR_ARG, "annot_all shape mismatch in precompute_residual_variances_bed");
+        if (B <= 0) fail(LDS_ERR_ARG, "annot_all must have at least one column");
+    }
     if (Cm && Rm && p > 0) {
         inv_resvar_projected_cov<T>(c, P, nsnps, Cm, Rm, p, eps, inv_out, snp_var);
-        return;
+    } else {
+        for (int64_t j = 0; j < nsnps; ++j) {
+            inv_out[j] = inv_resvar<T>(P, j, eps);
+            if (snp_var) snp_var[j] = sumsq_std<T>(P, j) > 0.0 ? 1.0 : 0.0;
+        }
     }
-    for (int64_t j = 0; j < nsnps; ++j) {
-        inv_out[j] = inv_resvar<T>(P, j, eps);
-        if (snp_var) snp_var[j] = sumsq_std<T>(P, j) > 0.0 ? 1.0 : 0.0;
-    }
+    if (mu22) mu22_impl<T>(c, P, nsnps, inv_out, annot_all, B, Cm, Rm, p, mu22);
 }
 
 // ---------------------------------------------------------------------------
@@ -2432,7 +2972,7 @@ LDS_API void lds_clear_device_cache(void) {
         int kmax_hint, int rand_dist, int has_seed, uint64_t seed, T *Xz2d_chunk,                \
         int64_t xz_rows, int64_t xz_cols, uint8_t *bin_init_mask, int impute_mode,              \
         int has_impute_seed, uint64_t impute_seed, T *inv_out, double resvar_eps, const T *C,   \
-        const T *R, int64_t p, const T *resvar_gram
+        const T *R, int64_t p, const T *resvar_gram, int project_right
 #define P1_CALL(T)                                                                              \
     guarded([&] {                                                                               \
         (void)kmax_hint;                                                                        \
@@ -2440,7 +2980,7 @@ LDS_API void lds_clear_device_cache(void) {
                            annot_blk, annot_rows, K, inv_right, v_start, v_count, rand_dist,    \
                            has_seed, seed, Xz2d_chunk, xz_rows, xz_cols, bin_init_mask,         \
                            impute_mode, has_impute_seed, impute_seed, inv_out, resvar_eps, C,   \
-                           R, p, resvar_gram);                                                  \
+                           R, p, resvar_gram, project_right);                                   \
     })
 LDS_API int lds_phase1_compute_Xz_bed_chunk_f32(P1_ARGS(float)) { return P1_CALL(float); }
 LDS_API int lds_phase1_compute_Xz_bed_chunk_f64(P1_ARGS(double)) { return P1_CALL(double); }
@@ -2450,13 +2990,14 @@ LDS_API int lds_phase1_compute_Xz_bed_chunk_f64(P1_ARGS(double)) { return P1_CAL
         const int64_t *row_sel, int64_t n_row_sel, int ddof, const T *inv_left, int64_t L,      \
         int tile_nvecs, const T *Xz2d, int64_t xz_rows, int64_t xz_cols, T *meansq_accum,       \
         int64_t M_rows, int64_t K, int N_denom, int impute_mode, int has_impute_seed,           \
-        uint64_t impute_seed, double *mc_aggregate_sumsq, double *mc_per_snp_sumsq
+        uint64_t impute_seed, double *mc_aggregate_sumsq, double *mc_per_snp_sumsq, const T *C, \
+        const T *R, int64_t p
 #define P2_CALL(T)                                                                              \
     guarded([&] {                                                                               \
         phase2_bed_impl<T>(bed_prefix, fam_path, blk_start, blk_end, row_sel, n_row_sel, ddof,  \
                            inv_left, L, tile_nvecs, Xz2d, xz_rows, xz_cols, meansq_accum,       \
                            M_rows, K, N_denom, impute_mode, has_impute_seed, impute_seed,       \
-                           mc_aggregate_sumsq, mc_per_snp_sumsq);                               \
+                           mc_aggregate_sumsq, mc_per_snp_sumsq, C, R, p, 0);                   \
     })
 LDS_API int lds_phase2_accum_XtXz_bed_f32(P2_ARGS(float)) { return P2_CALL(float); }
 LDS_API int lds_phase2_accum_XtXz_bed_f64(P2_ARGS(double)) { return P2_CALL(double); }
@@ -2488,13 +3029,13 @@ LDS_API int lds_phase1_compute_Xz_bed_chunk_rowmajor_f64(P1R_ARGS(double)) { ret
         const int64_t *row_sel, int64_t n_row_sel, int ddof, const T *inv_left, int64_t L,      \
         int tile_nvecs, const T *Xz2d, int64_t xz_rows, int64_t xz_cols, T *meansq_accum,       \
         int64_t M_rows, int64_t K, int N_denom, int has_impute_seed, uint64_t impute_seed,      \
-        double *mc_aggregate_sumsq, double *mc_per_snp_sumsq
+        double *mc_aggregate_sumsq, double *mc_per_snp_sumsq, const T *C, const T *R, int64_t p
 #define P2M_CALL(T)                                                                             \
     guarded([&] {                                                                               \
         phase2_bed_impl<T>(bed_prefix, fam_path, blk_start, blk_end, row_sel, n_row_sel, ddof,  \
                            inv_left, L, tile_nvecs, Xz2d, xz_rows, xz_cols, meansq_accum,       \
                            M_rows, K, N_denom, LDS_IMPUTE_HWE, has_impute_seed, impute_seed,    \
-                           mc_aggregate_sumsq, mc_per_snp_sumsq);                               \
+                           mc_aggregate_sumsq, mc_per_snp_sumsq, C, R, p, 1);                   \
     })
 LDS_API int lds_phase2_accum_XtXz_bed_mailman_f32(P2M_ARGS(float)) { return P2M_CALL(float); }
 LDS_API int lds_phase2_accum_XtXz_bed_mailman_f64(P2M_ARGS(double)) { return P2M_CALL(double); }
@@ -2567,15 +3108,109 @@ LDS_API int lds_standardize_dosage_inplace_f64(double* G, int64_t N, int64_t L, 
     const char *bed_prefix, const char *fam_path, int nsnps, int step_size,                     \
         const int64_t *row_sel, int64_t n_row_sel, int ddof, double eps, int impute_mode,       \
         int has_impute_seed, uint64_t impute_seed, T *inv_out, const T *C, const T *R,          \
-        int64_t p, double *snp_var_out
+        int64_t p, double *snp_var_out, int compute_mu22, const T *annot_all, int64_t annot_rows, \
+        int64_t B, double *mu22_out
 #define RV_CALL(T)                                                                              \
     guarded([&] {                                                                               \
-        (void)step_size;                                                                        \
+        if (step_size <= 0)                                                                     \
+            fail(LDS_ERR_ARG, "step_size must be > 0 in precompute_residual_variances_bed");     \
+        if (compute_mu22 && !mu22_out) fail(LDS_ERR_ARG, "mu22_out is NULL");                   \
         resvar_impl<T>(bed_prefix, fam_path, nsnps, row_sel, n_row_sel, ddof, eps, impute_mode, \
-                       has_impute_seed, impute_seed, inv_out, C, R, p, snp_var_out);            \
+                       has_impute_seed, impute_seed, inv_out, C, R, p, snp_var_out, annot_all,  \
+                       annot_rows, B, compute_mu22 ? mu22_out : nullptr);                       \
     })
 LDS_API int lds_precompute_residual_variances_bed_f32(RV_ARGS(float)) { return RV_CALL(float); }
 LDS_API int lds_precompute_residual_variances_bed_f64(RV_ARGS(double)) { return RV_CALL(double); }
+
+#define P1G_ARGS(T)                                                                             \
+    const T *geno, int64_t N, int64_t L, int blk_start, const T *annot_blk, int64_t annot_rows,  \
+        int64_t K, const T *inv_right, int v_start, int v_count, int kmax_hint, int rand_dist,  \
+        int has_seed, uint64_t seed, T *Xz2d_chunk, int64_t xz_rows, int64_t xz_cols,            \
+        uint8_t *bin_init_mask, const T *C, const T *R, int64_t p, const T *resvar_gram,         \
+        T *inv_out, double resvar_eps
+#define P1G_CALL(T)                                                                             \
+    guarded([&] {                                                                               \
+        (void)kmax_hint;                                                                        \
+        phase1_geno_impl<T>(geno, N, L, blk_start, annot_blk, annot_rows, K, inv_right, v_start, \
+                            v_count, rand_dist, has_seed, seed, Xz2d_chunk, xz_rows, xz_cols,   \
+                            bin_init_mask, inv_out, resvar_eps, C, R, p, resvar_gram);          \
+    })
+LDS_API int lds_phase1_compute_Xz_geno_chunk_f32(P1G_ARGS(float)) { return P1G_CALL(float); }
+LDS_API int lds_phase1_compute_Xz_geno_chunk_f64(P1G_ARGS(double)) { return P1G_CALL(double); }
+
+#define P2G_ARGS(T)                                                                             \
+    T *geno, int64_t N, int64_t L, int blk_start, const T *inv_left, int64_t L_in, int tile_nvecs, \
+        const T *Xz2d, int64_t xz_rows, int64_t xz_cols, T *meansq_accum, int64_t M_rows,        \
+        int64_t K, const T *C, const T *R, int64_t p, int N_denom, double *mc_aggregate_sumsq,   \
+        double *mc_per_snp_sumsq
+#define P2G_CALL(T)                                                                             \
+    guarded([&] {                                                                               \
+        phase2_geno_impl<T>(geno, N, L, blk_start, inv_left, L_in, tile_nvecs, Xz2d, xz_rows,   \
+                            xz_cols, meansq_accum, M_rows, K, C, R, p, N_denom,                 \
+                            mc_aggregate_sumsq, mc_per_snp_sumsq);                              \
+    })
+LDS_API int lds_phase2_accum_XtXz_geno_f32(P2G_ARGS(float)) { return P2G_CALL(float); }
+LDS_API int lds_phase2_accum_XtXz_geno_f64(P2G_ARGS(double)) { return P2G_CALL(double); }
+
+// Legacy direct form (gwldcore.cpp:2132-2327): meansq += the guarded
+// sum_c Work^2 inv^2 / (nvecs (N_denom - 1)^2); no Monte-Carlo sums.
+#define P2L_ARGS(T)                                                                             \
+    const char *bed_prefix, const char *fam_path, int blk_start, int blk_end,                   \
+        const int64_t *row_sel, int64_t n_row_sel, int ddof, const T *inv_left, int64_t L,      \
+        int nvecs, const T *Xz2d, int64_t xz_rows, int64_t xz_cols, T *meansq, int64_t M_rows,  \
+        int64_t K, const T *C, const T *R, int64_t p, int N_denom, int impute_mode,             \
+        int has_impute_seed, uint64_t impute_seed
+#define P2L_CALL(T)                                                                             \
+    guarded([&] {                                                                               \
+        if (nvecs <= 0 || xz_cols % nvecs)                                                      \
+            fail(LDS_ERR_ARG, "Xz2d col count must be multiple of nvecs");                       \
+        phase2_bed_impl<T>(bed_prefix, fam_path, blk_start, blk_end, row_sel, n_row_sel, ddof,  \
+                           inv_left, L, nvecs, Xz2d, xz_rows, xz_cols, meansq, M_rows, K,       \
+                           N_denom, impute_mode, has_impute_seed, impute_seed, nullptr, nullptr, \
+                           C, R, p, 0, 1.0 / (double)nvecs, "direct");                          \
+    })
+LDS_API int lds_phase2_compute_XtXz_bed_f32(P2L_ARGS(float)) { return P2L_CALL(float); }
+LDS_API int lds_phase2_compute_XtXz_bed_f64(P2L_ARGS(double)) { return P2L_CALL(double); }
+
+#define GRM_ARGS(T)                                                                             \
+    const char *bed_prefix, const char *fam_path, int nsnps, int step_size,                     \
+        const int64_t *row_sel, int64_t n_row_sel, int ddof, const T *inv_all, int64_t n_inv,   \
+        const T *panel_in, T *panel_out, int64_t rows, int64_t Q, const T *C, const T *R,       \
+        int64_t p, int impute_mode, int has_impute_seed, uint64_t impute_seed
+#define GRM_CALL(T)                                                                             \
+    guarded([&] {                                                                               \
+        apply_grm_impl<T>(bed_prefix, fam_path, nsnps, step_size, row_sel, n_row_sel, ddof,     \
+                          inv_all, n_inv, panel_in, panel_out, rows, Q, C, R, p, impute_mode,   \
+                          has_impute_seed, impute_seed, "apply_grm_bed_panel");                 \
+    })
+LDS_API int lds_apply_grm_bed_panel_f32(GRM_ARGS(float)) { return GRM_CALL(float); }
+LDS_API int lds_apply_grm_bed_panel_f64(GRM_ARGS(double)) { return GRM_CALL(double); }
+
+// Mailman form (gwldcore.cpp:1256-1497): HWE-completed genotypes.
+#define GRMM_ARGS(T)                                                                            \
+    const char *bed_prefix, const char *fam_path, int nsnps, int step_size,                     \
+        const int64_t *row_sel, int64_t n_row_sel, int ddof, const T *inv_all, int64_t n_inv,   \
+        const T *panel_in, T *panel_out, int64_t rows, int64_t Q, const T *C, const T *R,       \
+        int64_t p, int has_impute_seed, uint64_t impute_seed
+#define GRMM_CALL(T)                                                                            \
+    guarded([&] {                                                                               \
+        apply_grm_impl<T>(bed_prefix, fam_path, nsnps, step_size, row_sel, n_row_sel, ddof,     \
+                          inv_all, n_inv, panel_in, panel_out, rows, Q, C, R, p, LDS_IMPUTE_HWE, \
+                          has_impute_seed, impute_seed, "apply_grm_bed_panel_mailman");         \
+    })
+LDS_API int lds_apply_grm_bed_panel_mailman_f32(GRMM_ARGS(float)) { return GRMM_CALL(float); }
+LDS_API int lds_apply_grm_bed_panel_mailman_f64(GRMM_ARGS(double)) { return GRMM_CALL(double); }
+
+#define BCB_ARGS(T)                                                                             \
+    const double *meansq_raw, int64_t M, int64_t B, const double *mu22, const T *annot_all,     \
+        int N, double d, double *R2, double *rho2, double *bias, double *delta
+#define BCB_CALL(T)                                                                             \
+    guarded([&] {                                                                               \
+        block_corrections_impl<T>(meansq_raw, mu22, annot_all, M, B, N, d, R2, rho2, bias,      \
+                                  delta);                                                       \
+    })
+LDS_API int lds_compute_block_corrections_binary_f32(BCB_ARGS(float)) { return BCB_CALL(float); }
+LDS_API int lds_compute_block_corrections_binary_f64(BCB_ARGS(double)) { return BCB_CALL(double); }
 
 LDS_API int lds_gw_ldscore(const uint8_t* bed_rows, int64_t bed_row_bytes, int64_t n_total,
                            int64_t M, const int64_t* row_sel, int64_t n_row_sel,

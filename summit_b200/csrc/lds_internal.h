@@ -242,6 +242,36 @@ void launch_mlp_adam(float* p, float* m, float* v, const float* g, int64_t P, fl
                      float b2, float eps, float bc1, float bc2, cudaStream_t st);
 
 // Launch accounting.
+// ---- dense FP64 work (lds_dense.cu) ----
+// C[m, n] = alpha sum_k A(m, k) B(k, n) + beta C[m, n] with
+// A(m, k) = A[m a_ms + kk a_ks] (kk = a_kidx[k] when a_kidx is set; squared
+// when a_square), B(k, n) = B[k b_ks + n b_ns], C[m c_ms + n c_ns]; beta == 0
+// does not read C.
+struct DGemmArgs {
+    int64_t M = 0, N = 0, K = 0;
+    const double* A = nullptr;
+    int64_t a_ms = 1, a_ks = 1;
+    const int32_t* a_kidx = nullptr;
+    int a_square = 0;
+    const double* B = nullptr;
+    int64_t b_ks = 1, b_ns = 1;
+    double* C = nullptr;
+    int64_t c_ms = 1, c_ns = 1;
+    double alpha = 1.0, beta = 0.0;
+};
+void launch_dgemm(const DGemmArgs& a, cudaStream_t st);
+void launch_dense_p2_epilogue(const double* W, int64_t L, int K, int V, const double* ls,
+                              double* accum, double* mc, unsigned long long* guards,
+                              double extreme_warn, int drop_extreme, cudaStream_t st);
+void launch_decode_standardized(const DevGeno& g, int64_t j0, int64_t L, const double* mean,
+                                const double* sdinv, double* X, int64_t ldx, cudaStream_t st);
+void launch_col_sumsq(const double* X, int64_t N, int64_t ld, int64_t L, double* ss,
+                      cudaStream_t st);
+template <typename Tann>
+void launch_block_corrections(const double* meansq, const double* mu22, const Tann* annot,
+                              int64_t M, int B, double N, double d, double* R2, double* rho2,
+                              double* bias, double* delta, cudaStream_t st);
+
 void count_launch();
 
 // Set the text returned by lds_last_error() for the calling thread.

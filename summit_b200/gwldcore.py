@@ -146,10 +146,13 @@ def phase1_compute_Xz_bed_chunk(bed_prefix, fam_path, blk_start, blk_end, row_se
     _rw(Xz, dt, "F", "Xz2d_chunk")
     if Xz.ndim != 2:
         raise RuntimeError("Xz2d_chunk shape must be (N, B*v_count)")
-    if project_right:
-        raise RuntimeError("project_right is not supported by the B200 backend; project Xz2d "
-                           "after phase 1 (project_colmajor_inplace), as gw_ldscore.py does")
-    Cf, Rf, p, G = _cov(C, R, dt, resvar_gram) if inv_out is not None else (None, None, 0, None)
+    if inv_out is not None:
+        Cf, Rf, p, G = _cov(C, R, dt, resvar_gram)
+    elif project_right:
+        Cf, Rf, p = _cr(C, R, dt, Xz.shape[0], "phase1")
+        G = None
+    else:
+        Cf, Rf, p, G = None, None, 0, None
     ann = np.ascontiguousarray(_need("annot_blk", annot_blk), dtype=dt)
     if ann.ndim != 2:
         raise RuntimeError("L mismatch")
@@ -174,7 +177,45 @@ def phase1_compute_Xz_bed_chunk(bed_prefix, fam_path, blk_start, blk_end, row_se
              int(seed is not None), 0 if seed is None else int(seed) & (2**64 - 1), ptr(Xz),
              Xz.shape[0], Xz.shape[1], ptr(bin_init_mask), _impute(impute_mode),
              int(impute_seed is not None), 0 if impute_seed is None else int(impute_seed),
-             ptr(inv_out), float(resvar_eps), ptr(Cf), ptr(Rf), p, ptr(G)))
+             ptr(inv_out), float(resvar_eps), ptr(Cf), ptr(Rf), p, ptr(G), int(bool(project_right))))
+
+
+def phase1_compute_Xz_geno_chunk(Geno, blk_start, annot_blk=_REQUIRED, inv_right=_REQUIRED,
+                                 v_start=_REQUIRED, v_count=_REQUIRED, kmax_hint=_REQUIRED,
+                                 rand_dist="rademacher", seed=None, Xz2d_chunk=_REQUIRED,
+                                 bin_init_mask=None, C=None, R=None, resvar_gram=None,
+                                 inv_out=None, resvar_eps=1e-10):
+    """Phase 1 from a dense standardized genotype block (gwldcore.cpp:3690-3701)."""
+    t = _tsuffix(Geno)
+    dt = Geno.dtype
+    G = _rw(Geno, dt, "F", "Geno")
+    Xz = _rw(_need("Xz2d_chunk", Xz2d_chunk), dt, "F", "Xz2d_chunk")
+    ann = np.ascontiguousarray(_need("annot_blk", annot_blk), dtype=dt)
+    if ann.ndim != 2:
+        raise RuntimeError("L mismatch")
+    Cf, Rf, p, Gr = (None, None, 0, None)
+    inv_r = None
+    if inv_out is not None:
+        _rw(inv_out, dt, "C", "inv_out")
+        if inv_out.shape[0] != G.shape[1]:
+            raise RuntimeError("inv_out shape mismatch in phase1 fused residual variance")
+        Cf, Rf, p, Gr = _cov(C, R, dt, resvar_gram)
+        if p and Cf.shape[0] != G.shape[0]:
+            raise RuntimeError("C/R shape mismatch in fused residual variances")
+    else:
+        inv_r = np.ascontiguousarray(_need("inv_right", inv_right), dtype=dt)
+        if inv_r.shape[0] != G.shape[1]:
+            raise RuntimeError("inv_right shape mismatch in phase1")
+    if bin_init_mask is not None:
+        _rw(bin_init_mask, np.uint8, "C", "bin_init_mask")
+        if bin_init_mask.shape[0] != ann.shape[1]:
+            raise RuntimeError("bin_init_mask shape mismatch in phase1")
+    fn = getattr(_lib.load(), f"lds_phase1_compute_Xz_geno_chunk_{t}")
+    check(fn(ptr(G), G.shape[0], G.shape[1], int(blk_start), ptr(ann), ann.shape[0], ann.shape[1],
+             ptr(inv_r), int(_need("v_start", v_start)), int(_need("v_count", v_count)),
+             int(_need("kmax_hint", kmax_hint)), _dist(rand_dist), int(seed is not None),
+             0 if seed is None else int(seed) & (2**64 - 1), ptr(Xz), Xz.shape[0], Xz.shape[1],
+             ptr(bin_init_mask), ptr(Cf), ptr(Rf), p, ptr(Gr), ptr(inv_out), float(resvar_eps)))
 
 
 # ---------------------------------------------------------------------------
@@ -184,9 +225,6 @@ def phase2_accum_XtXz_bed(bed_prefix, fam_path, blk_start, blk_end, row_sel=None
                           inv_left=_REQUIRED, tile_nvecs=_REQUIRED, Xz2d=_REQUIRED,
                           meansq_accum=_REQUIRED, C=None, R=None, N_denom=0, impute_mode="hwe",
                           impute_seed=None, mc_aggregate_sumsq=None, mc_per_snp_sumsq=None):
-    if C is not None and R is not None:
-        raise RuntimeError("covariate projection inside phase 2 is not supported by the B200 "
-                           "backend; pass the projected sketch with C=R=None as gw_ldscore.py does")
     ms = _need("meansq_accum", meansq_accum)
     t = _tsuffix(ms)
     dt = ms.dtype
@@ -203,6 +241,7 @@ def phase2_accum_XtXz_bed(bed_prefix, fam_path, blk_start, blk_end, row_sel=None
         _rw(mc_per_snp_sumsq, np.float64, "C", "mc_per_snp_sumsq")
         if mc_per_snp_sumsq.shape != ms.shape:
             raise RuntimeError("mc_per_snp_sumsq shape must match meansq_accum")
+    Cf, Rf, p = _cr(C, R, dt, Xz.shape[0], "phase2_accum_XtXz_bed")
     rows, nr = _rows(row_sel)
     fn = getattr(_lib.load(), f"lds_phase2_accum_XtXz_bed_{t}")
     check(fn(enc(bed_prefix), enc(fam_path), int(blk_start), int(blk_end), ptr(rows), nr,
@@ -210,7 +249,60 @@ def phase2_accum_XtXz_bed(bed_prefix, fam_path, blk_start, blk_end, row_sel=None
              Xz.shape[0], Xz.shape[1], ptr(ms), ms.shape[0], ms.shape[1], int(N_denom),
              _impute(impute_mode), int(impute_seed is not None),
              0 if impute_seed is None else int(impute_seed), ptr(mc_aggregate_sumsq),
+             ptr(mc_per_snp_sumsq), ptr(Cf), ptr(Rf), p))
+
+
+def phase2_accum_XtXz_geno(Geno, blk_start, inv_left=_REQUIRED, tile_nvecs=_REQUIRED,
+                           Xz2d=_REQUIRED, meansq_accum=_REQUIRED, C=None, R=None, N_denom=0,
+                           mc_aggregate_sumsq=None, mc_per_snp_sumsq=None):
+    """Phase 2 from a dense standardized genotype block (gwldcore.cpp:3772-3783);
+    with C and R the block is projected in place, as the reference does."""
+    t = _tsuffix(Geno)
+    dt = Geno.dtype
+    G = _rw(Geno, dt, "F", "Geno")
+    ms = _rw(_need("meansq_accum", meansq_accum), dt, "C", "meansq_accum")
+    Xz = np.asfortranarray(_need("Xz2d", Xz2d), dtype=dt)
+    inv = np.ascontiguousarray(_need("inv_left", inv_left), dtype=dt)
+    if ms.ndim != 2:
+        raise RuntimeError("meansq_accum shape mismatch in phase2_accum_XtXz_bed")
+    if mc_aggregate_sumsq is not None:
+        _rw(mc_aggregate_sumsq, np.float64, "C", "mc_aggregate_sumsq")
+        if mc_aggregate_sumsq.shape[0] != ms.shape[1]:
+            raise RuntimeError("mc_aggregate_sumsq length must equal the annotation count")
+    if mc_per_snp_sumsq is not None:
+        _rw(mc_per_snp_sumsq, np.float64, "C", "mc_per_snp_sumsq")
+        if mc_per_snp_sumsq.shape != ms.shape:
+            raise RuntimeError("mc_per_snp_sumsq shape must match meansq_accum")
+    Cf, Rf, p = _cr(C, R, dt, G.shape[0], "phase2_accum_XtXz_bed")
+    fn = getattr(_lib.load(), f"lds_phase2_accum_XtXz_geno_{t}")
+    check(fn(ptr(G), G.shape[0], G.shape[1], int(blk_start), ptr(inv), inv.shape[0],
+             int(_need("tile_nvecs", tile_nvecs)), ptr(Xz), Xz.shape[0], Xz.shape[1], ptr(ms),
+             ms.shape[0], ms.shape[1], ptr(Cf), ptr(Rf), p, int(N_denom), ptr(mc_aggregate_sumsq),
              ptr(mc_per_snp_sumsq)))
+
+
+def phase2_compute_XtXz_bed(bed_prefix, fam_path, blk_start, blk_end, row_sel=None, ddof=1,
+                            inv_left=_REQUIRED, nvecs=_REQUIRED, vchunk=_REQUIRED, Xz2d=_REQUIRED,
+                            meansq=_REQUIRED, C=None, R=None, N_denom=0, impute_mode="hwe",
+                            impute_seed=None):
+    """Legacy direct phase 2 (gwldcore.cpp:3731-3740): meansq += the update / nvecs."""
+    _need("vchunk", vchunk)
+    ms = _need("meansq", meansq)
+    t = _tsuffix(ms)
+    dt = ms.dtype
+    _rw(ms, dt, "C", "meansq")
+    Xz = np.asfortranarray(_need("Xz2d", Xz2d), dtype=dt)
+    inv = np.ascontiguousarray(_need("inv_left", inv_left), dtype=dt)
+    if ms.ndim != 2:
+        raise RuntimeError("meansq shape mismatch")
+    Cf, Rf, p = _cr(C, R, dt, Xz.shape[0], "phase2_compute_XtXz_bed")
+    rows, nr = _rows(row_sel)
+    fn = getattr(_lib.load(), f"lds_phase2_compute_XtXz_bed_{t}")
+    check(fn(enc(bed_prefix), enc(fam_path), int(blk_start), int(blk_end), ptr(rows), nr,
+             int(ddof), ptr(inv), inv.shape[0], int(_need("nvecs", nvecs)), ptr(Xz), Xz.shape[0],
+             Xz.shape[1], ptr(ms), ms.shape[0], ms.shape[1], ptr(Cf), ptr(Rf), p, int(N_denom),
+             _impute(impute_mode), int(impute_seed is not None),
+             0 if impute_seed is None else int(impute_seed)))
 
 
 # ---------------------------------------------------------------------------
@@ -277,18 +369,16 @@ def phase2_accum_XtXz_bed_mailman(bed_prefix, fam_path, blk_start, blk_end, row_
                                   meansq_accum=_REQUIRED, C=None, R=None, N_denom=0,
                                   impute_seed=None, mc_aggregate_sumsq=None,
                                   mc_per_snp_sumsq=None):
-    if C is not None and R is not None:
-        raise RuntimeError("covariate projection inside phase 2 is not supported by the B200 "
-                           "backend; pass the projected sketch with C=R=None")
     t, ms, Xz, inv = _mailman_common(meansq_accum, Xz2d, "F", inv_left, mc_aggregate_sumsq,
                                      mc_per_snp_sumsq, "phase2_accum_XtXz_bed_mailman")
+    Cf, Rf, p = _cr(C, R, ms.dtype, Xz.shape[0], "phase2_accum_XtXz_bed_mailman")
     rows, nr = _rows(row_sel)
     fn = getattr(_lib.load(), f"lds_phase2_accum_XtXz_bed_mailman_{t}")
     check(fn(enc(bed_prefix), enc(fam_path), int(blk_start), int(blk_end), ptr(rows), nr,
              int(ddof), ptr(inv), inv.shape[0], int(_need("tile_nvecs", tile_nvecs)), ptr(Xz),
              Xz.shape[0], Xz.shape[1], ptr(ms), ms.shape[0], ms.shape[1], int(N_denom),
              int(impute_seed is not None), 0 if impute_seed is None else int(impute_seed),
-             ptr(mc_aggregate_sumsq), ptr(mc_per_snp_sumsq)))
+             ptr(mc_aggregate_sumsq), ptr(mc_per_snp_sumsq), ptr(Cf), ptr(Rf), p))
 
 
 def phase2_accum_XtXz_bed_mailman_rowmajor(bed_prefix, fam_path, blk_start, blk_end,
@@ -367,8 +457,12 @@ def precompute_residual_variances_bed(bed_prefix, fam_path, nsnps, step_size, ro
                                       ddof=1, eps=1e-10, compute_mu22=False, annot_all=None,
                                       C=None, R=None, impute_mode="hwe", impute_seed=None,
                                       snp_var_out=None, dtype=np.float64):
-    if compute_mu22:
-        raise RuntimeError("compute_mu22 is not supported by the B200 residual-variance entry")
+    # dtype selects the overload; an annotation or covariate array decides it
+    # when given, as the typed arrays do for the reference's two overloads
+    for a in (annot_all, C):
+        if isinstance(a, np.ndarray) and a.dtype in (np.float32, np.float64):
+            dtype = a.dtype
+            break
     t = "f32" if np.dtype(dtype) == np.float32 else "f64"
     dt = np.float32 if t == "f32" else np.float64
     out = np.empty(int(nsnps), dtype=dt)
@@ -385,13 +479,82 @@ def precompute_residual_variances_bed(bed_prefix, fam_path, nsnps, step_size, ro
         _rw(snp_var_out, np.float64, "C", "snp_var_out")
         if snp_var_out.shape[0] != int(nsnps):
             raise RuntimeError("snp_var_out shape mismatch in precompute_residual_variances_bed")
+    ann, B, mu22 = None, 0, None
+    if compute_mu22:
+        if annot_all is None:
+            raise RuntimeError("annot_all must be provided when compute_mu22=True")
+        ann = np.ascontiguousarray(annot_all, dtype=dt)
+        if ann.ndim != 2 or ann.shape[0] != int(nsnps):
+            raise RuntimeError("annot_all shape mismatch in precompute_residual_variances_bed")
+        B = ann.shape[1]
+        mu22 = np.zeros((B, B))
     rows, nr = _rows(row_sel)
     fn = getattr(_lib.load(), f"lds_precompute_residual_variances_bed_{t}")
     check(fn(enc(bed_prefix), enc(fam_path), int(nsnps), int(step_size), ptr(rows), nr, int(ddof),
              float(eps), _impute(impute_mode), int(impute_seed is not None),
              0 if impute_seed is None else int(impute_seed), ptr(out), ptr(Cf), ptr(Rf), p,
-             ptr(snp_var_out)))
-    return out, None
+             ptr(snp_var_out), int(bool(compute_mu22)), ptr(ann),
+             0 if ann is None else ann.shape[0], B, ptr(mu22)))
+    return out, mu22
+
+
+def compute_block_corrections_binary(meansq_raw, mu22, annot_all, N, d):
+    """R2, rho2, bias and delta (B x B each) of binary annotations
+    (gwldcore.cpp:3807-3810, impl :3569-3627)."""
+    A = np.asarray(annot_all)
+    t = _tsuffix(A)
+    A = np.ascontiguousarray(A)
+    m = np.ascontiguousarray(meansq_raw, dtype=np.float64)
+    u = np.ascontiguousarray(mu22, dtype=np.float64)
+    M, B = m.shape
+    if u.shape != (B, B):
+        raise RuntimeError("mu22 shape mismatch")
+    if A.shape != (M, B):
+        raise RuntimeError("annot_all shape mismatch")
+    out = [np.zeros((B, B)) for _ in range(4)]
+    check(getattr(_lib.load(), f"lds_compute_block_corrections_binary_{t}")(
+        ptr(m), M, B, ptr(u), ptr(A), int(N), float(d), *[ptr(o) for o in out]))
+    return tuple(out)
+
+
+def _grm(name, bed_prefix, fam_path, nsnps, step_size, row_sel, ddof, inv_all, panel_in,
+         panel_out, C, R):
+    pout = _need("panel_out", panel_out)
+    t = _tsuffix(pout)
+    dt = pout.dtype
+    _rw(pout, dt, "F", "panel_out")
+    pin = np.asfortranarray(_need("panel_in", panel_in), dtype=dt)
+    inv = np.ascontiguousarray(_need("inv_all", inv_all), dtype=dt)
+    if pin.shape[0] != pout.shape[0]:
+        raise RuntimeError(f"panel row mismatch in {name}")
+    if pin.shape[1] != pout.shape[1]:
+        raise RuntimeError(f"panel col mismatch in {name}")
+    Cf, Rf, p = _cr(C, R, dt, pin.shape[0], name)
+    rows, nr = _rows(row_sel)
+    head = (enc(bed_prefix), enc(fam_path), int(nsnps), int(step_size), ptr(rows), nr, int(ddof),
+            ptr(inv), inv.shape[0], ptr(pin), ptr(pout), pin.shape[0], pin.shape[1], ptr(Cf),
+            ptr(Rf), p)
+    return head, getattr(_lib.load(), f"lds_{name}_{t}")
+
+
+def apply_grm_bed_panel(bed_prefix, fam_path, nsnps, step_size, row_sel=None, ddof=1,
+                        inv_all=_REQUIRED, panel_in=_REQUIRED, panel_out=_REQUIRED, C=None,
+                        R=None, impute_mode="hwe", impute_seed=None) -> None:
+    """panel_out = P X D X^T P panel_in (gwldcore.cpp:3812-3820)."""
+    head, fn = _grm("apply_grm_bed_panel", bed_prefix, fam_path, nsnps, step_size, row_sel, ddof,
+                    inv_all, panel_in, panel_out, C, R)
+    check(fn(*head, _impute(impute_mode), int(impute_seed is not None),
+             0 if impute_seed is None else int(impute_seed)))
+
+
+def apply_grm_bed_panel_mailman(bed_prefix, fam_path, nsnps, step_size, row_sel=None, ddof=1,
+                                inv_all=_REQUIRED, panel_in=_REQUIRED, panel_out=_REQUIRED,
+                                C=None, R=None, impute_seed=None) -> None:
+    """Mailman form on HWE-completed genotypes (gwldcore.cpp:3821-3828)."""
+    head, fn = _grm("apply_grm_bed_panel_mailman", bed_prefix, fam_path, nsnps, step_size,
+                    row_sel, ddof, inv_all, panel_in, panel_out, C, R)
+    check(fn(*head, int(impute_seed is not None),
+             0 if impute_seed is None else int(impute_seed)))
 
 
 # ---------------------------------------------------------------------------
