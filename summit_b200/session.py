@@ -295,5 +295,8 @@ def window_seed(seed: int, w: int) -> int:
 
 
 def set_stream(stream_ptr: int | None) -> None:
-    """Launch library kernels on an external CUDA stream (e.g. torch.cuda.Stream.cuda_stream)."""
+    """Launch library kernels on an external CUDA stream (e.g. torch.cuda.Stream.cuda_stream).
+
+    0 / None restores the library's own stream, so the legacy default stream
+    (torch's default stream, handle 0) cannot be selected: use a created stream."""
     check(_lib.load().lds_set_stream(None if not stream_ptr else C.c_void_p(stream_ptr)))

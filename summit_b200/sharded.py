@@ -13,12 +13,13 @@ unsharded one up to the order of the final FP64 sums.  The annotation totals
 M_k of the finalize and the Monte-Carlo aggregate sums are all-reduced too.
 
 ``ShardedGw.run`` is the driver; the shard's work comes from an engine:
-``DeviceShard`` runs it on liblds's kernels (sketch buffers in device memory,
-the library on torch's current stream so the NCCL all-reduce orders after
-phase 1 and before phase 2).
+``DeviceShard`` runs it on liblds's kernels (sketch buffers in device memory;
+the library and torch share one created stream, so the NCCL all-reduce is
+ordered after phase 1 and before phase 2).
 """
 from __future__ import annotations
 
+import contextlib
 from dataclasses import dataclass
 
 import numpy as np
@@ -51,7 +52,11 @@ class DeviceShard:
 
         self.torch = torch
         self.device = torch.device("cuda", torch.cuda.current_device())
-        set_stream(torch.cuda.current_stream().cuda_stream)
+        # A stream of its own shared by the library and torch (and so the NCCL
+        # all-reduce): torch's default stream has the handle 0, which the
+        # library reads as "use your own stream".
+        self.stream = torch.cuda.Stream()
+        set_stream(self.stream.cuda_stream)
         self.session = GwSession(bed_rows, n_total, "mean", 0, ddof, row_sel)
         self.plan = self.session.shard_plan(annot, nvecs, step_size, seed, snp_offset, rand_dist,
                                             vtile, eps, as_float, with_mc)
@@ -60,6 +65,10 @@ class DeviceShard:
         self.N = self.session.N
         self.ddof = ddof
         self._sizes, self._rows = self.plan.tiles()
+
+    def context(self):
+        """Run torch work (sketch buffers, collectives) on the library's stream."""
+        return self.torch.cuda.stream(self.stream)
 
     def tile_sizes(self) -> list[int]:
         return list(self._sizes)
@@ -137,15 +146,17 @@ class ShardedGw:
         if b1 - b0 != self.engine.M:
             raise ValueError(f"rank {rank} holds {self.engine.M} SNPs, its shard is [{b0}, {b1})")
         eng = self.engine
-        # every rank takes the same collective steps in the same order
-        eng.set_bin_totals(self._allreduce_np(eng.bin_totals()))
-        for t in range(len(eng.tile_sizes())):
-            y = eng.new_sketch(t)
-            eng.phase1(t, y)
-            if dist is not None and world > 1:
-                dist.all_reduce(y, group=self.group)
-            eng.phase2(t, y)
-        loc = eng.results()
+        ctx = eng.context() if hasattr(eng, "context") else contextlib.nullcontext()
+        with ctx:
+            # every rank takes the same collective steps in the same order
+            eng.set_bin_totals(self._allreduce_np(eng.bin_totals()))
+            for t in range(len(eng.tile_sizes())):
+                y = eng.new_sketch(t)
+                eng.phase1(t, y)
+                if dist is not None and world > 1:
+                    dist.all_reduce(y, group=self.group)
+                eng.phase2(t, y)
+            loc = eng.results()
         mca = loc.get("mc_aggregate_sumsq")
         if mca is not None:
             mca = self._allreduce_np(mca)

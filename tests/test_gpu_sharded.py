@@ -41,33 +41,36 @@ def test_device_shards_match_unsharded(oracle, world, vtile):
     n, m, K, step, nvecs, seed = 1000, 2600, 4, 250, 150, 21
     rows, annot = _case(n, m, K, 5)
     want = oracle.gw_ldscore(rows, n, annot, nvecs, step, seed, vtile=vtile, with_mc=True)
-    stream = torch.cuda.current_stream()
+    # one non-default stream for the library and torch (torch's default
+    # stream has the handle 0, which lds_set_stream reads as "own stream")
+    stream = torch.cuda.Stream()
     set_stream(stream.cuda_stream)
     try:
-        sess, plans = [], []
-        bounds = shard_bounds(m, world, step)
-        for s, e in bounds:
-            g = GwSession(rows[s:e], n)
-            sess.append(g)
-            plans.append(g.shard_plan(annot[s:e], nvecs, step, seed, s, vtile=vtile,
-                                      with_mc=True))
-        sizes, nrows = plans[0].tiles()
-        assert all(p.tiles() == (sizes, nrows) for p in plans)
-        assert sum(sizes) == nvecs
-        Mk = np.sum([p.bin_totals() for p in plans], axis=0)
-        np.testing.assert_allclose(Mk, annot.sum(axis=0), rtol=1e-14)
-        for p in plans:
-            p.set_bin_totals(Mk)
-        for t, V in enumerate(sizes):
-            parts = [torch.empty((K * V, nrows), dtype=torch.float64, device="cuda")
-                     for _ in plans]
-            for p, y in zip(plans, parts):
-                p.phase1(t, y.data_ptr())
-            total = torch.stack(parts).sum(0)
-            assert torch.isfinite(total).all()
+        with torch.cuda.stream(stream):
+            sess, plans = [], []
+            bounds = shard_bounds(m, world, step)
+            for s, e in bounds:
+                g = GwSession(rows[s:e], n)
+                sess.append(g)
+                plans.append(g.shard_plan(annot[s:e], nvecs, step, seed, s, vtile=vtile,
+                                          with_mc=True))
+            sizes, nrows = plans[0].tiles()
+            assert all(p.tiles() == (sizes, nrows) for p in plans)
+            assert sum(sizes) == nvecs
+            Mk = np.sum([p.bin_totals() for p in plans], axis=0)
+            np.testing.assert_allclose(Mk, annot.sum(axis=0), rtol=1e-14)
             for p in plans:
-                p.phase2(t, total.data_ptr())
-        res = [p.results() for p in plans]
+                p.set_bin_totals(Mk)
+            for t, V in enumerate(sizes):
+                parts = [torch.empty((K * V, nrows), dtype=torch.float64, device="cuda")
+                         for _ in plans]
+                for p, y in zip(plans, parts):
+                    p.phase1(t, y.data_ptr())
+                total = torch.stack(parts).sum(0)
+                assert torch.isfinite(total).all()
+                for p in plans:
+                    p.phase2(t, total.data_ptr())
+            res = [p.results() for p in plans]
         torch.cuda.synchronize()
     finally:
         set_stream(None)
