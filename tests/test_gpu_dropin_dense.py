@@ -38,6 +38,15 @@ def _tol(dt):
     return 1e-4 if dt == np.float32 else 1e-10
 
 
+@pytest.fixture(autouse=True)
+def _fresh_reference_caches(reference):
+    """The reference caches phase-1 CSR lists keyed by the annotation and
+    inverse-sd buffer ADDRESSES (gwldcore.cpp:1065-1100); numpy reuses freed
+    addresses between tests, so a stale list would be returned.  Clear it."""
+    reference.clear_caches()
+    yield
+
+
 @pytest.mark.parametrize("dt", [np.float64, np.float32])
 @pytest.mark.parametrize("fused", [False, True])
 def test_phase1_geno_matches_reference(reference, dt, fused):
