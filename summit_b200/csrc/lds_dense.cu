@@ -183,6 +183,62 @@ __global__ void block_corrections_kernel(const double* __restrict__ meansq,
     delta[t] = de;
 }
 
+// Column restandardization over N rows with ddof 0 (restandardize_cols_inplace,
+// winldcore.cpp:215-267): x <- (x - mean) / sd, sd = 1 when the column has
+// no spread.  One thread per column, rows in order.
+__global__ void restandardize_cols_kernel(double* __restrict__ X, int64_t N, int64_t ld,
+                                          int64_t L) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= L) return;
+    double* col = X + j * ld;
+    double sum = 0.0, sumsq = 0.0;
+    for (int64_t i = 0; i < N; ++i) {
+        const double x = col[i];
+        sum += x;
+        sumsq += x * x;
+    }
+    const double mean = sum / (double)N;
+    double ss = sumsq - (sum * sum) / (double)N;
+    if (ss < 0.0 && ss > -1e-12) ss = 0.0;
+    double inv_sd = 1.0;
+    if (ss > 0.0 && isfinite(ss)) {
+        const double var = ss / (double)N;
+        if (var > 0.0 && isfinite(var)) inv_sd = 1.0 / sqrt(var);
+    }
+    for (int64_t i = 0; i < N; ++i) col[i] = (col[i] - mean) * inv_sd;
+}
+
+// Windowed LD of a row chunk from its FP64 Gram panel S (rows x P,
+// column-major, column i - p0): out[r, k] += sum_{i in [lo_r, hi_r)} f(r_ri)
+// annot[i, k] with r = S / N and f = r^2 or the unbiased r^2 - (1 - r^2) / (d - 1).
+// One warp per row; lane partial sums in shared memory, summed in lane order.
+constexpr int kWinWarps = 4;
+__global__ void __launch_bounds__(kWinWarps * 32)
+    window_cov_epilogue_kernel(const double* __restrict__ S, int64_t rows, int64_t p0,
+                               const int64_t* __restrict__ lo, const int64_t* __restrict__ hi,
+                               const double* __restrict__ annot, int64_t annot_row0, int K,
+                               double invN, double corr_den, double* __restrict__ out) {
+    extern __shared__ double acc[];  // [warp][k][lane]
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t r = (int64_t)blockIdx.x * kWinWarps + w;
+    if (r >= rows) return;
+    double* a = acc + (int64_t)w * K * 32;
+    for (int k = 0; k < K; ++k) a[k * 32 + lane] = 0.0;
+    for (int64_t i = lo[r] + lane; i < hi[r]; i += 32) {
+        const double rr = S[r + (i - p0) * rows] * invN;
+        const double r2 = rr * rr;
+        const double f = corr_den > 0.0 ? r2 - (1.0 - r2) * corr_den : r2;
+        const double* an = annot + (i - annot_row0) * K;
+        for (int k = 0; k < K; ++k) a[k * 32 + lane] += f * an[k];
+    }
+    __syncwarp();
+    for (int k = lane; k < K; k += 32) {
+        double t = 0.0;
+        for (int l = 0; l < 32; ++l) t += a[k * 32 + l];
+        out[r * K + k] += t;
+    }
+}
+
 unsigned grid_for_n(int64_t n, int threads) {
     const int64_t b = (n + threads - 1) / threads;
     return (unsigned)(b < 148 * 32 ? (b > 0 ? b : 1) : 148 * 32);
@@ -219,6 +275,31 @@ void launch_col_sumsq(const double* X, int64_t N, int64_t ld, int64_t L, double*
                       cudaStream_t st) {
     if (L <= 0) return;
     col_sumsq_kernel<<<(unsigned)((L + 127) / 128), 128, 0, st>>>(X, N, ld, L, ss);
+    count_launch();
+}
+
+void launch_restandardize_cols(double* X, int64_t N, int64_t ld, int64_t L, cudaStream_t st) {
+    if (L <= 0) return;
+    restandardize_cols_kernel<<<(unsigned)((L + 127) / 128), 128, 0, st>>>(X, N, ld, L);
+    count_launch();
+}
+
+int window_cov_max_bins() { return (int)(200 * 1024 / (kWinWarps * 32 * sizeof(double))); }
+
+void launch_window_cov_epilogue(const double* S, int64_t rows, int64_t p0, const int64_t* lo,
+                                const int64_t* hi, const double* annot, int64_t annot_row0, int K,
+                                double invN, double corr_den, double* out, cudaStream_t st) {
+    if (rows <= 0 || K <= 0) return;
+    const size_t smem = (size_t)kWinWarps * K * 32 * sizeof(double);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(window_cov_epilogue_kernel,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        attr = true;
+    }
+    window_cov_epilogue_kernel<<<(unsigned)((rows + kWinWarps - 1) / kWinWarps), kWinWarps * 32,
+                                 smem, st>>>(S, rows, p0, lo, hi, annot, annot_row0, K, invN,
+                                             corr_den, out);
     count_launch();
 }
 

@@ -3475,6 +3475,70 @@ LDS_API int lds_geno_window_ld(int64_t geno, int64_t row0, int64_t row1, const i
     });
 }
 
+// Exact windowed LD scores with covariates (winldcore.cpp:340-366 and
+// :783-931): the genotypes of each partner range are projected,
+// X <- (I - C R) X, and restandardized over the N rows (ddof 0), so r is no
+// longer an integer Gram: dense FP64 panels and FP64 Gram products per chunk
+// of rows, then the masked f(r) annotation sums.
+static void window_ld_cov_impl(Context& c, const Prepared& P, int64_t row0, int64_t row1,
+                               const int64_t* lo, const int64_t* hi, const double* annot,
+                               int64_t K, double corr_dim, const DevCov& cv, double* out,
+                               int64_t ld_row, int64_t ld_col) {
+    const int64_t m = row1 - row0, N = P.g.N;
+    if (K > window_cov_max_bins())
+        fail(LDS_ERR_ARG, "at most %d annotation columns with covariates", window_cov_max_bins());
+    DevBuf dann, dlo, dhi, dout, dX, dS, dtmp;
+    double* an = dann.as<double>((size_t)(m * K));
+    h2d(an, annot, (size_t)(m * K), c.st);
+    int64_t* dl = dlo.as<int64_t>((size_t)m);
+    int64_t* dh = dhi.as<int64_t>((size_t)m);
+    h2d(dl, lo, (size_t)m, c.st);
+    h2d(dh, hi, (size_t)m, c.st);
+    double* o = dout.as<double>((size_t)(m * K));
+    ck(cudaMemsetAsync(o, 0, sizeof(double) * (size_t)(m * K), c.st), "memset");
+    const double corr_den = corr_dim > 0.0 ? 1.0 / (corr_dim - 1.0) : 0.0;
+    constexpr int64_t T = 2048;
+    for (int64_t j0 = row0; j0 < row1; j0 += T) {
+        const int64_t j1 = std::min(row1, j0 + T);
+        int64_t p0 = j0, p1 = j1;
+        for (int64_t j = j0; j < j1; ++j) {
+            if (hi[j - row0] <= lo[j - row0]) continue;
+            p0 = std::min(p0, lo[j - row0]);
+            p1 = std::max(p1, hi[j - row0]);
+        }
+        const int64_t Pn = p1 - p0, rows = j1 - j0;
+        double* X = dX.as<double>((size_t)(N * Pn));
+        launch_decode_standardized(P.g, p0, Pn, static_cast<const double*>(P.d_mean.p),
+                                   static_cast<const double*>(P.d_sdinv.p), X, N, c.st);
+        project_cols(c, X, N, Pn, cv, false, dtmp);
+        launch_restandardize_cols(X, N, N, Pn, c.st);
+        double* S = dS.as<double>((size_t)(rows * Pn));
+        DGemmArgs a;
+        a.M = rows;
+        a.N = Pn;
+        a.K = N;
+        a.A = X + (j0 - p0) * N;  // X^T rows of the chunk
+        a.a_ms = N;
+        a.a_ks = 1;
+        a.B = X;
+        a.b_ks = 1;
+        a.b_ns = N;
+        a.C = S;
+        a.c_ms = 1;
+        a.c_ns = rows;
+        launch_dgemm(a, c.st);
+        launch_window_cov_epilogue(S, rows, p0, dl + (j0 - row0), dh + (j0 - row0), an, row0,
+                                   (int)K, 1.0 / (double)N, corr_den, o + (j0 - row0) * K, c.st);
+        ck(cudaGetLastError(), "windowed LD with covariates");
+        ck(cudaStreamSynchronize(c.st), "windowed LD with covariates");  // X, S are reused
+    }
+    std::vector<double> h((size_t)(m * K));
+    d2h(h.data(), o, h.size(), c.st);
+    ck(cudaStreamSynchronize(c.st), "windowed LD with covariates");
+    for (int64_t r = 0; r < m; ++r)
+        for (int64_t b = 0; b < K; ++b) out[r * ld_row + b * ld_col] = h[(size_t)(r * K + b)];
+}
+
 LDS_API int lds_compute_windowed_ld_chr(const char* bed_prefix, const char* fam_path,
                                         int chr_start, int chr_end, const int64_t* bp,
                                         const double* annot_chr, int64_t K, double ld_wind_kb,
@@ -3500,9 +3564,7 @@ LDS_API int lds_compute_windowed_ld_chr(const char* bed_prefix, const char* fam_
         if (K <= 0) fail(LDS_ERR_ARG, "annot_chr must have at least one column");
         if (impute_mode != LDS_IMPUTE_MEAN && impute_mode != LDS_IMPUTE_HWE)
             fail(LDS_ERR_ARG, "impute_mode must be 'mean' or 'hwe'");
-        if ((C != nullptr) != (R != nullptr)) fail(LDS_ERR_ARG, "C and R must be given together");
-        if (C && p > 0)
-            fail(LDS_ERR_ARG, "covariate projection (C, R) is not supported by the GPU windowed path");
+        const bool cov = C && R && p > 0;
         Context& c = ctx();
         std::lock_guard<std::mutex> lk(c.mu);
         ensure_device(c);
@@ -3512,7 +3574,7 @@ LDS_API int lds_compute_windowed_ld_chr(const char* bed_prefix, const char* fam_
         if (chr_start < 0 || chr_end > P.g.M)
             fail(LDS_ERR_IO, "BED file too small for requested block: %s.bed", bed_prefix);
         if (P.g.N <= 2) fail(LDS_ERR_ARG, "Too few rows for windowed LD score computation");
-        const double corr_dim = (double)(P.g.N - 1);
+        const double corr_dim = (double)(P.g.N - (cov ? p : 1));
         if (corr_dim <= 1.0)
             fail(LDS_ERR_ARG, "Too few residual dimensions for unbiased windowed r^2 correction");
         // Partner interval of SNP j: |bp_i - bp_j| <= W (winldcore.cpp:434-442), a
@@ -3529,6 +3591,13 @@ LDS_API int lds_compute_windowed_ld_chr(const char* bed_prefix, const char* fam_
         std::vector<double> ann((size_t)(m * K));
         for (int64_t j = 0; j < m; ++j)
             for (int64_t k = 0; k < K; ++k) ann[(size_t)(j * K + k)] = annot_chr[k * m + j];
+        if (cov) {
+            DevCov cv;
+            upload_cov<double>(c, cv, C, R, P.g.N, p);
+            window_ld_cov_impl(c, P, chr_start, chr_end, lo.data(), hi.data(), ann.data(), K,
+                               corr_dim, cv, out, 1, m);
+            return;
+        }
         window_ld_impl(c, P, chr_start, chr_end, lo.data(), hi.data(), ann.data(), K, corr_dim, out,
                        1, m);
     });

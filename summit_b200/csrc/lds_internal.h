@@ -267,6 +267,11 @@ void launch_decode_standardized(const DevGeno& g, int64_t j0, int64_t L, const d
                                 const double* sdinv, double* X, int64_t ldx, cudaStream_t st);
 void launch_col_sumsq(const double* X, int64_t N, int64_t ld, int64_t L, double* ss,
                       cudaStream_t st);
+void launch_restandardize_cols(double* X, int64_t N, int64_t ld, int64_t L, cudaStream_t st);
+int window_cov_max_bins();
+void launch_window_cov_epilogue(const double* S, int64_t rows, int64_t p0, const int64_t* lo,
+                                const int64_t* hi, const double* annot, int64_t annot_row0, int K,
+                                double invN, double corr_den, double* out, cudaStream_t st);
 template <typename Tann>
 void launch_block_corrections(const double* meansq, const double* mu22, const Tann* annot,
                               int64_t M, int B, double N, double d, double* R2, double* rho2,

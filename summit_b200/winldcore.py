@@ -67,6 +67,13 @@ def compute_windowed_ld_chr(bed_prefix, fam_path, chr_start, chr_end, bp, annot_
         Cp = np.asfortranarray(C, dtype=np.float64)
         Rp = np.asfortranarray(R, dtype=np.float64)
         p = int(Cp.shape[1])
+        if rows is not None:
+            n_rows = nr
+        else:
+            with open(fam_path, "rb") as f:
+                n_rows = sum(1 for line in f if line.strip())
+        if Cp.shape[0] != n_rows or Rp.shape != (p, n_rows):
+            raise RuntimeError("C/R shape mismatch in compute_windowed_ld_chr")
     out = np.empty((max(m, 0), annot.shape[1]), dtype=np.float64, order="F")
     check(_lib.load().lds_compute_windowed_ld_chr(
         enc(bed_prefix), enc(fam_path), int(chr_start), int(chr_end), ptr(bp), ptr(annot),

@@ -45,6 +45,34 @@ def test_windowed_ld_matches_reference(small_bed, refwin, impute, kb):
     assert rel_err(gpu, ref) < 1e-11
 
 
+@pytest.mark.parametrize("impute", ["mean", "hwe"])
+@pytest.mark.parametrize("rows_sel", [False, True])
+def test_windowed_ld_with_covariates_matches_reference(small_bed, refwin, impute, rows_sel):
+    """Covariates: genotypes projected by (I - C R) and restandardized per
+    panel, corr_dim = N - p (winldcore.cpp:340-366, :853)."""
+    from summit_b200 import winldcore
+
+    n, prefix = small_bed["n"], small_bed["prefix"]
+    rng = np.random.default_rng(21)
+    rows = np.sort(rng.choice(n, 280, replace=False)) if rows_sel else None
+    N = n if rows is None else rows.size
+    a, b = 10, 390
+    bp = _bp(b - a, seed=6)
+    annot = np.column_stack([np.ones(b - a), rng.random(b - a) < 0.4])
+    C = np.column_stack([np.ones(N), rng.normal(size=N), rng.normal(size=N)])
+    R = np.linalg.pinv(C)
+    seed = 5 if impute == "hwe" else None
+    ref = refwin.compute_windowed_ld_chr(prefix, a, b, bp, annot, 120.0, 64, row_sel=rows, C=C,
+                                         R=R, impute_mode=impute, impute_seed=seed)
+    gpu = winldcore.compute_windowed_ld_chr(prefix, prefix + ".fam", a, b, bp, annot, 120.0, 64,
+                                            row_sel=rows, C=C, R=R, impute_mode=impute,
+                                            impute_seed=seed)
+    assert rel_err(gpu, ref) < 1e-10
+    with pytest.raises(RuntimeError, match="C/R shape mismatch"):
+        winldcore.compute_windowed_ld_chr(prefix, prefix + ".fam", a, b, bp, annot, 120.0, 64,
+                                          row_sel=rows, C=C[:-1], R=R[:, :-1])
+
+
 def test_windowed_ld_subrange_and_row_selection(small_bed, refwin):
     from summit_b200 import winldcore
 

@@ -102,9 +102,10 @@ def test_dropin_windowed_argument_checks_match_reference():
         winldcore.compute_windowed_ld_chr("x", "x.fam", 0, 3, bp[::-1].copy(), ones, 1.0, 10)
     with pytest.raises(RuntimeError, match="bp length mismatch"):
         winldcore.compute_windowed_ld_chr("x", "x.fam", 0, 3, bp[:2], ones, 1.0, 10)
-    with pytest.raises(RuntimeError, match="covariate projection"):
+    with pytest.raises(RuntimeError, match="C/R shape mismatch"):
         winldcore.compute_windowed_ld_chr("x", "x.fam", 0, 3, bp, ones, 1.0, 10,
-                                          C=np.ones((5, 1)), R=np.ones((1, 5)))
+                                          row_sel=np.arange(4), C=np.ones((5, 1)),
+                                          R=np.ones((1, 5)))
     with pytest.raises(RuntimeError, match="impute_mode"):
         winldcore.compute_windowed_ld_chr("x", "x.fam", 0, 3, bp, ones, 1.0, 10,
                                           impute_mode="median")
