@@ -567,6 +567,18 @@ int lds_gxe_create(int64_t geno, int64_t E, const double* environments, int64_t 
                    const int64_t* power_offsets, const int32_t* ranks, int annotation_bins,
                    int64_t* handle_out);
 int lds_gxe_destroy(int64_t gxe);
+/* Generalized per-SNP GxE packed products (GeneralizedGxELDScoreDirectContext::
+ * packed_source_product / packed_target_product, generalized_gxe_variant.inc:
+ * 1749-1988) on a mean-imputed resident image (lds_geno_create): with the
+ * Mailman mean pack's scale inv_j = sqrt((N - ddof) / M2_j) (genotype.cpp:
+ * 1115-1131) and x'_j = inv_j (g_j - mu_j) on observed calls, 0 on missing,
+ *   source: out (N x cols) = -X' rhs,   rhs (j1-j0) x cols column-major;
+ *   target: out ((j1-j0) x cols) = -X'^T rhs,   rhs N x cols column-major
+ * (the reference's out = mu sum - raw over packed allele counts). */
+int lds_generalized_source_product(int64_t geno, int64_t j0, int64_t j1, const double* rhs,
+                                   int64_t cols, double* out);
+int lds_generalized_target_product(int64_t geno, int64_t j0, int64_t j1, const double* rhs,
+                                   int64_t cols, double* out);
 int lds_gxe_source_block(int64_t gxe, int64_t j0, int64_t j1, const double* probes, int64_t B,
                          const double* annotation, int annotation_is_sqrt, const double* scale_x,
                          const double* scale_w, int64_t T, int environment_start, double* target,

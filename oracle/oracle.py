@@ -320,6 +320,8 @@ class Reference:
                 _str, _str, _int, _int, _int, _str, _p, _i64, _p, _p, _i64, _i64, _p, _p]
             getattr(L, f"ref_block_corrections_{t}").argtypes = [
                 _p, _i64, _i64, _p, _p, _int, _dbl, _p]
+        L.ref_mailman_mean_stats.argtypes = [_p, _i64, _int, _i64, _int, _int, _p, _i64, _int, _p,
+                                             _p, _p]
         L.ref_set_num_threads.argtypes = [_int]
         L.ref_set_omp_threads.argtypes = [_int]
         L.ref_set_blas_threads.argtypes = [_int]
@@ -549,6 +551,17 @@ class Reference:
             impute_mode.encode(), _ptr(ann), ann.shape[1], _ptr(Cf), _ptr(Rf), N, p, _ptr(inv),
             _ptr(mu22)))
         return inv, mu22
+
+    def mailman_mean_stats(self, bed_path, n_total, start, stop, rows=None, ddof=1):
+        """Mean, inverse scale and observed count of the Mailman mean pack."""
+        bed = np.fromfile(str(bed_path), dtype=np.uint8)
+        L = stop - start
+        mean, inv, obs = np.empty(L), np.empty(L), np.empty(L, dtype=np.int32)
+        rows_a = None if rows is None else np.ascontiguousarray(rows, dtype=np.int64)
+        self._chk(self.lib.ref_mailman_mean_stats(
+            _ptr(bed), bed.size, n_total, (n_total + 3) // 4, start, stop, _ptr(rows_a),
+            0 if rows_a is None else rows_a.size, ddof, _ptr(mean), _ptr(inv), _ptr(obs)))
+        return mean, inv, obs
 
     def block_corrections(self, meansq_raw, mu22, annot, N, d):
         m = np.ascontiguousarray(meansq_raw, dtype=np.float64)

@@ -563,3 +563,27 @@ REF_BOTH(ref_resvar_mu22, MU22_SIG(float), MU22_CALL(float), MU22_SIG(double), M
     double d, double* out4)
 #define BCB_CALL(T) block_corrections<T>(m, M, B, u, a, N, d, out4)
 REF_BOTH(ref_block_corrections, BCB_SIG(float), BCB_CALL(float), BCB_SIG(double), BCB_CALL(double))
+
+// Mailman mean pack statistics (read_block_mailman_mean_memory,
+// genotype.cpp:1249-1263): per SNP the observed mean, the pack's inverse
+// scale and the observed count, from an in-memory BED image (with header).
+REF_EXPORT int ref_mailman_mean_stats(const uint8_t* bed, int64_t bed_size, int n_total,
+                                      int64_t bytes_per_snp, int start, int stop,
+                                      const int64_t* rows, int64_t n_rows, int ddof,
+                                      double* mean, double* inv_std, int* observed) {
+    return guarded([&] {
+        std::vector<int> r;
+        if (rows)
+            for (int64_t i = 0; i < n_rows; ++i) r.push_back((int)rows[i]);
+        else
+            for (int i = 0; i < n_total; ++i) r.push_back(i);
+        MailmanPackedBlock pack;
+        read_block_mailman_mean_memory(bed, (size_t)bed_size, n_total, (size_t)bytes_per_snp,
+                                       start, stop, r, ddof, pack);
+        for (int j = 0; j < pack.L; ++j) {
+            mean[j] = pack.mean[(size_t)j];
+            inv_std[j] = pack.inv_std[(size_t)j];
+            observed[j] = pack.observed[(size_t)j];
+        }
+    });
+}

@@ -4210,6 +4210,83 @@ LDS_API int lds_gxe_create(int64_t geno, int64_t E, const double* environments, 
     });
 }
 
+// Generalized GxE packed products (generalized_gxe_variant.inc:1749-1988) on
+// a resident mean-imputed image.  The reference's Mailman mean pack scales
+// SNP j by inv_j = sqrt((N - ddof) / M2_j) (genotype.cpp:1115-1131) and its
+// products use out = mu sum - raw over the packed allele counts, i.e. the
+// negated standardized genotypes: source = -X' rhs (N x cols), target =
+// -X'^T rhs (L x cols), X' = inv (g - mu) on observed calls, 0 on missing.
+// The products run on the phase-1 and phase-2 tensor-core kernels with the
+// image's scale s_j, rescaled per SNP by inv_j / s_j.
+static std::vector<double> pack_scale_ratio(const Prepared& P, int64_t j0, int64_t j1) {
+    std::vector<double> r((size_t)(j1 - j0));
+    const long long denominator = P.g.N - (long long)P.ddof;
+    for (int64_t j = j0; j < j1; ++j) {
+        const SnpCounts& k = P.counts[(size_t)j];
+        const long long nobs = (long long)k.n[0] + k.n[1] + k.n[2];
+        const long long sum = (long long)k.n[1] + 2LL * k.n[2];
+        const long long sumsq = (long long)k.n[1] + 4LL * k.n[2];
+        double inv = 1.0;
+        if (nobs > 0) {
+            double m2 = (double)sumsq - (double)sum * (double)sum / (double)nobs;
+            if (m2 < 0.0 && m2 > -1.0e-12) m2 = 0.0;
+            if (denominator > 0 && m2 > 0.0) inv = std::sqrt((double)denominator / m2);
+        }
+        r[(size_t)(j - j0)] = inv / P.sdinv[(size_t)j];
+    }
+    return r;
+}
+
+static Prepared& generalized_image(int64_t geno, int64_t j0, int64_t j1, int64_t cols) {
+    auto it = geno_table().find(geno);
+    if (it == geno_table().end()) fail(LDS_ERR_ARG, "unknown genotype handle");
+    Prepared& P = *it->second;
+    if (P.impute != LDS_IMPUTE_MEAN)
+        fail(LDS_ERR_ARG, "generalized packed products need a mean-imputed genotype image");
+    if (j0 < 0 || j1 > P.g.M || j1 <= j0 || cols <= 0)
+        fail(LDS_ERR_ARG, "Generalized packed product is mis-sized");
+    return P;
+}
+
+LDS_API int lds_generalized_source_product(int64_t geno, int64_t j0, int64_t j1,
+                                           const double* rhs, int64_t cols, double* out) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        ensure_device(c);
+        Prepared& P = generalized_image(geno, j0, j1, cols);
+        const int64_t L = j1 - j0, N = P.g.N, Np = P.g.N_pad;
+        const std::vector<double> ratio = pack_scale_ratio(P, j0, j1);
+        std::vector<double> Z((size_t)(L * cols)), ones((size_t)L, 1.0);
+        for (size_t i = 0; i < Z.size(); ++i) Z[i] = -rhs[i];
+        const int Vp = (int)round_up(cols, kColTile);
+        const Csr cs = build_csr<double>(ones.data(), ratio.data(), L, 1, j0, Vp, c.slices);
+        run_phase1(c, P, cs, 1, (int)cols, Z.data(), L, L, j0);
+        std::vector<double> y((size_t)(Np * cols));
+        d2h(y.data(), static_cast<double*>(c.y.p), y.size(), c.st);
+        ck(cudaStreamSynchronize(c.st), "generalized source product");
+        for (int64_t q = 0; q < cols; ++q)
+            std::memcpy(out + q * N, &y[(size_t)(q * Np)], sizeof(double) * (size_t)N);
+    });
+}
+
+LDS_API int lds_generalized_target_product(int64_t geno, int64_t j0, int64_t j1,
+                                           const double* rhs, int64_t cols, double* out) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        ensure_device(c);
+        Prepared& P = generalized_image(geno, j0, j1, cols);
+        const int64_t L = j1 - j0, N = P.g.N;
+        const std::vector<double> ratio = pack_scale_ratio(P, j0, j1);
+        const std::vector<double> Y(rhs, rhs + N * cols);
+        const std::vector<double> pr = snp_products(c, P, j0, j1, Y, cols);
+        for (int64_t j = 0; j < L; ++j)
+            for (int64_t q = 0; q < cols; ++q)
+                out[q * L + j] = -ratio[(size_t)j] * pr[(size_t)(j * cols + q)];
+    });
+}
+
 LDS_API int lds_gxe_destroy(int64_t gxe) {
     return guarded([&] {
         Context& c = ctx();

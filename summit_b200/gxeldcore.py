@@ -248,3 +248,32 @@ class MultiEnvironmentKernel:
                 _lib.load().lds_gxe_destroy(h)
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------------------
+# Generalized per-SNP GxE products (GeneralizedGxELDScoreDirectContext::
+# packed_source_product / packed_target_product, generalized_gxe_variant.inc:
+# 1749-1988): mean-imputed genotypes scaled by the Mailman mean pack's
+# sqrt((N - ddof) / M2_j), with the reference's sign convention.
+# ---------------------------------------------------------------------------
+def generalized_source_product(genotype: GenotypeBlock, rhs) -> np.ndarray:
+    """-X' rhs: rhs (L x columns) -> N x columns (column-major)."""
+    rhs = np.asfortranarray(rhs, dtype=np.float64)
+    L = genotype.stop - genotype.start
+    if rhs.ndim != 2 or rhs.shape[0] != L or rhs.shape[1] <= 0:
+        raise RuntimeError("Generalized packed source product is mis-sized")
+    out = np.empty((genotype.session.N, rhs.shape[1]), order="F")
+    check(_lib.load().lds_generalized_source_product(
+        genotype.session.handle, genotype.start, genotype.stop, ptr(rhs), rhs.shape[1], ptr(out)))
+    return out
+
+
+def generalized_target_product(genotype: GenotypeBlock, rhs) -> np.ndarray:
+    """-X'^T rhs: rhs (N x columns) -> L x columns (column-major)."""
+    rhs = np.asfortranarray(rhs, dtype=np.float64)
+    if rhs.ndim != 2 or rhs.shape[0] != genotype.session.N or rhs.shape[1] <= 0:
+        raise RuntimeError("Generalized packed target product is mis-sized")
+    out = np.empty((genotype.stop - genotype.start, rhs.shape[1]), order="F")
+    check(_lib.load().lds_generalized_target_product(
+        genotype.session.handle, genotype.start, genotype.stop, ptr(rhs), rhs.shape[1], ptr(out)))
+    return out
