@@ -10,7 +10,11 @@
 namespace lds {
 namespace umma {
 
-constexpr long long kWaitLimit = 1LL << 26;
+// Each try_wait suspends the thread for at most kSuspendNs (it returns as
+// soon as the phase completes), so a wait gives up after at most about
+// kWaitLimit * kSuspendNs = 6.7 s.
+constexpr long long kWaitLimit = 1LL << 25;
+constexpr uint32_t kSuspendNs = 200;
 
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
@@ -31,10 +35,10 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
     for (long long i = 0; i < kWaitLimit; ++i) {
         uint32_t done;
         asm volatile(
-            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
             "selp.u32 %0, 1, 0, p;\n\t}"
             : "=r"(done)
-            : "r"(addr), "r"(parity)
+            : "r"(addr), "r"(parity), "n"(kSuspendNs)
             : "memory");
         if (done) return true;
     }

@@ -37,7 +37,14 @@ constexpr int kATile = kBM * kBK;     // 16 KB
 constexpr int kPkStages = 8;          // packed-code ring (HBM latency)
 constexpr int kAStages = 2;           // decoded G/O operand ring
 constexpr int kBStages = 4;           // sketch-digit ring (L2 latency)
-constexpr int kThreads = 224;
+// Decoder sets: set d decodes the K-steps it with it % kDecSets == d, so two
+// sets keep two operand tiles in flight while the first set also runs the
+// epilogue.
+#ifndef LDS_P2_DEC_SETS
+#define LDS_P2_DEC_SETS 2
+#endif
+constexpr int kDecSets = LDS_P2_DEC_SETS;
+constexpr int kThreads = 96 + 128 * kDecSets;
 constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kOCol = 256;       // TMEM column of the O accumulator
 
@@ -184,8 +191,9 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
         }
     } else {
-        // ---------------- decoders + epilogue (warps 3..6) ----------------
-        const int r = tid - 96;              // operand row this thread decodes
+        // ---------------- decoders (warps 3..) + epilogue (warps 3..6) ----------------
+        const int dset = (warp - 3) >> 2;    // decoder set of this warp
+        const int r = (tid - 96) & 127;      // operand row this thread decodes
         const int q = warp & 3;              // TMEM lane quadrant this warp may access
         const int row = q * 32 + lane;       // accumulator row (SNP) of this thread
         const int64_t j = jt0 + row;
@@ -225,6 +233,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         int it = 0;
         for (int g = 0; g < ngroups; ++g) {
             for (int kt = 0; kt < a.nkt; ++kt, ++it) {
+                if (it % kDecSets != dset) continue;
                 const int sp = it % kPkStages, sa = it % kAStages;
                 if (!mbar_wait(&pk_full[sp], (uint32_t)(it / kPkStages) & 1u)) { fail(5); break; }
                 if (*abort_flag) break;
@@ -239,6 +248,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 mbar_arrive(&a_full[sa]);
             }
             if (*abort_flag) break;
+            if (dset != 0) continue;
             // Epilogue of column group g.
             if (!mbar_wait(acc_full, (uint32_t)g & 1u)) { fail(7); break; }
             tc_fence_after();
@@ -283,7 +293,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             tc_fence_before();
             mbar_arrive(acc_empty);
         }
-        flush();
+        if (dset == 0) flush();
     }
     tc_fence_before();
     __syncthreads();

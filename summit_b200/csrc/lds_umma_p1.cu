@@ -309,7 +309,9 @@ __global__ void __launch_bounds__(p1::kThreads, 1)
                             w |= ((uint32_t)(U >> 14) & 127u) << 8;
                             w |= ((uint32_t)(U >> 7) & 127u) << 16;
                             w |= ((uint32_t)U & 127u) << 24;
-                            w = __vsub4(w, 0x3F3F3F00u);
+                            // bytes 1..3 hold d + 63 >= 0: a plain subtraction
+                            // borrows across no byte
+                            w -= 0x3F3F3F00u;
                             // Digit t of probe v for this lane's sample: one byte
                             // store per digit row; the warp's 32 lanes write 32
                             // consecutive samples, one full sector per store.

@@ -44,7 +44,7 @@ class CvConfig:
     band: int = 8              # exact near field |i - j| <= band (4, 8 or 15)
     train_frac: float = 0.1    # SNPs whose noisy far-field scores train the network
     val_frac: float = 0.05     # disjoint SNPs that set the shrinkage weights
-    epochs: int = 30
+    epochs: int = 10
     batch: int = 4096
     lr: float = 2e-3
     seed: int = 0
@@ -76,10 +76,8 @@ class LearnedCV:
         ws_t = torch.from_numpy(ws).to(dev)
         win = torch.repeat_interleave(torch.arange(W, device=dev), torch.from_numpy(sizes).to(dev))
         # correlation null M_k(window) / (N - ddof), as the plain estimator applies it;
-        # window sums from one prefix sum over the SNPs (exact for 0/1 annotations)
-        cs = torch.cat([torch.zeros((1, K), dtype=torch.float64, device=dev),
-                        torch.cumsum(self.annot, 0)])
-        mkw = cs[ws_t[1:]] - cs[ws_t[:-1]]
+        # per-window annotation sums in SNP order on the host (W x K), gathered per SNP
+        mkw = torch.from_numpy(np.add.reduceat(annot, ws[:-1], axis=0)).to(dev)
         nd = float(session.N - 1)
         self.null = mkw[win] / nd
         # static features: MAF, annotations, window geometry
