@@ -45,6 +45,7 @@ class CvConfig:
     train_frac: float = 0.1    # SNPs whose noisy far-field scores train the network
     val_frac: float = 0.05     # disjoint SNPs that set the shrinkage weights
     epochs: int = 10
+    min_steps: int = 150       # at least this many optimizer steps (small training sets)
     batch: int = 4096
     lr: float = 2e-3
     seed: int = 0
@@ -149,7 +150,9 @@ class LearnedCV:
         net = Surrogate(self.n_features, K, seed=cfg.seed)
         Xtr, Ytr = X[tr].contiguous(), Y[tr].contiguous()
         t2 = time.perf_counter()
-        losses = net.train(Xtr, Ytr, epochs=cfg.epochs, batch=cfg.batch, lr=cfg.lr, seed=cfg.seed)
+        per_epoch = -(-Xtr.shape[0] // cfg.batch)
+        epochs = max(cfg.epochs, -(-cfg.min_steps // per_epoch))
+        losses = net.train(Xtr, Ytr, epochs=epochs, batch=cfg.batch, lr=cfg.lr, seed=cfg.seed)
         t3 = time.perf_counter()
         h = (net.forward(X).double() * tstd.double() + tmean.double())
         resid2 = ((target.double()[va] - h[va]) ** 2).mean(0)
