@@ -45,7 +45,7 @@ class CvConfig:
     train_frac: float = 0.1    # SNPs whose noisy far-field scores train the network
     val_frac: float = 0.05     # disjoint SNPs that set the shrinkage weights
     epochs: int = 10
-    min_steps: int = 150       # at least this many optimizer steps (small training sets)
+    min_steps: int = 30        # at least this many optimizer steps (small training sets)
     batch: int = 4096
     lr: float = 2e-3
     seed: int = 0
