@@ -309,9 +309,11 @@ __global__ void __launch_bounds__(p1::kThreads, 1)
                             w |= ((uint32_t)(U >> 14) & 127u) << 8;
                             w |= ((uint32_t)(U >> 7) & 127u) << 16;
                             w |= ((uint32_t)U & 127u) << 24;
-                            // bytes 1..3 hold d + 63 >= 0: a plain subtraction
-                            // borrows across no byte
-                            w -= 0x3F3F3F00u;
+                            // Byte-wise subtraction of 63 from bytes 1..3 (which
+                            // hold d + 63 in [0, 127]): with their top bits set
+                            // first, no byte borrows from the next; byte 0
+                            // subtracts 0.
+                            w = ((w | 0x80808000u) - 0x3F3F3F00u) ^ 0x80808000u;
                             // Digit t of probe v for this lane's sample: one byte
                             // store per digit row; the warp's 32 lanes write 32
                             // consecutive samples, one full sector per store.
