@@ -489,7 +489,7 @@ def ours_arm(args) -> None:
         s2 = GwSession(bed_host, n, impute_mode="mean")
         p2 = WinPlan(s2, annot, ws, B_PROBES, BLOCK, PROBE_SEED, "rademacher")
         p2.execute()
-        out = p2.results()
+        out = p2.results(meansq=False)
         p2.close()
         s2.close()
         return out
@@ -598,7 +598,11 @@ def exact_arm(args) -> None:
 
     torch.cuda.set_device(env_int("LOCAL_RANK", 0))
     n, m = N_SAMPLES, env_int("LDS_BENCH_M", M_SNPS)
-    bed = gwldcore.synth_bed_rows(n, m, DATA_SEED)
+    rows = gwldcore.synth_bed_rows(n, m, DATA_SEED)
+    pinned = torch.empty(rows.shape, dtype=torch.uint8, pin_memory=True)
+    pinned.numpy()[:] = rows
+    bed = pinned.numpy()  # the end-to-end copy starts from pinned host memory
+    del rows
     annot = annotations(m)
     ws = windows(m)
     win = np.repeat(np.arange(ws.size - 1), np.diff(ws))

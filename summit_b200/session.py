@@ -225,12 +225,14 @@ class WinPlan:
     def execute(self) -> None:
         check(_lib.load().lds_win_plan_execute(self.handle))
 
-    def results(self) -> dict:
+    def results(self, meansq: bool = True) -> dict:
+        """LD scores (M x K); with ``meansq`` also the raw accumulators and the
+        inverse residual sds (and the MC sums of a with_mc plan)."""
         M, K = self.M, self.K
         ld = np.empty((M, K))
-        ms = np.empty((M, K))
-        inv = np.empty(M)
-        mcp = np.empty((M, K)) if self.with_mc else None
+        ms = np.empty((M, K)) if meansq else None
+        inv = np.empty(M) if meansq else None
+        mcp = np.empty((M, K)) if (self.with_mc and meansq) else None
         check(_lib.load().lds_win_plan_results(self.handle, ptr(ld), ptr(ms), ptr(inv), ptr(mcp)))
         return {"ldscore": ld, "meansq_accum": ms, "inv": inv, "mc_per_snp_sumsq": mcp}
 
