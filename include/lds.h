@@ -302,6 +302,11 @@ int lds_win_plan_cv_outputs(int64_t plan, int device_ptrs, double* meansq_tiles,
 /* Device time (ms) of the control-variate kernels of the last execute. */
 int lds_win_plan_cv_ms(int64_t plan, double* ms);
 uint64_t lds_window_seed(uint64_t root, int64_t w);
+/* One Rademacher probe block generated on the device (L x V column-major, host
+ * output): the std::mt19937_64 stream of make_seed(root, blk_start, v_start)
+ * (gwldcore.cpp:452-458, :1702-1706) that the plans use for Rademacher probes. */
+int lds_debug_rademacher_block(uint64_t root, int blk_start, int v_start, int L, int V,
+                               double* out);
 
 /* Device timing of the last lds_gw_ldscore call (milliseconds, CUDA events
  * on the library stream): [0] upload+prepare, [1] phase 1 total, [2] phase 2

@@ -399,14 +399,18 @@ T inv_resvar(const Prepared& P, int64_t j, double eps) {
 // Probe streams: mt19937_64 seeded per (root, block start, V-tile start)
 // (gwldcore.cpp:452-458, :1691-1716).  Column-major L x V into Z (ld = z_ld).
 // ---------------------------------------------------------------------------
-template <typename T>
-void make_probes(uint64_t root, int blk_start, int v_start, int L, int V, int dist, double* Z,
-                 int64_t z_ld) {
+uint64_t probe_seed(uint64_t root, int blk_start, int v_start) {
     uint64_t s = 0x1234abcdULL;
     s ^= mix64(root);
     s ^= mix64((uint64_t)blk_start + 0x9e37ULL);
     s ^= mix64((uint64_t)v_start + 0x85ebULL);
-    std::mt19937_64 rng(s);
+    return s;
+}
+
+template <typename T>
+void make_probes(uint64_t root, int blk_start, int v_start, int L, int V, int dist, double* Z,
+                 int64_t z_ld) {
+    std::mt19937_64 rng(probe_seed(root, blk_start, v_start));
     std::normal_distribution<T> gN(0, (T)1);
     std::vector<T> col((size_t)L);
     for (int c = 0; c < V; ++c) {
@@ -422,6 +426,19 @@ void make_probes(uint64_t root, int blk_start, int v_start, int L, int V, int di
         }
         for (int r = 0; r < L; ++r) Z[(int64_t)c * z_ld + r] = (double)col[(size_t)r];
     }
+}
+
+// Rademacher probe blocks generated on the device (lds_probes.cu): the same
+// mt19937_64 streams as make_probes, written straight into dZ.
+void device_rademacher(Context& c, const std::vector<ProbeUnit>& units, int V, double* dZ,
+                       int64_t ld) {
+    if (units.empty()) return;
+    DevBuf du;
+    ProbeUnit* d = du.as<ProbeUnit>(units.size());
+    h2d(d, units.data(), units.size(), c.st);
+    launch_rademacher_units(d, (int64_t)units.size(), V, dZ, ld, c.st);
+    ck(cudaGetLastError(), "probe streams");
+    ck(cudaStreamSynchronize(c.st), "probe streams");  // the unit table is freed on return
 }
 
 // ---------------------------------------------------------------------------
@@ -1662,33 +1679,45 @@ std::unique_ptr<GwPlan> plan_create(Context& c, std::shared_ptr<Prepared> P, con
         const int64_t pad = tc ? 128 : kSnpStep;
         t->csr = as_float ? build_csr<float>(annot_f.data(), inv_f.data(), M, K, 0, t->Vp, pl->S, pad)
                           : build_csr<double>(annot, pl->inv.data(), M, K, 0, t->Vp, pl->S, pad);
-        // Probe streams per SNP block (mt19937_64), generated in parallel.
-        std::vector<double> Z((size_t)(M * V));
-        std::vector<std::thread> th;
-        std::atomic<int> next{0};
-        for (unsigned w = 0; w < hw; ++w)
-            th.emplace_back([&] {
-                for (int b; (b = next.fetch_add(1)) < nblk;) {
-                    const int s = b * step;
-                    const int L = (int)std::min<int64_t>(step, M - s);
-                    std::vector<double> blk((size_t)L * V);
-                    // Probe streams are keyed by the block's start in the whole
-                    // fileset (make_seed, gwldcore.cpp:452-458).
-                    const int gs = (int)(snp_offset + s);
-                    if (as_float) make_probes<float>(seed, gs, v0, L, V, dist, blk.data(), L);
-                    else make_probes<double>(seed, gs, v0, L, V, dist, blk.data(), L);
-                    for (int cc = 0; cc < V; ++cc)
-                        std::memcpy(&Z[(size_t)cc * M + s], &blk[(size_t)cc * L], sizeof(double) * L);
-                }
-            });
-        for (auto& x : th) x.join();
+        // Probe streams per SNP block (mt19937_64), keyed by the block's start
+        // in the whole fileset (make_seed, gwldcore.cpp:452-458): Rademacher
+        // streams on the device, Gaussian ones on host threads.
+        std::vector<double> Z;
+        if (dist == LDS_DIST_RADEMACHER) {
+            std::vector<ProbeUnit> units((size_t)nblk);
+            for (int b = 0; b < nblk; ++b) {
+                const int s = b * step;
+                units[(size_t)b] = {s, (int32_t)std::min<int64_t>(step, M - s), 0,
+                                    probe_seed(seed, (int)(snp_offset + s), v0)};
+            }
+            device_rademacher(c, units, V, t->z.as<double>((size_t)(M * V)), M);
+        } else {
+            Z.resize((size_t)(M * V));
+            std::vector<std::thread> th;
+            std::atomic<int> next{0};
+            for (unsigned w = 0; w < hw; ++w)
+                th.emplace_back([&] {
+                    for (int b; (b = next.fetch_add(1)) < nblk;) {
+                        const int s = b * step;
+                        const int L = (int)std::min<int64_t>(step, M - s);
+                        std::vector<double> blk((size_t)L * V);
+                        const int gs = (int)(snp_offset + s);
+                        if (as_float) make_probes<float>(seed, gs, v0, L, V, dist, blk.data(), L);
+                        else make_probes<double>(seed, gs, v0, L, V, dist, blk.data(), L);
+                        for (int cc = 0; cc < V; ++cc)
+                            std::memcpy(&Z[(size_t)cc * M + s], &blk[(size_t)cc * L],
+                                        sizeof(double) * L);
+                    }
+                });
+            for (auto& x : th) x.join();
+        }
         const Csr& cs = t->csr;
         const size_t nm = std::max<size_t>(cs.rowind.size(), 1);
         h2d(t->rowind.as<int32_t>(nm), cs.rowind.data(), cs.rowind.size(), c.st);
         h2d(t->sc.as<double>(nm), cs.sc.data(), cs.sc.size(), c.st);
         h2d(t->binoff.as<int64_t>(cs.bin_off.size()), cs.bin_off.data(), cs.bin_off.size(), c.st);
         h2d(t->wqoff.as<int64_t>(cs.wq_off.size()), cs.wq_off.data(), cs.wq_off.size(), c.st);
-        h2d(t->z.as<double>(Z.size()), Z.data(), Z.size(), c.st);
+        if (!Z.empty()) h2d(t->z.as<double>(Z.size()), Z.data(), Z.size(), c.st);
         if (tc) {
             for (int64_t kk = 0; kk < K; ++kk)
                 t->lmax = std::max(t->lmax, cs.bin_off[(size_t)kk + 1] - cs.bin_off[(size_t)kk]);
@@ -2144,6 +2173,19 @@ std::unique_ptr<WinPlan> win_plan_create(Context& c, std::shared_ptr<Prepared> P
         for (int64_t s = 0; s < ws[w + 1] - ws[w]; s += step) units.push_back({w, s});
     int v0 = 0;
     for (int V : pl->vt) {
+        pl->z.emplace_back();
+        double* dZ = pl->z.back().as<double>((size_t)(M * V));
+        if (dist == LDS_DIST_RADEMACHER) {
+            std::vector<ProbeUnit> pu(units.size());
+            for (size_t u = 0; u < units.size(); ++u) {
+                const int64_t w = units[u].first, s = units[u].second;
+                pu[u] = {ws[w] + s, (int32_t)std::min<int64_t>(step, ws[w + 1] - ws[w] - s), 0,
+                         probe_seed(window_seed(seed, w), (int)s, v0)};
+            }
+            device_rademacher(c, pu, V, dZ, M);
+            v0 += V;
+            continue;
+        }
         std::vector<double> Z((size_t)(M * V));
         std::vector<std::thread> th;
         std::atomic<size_t> next{0};
@@ -2159,8 +2201,7 @@ std::unique_ptr<WinPlan> win_plan_create(Context& c, std::shared_ptr<Prepared> P
                 }
             });
         for (auto& x : th) x.join();
-        pl->z.emplace_back();
-        h2d(pl->z.back().as<double>(Z.size()), Z.data(), Z.size(), c.st);
+        h2d(dZ, Z.data(), Z.size(), c.st);
         ck(cudaStreamSynchronize(c.st), "probe upload");
         v0 += V;
     }
@@ -4108,6 +4149,21 @@ LDS_API int lds_win_plan_destroy(int64_t plan) {
 }
 
 LDS_API uint64_t lds_window_seed(uint64_t root, int64_t w) { return window_seed(root, w); }
+
+LDS_API int lds_debug_rademacher_block(uint64_t root, int blk_start, int v_start, int L, int V,
+                                       double* out) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        ensure_device(c);
+        if (L <= 0 || V <= 0) fail(LDS_ERR_ARG, "invalid sizes");
+        DevBuf dz;
+        double* z = dz.as<double>((size_t)L * (size_t)V);
+        device_rademacher(c, {ProbeUnit{0, L, 0, probe_seed(root, blk_start, v_start)}}, V, z, L);
+        d2h(out, z, (size_t)L * (size_t)V, c.st);
+        ck(cudaStreamSynchronize(c.st), "probe block");
+    });
+}
 
 LDS_API int lds_last_timings(double* ms_out, int n) {
     Context& c = ctx();

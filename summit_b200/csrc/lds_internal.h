@@ -242,6 +242,18 @@ void launch_mlp_adam(float* p, float* m, float* v, const float* g, int64_t P, fl
                      float b2, float eps, float bc1, float bc2, cudaStream_t st);
 
 // Launch accounting.
+// ---- device Rademacher probe streams (lds_probes.cu) ----
+// One std::mt19937_64 stream per unit: its L x V block (column-major, rows
+// row0 .. row0 + L of Z with leading dimension ld) in stream order.
+struct ProbeUnit {
+    int64_t row0;
+    int32_t L;
+    int32_t pad;
+    uint64_t seed;
+};
+void launch_rademacher_units(const ProbeUnit* units, int64_t n_units, int V, double* Z, int64_t ld,
+                             cudaStream_t st);
+
 // ---- dense FP64 work (lds_dense.cu) ----
 // C[m, n] = alpha sum_k A(m, k) B(k, n) + beta C[m, n] with
 // A(m, k) = A[m a_ms + kk a_ks] (kk = a_kidx[k] when a_kidx is set; squared
