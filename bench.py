@@ -287,12 +287,13 @@ def reference_arm(args) -> None:
 # GPU arm
 # ---------------------------------------------------------------------------
 def read_traffic() -> dict | None:
-    """Per-launch DRAM bytes of the phase-2 kernel from the committed ncu summary."""
-    f = ROOT / "profiles" / "p2_kernel_gw_n50k_m500k.md"
+    """DRAM bytes of the windowed phase-2 kernel per full-size estimate, from the
+    committed ncu summary (a captured launch scaled by the CTA count)."""
+    f = ROOT / "profiles" / "p2_kernel_windowed_n50k_m100k.md"
     if not f.exists():
         return None
     for line in f.read_text().splitlines():
-        if line.startswith("traffic_bytes_per_launch:"):
+        if line.startswith("traffic_bytes_per_estimate:"):
             try:
                 return {"bytes": float(line.split(":", 1)[1].strip())}
             except ValueError:
@@ -541,12 +542,14 @@ def ours_arm(args) -> None:
                             "unit": "TOPS", "ms_per_step": round(gw_ms, 3),
                             "kernel_ms": {k: round(v, 3) for k, v in gw_kms.items()}},
             "roofline": {
-                "kernel": "p2_umma_kernel (phase 2: X^T Y + LD epilogue)", "bound": "tensor",
+                "kernel": "p2_umma_kernel (windowed phase 2: X^T Y + LD epilogue, all launches "
+                          "of one estimate)", "bound": "tensor",
                 "achieved": None if achieved is None else round(achieved, 3),
                 "peak": peak, "unit": "TFLOP/s",
                 "frac": None if achieved is None else round(achieved / peak, 4),
                 "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)" if peaks else "fallback",
                 "traffic": None if tr is None else tr["bytes"],
+                "traffic_source": "profiles/p2_kernel_windowed_n50k_m100k.md (per estimate)",
                 "algorithmic_ops_per_launch": ops2},
             "e2e": {"value": round(world * ops / (e2e_ms * 1e-3) / 1e12, 3), "unit": "TOPS",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
