@@ -820,17 +820,114 @@ def gxe_arm(args) -> None:
         print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# Biobank-scale workload (config-5 shape): N = 400,000 x M = 800,000 (80 GB of
+# packed codes, resident in HBM, generated on the device), B = 50 +-1 probes.
+# One step = one plain genome-wide estimate (K = 1); the GxE reference build
+# with E = 4 continuous exposures (B = 50 +-1 probes) is timed beside it.
+# ---------------------------------------------------------------------------
+BIO_N, BIO_M, BIO_B, BIO_E = 400_000, 800_000, 50, 4
+BIO_METRIC = "geno x probe TOPS (biobank-scale genome-wide LD scores, HBM-resident BED)"
+
+
+def biobank_arm(args) -> None:
+    import torch
+
+    torch.cuda.set_device(env_int("LOCAL_RANK", 0))
+    from summit_b200 import _lib
+    from summit_b200.gxe import GxeReference, synthetic_design
+    from summit_b200.session import GwSession
+
+    n, m = env_int("LDS_BIO_N", BIO_N), env_int("LDS_BIO_M", BIO_M)
+    B, E = BIO_B, BIO_E
+    lib = _lib.load()
+    t0 = time.perf_counter()
+    sess = GwSession.synthetic(n, m, DATA_SEED)
+    torch.cuda.synchronize()
+    gen_s = time.perf_counter() - t0
+    image_bytes = m * (-(-n // 256) * 256) // 4
+    annot = np.ones((m, 1))
+    plan = sess.plan(annot, B, BLOCK, PROBE_SEED, "rademacher")
+    for _ in range(args.warmup):
+        plan.execute()
+    torch.cuda.synchronize()
+    plan.kernel_ms()
+    stream_ms = []
+    launches0 = lib.lds_kernel_launches()
+    with Clocks(env_int("LOCAL_RANK", 0)) as clk:
+        for _ in range(args.steps):
+            plan.execute()
+            km = plan.kernel_ms()
+            stream_ms.append(km)
+    launches = int(lib.lds_kernel_launches() - launches0) // max(args.steps, 1)
+    res = plan.results()
+    assert np.isfinite(res["ldscore"]).all()
+    p1 = float(np.mean([k["phase1"] for k in stream_ms]))
+    p2 = float(np.mean([k["phase2"] for k in stream_ms]))
+    ms = float(np.mean([sum(k.values()) for k in stream_ms]))
+    ops = 4.0 * n * m * B  # 2 N M B (phase 1, K = 1) + 2 N M B (phase 2)
+    plan.close()
+    # GxE reference build on the same image: E continuous exposures, +-1 probes
+    d = synthetic_design(n, E, seed=3, categorical=0)
+    dev = torch.device("cuda")
+    g = torch.Generator(device=dev)
+    g.manual_seed(4321)
+    probes = (torch.randint(0, 2, (B, m), generator=g, device=dev).double() * 2.0 - 1.0).T
+    ones1 = torch.ones((1, m), dtype=torch.float64, device=dev).T
+    scale = torch.ones((E, m), dtype=torch.float64, device=dev).T
+    keys = ("environments", "feature_basis", "power_indices", "power_offsets", "ranks",
+            "gram_values", "gram_offsets", "e2_gram_values", "common_basis", "directions")
+    gx = GxeReference(sess, *[d[k] for k in keys], annotation_bins=1)
+    gx.run(probes, ones1, scale, scale)  # warm-up
+    gres = gx.run(probes, ones1, scale, scale)
+    gxe_ms = gres["timings"]["total"]
+    gxe_ops_ = gxe_ops(n, m, E, 1, B)
+    sess.close()
+    line = {
+        "metric": BIO_METRIC, "value": round(ops / (ms * 1e-3) / 1e12, 3), "unit": "TOPS",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 2),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int8-digit exact products, f64 epilogue",
+        "data": "synthetic (seeded HWE/AR(1) generator, image generated on the device)",
+        "config": {"workload": "biobank_gw_n400k_m800k_k1_b50_rademacher", "N": n, "M": m, "K": 1,
+                   "B": B, "image_gb": round(image_bytes / 1e9, 2),
+                   "l2": "inputs larger than L2 (%.0f GB image)" % (image_bytes / 1e9)},
+        "kernel_ms": {"phase1": round(p1, 2), "phase2": round(p2, 2)},
+        "decode_stream_gbs": {"phase1": round(image_bytes / (p1 * 1e-3) / 1e9, 1),
+                              "phase2": round(image_bytes / (p2 * 1e-3) / 1e9, 1),
+                              "note": "packed image bytes streamed per phase / phase time"},
+        "image_generation_s": round(gen_s, 2),
+        "gxe_reference": {"E": E, "B": B, "columns": E * 2 * B, "ms": round(gxe_ms, 1),
+                          "TOPS": round(gxe_ops_ / (gxe_ms * 1e-3) / 1e12, 3),
+                          "stage_ms": {k: round(v, 1) for k, v in gres["timings"].items()},
+                          "max_leakage": float(np.max(gres["leakages"]))},
+        "e2e": None,
+        "e2e_note": ("not measured: the 80 GB BED would have to be staged in pinned host "
+                     "memory; the image is generated on the device"),
+        "gpu_launches": launches, "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["windowed", "gxe", "exact"], default="windowed")
+    ap.add_argument("--workload", choices=["windowed", "gxe", "exact", "biobank"],
+                    default="windowed")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.workload == "exact":
+    if args.workload == "biobank":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "workload": "biobank",
+                              "unavailable": "the biobank workload has no reference arm; "
+                                             "the reference arm runs the default workload"}))
+            return
+        biobank_arm(args)
+    elif args.workload == "exact":
         exact_arm(args)
     elif args.workload == "gxe":
         if args.impl == "reference":

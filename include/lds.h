@@ -206,6 +206,12 @@ int lds_set_stream(void* cuda_stream); /* NULL restores the library's own stream
 int lds_geno_create(const uint8_t* bed_rows, int64_t bed_row_bytes, int64_t n_total, int64_t M,
                     const int64_t* row_sel, int64_t n_row_sel, int impute_mode,
                     uint64_t impute_seed, int ddof, int64_t* handle_out);
+/* Resident image of the library's seeded synthetic genotypes (the bytes of
+ * lds_synth_bed) generated on the device, with no host copy: t0/t1 are the
+ * per-SNP HWE thresholds (M each); no counterpart in the reference. */
+int lds_geno_create_synthetic(int64_t n_total, int64_t M, uint64_t seed, const int64_t* t0,
+                              const int64_t* t1, int missing, int impute_mode,
+                              uint64_t impute_seed, int ddof, int64_t* handle_out);
 int lds_geno_destroy(int64_t handle);
 int lds_gw_plan_create(int64_t geno, const double* annot, int64_t K, int nvecs, int step_size,
                        int vtile, uint64_t seed, int rand_dist, double resvar_eps, int as_float,

@@ -92,6 +92,7 @@ SIGNATURES: dict[str, tuple] = {
     "lds_generalized_source_product": (_int, [_i64, _i64, _i64, _p, _i64, _p]),
     "lds_generalized_target_product": (_int, [_i64, _i64, _i64, _p, _i64, _p]),
     "lds_debug_rademacher_block": (_int, [_u64, _int, _int, _int, _int, _p]),
+    "lds_geno_create_synthetic": (_int, [_i64, _i64, _u64, _p, _p, _int, _int, _u64, _int, _p]),
     "lds_gw_plan_create_shard": (_int, [_i64, _p, _i64, _int, _int, _int, _u64, _int, _dbl, _int,
                                         _int, _i64, _p]),
     "lds_gw_plan_tiles": (_int, [_i64, _p, _p, _p]),

@@ -263,10 +263,18 @@ uint64_t fnv1a(const void* data, size_t n, uint64_t h = 1469598103934665603ULL) 
 
 // Upload raw SNP-major rows, repack, count, impute, and compute statistics.
 // `global_snp0` is the genome index of the first row (HWE seeds use it).
+// Seeded synthetic genotypes generated straight into the image (no host copy).
+struct SynthSpec {
+    uint64_t seed;
+    const int64_t* t0;  // host, M thresholds each
+    const int64_t* t1;
+    int missing;
+};
+
 std::unique_ptr<Prepared> prepare(Context& c, const uint8_t* host_rows, int64_t row_bytes,
                                   int64_t n_total, int64_t M, const int64_t* row_sel,
                                   int64_t n_sel, int impute, uint64_t impute_seed, int ddof,
-                                  const std::string& key) {
+                                  const std::string& key, const SynthSpec* synth = nullptr) {
     auto P = std::make_unique<Prepared>();
     P->key = key;
     P->impute = impute;
@@ -292,11 +300,21 @@ std::unique_ptr<Prepared> prepare(Context& c, const uint8_t* host_rows, int64_t 
         d_rows = c.rows_dev.as<int32_t>(rows32.size());
         h2d(d_rows, rows32.data(), rows32.size(), c.st);
     }
+    if (synth) {
+        if (row_sel) fail(LDS_ERR_ARG, "synthetic images take no sample selection");
+        DevBuf dt0, dt1;
+        int64_t* a = dt0.as<int64_t>((size_t)std::max<int64_t>(M, 1));
+        int64_t* b = dt1.as<int64_t>((size_t)std::max<int64_t>(M, 1));
+        h2d(a, synth->t0, (size_t)M, c.st);
+        h2d(b, synth->t1, (size_t)M, c.st);
+        launch_synth(n_total, M, synth->seed, a, b, synth->missing, g.codes, c.st, g.nbp, 1);
+        ck(cudaStreamSynchronize(c.st), "synthetic image");
+    }
     // Upload in slabs to bound the staging buffer.
     const int64_t slab_rows =
         std::max<int64_t>(1, std::min<int64_t>(M, (int64_t)(1LL << 30) / std::max<int64_t>(row_bytes, 1)));
-    uint8_t* d_raw = c.raw.as<uint8_t>((size_t)(slab_rows * row_bytes));
-    for (int64_t j0 = 0; j0 < M; j0 += slab_rows) {
+    uint8_t* d_raw = synth ? nullptr : c.raw.as<uint8_t>((size_t)(slab_rows * row_bytes));
+    for (int64_t j0 = 0; !synth && j0 < M; j0 += slab_rows) {
         const int64_t nr = std::min(slab_rows, M - j0);
         h2d(d_raw, host_rows + j0 * row_bytes, (size_t)(nr * row_bytes), c.st);
         DevGeno sub = g;
@@ -3348,6 +3366,26 @@ LDS_API int lds_geno_create(const uint8_t* bed_rows, int64_t bed_row_bytes, int6
             fail(LDS_ERR_ARG, "impute_mode must be 'mean' or 'hwe'");
         std::shared_ptr<Prepared> P(prepare(c, bed_rows, bed_row_bytes, n_total, M, row_sel,
                                             n_row_sel, impute_mode, impute_seed, ddof, "handle"));
+        const int64_t h = next_handle();
+        geno_table()[h] = P;
+        *handle_out = h;
+    });
+}
+
+LDS_API int lds_geno_create_synthetic(int64_t n_total, int64_t M, uint64_t seed,
+                                      const int64_t* t0, const int64_t* t1, int missing,
+                                      int impute_mode, uint64_t impute_seed, int ddof,
+                                      int64_t* handle_out) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        ensure_device(c);
+        if (n_total <= 0 || M <= 0) fail(LDS_ERR_ARG, "invalid sizes");
+        if (impute_mode != LDS_IMPUTE_MEAN && impute_mode != LDS_IMPUTE_HWE)
+            fail(LDS_ERR_ARG, "impute_mode must be 'mean' or 'hwe'");
+        const SynthSpec spec{seed, t0, t1, missing};
+        std::shared_ptr<Prepared> P(prepare(c, nullptr, (n_total + 3) / 4, n_total, M, nullptr, 0,
+                                            impute_mode, impute_seed, ddof, "synthetic", &spec));
         const int64_t h = next_handle();
         geno_table()[h] = P;
         *handle_out = h;

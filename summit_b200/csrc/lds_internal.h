@@ -92,7 +92,7 @@ void launch_p2(const DevGeno& g, const P2Args& a, cudaStream_t st);
 // Synthetic generator (bedfile.py), writing n samples x M SNPs, row stride
 // ceil(n/4), into `out` (device).
 void launch_synth(int64_t n, int64_t M, uint64_t seed, const int64_t* t0, const int64_t* t1,
-                  int missing, uint8_t* out, cudaStream_t st);
+                  int missing, uint8_t* out, cudaStream_t st, int64_t ld = 0, int pad_missing = 0);
 
 // Exact products with the D nearest right-hand neighbours (lds_band.cu):
 // counts[(j (D+1) + d) 4 + {0..3}] = GG, GO, OG, OO integer sums of SNPs j, j+d;

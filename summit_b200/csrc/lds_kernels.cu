@@ -634,19 +634,29 @@ __device__ __forceinline__ uint64_t synth_draw(uint64_t key, uint64_t i, uint64_
     return mix64(key ^ mix64((j << 32) | i));
 }
 
+// Rows of `ld` bytes; with pad_missing the samples past n (and the bytes past
+// ceil(n/4)) carry the missing code 01, as the padded genotype image needs.
 __global__ void synth_kernel(int64_t n, int64_t M, uint64_t k2, uint64_t k3,
                              const int64_t* __restrict__ t0, const int64_t* __restrict__ t1,
-                             int missing, uint8_t* __restrict__ out) {
+                             int missing, uint8_t* __restrict__ out, int64_t ld,
+                             int pad_missing) {
     const int64_t nb = (n + 3) / 4;
     const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= nb) return;
+    if (b >= ld) return;
+    if (b >= nb) {
+        for (int64_t j = 0; j < M; ++j) out[j * ld + b] = 0x55;
+        return;
+    }
     long long u[4] = {0, 0, 0, 0};
     for (int64_t j = 0; j < M; ++j) {
         const long long a0 = t0[j], a1 = t1[j];
         uint32_t byte = 0;
         for (int t = 0; t < 4; ++t) {
             const int64_t i = b * 4 + t;
-            if (i >= n) break;
+            if (i >= n) {
+                if (pad_missing) byte |= 1u << (2 * t);
+                continue;
+            }
             const uint64_t r = synth_draw(k2, (uint64_t)i, (uint64_t)j);
             const long long e = (long long)(r & 0xFFFFULL) + (long long)((r >> 16) & 0xFFFFULL) +
                                 (long long)((r >> 32) & 0xFFFFULL) + (long long)(r >> 48) - 131070LL;
@@ -655,16 +665,18 @@ __global__ void synth_kernel(int64_t n, int64_t M, uint64_t k2, uint64_t k3,
             if (missing && (synth_draw(k3, (uint64_t)i, (uint64_t)j) >> 32) < 42949673ULL) code = 1u;
             byte |= code << (2 * t);
         }
-        out[j * nb + b] = (uint8_t)byte;
+        out[j * ld + b] = (uint8_t)byte;
     }
 }
 
 void launch_synth(int64_t n, int64_t M, uint64_t seed, const int64_t* t0, const int64_t* t1,
-                  int missing, uint8_t* out, cudaStream_t st) {
+                  int missing, uint8_t* out, cudaStream_t st, int64_t ld, int pad_missing) {
     const uint64_t k2 = mix64(seed ^ mix64(2ULL));
     const uint64_t k3 = mix64(seed ^ mix64(3ULL));
     const int64_t nb = (n + 3) / 4;
-    synth_kernel<<<(unsigned)((nb + 127) / 128), 128, 0, st>>>(n, M, k2, k3, t0, t1, missing, out);
+    if (ld <= 0) ld = nb;
+    synth_kernel<<<(unsigned)((ld + 127) / 128), 128, 0, st>>>(n, M, k2, k3, t0, t1, missing, out,
+                                                              ld, pad_missing);
     count_launch();
 }
 

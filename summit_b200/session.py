@@ -101,6 +101,25 @@ class GwSession:
                                           int(ddof), C.byref(h)))
         self.handle = h.value
 
+    @classmethod
+    def synthetic(cls, n: int, m: int, seed: int, missing: bool = True, impute_mode: str = "mean",
+                  impute_seed: int = 0, ddof: int = 1) -> "GwSession":
+        """Image of the seeded synthetic genotypes (gwldcore.synth_bed_rows'
+        bytes) generated on the device, with no host copy of the BED rows."""
+        from .bedfile import allele_freqs, hwe_thresholds
+
+        t0, t1 = hwe_thresholds(allele_freqs(seed, m))
+        self = cls.__new__(cls)
+        self.M, self.row_bytes = int(m), (int(n) + 3) // 4
+        self.n_total = self.N = int(n)
+        h = C.c_int64(0)
+        check(_lib.load().lds_geno_create_synthetic(
+            int(n), int(m), int(seed), ptr(np.ascontiguousarray(t0, dtype=np.int64)),
+            ptr(np.ascontiguousarray(t1, dtype=np.int64)), int(missing), _impute(impute_mode),
+            int(impute_seed), int(ddof), C.byref(h)))
+        self.handle = h.value
+        return self
+
     def plan(self, annot, nvecs: int, step_size: int, seed: int, rand_dist: str = "rademacher",
              vtile: int | None = None, eps: float = 1e-10, as_float: bool = False,
              with_mc: bool = False) -> GwPlan:

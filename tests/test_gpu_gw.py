@@ -195,3 +195,25 @@ def test_dropin_float32_overload(gw, reference, small_bed):
     # difference is the reference's single-precision GEMM error.
     assert rel_err(ours["meansq"], ref32["meansq_accum"]) < 1e-4
     assert np.isfinite(ours["meansq"]).all() and rel_err(ref32["meansq_accum"], ref64["meansq_accum"]) < 1.0
+
+
+@pytest.mark.parametrize("n,m", [(333, 410), (1000, 2600)])
+def test_synthetic_image_equals_uploaded_rows(gw, n, m):
+    """The image generated on the device equals the one uploaded from the same
+    generator's host rows: identical statistics and identical estimates."""
+    from summit_b200.session import GwSession
+
+    rows = gw.synth_bed_rows(n, m, 77)
+    a, b = GwSession(rows, n), GwSession.synthetic(n, m, 77)
+    sa, sb = a.stats(), b.stats()
+    np.testing.assert_array_equal(sa["mean"], sb["mean"])
+    np.testing.assert_array_equal(sa["sdinv"], sb["sdinv"])
+    annot = np.ones((m, 2))
+    annot[::3, 1] = 0
+    ra = a.plan(annot, 20, 250, 5)
+    rb = b.plan(annot, 20, 250, 5)
+    ra.execute()
+    rb.execute()
+    np.testing.assert_array_equal(ra.results()["ldscore"], rb.results()["ldscore"])
+    for x in (ra, rb, a, b):
+        x.close()
