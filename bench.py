@@ -906,6 +906,29 @@ def biobank_arm(args) -> None:
                      "memory; the image is generated on the device"),
         "gpu_launches": launches, "clocks": clk.summary(),
     }
+    if not os.environ.get("LDS_SKIP_CPU_BASELINE"):
+        # The reference's per-block native calls (gwldcore.cpp, compiled
+        # unchanged) on the leading SNPs of the same data (the generator's
+        # first L SNPs do not depend on M).
+        from oracle.oracle import Reference
+        from summit_b200 import bedfile, gwldcore
+
+        threads = cpu_threads()
+        L = env_int("LDS_BIO_CPU_SNPS", 2000)
+        ref = Reference()
+        ref.set_threads(threads)
+        with tempfile.TemporaryDirectory() as td:
+            pre = bedfile.write_plink(Path(td) / "bio", packed=gwldcore.synth_bed_rows(n, L, DATA_SEED),
+                                      n=n)
+            t0 = time.perf_counter()
+            ref.gw_ldscore(pre, n, L, np.ones((L, 1)), B, BLOCK, PROBE_SEED, dist="rademacher",
+                           impute="mean", dtype=np.float32)
+            sec = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": round(4.0 * n * L * B / sec / 1e12, 6), "unit": "TOPS",
+                                "cores": threads, "kind": "reference",
+                                "sample": f"first {L} SNPs of the workload (N={n}, K=1, B={B}); "
+                                          f"reference gwldcore.cpp compiled unchanged, float32, "
+                                          f"{sec:.1f} s"}
     print(json.dumps(line), flush=True)
 
 
