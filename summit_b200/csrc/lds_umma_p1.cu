@@ -37,8 +37,9 @@ constexpr int kThreads = 704;
 constexpr int kEpiThreads = 512;         // warps 6..21: four per TMEM lane quadrant
 constexpr int kAccCols = 256;            // one accumulator: <= 256 digit columns
 constexpr uint32_t kTmemCols = 512;      // two accumulators (MMA of job j+1 || epilogue of j)
-constexpr int kRing = 8;                 // gathered packed rows in flight per decoder thread
+constexpr int kRing = 6;                 // gathered packed rows in flight per decoder thread
 constexpr int kRingSlot = 128 * 32;      // 128 member rows x 32 bytes
+constexpr int kStageTile = 16 * 32;      // per epilogue warp: 16 digit rows x 32 samples
 }  // namespace p1
 
 __global__ void __launch_bounds__(p1::kThreads, 1)
@@ -48,7 +49,8 @@ __global__ void __launch_bounds__(p1::kThreads, 1)
     uint8_t* smem = reinterpret_cast<uint8_t*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* ring = smem + kStages * kStageBytes;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(ring + kRing * kRingSlot);
+    uint8_t* digit_stage = ring + kRing * kRingSlot;  // [epilogue warp][16 rows][32 samples]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(digit_stage + (kEpiThreads / 32) * kStageTile);
     uint64_t* full_w = bars;                    // [kStages] weight tiles landed (TMA)
     uint64_t* full_dec = bars + kStages;        // [kStages] genotype tiles decoded
     uint64_t* empty = bars + 2 * kStages;       // [kStages] stage consumed by the MMAs
@@ -269,7 +271,10 @@ __global__ void __launch_bounds__(p1::kThreads, 1)
                         if (vb < a.V) scB = a.colscale[o + vb];
                     }
                 }
-                int8_t* const yrow = a.yq ? a.yq + (int64_t)k * a.ncolp * a.N_pad + i : nullptr;
+                // The warp's 32 samples of this super-bin's digit rows start here.
+                int8_t* const ywarp =
+                    a.yq ? a.yq + (int64_t)k * a.ncolp * a.N_pad + i0 + q * 32 : nullptr;
+                uint8_t* const stage = digit_stage + (warp - 6) * kStageTile;
                 if (!mbar_wait(&acc_full[b], (uint32_t)u & 1u)) { fail(15); break; }
                 tc_fence_after();
                 const int ncols = min(kAccCols, a.ncolp - g * 256);
@@ -314,18 +319,31 @@ __global__ void __launch_bounds__(p1::kThreads, 1)
                             // first, no byte borrows from the next; byte 0
                             // subtracts 0.
                             w = ((w | 0x80808000u) - 0x3F3F3F00u) ^ 0x80808000u;
-                            // Digit t of probe v for this lane's sample: one byte
-                            // store per digit row; the warp's 32 lanes write 32
-                            // consecutive samples, one full sector per store.
-                            int8_t* dst = yrow + (int64_t)(4 * v) * a.N_pad;
-                            dst[0] = (int8_t)(w & 0xFFu);
-                            dst[a.N_pad] = (int8_t)((w >> 8) & 0xFFu);
-                            dst[2 * a.N_pad] = (int8_t)((w >> 16) & 0xFFu);
-                            dst[3 * a.N_pad] = (int8_t)(w >> 24);
+                            // Digit t of probe p of this chunk for this lane's
+                            // sample, staged as row 4p + t of a 16 x 32 byte tile.
+                            stage[(4 * p + 0) * 32 + lane] = (uint8_t)(w & 0xFFu);
+                            stage[(4 * p + 1) * 32 + lane] = (uint8_t)((w >> 8) & 0xFFu);
+                            stage[(4 * p + 2) * 32 + lane] = (uint8_t)((w >> 16) & 0xFFu);
+                            stage[(4 * p + 3) * 32 + lane] = (uint8_t)(w >> 24);
                         } else {
                             const double sc = __shfl_sync(0xffffffffu, vl < 32 ? scA : scB, vl & 31);
                             a.Y[((int64_t)k * a.V + v) * a.N_pad + i] = sc * (double)T;
                         }
+                    }
+                    if (a.yq) {
+                        // Write the staged tile: lane l stores 16 samples of digit
+                        // row l / 2 (one 16-byte store; the warp writes 16 rows x
+                        // 32 consecutive samples).
+                        __syncwarp();
+                        const int row = lane >> 1, half = lane & 1;
+                        const int v = g * 64 + c0c / 4 + (row >> 2);
+                        if (v < a.V) {
+                            const uint4 val =
+                                *reinterpret_cast<const uint4*>(stage + row * 32 + half * 16);
+                            *reinterpret_cast<uint4*>(ywarp + (int64_t)(4 * v + (row & 3)) * a.N_pad +
+                                                      half * 16) = val;
+                        }
+                        __syncwarp();
                     }
                 }
                 tc_fence_before();
@@ -438,7 +456,8 @@ void launch_p1_weights4(const P1UWeights& w, const double* mean, const double* s
 }
 
 size_t p1_umma_smem_bytes() {
-    return (size_t)p1::kStages * p1::kStageBytes + (size_t)p1::kRing * p1::kRingSlot + 1024 + 256;
+    return (size_t)p1::kStages * p1::kStageBytes + (size_t)p1::kRing * p1::kRingSlot +
+           (size_t)(p1::kEpiThreads / 32) * p1::kStageTile + 1024 + 256;
 }
 
 void prepare_p1_umma() {
