@@ -24,6 +24,7 @@
 #include <string>
 #include <sys/mman.h>
 #include <sys/stat.h>
+#include <functional>
 #include <thread>
 #include <unistd.h>
 #include <vector>
@@ -2114,10 +2115,24 @@ std::unique_ptr<WinPlan> win_plan_create(Context& c, std::shared_ptr<Prepared> P
     for (int64_t j = 0; j < M; ++j)
         pl->inv[(size_t)j] =
             as_float ? (double)inv_resvar<float>(*P, j, eps) : inv_resvar<double>(*P, j, eps);
+    // Per-window annotation totals, summed in SNP order within each window
+    // (windows in parallel on host threads).
     pl->Mkw.assign((size_t)(W * K), 0.0);
-    for (int64_t j = 0; j < M; ++j)
-        for (int64_t k = 0; k < K; ++k)
-            pl->Mkw[(size_t)(pl->win_of[(size_t)j] * K + k)] += annot[j * K + k];
+    const unsigned hw_win = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+    auto par_windows = [&](const std::function<void(int64_t)>& body) {
+        std::vector<std::thread> th;
+        std::atomic<int64_t> next{0};
+        for (unsigned t = 0; t < hw_win; ++t)
+            th.emplace_back([&] {
+                for (int64_t w; (w = next.fetch_add(1)) < W;) body(w);
+            });
+        for (auto& x : th) x.join();
+    };
+    par_windows([&](int64_t w) {
+        double* mk = &pl->Mkw[(size_t)(w * K)];
+        for (int64_t j = ws[w]; j < ws[w + 1]; ++j)
+            for (int64_t k = 0; k < K; ++k) mk[k] += annot[j * K + k];
+    });
     const double denom = std::max(1.0, (double)(N - P->ddof + 1) - 1.0);
     const double inv_denom2 = 1.0 / (denom * denom);
     std::vector<double> ls((size_t)M);
@@ -2137,6 +2152,14 @@ std::unique_ptr<WinPlan> win_plan_create(Context& c, std::shared_ptr<Prepared> P
         inv_f.resize((size_t)M);
         for (int64_t j = 0; j < M; ++j) inv_f[(size_t)j] = (float)pl->inv[(size_t)j];
     }
+    // Member lists of every (window, bin), built on host threads.
+    std::vector<Csr> parts((size_t)W);
+    par_windows([&](int64_t w) {
+        const int64_t a0 = ws[w], L = ws[w + 1] - ws[w];
+        parts[(size_t)w] = as_float
+            ? build_csr<float>(annot_f.data() + a0 * K, inv_f.data() + a0, L, K, a0, 16, 4, 128)
+            : build_csr<double>(annot + a0 * K, pl->inv.data() + a0, L, K, a0, 16, 4, 128);
+    });
     int64_t max_ksup = 0, max_wq = 0;
     for (int64_t w0 = 0; w0 < W; w0 += wb) {
         WinPlan::Batch b;
@@ -2151,10 +2174,7 @@ std::unique_ptr<WinPlan> win_plan_create(Context& c, std::shared_ptr<Prepared> P
         std::vector<double> scv;
         int64_t off = 0;
         for (int64_t w = b.w0; w < b.w1; ++w) {
-            const int64_t a0 = ws[w], L = ws[w + 1] - ws[w];
-            Csr part = as_float
-                           ? build_csr<float>(annot_f.data() + a0 * K, inv_f.data() + a0, L, K, a0, 16, 4, 128)
-                           : build_csr<double>(annot + a0 * K, pl->inv.data() + a0, L, K, a0, 16, 4, 128);
+            const Csr& part = parts[(size_t)w];
             for (int64_t k = 0; k < K; ++k) {
                 const int64_t sbk = (w - b.w0) * K + k;
                 cs.bin_off[(size_t)sbk] = off;
