@@ -417,7 +417,7 @@ def ours_arm(args) -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
 
     from summit_b200 import _lib, gwldcore
-    from summit_b200.session import GwSession, WinPlan, set_stream
+    from summit_b200.session import GwSession, WinPlan, set_stream, windowed_ldscore
 
     lib = _lib.load()
     stream = torch.cuda.Stream()
@@ -485,15 +485,12 @@ def ours_arm(args) -> None:
     if rank == 0 and not os.environ.get("LDS_SKIP_LEARNED"):
         lvp = learned_vs_plain(sess, annot, ws, stream)
 
-    # ---- end to end through the C ABI from pinned host buffers ----
+    # ---- end to end through the one-call C ABI entry from pinned host buffers ----
+    chunks = env_int("LDS_E2E_CHUNKS", 8)
+
     def e2e_once():
-        s2 = GwSession(bed_host, n, impute_mode="mean")
-        p2 = WinPlan(s2, annot, ws, B_PROBES, BLOCK, PROBE_SEED, "rademacher")
-        p2.execute()
-        out = p2.results(meansq=False)
-        p2.close()
-        s2.close()
-        return out
+        return windowed_ldscore(bed_host, n, annot, ws, B_PROBES, BLOCK, PROBE_SEED,
+                                "rademacher", impute_mode="mean", chunks=chunks)
 
     e2e_steps = max(1, min(args.steps, env_int("LDS_E2E_STEPS", 2)))
     e2e_once()  # warm
@@ -504,11 +501,16 @@ def ours_arm(args) -> None:
         out = e2e_once()
     torch.cuda.synchronize()
     e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
+    stage = np.zeros(4)
+    lib.lds_last_timings(_lib.ptr(stage), 4)  # host stage times of the last call
     barrier()
     assert np.allclose(out["ldscore"], res["ldscore"], rtol=0, atol=0)
     nnz = int((annot > 0).sum())
-    h2d = int(bed_host.nbytes + m * B_PROBES * 8 + nnz * 12 + m * 8 + ws.nbytes)
-    d2h = int(m * K_BINS * 8)
+    # uploads: BED rows, member lists (index + scale), per-SNP scale and window
+    # index, per-window bin totals; downloads: per-SNP code counts and LD scores
+    nw = int(len(ws) - 1)
+    h2d = int(bed_host.nbytes + nnz * 12 + m * 12 + nw * K_BINS * 8)
+    d2h = int(m * 16 + m * K_BINS * 8)
     sess.close()
 
     t = torch.tensor([ms, e2e_ms, gw_ms], dtype=torch.float64, device="cuda")
@@ -553,7 +555,12 @@ def ours_arm(args) -> None:
                 "algorithmic_ops_per_launch": ops2},
             "e2e": {"value": round(world * ops / (e2e_ms * 1e-3) / 1e12, 3), "unit": "TOPS",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "ms_per_step": round(e2e_ms, 1)},
+                    "ms_per_step": round(e2e_ms, 1),
+                    "call": f"lds_win_ldscore (upload streamed in {chunks} window-aligned chunks)",
+                    "stages_ms": {"first_estimate_enqueued": round(float(stage[0]), 1),
+                                  "all_enqueued": round(float(stage[1]), 1),
+                                  "results_copied": round(float(stage[2]), 1),
+                                  "buffers_released": round(float(stage[3]), 1)}},
             "gpu_launches": launches,
             "clocks": clocks,
         }

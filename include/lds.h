@@ -283,7 +283,35 @@ int lds_win_plan_execute(int64_t plan);
 int lds_win_plan_results(int64_t plan, double* ldscore, double* meansq_accum, double* inv_out,
                          double* mc_per_snp_sumsq);
 int lds_win_plan_kernel_ms(int64_t plan, double* ms4);
+/* Per-window annotation totals M_{w,k} (n_windows x K row-major, summed in SNP
+ * order within each window), the null the finalize subtracts as
+ * M_{w,k} / (N - ddof); the windowed counterpart of lds_gw_plan_bin_totals. */
+int lds_win_plan_bin_totals(int64_t plan, double* mkw_out);
 int lds_win_plan_destroy(int64_t plan);
+
+/* Windowed + partitioned LD scores in one call from host BED rows (the
+ * one-call form of lds_geno_create + lds_win_plan_create/execute/results,
+ * like lds_gw_ldscore for the genome-wide estimate; no single reference
+ * counterpart, see lds_win_plan_create).  The upload is streamed: the windows
+ * are cut into window-aligned chunks of about M / n_chunks SNPs (n_chunks <= 0:
+ * 8; 1: one chunk, no overlap), the first two of them a quarter and a half of
+ * that size, and chunk i+1's upload, repack, per-SNP statistics and plan
+ * set-up run on a second stream while chunk i's estimate runs on the library
+ * stream.  Chunk memory
+ * comes from a library-private stream-ordered pool that keeps its
+ * reservation between calls (lds_clear_device_cache releases it).
+ * Window seeds are counted from the global window index and HWE imputation
+ * seeds from the global SNP index, so the scores equal lds_win_plan_results
+ * of one plan over the whole image (same seed, windows, V-tiles) bit for bit.
+ * bed_rows: M rows of bed_row_bytes >= ceil(n_total/4) bytes (pinned host
+ * memory uploads at full PCIe rate).  ldscore: M x K; meansq_accum (M x K)
+ * and inv_out (M) may be NULL.  Returns after all outputs are written. */
+int lds_win_ldscore(const uint8_t* bed_rows, int64_t bed_row_bytes, int64_t n_total, int64_t M,
+                    const int64_t* row_sel, int64_t n_row_sel, const double* annot, int64_t K,
+                    const int64_t* window_starts, int64_t n_windows, int nvecs, int step_size,
+                    int vtile, uint64_t seed, int rand_dist, int ddof, int impute_mode,
+                    uint64_t impute_seed, double resvar_eps, int as_float, int n_chunks,
+                    double* ldscore, double* meansq_accum, double* inv_out);
 
 /* Control-variate outputs of a windowed plan (no counterpart in the reference;
  * they serve the learned control variate).  Call lds_win_plan_set_cv before the
@@ -316,7 +344,10 @@ int lds_debug_rademacher_block(uint64_t root, int blk_start, int v_start, int L,
 
 /* Device timing of the last lds_gw_ldscore call (milliseconds, CUDA events
  * on the library stream): [0] upload+prepare, [1] phase 1 total, [2] phase 2
- * total, [3] whole call. */
+ * total, [3] whole call.  After lds_win_ldscore: host wall-clock milliseconds
+ * from its start to [0] the first chunk's estimate enqueued, [1] every
+ * chunk's estimate enqueued, [2] every result copied out, [3] the chunks'
+ * device buffers released (the whole call). */
 int lds_last_timings(double* ms_out, int n);
 
 /* Verification entry: exact int64 products G^T y and O^T y of the int8

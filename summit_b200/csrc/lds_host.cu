@@ -81,23 +81,43 @@ int guarded(F&& f) {
 // Device buffers
 // ---------------------------------------------------------------------------
 // Owning device allocation; move-only so containers never double-free.
+// Stream-ordered allocation target of this thread: while a PoolScope is alive,
+// DevBuf allocations come from the library's private memory pool on its stream
+// and go back to it with cudaFreeAsync, which (unlike cudaFree) does not wait
+// for the whole device; the pool keeps its reservation for later calls.
+struct PoolTarget {
+    cudaMemPool_t pool = nullptr;
+    cudaStream_t st = nullptr;
+};
+thread_local PoolTarget t_pool;
+
+struct PoolScope {
+    PoolTarget saved;
+    PoolScope(cudaMemPool_t pool, cudaStream_t st) : saved(t_pool) { t_pool = {pool, st}; }
+    ~PoolScope() { t_pool = saved; }
+};
+
 struct DevBuf {
     void* p = nullptr;
     size_t n = 0;
+    cudaStream_t pool_st = nullptr;  // non-null: pool memory, freed in this stream's order
     DevBuf() = default;
     DevBuf(const DevBuf&) = delete;
     DevBuf& operator=(const DevBuf&) = delete;
-    DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) {
+    DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n), pool_st(o.pool_st) {
         o.p = nullptr;
         o.n = 0;
+        o.pool_st = nullptr;
     }
     DevBuf& operator=(DevBuf&& o) noexcept {
         if (this != &o) {
             release();
             p = o.p;
             n = o.n;
+            pool_st = o.pool_st;
             o.p = nullptr;
             o.n = 0;
+            o.pool_st = nullptr;
         }
         return *this;
     }
@@ -105,16 +125,25 @@ struct DevBuf {
         if (bytes <= n && p) return p;
         release();
         if (bytes == 0) bytes = 16;
-        ck(cudaMalloc(&p, bytes), "cudaMalloc");
+        if (t_pool.pool) {
+            ck(cudaMallocFromPoolAsync(&p, bytes, t_pool.pool, t_pool.st), "pool allocation");
+            pool_st = t_pool.st;
+        } else {
+            ck(cudaMalloc(&p, bytes), "cudaMalloc");
+        }
         n = bytes;
         return p;
     }
     template <typename T>
     T* as(size_t count) { return static_cast<T*>(get(count * sizeof(T))); }
     void release() {
-        if (p) cudaFree(p);
+        if (p) {
+            if (pool_st) cudaFreeAsync(p, pool_st);
+            else cudaFree(p);
+        }
         p = nullptr;
         n = 0;
+        pool_st = nullptr;
     }
     ~DevBuf() { release(); }
 };
@@ -185,7 +214,14 @@ struct Context {
     cudaStream_t st = nullptr;
     cudaEvent_t ev[8];
     std::list<std::unique_ptr<Prepared>> cache;  // most recent first
-    DevBuf raw, rows_dev, hwe_q0, hwe_q01, hwe_sb, counts_dev;
+    DevBuf raw, rows_dev, hwe_q0, hwe_q01, hwe_sb, counts_dev, units_dev;
+    // Image preparation stream of the streamed one-call windowed estimate
+    // (highest priority, so its short kernels are scheduled between the
+    // estimate's CTAs), and a grow-only pinned staging area for its results.
+    cudaStream_t st_prep = nullptr;
+    cudaMemPool_t pool = nullptr;   // chunk images and plans (PoolScope on st_prep)
+    void* pinned = nullptr;
+    size_t pinned_n = 0;
     DevBuf y, yq, ycs, wq, wcs, z, rowind, sc, binoff, wqoff, accum, mc, guards, lscale, xin;
     // Surrogate-network workspace, grow-only so that repeated training and
     // inference calls make no device allocations (cudaFree synchronizes).
@@ -275,7 +311,8 @@ struct SynthSpec {
 std::unique_ptr<Prepared> prepare(Context& c, const uint8_t* host_rows, int64_t row_bytes,
                                   int64_t n_total, int64_t M, const int64_t* row_sel,
                                   int64_t n_sel, int impute, uint64_t impute_seed, int ddof,
-                                  const std::string& key, const SynthSpec* synth = nullptr) {
+                                  const std::string& key, const SynthSpec* synth = nullptr,
+                                  int64_t snp_base = 0) {
     auto P = std::make_unique<Prepared>();
     P->key = key;
     P->impute = impute;
@@ -353,7 +390,7 @@ std::unique_ptr<Prepared> prepare(Context& c, const uint8_t* host_rows, int64_t 
             }
             q0[(size_t)j] = (1.0 - p) * (1.0 - p);
             q01[(size_t)j] = q0[(size_t)j] + 2.0 * p * (1.0 - p);
-            sb[(size_t)j] = hwe_seed_base(impute_seed, (int)j);
+            sb[(size_t)j] = hwe_seed_base(impute_seed, (int)(snp_base + j));
             any_missing |= k.n[3] > 0;
         }
         if (any_missing) {
@@ -452,12 +489,13 @@ void make_probes(uint64_t root, int blk_start, int v_start, int L, int V, int di
 void device_rademacher(Context& c, const std::vector<ProbeUnit>& units, int V, double* dZ,
                        int64_t ld) {
     if (units.empty()) return;
-    DevBuf du;
-    ProbeUnit* d = du.as<ProbeUnit>(units.size());
+    // The unit table lives in a grow-only context buffer: no cudaFree (which
+    // waits for the whole device) while other streams are busy.
+    ProbeUnit* d = c.units_dev.as<ProbeUnit>(units.size());
     h2d(d, units.data(), units.size(), c.st);
     launch_rademacher_units(d, (int64_t)units.size(), V, dZ, ld, c.st);
     ck(cudaGetLastError(), "probe streams");
-    ck(cudaStreamSynchronize(c.st), "probe streams");  // the unit table is freed on return
+    ck(cudaStreamSynchronize(c.st), "probe streams");  // the table is reused by the next call
 }
 
 // ---------------------------------------------------------------------------
@@ -2068,6 +2106,7 @@ struct WinPlan {
 
 // A context workspace of at least `bytes` (slot 0 sketch digits, 1 weight digits).
 std::shared_ptr<DevBuf> shared_workspace(Context& c, int slot, size_t bytes) {
+    PoolScope plain(nullptr, nullptr);  // outlives its plan: ordinary device memory
     std::shared_ptr<DevBuf>& w = c.ws[slot];
     if (!w || w->n < bytes) {
         w.reset();  // plans that captured the old buffer keep it alive
@@ -2086,7 +2125,7 @@ std::unique_ptr<WinPlan> win_plan_create(Context& c, std::shared_ptr<Prepared> P
                                          const double* annot, int64_t K, const int64_t* ws,
                                          int64_t W, int nvecs, int step, int vtile, uint64_t seed,
                                          int dist, double eps, int as_float, int with_mc,
-                                         double batch_gb) {
+                                         double batch_gb, int64_t w_base = 0) {
     const int64_t M = P->g.M, N = P->g.N, Np = P->g.N_pad;
     if (nvecs <= 0 || step <= 0 || K <= 0 || W <= 0) fail(LDS_ERR_ARG, "invalid sizes");
     if (ws[0] != 0 || ws[W] != M) fail(LDS_ERR_ARG, "windows must partition [0, M)");
@@ -2218,7 +2257,7 @@ std::unique_ptr<WinPlan> win_plan_create(Context& c, std::shared_ptr<Prepared> P
             for (size_t u = 0; u < units.size(); ++u) {
                 const int64_t w = units[u].first, s = units[u].second;
                 pu[u] = {ws[w] + s, (int32_t)std::min<int64_t>(step, ws[w + 1] - ws[w] - s), 0,
-                         probe_seed(window_seed(seed, w), (int)s, v0)};
+                         probe_seed(window_seed(seed, w_base + w), (int)s, v0)};
             }
             device_rademacher(c, pu, V, dZ, M);
             v0 += V;
@@ -2233,7 +2272,7 @@ std::unique_ptr<WinPlan> win_plan_create(Context& c, std::shared_ptr<Prepared> P
                     const int64_t w = units[u].first, s = units[u].second;
                     const int64_t a0 = ws[w];
                     const int L = (int)std::min<int64_t>(step, ws[w + 1] - a0 - s);
-                    const uint64_t rw = window_seed(seed, w);
+                    const uint64_t rw = window_seed(seed, w_base + w);
                     if (as_float) make_probes<float>(rw, (int)s, v0, L, V, dist, &Z[(size_t)(a0 + s)], M);
                     else make_probes<double>(rw, (int)s, v0, L, V, dist, &Z[(size_t)(a0 + s)], M);
                 }
@@ -2457,6 +2496,187 @@ void win_results(Context& c, WinPlan& pl, double* ldscore, double* meansq_out, d
     if (pl.with_mc && mc_snp) d2h(mc_snp, static_cast<double*>(pl.mc.p), MK, c.st);
     ck(cudaStreamSynchronize(c.st), "results copy");
     if (inv_out) std::memcpy(inv_out, pl.inv.data(), sizeof(double) * (size_t)M);
+}
+
+// Finalize of a windowed plan on c.st, outputs copied into pinned host memory
+// without waiting (the caller synchronizes before reading them).
+void win_results_async(Context& c, WinPlan& pl, double* h_ld, double* h_ms, unsigned* h_status) {
+    const int64_t M = pl.P->g.M, K = pl.K, N = pl.P->g.N;
+    const size_t MK = (size_t)(M * K);
+    double* dld = pl.ld_d.as<double>(MK);
+    double* dms = pl.ms_d.as<double>(MK);
+    launch_win_finalize(static_cast<double*>(pl.accum.p), pl.ntiles_out(), M, (int)K,
+                        (double)pl.nvecs, (double)(N - pl.P->ddof),
+                        static_cast<int32_t*>(pl.winof_d.p), static_cast<double*>(pl.mkw_d.p),
+                        dld, dms, c.st);
+    ck(cudaGetLastError(), "finalize");
+    d2h(h_status, static_cast<unsigned*>(pl.status.p), 1, c.st);
+    d2h(h_ld, dld, MK, c.st);
+    if (h_ms) d2h(h_ms, dms, MK, c.st);
+}
+
+// Windowed estimate in one call from host BED rows, with the upload streamed:
+// the windows are cut into window-aligned chunks of about M / n_chunks SNPs,
+// and chunk i+1's upload, repack, per-SNP statistics, residual variances,
+// member lists and probe streams (image preparation stream, highest priority)
+// run while chunk i's estimate runs on the library stream.  Every chunk is a
+// windowed plan over its own image with window seeds counted from the global
+// window index (and HWE seeds from the global SNP index), so the scores equal
+// those of one plan over the whole image bit for bit.  Nothing is freed while
+// estimates are in flight: cudaFree waits for the whole device.
+void win_ldscore_impl(const uint8_t* bed_rows, int64_t row_bytes, int64_t n_total, int64_t M,
+                      const int64_t* row_sel, int64_t n_sel, const double* annot, int64_t K,
+                      const int64_t* ws, int64_t W, int nvecs, int step, int vtile, uint64_t seed,
+                      int dist, int ddof, int impute, uint64_t iseed, double eps, int as_float,
+                      int n_chunks, double* ldscore, double* meansq_out, double* inv_out) {
+    using clk = std::chrono::steady_clock;
+    const auto t_start = clk::now();
+    auto ms_since = [&](clk::time_point t) {
+        return std::chrono::duration<double, std::milli>(clk::now() - t).count();
+    };
+    Context& c = ctx();
+    std::lock_guard<std::mutex> lk(c.mu);
+    ensure_device(c);
+    if (!bed_rows || !annot || !ws || !ldscore) fail(LDS_ERR_ARG, "null input or output");
+    if (row_bytes < (n_total + 3) / 4) fail(LDS_ERR_ARG, "bed_row_bytes smaller than ceil(N/4)");
+    if (impute != LDS_IMPUTE_MEAN && impute != LDS_IMPUTE_HWE)
+        fail(LDS_ERR_ARG, "impute_mode must be 'mean' or 'hwe'");
+    if (M <= 0 || K <= 0 || W <= 0) fail(LDS_ERR_ARG, "invalid sizes");
+    if (ws[0] != 0 || ws[W] != M) fail(LDS_ERR_ARG, "windows must partition [0, M)");
+    for (int64_t w = 0; w < W; ++w)
+        if (ws[w + 1] <= ws[w]) fail(LDS_ERR_ARG, "window starts must increase");
+    if (n_chunks <= 0) n_chunks = 8;
+    // Chunk boundaries: the first window start at or after M*f for f = 1/(4n),
+    // 3/(4n), then steps of 1/n.  The two short leading chunks make the one
+    // upload nothing overlaps short; each next chunk's set-up (about twice as
+    // fast as its estimate) still hides behind the previous chunk's estimate.
+    std::vector<int64_t> cw{0};
+    for (int i = 1; n_chunks > 1; ++i) {
+        const double f = i == 1 ? 0.25 / n_chunks : (i - 1.25) / n_chunks;
+        if (f >= 1.0) break;
+        const int64_t target = (int64_t)(f * (double)M);
+        int64_t w = cw.back() + 1;
+        while (w < W && ws[w] < target) ++w;
+        if (w < W) cw.push_back(w);
+    }
+    cw.push_back(W);
+    const size_t nc = cw.size() - 1;
+    if (!c.st_prep) {
+        int lo = 0, hi = 0;
+        ck(cudaDeviceGetStreamPriorityRange(&lo, &hi), "stream priorities");
+        ck(cudaStreamCreateWithPriority(&c.st_prep, cudaStreamNonBlocking, hi), "prep stream");
+    }
+    if (!c.pool) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = c.device;
+        ck(cudaMemPoolCreate(&c.pool, &props), "memory pool");
+        uint64_t keep = UINT64_MAX;  // keep the reservation (lds_clear_device_cache trims it)
+        ck(cudaMemPoolSetAttribute(c.pool, cudaMemPoolAttrReleaseThreshold, &keep), "pool attr");
+    }
+    // Grow the context buffers the chunks share to the largest chunk first, so
+    // that no chunk's preparation frees (and waits for) a buffer.
+    int64_t maxL = 0, max_units = 0;
+    for (size_t i = 0; i < nc; ++i) {
+        maxL = std::max(maxL, ws[cw[i + 1]] - ws[cw[i]]);
+        int64_t u = 0;
+        for (int64_t w = cw[i]; w < cw[i + 1]; ++w) u += (ws[w + 1] - ws[w] + step - 1) / step;
+        max_units = std::max(max_units, u);
+    }
+    c.counts_dev.as<SnpCounts>((size_t)maxL);
+    c.raw.as<uint8_t>((size_t)(std::max<int64_t>(
+                          1, std::min<int64_t>(maxL, (int64_t)(1LL << 30) / row_bytes)) *
+                      row_bytes));
+    c.units_dev.as<ProbeUnit>((size_t)std::max<int64_t>(max_units, 1));
+    if (row_sel) c.rows_dev.as<int32_t>((size_t)n_sel);
+    if (impute == LDS_IMPUTE_HWE) {
+        c.hwe_q0.as<double>((size_t)maxL);
+        c.hwe_q01.as<double>((size_t)maxL);
+        c.hwe_sb.as<uint64_t>((size_t)maxL);
+    }
+    const size_t MK = (size_t)(M * K);
+    const size_t need = sizeof(double) * MK * (meansq_out ? 2 : 1) + sizeof(unsigned) * nc;
+    if (c.pinned_n < need) {
+        if (c.pinned) cudaFreeHost(c.pinned);
+        c.pinned = nullptr;
+        c.pinned_n = 0;
+        ck(cudaHostAlloc(&c.pinned, need, cudaHostAllocDefault), "pinned staging");
+        c.pinned_n = need;
+    }
+    double* hld = static_cast<double*>(c.pinned);
+    double* hms = meansq_out ? hld + MK : nullptr;
+    unsigned* hst = reinterpret_cast<unsigned*>(hld + MK * (meansq_out ? 2 : 1));
+
+    struct Chunk {
+        std::shared_ptr<Prepared> P;
+        std::unique_ptr<WinPlan> plan;
+        cudaEvent_t done = nullptr;
+        bool copied = false;
+    };
+    std::vector<Chunk> ch(nc);
+    const cudaStream_t st_main = c.st;
+    struct Cleanup {
+        Context& c;
+        cudaStream_t st;
+        std::vector<Chunk>& ch;
+        ~Cleanup() {
+            c.st = st;
+            cudaStreamSynchronize(c.st_prep);
+            cudaStreamSynchronize(st);
+            for (Chunk& x : ch)
+                if (x.done) cudaEventDestroy(x.done);
+        }
+    } cleanup{c, st_main, ch};
+    auto copy_out = [&](size_t i) {
+        const int64_t j0 = ws[cw[i]], L = ws[cw[i + 1]] - j0;
+        if (hst[i]) fail(LDS_ERR_CUDA, "tensor-core pipeline wait timed out (code %u)", hst[i]);
+        std::memcpy(ldscore + j0 * K, hld + j0 * K, sizeof(double) * (size_t)(L * K));
+        if (meansq_out)
+            std::memcpy(meansq_out + j0 * K, hms + j0 * K, sizeof(double) * (size_t)(L * K));
+        if (inv_out) std::memcpy(inv_out + j0, ch[i].plan->inv.data(), sizeof(double) * (size_t)L);
+        ch[i].copied = true;
+    };
+    for (size_t i = 0; i < nc; ++i) {
+        const int64_t wa = cw[i], wb = cw[i + 1], j0 = ws[wa], L = ws[wb] - j0;
+        std::vector<int64_t> lws((size_t)(wb - wa + 1));
+        for (int64_t w = wa; w <= wb; ++w) lws[(size_t)(w - wa)] = ws[w] - j0;
+        c.st = c.st_prep;
+        {
+            // Chunk-owned memory from the pool, in st_prep's order; the host
+            // synchronizes st_prep before the library stream touches it.
+            PoolScope scope(c.pool, c.st_prep);
+            ch[i].P = prepare(c, bed_rows + j0 * row_bytes, row_bytes, n_total, L, row_sel, n_sel,
+                              impute, iseed, ddof, "stream", nullptr, j0);
+            ch[i].plan = win_plan_create(c, ch[i].P, annot + j0 * K, K, lws.data(), wb - wa,
+                                         nvecs, step, vtile, seed, dist, eps, as_float, 0, 8.0, wa);
+            ch[i].plan->ld_d.as<double>((size_t)(L * K));
+            ch[i].plan->ms_d.as<double>((size_t)(L * K));
+            ck(cudaStreamSynchronize(c.st_prep), "chunk set-up");
+        }
+        c.st = st_main;
+        win_execute(c, *ch[i].plan);
+        win_results_async(c, *ch[i].plan, hld + j0 * K, hms ? hms + j0 * K : nullptr, hst + i);
+        ck(cudaEventCreateWithFlags(&ch[i].done, cudaEventDisableTiming), "event");
+        ck(cudaEventRecord(ch[i].done, c.st), "event");
+        if (i == 0) c.timings[0] = ms_since(t_start);
+        // Copy out the chunks that have finished while later ones still run.
+        for (size_t q = 0; q < i; ++q)
+            if (!ch[q].copied && cudaEventQuery(ch[q].done) == cudaSuccess) copy_out(q);
+        (void)cudaGetLastError();  // cudaEventQuery's cudaErrorNotReady is not an error
+    }
+    c.timings[1] = ms_since(t_start);
+    for (size_t i = 0; i < nc; ++i) {
+        if (ch[i].copied) continue;
+        ck(cudaEventSynchronize(ch[i].done), "chunk results");
+        copy_out(i);
+    }
+    c.timings[2] = ms_since(t_start);
+    for (Chunk& x : ch) {
+        x.plan.reset();
+        x.P.reset();
+    }
+    c.timings[3] = ms_since(t_start);
 }
 
 // Control-variate outputs of a windowed plan; call before its first execute.
@@ -3040,8 +3260,15 @@ LDS_API void lds_clear_device_cache(void) {
     for (auto& w : c.ws) w.reset();
     for (DevBuf* b : {&c.raw, &c.rows_dev, &c.hwe_q0, &c.hwe_q01, &c.hwe_sb, &c.counts_dev, &c.y,
                       &c.yq, &c.ycs, &c.wq, &c.wcs, &c.z, &c.rowind, &c.sc, &c.binoff, &c.wqoff,
-                      &c.accum, &c.mc, &c.guards, &c.lscale, &c.xin})
+                      &c.accum, &c.mc, &c.guards, &c.lscale, &c.xin, &c.units_dev})
         b->release();
+    if (c.pool) {
+        cudaDeviceSynchronize();
+        cudaMemPoolTrimTo(c.pool, 0);
+    }
+    if (c.pinned) cudaFreeHost(c.pinned);
+    c.pinned = nullptr;
+    c.pinned_n = 0;
 }
 
 #define P1_ARGS(T)                                                                              \
@@ -3978,6 +4205,21 @@ LDS_API int lds_win_plan_create(int64_t geno, const double* annot, int64_t K,
     });
 }
 
+LDS_API int lds_win_ldscore(const uint8_t* bed_rows, int64_t bed_row_bytes, int64_t n_total,
+                            int64_t M, const int64_t* row_sel, int64_t n_row_sel,
+                            const double* annot, int64_t K, const int64_t* window_starts,
+                            int64_t n_windows, int nvecs, int step_size, int vtile, uint64_t seed,
+                            int rand_dist, int ddof, int impute_mode, uint64_t impute_seed,
+                            double resvar_eps, int as_float, int n_chunks, double* ldscore,
+                            double* meansq_accum, double* inv_out) {
+    return guarded([&] {
+        win_ldscore_impl(bed_rows, bed_row_bytes, n_total, M, row_sel, n_row_sel, annot, K,
+                         window_starts, n_windows, nvecs, step_size, vtile, seed, rand_dist, ddof,
+                         impute_mode, impute_seed, resvar_eps, as_float, n_chunks, ldscore,
+                         meansq_accum, inv_out);
+    });
+}
+
 static WinPlan& win_of_handle(int64_t h) {
     auto it = win_table().find(h);
     if (it == win_table().end()) fail(LDS_ERR_ARG, "unknown windowed plan handle");
@@ -4009,6 +4251,16 @@ LDS_API int lds_win_plan_kernel_ms(int64_t plan, double* ms4) {
         ck(cudaStreamSynchronize(c.st), "sync");
         win_times(pl);
         for (int i = 0; i < 4; ++i) ms4[i] = pl.kernel_ms[i];
+    });
+}
+
+LDS_API int lds_win_plan_bin_totals(int64_t plan, double* mkw_out) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        const WinPlan& pl = win_of_handle(plan);
+        if (!mkw_out) fail(LDS_ERR_ARG, "null output");
+        std::memcpy(mkw_out, pl.Mkw.data(), sizeof(double) * pl.Mkw.size());
     });
 }
 

@@ -76,9 +76,9 @@ class LearnedCV:
         self.annot = torch.from_numpy(annot).to(dev)
         ws_t = torch.from_numpy(ws).to(dev)
         win = torch.repeat_interleave(torch.arange(W, device=dev), torch.from_numpy(sizes).to(dev))
-        # correlation null M_k(window) / (N - ddof), as the plain estimator applies it;
-        # per-window annotation sums in SNP order on the host (W x K), gathered per SNP
-        mkw = torch.from_numpy(np.add.reduceat(annot, ws[:-1], axis=0)).to(dev)
+        # correlation null M_k(window) / (N - ddof), as the plain estimator applies it:
+        # the plan's per-window annotation totals (W x K, SNP order), gathered per SNP
+        mkw = torch.from_numpy(self.plan.bin_totals()).to(dev)
         nd = float(session.N - 1)
         self.null = mkw[win] / nd
         # static features: MAF, annotations, window geometry
@@ -92,12 +92,13 @@ class LearnedCV:
                            edge / torch.clamp(size, min=1).double(),
                            torch.clamp(edge, max=100.0) / 100.0], 1)
         self.static = torch.cat([2.0 * maf[:, None], self.annot, geo], 1).float().contiguous()
-        rng = np.random.default_rng(cfg.seed)
-        perm = rng.permutation(M)
+        gen = torch.Generator(device=dev)
+        gen.manual_seed(cfg.seed)
+        perm = torch.randperm(M, generator=gen, device=dev)
         ntr = max(1, int(round(cfg.train_frac * M)))
         nva = max(1, int(round(cfg.val_frac * M)))
-        self.train_rows = torch.from_numpy(np.sort(perm[:ntr])).to(dev)
-        self.val_rows = torch.from_numpy(np.sort(perm[ntr:ntr + nva])).to(dev)
+        self.train_rows = torch.sort(perm[:ntr]).values
+        self.val_rows = torch.sort(perm[ntr:ntr + nva]).values
         T = 2
         f64 = dict(dtype=torch.float64, device=dev)
         self.meansq = torch.empty((T, M, K), **f64)

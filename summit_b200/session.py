@@ -232,6 +232,7 @@ class WinPlan:
         annot = np.ascontiguousarray(annot, dtype=np.float64)
         ws = np.ascontiguousarray(window_starts, dtype=np.int64)
         self.M, self.K = annot.shape
+        self.W = ws.size - 1
         self.with_mc = with_mc
         h = C.c_int64(0)
         check(_lib.load().lds_win_plan_create(session.handle, ptr(annot), self.K, ptr(ws),
@@ -261,6 +262,12 @@ class WinPlan:
         return {"weights": buf[0], "phase1": buf[1], "digits": buf[2], "phase2": buf[3]}
 
     # ---- control-variate outputs (see lds_win_plan_set_cv) ----
+    def bin_totals(self) -> np.ndarray:
+        """Per-window annotation totals M_{w,k} (W x K, summed in SNP order)."""
+        out = np.empty((self.W, self.K))
+        check(_lib.load().lds_win_plan_bin_totals(self.handle, ptr(out)))
+        return out
+
     def set_cv(self, annot, split_tiles: bool = True, band: int = 8) -> None:
         annot = np.ascontiguousarray(annot, dtype=np.float64)
         check(_lib.load().lds_win_plan_set_cv(self.handle, ptr(annot), int(split_tiles), int(band)))
@@ -308,6 +315,40 @@ class WinPlan:
             self.close()
         except Exception:
             pass
+
+
+def windowed_ldscore(bed_rows, n_total: int, annot, window_starts, nvecs: int, step_size: int,
+                     seed: int, rand_dist: str = "rademacher", vtile: int | None = None,
+                     ddof: int = 1, impute_mode: str = "mean", impute_seed: int = 0,
+                     eps: float = 1e-10, as_float: bool = False, row_sel=None, chunks: int = 8,
+                     meansq: bool = False) -> dict:
+    """Windowed + partitioned LD scores in one call from host BED rows.
+
+    Same estimate as ``WinPlan(GwSession(bed_rows, ...), ...)`` (bit for bit),
+    with the upload streamed in ``chunks`` window-aligned pieces: the next
+    piece's upload and set-up overlap the current piece's kernels.  Pass
+    ``bed_rows`` in pinned memory (e.g. a ``pin_memory=True`` torch tensor's
+    ``.numpy()``) for full-rate uploads.  Returns ``ldscore`` (M x K) and, with
+    ``meansq``, ``meansq_accum`` and ``inv``.
+    """
+    bed_rows = np.ascontiguousarray(bed_rows, dtype=np.uint8)
+    M, row_bytes = bed_rows.shape
+    annot = np.ascontiguousarray(annot, dtype=np.float64)
+    ws = np.ascontiguousarray(window_starts, dtype=np.int64)
+    if annot.ndim != 2 or annot.shape[0] != M:
+        raise ValueError("annot must be (M, K) with M = bed_rows.shape[0]")
+    K = annot.shape[1]
+    ld = np.empty((M, K))
+    ms = np.empty((M, K)) if meansq else None
+    inv = np.empty(M) if meansq else None
+    rows, nr = _rows(row_sel)
+    check(_lib.load().lds_win_ldscore(ptr(bed_rows), row_bytes, int(n_total), M, ptr(rows), nr,
+                                      ptr(annot), K, ptr(ws), ws.size - 1, int(nvecs),
+                                      int(step_size), int(vtile or 0), int(seed), _dist(rand_dist),
+                                      int(ddof), _impute(impute_mode), int(impute_seed),
+                                      float(eps), int(as_float), int(chunks), ptr(ld), ptr(ms),
+                                      ptr(inv)))
+    return {"ldscore": ld, "meansq_accum": ms, "inv": inv}
 
 
 def window_seed(seed: int, w: int) -> int:
