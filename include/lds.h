@@ -370,6 +370,13 @@ int lds_debug_xt_products_umma(const uint8_t* bed_rows, int64_t bed_row_bytes, i
 /* Phase-2 kernel selection: 1 = tcgen05 (default), 0 = mma.sync.  Applies to
  * plans created afterwards.  No reference counterpart. */
 int lds_set_p2_kernel(int impl);
+/* Windowed phase 2 on SM pairs: on != 0 runs the windowed plans' phase 2 as
+ * clusters of two CTAs (tcgen05.mma.cta_group::2, M = 256: two 128-SNP tiles
+ * of a window share each sketch tile, each SM holding half of its columns).
+ * Same results bit for bit.  Applies to plans executed for the first time
+ * afterwards (the first execute captures the graph).  No reference
+ * counterpart. */
+int lds_set_p2_pairs(int on);
 
 /* Synthetic genotype image generated on the device with the integer-exact
  * generator (identical bytes to the numpy generator in bedfile.py):

@@ -185,6 +185,12 @@ CUtensorMap make_map_2d(void* base, uint64_t inner, uint64_t outer, uint64_t row
 }
 
 // Phase-2 implementation: 1 = tcgen05 (default; needs 4 digits), 0 = mma.sync.
+// Windowed phase 2 on SM pairs (p2_umma_pair_kernel): 1 = on.
+int& p2_pairs() {
+    static int on = 0;
+    return on;
+}
+
 int& p2_impl() {
     static int v = [] {
         const char* s = std::getenv("LDS_P2_KERNEL");
@@ -2065,8 +2071,8 @@ struct WinPlan {
     struct Batch {
         int64_t w0 = 0, w1 = 0, ksup = 0, lmax = 0;
         Csr csr;
-        DevBuf rowind, sc, binoff, tiles;
-        int64_t ntiles = 0;
+        DevBuf rowind, sc, binoff, tiles, ptiles;
+        int64_t ntiles = 0, nptiles = 0;   // 128-SNP tiles; pairs of tiles (SM-pair kernel)
     };
     std::vector<Batch> batches;
     std::vector<DevBuf> z;              // per V-tile, M x V FP64 probes
@@ -2237,6 +2243,12 @@ std::unique_ptr<WinPlan> win_plan_create(Context& c, std::shared_ptr<Prepared> P
                 tiles.push_back(make_int4((int)j, (int)ws[w + 1], (int)((w - b.w0) * K), 0));
         b.ntiles = (int64_t)tiles.size();
         h2d(b.tiles.as<int4>(tiles.size()), tiles.data(), tiles.size(), c.st);
+        std::vector<int4> ptiles;  // pairs of consecutive tiles of one window
+        for (int64_t w = b.w0; w < b.w1; ++w)
+            for (int64_t j = ws[w]; j < ws[w + 1]; j += 256)
+                ptiles.push_back(make_int4((int)j, (int)ws[w + 1], (int)((w - b.w0) * K), 0));
+        b.nptiles = (int64_t)ptiles.size();
+        h2d(b.ptiles.as<int4>(ptiles.size()), ptiles.data(), ptiles.size(), c.st);
         ck(cudaStreamSynchronize(c.st), "window batch upload");
         max_ksup = std::max(max_ksup, b.ksup);
         max_wq = std::max(max_wq, b.ksup * 2 * ncmax * b.lmax);
@@ -2297,6 +2309,7 @@ std::unique_ptr<WinPlan> win_plan_create(Context& c, std::shared_ptr<Prepared> P
     for (auto& e : pl->ev) ck(cudaEventCreate(&e), "event");
     umma::prepare_p1_umma();
     umma::prepare_p2_umma();
+    umma::prepare_p2_umma_pair();
     ck(cudaStreamSynchronize(c.st), "window plan");
     return pl;
 }
@@ -2421,8 +2434,18 @@ void win_enqueue(Context& c, WinPlan& pl) {
             u.extreme_warn = extreme_warn_env();
             u.drop_extreme = drop_extreme_env();
             u.status = static_cast<unsigned*>(pl.status.p);
-            u.tiles = static_cast<int4*>(b.tiles.p);
-            umma::launch_p2_umma(pl.tmA, tmB, u, c.st);
+            if (p2_pairs()) {
+                // Each CTA of a pair copies half of the sketch tile's columns.
+                const CUtensorMap tmBh =
+                    make_map_2d(pl.yq->p, (uint64_t)Np, (uint64_t)(b.ksup * nc), (uint64_t)Np, 128,
+                                (uint32_t)(std::min(256, nb * nc) / 2), CU_TENSOR_MAP_SWIZZLE_128B);
+                u.tiles = static_cast<int4*>(b.ptiles.p);
+                u.j1 = b.nptiles;  // number of tile pairs
+                umma::launch_p2_umma_pair(pl.tmA, tmBh, u, c.st);
+            } else {
+                u.tiles = static_cast<int4*>(b.tiles.p);
+                umma::launch_p2_umma(pl.tmA, tmB, u, c.st);
+            }
             ck(cudaEventRecordWithFlags(pl.ev[(size_t)e++], c.st, cudaEventRecordExternal), "event");
         }
     }
@@ -4174,6 +4197,11 @@ LDS_API int lds_debug_xt_products_umma(const uint8_t* bed_rows, int64_t bed_row_
         ck(cudaStreamSynchronize(c.st), "debug umma products");
         if (stv) fail(LDS_ERR_CUDA, "phase-2 tensor-core pipeline wait timed out (code %u)", stv);
     });
+}
+
+LDS_API int lds_set_p2_pairs(int on) {
+    p2_pairs() = on ? 1 : 0;
+    return LDS_OK;
 }
 
 LDS_API int lds_set_p2_kernel(int impl) {
