@@ -454,8 +454,22 @@ def ours_arm(args) -> None:
 
     sess = GwSession(bed_host, n, impute_mode="mean")
 
+    # ---- tiling of the windowed plans: the project's autotuner, timed on this
+    # device before the measured region (phase-1 split, window batching,
+    # phase-2 tile shape; every candidate's scores must agree bit for bit) ----
+    from summit_b200 import autotune
+
+    cands = ([{"p1_sb_per_cta": s, "batch_gb": 8.0, "p2_pairs": 0} for s in (4, 8, 16)] +
+             [{"p1_sb_per_cta": 8, "batch_gb": 4.0, "p2_pairs": 0},
+              {"p1_sb_per_cta": 8, "batch_gb": 8.0, "p2_pairs": 1}])
+    t_tune = time.perf_counter()
+    tune = autotune.tune_windowed(sess, annot, ws, B_PROBES, BLOCK, PROBE_SEED, "rademacher",
+                                  candidates=cands, reps=1)
+    tune_s = time.perf_counter() - t_tune
+
     # ---- headline: windowed + partitioned, one graph launch per estimate ----
-    wplan = WinPlan(sess, annot, ws, B_PROBES, BLOCK, PROBE_SEED, "rademacher")
+    wplan = autotune.tuned_win_plan(sess, annot, ws, B_PROBES, BLOCK, PROBE_SEED, "rademacher",
+                                    tune_if_missing=False)
     for _ in range(args.warmup):
         wplan.execute()
     torch.cuda.synchronize()
@@ -490,7 +504,8 @@ def ours_arm(args) -> None:
 
     def e2e_once():
         return windowed_ldscore(bed_host, n, annot, ws, B_PROBES, BLOCK, PROBE_SEED,
-                                "rademacher", impute_mode="mean", chunks=chunks)
+                                "rademacher", impute_mode="mean", chunks=chunks,
+                                tiling=tune["config"])
 
     e2e_steps = max(1, min(args.steps, env_int("LDS_E2E_STEPS", 2)))
     e2e_once()  # warm
@@ -538,6 +553,9 @@ def ours_arm(args) -> None:
                        "K": K_BINS, "B": B_PROBES, "block": BLOCK, "impute": "mean",
                        "digits": lib.lds_get_slices(), "parallelism": f"partition x{world} (each rank its own chromosome; no collective)",
                        "graph": "one CUDA graph launch per estimate",
+                       "tiling": {"config": tune["config"], "tuned_ms": tune["ms"],
+                                  "cached": tune["cached"], "tune_s": round(tune_s, 1),
+                                  "trials": tune.get("trials")},
                        "l2": "inputs larger than L2 (6.3 GB genotype image per step)"},
             "kernel_ms": {k: round(v, 3) for k, v in kms.items()},
             "genome_wide": {"value": round(world * ops / (gw_ms * 1e-3) / 1e12, 3),

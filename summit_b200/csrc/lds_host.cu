@@ -2081,6 +2081,9 @@ struct WinPlan {
     // Optional outputs for the control variate (lds_win_plan_set_cv): per-V-tile
     // meansq slices, near-field sums C and known means mu, neighbour products.
     int split = 0, cv_D = 0;
+    // Tiling chosen for this plan (lds_win_plan_set_tiling): phase-1 super-bins
+    // per CTA (0: default) and phase 2 on SM pairs (-1: the global switch).
+    int p1_spc = 0, pairs = -1;
     DevBuf annot_d, winof_d, sqrt_ls, xx, band_cnt, cvC, cvMu;
     DevBuf mkw_d, ld_d, ms_d;           // finalize inputs and outputs
     cudaEvent_t cv_ev[2] = {nullptr, nullptr};
@@ -2396,7 +2399,7 @@ void win_enqueue(Context& c, WinPlan& pl) {
                 const int v = e ? std::atoi(e) : 0;
                 return v > 0 ? v : 8;
             }();
-            pa.sb_per_cta = spc;
+            pa.sb_per_cta = pl.p1_spc > 0 ? pl.p1_spc : spc;
             pa.yq = static_cast<int8_t*>(pl.yq->p);
             pa.ycolscale = static_cast<double*>(pl.ycs.p);
             pa.yshift = static_cast<int*>(pl.yshift.p);
@@ -2434,7 +2437,7 @@ void win_enqueue(Context& c, WinPlan& pl) {
             u.extreme_warn = extreme_warn_env();
             u.drop_extreme = drop_extreme_env();
             u.status = static_cast<unsigned*>(pl.status.p);
-            if (p2_pairs()) {
+            if (pl.pairs >= 0 ? pl.pairs != 0 : p2_pairs() != 0) {
                 // Each CTA of a pair copies half of the sketch tile's columns.
                 const CUtensorMap tmBh =
                     make_map_2d(pl.yq->p, (uint64_t)Np, (uint64_t)(b.ksup * nc), (uint64_t)Np, 128,
@@ -2551,7 +2554,8 @@ void win_ldscore_impl(const uint8_t* bed_rows, int64_t row_bytes, int64_t n_tota
                       const int64_t* row_sel, int64_t n_sel, const double* annot, int64_t K,
                       const int64_t* ws, int64_t W, int nvecs, int step, int vtile, uint64_t seed,
                       int dist, int ddof, int impute, uint64_t iseed, double eps, int as_float,
-                      int n_chunks, double* ldscore, double* meansq_out, double* inv_out) {
+                      int n_chunks, int p1_spc, int pairs, double* ldscore, double* meansq_out,
+                      double* inv_out) {
     using clk = std::chrono::steady_clock;
     const auto t_start = clk::now();
     auto ms_since = [&](clk::time_point t) {
@@ -2673,6 +2677,8 @@ void win_ldscore_impl(const uint8_t* bed_rows, int64_t row_bytes, int64_t n_tota
                               impute, iseed, ddof, "stream", nullptr, j0);
             ch[i].plan = win_plan_create(c, ch[i].P, annot + j0 * K, K, lws.data(), wb - wa,
                                          nvecs, step, vtile, seed, dist, eps, as_float, 0, 8.0, wa);
+            ch[i].plan->p1_spc = std::max(0, p1_spc);
+            ch[i].plan->pairs = pairs < 0 ? -1 : (pairs ? 1 : 0);
             ch[i].plan->ld_d.as<double>((size_t)(L * K));
             ch[i].plan->ms_d.as<double>((size_t)(L * K));
             ck(cudaStreamSynchronize(c.st_prep), "chunk set-up");
@@ -4238,13 +4244,13 @@ LDS_API int lds_win_ldscore(const uint8_t* bed_rows, int64_t bed_row_bytes, int6
                             const double* annot, int64_t K, const int64_t* window_starts,
                             int64_t n_windows, int nvecs, int step_size, int vtile, uint64_t seed,
                             int rand_dist, int ddof, int impute_mode, uint64_t impute_seed,
-                            double resvar_eps, int as_float, int n_chunks, double* ldscore,
-                            double* meansq_accum, double* inv_out) {
+                            double resvar_eps, int as_float, int n_chunks, int p1_sb_per_cta,
+                            int p2_pairs, double* ldscore, double* meansq_accum, double* inv_out) {
     return guarded([&] {
         win_ldscore_impl(bed_rows, bed_row_bytes, n_total, M, row_sel, n_row_sel, annot, K,
                          window_starts, n_windows, nvecs, step_size, vtile, seed, rand_dist, ddof,
-                         impute_mode, impute_seed, resvar_eps, as_float, n_chunks, ldscore,
-                         meansq_accum, inv_out);
+                         impute_mode, impute_seed, resvar_eps, as_float, n_chunks, p1_sb_per_cta,
+                         p2_pairs, ldscore, meansq_accum, inv_out);
     });
 }
 
@@ -4279,6 +4285,19 @@ LDS_API int lds_win_plan_kernel_ms(int64_t plan, double* ms4) {
         ck(cudaStreamSynchronize(c.st), "sync");
         win_times(pl);
         for (int i = 0; i < 4; ++i) ms4[i] = pl.kernel_ms[i];
+    });
+}
+
+LDS_API int lds_win_plan_set_tiling(int64_t plan, int p1_sb_per_cta, int p2_pairs) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        WinPlan& pl = win_of_handle(plan);
+        if (pl.graph) fail(LDS_ERR_ARG, "set the tiling before the plan's first execute");
+        if (p1_sb_per_cta < 0 || p1_sb_per_cta > 4096)
+            fail(LDS_ERR_ARG, "p1_sb_per_cta must be in [0, 4096]");
+        pl.p1_spc = p1_sb_per_cta;
+        pl.pairs = p2_pairs < 0 ? -1 : (p2_pairs ? 1 : 0);
     });
 }
 

@@ -262,6 +262,11 @@ class WinPlan:
         return {"weights": buf[0], "phase1": buf[1], "digits": buf[2], "phase2": buf[3]}
 
     # ---- control-variate outputs (see lds_win_plan_set_cv) ----
+    def set_tiling(self, p1_sb_per_cta: int = 0, p2_pairs: int = -1) -> None:
+        """Phase-1 super-bins per CTA (0: default) and phase 2 on SM pairs
+        (1/0; -1: the global switch); call before the first execute."""
+        check(_lib.load().lds_win_plan_set_tiling(self.handle, int(p1_sb_per_cta), int(p2_pairs)))
+
     def bin_totals(self) -> np.ndarray:
         """Per-window annotation totals M_{w,k} (W x K, summed in SNP order)."""
         out = np.empty((self.W, self.K))
@@ -321,7 +326,7 @@ def windowed_ldscore(bed_rows, n_total: int, annot, window_starts, nvecs: int, s
                      seed: int, rand_dist: str = "rademacher", vtile: int | None = None,
                      ddof: int = 1, impute_mode: str = "mean", impute_seed: int = 0,
                      eps: float = 1e-10, as_float: bool = False, row_sel=None, chunks: int = 8,
-                     meansq: bool = False) -> dict:
+                     meansq: bool = False, tiling: dict | None = None) -> dict:
     """Windowed + partitioned LD scores in one call from host BED rows.
 
     Same estimate as ``WinPlan(GwSession(bed_rows, ...), ...)`` (bit for bit),
@@ -329,8 +334,10 @@ def windowed_ldscore(bed_rows, n_total: int, annot, window_starts, nvecs: int, s
     piece's upload and set-up overlap the current piece's kernels.  Pass
     ``bed_rows`` in pinned memory (e.g. a ``pin_memory=True`` torch tensor's
     ``.numpy()``) for full-rate uploads.  Returns ``ldscore`` (M x K) and, with
-    ``meansq``, ``meansq_accum`` and ``inv``.
+    ``meansq``, ``meansq_accum`` and ``inv``.  ``tiling`` (``p1_sb_per_cta``,
+    ``p2_pairs``, e.g. an autotuner record's config) sets the chunks' tiling.
     """
+    tiling = tiling or {}
     bed_rows = np.ascontiguousarray(bed_rows, dtype=np.uint8)
     M, row_bytes = bed_rows.shape
     annot = np.ascontiguousarray(annot, dtype=np.float64)
@@ -346,8 +353,9 @@ def windowed_ldscore(bed_rows, n_total: int, annot, window_starts, nvecs: int, s
                                       ptr(annot), K, ptr(ws), ws.size - 1, int(nvecs),
                                       int(step_size), int(vtile or 0), int(seed), _dist(rand_dist),
                                       int(ddof), _impute(impute_mode), int(impute_seed),
-                                      float(eps), int(as_float), int(chunks), ptr(ld), ptr(ms),
-                                      ptr(inv)))
+                                      float(eps), int(as_float), int(chunks),
+                                      int(tiling.get("p1_sb_per_cta", 0)),
+                                      int(tiling.get("p2_pairs", -1)), ptr(ld), ptr(ms), ptr(inv)))
     return {"ldscore": ld, "meansq_accum": ms, "inv": inv}
 
 
