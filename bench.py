@@ -340,10 +340,10 @@ def learned_vs_plain(sess, annot, ws, stream) -> dict:
                     "mean_ld_rel_err": 0.0, "snp_rel_rmse": 0.0,
                     "method": "exact expectation of the estimator (int8 Gram tensor-core kernel)"}
 
-    def plain(B, device=True):
+    def plain(B, device=True, seed=PROBE_SEED):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        p = WinPlan(sess, annot, ws, B, BLOCK, PROBE_SEED, "rademacher")
+        p = WinPlan(sess, annot, ws, B, BLOCK, seed, "rademacher")
         p.execute()
         ld = p.results()["ldscore"]
         wall = time.perf_counter() - t0
@@ -363,7 +363,7 @@ def learned_vs_plain(sess, annot, ws, stream) -> dict:
 
     _, out["plain_b10"] = plain(10)
     p100, out["plain_b100"] = plain(100)
-    p1000, out["plain_b1000"] = plain(1000, device=False)
+    p1000, out["plain_b1000"] = plain(1000, device=False, seed=PROBE_SEED + 7)  # own probes
     cfg = CvConfig(nvecs=10)
     # Warm the code paths once (first use of the torch and network kernels
     # loads them), as the plain runs above are warm from the headline runs;
@@ -459,7 +459,7 @@ def ours_arm(args) -> None:
     # phase-2 tile shape; every candidate's scores must agree bit for bit) ----
     from summit_b200 import autotune
 
-    cands = ([{"p1_sb_per_cta": s, "batch_gb": 8.0, "p2_pairs": 0} for s in (4, 8, 16)] +
+    cands = ([{"p1_sb_per_cta": s, "batch_gb": 8.0, "p2_pairs": 0} for s in (4, 8, 16, 32)] +
              [{"p1_sb_per_cta": 8, "batch_gb": 4.0, "p2_pairs": 0},
               {"p1_sb_per_cta": 8, "batch_gb": 8.0, "p2_pairs": 1}])
     t_tune = time.perf_counter()
@@ -574,7 +574,7 @@ def ours_arm(args) -> None:
             "e2e": {"value": round(world * ops / (e2e_ms * 1e-3) / 1e12, 3), "unit": "TOPS",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": round(e2e_ms, 1),
-                    "call": f"lds_win_ldscore (upload streamed in {chunks} window-aligned chunks)",
+                    "call": f"lds_win_ldscore (upload streamed in window-aligned chunks, n_chunks={chunks})",
                     "stages_ms": {"first_estimate_enqueued": round(float(stage[0]), 1),
                                   "all_enqueued": round(float(stage[1]), 1),
                                   "results_copied": round(float(stage[2]), 1),
@@ -855,6 +855,83 @@ BIO_N, BIO_M, BIO_B, BIO_E = 400_000, 800_000, 50, 4
 BIO_METRIC = "geno x probe TOPS (biobank-scale genome-wide LD scores, HBM-resident BED)"
 
 
+def biobank_learned(sess, m: int, stream=None) -> dict:
+    """Learned control variate at B = 8 on the biobank image (one window: the
+    genome-wide estimator with the near-field control variate and the network
+    far field) against the plain estimator at B = 8 and 50, all judged by the
+    plain estimator at B = 1,000 (an exact Gram of 800k SNPs is out of reach;
+    the judge's own per-SNP noise is about sqrt(8/1000) of plain B = 8's)."""
+    import math
+
+    import torch
+
+    from summit_b200.learned_cv import CvConfig, LearnedCV
+    from summit_b200.session import WinPlan
+
+    annot = np.ones((m, 1))
+    ws = np.array([0, m], dtype=np.int64)
+
+    def plain(B, seed=PROBE_SEED):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        p = WinPlan(sess, annot, ws, B, BLOCK, seed, "rademacher")
+        p.execute()
+        ld = p.results(meansq=False)["ldscore"]
+        wall = time.perf_counter() - t0
+        p.execute()
+        dev = float(sum(p.kernel_ms().values()))
+        p.close()
+        return ld, {"B": B, "wall_ms": round(wall * 1e3, 1), "device_ms": round(dev, 2)}
+
+    # the judge draws its own probes (a shared seed would make its first
+    # probes those of the plain runs and understate their error)
+    judge, rj = plain(1000, seed=PROBE_SEED + 7)
+    out = {"judge": rj}
+    for B in (8, 50):
+        ld, rec = plain(B)
+        out[f"plain_b{B}"] = dict(rec, **ld_errors(ld, judge))
+    cfg = CvConfig(nvecs=8)
+    warm = LearnedCV(sess, annot, ws, BLOCK, PROBE_SEED + 2, cfg=cfg)
+    warm.run()
+    warm.close()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    cv = LearnedCV(sess, annot, ws, BLOCK, PROBE_SEED + 1, cfg=cfg)
+    res = cv.run()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    res = cv.run()
+    cv.close()
+    ld = res["ldscore"].double().cpu().numpy()
+    out["learned_b8"] = {"B": 8, "wall_ms": round(wall * 1e3, 1),
+                         "device_ms": round(res["timings"]["total_ms"], 2),
+                         "stages_ms": {k: round(v, 2) for k, v in res["timings"].items()},
+                         **ld_errors(ld, judge),
+                         "near_field_only": ld_errors(res["nearcv_ldscore"].double().cpu().numpy(),
+                                                      judge)}
+    # plain probes for the learned per-SNP error (error ~ B^-1/2), from B = 50
+    ratio = out["plain_b50"]["snp_rel_rmse"] / max(out["learned_b8"]["snp_rel_rmse"], 1e-12)
+    b_eq = int(math.ceil(50.0 * ratio * ratio / 10.0) * 10)
+    out["plain_B_for_learned_snp_error"] = b_eq
+    # The judge's own per-SNP noise inflates every error: with plain variance
+    # c/B, plain B=8 measures c/8 + c/1000 against the judge, so c follows,
+    # and the learned estimator's variance net of the judge's gives the
+    # plain probe count that matches it without that bias.
+    c = out["plain_b8"]["snp_rel_rmse"] ** 2 / (1.0 / 8 + 1.0 / 1000)
+    net = out["learned_b8"]["snp_rel_rmse"] ** 2 - c / 1000
+    out["judge_noise_snp_rel_rmse"] = round(math.sqrt(c / 1000), 5)
+    out["plain_B_for_learned_snp_error_net_of_judge"] = (int(round(c / net)) if net > 0 else None)
+    if b_eq <= 1000:
+        ld, rec = plain(b_eq)
+        out["plain_matched"] = dict(rec, **ld_errors(ld, judge))
+        out["speedup_at_matched_snp_error"] = {
+            "wall": round(out["plain_matched"]["wall_ms"] / out["learned_b8"]["wall_ms"], 2),
+            "device": round(out["plain_matched"]["device_ms"] / out["learned_b8"]["device_ms"], 2)}
+    out["error_metric"] = ("vs plain B=1000: mean_ld_rel_err = |mean est - mean judge| / "
+                           "|mean judge|; snp_rel_rmse = per-SNP RMS difference / RMS judge")
+    return out
+
+
 def biobank_arm(args) -> None:
     import torch
 
@@ -907,6 +984,10 @@ def biobank_arm(args) -> None:
     gres = gx.run(probes, ones1, scale, scale)
     gxe_ms = gres["timings"]["total"]
     gxe_ops_ = gxe_ops(n, m, E, 1, B)
+    del gx
+    learned = None
+    if not os.environ.get("LDS_SKIP_LEARNED"):
+        learned = biobank_learned(sess, m)
     sess.close()
     line = {
         "metric": BIO_METRIC, "value": round(ops / (ms * 1e-3) / 1e12, 3), "unit": "TOPS",
@@ -926,6 +1007,7 @@ def biobank_arm(args) -> None:
                           "TOPS": round(gxe_ops_ / (gxe_ms * 1e-3) / 1e12, 3),
                           "stage_ms": {k: round(v, 1) for k, v in gres["timings"].items()},
                           "max_leakage": float(np.max(gres["leakages"]))},
+        "learned_vs_plain": learned,
         "e2e": None,
         "e2e_note": ("not measured: the 80 GB BED would have to be staged in pinned host "
                      "memory; the image is generated on the device"),

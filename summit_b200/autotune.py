@@ -37,7 +37,7 @@ DEFAULT_CONFIG = {"p1_sb_per_cta": 8, "batch_gb": 8.0, "p2_pairs": 0}
 def default_candidates() -> list[dict]:
     """Phase-1 split x window batching x phase-2 tile shape."""
     return [{"p1_sb_per_cta": s, "batch_gb": b, "p2_pairs": p}
-            for s in (4, 8, 16) for b in (4.0, 8.0) for p in (0, 1)]
+            for s in (4, 8, 16, 32) for b in (4.0, 8.0) for p in (0, 1)]
 
 
 def cache_path() -> Path:
