@@ -318,8 +318,9 @@ def learned_vs_plain(sess, annot, ws, stream) -> dict:
     against the exact expectation of the estimator (exact windowed Gram
     kernel) and against the plain estimator at B = 1,000.  Wall times are
     from the resident image to host results (plan set-up, probe streams and
-    any training included), with every code path warmed once beforehand;
-    device times are one steady-state execute."""
+    any training included), with every code path warmed once beforehand,
+    the better of two independent runs for each estimator; device times the
+    better of two steady-state executes."""
     import math
 
     import torch
@@ -340,30 +341,36 @@ def learned_vs_plain(sess, annot, ws, stream) -> dict:
                     "mean_ld_rel_err": 0.0, "snp_rel_rmse": 0.0,
                     "method": "exact expectation of the estimator (int8 Gram tensor-core kernel)"}
 
-    def plain(B, device=True, seed=PROBE_SEED):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        p = WinPlan(sess, annot, ws, B, BLOCK, seed, "rademacher")
-        p.execute()
-        ld = p.results()["ldscore"]
-        wall = time.perf_counter() - t0
-        dev = None
-        if device:
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            p.execute()
-            e1.record(stream)
+    # Both estimators get the same treatment: wall = the better of two
+    # independent runs from the resident image (plan set-up to host results),
+    # device = the better of two steady-state executes.
+    def plain(B, device=True, seed=PROBE_SEED, reps=2):
+        wall, dev, ld = math.inf, math.inf, None
+        for _ in range(reps):
             torch.cuda.synchronize()
-            dev = e0.elapsed_time(e1)
-        p.close()
+            t0 = time.perf_counter()
+            p = WinPlan(sess, annot, ws, B, BLOCK, seed, "rademacher")
+            p.execute()
+            ld = p.results()["ldscore"]
+            wall = min(wall, time.perf_counter() - t0)
+            if device:
+                for _ in range(2):
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    p.execute()
+                    e1.record(stream)
+                    torch.cuda.synchronize()
+                    dev = min(dev, e0.elapsed_time(e1))
+            p.close()
         rec = {"B": B, "wall_ms": round(wall * 1e3, 1), **ld_errors(ld, truth)}
-        if dev is not None:
+        if device:
             rec["device_ms"] = round(dev, 2)
         return ld, rec
 
     _, out["plain_b10"] = plain(10)
     p100, out["plain_b100"] = plain(100)
-    p1000, out["plain_b1000"] = plain(1000, device=False, seed=PROBE_SEED + 7)  # own probes
+    p1000, out["plain_b1000"] = plain(1000, device=False, seed=PROBE_SEED + 7, reps=1)
     cfg = CvConfig(nvecs=10)
     # Warm the code paths once (first use of the torch and network kernels
     # loads them), as the plain runs above are warm from the headline runs;
@@ -371,14 +378,20 @@ def learned_vs_plain(sess, annot, ws, stream) -> dict:
     warm = LearnedCV(sess, annot, ws, BLOCK, PROBE_SEED + 2, cfg=cfg)
     warm.run()
     warm.close()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    cv = LearnedCV(sess, annot, ws, BLOCK, PROBE_SEED + 1, cfg=cfg)
-    res = cv.run()
-    torch.cuda.synchronize()
-    wall = time.perf_counter() - t0
-    res = cv.run()  # steady state (graph captured, workspace allocated)
-    cv.close()
+    wall, best = math.inf, None
+    for _ in range(2):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        cv = LearnedCV(sess, annot, ws, BLOCK, PROBE_SEED + 1, cfg=cfg)
+        res = cv.run()
+        torch.cuda.synchronize()
+        wall = min(wall, time.perf_counter() - t0)
+        for _ in range(2):
+            res = cv.run()  # steady state (graph captured, workspace allocated)
+            if best is None or res["timings"]["total_ms"] < best["timings"]["total_ms"]:
+                best = res
+        cv.close()
+    res = best
     ld = res["ldscore"].double().cpu().numpy()
     near = res["nearcv_ldscore"].double().cpu().numpy()
     out["learned_b10"] = {"B": 10, "wall_ms": round(wall * 1e3, 1),
@@ -390,7 +403,7 @@ def learned_vs_plain(sess, annot, ws, stream) -> dict:
     ratio = out["plain_b100"]["snp_rel_rmse"] / max(out["learned_b10"]["snp_rel_rmse"], 1e-12)
     b_eq = int(math.ceil(100.0 * ratio * ratio / 10.0) * 10)
     if b_eq <= 2000:
-        _, out["plain_matched"] = plain(b_eq)
+        _, out["plain_matched"] = plain(b_eq)  # same seed as above: the same estimate each rep
         out["speedup_at_matched_snp_error"] = {
             "wall": round(out["plain_matched"]["wall_ms"] / out["learned_b10"]["wall_ms"], 2),
             "device": round(out["plain_matched"]["device_ms"] / out["learned_b10"]["device_ms"], 2)}
