@@ -17,8 +17,9 @@ The LD scores do not depend on any of them, and the tuner checks that: every
 candidate's scores must equal the first candidate's bit for bit.  A
 candidate's cost is the device time of one estimate, as the sum of the plan's
 CUDA-event intervals inside its graph, and the minimum over repeats is kept.
-The winner is stored under a key of the device name and the workload's shape
-(samples, SNPs, bins, probes, window-size quantiles on a log2 grid).
+The winner is stored under a key of the device name, the library build and the
+workload's shape (samples, SNPs, bins, probes, window-size quantiles on a log2
+grid).
 """
 from __future__ import annotations
 
@@ -37,7 +38,7 @@ DEFAULT_CONFIG = {"p1_sb_per_cta": 8, "batch_gb": 8.0, "p2_pairs": 0}
 def default_candidates() -> list[dict]:
     """Phase-1 split x window batching x phase-2 tile shape."""
     return [{"p1_sb_per_cta": s, "batch_gb": b, "p2_pairs": p}
-            for s in (4, 8, 16, 32) for b in (4.0, 8.0) for p in (0, 1)]
+            for s in (4, 8, 16, 32, 64) for b in (4.0, 8.0) for p in (0, 1)]
 
 
 def cache_path() -> Path:
@@ -58,6 +59,18 @@ def workload_key(device: str, n: int, m: int, k: int, nvecs: int, window_starts)
     q = [_log2_bucket(v) for v in np.percentile(sizes, [10, 50, 90])] if sizes.size else [0, 0, 0]
     return (f"{device}|N{int(n)}|M{_log2_bucket(m)}|K{int(k)}|B{int(nvecs)}|"
             f"w{q[0]}-{q[1]}-{q[2]}")
+
+
+def library_id() -> str:
+    """Identity of the loaded build (size and mtime of liblds.so): a rebuilt
+    library is tuned afresh."""
+    try:
+        from . import _lib
+
+        st = os.stat(_lib.LIB_PATH)
+        return f"{st.st_size:x}{int(st.st_mtime):x}"
+    except OSError:
+        return "nolib"
 
 
 def device_name() -> str:
@@ -144,8 +157,8 @@ def tune_windowed(session, annot, window_starts, nvecs: int, step: int, seed: in
     """Tuned record for this workload: from the cache, or measured and stored."""
     annot = np.ascontiguousarray(annot, dtype=np.float64)
     cache = cache if cache is not None else TuneCache()
-    key = workload_key(device_name(), session.N, annot.shape[0], annot.shape[1], nvecs,
-                       window_starts)
+    key = workload_key(f"{device_name()}|{library_id()}", session.N, annot.shape[0],
+                       annot.shape[1], nvecs, window_starts)
     if not force:
         hit = cache.get(key)
         if hit is not None:
@@ -166,8 +179,8 @@ def tuned_win_plan(session, annot, window_starts, nvecs: int, step: int, seed: i
 
     cache = cache if cache is not None else TuneCache()
     annot = np.ascontiguousarray(annot, dtype=np.float64)
-    key = workload_key(device_name(), session.N, annot.shape[0], annot.shape[1], nvecs,
-                       window_starts)
+    key = workload_key(f"{device_name()}|{library_id()}", session.N, annot.shape[0],
+                       annot.shape[1], nvecs, window_starts)
     rec = cache.get(key)
     if rec is None and tune_if_missing:
         rec = tune_windowed(session, annot, window_starts, nvecs, step, seed, rand_dist,

@@ -3259,7 +3259,7 @@ using namespace lds;
 LDS_API const char* lds_last_error(void) { return g_err.c_str(); }
 
 LDS_API const char* lds_version(void) {
-    return "liblds 0.1 sm_100a (int8 digit-sliced exact products; mma.sync path)";
+    return "liblds 0.2 sm_100a (int8 digit-sliced exact products on tcgen05 tensor cores)";
 }
 
 LDS_API int lds_device_count(void) {

@@ -34,9 +34,18 @@ constexpr int kBM = 128;              // SNP rows per CTA (UMMA M)
 constexpr int kBK = 128;              // samples per stage (bytes per operand row)
 constexpr int kPkBytes = kBM * 32;    // packed tile: 128 rows x 32 bytes
 constexpr int kATile = kBM * kBK;     // 16 KB
-constexpr int kPkStages = 8;          // packed-code ring (HBM latency)
-constexpr int kAStages = 2;           // decoded G/O operand ring
-constexpr int kBStages = 4;           // sketch-digit ring (L2 latency)
+#ifndef LDS_P2_PK_STAGES
+#define LDS_P2_PK_STAGES 8
+#endif
+#ifndef LDS_P2_A_STAGES
+#define LDS_P2_A_STAGES 2
+#endif
+#ifndef LDS_P2_B_STAGES
+#define LDS_P2_B_STAGES 4
+#endif
+constexpr int kPkStages = LDS_P2_PK_STAGES;  // packed-code ring (HBM latency)
+constexpr int kAStages = LDS_P2_A_STAGES;    // decoded G/O operand ring
+constexpr int kBStages = LDS_P2_B_STAGES;    // sketch-digit ring (L2 latency)
 // Decoder sets: set d decodes the K-steps it with it % kDecSets == d, so two
 // sets keep two operand tiles in flight while the first set also runs the
 // epilogue.
