@@ -337,6 +337,11 @@ int lds_win_ldscore(const uint8_t* bed_rows, int64_t bed_row_bytes, int64_t n_to
  * that meansq - C + V mu is an unbiased near-field control-variate estimate
  * of meansq.  band_D = 0 disables it.  annot: M x K row-major (as at create). */
 int lds_win_plan_set_cv(int64_t plan, const double* annot, int split_tiles, int band_D);
+/* Device address of the plan's copy of the annotation matrix (M x K
+ * row-major float64, uploaded by lds_win_plan_set_cv; valid until the plan is
+ * destroyed, read-only), so that callers on other streams need not upload it
+ * again; the library stream is synchronized first. */
+int lds_win_plan_cv_annot(int64_t plan, const double** d_annot);
 /* Number of V-tiles and their probe counts (tile_sizes may be NULL). */
 int lds_win_plan_tiles(int64_t plan, int* n_tiles, int* tile_sizes);
 /* After execute: copy the outputs (host pointers, or device pointers when

@@ -38,7 +38,7 @@ DEFAULT_CONFIG = {"p1_sb_per_cta": 8, "batch_gb": 8.0, "p2_pairs": 0}
 def default_candidates() -> list[dict]:
     """Phase-1 split x window batching x phase-2 tile shape."""
     return [{"p1_sb_per_cta": s, "batch_gb": b, "p2_pairs": p}
-            for s in (4, 8, 16, 32, 64) for b in (4.0, 8.0) for p in (0, 1)]
+            for s in (8, 16, 32, 64, 128) for b in (4.0, 8.0, 16.0) for p in (0, 1)]
 
 
 def cache_path() -> Path:

@@ -2622,6 +2622,15 @@ void win_ldscore_impl(const uint8_t* bed_rows, int64_t row_bytes, int64_t n_tota
         c.hwe_q01.as<double>((size_t)maxL);
         c.hwe_sb.as<uint64_t>((size_t)maxL);
     }
+    // One window batch per chunk (a chunk's windows in one phase-1 and one
+    // phase-2 launch), within 8..32 GB of sketch digits.
+    int64_t max_w = 0;
+    for (size_t i = 0; i < nc; ++i) max_w = std::max(max_w, cw[i + 1] - cw[i]);
+    int vmax = std::min(nvecs, vtile > 0 ? vtile : nvecs);
+    if (vmax >= 64) vmax = std::max(64, (vmax / 64) * 64);
+    const double per_window =
+        (double)round_up(row_sel ? n_sel : n_total, kSamplePad) * (double)K * umma::ncolp_for(vmax);
+    const double chunk_gb = std::min(32.0, std::max(8.0, 1.01 * (double)max_w * per_window / 1e9));
     const size_t MK = (size_t)(M * K);
     const size_t need = sizeof(double) * MK * (meansq_out ? 2 : 1) + sizeof(unsigned) * nc;
     if (c.pinned_n < need) {
@@ -2676,7 +2685,8 @@ void win_ldscore_impl(const uint8_t* bed_rows, int64_t row_bytes, int64_t n_tota
             ch[i].P = prepare(c, bed_rows + j0 * row_bytes, row_bytes, n_total, L, row_sel, n_sel,
                               impute, iseed, ddof, "stream", nullptr, j0);
             ch[i].plan = win_plan_create(c, ch[i].P, annot + j0 * K, K, lws.data(), wb - wa,
-                                         nvecs, step, vtile, seed, dist, eps, as_float, 0, 8.0, wa);
+                                         nvecs, step, vtile, seed, dist, eps, as_float, 0,
+                                         chunk_gb, wa);
             ch[i].plan->p1_spc = std::max(0, p1_spc);
             ch[i].plan->pairs = pairs < 0 ? -1 : (pairs ? 1 : 0);
             ch[i].plan->ld_d.as<double>((size_t)(L * K));
@@ -4298,6 +4308,18 @@ LDS_API int lds_win_plan_set_tiling(int64_t plan, int p1_sb_per_cta, int p2_pair
             fail(LDS_ERR_ARG, "p1_sb_per_cta must be in [0, 4096]");
         pl.p1_spc = p1_sb_per_cta;
         pl.pairs = p2_pairs < 0 ? -1 : (p2_pairs ? 1 : 0);
+    });
+}
+
+LDS_API int lds_win_plan_cv_annot(int64_t plan, const double** d_annot) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        const WinPlan& pl = win_of_handle(plan);
+        if (!d_annot) fail(LDS_ERR_ARG, "null output");
+        if (!pl.annot_d.p) fail(LDS_ERR_ARG, "plan has no control-variate inputs (lds_win_plan_set_cv)");
+        ck(cudaStreamSynchronize(c.st), "sync");  // the upload is complete for other streams
+        *d_annot = static_cast<const double*>(pl.annot_d.p);
     });
 }
 

@@ -73,7 +73,7 @@ class LearnedCV:
         M, K, D = self.M, self.K, cfg.band
         W = ws.size - 1
         sizes = np.diff(ws)
-        self.annot = torch.from_numpy(annot).to(dev)
+        self.annot = self.plan.cv_annot_view()  # the plan's device copy, no second upload
         ws_t = torch.from_numpy(ws).to(dev)
         win = torch.repeat_interleave(torch.arange(W, device=dev), torch.from_numpy(sizes).to(dev))
         # correlation null M_k(window) / (N - ddof), as the plain estimator applies it:

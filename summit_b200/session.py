@@ -267,6 +267,21 @@ class WinPlan:
         (1/0; -1: the global switch); call before the first execute."""
         check(_lib.load().lds_win_plan_set_tiling(self.handle, int(p1_sb_per_cta), int(p2_pairs)))
 
+    def cv_annot_view(self):
+        """Read-only torch view (cuda, float64, M x K) of the annotation matrix the
+        plan uploaded in set_cv; valid while the plan lives."""
+        import torch
+
+        p = C.c_void_p(0)
+        check(_lib.load().lds_win_plan_cv_annot(self.handle, C.byref(p)))
+
+        class _View:  # __cuda_array_interface__ v3 of the plan's buffer
+            __cuda_array_interface__ = {"shape": (self.M, self.K), "typestr": "<f8",
+                                        "data": (int(p.value), False), "version": 3,
+                                        "strides": None}
+
+        return torch.as_tensor(_View(), device="cuda")
+
     def bin_totals(self) -> np.ndarray:
         """Per-window annotation totals M_{w,k} (W x K, summed in SNP order)."""
         out = np.empty((self.W, self.K))
