@@ -74,3 +74,22 @@ def test_streamed_rejects_bad_windows(small_bed):
         windowed_ldscore(packed, n, annot, np.array([0, 100, 100, m]), 8, 50, 1)
     with pytest.raises(ValueError):
         windowed_ldscore(packed, n, annot[:-1], np.array([0, m]), 8, 50, 1)
+
+
+def test_streamed_after_clearing_the_device_cache(small_bed):
+    """The chunk pool is released by lds_clear_device_cache and rebuilt by the
+    next call: results stay identical across calls."""
+    from summit_b200 import _lib
+    from summit_b200.session import windowed_ldscore
+
+    n, m, packed = small_bed["n"], small_bed["m"], small_bed["rows"]
+    ws = np.array([0, 100, 250, m], dtype=np.int64)
+    annot = np.ones((m, 2))
+    annot[::3, 1] = 0.0
+    a = windowed_ldscore(packed, n, annot, ws, 16, 50, 5, chunks=3)["ldscore"]
+    _lib.load().lds_clear_device_cache()
+    b = windowed_ldscore(packed, n, annot, ws, 16, 50, 5, chunks=3)["ldscore"]
+    c = windowed_ldscore(packed, n, annot, ws, 16, 50, 5, chunks=2,
+                         tiling={"p1_sb_per_cta": 64, "p2_pairs": 1})["ldscore"]
+    np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(a, c)
