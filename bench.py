@@ -438,11 +438,8 @@ def ours_arm(args) -> None:
 
     n, m = N_SAMPLES, env_int("LDS_BENCH_M", M_SNPS)
     seed = DATA_SEED + rank  # weak scaling: every rank estimates its own batch
-    bed = gwldcore.synth_bed_rows(n, m, seed)
-    pinned = torch.empty(bed.shape, dtype=torch.uint8, pin_memory=True)
-    pinned.numpy()[:] = bed
-    bed_host = pinned.numpy()
-    del bed
+    pinned = torch.empty((m, (n + 3) // 4), dtype=torch.uint8, pin_memory=True)
+    bed_host = gwldcore.synth_bed_rows(n, m, seed, out=pinned.numpy())
     annot = annotations(m)
     ws = windows(m)
     ops1, ops2 = algorithmic_ops(n, annot, B_PROBES)
@@ -791,7 +788,9 @@ def gxe_arm(args) -> None:
 
     n, m = env_int("LDS_GXE_N", GXE_N), env_int("LDS_GXE_M", GXE_M)
     E, B, K = GXE_E, GXE_B, 1
-    bed = gwldcore.synth_bed_rows(n, m, DATA_SEED + rank)
+    # host BED rows in pinned memory (the end-to-end leg uploads them each step)
+    pinned = torch.empty((m, (n + 3) // 4), dtype=torch.uint8, pin_memory=True)
+    bed = gwldcore.synth_bed_rows(n, m, DATA_SEED + rank, out=pinned.numpy())
     d = synthetic_design(n, E, seed=3, categorical=2)
     dev = torch.device("cuda")
     g = torch.Generator(device=dev)

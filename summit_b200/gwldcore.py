@@ -639,13 +639,20 @@ def set_slices(s: int) -> None:
     check(_lib.load().lds_set_slices(int(s)))
 
 
-def synth_bed_rows(n: int, m: int, seed: int, missing: bool = True) -> np.ndarray:
-    """Synthetic packed BED rows generated on the device (same bytes as bedfile.py)."""
+def synth_bed_rows(n: int, m: int, seed: int, missing: bool = True, out=None) -> np.ndarray:
+    """Synthetic packed BED rows generated on the device (same bytes as bedfile.py).
+
+    ``out``: optional C-contiguous (m, ceil(n/4)) uint8 array to fill (e.g. the
+    numpy view of a pinned torch tensor)."""
     from .bedfile import allele_freqs, hwe_thresholds
 
     p = allele_freqs(seed, m)
     t0, t1 = hwe_thresholds(p)
-    out = np.empty((m, (n + 3) // 4), dtype=np.uint8)
+    shape = (m, (n + 3) // 4)
+    if out is None:
+        out = np.empty(shape, dtype=np.uint8)
+    elif out.shape != shape or out.dtype != np.uint8 or not out.flags["C_CONTIGUOUS"]:
+        raise ValueError(f"out must be a C-contiguous uint8 array of shape {shape}")
     check(_lib.load().lds_synth_bed(int(n), int(m), int(seed), ptr(np.ascontiguousarray(t0)),
                                     ptr(np.ascontiguousarray(t1)), int(missing), ptr(out)))
     return out
