@@ -314,8 +314,8 @@ def ld_errors(est, truth) -> dict:
 
 def learned_vs_plain(sess, annot, ws, stream) -> dict:
     """LD-score time and error of the plain windowed estimator and of the
-    learned control variate (B = 10) on the same resident image, judged
-    against the exact expectation of the estimator (exact windowed Gram
+    learned control variate (B = 10) on the same resident image, compared
+    with the exact expectation of the estimator (exact windowed Gram
     kernel) and against the plain estimator at B = 1,000.  Wall times are
     from the resident image to host results (plan set-up, probe streams and
     any training included), with every code path warmed once beforehand,
@@ -407,7 +407,7 @@ def learned_vs_plain(sess, annot, ws, stream) -> dict:
         out["speedup_at_matched_snp_error"] = {
             "wall": round(out["plain_matched"]["wall_ms"] / out["learned_b10"]["wall_ms"], 2),
             "device": round(out["plain_matched"]["device_ms"] / out["learned_b10"]["device_ms"], 2)}
-    out["judge_plain_b1000"] = {"learned_b10": ld_errors(ld, p1000),
+    out["vs_plain_b1000"] = {"learned_b10": ld_errors(ld, p1000),
                                 "plain_b100": ld_errors(p100, p1000)}
     out["error_metric"] = ("mean_ld_rel_err: max over bins of |mean est - mean truth| / |mean truth|; "
                            "snp_rel_rmse: per-SNP RMS error / RMS truth, mean over bins")
@@ -870,9 +870,9 @@ BIO_METRIC = "geno x probe TOPS (biobank-scale genome-wide LD scores, HBM-reside
 def biobank_learned(sess, m: int, stream=None) -> dict:
     """Learned control variate at B = 8 on the biobank image (one window: the
     genome-wide estimator with the near-field control variate and the network
-    far field) against the plain estimator at B = 8 and 50, all judged by the
+    far field) against the plain estimator at B = 8 and 50, all measured against the
     plain estimator at B = 1,000 (an exact Gram of 800k SNPs is out of reach;
-    the judge's own per-SNP noise is about sqrt(8/1000) of plain B = 8's)."""
+    that estimate's own per-SNP noise is about sqrt(8/1000) of plain B = 8's)."""
     import math
 
     import torch
@@ -895,13 +895,13 @@ def biobank_learned(sess, m: int, stream=None) -> dict:
         p.close()
         return ld, {"B": B, "wall_ms": round(wall * 1e3, 1), "device_ms": round(dev, 2)}
 
-    # the judge draws its own probes (a shared seed would make its first
+    # the B = 1,000 estimate draws its own probes (a shared seed would make its first
     # probes those of the plain runs and understate their error)
-    judge, rj = plain(1000, seed=PROBE_SEED + 7)
-    out = {"judge": rj}
+    hi_est, rj = plain(1000, seed=PROBE_SEED + 7)
+    out = {"plain_b1000": rj}
     for B in (8, 50):
         ld, rec = plain(B)
-        out[f"plain_b{B}"] = dict(rec, **ld_errors(ld, judge))
+        out[f"plain_b{B}"] = dict(rec, **ld_errors(ld, hi_est))
     cfg = CvConfig(nvecs=8)
     warm = LearnedCV(sess, annot, ws, BLOCK, PROBE_SEED + 2, cfg=cfg)
     warm.run()
@@ -918,29 +918,29 @@ def biobank_learned(sess, m: int, stream=None) -> dict:
     out["learned_b8"] = {"B": 8, "wall_ms": round(wall * 1e3, 1),
                          "device_ms": round(res["timings"]["total_ms"], 2),
                          "stages_ms": {k: round(v, 2) for k, v in res["timings"].items()},
-                         **ld_errors(ld, judge),
+                         **ld_errors(ld, hi_est),
                          "near_field_only": ld_errors(res["nearcv_ldscore"].double().cpu().numpy(),
-                                                      judge)}
+                                                      hi_est)}
     # plain probes for the learned per-SNP error (error ~ B^-1/2), from B = 50
     ratio = out["plain_b50"]["snp_rel_rmse"] / max(out["learned_b8"]["snp_rel_rmse"], 1e-12)
     b_eq = int(math.ceil(50.0 * ratio * ratio / 10.0) * 10)
     out["plain_B_for_learned_snp_error"] = b_eq
-    # The judge's own per-SNP noise inflates every error: with plain variance
-    # c/B, plain B=8 measures c/8 + c/1000 against the judge, so c follows,
-    # and the learned estimator's variance net of the judge's gives the
+    # The B = 1,000 estimate's own per-SNP noise inflates every error: with
+    # plain variance c/B, plain B=8 measures c/8 + c/1000 against it, so c
+    # follows, and the learned estimator's variance net of that noise gives the
     # plain probe count that matches it without that bias.
     c = out["plain_b8"]["snp_rel_rmse"] ** 2 / (1.0 / 8 + 1.0 / 1000)
     net = out["learned_b8"]["snp_rel_rmse"] ** 2 - c / 1000
-    out["judge_noise_snp_rel_rmse"] = round(math.sqrt(c / 1000), 5)
-    out["plain_B_for_learned_snp_error_net_of_judge"] = (int(round(c / net)) if net > 0 else None)
+    out["plain_b1000_noise_snp_rel_rmse"] = round(math.sqrt(c / 1000), 5)
+    out["plain_B_for_learned_snp_error_net_of_noise"] = (int(round(c / net)) if net > 0 else None)
     if b_eq <= 1000:
         ld, rec = plain(b_eq)
-        out["plain_matched"] = dict(rec, **ld_errors(ld, judge))
+        out["plain_matched"] = dict(rec, **ld_errors(ld, hi_est))
         out["speedup_at_matched_snp_error"] = {
             "wall": round(out["plain_matched"]["wall_ms"] / out["learned_b8"]["wall_ms"], 2),
             "device": round(out["plain_matched"]["device_ms"] / out["learned_b8"]["device_ms"], 2)}
-    out["error_metric"] = ("vs plain B=1000: mean_ld_rel_err = |mean est - mean judge| / "
-                           "|mean judge|; snp_rel_rmse = per-SNP RMS difference / RMS judge")
+    out["error_metric"] = ("vs plain B=1000: mean_ld_rel_err = |mean est - mean B1000| / "
+                           "|mean B1000|; snp_rel_rmse = per-SNP RMS difference / RMS B1000")
     return out
 
 

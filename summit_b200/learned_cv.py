@@ -21,7 +21,7 @@ u_jv = sum_{i in window} c_ji annot_ik z_iv.  Two steps reduce its variance:
    (1 - lambda_k) mean_j (T - h) keeps each bin's mean over SNPs equal to the
    unbiased near-field estimate's.
 
-The plain estimator stays available (``plain_ldscore``) and is the judge:
+The plain estimator stays available (``plain_ldscore``) and is the yardstick:
 tests and the benchmark compare both against the exact expectation of the
 windowed estimator (GwSession.partition_ld_expectation, exact tensor-core Gram
 products) and against plain runs with 10x and 100x the probes.
