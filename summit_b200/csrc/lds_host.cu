@@ -159,7 +159,8 @@ void d2h(T* h, const T* d, size_t count, cudaStream_t st) {
 
 inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 
-// 2-D uint8 TMA descriptor over a row-major device buffer (no multicast use).
+// 2-D uint8 TMA descriptor over a row-major device buffer (each copy lands in the
+// issuing CTA's own shared memory).
 CUtensorMap make_map_2d(void* base, uint64_t inner, uint64_t outer, uint64_t row_bytes,
                         uint32_t box_inner, uint32_t box_outer, CUtensorMapSwizzle swz) {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = [] {

@@ -2,7 +2,7 @@
 //
 // Work[j, c] = x_j^T Y[:, c] for a tile of 128 SNPs and one annotation bin,
 // with the LD-score epilogue, as in p2_kernel (lds_kernels.cu) but with:
-//   * TMA (cp.async.bulk.tensor, no multicast) bringing the packed 2-bit
+//   * TMA tile copies (cp.async.bulk.tensor into the CTA's own shared memory) bringing the packed 2-bit
 //     genotype tile (128 SNPs x 128 samples = 4 KB) and the sketch digit tile
 //     (bin columns x 128 samples, SWIZZLE_128B) into a 3-stage smem ring;
 //   * 4 decoder warps expanding packed codes into the G (value) and O

@@ -19,9 +19,10 @@
 //   * decoded operand tiles: the decoders of both ranks arrive on the leader's
 //     a_full barrier (release at cluster scope after a proxy fence);
 //   * the leader's MMA commits arrive on a_empty / b_empty / acc_full of both
-//     ranks (multicast commit, mask 0b11);
+//     ranks (one tcgen05.commit addressed to both, mask 0b11);
 //   * the epilogue threads of both ranks arrive on the leader's acc_empty.
-// Remote barrier addresses come from mapa.  No TMA load uses multicast.
+// Remote barrier addresses come from mapa; every TMA copy lands in the issuing
+// CTA's own shared memory.
 // Every mbarrier wait is bounded (status code on timeout); both CTAs always
 // reach the final cluster barrier, after the leader's MMAs have drained, so
 // no CTA exits while its peer can still read its shared memory.
@@ -117,7 +118,7 @@ __device__ __forceinline__ void commit_own(uint64_t* bar) {
                  : "memory");
 }
 // Tile copy into this CTA's shared memory whose bytes complete on the
-// barrier at `bar_cluster` (the leader's), no multicast.
+// barrier at `bar_cluster` (the leader's).
 __device__ __forceinline__ void tma_load_2d_pair(void* dst, const CUtensorMap* map, int x, int y,
                                                  uint32_t bar_cluster) {
     asm volatile(
