@@ -59,6 +59,28 @@ int lds_device_count(void);
 int lds_set_slices(int slices);
 int lds_get_slices(void);
 
+/* Guard counts of the last per-block phase-2 call on this process's
+ * context: out2[0] = non-finite updates dropped, out2[1] = finite updates
+ * above the extreme-LD threshold (dropped unless SUMMIT_P2_DROP_EXTREME=0).
+ * The reference prints the same two counts per call
+ * (phase2_log_guard_counts, gwldcore.cpp:364-417). */
+int lds_phase2_guard_counts(uint64_t* out2);
+
+/* Bounded waits.  Every wait of the tensor-core kernels on an mbarrier gives
+ * up after `iters` tries (each suspends the thread for at most 200 ns;
+ * default 2^25, about 6.7 s), records an error status and lets the kernel
+ * return, so a stalled pipeline surfaces as LDS_ERR_CUDA instead of a hung
+ * GPU.  lds_set_wait_limit applies to the current device and waits for the
+ * library's work in flight; lds_get_wait_limit returns the value last set.
+ * No counterpart in the reference (its CPU loops have no device waits). */
+int lds_set_wait_limit(long long iters);
+long long lds_get_wait_limit(void);
+/* Self-test of the bounded wait: one thread waits on an mbarrier that nothing
+ * arrives at, under the current limit.  *status_out = 1 when the wait ran
+ * out and the kernel returned its error status (the expected result), 2 if
+ * the wait completed. */
+int lds_selftest_wait_timeout(unsigned* status_out);
+
 /* Counters of the library's own CUDA kernel launches since process start
  * (all kernels) — used to report launches inside timed regions. */
 uint64_t lds_kernel_launches(void);
@@ -739,8 +761,17 @@ int lds_mlp_train(float* d_params, int in_dim, int out_dim, const float* d_x, co
  *   d_Y: sketch, N_pad x (K*V) column-major (column k*V + v), FP64.
  *   d_mean, d_sdinv, d_left_scale: per SNP row (index j), FP64.
  *   d_accum: (j1-j0) x K row-major FP64, += sum_v Work^2 * left_scale with
- *     the guards of lds_phase2_accum_XtXz_bed; d_mc (may be NULL) += the
- *     fourth-moment sums.  Asynchronous on `stream` (cudaStream_t or NULL).
+ *     the guards of lds_phase2_accum_XtXz_bed (SUMMIT_P2_EXTREME_LD_WARN,
+ *     SUMMIT_P2_DROP_EXTREME); d_mc (may be NULL) += the fourth-moment sums.
+ *   d_status (may be NULL): one caller-owned device word that receives the
+ *     kernel's status (0 = ok; nonzero = a pipeline wait ran out and the
+ *     accumulators are incomplete); d_guards (may be NULL): two device
+ *     words that receive the numbers of non-finite and extreme updates
+ *     dropped.  With d_status given the call is asynchronous on `stream`
+ *     (cudaStream_t or NULL) and the words are written on that stream after
+ *     the kernel.  With d_status NULL the call waits for its own work on
+ *     `stream`, prints the guard warnings, and returns LDS_ERR_CUDA when the
+ *     kernel aborted.
  * The first call on each device looks up the scratch array's address
  * (cudaGetSymbolAddress) and must come before any stream capture.  All
  * calls share the array and it keeps the last call's contents, so calls
@@ -751,6 +782,7 @@ int lds_phase2_accum_device_noalloc(const uint8_t* d_codes, int64_t row_bytes, i
                                     int64_t rows_total, int64_t j0, int64_t j1, const double* d_Y,
                                     int K, int V, const double* d_mean, const double* d_sdinv,
                                     const double* d_left_scale, double* d_accum, double* d_mc,
+                                    unsigned* d_status, unsigned long long* d_guards,
                                     void* stream);
 
 #ifdef __cplusplus

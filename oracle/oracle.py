@@ -730,6 +730,8 @@ class ReferenceGxe:
                                               _i64, _i64, _int, _int, _int, _int]
         L.refg_normalize_scores.argtypes = [_p, _p, _p, _p, _p, _i64, _i64, _int]
         L.refg_philox_rademacher.argtypes = [_p, _i64, _int, _int, _p]
+        L.refg_generalized_products.argtypes = [_p, _i64, _int, _i64, _int, _int, _int, _int, _p,
+                                                _p, _p, _p]
         self.lib = L
 
     def _chk(self, rc):
@@ -742,6 +744,23 @@ class ReferenceGxe:
         return _RefGxeKernel(self, environments, feature_basis, power_indices, power_offsets,
                              ranks, gram_values, gram_offsets, e2_gram_values, common_basis,
                              directions, ddof, annotation_bins, threads)
+
+    def generalized_products(self, bed_path, n_total, start, stop, rhs_src, rhs_tgt, ddof=1):
+        """The reference's packed_source_product / packed_target_product
+        (generalized_gxe_variant.inc:1749-1988) on the mean-imputed Mailman pack
+        of SNPs [start, stop): returns (N x cols source, L x cols target)."""
+        bed = np.fromfile(str(bed_path), dtype=np.uint8)
+        L = stop - start
+        cols = rhs_src.shape[1]
+        rs = np.asfortranarray(rhs_src, dtype=np.float64)
+        rt = np.asfortranarray(rhs_tgt, dtype=np.float64)
+        assert rs.shape == (L, cols) and rt.shape == (n_total, cols)
+        src = np.empty((n_total, cols), order="F")
+        tgt = np.empty((L, cols), order="F")
+        self._chk(self.lib.refg_generalized_products(
+            _ptr(bed), bed.size, n_total, (n_total + 3) // 4, start, stop, ddof, cols, _ptr(rs),
+            _ptr(src), _ptr(rt), _ptr(tgt)))
+        return src, tgt
 
     def philox_rademacher(self, keys, rows, threads=1):
         keys = np.ascontiguousarray(keys, dtype=np.uint64)

@@ -144,3 +144,81 @@ REF_EXPORT int refg_philox_rademacher(const uint64_t* keys, int64_t P, int rows,
         std::memcpy(out, res.data(), sizeof(double) * (size_t)rows * (size_t)P);
     });
 }
+
+// ---------------------------------------------------------------------------
+// Generalized per-SNP GxE packed products (generalized_gxe_variant.inc:
+// 1749-1988).  They are private members of
+// GeneralizedGxELDScoreDirectContext, whose constructor needs a whole run's
+// tables; the two products read only the context's sample count (rows_) and
+// thread count (threads_).  The pointers to those members are obtained
+// through explicit template instantiation, which the language lets name
+// private members, and the products run on zero-initialized storage with
+// just those two fields set.  The reference's code itself is unchanged.
+// ---------------------------------------------------------------------------
+namespace {
+
+using GenCtx = GeneralizedGxELDScoreDirectContext;
+
+template <typename Tag, typename Tag::type Member>
+struct MemberOf {
+    friend typename Tag::type member(Tag) { return Member; }
+};
+struct RowsTag {
+    using type = int GenCtx::*;
+    friend type member(RowsTag);
+};
+struct ThreadsTag {
+    using type = int GenCtx::*;
+    friend type member(ThreadsTag);
+};
+struct SourceTag {
+    using type = void (GenCtx::*)(const MailmanPackedBlock&, const std::vector<double>&, int,
+                                  std::vector<double>&) const;
+    friend type member(SourceTag);
+};
+struct TargetTag {
+    using type = void (GenCtx::*)(const MailmanPackedBlock&, const double*, int,
+                                  std::vector<double>&) const;
+    friend type member(TargetTag);
+};
+template struct MemberOf<RowsTag, &GenCtx::rows_>;
+template struct MemberOf<ThreadsTag, &GenCtx::threads_>;
+template struct MemberOf<SourceTag, &GenCtx::packed_source_product>;
+template struct MemberOf<TargetTag, &GenCtx::packed_target_product>;
+
+}  // namespace
+
+// Mean-imputed Mailman pack of SNPs [start, stop) of an in-memory BED image
+// (all n_total samples), then source = packed_source_product(rhs_src) (N x
+// cols, column-major; rhs_src L x cols column-major) and target =
+// packed_target_product(rhs_tgt) (L x cols; rhs_tgt N x cols), either may be
+// skipped with null pointers.
+REF_EXPORT int refg_generalized_products(const uint8_t* bed, int64_t bed_size, int n_total,
+                                         int64_t bytes_per_snp, int start, int stop, int ddof,
+                                         int cols, const double* rhs_src, double* out_src,
+                                         const double* rhs_tgt, double* out_tgt) {
+    return guarded([&] {
+        std::vector<int> rows((size_t)n_total);
+        for (int i = 0; i < n_total; ++i) rows[(size_t)i] = i;
+        MailmanPackedBlock pack;
+        read_block_mailman_mean_memory(bed, (size_t)bed_size, n_total, (size_t)bytes_per_snp,
+                                       start, stop, rows, ddof, pack);
+        std::vector<unsigned char> storage(sizeof(GenCtx) + alignof(GenCtx), 0);
+        void* raw = storage.data();
+        size_t space = storage.size();
+        auto* ctx = static_cast<GenCtx*>(std::align(alignof(GenCtx), sizeof(GenCtx), raw, space));
+        ctx->*member(RowsTag{}) = n_total;
+        ctx->*member(ThreadsTag{}) = 1;
+        const int L = stop - start;
+        std::vector<double> out;
+        if (rhs_src && out_src) {
+            std::vector<double> rhs(rhs_src, rhs_src + (size_t)L * (size_t)cols);
+            (ctx->*member(SourceTag{}))(pack, rhs, cols, out);
+            std::memcpy(out_src, out.data(), sizeof(double) * out.size());
+        }
+        if (rhs_tgt && out_tgt) {
+            (ctx->*member(TargetTag{}))(pack, rhs_tgt, cols, out);
+            std::memcpy(out_tgt, out.data(), sizeof(double) * out.size());
+        }
+    });
+}

@@ -65,8 +65,12 @@ SIGNATURES: dict[str, tuple] = {
     "lds_mlp_loss_grad": (_int, [_p, _int, _int, _p, _p, _i64, _p, _p]),
     "lds_mlp_train": (_int, [_p, _int, _int, _p, _p, _i64, _int, _int, C.c_float, _u64, _p]),
     "lds_window_seed": (_u64, [_u64, _i64]),
+    "lds_set_wait_limit": (_int, [C.c_longlong]),
+    "lds_phase2_guard_counts": (_int, [_p]),
+    "lds_get_wait_limit": (C.c_longlong, []),
+    "lds_selftest_wait_timeout": (_int, [_p]),
     "lds_phase2_accum_device_noalloc": (_int, [_p, _i64, _i64, _i64, _i64, _i64, _p, _int, _int,
-                                               _p, _p, _p, _p, _p, _p]),
+                                               _p, _p, _p, _p, _p, _p, _p, _p]),
     "lds_geno_create": (_int, [_p, _i64, _i64, _i64, _p, _i64, _int, _u64, _int, _p]),
     "lds_geno_destroy": (_int, [_i64]),
     "lds_nn_band": (_int, [_i64, _int, _p, _p]),

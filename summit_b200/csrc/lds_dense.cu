@@ -291,12 +291,11 @@ void launch_window_cov_epilogue(const double* S, int64_t rows, int64_t p0, const
                                 double invN, double corr_den, double* out, cudaStream_t st) {
     if (rows <= 0 || K <= 0) return;
     const size_t smem = (size_t)kWinWarps * K * 32 * sizeof(double);
-    static bool attr = false;
-    if (!attr) {
+    static std::atomic<unsigned long long> attr{0};
+    once_per_device(attr, [] {
         cudaFuncSetAttribute(window_cov_epilogue_kernel,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        attr = true;
-    }
+    });
     window_cov_epilogue_kernel<<<(unsigned)((rows + kWinWarps - 1) / kWinWarps), kWinWarps * 32,
                                  smem, st>>>(S, rows, p0, lo, hi, annot, annot_row0, K, invN,
                                              corr_den, out);

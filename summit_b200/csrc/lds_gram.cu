@@ -266,12 +266,11 @@ size_t gram_ld_smem_bytes() { return gram::kSmemBytes; }
 
 void launch_gram_ld(const CUtensorMap& tmC, const GramArgs& a, int n_items, cudaStream_t st) {
     if (n_items <= 0) return;
-    static bool attr = false;
-    if (!attr) {
+    static std::atomic<unsigned long long> attr{0};
+    once_per_device(attr, [] {
         cudaFuncSetAttribute(gram::gram_ld_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)gram::kSmemBytes);
-        attr = true;
-    }
+    });
     gram::gram_ld_kernel<<<(unsigned)n_items, gram::kThreads, gram::kSmemBytes, st>>>(tmC, a);
     count_launch();
 }

@@ -239,6 +239,8 @@ struct Context {
     std::shared_ptr<DevBuf> ws[2];
     double timings[4] = {0, 0, 0, 0};
     int slices = 4;
+    // Non-finite / extreme updates dropped by the last per-block phase 2.
+    unsigned long long last_guards[2] = {0, 0};
 };
 
 Context& ctx() {
@@ -602,8 +604,21 @@ void run_phase1(Context& c, Prepared& P, const Csr& csr, int64_t K, int V, const
     launch_p1(P.g, w, csr.bin_off.data(), Y, c.st);
 }
 
+// The per-block phase 2 runs on the tcgen05 kernel (lds_umma.cu) with the
+// default 4 digits; other digit counts, or the mma.sync kernel selected for
+// cross-checks (lds_set_p2_kernel), use the warp-level kernel.
+bool per_block_umma(const Context& c) { return c.slices == 4 && p2_impl() == 1; }
+
 // Quantize the device sketch in c.y (N_pad x K*V) into c.yq.
 void quantize_sketch(Context& c, Prepared& P, int64_t K, int V) {
+    if (per_block_umma(c)) {
+        const int nc = umma::ncolp_for(V);
+        int8_t* yq = c.yq.as<int8_t>((size_t)(K * nc * P.g.N_pad));
+        double* cs = c.ycs.as<double>((size_t)(K * V));
+        umma::launch_quantize_y4(static_cast<double*>(c.y.p), P.g.N, P.g.N_pad, (int)K, V, nc, yq,
+                                 cs, c.st);
+        return;
+    }
     const int S = c.slices;
     const int Vp = (int)round_up(V, kColTile);
     int8_t* yq = c.yq.as<int8_t>((size_t)(S * K * Vp * P.g.N_pad));
@@ -642,6 +657,41 @@ int drop_extreme_env() {
 
 void run_phase2(Context& c, Prepared& P, int64_t K, int V, int64_t j0, int64_t j1,
                 int64_t out_row0, double* d_accum, double* d_mc, const double* d_lscale) {
+    // c.guards: [0] non-finite drops, [1] extreme drops, [2] kernel status
+    // (zeroed by the caller before each call).
+    unsigned long long* guards = c.guards.as<unsigned long long>(4);
+    if (per_block_umma(c)) {
+        const int nc = umma::ncolp_for(V);
+        umma::P2UArgs u;
+        u.K = (int)K;
+        u.V = V;
+        u.ncolp = nc;
+        u.bins_per_cta = umma::p2_bins_per_cta(nc, (int)K);
+        u.ngroups = (u.bins_per_cta * nc + 255) / 256;
+        u.box_rows = std::min(256, u.bins_per_cta * nc);
+        u.nkt = (int)(P.g.N_pad / 128);
+        u.M = P.g.M;
+        u.j0 = j0;
+        u.j1 = j1;
+        u.out_row0 = out_row0;
+        u.colscale = static_cast<double*>(c.ycs.p);
+        u.mean = static_cast<double*>(P.d_mean.p);
+        u.sdinv = static_cast<double*>(P.d_sdinv.p);
+        u.left_scale = d_lscale;
+        u.accum = d_accum;
+        u.mc = d_mc;
+        u.guard_counts = guards;
+        u.extreme_warn = extreme_warn_env();
+        u.drop_extreme = drop_extreme_env();
+        u.status = reinterpret_cast<unsigned*>(guards + 2);
+        const CUtensorMap tA = make_map_2d(P.g.codes, (uint64_t)P.g.nbp, (uint64_t)P.g.M_pad,
+                                           (uint64_t)P.g.nbp, 32, 128, CU_TENSOR_MAP_SWIZZLE_NONE);
+        const CUtensorMap tB =
+            make_map_2d(c.yq.p, (uint64_t)P.g.N_pad, (uint64_t)(K * nc), (uint64_t)P.g.N_pad, 128,
+                        (uint32_t)u.box_rows, CU_TENSOR_MAP_SWIZZLE_128B);
+        umma::launch_p2_umma(tA, tB, u, c.st);
+        return;
+    }
     P2Args a;
     a.K = (int)K;
     a.V = V;
@@ -657,16 +707,21 @@ void run_phase2(Context& c, Prepared& P, int64_t K, int V, int64_t j0, int64_t j
     a.left_scale = d_lscale;
     a.accum = d_accum;
     a.mc = d_mc;
-    a.guard_counts = c.guards.as<unsigned long long>(2);
+    a.guard_counts = guards;
     a.extreme_warn = extreme_warn_env();
     a.drop_extreme = drop_extreme_env();
     launch_p2(P.g, a, c.st);
 }
 
 void report_guards(Context& c, const char* label, int blk_start, int blk_end) {
-    unsigned long long h[2] = {0, 0};
-    d2h(h, static_cast<unsigned long long*>(c.guards.p), 2, c.st);
+    unsigned long long h[3] = {0, 0, 0};
+    d2h(h, static_cast<unsigned long long*>(c.guards.p), 3, c.st);
     ck(cudaStreamSynchronize(c.st), "guards");
+    c.last_guards[0] = h[0];
+    c.last_guards[1] = h[1];
+    if ((unsigned)h[2] != 0)
+        fail(LDS_ERR_CUDA, "phase-2 kernel aborted in %s block [%d:%d): a pipeline wait ran out "
+             "(status %u)", label, blk_start, blk_end, (unsigned)h[2]);
     if (h[0])
         std::fprintf(stderr,
                      "[phase2-warning] %s block [%d:%d): dropped %llu non-finite LD-score updates.\n",
@@ -1192,8 +1247,8 @@ void dense_p2_finish(Context& c, const double* W, int64_t L, int64_t K, int V, c
         d_mc = dmc.as<double>((size_t)(L * K));
         ck(cudaMemsetAsync(d_mc, 0, sizeof(double) * (size_t)(L * K), c.st), "memset");
     }
-    unsigned long long* g = c.guards.as<unsigned long long>(2);
-    ck(cudaMemsetAsync(g, 0, 16, c.st), "memset");
+    unsigned long long* g = c.guards.as<unsigned long long>(4);
+    ck(cudaMemsetAsync(g, 0, 32, c.st), "memset");
     launch_dense_p2_epilogue(W, L, (int)K, V, d_ls, d_acc, d_mc, g, extreme_warn_env(),
                              drop_extreme_env(), c.st);
     ck(cudaGetLastError(), "launch");
@@ -1577,7 +1632,7 @@ void phase2_bed_impl(const char* bed_prefix, const char* fam_path, int blk_start
         d_mc = c.mc.as<double>((size_t)(L * K));
         ck(cudaMemsetAsync(d_mc, 0, sizeof(double) * (size_t)(L * K), c.st), "memset");
     }
-    ck(cudaMemsetAsync(c.guards.as<unsigned long long>(2), 0, 16, c.st), "memset");
+    ck(cudaMemsetAsync(c.guards.as<unsigned long long>(4), 0, 32, c.st), "memset");
     run_phase2(c, P, K, tile_nvecs, blk_start, blk_end, blk_start, d_acc, d_mc, d_ls);
     std::vector<double> upd((size_t)(L * K)), mcv;
     d2h(upd.data(), d_acc, upd.size(), c.st);
@@ -3261,6 +3316,26 @@ void gw_ldscore_impl(const uint8_t* bed_rows, int64_t row_bytes, int64_t n_total
 
 void set_last_error(const std::string& msg) { g_err = msg; }
 
+double phase2_extreme_warn() { return extreme_warn_env(); }
+int phase2_drop_extreme() { return drop_extreme_env(); }
+
+// Setters registered by each file holding a copy of the bounded-wait limit.
+// Registration runs during the library's static initialization (one thread);
+// the list is read afterwards.
+static std::vector<WaitLimitSetter>& wait_limit_setters() {
+    static std::vector<WaitLimitSetter> v;
+    return v;
+}
+void register_wait_limit_setter(WaitLimitSetter f) { wait_limit_setters().push_back(f); }
+cudaError_t set_wait_limit_all(long long iters) {
+    cudaError_t first = cudaSuccess;
+    for (WaitLimitSetter f : wait_limit_setters()) {
+        const cudaError_t e = f(iters);
+        if (e != cudaSuccess && first == cudaSuccess) first = e;
+    }
+    return first;
+}
+
 }  // namespace lds
 
 using namespace lds;
@@ -3290,6 +3365,57 @@ LDS_API int lds_set_slices(int s) {
 }
 
 LDS_API int lds_get_slices(void) { return ctx().slices; }
+
+LDS_API int lds_phase2_guard_counts(uint64_t* out2) {
+    if (!out2) {
+        g_err = "null output";
+        return LDS_ERR_ARG;
+    }
+    Context& c = ctx();
+    std::lock_guard<std::mutex> lk(c.mu);
+    out2[0] = c.last_guards[0];
+    out2[1] = c.last_guards[1];
+    return LDS_OK;
+}
+
+// Bounded waits of the tensor-core kernels (see lds.h).
+static std::atomic<long long> g_wait_limit{1LL << 25};
+
+LDS_API int lds_set_wait_limit(long long iters) {
+    if (iters < 1) {
+        g_err = "wait limit must be >= 1";
+        return LDS_ERR_ARG;
+    }
+    Context& c = ctx();
+    std::lock_guard<std::mutex> lk(c.mu);
+    return guarded([&] {
+        ensure_device(c);
+        // No library work may be in flight while the limit changes.
+        ck(cudaStreamSynchronize(c.st), "wait limit");
+        ck(set_wait_limit_all(iters), "wait limit");
+        ck(cudaDeviceSynchronize(), "wait limit");
+        g_wait_limit.store(iters);
+    });
+}
+
+LDS_API long long lds_get_wait_limit(void) { return g_wait_limit.load(); }
+
+LDS_API int lds_selftest_wait_timeout(unsigned* status_out) {
+    Context& c = ctx();
+    std::lock_guard<std::mutex> lk(c.mu);
+    return guarded([&] {
+        ensure_device(c);
+        DevBuf d;
+        unsigned* ds = d.as<unsigned>(1);
+        ck(cudaMemsetAsync(ds, 0, sizeof(unsigned), c.st), "memset");
+        launch_wait_timeout_probe(ds, c.st);
+        ck(cudaGetLastError(), "launch");
+        unsigned h = 0;
+        d2h(&h, ds, 1, c.st);
+        ck(cudaStreamSynchronize(c.st), "wait probe");
+        if (status_out) *status_out = h;
+    });
+}
 
 LDS_API uint64_t lds_kernel_launches(void) { return g_launches.load(); }
 

@@ -1,6 +1,7 @@
 // Internal interfaces between the host orchestration (lds_host.cu) and the
 // kernels (lds_kernels.cu).  Not part of the C ABI.
 #pragma once
+#include <atomic>
 #include <cstdint>
 #include <string>
 #include <cuda.h>
@@ -293,5 +294,41 @@ void count_launch();
 
 // Set the text returned by lds_last_error() for the calling thread.
 void set_last_error(const std::string& msg);
+
+// Phase-2 guard settings from the environment, read once per process like
+// the reference's (gwldcore.cpp:295-308): SUMMIT_P2_EXTREME_LD_WARN (or
+// SUMMIT_P2_ABS_LD_MAX; default 1e10, <= 0 disables) and
+// SUMMIT_P2_DROP_EXTREME (default on).
+double phase2_extreme_warn();
+int phase2_drop_extreme();
+
+// Setters of the per-file copies of the bounded-wait iteration limit of the
+// tensor-core kernels (lds_tc.cuh); each applies to the current device.
+using WaitLimitSetter = cudaError_t (*)(long long);
+void register_wait_limit_setter(WaitLimitSetter f);
+// Calls every registered setter; returns the first error.
+cudaError_t set_wait_limit_all(long long iters);
+// Self-test of the bounded wait (lds_umma.cu): one thread waits on an
+// mbarrier that nothing arrives at; *status_dev = 1 when the wait ran out,
+// 2 if it (wrongly) completed.
+void launch_wait_timeout_probe(unsigned* status_dev, cudaStream_t st);
+
+// Run `set` (a cudaFuncSetAttribute call) once for each device it is needed
+// on.  Function attributes apply to the current device only, so a process
+// that drives several GPUs must set them on every one; `done` holds one bit
+// per device id.  Two threads racing here may both call `set`, which is
+// harmless (the attribute call is idempotent).
+template <typename F>
+inline void once_per_device(std::atomic<unsigned long long>& done, F&& set) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        set();
+        return;
+    }
+    const unsigned long long bit = 1ULL << dev;
+    if (done.load(std::memory_order_acquire) & bit) return;
+    set();
+    done.fetch_or(bit, std::memory_order_acq_rel);
+}
 
 }  // namespace lds

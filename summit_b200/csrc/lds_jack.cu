@@ -258,12 +258,11 @@ void launch_sym_solve(const double* sys, int64_t nsys, int K, double rtol, int r
                       double* x, int* rank, double* eig, int* status, cudaStream_t st) {
     if (nsys == 0) return;
     const size_t smem = (size_t)3 * K * (K + 1) * sizeof(double);
-    static bool attr = false;
-    if (!attr) {
+    static std::atomic<unsigned long long> attr{0};
+    once_per_device(attr, [] {
         cudaFuncSetAttribute(sym_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)((size_t)3 * kMaxK * (kMaxK + 1) * sizeof(double)));
-        attr = true;
-    }
+    });
     sym_solve_kernel<<<(unsigned)nsys, kSolveThreads, smem, st>>>(sys, K, rtol, require_full_rank, x,
                                                                    rank, eig, status);
     count_launch();

@@ -9,6 +9,7 @@
 // digit product is an exact int32 tensor-core accumulation; digits are
 // recombined exactly in int64 and converted to FP64 once.  The only error is
 // the representation error of the floating operand, |dy| <= 2^(e-8-7(S-1)).
+#include <cfloat>
 #include <cstdint>
 #include <cstdio>
 
@@ -268,19 +269,28 @@ __global__ void quantize_y_kernel(const double* __restrict__ Y, int64_t N, int64
     }
     const double* y = Y + ((int64_t)k * V + v) * N_pad;
     double amax = 0.0;
-    for (int64_t i = threadIdx.x; i < N; i += blockDim.x) amax = fmax(amax, fabs(y[i]));
-    amax = block_max(amax, red);
+    int bad = 0;
+    for (int64_t i = threadIdx.x; i < N; i += blockDim.x) {
+        const double a = fabs(y[i]);
+        bad |= !(a <= DBL_MAX);  // NaN or infinite
+        amax = fmax(amax, a);
+    }
+    // A non-finite sketch value makes every product with this column
+    // non-finite in the reference's GEMM; a NaN scale does the same here, so
+    // the phase-2 guards drop those updates just as the reference does.
+    bad = __syncthreads_or(bad);
+    amax = block_max(bad ? 0.0 : amax, red);
     const int e = digit_exponent(amax);
     for (int64_t i = threadIdx.x; i < N_pad; i += blockDim.x) {
         int8_t d[S];
-        if (i < N) {
+        if (i < N && !bad) {
             split_digits<S>(y[i], e, d);
         } else {
             for (int t = 0; t < S; ++t) d[t] = 0;
         }
         for (int t = 0; t < S; ++t) Yq[((int64_t)t * KVp + col) * N_pad + i] = d[t];
     }
-    if (threadIdx.x == 0) colscale[col] = ldexp(1.0, e - 7 - 7 * (S - 1));
+    if (threadIdx.x == 0) colscale[col] = bad ? (double)NAN : ldexp(1.0, e - 7 - 7 * (S - 1));
 }
 
 void launch_quantize_y(const double* Y, int64_t N, int64_t N_pad, int K, int V, int Vp, int S,

@@ -20,6 +20,12 @@
 //     threads without ordering) race on it; serialize them.
 //   * Sizes that do not fit are rejected with LDS_ERR_ARG and a message giving
 //     the bytes needed and the limit; nothing is allocated.
+//   * The kernel's status word (nonzero when a pipeline wait ran out) and its
+//     guard counters (non-finite / extreme updates dropped) are copied on the
+//     same stream into caller-owned device words when the caller passes them,
+//     so the call stays asynchronous.  Without them the call waits for its own
+//     work on the stream and returns the status itself, so a failed kernel is
+//     never reported as LDS_OK.
 // It calls no cudaMalloc, cudaFree or allocating library routine.
 #include <cstdint>
 #include <cstdio>
@@ -74,6 +80,9 @@ static int scratch_address(uint8_t** out) {
                     cudaGetErrorString(e);
             return LDS_ERR_CUDA;
         }
+        // The phase-2 kernel's shared-memory limit is a per-device attribute;
+        // set it here too, so that it is in place before any capture.
+        umma::prepare_p2_umma();
         slots[dev].addr = static_cast<uint8_t*>(p);
         slots[dev].ready = true;
     }
@@ -110,7 +119,7 @@ static bool map2d(CUtensorMap* m, const void* base, uint64_t inner, uint64_t out
 static int run(const uint8_t* d_codes, int64_t row_bytes, int64_t n, int64_t rows_total,
                int64_t j0, int64_t j1, const double* d_Y, int K, int V, const double* d_mean,
                const double* d_sdinv, const double* d_left_scale, double* d_accum, double* d_mc,
-               cudaStream_t st) {
+               unsigned* d_status_out, unsigned long long* d_guards_out, cudaStream_t st) {
     if (!d_codes || !d_Y || !d_mean || !d_sdinv || !d_left_scale || !d_accum) {
         g_msg = "null device pointer";
         return LDS_ERR_ARG;
@@ -180,11 +189,58 @@ static int run(const uint8_t* d_codes, int64_t row_bytes, int64_t n, int64_t row
     u.accum = d_accum;
     u.mc = d_mc;
     u.guard_counts = guards;
+    u.extreme_warn = phase2_extreme_warn();
+    u.drop_extreme = phase2_drop_extreme();
     u.status = status;
     umma::launch_p2_umma(tA, tB, u, st);
-    const cudaError_t e = cudaGetLastError();
+    cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         g_msg = std::string("launch failed: ") + cudaGetErrorString(e);
+        return LDS_ERR_CUDA;
+    }
+    if (d_status_out || d_guards_out) {
+        // Asynchronous report: the header words follow the kernel on `st`.
+        if (d_status_out)
+            e = cudaMemcpyAsync(d_status_out, status, sizeof(unsigned), cudaMemcpyDeviceToDevice, st);
+        if (e == cudaSuccess && d_guards_out)
+            e = cudaMemcpyAsync(d_guards_out, guards, 2 * sizeof(unsigned long long),
+                                cudaMemcpyDeviceToDevice, st);
+        if (e != cudaSuccess) {
+            g_msg = std::string("copy of the status words failed: ") + cudaGetErrorString(e);
+            return LDS_ERR_CUDA;
+        }
+        return LDS_OK;
+    }
+    // No caller-owned status words: wait for this call's work and read them
+    // here (into host stack memory; nothing is allocated).
+    unsigned h_status = 0;
+    unsigned long long h_guards[2] = {0, 0};
+    e = cudaMemcpyAsync(&h_status, status, sizeof h_status, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(h_guards, guards, sizeof h_guards, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        g_msg = std::string("phase 2 failed: ") + cudaGetErrorString(e);
+        return LDS_ERR_CUDA;
+    }
+    if (h_guards[0])
+        std::fprintf(stderr,
+                     "[phase2-warning] noalloc rows [%lld:%lld): dropped %llu non-finite LD-score "
+                     "updates.\n",
+                     (long long)j0, (long long)j1, h_guards[0]);
+    if (h_guards[1])
+        std::fprintf(stderr,
+                     "[phase2-warning] noalloc rows [%lld:%lld): %llu finite updates exceeded the "
+                     "LD-score warning threshold. They were %s; inspect this run before using it.\n",
+                     (long long)j0, (long long)j1, h_guards[1],
+                     u.drop_extreme ? "dropped" : "kept");
+    if (h_status) {
+        char buf[160];
+        std::snprintf(buf, sizeof buf,
+                      "phase-2 kernel aborted: a pipeline wait ran out (status %u); the "
+                      "accumulators are incomplete",
+                      h_status);
+        g_msg = buf;
         return LDS_ERR_CUDA;
     }
     return LDS_OK;
@@ -196,8 +252,10 @@ static int run(const uint8_t* d_codes, int64_t row_bytes, int64_t n, int64_t row
 extern "C" __attribute__((visibility("default"))) int lds_phase2_accum_device_noalloc(
     const uint8_t* d_codes, int64_t row_bytes, int64_t n, int64_t rows_total, int64_t j0,
     int64_t j1, const double* d_Y, int K, int V, const double* d_mean, const double* d_sdinv,
-    const double* d_left_scale, double* d_accum, double* d_mc, void* stream) {
+    const double* d_left_scale, double* d_accum, double* d_mc, unsigned* d_status,
+    unsigned long long* d_guards, void* stream) {
     return lds::noalloc::run(d_codes, row_bytes, n, rows_total, j0, j1, d_Y, K, V, d_mean, d_sdinv,
-                             d_left_scale, d_accum, d_mc, static_cast<cudaStream_t>(stream));
+                             d_left_scale, d_accum, d_mc, d_status, d_guards,
+                             static_cast<cudaStream_t>(stream));
 }
 

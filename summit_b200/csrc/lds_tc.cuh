@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include "lds_device.cuh"
+#include "lds_internal.h"
 
 namespace lds {
 namespace umma {
@@ -15,6 +16,18 @@ namespace umma {
 // kWaitLimit * kSuspendNs = 6.7 s.
 constexpr long long kWaitLimit = 1LL << 25;
 constexpr uint32_t kSuspendNs = 200;
+
+// The iteration limit in force: one copy per translation unit and device,
+// kWaitLimit unless lds_set_wait_limit() changed it.  Each file that includes
+// this header registers a setter for its copy (WaitLimitRegistrar below).
+static __constant__ long long c_wait_limit = kWaitLimit;
+
+__device__ __forceinline__ long long wait_limit() { return c_wait_limit; }
+
+// Host side: set this translation unit's copy on the current device.
+static inline cudaError_t set_wait_limit_here(long long iters) {
+    return cudaMemcpyToSymbol(c_wait_limit, &iters, sizeof iters);
+}
 
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
@@ -32,7 +45,8 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
 // Bounded wait for the phase with the given parity.  Returns false on timeout.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
     const uint32_t addr = smem_u32(bar);
-    for (long long i = 0; i < kWaitLimit; ++i) {
+    const long long limit = wait_limit();
+    for (long long i = 0; i < limit; ++i) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
@@ -145,6 +159,13 @@ __device__ __forceinline__ void decode_row_sw128(uint4 p0, uint4 p1, uint8_t* gR
         *reinterpret_cast<uint4*>(oRow + off) = make_uint4(o0, o1, o2, o3);
     }
 }
+
+// Registers set_wait_limit_here of the including file with the library, so
+// that lds_set_wait_limit reaches every copy of c_wait_limit.
+struct WaitLimitRegistrar {
+    WaitLimitRegistrar() { register_wait_limit_setter(&set_wait_limit_here); }
+};
+static WaitLimitRegistrar g_wait_limit_registrar;
 
 }  // namespace umma
 }  // namespace lds

@@ -17,6 +17,7 @@
 //
 // Every wait on an mbarrier is bounded; on timeout the kernel records an
 // error code in `status`, stops issuing work and releases its TMEM.
+#include <cfloat>
 #include <cstdint>
 #include <cstdio>
 #include <cuda.h>
@@ -147,7 +148,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (warp == 0) {
         // ---------------- packed-code producer (runs up to 8 stages ahead) ----------------
         if (lane == 0) {
-            for (int it = 0; it < total; ++it) {
+            int it = 0;
+            for (; it < total; ++it) {
                 const int s = it % kPkStages;
                 if (it >= kPkStages &&
                     !mbar_wait(&pk_empty[s], ((uint32_t)(it / kPkStages) & 1u) ^ 1u)) { fail(1); break; }
@@ -155,11 +157,17 @@ __global__ void __launch_bounds__(kThreads, 1)
                 mbar_expect_tx(&pk_full[s], (uint32_t)kPkBytes);
                 tma_load_2d(smem + lay.pk_off(s), &tmA, (it % a.nkt) * 32, (int)jt0, &pk_full[s]);
             }
+            // Drain: no tile copy may still be landing when the CTA exits (only
+            // reachable with copies outstanding after an abort).  Each slot's
+            // latest copy is among the last kPkStages issued.
+            for (int j = max(0, it - kPkStages); j < it; ++j)
+                mbar_wait(&pk_full[j % kPkStages], (uint32_t)(j / kPkStages) & 1u);
         }
     } else if (warp == 2) {
         // ---------------- sketch-digit producer ----------------
         if (lane == 0) {
-            for (int it = 0; it < total; ++it) {
+            int it = 0;
+            for (; it < total; ++it) {
                 const int s = it % kBStages;
                 if (it >= kBStages &&
                     !mbar_wait(&b_empty[s], ((uint32_t)(it / kBStages) & 1u) ^ 1u)) { fail(2); break; }
@@ -168,6 +176,8 @@ __global__ void __launch_bounds__(kThreads, 1)
                 mbar_expect_tx(&b_full[s], (uint32_t)(a.box_rows * kBK));
                 tma_load_2d(smem + lay.b_off(s), &tmB, kt * kBK, kb * a.ncolp + g * 256, &b_full[s]);
             }
+            for (int j = max(0, it - kBStages); j < it; ++j)
+                mbar_wait(&b_full[j % kBStages], (uint32_t)(j / kBStages) & 1u);
         }
     } else if (warp == 1) {
         // ---------------- MMA issuer ----------------
@@ -324,7 +334,17 @@ __global__ void quantize_y4_kernel(const double* __restrict__ Y, int64_t N, int6
     const int k = blockIdx.x / V, v = blockIdx.x - (blockIdx.x / V) * V;
     const double* y = Y + ((int64_t)k * V + v) * N_pad;
     double amax = 0.0;
-    for (int64_t i = threadIdx.x; i < N; i += blockDim.x) amax = fmax(amax, fabs(y[i]));
+    int bad = 0;
+    for (int64_t i = threadIdx.x; i < N; i += blockDim.x) {
+        const double av = fabs(y[i]);
+        bad |= !(av <= DBL_MAX);  // NaN or infinite
+        amax = fmax(amax, av);
+    }
+    // A non-finite sketch value makes every product with this column
+    // non-finite in the reference's GEMM; a NaN column scale does the same
+    // here, so the phase-2 guards drop those updates as the reference does.
+    bad = __syncthreads_or(bad);
+    if (bad) amax = 0.0;
     for (int o = 16; o; o >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = amax;
     __syncthreads();
@@ -343,7 +363,7 @@ __global__ void quantize_y4_kernel(const double* __restrict__ Y, int64_t N, int6
     int8_t* base = Yq + ((int64_t)k * ncolp + 4 * v) * N_pad;
     for (int64_t i = threadIdx.x; i < N_pad; i += blockDim.x) {
         int8_t d[4] = {0, 0, 0, 0};
-        if (i < N) {
+        if (i < N && !bad) {
             double t = ldexp(y[i], 7 - e);
             double rr = rint(t);
             d[0] = (int8_t)rr;
@@ -357,7 +377,7 @@ __global__ void quantize_y4_kernel(const double* __restrict__ Y, int64_t N, int6
         }
         for (int s = 0; s < 4; ++s) base[(int64_t)s * N_pad + i] = d[s];
     }
-    if (threadIdx.x == 0) colscale[(int64_t)k * V + v] = ldexp(1.0, e - 7 - 21);
+    if (threadIdx.x == 0) colscale[(int64_t)k * V + v] = bad ? (double)NAN : ldexp(1.0, e - 7 - 21);
 }
 
 __global__ void zero_pad_cols_kernel(int8_t* Yq, int64_t N_pad, int K, int V, int ncolp) {
@@ -379,6 +399,29 @@ void launch_quantize_y4(const double* Y, int64_t N, int64_t N_pad, int K, int V,
     }
 }
 
+// Self-test of the bounded wait: one thread initializes an mbarrier that
+// expects one arrival and waits for its first phase.  Nothing arrives, so the
+// wait must give up after the configured number of tries and the kernel
+// reports 1 (a completed wait would report 2).  No copy or MMA is in flight,
+// so the CTA exits cleanly either way.
+__global__ void wait_timeout_probe_kernel(unsigned* status) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        *status = mbar_wait(&bar, 0u) ? 2u : 1u;
+    }
+}
+
+}  // namespace umma
+
+void launch_wait_timeout_probe(unsigned* status_dev, cudaStream_t st) {
+    umma::wait_timeout_probe_kernel<<<1, 32, 0, st>>>(status_dev);
+    count_launch();
+}
+
+namespace umma {
+
 size_t p2_umma_smem_bytes(int box_rows) { return (size_t)Layout(box_rows).bytes() + 1024; }
 
 void prepare_p2_umma() {
@@ -391,12 +434,10 @@ void launch_p2_umma(const CUtensorMap& tmA, const CUtensorMap& tmB, const P2UArg
     const int64_t rows = a.j1 - a.j0;
     if ((!a.tiles && rows <= 0) || a.K <= 0) return;
     const size_t smem = p2_umma_smem_bytes(a.box_rows);
-    static size_t attr = 0;
-    if (attr < smem) {
-        cudaFuncSetAttribute(p2_umma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)p2_umma_smem_bytes(256));
-        attr = p2_umma_smem_bytes(256);
-    }
+    // The attribute is set for the largest tile (256 sketch rows), which
+    // covers every launch; function attributes are per device.
+    static std::atomic<unsigned long long> attr{0};
+    once_per_device(attr, [] { prepare_p2_umma(); });
     // With a tile table, j0 is unused and j1 - j0 carries the number of tiles.
     const int nb = a.bins_per_cta > 0 ? a.bins_per_cta : 1;
     dim3 grid((unsigned)(a.tiles ? rows : (rows + kBM - 1) / kBM), (unsigned)((a.K + nb - 1) / nb));

@@ -466,12 +466,8 @@ void prepare_p1_umma() {
 }
 
 void launch_p1_umma(const CUtensorMap& tmW, const P1UArgs& a, int64_t N_pad, cudaStream_t st) {
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(p1_umma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)p1_umma_smem_bytes());
-        attr = true;
-    }
+    static std::atomic<unsigned long long> attr{0};
+    once_per_device(attr, [] { prepare_p1_umma(); });
     const int spc = a.sb_per_cta > 0 ? a.sb_per_cta : 1;
     P1UArgs b = a;
     b.sb_per_cta = spc;

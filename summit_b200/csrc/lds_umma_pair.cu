@@ -83,7 +83,8 @@ __device__ __forceinline__ void arrive_cluster(uint32_t cluster_addr) {
 // Bounded wait with cluster-scope acquire (arrivals may come from the peer).
 __device__ __forceinline__ bool wait_cluster(uint64_t* bar, uint32_t parity) {
     const uint32_t addr = smem_u32(bar);
-    for (long long i = 0; i < kWaitLimit; ++i) {
+    const long long limit = wait_limit();
+    for (long long i = 0; i < limit; ++i) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -400,11 +401,8 @@ void launch_p2_umma_pair(const CUtensorMap& tmA, const CUtensorMap& tmB, const P
                          cudaStream_t st) {
     const int64_t rows = a.j1 - a.j0;
     if ((!a.tiles && rows <= 0) || a.K <= 0) return;
-    static bool attr = false;
-    if (!attr) {
-        prepare_p2_umma_pair();
-        attr = true;
-    }
+    static std::atomic<unsigned long long> attr{0};
+    once_per_device(attr, [] { prepare_p2_umma_pair(); });
     // With a tile table, j1 - j0 carries the number of PAIRS.
     const int nb = a.bins_per_cta > 0 ? a.bins_per_cta : 1;
     const int64_t pairs = a.tiles ? rows : (rows + 2 * pair::kBM - 1) / (2 * pair::kBM);

@@ -1,18 +1,22 @@
 """Golden vectors for the jackknife / normal-equation row, written by the
 reference's own Python (src/summit/inference/jackknife.py block boundaries,
 src/summit/context/fit.py solve_context_normal_equations, the replicate SE of
-src/summit/inference/gxe.py:2052-2057), imported from the reference tree.
+src/summit/inference/gxe.py:2052-2057), imported from the reference tree
+named by the SUMMIT_REFERENCE_DIR environment variable.
 
-    python tests/golden/make_golden_jackknife.py
+    SUMMIT_REFERENCE_DIR=<SUMMIT checkout> python tests/golden/make_golden_jackknife.py
 """
 from __future__ import annotations
 
+import os
 import sys
 from pathlib import Path
 
 import numpy as np
 
-REF = Path("/root/reference/src")
+if not os.environ.get("SUMMIT_REFERENCE_DIR"):
+    raise SystemExit("set SUMMIT_REFERENCE_DIR to the SUMMIT source tree")
+REF = Path(os.environ["SUMMIT_REFERENCE_DIR"]) / "src"
 sys.path.insert(0, str(REF))
 
 from summit.context import fit as F  # noqa: E402

@@ -56,3 +56,12 @@ def test_shim_argument_validation_matches_nanobind_rules():
         gwldcore._impute("median")
     assert gwldcore._dist("rademacher") == 0 and gwldcore._dist("normal") == 1
     assert gwldcore._dist("spherical") == 2
+
+
+def test_wait_limit_argument_check_without_gpu():
+    from summit_b200 import _lib
+
+    lib = _lib.load()
+    assert lib.lds_set_wait_limit(0) == -1
+    assert "wait limit" in lib.lds_last_error().decode()
+    assert lib.lds_get_wait_limit() == 1 << 25
