@@ -209,6 +209,14 @@ struct Prepared {
     DevBuf codes;
     std::vector<SnpCounts> counts;    // after imputation (HWE) or raw (mean)
     std::vector<double> mean, sdinv;  // per SNP, the reference's formulas
+    // 1 for a SNP whose standardized genotypes are identically zero: all
+    // calls missing, or every observed (or completed) call the same.  Such a
+    // SNP contributes exactly nothing to any product, but the reference's
+    // residual-variance weight for it is 1/sqrt(eps) (1e5 at the default
+    // eps); left in a phase-1 weight column it would set that column's digit
+    // scale and cost every other SNP in the column ~17 bits of precision, so
+    // the member lists leave it out.
+    std::vector<uint8_t> constant;
     int impute = LDS_IMPUTE_MEAN;
     int ddof = 1;
     DevBuf d_mean, d_sdinv;
@@ -429,6 +437,12 @@ std::unique_ptr<Prepared> prepare(Context& c, const uint8_t* host_rows, int64_t 
             stats_observed(nobs, sum, sumsq, ddof, P->mean[(size_t)j], P->sdinv[(size_t)j]);
         }
     }
+    P->constant.resize((size_t)M);
+    for (int64_t j = 0; j < M; ++j) {
+        const SnpCounts& k = P->counts[(size_t)j];
+        const int classes = (k.n[0] > 0) + (k.n[1] > 0) + (k.n[2] > 0);
+        P->constant[(size_t)j] = classes <= 1 ? 1 : 0;
+    }
     double* dm = P->d_mean.as<double>((size_t)std::max<int64_t>(M, 1));
     double* ds = P->d_sdinv.as<double>((size_t)std::max<int64_t>(M, 1));
     h2d(dm, P->mean.data(), (size_t)M, c.st);
@@ -522,7 +536,7 @@ struct Csr {
 
 template <typename T>
 Csr build_csr(const T* annot, const T* inv, int64_t L, int64_t K, int64_t snp0, int Vp, int S,
-              int64_t pad = kSnpStep) {
+              int64_t pad = kSnpStep, const uint8_t* constant = nullptr) {
     Csr c;
     c.bin_off.assign((size_t)K + 1, 0);
     c.nnz.assign((size_t)K, 0);
@@ -532,6 +546,7 @@ Csr build_csr(const T* annot, const T* inv, int64_t L, int64_t K, int64_t snp0, 
         for (int64_t i = 0; i < L; ++i) {
             const T a = annot[i * K + k];
             if (a == T(0)) continue;
+            if (constant && constant[snp0 + i]) continue;  // contributes exactly zero
             const double ad = (double)a;
             if (!(ad > 0.0) || !std::isfinite(ad)) continue;
             const double invd = (double)inv[i];
@@ -1371,7 +1386,8 @@ void apply_grm_impl(const char* bed_prefix, const char* fam_path, int nsnps, int
     for (int64_t j = 0; j < nsnps; ++j)
         for (int64_t q = 0; q < Q; ++q) Z[(size_t)(q * nsnps + j)] = (double)(T)coef[(size_t)(j * Q + q)];
     const int Vp = (int)round_up(Q, kColTile);
-    const Csr cs = build_csr<T>(ones.data(), w.data(), nsnps, 1, 0, Vp, c.slices);
+    const Csr cs = build_csr<T>(ones.data(), w.data(), nsnps, 1, 0, Vp, c.slices, kSnpStep,
+                                P.constant.data());
     if (cs.nnz[0] == 0) return;
     run_phase1(c, P, cs, 1, (int)Q, Z.data(), nsnps, nsnps, 0);
     double* Y = static_cast<double*>(c.y.p);
@@ -1533,7 +1549,7 @@ void phase1_bed_impl(const char* bed_prefix, const char* fam_path, int blk_start
     if (v_count <= 0) return;
     const int S = c.slices;
     const int Vp = (int)round_up(v_count, kColTile);
-    Csr csr = build_csr<T>(annot, inv.data(), L, K, blk_start, Vp, S);
+    Csr csr = build_csr<T>(annot, inv.data(), L, K, blk_start, Vp, S, kSnpStep, P.constant.data());
     const uint64_t root = has_seed ? seed : std::random_device{}();
     std::vector<double> Z((size_t)(L * v_count));
     make_probes<T>(root, blk_start, v_start, (int)L, v_count, rand_dist, Z.data(), L);
@@ -1796,8 +1812,10 @@ std::unique_ptr<GwPlan> plan_create(Context& c, std::shared_ptr<Prepared> P, con
         t->Vp = (int)round_up(V, kColTile);
         const bool tc = (p2_impl() == 1 && pl->S == 4);
         const int64_t pad = tc ? 128 : kSnpStep;
-        t->csr = as_float ? build_csr<float>(annot_f.data(), inv_f.data(), M, K, 0, t->Vp, pl->S, pad)
-                          : build_csr<double>(annot, pl->inv.data(), M, K, 0, t->Vp, pl->S, pad);
+        const uint8_t* cst = P->constant.data();
+        t->csr = as_float
+            ? build_csr<float>(annot_f.data(), inv_f.data(), M, K, 0, t->Vp, pl->S, pad, cst)
+            : build_csr<double>(annot, pl->inv.data(), M, K, 0, t->Vp, pl->S, pad, cst);
         // Probe streams per SNP block (mt19937_64), keyed by the block's start
         // in the whole fileset (make_seed, gwldcore.cpp:452-458): Rademacher
         // streams on the device, Gaussian ones on host threads.
@@ -2260,9 +2278,10 @@ std::unique_ptr<WinPlan> win_plan_create(Context& c, std::shared_ptr<Prepared> P
     std::vector<Csr> parts((size_t)W);
     par_windows([&](int64_t w) {
         const int64_t a0 = ws[w], L = ws[w + 1] - ws[w];
+        const uint8_t* cst = P->constant.data();
         parts[(size_t)w] = as_float
-            ? build_csr<float>(annot_f.data() + a0 * K, inv_f.data() + a0, L, K, a0, 16, 4, 128)
-            : build_csr<double>(annot + a0 * K, pl->inv.data() + a0, L, K, a0, 16, 4, 128);
+            ? build_csr<float>(annot_f.data() + a0 * K, inv_f.data() + a0, L, K, a0, 16, 4, 128, cst)
+            : build_csr<double>(annot + a0 * K, pl->inv.data() + a0, L, K, a0, 16, 4, 128, cst);
     });
     int64_t max_ksup = 0, max_wq = 0;
     for (int64_t w0 = 0; w0 < W; w0 += wb) {
@@ -4822,7 +4841,8 @@ LDS_API int lds_generalized_source_product(int64_t geno, int64_t j0, int64_t j1,
         std::vector<double> Z((size_t)(L * cols)), ones((size_t)L, 1.0);
         for (size_t i = 0; i < Z.size(); ++i) Z[i] = -rhs[i];
         const int Vp = (int)round_up(cols, kColTile);
-        const Csr cs = build_csr<double>(ones.data(), ratio.data(), L, 1, j0, Vp, c.slices);
+        const Csr cs = build_csr<double>(ones.data(), ratio.data(), L, 1, j0, Vp, c.slices,
+                                         kSnpStep, P.constant.data());
         run_phase1(c, P, cs, 1, (int)cols, Z.data(), L, L, j0);
         std::vector<double> y((size_t)(Np * cols));
         d2h(y.data(), static_cast<double*>(c.y.p), y.size(), c.st);
