@@ -654,6 +654,28 @@ int lds_gxe_create(int64_t geno, int64_t E, const double* environments, int64_t 
                    const double* feature_basis, const int64_t* power_indices,
                    const int64_t* power_offsets, const int32_t* ranks, int annotation_bins,
                    int64_t* handle_out);
+/* Dense-block form, the reference binding's own argument: a context for N
+ * samples whose source_block / target_score_block take the N x L column-major
+ * FP64 standardized genotype block the reference's driver passes
+ * (gxe_multi.py:3066-3230 -> gxeldcore.cpp:16420-16474) instead of an image
+ * block; the products run as FP64 GEMMs on the device.  The other calls
+ * (project_sources, pair_create, normalize_scores) take either context. */
+int lds_gxe_create_dense(int64_t N, int64_t E, const double* environments, int64_t r,
+                         const double* common_basis, const double* directions, int64_t F,
+                         const double* feature_basis, const int64_t* power_indices,
+                         const int64_t* power_offsets, const int32_t* ranks, int annotation_bins,
+                         int64_t* handle_out);
+int lds_gxe_source_block_dense(int64_t gxe, const double* genotype, int64_t L,
+                               const double* probes, int64_t B, const double* annotation,
+                               int annotation_is_sqrt, const double* scale_x,
+                               const double* scale_w, int64_t T, int environment_start,
+                               double* target, int device_ptrs);
+int lds_gxe_target_score_block_dense(int64_t gxe, const double* genotype, int64_t L, int64_t pair,
+                                     const double* scale_x, const double* scale_w, int64_t T,
+                                     double* accum_xx, double* accum_xw, double* accum_wx,
+                                     double* accum_ww, int64_t block_start,
+                                     int64_t total_variants, int probe_count,
+                                     int environment_start, int device_ptrs);
 int lds_gxe_destroy(int64_t gxe);
 /* Generalized per-SNP GxE packed products (GeneralizedGxELDScoreDirectContext::
  * packed_source_product / packed_target_product, generalized_gxe_variant.inc:

@@ -2972,8 +2972,10 @@ int64_t standardize_dosage_impl(T* G, int64_t N, int64_t L, int ddof, double mis
 // reference's driver passes (GenomewideEnvLDScore._read_genotype_block).
 // ---------------------------------------------------------------------------
 struct GxeCtx {
+    // The resident image whose blocks the products read, or null for a
+    // context that takes the reference's dense standardized genotype blocks.
     std::shared_ptr<Prepared> P;
-    int64_t N = 0, E = 0, r = 0;
+    int64_t N = 0, N_pad = 0, E = 0, r = 0;
     int K = 0;
     std::vector<int32_t> ranks;
     DevBuf env, common, dirs_ones, ranks_d, ones_M;
@@ -2981,6 +2983,7 @@ struct GxeCtx {
     // workspaces (grow-only)
     DevBuf probes, annot, sx, sw, panel, y, wq, wcs, rowind, sc, binoff, coef, coef2, denom;
     DevBuf sacc, acc4, guards, status, flag;
+    DevBuf dgeno, dw, ones_L;            // dense-block path
 };
 
 struct GxePair {
@@ -3011,12 +3014,16 @@ const T* dev_in(Context& c, DevBuf& buf, const T* p, size_t n, int device_ptrs) 
 
 // source_block: target (N x T 2 K B, column-major) += the contribution of SNPs
 // [j0, j1) (gxeldcore.cpp:11008-11240).
+// With `dense` (N x (j1 - j0) column-major standardized genotypes, host or
+// device memory as device_ptrs says) the block comes from the caller, as in
+// the reference's binding; otherwise it is SNPs [j0, j1) of the image.
 void gxe_source_impl(Context& c, GxeCtx& g, int64_t j0, int64_t j1, const double* probes, int64_t B,
                      const double* annot, int is_sqrt, const double* sx, const double* sw, int64_t T,
-                     int env_start, double* target, int device_ptrs) {
-    const Prepared& P = *g.P;
-    const int64_t L = j1 - j0, N = P.g.N, Np = P.g.N_pad, K = g.K;
-    if (B <= 0 || T <= 0 || env_start < 0 || env_start + T > g.E || L <= 0 || j0 < 0 || j1 > P.g.M)
+                     int env_start, double* target, int device_ptrs, const double* dense = nullptr) {
+    const int64_t L = j1 - j0, N = g.N, Np = g.N_pad, K = g.K;
+    if (!dense && !g.P) fail(LDS_ERR_ARG, "this kernel takes dense genotype blocks");
+    if (B <= 0 || T <= 0 || env_start < 0 || env_start + T > g.E || L <= 0 || j0 < 0 ||
+        (!dense && j1 > g.P->g.M))
         fail(LDS_ERR_ARG, "Multi-environment native source inputs have incompatible dimensions");
     const int64_t G = T * 2 * K, C = G * B;
     const double* dz = dev_in(c, g.probes, probes, (size_t)(L * B), device_ptrs);
@@ -3037,6 +3044,55 @@ void gxe_source_impl(Context& c, GxeCtx& g, int64_t j0, int64_t j1, const double
     if (fv) fail(LDS_ERR_ARG, "Multi-environment native source inputs contain invalid values");
     double* dtarget = device_ptrs ? target : g.panel.as<double>((size_t)(N * C));
     if (!device_ptrs) h2d(dtarget, target, (size_t)(N * C), c.st);
+    if (dense) {
+        // The caller's block is arbitrary FP64: weights[j, ((e 2 + h) K + k) B + b] =
+        // sqrt(a_jk) s_h,e[j] z_jb (gxeldcore.cpp:11008-11240) and Y = X weights as
+        // an FP64 product on the device.
+        std::vector<double> hz((size_t)(L * B));
+        d2h(hz.data(), dz, hz.size(), c.st);
+        ck(cudaStreamSynchronize(c.st), "gxe probes");
+        std::vector<double> W((size_t)(L * C), 0.0);
+        for (int64_t e = 0; e < T; ++e)
+            for (int h = 0; h < 2; ++h) {
+                const double* sh = (h == 0 ? hx.data() : hw.data()) + e * L;
+                for (int64_t k = 0; k < K; ++k) {
+                    const int64_t col0 = ((e * 2 + h) * K + k) * B;
+                    for (int64_t j = 0; j < L; ++j) {
+                        const double av = ha[(size_t)(k * L + j)];
+                        const double sa = is_sqrt ? av : std::sqrt(std::max(0.0, av));
+                        if (!(sa > 0.0)) continue;
+                        const double f = sa * sh[j];
+                        for (int64_t bq = 0; bq < B; ++bq)
+                            W[(size_t)((col0 + bq) * L + j)] = f * hz[(size_t)(bq * L + j)];
+                    }
+                }
+            }
+        const double* dg = dev_in(c, g.dgeno, dense, (size_t)(N * L), device_ptrs);
+        double* dW = g.dw.as<double>(W.size());
+        h2d(dW, W.data(), W.size(), c.st);
+        double* Y = g.y.as<double>((size_t)(Np * C));
+        DGemmArgs ga;
+        ga.M = N;
+        ga.N = C;
+        ga.K = L;
+        ga.A = dg;
+        ga.a_ms = 1;
+        ga.a_ks = N;
+        ga.B = dW;
+        ga.b_ks = 1;
+        ga.b_ns = L;
+        ga.C = Y;
+        ga.c_ms = 1;
+        ga.c_ns = Np;
+        launch_dgemm(ga, c.st);
+        launch_gxe_source_finalize(Y, N, Np, C, (int)(K * B), static_cast<double*>(g.env.p), N,
+                                   env_start, dtarget, N, c.st);
+        ck(cudaGetLastError(), "launch");
+        if (!device_ptrs) d2h(target, dtarget, (size_t)(N * C), c.st);
+        ck(cudaStreamSynchronize(c.st), "gxe source");
+        return;
+    }
+    const Prepared& P = *g.P;
     const int nc = umma::ncolp_for((int)B);
     // SNP chunks bound the weight-digit buffer (G x 2 x ncolp x chunk bytes).
     const int64_t cap = (int64_t)1 << 30;
@@ -3193,9 +3249,9 @@ void gxe_project_impl(Context& c, GxeCtx& g, double* panel, int64_t cols, int cp
 
 // [right, w o right] sealed on the device (prepare_protected_row_weighted_pair,
 // gxeldcore.cpp:9808); column c uses weight column c / (C / G).
-std::unique_ptr<GxePair> gxe_pair_impl(Context& c, const Prepared& P, const double* right, int64_t N,
+std::unique_ptr<GxePair> gxe_pair_impl(Context& c, const GxeCtx& g, const double* right, int64_t N,
                                        int64_t C, const double* w, int64_t G, int device_ptrs) {
-    if (N != P.g.N || C <= 0 || G <= 0 || C % G != 0)
+    if (N != g.N || C <= 0 || G <= 0 || C % G != 0)
         fail(LDS_ERR_ARG, "Protected GxE right-pair inputs have incompatible dimensions");
     auto pr = std::make_unique<GxePair>();
     pr->N = N;
@@ -3204,8 +3260,8 @@ std::unique_ptr<GxePair> gxe_pair_impl(Context& c, const Prepared& P, const doub
     DevBuf tr, tw;
     const double* dr = dev_in(c, tr, right, (size_t)(N * C), device_ptrs);
     const double* dw = dev_in(c, tw, w, (size_t)(N * G), device_ptrs);
-    double* yp = pr->ypair.as<double>((size_t)(P.g.N_pad * 2 * C));
-    launch_gxe_pair(dr, N, N, P.g.N_pad, C, C / G, dw, N, 0, yp, c.st);
+    double* yp = pr->ypair.as<double>((size_t)(g.N_pad * 2 * C));
+    launch_gxe_pair(dr, N, N, g.N_pad, C, C / G, dw, N, 0, yp, c.st);
     ck(cudaGetLastError(), "launch");
     ck(cudaStreamSynchronize(c.st), "gxe pair");
     return pr;
@@ -3215,18 +3271,18 @@ std::unique_ptr<GxePair> gxe_pair_impl(Context& c, const Prepared& P, const doub
 void gxe_target_impl(Context& c, GxeCtx& g, int64_t j0, int64_t j1, GxePair& pr, const double* sx,
                      const double* sw, int64_t T, double* axx, double* axw, double* awx, double* aww,
                      int64_t block_start, int64_t total, int probe_count, int env_start,
-                     int device_ptrs) {
-    const Prepared& P = *g.P;
-    const int64_t L = j1 - j0, N = P.g.N, Np = P.g.N_pad, K = g.K;
+                     int device_ptrs, const double* dense = nullptr) {
+    const int64_t L = j1 - j0, N = g.N, Np = g.N_pad, K = g.K;
+    if (!dense && !g.P) fail(LDS_ERR_ARG, "this kernel takes dense genotype blocks");
     if (block_start < 0 || total <= 0 || block_start + L > total || probe_count <= 0 || T <= 0 ||
-        env_start < 0 || env_start + T > g.E || L <= 0 || j0 < 0 || j1 > P.g.M)
+        env_start < 0 || env_start + T > g.E || L <= 0 || j0 < 0 || (!dense && j1 > g.P->g.M))
         fail(LDS_ERR_ARG, "Multi-environment native target scale/block metadata is invalid");
     const int64_t B = probe_count, pair_cols = T * 2 * K * B;
     if (pr.N != N || pr.C != pair_cols)
         fail(LDS_ERR_ARG, "Multi-environment native target pair is incompatible with the tile");
     const int64_t Kp = 2 * T * 2 * K;
     const int nc = umma::ncolp_for((int)B);
-    if (pr.B != (int)B) {
+    if (!dense && pr.B != (int)B) {
         int8_t* yq = pr.yq.as<int8_t>((size_t)(Kp * nc * Np));
         umma::launch_quantize_y4(static_cast<double*>(pr.ypair.p), N, Np, (int)Kp, (int)B, nc, yq,
                                  pr.ycs.as<double>((size_t)(Kp * B)), c.st);
@@ -3246,6 +3302,37 @@ void gxe_target_impl(Context& c, GxeCtx& g, int64_t j0, int64_t j1, GxePair& pr,
     if (fv) fail(LDS_ERR_ARG, "Multi-environment native target scales contain invalid values");
     double* S = g.sacc.as<double>((size_t)(L * Kp));
     ck(cudaMemsetAsync(S, 0, sizeof(double) * (size_t)(L * Kp), c.st), "memset");
+    unsigned* status = g.status.as<unsigned>(1);
+    ck(cudaMemsetAsync(status, 0, 4, c.st), "memset");
+    if (dense) {
+        // Work = X^T [S, w o S] (L x 2C) as an FP64 product, then per (SNP,
+        // group) the sum of squares over the group's B probes.
+        const double* dg = dev_in(c, g.dgeno, dense, (size_t)(N * L), device_ptrs);
+        double* Wk = g.dw.as<double>((size_t)(L * Kp * B));
+        DGemmArgs ga;
+        ga.M = L;
+        ga.N = Kp * B;
+        ga.K = N;
+        ga.A = dg;
+        ga.a_ms = N;
+        ga.a_ks = 1;
+        ga.B = static_cast<const double*>(pr.ypair.p);
+        ga.b_ks = 1;
+        ga.b_ns = Np;
+        ga.C = Wk;
+        ga.c_ms = 1;
+        ga.c_ns = L;
+        launch_dgemm(ga, c.st);
+        if ((int64_t)(g.ones_L.n / sizeof(double)) < L) {
+            std::vector<double> ones((size_t)L, 1.0);
+            h2d(g.ones_L.as<double>((size_t)L), ones.data(), ones.size(), c.st);
+        }
+        unsigned long long* gd = g.guards.as<unsigned long long>(2);
+        ck(cudaMemsetAsync(gd, 0, 16, c.st), "memset");
+        launch_dense_p2_epilogue(Wk, L, (int)Kp, (int)B, static_cast<double*>(g.ones_L.p), S,
+                                 nullptr, gd, std::numeric_limits<double>::infinity(), 0, c.st);
+    } else {
+    const Prepared& P = *g.P;
     const int nb = umma::p2_bins_per_cta(nc, (int)Kp);
     umma::P2UArgs u;
     u.K = (int)Kp;
@@ -3267,11 +3354,11 @@ void gxe_target_impl(Context& c, GxeCtx& g, int64_t j0, int64_t j1, GxePair& pr,
     u.guard_counts = g.guards.as<unsigned long long>(2);
     u.extreme_warn = std::numeric_limits<double>::infinity();
     u.drop_extreme = 0;
-    u.status = g.status.as<unsigned>(1);
-    ck(cudaMemsetAsync(u.status, 0, 4, c.st), "memset");
+    u.status = status;
     const CUtensorMap tmA = make_map_2d(P.g.codes, (uint64_t)P.g.nbp, (uint64_t)P.g.M_pad,
                                         (uint64_t)P.g.nbp, 32, 128, CU_TENSOR_MAP_SWIZZLE_NONE);
     umma::launch_p2_umma(tmA, pr.tmB, u, c.st);
+    }
     const size_t nacc = (size_t)(g.E * total * K);
     double* A[4];
     if (device_ptrs) {
@@ -3292,7 +3379,7 @@ void gxe_target_impl(Context& c, GxeCtx& g, int64_t j0, int64_t j1, GxePair& pr,
                                A[0], A[1], A[2], A[3], c.st);
     ck(cudaGetLastError(), "launch");
     unsigned stv = 0;
-    d2h(&stv, u.status, 1, c.st);
+    d2h(&stv, status, 1, c.st);
     if (!device_ptrs) {
         double* hs[4] = {axx, axw, awx, aww};
         for (int q = 0; q < 4; ++q) d2h(hs[q], A[q], nacc, c.st);
@@ -4730,18 +4817,19 @@ static GxePair& gxe_pair_of(int64_t h) {
     return *it->second;
 }
 
-LDS_API int lds_gxe_create(int64_t geno, int64_t E, const double* environments, int64_t r,
-                           const double* common_basis, const double* directions, int64_t F,
-                           const double* feature_basis, const int64_t* power_indices,
-                           const int64_t* power_offsets, const int32_t* ranks, int annotation_bins,
-                           int64_t* handle_out) {
+// The kernel's constructor state (MultiEnvironmentKernel, gxeldcore.cpp:
+// 10281-10297) for N samples; P is the resident image its blocks come from,
+// or null when the caller passes dense standardized genotype blocks.
+static int gxe_create_impl(std::shared_ptr<Prepared> P, int64_t N, int64_t E,
+                           const double* environments, int64_t r, const double* common_basis,
+                           const double* directions, int64_t F, const double* feature_basis,
+                           const int64_t* power_indices, const int64_t* power_offsets,
+                           const int32_t* ranks, int annotation_bins, int64_t* handle_out) {
     return guarded([&] {
         Context& c = ctx();
         std::lock_guard<std::mutex> lk(c.mu);
         ensure_device(c);
-        auto it = geno_table().find(geno);
-        if (it == geno_table().end()) fail(LDS_ERR_ARG, "unknown genotype handle");
-        const int64_t N = it->second->g.N;
+        if (!handle_out) fail(LDS_ERR_ARG, "null argument");
         if (N <= 2 || E <= 0 || F <= 0 || r < 0 || annotation_bins <= 0 || !environments ||
             !directions || !feature_basis || !power_indices || !power_offsets || !ranks ||
             (r > 0 && !common_basis))
@@ -4749,8 +4837,9 @@ LDS_API int lds_gxe_create(int64_t geno, int64_t E, const double* environments, 
         if (power_offsets[0] != 0)
             fail(LDS_ERR_ARG, "Multi-environment native feature offsets do not span their buffers");
         auto g = std::make_unique<GxeCtx>();
-        g->P = it->second;
+        g->P = P;
         g->N = N;
+        g->N_pad = P ? P->g.N_pad : round_up(N, kSamplePad);
         g->E = E;
         g->r = r;
         g->K = annotation_bins;
@@ -4770,7 +4859,7 @@ LDS_API int lds_gxe_create(int64_t geno, int64_t E, const double* environments, 
             std::memcpy(&dones[(size_t)(2 * e * N)], directions + e * N, sizeof(double) * (size_t)N);
         h2d(g->dirs_ones.as<double>(dones.size()), dones.data(), dones.size(), c.st);
         h2d(g->ranks_d.as<int32_t>((size_t)E), ranks, (size_t)E, c.st);
-        std::vector<double> ones((size_t)std::max<int64_t>(it->second->g.M, 1), 1.0);
+        std::vector<double> ones((size_t)std::max<int64_t>(P ? P->g.M : 1, 1), 1.0);
         h2d(g->ones_M.as<double>(ones.size()), ones.data(), ones.size(), c.st);
         g->basis0.resize((size_t)E);
         for (int64_t e = 0; e < E; ++e) {
@@ -4789,6 +4878,37 @@ LDS_API int lds_gxe_create(int64_t geno, int64_t E, const double* environments, 
         gxe_table()[h] = std::move(g);
         *handle_out = h;
     });
+}
+
+LDS_API int lds_gxe_create(int64_t geno, int64_t E, const double* environments, int64_t r,
+                           const double* common_basis, const double* directions, int64_t F,
+                           const double* feature_basis, const int64_t* power_indices,
+                           const int64_t* power_offsets, const int32_t* ranks, int annotation_bins,
+                           int64_t* handle_out) {
+    std::shared_ptr<Prepared> P;
+    {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        auto it = geno_table().find(geno);
+        if (it == geno_table().end()) {
+            set_last_error("unknown genotype handle");
+            return LDS_ERR_ARG;
+        }
+        P = it->second;
+    }
+    return gxe_create_impl(P, P->g.N, E, environments, r, common_basis, directions, F,
+                           feature_basis, power_indices, power_offsets, ranks, annotation_bins,
+                           handle_out);
+}
+
+LDS_API int lds_gxe_create_dense(int64_t N, int64_t E, const double* environments, int64_t r,
+                                 const double* common_basis, const double* directions, int64_t F,
+                                 const double* feature_basis, const int64_t* power_indices,
+                                 const int64_t* power_offsets, const int32_t* ranks,
+                                 int annotation_bins, int64_t* handle_out) {
+    return gxe_create_impl(nullptr, N, E, environments, r, common_basis, directions, F,
+                           feature_basis, power_indices, power_offsets, ranks, annotation_bins,
+                           handle_out);
 }
 
 // Generalized GxE packed products (generalized_gxe_variant.inc:1749-1988) on
@@ -4891,6 +5011,39 @@ LDS_API int lds_gxe_source_block(int64_t gxe, int64_t j0, int64_t j1, const doub
     });
 }
 
+LDS_API int lds_gxe_source_block_dense(int64_t gxe, const double* genotype, int64_t L,
+                                       const double* probes, int64_t B, const double* annotation,
+                                       int annotation_is_sqrt, const double* scale_x,
+                                       const double* scale_w, int64_t T, int environment_start,
+                                       double* target, int device_ptrs) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        if (!genotype || !probes || !annotation || !scale_x || !scale_w || !target)
+            fail(LDS_ERR_ARG, "null argument");
+        gxe_source_impl(c, gxe_of(gxe), 0, L, probes, B, annotation, annotation_is_sqrt, scale_x,
+                        scale_w, T, environment_start, target, device_ptrs, genotype);
+    });
+}
+
+LDS_API int lds_gxe_target_score_block_dense(int64_t gxe, const double* genotype, int64_t L,
+                                             int64_t pair, const double* scale_x,
+                                             const double* scale_w, int64_t T, double* accum_xx,
+                                             double* accum_xw, double* accum_wx, double* accum_ww,
+                                             int64_t block_start, int64_t total_variants,
+                                             int probe_count, int environment_start,
+                                             int device_ptrs) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        if (!genotype || !scale_x || !scale_w || !accum_xx || !accum_xw || !accum_wx || !accum_ww)
+            fail(LDS_ERR_ARG, "null argument");
+        gxe_target_impl(c, gxe_of(gxe), 0, L, gxe_pair_of(pair), scale_x, scale_w, T, accum_xx,
+                        accum_xw, accum_wx, accum_ww, block_start, total_variants, probe_count,
+                        environment_start, device_ptrs, genotype);
+    });
+}
+
 LDS_API int lds_gxe_project_sources(int64_t gxe, double* panel, int64_t columns,
                                     int columns_per_environment, int environment_start,
                                     double* leakages, int device_ptrs) {
@@ -4911,7 +5064,7 @@ LDS_API int lds_gxe_pair_create(int64_t gxe, const double* right, int64_t column
         std::lock_guard<std::mutex> lk(c.mu);
         if (!right || !row_weights) fail(LDS_ERR_ARG, "null argument");
         GxeCtx& g = gxe_of(gxe);
-        auto pr = gxe_pair_impl(c, *g.P, right, g.N, columns, row_weights, groups, device_ptrs);
+        auto pr = gxe_pair_impl(c, g, right, g.N, columns, row_weights, groups, device_ptrs);
         const int64_t h = next_handle();
         gxe_pair_table()[h] = std::move(pr);
         *pair_out = h;

@@ -5,12 +5,16 @@
 names, argument order, array layouts (column-major panels and genotype-side
 arrays, row-major ``(E * total_variants) x K`` score accumulators) and error
 messages (``src/native/gxeldcore.cpp:16420-16474``).  ``source_block`` and
-``target_score_block`` run on the GPU's int8 tensor cores from a resident
-genotype image, so their ``genotype`` argument is a block of one
-(``GwSession.block(start, stop)``) rather than a dense decoded matrix - the
-same role the reference's packed-genotype variants give a MailmanPackedBlock.
-The block's standardization is the image's (mean imputation, its ddof), which
-is what the reference's driver decodes into its dense blocks.
+``target_score_block`` take the ``genotype`` argument in either of two forms:
+
+* the reference's own: a dense N x L FP64 block of standardized genotypes (the
+  reference's driver passes ``np.asfortranarray(genotype, dtype=np.float64)``,
+  ``gxe_multi.py:3066-3230``), multiplied as FP64 GEMMs on the device; or
+* a block of a resident genotype image (``GwSession.block(start, stop)``),
+  multiplied on the int8 tensor cores straight from the packed codes - the
+  role the reference's packed-genotype variants give a MailmanPackedBlock.  Its
+  standardization is the image's (mean imputation, its ddof), which is what the
+  reference's driver decodes into its dense blocks.
 
 ``prepare_protected_row_weighted_pair`` and ``numpy_philox_rademacher_block``
 mirror the module functions of the same names.  There is no CPU fallback.
@@ -162,17 +166,35 @@ class MultiEnvironmentKernel:
             h = self._handles[session.handle] = out.value
         return h
 
-    @staticmethod
-    def _block(genotype) -> GenotypeBlock:
-        if not isinstance(genotype, GenotypeBlock):
-            raise TypeError("the GPU kernel takes genotype blocks of a resident image "
-                            "(summit_b200.session.GwSession.block(start, stop))")
-        return genotype
+    def _dense_ctx(self) -> int:
+        h = self._handles.get("dense")
+        if h is None:
+            out = C.c_int64(0)
+            check(_lib.load().lds_gxe_create_dense(
+                self._rows, self._E, ptr(self._env), self._cb.shape[1],
+                ptr(self._cb) if self._cb.shape[1] else None, ptr(self._dr), self._fb.shape[1],
+                ptr(self._fb), ptr(self._pidx), ptr(self._poff), ptr(self._ranks), self._bins,
+                C.byref(out)))
+            h = self._handles["dense"] = out.value
+        return h
+
+    def _dense(self, genotype):
+        """The reference's dense genotype argument (N x L, float64), or None
+        for a resident-image block."""
+        if isinstance(genotype, GenotypeBlock):
+            return None
+        if not isinstance(genotype, np.ndarray) or genotype.dtype != np.float64 \
+                or genotype.ndim != 2:
+            raise TypeError("incompatible function arguments: genotype must be a float64 "
+                            "(N, L) array or a resident-image block (GwSession.block)")
+        if genotype.shape[0] != self._rows:
+            raise RuntimeError("Multi-environment native source genotype rows do not match")
+        return np.asfortranarray(genotype)
 
     def source_block(self, target, genotype, probes, annotation, scale_x, scale_w,
                      environment_start, annotation_is_sqrt=False) -> int:
-        blk = self._block(genotype)
-        L = blk.stop - blk.start
+        dense = self._dense(genotype)
+        L = dense.shape[1] if dense is not None else genotype.stop - genotype.start
         target = _rw(target, "F", "target")
         z = _f64f(probes, "probes")
         a = _f64f(annotation, "annotation")
@@ -184,8 +206,13 @@ class MultiEnvironmentKernel:
             raise RuntimeError("Multi-environment native source inputs have incompatible dimensions")
         if target.shape != (self._rows, 2 * T * self._bins * B):
             raise RuntimeError("Multi-environment native packed source target is mis-sized")
+        if dense is not None:
+            check(_lib.load().lds_gxe_source_block_dense(
+                self._dense_ctx(), ptr(dense), L, ptr(z), B, ptr(a), int(bool(annotation_is_sqrt)),
+                ptr(sx), ptr(sw), T, int(environment_start), ptr(target), 0))
+            return 0
         check(_lib.load().lds_gxe_source_block(
-            self._ctx(blk.session), blk.start, blk.stop, ptr(z), B, ptr(a),
+            self._ctx(genotype.session), genotype.start, genotype.stop, ptr(z), B, ptr(a),
             int(bool(annotation_is_sqrt)), ptr(sx), ptr(sw), T, int(environment_start),
             ptr(target), 0))
         return 0
@@ -194,9 +221,7 @@ class MultiEnvironmentKernel:
         panel = _rw(panel, "F", "panel")
         if panel.shape[0] != self._rows:
             raise RuntimeError("Multi-environment native projection panel is mis-sized")
-        if not self._handles:
-            raise RuntimeError("project_sources follows a source_block call on a genotype image")
-        h = next(iter(self._handles.values()))
+        h = next(iter(self._handles.values())) if self._handles else self._dense_ctx()
         tile = panel.shape[1] // (2 * max(int(columns_per_environment), 1))
         leak = np.empty(max(tile, 1))
         check(_lib.load().lds_gxe_project_sources(h, ptr(panel), panel.shape[1],
@@ -207,8 +232,8 @@ class MultiEnvironmentKernel:
     def target_score_block(self, genotype, right_pair, scale_x, scale_w, accum_xx, accum_xw,
                            accum_wx, accum_ww, block_start, total_variants, probe_count,
                            environment_start) -> int:
-        blk = self._block(genotype)
-        L = blk.stop - blk.start
+        dense = self._dense(genotype)
+        L = dense.shape[1] if dense is not None else genotype.stop - genotype.start
         sx, sw = _f64f(scale_x, "scale_x"), _f64f(scale_w, "scale_w")
         accs = [_rw(x, "C", n) for x, n in ((accum_xx, "accum_xx"), (accum_xw, "accum_xw"),
                                              (accum_wx, "accum_wx"), (accum_ww, "accum_ww"))]
@@ -223,11 +248,18 @@ class MultiEnvironmentKernel:
         for x in accs:
             if x.shape != (self._E * total_variants, self._bins):
                 raise RuntimeError("Multi-environment native score accumulator is mis-sized")
-        h = self._ctx(blk.session)
+        if dense is not None:
+            h = self._dense_ctx()
+            check(_lib.load().lds_gxe_target_score_block_dense(
+                h, ptr(dense), L, right_pair._handle(h), ptr(sx), ptr(sw), T, ptr(accs[0]),
+                ptr(accs[1]), ptr(accs[2]), ptr(accs[3]), int(block_start), int(total_variants),
+                int(probe_count), int(environment_start), 0))
+            return 0
+        h = self._ctx(genotype.session)
         check(_lib.load().lds_gxe_target_score_block(
-            h, blk.start, blk.stop, right_pair._handle(h), ptr(sx), ptr(sw), T, ptr(accs[0]),
-            ptr(accs[1]), ptr(accs[2]), ptr(accs[3]), int(block_start), int(total_variants),
-            int(probe_count), int(environment_start), 0))
+            h, genotype.start, genotype.stop, right_pair._handle(h), ptr(sx), ptr(sw), T,
+            ptr(accs[0]), ptr(accs[1]), ptr(accs[2]), ptr(accs[3]), int(block_start),
+            int(total_variants), int(probe_count), int(environment_start), 0))
         return 0
 
     def normalize_scores(self, accum_xx, accum_xw, accum_wx, accum_ww, probe_count) -> None:

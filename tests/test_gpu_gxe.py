@@ -118,10 +118,66 @@ def test_gxe_rejects_invalid_inputs(small_bed):
     bad[3, 0] = 0.0
     with pytest.raises(RuntimeError, match="invalid values"):
         k.source_block(target, sess.block(0, L), z, np.ones((L, 1)), bad, np.ones((L, 1)), 0)
-    with pytest.raises(TypeError, match="genotype blocks"):
-        k.source_block(target, np.zeros((n, L)), z, np.ones((L, 1)), np.ones((L, 1)),
+    with pytest.raises(TypeError, match="float64"):
+        k.source_block(target, np.zeros((n, L), dtype=np.float32), z, np.ones((L, 1)),
+                       np.ones((L, 1)), np.ones((L, 1)), 0)
+    with pytest.raises(RuntimeError, match="rows do not match"):
+        k.source_block(target, np.zeros((n - 1, L)), z, np.ones((L, 1)), np.ones((L, 1)),
                        np.ones((L, 1)), 0)
     with pytest.raises(RuntimeError, match="mis-sized"):
         k.source_block(np.zeros((n, 5), order="F"), sess.block(0, L), z, np.ones((L, 1)),
                        np.ones((L, 1)), np.ones((L, 1)), 0)
     sess.close()
+
+
+@pytest.mark.parametrize("T,env_start,K", [(3, 0, 1), (2, 1, 2)])
+def test_gxe_dense_genotype_dropin_matches_reference(oracle, refgxe, small_bed, T, env_start, K):
+    """The reference builder's call sequence (GenomewideEnvLDScore.native_source_block /
+    native_target_score_block, gxe_multi.py:3066-3230) with the reference's own
+    argument: dense N x L FP64 standardized genotype blocks, the same arrays
+    handed to the reference's compiled gxeldcore.cpp and to the shim."""
+    from oracle.gxe_oracle import design, rademacher_block
+    from summit_b200.gxeldcore import prepare_protected_row_weighted_pair
+
+    n, m, packed = small_bed["n"], small_bed["m"], small_bed["rows"]
+    X = oracle.standardize(packed, n, 0, m)[0]
+    E = 3
+    d = design(n, E, seed=5, categorical=1)
+    ref, gpu = _kernels(refgxe, d, K)
+    rng = np.random.default_rng(9)
+    B = 5
+    cols = T * 2 * K * B
+    blocks = [(0, 97), (97, 98), (98, m)]
+    target_r = np.zeros((n, cols), order="F")
+    target_g = np.zeros((n, cols), order="F")
+    scales = {}
+    for (a, b) in blocks:
+        L = b - a
+        z = rademacher_block(11, a, L, range(B))
+        ann = rng.random((L, K)) + 0.05
+        ann[::7, 0] = 0.0
+        sx = 0.5 + rng.random((L, T))
+        sw = 0.5 + rng.random((L, T))
+        scales[(a, b)] = (sx, sw)
+        geno = np.asfortranarray(X[:, a:b], dtype=np.float64)
+        ref.source_block(target_r, geno, z, ann, sx, sw, env_start, False)
+        assert gpu.source_block(target_g, geno, z, ann, sx, sw, env_start) == 0
+    assert rel_err(target_g, target_r) < 1e-12
+    ref.project_sources(target_r, K * B, env_start)
+    gpu.project_sources(target_g, K * B, env_start)
+    assert rel_err(target_g, target_r) < 1e-12
+    w = d["environments"][:, env_start:env_start + T]
+    pair_r = ref.pair(target_r, w)
+    pair_g = prepare_protected_row_weighted_pair(target_g, w, 2)
+    accs_r = [np.zeros((E * m, K)) for _ in range(4)]
+    accs_g = [np.zeros((E * m, K)) for _ in range(4)]
+    for (a, b) in blocks:
+        sx, sw = scales[(a, b)]
+        geno = np.asfortranarray(X[:, a:b], dtype=np.float64)
+        ref.target_score_block(geno, pair_r, sx, sw, accs_r, a, m, B, env_start)
+        gpu.target_score_block(geno, pair_g, sx, sw, *accs_g, a, m, B, env_start)
+    ref.normalize_scores(accs_r, B)
+    gpu.normalize_scores(*accs_g, B)
+    for name, r_, g_ in zip(("xx", "xw", "wx", "ww"), accs_r, accs_g):
+        assert rel_err(g_, r_) < 1e-12, name
+    refgxe.lib.refg_pair_destroy(pair_r)
