@@ -121,3 +121,75 @@ def test_shard_offset_must_be_block_aligned():
     with pytest.raises(RuntimeError, match="mean"):
         h.shard_plan(annot[128:], 16, 64, 1, 128)
     h.close()
+
+
+def test_gxe_device_shards_match_unsharded_build(oracle):
+    """SNP-sharded GxE build on liblds (two shards run one after another on
+    one GPU; source panels summed with torch, the all-reduce of a multi-GPU
+    run), against the unsharded GxeReference build on the whole image, and
+    the one-rank ShardedGxe driver against the same build."""
+    import torch
+
+    from oracle.gxe_oracle import design, rademacher_block
+    from summit_b200.gxe import GxeReference
+    from summit_b200.session import GwSession, set_stream
+    from summit_b200.sharded import DeviceGxeShard, ShardedGxe, shard_bounds
+
+    n, m, E, K, B, T, step = 600, 900, 3, 1, 8, 3, 128
+    rows = oracle.synth_bed_rows(n, m, 13)
+    d = design(n, E, seed=2, categorical=1)
+    rng = np.random.default_rng(3)
+    probes = rademacher_block(9, 0, m, range(B))
+    ann = rng.random((m, K)) + 0.05
+    sx = 0.5 + rng.random((m, T))
+    sw = 0.5 + rng.random((m, T))
+    names = ("accum_xx", "accum_xw", "accum_wx", "accum_ww")
+
+    def cm(a):
+        return torch.from_numpy(np.ascontiguousarray(a.T)).cuda().T
+
+    g = GwSession(rows, n)
+    ref = GxeReference(g, d["environments"], d["feature_basis"], d["power_indices"],
+                       d["power_offsets"], d["ranks"], d["gram_values"], d["gram_offsets"],
+                       d["e2_gram_values"], d["common_basis"], d["directions"], K)
+    want = ref.run(cm(probes), cm(ann), cm(sx), cm(sw), 0)
+    want = {k: want[k].cpu().numpy() for k in names}
+    ref.close()
+    g.close()
+
+    # one rank: the driver equals the unsharded build
+    eng = DeviceGxeShard(rows, n, d, K)
+    try:
+        one = ShardedGxe(eng, shard_bounds(m, 1, step)).run(probes, ann, sx, sw, 0)
+    finally:
+        eng.close()
+    for k in names:
+        np.testing.assert_allclose(one.accums[k], want[k], rtol=1e-12, atol=0, err_msg=k)
+
+    # two shards on one device
+    bounds = shard_bounds(m, 2, step)
+    engines = [DeviceGxeShard(rows[s:e], n, d, K) for s, e in bounds]
+    stream = torch.cuda.Stream()
+    set_stream(stream.cuda_stream)
+    try:
+        with torch.cuda.stream(stream):
+            cols = T * 2 * K * B
+            panels = []
+            for eng_, (s, e) in zip(engines, bounds):
+                p = eng_.new_panel(cols)
+                eng_.source(p, probes[s:e], ann[s:e], sx[s:e], sw[s:e], 0)
+                panels.append(p)
+            total = torch.stack(panels).sum(0)
+            parts = []
+            for eng_ in engines:
+                p = total.clone()
+                assert eng_.project(p, K * B, 0).max() < 1e-9
+                parts.append(eng_.target(p, 0, B).reshape(4, E, eng_.M, K))
+            full = (torch.cat(parts, dim=2).reshape(4, -1, K) / float(B)).cpu().numpy()
+        torch.cuda.synchronize()
+    finally:
+        set_stream(None)
+        for eng_ in engines:
+            eng_.close()
+    for i, k in enumerate(names):
+        assert rel_err(full[i], want[k]) < 1e-6, k
