@@ -39,7 +39,6 @@ constexpr int kAccCols = 256;            // one accumulator: <= 256 digit column
 constexpr uint32_t kTmemCols = 512;      // two accumulators (MMA of job j+1 || epilogue of j)
 constexpr int kRing = 6;                 // gathered packed rows in flight per decoder thread
 constexpr int kRingSlot = 128 * 32;      // 128 member rows x 32 bytes
-constexpr int kStageTile = 16 * 32;      // per epilogue warp: 16 digit rows x 32 samples
 }  // namespace p1
 
 __global__ void __launch_bounds__(p1::kThreads, 1)
@@ -49,8 +48,7 @@ __global__ void __launch_bounds__(p1::kThreads, 1)
     uint8_t* smem = reinterpret_cast<uint8_t*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* ring = smem + kStages * kStageBytes;
-    uint8_t* digit_stage = ring + kRing * kRingSlot;  // [epilogue warp][16 rows][32 samples]
-    uint64_t* bars = reinterpret_cast<uint64_t*>(digit_stage + (kEpiThreads / 32) * kStageTile);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(ring + kRing * kRingSlot);
     uint64_t* full_w = bars;                    // [kStages] weight tiles landed (TMA)
     uint64_t* full_dec = bars + kStages;        // [kStages] genotype tiles decoded
     uint64_t* empty = bars + 2 * kStages;       // [kStages] stage consumed by the MMAs
@@ -274,11 +272,67 @@ __global__ void __launch_bounds__(p1::kThreads, 1)
                 // The warp's 32 samples of this super-bin's digit rows start here.
                 int8_t* const ywarp =
                     a.yq ? a.yq + (int64_t)k * a.ncolp * a.N_pad + i0 + q * 32 : nullptr;
-                uint8_t* const stage = digit_stage + (warp - 6) * kStageTile;
                 if (!mbar_wait(&acc_full[b], (uint32_t)u & 1u)) { fail(15); break; }
                 tc_fence_after();
                 const int ncols = min(kAccCols, a.ncolp - g * 256);
                 const uint32_t tbase = tmem + (uint32_t)(b * kAccCols) + ((uint32_t)(q * 32) << 16);
+                if (a.yq) {
+                    // Digits straight into phase 2's operand layout, 8 probes (32
+                    // digit columns) per TMEM load; the quadrant's four warps take
+                    // every fourth chunk.  With y = T 2^(eW-28) and the column
+                    // exponent eY fixed in advance by a bound on |y|, the sketch's
+                    // 28-bit value is R = rint(T 2^(eW-eY)) (round half to even);
+                    // its balanced base-128 digits are exact integer work.  A 4 x 4
+                    // byte transpose within each lane quad turns the lanes' digit
+                    // words (4 digits of one sample) into words of one digit for 4
+                    // consecutive samples, stored straight to global memory (a warp
+                    // writes 4 digit rows x 32 samples per probe).
+                    const int qd = lane & 3;
+                    const uint32_t selA = qd < 2 ? 0x5410u : 0x3276u;
+                    const uint32_t selB = (qd & 1) ? 0x3715u : 0x6240u;
+                    int8_t* const ylane = ywarp + 4 * (lane >> 2) + (int64_t)qd * a.N_pad;
+                    for (int c0 = 32 * h; c0 < ncols; c0 += 128) {
+                        int rr[32];
+                        tmem_ld32(tbase + (uint32_t)c0, rr);
+                        tmem_wait_ld();
+                        const int vl0 = c0 >> 2;                    // first probe of the chunk
+                        const int nv = a.V - (g * 64 + vl0);        // probes left (warp-uniform)
+#pragma unroll
+                        for (int p = 0; p < 8; ++p) {
+                            const int vl = vl0 + p;
+                            const int sh = __shfl_sync(0xffffffffu, vl < 32 ? shA : shB, vl & 31);
+                            const long long T =
+                                (((long long)rr[4 * p] * 128 + rr[4 * p + 1]) * 128 +
+                                 rr[4 * p + 2]) * 128 + rr[4 * p + 3];
+                            long long R;
+                            if (sh >= 0) {
+                                R = T << sh;
+                            } else {
+                                const int r = -sh;
+                                R = (T + ((1LL << (r - 1)) - 1) + ((T >> r) & 1)) >> r;
+                            }
+                            // |R| < 2^28 (the bound fixed eY): with U = R + 63 (2^14 +
+                            // 2^7 + 1) the low three base-128 digits of U are the
+                            // balanced digits d1..d3 (in [-63, 64]) plus 63 and U >> 21
+                            // is d0; the byte-wise subtraction of 63 from bytes 1..3
+                            // (their top bits set first, so no byte borrows) leaves
+                            // the word [d0, d1, d2, d3].
+                            const int U = (int)R + 63 * (16384 + 128 + 1);
+                            uint32_t w = (uint32_t)(U >> 21) & 0xFFu;
+                            w |= ((uint32_t)(U >> 14) & 127u) << 8;
+                            w |= ((uint32_t)(U >> 7) & 127u) << 16;
+                            w |= ((uint32_t)U & 127u) << 24;
+                            w = ((w | 0x80808000u) - 0x3F3F3F00u) ^ 0x80808000u;
+                            // 4 x 4 byte transpose across the quad: lane 4a + t ends
+                            // with digit t of samples 4a .. 4a + 3.
+                            w = __byte_perm(w, __shfl_xor_sync(0xffffffffu, w, 2), selA);
+                            w = __byte_perm(w, __shfl_xor_sync(0xffffffffu, w, 1), selB);
+                            if (p < nv)
+                                *reinterpret_cast<uint32_t*>(
+                                    ylane + (int64_t)(4 * (g * 64 + vl)) * a.N_pad) = w;
+                        }
+                    }
+                } else {
                 for (int c0c = 16 * h; c0c < ncols; c0c += 64) {
                     int rr[16];
                     tmem_ld16(tbase + (uint32_t)c0c, rr);
@@ -291,60 +345,10 @@ __global__ void __launch_bounds__(p1::kThreads, 1)
                         const long long T =
                             (((long long)rr[4 * p] * 128 + rr[4 * p + 1]) * 128 + rr[4 * p + 2]) *
                                 128 + rr[4 * p + 3];
-                        if (a.yq) {
-                            // Digits straight into phase 2's operand layout.  With
-                            // y = T 2^(eW-28) and the column exponent eY fixed in
-                            // advance by a bound on |y|, the sketch's 28-bit value is
-                            // R = rint(T 2^(eW-eY)) (round half to even); its
-                            // balanced base-128 digits are exact integer work.
-                            const int sh = __shfl_sync(0xffffffffu, vl < 32 ? shA : shB, vl & 31);
-                            long long R;
-                            if (sh >= 0) {
-                                R = T << sh;
-                            } else {
-                                const int r = -sh;
-                                R = (T + ((1LL << (r - 1)) - 1) + ((T >> r) & 1)) >> r;
-                            }
-                            // |R| < 2^28 (the bound fixed eY), so 32 bits suffice: with
-                            // U = R + 63 (2^14 + 2^7 + 1) the low three base-128 digits
-                            // of U are the balanced digits d1..d3 (in [-63, 64]) plus 63
-                            // and U >> 21 is d0.
-                            const int U = (int)R + 63 * (16384 + 128 + 1);
-                            uint32_t w = (uint32_t)(U >> 21) & 0xFFu;
-                            w |= ((uint32_t)(U >> 14) & 127u) << 8;
-                            w |= ((uint32_t)(U >> 7) & 127u) << 16;
-                            w |= ((uint32_t)U & 127u) << 24;
-                            // Byte-wise subtraction of 63 from bytes 1..3 (which
-                            // hold d + 63 in [0, 127]): with their top bits set
-                            // first, no byte borrows from the next; byte 0
-                            // subtracts 0.
-                            w = ((w | 0x80808000u) - 0x3F3F3F00u) ^ 0x80808000u;
-                            // Digit t of probe p of this chunk for this lane's
-                            // sample, staged as row 4p + t of a 16 x 32 byte tile.
-                            stage[(4 * p + 0) * 32 + lane] = (uint8_t)(w & 0xFFu);
-                            stage[(4 * p + 1) * 32 + lane] = (uint8_t)((w >> 8) & 0xFFu);
-                            stage[(4 * p + 2) * 32 + lane] = (uint8_t)((w >> 16) & 0xFFu);
-                            stage[(4 * p + 3) * 32 + lane] = (uint8_t)(w >> 24);
-                        } else {
-                            const double sc = __shfl_sync(0xffffffffu, vl < 32 ? scA : scB, vl & 31);
-                            a.Y[((int64_t)k * a.V + v) * a.N_pad + i] = sc * (double)T;
-                        }
+                        const double sc = __shfl_sync(0xffffffffu, vl < 32 ? scA : scB, vl & 31);
+                        a.Y[((int64_t)k * a.V + v) * a.N_pad + i] = sc * (double)T;
                     }
-                    if (a.yq) {
-                        // Write the staged tile: lane l stores 16 samples of digit
-                        // row l / 2 (one 16-byte store; the warp writes 16 rows x
-                        // 32 consecutive samples).
-                        __syncwarp();
-                        const int row = lane >> 1, half = lane & 1;
-                        const int v = g * 64 + c0c / 4 + (row >> 2);
-                        if (v < a.V) {
-                            const uint4 val =
-                                *reinterpret_cast<const uint4*>(stage + row * 32 + half * 16);
-                            *reinterpret_cast<uint4*>(ywarp + (int64_t)(4 * v + (row & 3)) * a.N_pad +
-                                                      half * 16) = val;
-                        }
-                        __syncwarp();
-                    }
+                }
                 }
                 tc_fence_before();
                 mbar_arrive(&acc_empty[b]);
@@ -456,8 +460,7 @@ void launch_p1_weights4(const P1UWeights& w, const double* mean, const double* s
 }
 
 size_t p1_umma_smem_bytes() {
-    return (size_t)p1::kStages * p1::kStageBytes + (size_t)p1::kRing * p1::kRingSlot +
-           (size_t)(p1::kEpiThreads / 32) * p1::kStageTile + 1024 + 256;
+    return (size_t)p1::kStages * p1::kStageBytes + (size_t)p1::kRing * p1::kRingSlot + 1024 + 256;
 }
 
 void prepare_p1_umma() {
