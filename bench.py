@@ -556,6 +556,25 @@ def ours_arm(args) -> None:
     gw_kms = plan.kernel_ms()
     plan.close()
 
+    # ---- the same windowed estimate on an HWE-completed image: no call is
+    # missing after imputation, so phase 2 runs no observed-count products ----
+    hwe = None
+    if not os.environ.get("LDS_SKIP_HWE"):
+        sess_h = GwSession(bed_host, n, impute_mode="hwe", impute_seed=PROBE_SEED)
+        hplan = autotune.tuned_win_plan(sess_h, annot, ws, B_PROBES, BLOCK, PROBE_SEED,
+                                        "rademacher", tune_if_missing=False)
+        for _ in range(args.warmup):
+            hplan.execute()
+        torch.cuda.synchronize()
+        hplan.kernel_ms()
+        h_ms = timed(hplan.execute, args.steps)
+        hkms = hplan.kernel_ms()
+        hplan.close()
+        sess_h.close()
+        hwe = {"value": round(world * ops / (h_ms * 1e-3) / 1e12, 3), "unit": "TOPS",
+               "ms_per_step": round(h_ms, 3), "impute": "hwe",
+               "kernel_ms": {k: round(v, 3) for k, v in hkms.items()}}
+
     # ---- learned control variate vs plain (config-2 shape, B = 10 vs 100) ----
     lvp = None
     if rank == 0 and not os.environ.get("LDS_SKIP_LEARNED"):
@@ -644,6 +663,8 @@ def ours_arm(args) -> None:
             "gpu_launches": launches,
             "clocks": clocks,
         }
+        if hwe is not None:
+            line["windowed_hwe"] = hwe
         if lvp is not None:
             line["learned_vs_plain"] = lvp
         if world == 1 and not os.environ.get("LDS_SKIP_CPU_BASELINE"):

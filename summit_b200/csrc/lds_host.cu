@@ -220,6 +220,11 @@ struct Prepared {
     int impute = LDS_IMPUTE_MEAN;
     int ddof = 1;
     DevBuf d_mean, d_sdinv;
+    // Per SNP row: 1 when the row has a missing call (after imputation).  When
+    // some rows have none (HWE-completed images, fully observed data), phase 2
+    // skips the O plane on 128-SNP tiles without missing calls.
+    DevBuf d_missing;
+    bool has_complete = false;
 };
 
 struct Context {
@@ -238,6 +243,7 @@ struct Context {
     void* pinned = nullptr;
     size_t pinned_n = 0;
     DevBuf y, yq, ycs, wq, wcs, z, rowind, sc, binoff, wqoff, accum, mc, guards, lscale, xin;
+    DevBuf colsum;  // per-block phase 2: sketch digit column sums (images with complete tiles)
     // Surrogate-network workspace, grow-only so that repeated training and
     // inference calls make no device allocations (cudaFree synchronizes).
     DevBuf mlp_m, mlp_v, mlp_g, mlp_zs, mlp_dzs, mlp_dout, mlp_rows, mlp_loss, mlp_pack;
@@ -438,11 +444,15 @@ std::unique_ptr<Prepared> prepare(Context& c, const uint8_t* host_rows, int64_t 
         }
     }
     P->constant.resize((size_t)M);
+    std::vector<uint8_t> miss((size_t)M);
     for (int64_t j = 0; j < M; ++j) {
         const SnpCounts& k = P->counts[(size_t)j];
         const int classes = (k.n[0] > 0) + (k.n[1] > 0) + (k.n[2] > 0);
         P->constant[(size_t)j] = classes <= 1 ? 1 : 0;
+        miss[(size_t)j] = k.n[3] > 0 ? 1 : 0;
+        if (!miss[(size_t)j]) P->has_complete = true;
     }
+    h2d(P->d_missing.as<uint8_t>((size_t)std::max<int64_t>(M, 1)), miss.data(), (size_t)M, c.st);
     double* dm = P->d_mean.as<double>((size_t)std::max<int64_t>(M, 1));
     double* ds = P->d_sdinv.as<double>((size_t)std::max<int64_t>(M, 1));
     h2d(dm, P->mean.data(), (size_t)M, c.st);
@@ -630,8 +640,9 @@ void quantize_sketch(Context& c, Prepared& P, int64_t K, int V) {
         const int nc = umma::ncolp_for(V);
         int8_t* yq = c.yq.as<int8_t>((size_t)(K * nc * P.g.N_pad));
         double* cs = c.ycs.as<double>((size_t)(K * V));
+        int* colsum = P.has_complete ? c.colsum.as<int>((size_t)(K * nc)) : nullptr;
         umma::launch_quantize_y4(static_cast<double*>(c.y.p), P.g.N, P.g.N_pad, (int)K, V, nc, yq,
-                                 cs, c.st);
+                                 cs, c.st, colsum);
         return;
     }
     const int S = c.slices;
@@ -699,6 +710,10 @@ void run_phase2(Context& c, Prepared& P, int64_t K, int V, int64_t j0, int64_t j
         u.extreme_warn = extreme_warn_env();
         u.drop_extreme = drop_extreme_env();
         u.status = reinterpret_cast<unsigned*>(guards + 2);
+        if (P.has_complete) {
+            u.snp_missing = static_cast<const uint8_t*>(P.d_missing.p);
+            u.colsum = static_cast<const int*>(c.colsum.p);
+        }
         const CUtensorMap tA = make_map_2d(P.g.codes, (uint64_t)P.g.nbp, (uint64_t)P.g.M_pad,
                                            (uint64_t)P.g.nbp, 32, 128, CU_TENSOR_MAP_SWIZZLE_NONE);
         const CUtensorMap tB =
@@ -1727,6 +1742,7 @@ struct GwPlan {
     };
     std::vector<std::unique_ptr<Tile>> tiles;
     DevBuf y, yq, ycs, accum, mc, lscale, guards, status;
+    DevBuf colsum;                   // sketch digit column sums (images with complete tiles)
     bool umma = false;
     std::vector<CUtensorMap> tmB;    // per V-tile (sketch digit layout depends on V)
     CUtensorMap tmA;
@@ -1881,6 +1897,7 @@ std::unique_ptr<GwPlan> plan_create(Context& c, std::shared_ptr<Prepared> P, con
         const int ncolp = umma::ncolp_for(vmax);
         int8_t* yq = pl->yq.as<int8_t>((size_t)(K * ncolp * P->g.N_pad));
         pl->ycs.as<double>((size_t)(K * vmax));
+        if (P->has_complete) pl->colsum.as<int>((size_t)(K * ncolp));
         pl->tmA = make_map_2d(P->g.codes, (uint64_t)P->g.nbp, (uint64_t)P->g.M_pad,
                               (uint64_t)P->g.nbp, 32, 128, CU_TENSOR_MAP_SWIZZLE_NONE);
         for (int V : pl->vt) {
@@ -1978,9 +1995,10 @@ void plan_enqueue_phase2(Context& c, GwPlan& pl, size_t ti, const double* y, cud
     GwPlan::Tile& t = *pl.tiles[ti];
     if (pl.umma) {
         const int nc = umma::ncolp_for(t.V);
+        int* colsum = P.has_complete ? static_cast<int*>(pl.colsum.p) : nullptr;
         umma::launch_quantize_y4(y, P.g.N, P.g.N_pad, (int)K, t.V, nc,
                                  static_cast<int8_t*>(pl.yq.p), static_cast<double*>(pl.ycs.p),
-                                 c.st);
+                                 c.st, colsum);
         if (ev) ck(cudaEventRecord(ev[e++], c.st), "event");
         umma::P2UArgs u;
         u.K = (int)K;
@@ -2004,6 +2022,10 @@ void plan_enqueue_phase2(Context& c, GwPlan& pl, size_t ti, const double* y, cud
         u.extreme_warn = extreme_warn_env();
         u.drop_extreme = drop_extreme_env();
         u.status = static_cast<unsigned*>(pl.status.p);
+        if (colsum) {
+            u.snp_missing = static_cast<const uint8_t*>(P.d_missing.p);
+            u.colsum = colsum;
+        }
         umma::launch_p2_umma(pl.tmA, pl.tmB[ti], u, c.st);
         if (ev) ck(cudaEventRecord(ev[e++], c.st), "event");
         return;
@@ -2151,6 +2173,7 @@ struct WinPlan {
     std::vector<Batch> batches;
     std::vector<DevBuf> z;              // per V-tile, M x V FP64 probes
     DevBuf y, ycs, yshift, wcs, accum, mc, lscale, guards, status;
+    DevBuf colsum;                      // sketch digit column sums (images with complete tiles)
     std::shared_ptr<DevBuf> yq, wq;     // shared context workspaces (Context::ws)
     // Optional outputs for the control variate (lds_win_plan_set_cv): per-V-tile
     // meansq slices, near-field sums C and known means mu, neighbour products.
@@ -2375,6 +2398,7 @@ std::unique_ptr<WinPlan> win_plan_create(Context& c, std::shared_ptr<Prepared> P
     pl->yq = shared_workspace(c, 0, (size_t)(max_ksup * ncmax * Np));
     pl->ycs.as<double>((size_t)(max_ksup * vmax));
     pl->yshift.as<int>((size_t)(max_ksup * vmax));
+    if (P->has_complete) pl->colsum.as<int>((size_t)(max_ksup * ncmax));
     pl->wq = shared_workspace(c, 1, (size_t)std::max<int64_t>(max_wq, 16));
     pl->wcs.as<double>((size_t)(max_ksup * vmax));
     pl->accum.as<double>((size_t)(M * K));
@@ -2480,7 +2504,12 @@ void win_enqueue(Context& c, WinPlan& pl) {
             pa.yshift = static_cast<int*>(pl.yshift.p);
             umma::launch_p1_umma(tmW, pa, Np, c.st);
             ck(cudaEventRecordWithFlags(pl.ev[(size_t)e++], c.st, cudaEventRecordExternal), "event");
-            // (sketch digits were written by phase 1's epilogue)
+            // (sketch digits were written by phase 1's epilogue; their column
+            // sums stand in for the O plane of tiles without missing calls)
+            int* colsum = P.has_complete ? static_cast<int*>(pl.colsum.p) : nullptr;
+            if (colsum)
+                umma::launch_digit_colsum(static_cast<const int8_t*>(pl.yq->p), b.ksup * nc, Np,
+                                          colsum, c.st);
             ck(cudaEventRecordWithFlags(pl.ev[(size_t)e++], c.st, cudaEventRecordExternal), "event");
             const int nb = umma::p2_bins_per_cta(nc, (int)K);
             const CUtensorMap tmB =
@@ -2512,6 +2541,10 @@ void win_enqueue(Context& c, WinPlan& pl) {
             u.extreme_warn = extreme_warn_env();
             u.drop_extreme = drop_extreme_env();
             u.status = static_cast<unsigned*>(pl.status.p);
+            if (colsum) {
+                u.snp_missing = static_cast<const uint8_t*>(P.d_missing.p);
+                u.colsum = colsum;
+            }
             if (pl.pairs >= 0 ? pl.pairs != 0 : p2_pairs() != 0) {
                 // Each CTA of a pair copies half of the sketch tile's columns.
                 const CUtensorMap tmBh =
@@ -3532,7 +3565,7 @@ LDS_API void lds_clear_device_cache(void) {
     for (auto& w : c.ws) w.reset();
     for (DevBuf* b : {&c.raw, &c.rows_dev, &c.hwe_q0, &c.hwe_q01, &c.hwe_sb, &c.counts_dev, &c.y,
                       &c.yq, &c.ycs, &c.wq, &c.wcs, &c.z, &c.rowind, &c.sc, &c.binoff, &c.wqoff,
-                      &c.accum, &c.mc, &c.guards, &c.lscale, &c.xin, &c.units_dev})
+                      &c.accum, &c.mc, &c.guards, &c.lscale, &c.xin, &c.units_dev, &c.colsum})
         b->release();
     if (c.pool) {
         cudaDeviceSynchronize();

@@ -167,5 +167,17 @@ struct WaitLimitRegistrar {
 };
 static WaitLimitRegistrar g_wait_limit_registrar;
 
+// The G row only (tiles whose O plane is not needed).
+__device__ __forceinline__ void decode_row_sw128_g(uint4 p0, uint4 p1, uint8_t* gRow, int r) {
+    const uint32_t words[8] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w};
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        uint32_t g0, g1, g2, g3, o0, o1, o2, o3;
+        decode8(words[c] & 0xFFFFu, g0, g1, o0, o1);
+        decode8(words[c] >> 16, g2, g3, o2, o3);
+        *reinterpret_cast<uint4*>(gRow + ((c ^ (r & 7)) << 4)) = make_uint4(g0, g1, g2, g3);
+    }
+}
+
 }  // namespace umma
 }  // namespace lds

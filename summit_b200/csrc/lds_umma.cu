@@ -137,6 +137,13 @@ __global__ void __launch_bounds__(kThreads, 1)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
+    // A tile whose output rows have no missing call needs no O plane.
+    int no_missing = (a.snp_missing && a.colsum) ? 1 : 0;
+    if (no_missing && tid < kBM) {
+        const int64_t j = jt0 + tid;
+        if (j < jend && j < a.M && a.snp_missing[j]) no_missing = 0;
+    }
+    const bool complete = __syncthreads_and(no_missing) != 0;
 
     auto fail = [&](int code) {
         atomicCAS(a.status, 0u, (unsigned)code);
@@ -201,7 +208,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                     for (int kk = 0; kk < kBK / 32; ++kk) {
                         const uint32_t acc = (kt | kk) ? 1u : 0u;
                         umma_i8(tmem, dG + 2 * kk, dB + 2 * kk, idesc, acc);
-                        umma_i8(tmem + kOCol, dO + 2 * kk, dB + 2 * kk, idesc, acc);
+                        if (!complete) umma_i8(tmem + kOCol, dO + 2 * kk, dB + 2 * kk, idesc, acc);
                     }
                     umma_commit(&a_empty[sa]);
                     umma_commit(&b_empty[sb]);
@@ -262,7 +269,8 @@ __global__ void __launch_bounds__(kThreads, 1)
                 if (it >= kAStages &&
                     !mbar_wait(&a_empty[sa], ((uint32_t)(it / kAStages) & 1u) ^ 1u)) { fail(6); break; }
                 uint8_t* gRow = smem + lay.a_off(sa) + (r >> 3) * 1024 + (r & 7) * 128;
-                decode_row_sw128(p0, p1, gRow, gRow + kATile, r);
+                if (complete) decode_row_sw128_g(p0, p1, gRow, r);
+                else decode_row_sw128(p0, p1, gRow, gRow + kATile, r);
                 fence_async_smem();
                 mbar_arrive(&a_full[sa]);
             }
@@ -276,7 +284,16 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (int c0 = 0; c0 < ncols; c0 += 32) {
                 int rg[32], ro[32];
                 tmem_ld32(tbase + (uint32_t)c0, rg);
-                tmem_ld32(tbase + kOCol + (uint32_t)c0, ro);
+                if (complete) {
+                    // every call observed: O^T y = the digit columns' sums
+                    // (columns past this CTA's bins belong to no output)
+                    const int live = min(ncols, nbk * a.ncolp - g * 256) - c0;
+                    const int* cs = a.colsum + (int64_t)kb * a.ncolp + g * 256 + c0;
+#pragma unroll
+                    for (int q = 0; q < 32; ++q) ro[q] = q < live ? cs[q] : 0;
+                } else {
+                    tmem_ld32(tbase + kOCol + (uint32_t)c0, ro);
+                }
                 tmem_wait_ld();
 #pragma unroll
                 for (int p = 0; p < 8; ++p) {
@@ -329,8 +346,9 @@ __global__ void __launch_bounds__(kThreads, 1)
 // ---------------------------------------------------------------------------
 __global__ void quantize_y4_kernel(const double* __restrict__ Y, int64_t N, int64_t N_pad, int K,
                                    int V, int ncolp, int8_t* __restrict__ Yq,
-                                   double* __restrict__ colscale) {
+                                   double* __restrict__ colscale, int* __restrict__ colsum) {
     __shared__ double red[32];
+    __shared__ int isum[4][32];
     const int k = blockIdx.x / V, v = blockIdx.x - (blockIdx.x / V) * V;
     const double* y = Y + ((int64_t)k * V + v) * N_pad;
     double amax = 0.0;
@@ -361,6 +379,7 @@ __global__ void quantize_y4_kernel(const double* __restrict__ Y, int64_t N, int6
         if (ldexp(amax, 7 - e) > 127.0) e += 1;
     }
     int8_t* base = Yq + ((int64_t)k * ncolp + 4 * v) * N_pad;
+    int dsum[4] = {0, 0, 0, 0};
     for (int64_t i = threadIdx.x; i < N_pad; i += blockDim.x) {
         int8_t d[4] = {0, 0, 0, 0};
         if (i < N && !bad) {
@@ -375,28 +394,77 @@ __global__ void quantize_y4_kernel(const double* __restrict__ Y, int64_t N, int6
                 t -= rr;
             }
         }
-        for (int s = 0; s < 4; ++s) base[(int64_t)s * N_pad + i] = d[s];
+        for (int s = 0; s < 4; ++s) {
+            base[(int64_t)s * N_pad + i] = d[s];
+            dsum[s] += d[s];
+        }
     }
     if (threadIdx.x == 0) colscale[(int64_t)k * V + v] = bad ? (double)NAN : ldexp(1.0, e - 7 - 21);
+    if (colsum) {
+        for (int s = 0; s < 4; ++s)
+            for (int o = 16; o; o >>= 1) dsum[s] += __shfl_xor_sync(0xffffffffu, dsum[s], o);
+        if ((threadIdx.x & 31) == 0)
+            for (int s = 0; s < 4; ++s) isum[s][threadIdx.x >> 5] = dsum[s];
+        __syncthreads();
+        if (threadIdx.x < 4) {
+            int tot = 0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += isum[threadIdx.x][w];
+            colsum[(int64_t)k * ncolp + 4 * v + threadIdx.x] = tot;
+        }
+    }
 }
 
-__global__ void zero_pad_cols_kernel(int8_t* Yq, int64_t N_pad, int K, int V, int ncolp) {
+// colsum[c] = sum of digit column c over its N_pad samples (one CTA per column).
+__global__ void digit_colsum_kernel(const int8_t* __restrict__ Yq, int64_t N_pad,
+                                    int* __restrict__ colsum) {
+    __shared__ int part[32];
+    const int8_t* col = Yq + (int64_t)blockIdx.x * N_pad;
+    int s = 0;
+    for (int64_t i = (int64_t)threadIdx.x * 16; i < N_pad; i += (int64_t)blockDim.x * 16) {
+        const int4 v = *reinterpret_cast<const int4*>(col + i);
+        const int w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            s += (int)(int8_t)(w[q]) + (int)(int8_t)(w[q] >> 8) + (int)(int8_t)(w[q] >> 16) +
+                 (int)(int8_t)(w[q] >> 24);
+    }
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int tot = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += part[w];
+        colsum[blockIdx.x] = tot;
+    }
+}
+
+__global__ void zero_pad_cols_kernel(int8_t* Yq, int64_t N_pad, int K, int V, int ncolp,
+                                     int* colsum) {
     const int k = blockIdx.y;
     const int c = 4 * V + blockIdx.x;
     if (c >= ncolp) return;
     int8_t* base = Yq + ((int64_t)k * ncolp + c) * N_pad;
     for (int64_t i = threadIdx.x; i < N_pad; i += blockDim.x) base[i] = 0;
+    if (colsum && threadIdx.x == 0) colsum[(int64_t)k * ncolp + c] = 0;
 }
 
 void launch_quantize_y4(const double* Y, int64_t N, int64_t N_pad, int K, int V, int ncolp,
-                        int8_t* Yq, double* colscale, cudaStream_t st) {
-    quantize_y4_kernel<<<(unsigned)(K * V), 256, 0, st>>>(Y, N, N_pad, K, V, ncolp, Yq, colscale);
+                        int8_t* Yq, double* colscale, cudaStream_t st, int* colsum) {
+    quantize_y4_kernel<<<(unsigned)(K * V), 256, 0, st>>>(Y, N, N_pad, K, V, ncolp, Yq, colscale,
+                                                          colsum);
     count_launch();
     if (ncolp > 4 * V) {
         zero_pad_cols_kernel<<<dim3((unsigned)(ncolp - 4 * V), (unsigned)K), 256, 0, st>>>(
-            Yq, N_pad, K, V, ncolp);
+            Yq, N_pad, K, V, ncolp, colsum);
         count_launch();
     }
+}
+
+void launch_digit_colsum(const int8_t* Yq, int64_t ncols, int64_t N_pad, int* colsum,
+                         cudaStream_t st) {
+    if (ncols <= 0) return;
+    digit_colsum_kernel<<<(unsigned)ncols, 256, 0, st>>>(Yq, N_pad, colsum);
+    count_launch();
 }
 
 // Self-test of the bounded wait: one thread initializes an mbarrier that

@@ -38,6 +38,13 @@ struct P2UArgs {
     // box_rows = min(256, bins_per_cta * ncolp) and ngroups =
     // ceil(bins_per_cta * ncolp / 256) must match.  1 unless ncolp <= 128.
     int bins_per_cta = 1;
+    // Tiles with every call observed: snp_missing[j] != 0 marks SNP row j as
+    // having a missing call.  A 128-SNP tile whose output rows have none
+    // skips the O plane: its observed-count products O^T y equal the sketch
+    // digits' column sums, colsum[global digit column] (int32, over all padded
+    // samples; padding samples carry zero digits).  Unused if either is null.
+    const uint8_t* snp_missing = nullptr;
+    const int* colsum = nullptr;
 };
 
 // Bins that share one CTA in phase 2: as many whole bins as fit 256 columns.
@@ -88,8 +95,12 @@ void launch_p1_umma(const CUtensorMap& tmW, const P1UArgs& a, int64_t N_pad, cud
 // Columns per bin (4 digits per probe, padded to a multiple of 16).
 inline int ncolp_for(int V) { return ((4 * V + 15) / 16) * 16; }
 
+// colsum (optional, K * ncolp ints): the digit columns' sums over all samples.
 void launch_quantize_y4(const double* Y, int64_t N, int64_t N_pad, int K, int V, int ncolp,
-                        int8_t* Yq, double* colscale, cudaStream_t st);
+                        int8_t* Yq, double* colscale, cudaStream_t st, int* colsum = nullptr);
+// colsum[c] = sum over the N_pad samples of digit column c of Yq (ncols columns).
+void launch_digit_colsum(const int8_t* Yq, int64_t ncols, int64_t N_pad, int* colsum,
+                         cudaStream_t st);
 size_t p2_umma_smem_bytes(int box_rows);
 // Set the kernels' shared-memory attributes ahead of any stream capture.
 void prepare_p2_umma();

@@ -188,3 +188,41 @@ def test_synthetic_image_equals_uploaded_rows(gw, n, m):
     np.testing.assert_array_equal(ra.results()["ldscore"], rb.results()["ldscore"])
     for x in (ra, rb, a, b):
         x.close()
+
+
+@pytest.mark.parametrize("impute", ["mean", "hwe"])
+def test_tiles_without_missing_calls_skip_the_o_plane(gw, oracle, impute):
+    """Phase 2 skips the observed-count products of 128-SNP tiles whose SNPs
+    have no missing call (their O^T y equals the sketch digits' column sums).
+    An image mixing complete and incomplete tiles, in the genome-wide session
+    and the windowed plan, against the oracle (HWE-completed images have no
+    missing call at all: every tile skips)."""
+    from summit_b200 import bedfile
+    from summit_b200.session import GwSession, WinPlan, window_seed
+
+    n, m = 300, 700
+    geno = bedfile.synth_genotypes(n, m, seed=606)
+    full = bedfile.synth_genotypes(n, m, seed=606, missing=False)
+    geno[:256] = full[:256]        # two complete tiles, then tiles with missing calls
+    geno[400:520] = full[400:520]  # a complete run that straddles tile boundaries
+    rows = bedfile.pack_bed_rows(geno)
+    annot = np.ones((m, 2))
+    annot[::3, 1] = 0.0
+    kw = dict(nvecs=24, seed=5, vtile=24, impute_seed=3)
+    got = gw.gw_ldscore(rows, n, annot, step_size=100, impute_mode=impute, with_mc=True, **kw)
+    want = oracle.gw_ldscore(rows, n, annot, step=100, impute=impute, with_mc=True, **kw)
+    assert_rel_elementwise(got["meansq_accum"], want["meansq_accum"], LD_RTOL, "session")
+    assert rel_err(got["mc_per_snp_sumsq"], want["mc_per_snp_sumsq"]) < 10 * LD_RTOL
+    ws = np.array([0, 130, 460, 700], dtype=np.int64)
+    sess = GwSession(rows, n, impute_mode=impute, impute_seed=3)
+    plan = WinPlan(sess, annot, ws, 24, 100, 9, "rademacher")
+    plan.execute()
+    res = plan.results()
+    plan.close()
+    sess.close()
+    for w in range(len(ws) - 1):
+        a, b = int(ws[w]), int(ws[w + 1])
+        ref = oracle.gw_ldscore(rows, n, annot[a:b], nvecs=24, step=100, seed=window_seed(9, w),
+                                impute=impute, impute_seed=3, snp0=a)
+        assert_rel_elementwise(res["meansq_accum"][a:b], ref["meansq_accum"], LD_RTOL,
+                               f"window {w}")
