@@ -521,9 +521,8 @@ def ours_arm(args) -> None:
     # phase-2 tile shape; every candidate's scores must agree bit for bit) ----
     from summit_b200 import autotune
 
-    cands = ([{"p1_sb_per_cta": s, "batch_gb": 8.0, "p2_pairs": 0} for s in (8, 16, 32, 64, 128)] +
-             [{"p1_sb_per_cta": 64, "batch_gb": b, "p2_pairs": 0} for b in (4.0, 16.0)] +
-             [{"p1_sb_per_cta": 64, "batch_gb": 8.0, "p2_pairs": 1}])
+    cands = ([{"p1_sb_per_cta": s, "batch_gb": 8.0} for s in (8, 16, 32, 64, 128)] +
+             [{"p1_sb_per_cta": 64, "batch_gb": b} for b in (4.0, 16.0)])
     t_tune = time.perf_counter()
     tune = autotune.tune_windowed(sess, annot, ws, B_PROBES, BLOCK, PROBE_SEED, "rademacher",
                                   candidates=cands, reps=1)

@@ -310,14 +310,13 @@ int lds_win_plan_kernel_ms(int64_t plan, double* ms4);
  * M_{w,k} / (N - ddof); the windowed counterpart of lds_gw_plan_bin_totals. */
 int lds_win_plan_bin_totals(int64_t plan, double* mkw_out);
 /* Tiling of one windowed plan, set before its first execute (the autotuner's
- * knobs; summit_b200/autotune.py chooses them by timing):
+ * knob; summit_b200/autotune.py chooses it, with the window batch size, by
+ * timing):
  *   p1_sb_per_cta: phase-1 super-bins (window x bin) per CTA, i.e. how the
- *     super-bin work list is split across CTAs (0: default 8);
- *   p2_pairs: phase 2 on SM pairs (1, M = 256) or one SM (0, M = 128);
- *     -1 follows lds_set_p2_pairs.
+ *     super-bin work list is split across CTAs (0: default 8).
  * The LD scores do not depend on the tiling (bit for bit).  No reference
  * counterpart (it replaces the reference's CPU tiling environment knobs). */
-int lds_win_plan_set_tiling(int64_t plan, int p1_sb_per_cta, int p2_pairs);
+int lds_win_plan_set_tiling(int64_t plan, int p1_sb_per_cta);
 int lds_win_plan_destroy(int64_t plan);
 
 /* Windowed + partitioned LD scores in one call from host BED rows (the
@@ -335,8 +334,8 @@ int lds_win_plan_destroy(int64_t plan);
  * seeds from the global SNP index, so the scores equal lds_win_plan_results
  * of one plan over the whole image (same seed, windows, V-tiles) bit for bit.
  * bed_rows: M rows of bed_row_bytes >= ceil(n_total/4) bytes (pinned host
- * memory uploads at full PCIe rate).  p1_sb_per_cta / p2_pairs: the chunks'
- * tiling as in lds_win_plan_set_tiling (0 / -1: defaults).  ldscore: M x K;
+ * memory uploads at full PCIe rate).  p1_sb_per_cta: the chunks' tiling as
+ * in lds_win_plan_set_tiling (0: default).  ldscore: M x K;
  * meansq_accum (M x K) and inv_out (M) may be NULL.  Returns after all
  * outputs are written. */
 int lds_win_ldscore(const uint8_t* bed_rows, int64_t bed_row_bytes, int64_t n_total, int64_t M,
@@ -344,8 +343,7 @@ int lds_win_ldscore(const uint8_t* bed_rows, int64_t bed_row_bytes, int64_t n_to
                     const int64_t* window_starts, int64_t n_windows, int nvecs, int step_size,
                     int vtile, uint64_t seed, int rand_dist, int ddof, int impute_mode,
                     uint64_t impute_seed, double resvar_eps, int as_float, int n_chunks,
-                    int p1_sb_per_cta, int p2_pairs, double* ldscore, double* meansq_accum,
-                    double* inv_out);
+                    int p1_sb_per_cta, double* ldscore, double* meansq_accum, double* inv_out);
 
 /* Control-variate outputs of a windowed plan (no counterpart in the reference;
  * they serve the learned control variate).  Call lds_win_plan_set_cv before the
@@ -409,13 +407,6 @@ int lds_debug_xt_products_umma(const uint8_t* bed_rows, int64_t bed_row_bytes, i
 /* Phase-2 kernel selection: 1 = tcgen05 (default), 0 = mma.sync.  Applies to
  * plans created afterwards.  No reference counterpart. */
 int lds_set_p2_kernel(int impl);
-/* Windowed phase 2 on SM pairs: on != 0 runs the windowed plans' phase 2 as
- * clusters of two CTAs (tcgen05.mma.cta_group::2, M = 256: two 128-SNP tiles
- * of a window share each sketch tile, each SM holding half of its columns).
- * Same results bit for bit.  Applies to plans executed for the first time
- * afterwards (the first execute captures the graph).  No reference
- * counterpart. */
-int lds_set_p2_pairs(int on);
 
 /* Synthetic genotype image generated on the device with the integer-exact
  * generator (identical bytes to the numpy generator in bedfile.py):

@@ -43,18 +43,17 @@ SIGNATURES: dict[str, tuple] = {
     "lds_set_stream": (_int, [_p]),
     "lds_debug_xt_products_umma": (_int, [_p, _i64, _i64, _i64, _p, _i64, _p, _p]),
     "lds_set_p2_kernel": (_int, [_int]),
-    "lds_set_p2_pairs": (_int, [_int]),
     "lds_win_plan_create": (_int, [_i64, _p, _i64, _p, _i64, _int, _int, _int, _u64, _int, _dbl,
                                    _int, _int, _dbl, _p]),
     "lds_win_ldscore": (_int, [_p, _i64, _i64, _i64, _p, _i64, _p, _i64, _p, _i64, _int, _int,
-                               _int, _u64, _int, _int, _int, _u64, _dbl, _int, _int, _int, _int,
+                               _int, _u64, _int, _int, _int, _u64, _dbl, _int, _int, _int,
                                _p, _p, _p]),
     "lds_win_plan_execute": (_int, [_i64]),
     "lds_win_plan_results": (_int, [_i64, _p, _p, _p, _p]),
     "lds_win_plan_kernel_ms": (_int, [_i64, _p]),
     "lds_win_plan_bin_totals": (_int, [_i64, _p]),
     "lds_win_plan_cv_annot": (_int, [_i64, _p]),
-    "lds_win_plan_set_tiling": (_int, [_i64, _int, _int]),
+    "lds_win_plan_set_tiling": (_int, [_i64, _int]),
     "lds_win_plan_destroy": (_int, [_i64]),
     "lds_win_plan_set_cv": (_int, [_i64, _p, _int, _int]),
     "lds_win_plan_tiles": (_int, [_i64, _p, _p]),

@@ -9,9 +9,7 @@ device work of a windowed estimate are chosen by timing them on the device:
   split across CTAs (super-bins per CTA: longer per-CTA pipelines against
   more CTAs to balance);
 * ``batch_gb``: how the windows are split into launches (the sketch digits of
-  one batch stay under this many GB);
-* ``p2_pairs``: the phase-2 tile shape, one SM (M = 128) or an SM pair
-  (M = 256, ``tcgen05.mma.cta_group::2``).
+  one batch stay under this many GB).
 
 The LD scores do not depend on any of them, and the tuner checks that: every
 candidate's scores must equal the first candidate's bit for bit.  A
@@ -32,13 +30,13 @@ from typing import Callable, Iterable
 
 import numpy as np
 
-DEFAULT_CONFIG = {"p1_sb_per_cta": 8, "batch_gb": 8.0, "p2_pairs": 0}
+DEFAULT_CONFIG = {"p1_sb_per_cta": 8, "batch_gb": 8.0}
 
 
 def default_candidates() -> list[dict]:
-    """Phase-1 split x window batching x phase-2 tile shape."""
-    return [{"p1_sb_per_cta": s, "batch_gb": b, "p2_pairs": p}
-            for s in (8, 16, 32, 64, 128) for b in (4.0, 8.0, 16.0) for p in (0, 1)]
+    """Phase-1 split x window batching."""
+    return [{"p1_sb_per_cta": s, "batch_gb": b}
+            for s in (8, 16, 32, 64, 128) for b in (4.0, 8.0, 16.0)]
 
 
 def cache_path() -> Path:
@@ -117,7 +115,7 @@ def _plan_runner(session, annot, window_starts, nvecs, step, seed, rand_dist, re
         plan = WinPlan(session, annot, window_starts, nvecs, step, seed, rand_dist,
                        batch_gb=float(cand["batch_gb"]))
         try:
-            plan.set_tiling(int(cand["p1_sb_per_cta"]), int(cand["p2_pairs"]))
+            plan.set_tiling(int(cand["p1_sb_per_cta"]))
             plan.execute()  # captures the graph
             ld = plan.results(meansq=False)["ldscore"]
             best = math.inf
@@ -188,5 +186,5 @@ def tuned_win_plan(session, annot, window_starts, nvecs: int, step: int, seed: i
     cfg = dict(DEFAULT_CONFIG, **(rec["config"] if rec else {}))
     plan = WinPlan(session, annot, window_starts, nvecs, step, seed, rand_dist,
                    batch_gb=float(cfg["batch_gb"]), **plan_kw)
-    plan.set_tiling(int(cfg["p1_sb_per_cta"]), int(cfg["p2_pairs"]))
+    plan.set_tiling(int(cfg["p1_sb_per_cta"]))
     return plan

@@ -186,12 +186,6 @@ CUtensorMap make_map_2d(void* base, uint64_t inner, uint64_t outer, uint64_t row
 }
 
 // Phase-2 implementation: 1 = tcgen05 (default; needs 4 digits), 0 = mma.sync.
-// Windowed phase 2 on SM pairs (p2_umma_pair_kernel): 1 = on.
-int& p2_pairs() {
-    static int on = 0;
-    return on;
-}
-
 int& p2_impl() {
     static int v = [] {
         const char* s = std::getenv("LDS_P2_KERNEL");
@@ -2167,8 +2161,8 @@ struct WinPlan {
     struct Batch {
         int64_t w0 = 0, w1 = 0, ksup = 0, lmax = 0;
         Csr csr;
-        DevBuf rowind, sc, binoff, tiles, ptiles;
-        int64_t ntiles = 0, nptiles = 0;   // 128-SNP tiles; pairs of tiles (SM-pair kernel)
+        DevBuf rowind, sc, binoff, tiles;
+        int64_t ntiles = 0;                // 128-SNP tiles
     };
     std::vector<Batch> batches;
     std::vector<DevBuf> z;              // per V-tile, M x V FP64 probes
@@ -2179,8 +2173,8 @@ struct WinPlan {
     // meansq slices, near-field sums C and known means mu, neighbour products.
     int split = 0, cv_D = 0;
     // Tiling chosen for this plan (lds_win_plan_set_tiling): phase-1 super-bins
-    // per CTA (0: default) and phase 2 on SM pairs (-1: the global switch).
-    int p1_spc = 0, pairs = -1;
+    // per CTA (0: default).
+    int p1_spc = 0;
     DevBuf annot_d, winof_d, sqrt_ls, xx, band_cnt, cvC, cvMu;
     DevBuf mkw_d, ld_d, ms_d;           // finalize inputs and outputs
     cudaEvent_t cv_ev[2] = {nullptr, nullptr};
@@ -2344,12 +2338,6 @@ std::unique_ptr<WinPlan> win_plan_create(Context& c, std::shared_ptr<Prepared> P
                 tiles.push_back(make_int4((int)j, (int)ws[w + 1], (int)((w - b.w0) * K), 0));
         b.ntiles = (int64_t)tiles.size();
         h2d(b.tiles.as<int4>(tiles.size()), tiles.data(), tiles.size(), c.st);
-        std::vector<int4> ptiles;  // pairs of consecutive tiles of one window
-        for (int64_t w = b.w0; w < b.w1; ++w)
-            for (int64_t j = ws[w]; j < ws[w + 1]; j += 256)
-                ptiles.push_back(make_int4((int)j, (int)ws[w + 1], (int)((w - b.w0) * K), 0));
-        b.nptiles = (int64_t)ptiles.size();
-        h2d(b.ptiles.as<int4>(ptiles.size()), ptiles.data(), ptiles.size(), c.st);
         ck(cudaStreamSynchronize(c.st), "window batch upload");
         max_ksup = std::max(max_ksup, b.ksup);
         max_wq = std::max(max_wq, b.ksup * 2 * ncmax * b.lmax);
@@ -2411,7 +2399,6 @@ std::unique_ptr<WinPlan> win_plan_create(Context& c, std::shared_ptr<Prepared> P
     for (auto& e : pl->ev) ck(cudaEventCreate(&e), "event");
     umma::prepare_p1_umma();
     umma::prepare_p2_umma();
-    umma::prepare_p2_umma_pair();
     ck(cudaStreamSynchronize(c.st), "window plan");
     return pl;
 }
@@ -2545,18 +2532,8 @@ void win_enqueue(Context& c, WinPlan& pl) {
                 u.snp_missing = static_cast<const uint8_t*>(P.d_missing.p);
                 u.colsum = colsum;
             }
-            if (pl.pairs >= 0 ? pl.pairs != 0 : p2_pairs() != 0) {
-                // Each CTA of a pair copies half of the sketch tile's columns.
-                const CUtensorMap tmBh =
-                    make_map_2d(pl.yq->p, (uint64_t)Np, (uint64_t)(b.ksup * nc), (uint64_t)Np, 128,
-                                (uint32_t)(std::min(256, nb * nc) / 2), CU_TENSOR_MAP_SWIZZLE_128B);
-                u.tiles = static_cast<int4*>(b.ptiles.p);
-                u.j1 = b.nptiles;  // number of tile pairs
-                umma::launch_p2_umma_pair(pl.tmA, tmBh, u, c.st);
-            } else {
-                u.tiles = static_cast<int4*>(b.tiles.p);
-                umma::launch_p2_umma(pl.tmA, tmB, u, c.st);
-            }
+            u.tiles = static_cast<int4*>(b.tiles.p);
+            umma::launch_p2_umma(pl.tmA, tmB, u, c.st);
             ck(cudaEventRecordWithFlags(pl.ev[(size_t)e++], c.st, cudaEventRecordExternal), "event");
         }
     }
@@ -2662,7 +2639,7 @@ void win_ldscore_impl(const uint8_t* bed_rows, int64_t row_bytes, int64_t n_tota
                       const int64_t* row_sel, int64_t n_sel, const double* annot, int64_t K,
                       const int64_t* ws, int64_t W, int nvecs, int step, int vtile, uint64_t seed,
                       int dist, int ddof, int impute, uint64_t iseed, double eps, int as_float,
-                      int n_chunks, int p1_spc, int pairs, double* ldscore, double* meansq_out,
+                      int n_chunks, int p1_spc, double* ldscore, double* meansq_out,
                       double* inv_out) {
     using clk = std::chrono::steady_clock;
     const auto t_start = clk::now();
@@ -2796,7 +2773,6 @@ void win_ldscore_impl(const uint8_t* bed_rows, int64_t row_bytes, int64_t n_tota
                                          nvecs, step, vtile, seed, dist, eps, as_float, 0,
                                          chunk_gb, wa);
             ch[i].plan->p1_spc = std::max(0, p1_spc);
-            ch[i].plan->pairs = pairs < 0 ? -1 : (pairs ? 1 : 0);
             ch[i].plan->ld_d.as<double>((size_t)(L * K));
             ch[i].plan->ms_d.as<double>((size_t)(L * K));
             ck(cudaStreamSynchronize(c.st_prep), "chunk set-up");
@@ -4481,11 +4457,6 @@ LDS_API int lds_debug_xt_products_umma(const uint8_t* bed_rows, int64_t bed_row_
     });
 }
 
-LDS_API int lds_set_p2_pairs(int on) {
-    p2_pairs() = on ? 1 : 0;
-    return LDS_OK;
-}
-
 LDS_API int lds_set_p2_kernel(int impl) {
     if (impl != 0 && impl != 1) {
         g_err = "p2 kernel must be 0 (mma.sync) or 1 (tcgen05)";
@@ -4521,12 +4492,12 @@ LDS_API int lds_win_ldscore(const uint8_t* bed_rows, int64_t bed_row_bytes, int6
                             int64_t n_windows, int nvecs, int step_size, int vtile, uint64_t seed,
                             int rand_dist, int ddof, int impute_mode, uint64_t impute_seed,
                             double resvar_eps, int as_float, int n_chunks, int p1_sb_per_cta,
-                            int p2_pairs, double* ldscore, double* meansq_accum, double* inv_out) {
+                            double* ldscore, double* meansq_accum, double* inv_out) {
     return guarded([&] {
         win_ldscore_impl(bed_rows, bed_row_bytes, n_total, M, row_sel, n_row_sel, annot, K,
                          window_starts, n_windows, nvecs, step_size, vtile, seed, rand_dist, ddof,
                          impute_mode, impute_seed, resvar_eps, as_float, n_chunks, p1_sb_per_cta,
-                         p2_pairs, ldscore, meansq_accum, inv_out);
+                         ldscore, meansq_accum, inv_out);
     });
 }
 
@@ -4564,7 +4535,7 @@ LDS_API int lds_win_plan_kernel_ms(int64_t plan, double* ms4) {
     });
 }
 
-LDS_API int lds_win_plan_set_tiling(int64_t plan, int p1_sb_per_cta, int p2_pairs) {
+LDS_API int lds_win_plan_set_tiling(int64_t plan, int p1_sb_per_cta) {
     return guarded([&] {
         Context& c = ctx();
         std::lock_guard<std::mutex> lk(c.mu);
@@ -4573,7 +4544,6 @@ LDS_API int lds_win_plan_set_tiling(int64_t plan, int p1_sb_per_cta, int p2_pair
         if (p1_sb_per_cta < 0 || p1_sb_per_cta > 4096)
             fail(LDS_ERR_ARG, "p1_sb_per_cta must be in [0, 4096]");
         pl.p1_spc = p1_sb_per_cta;
-        pl.pairs = p2_pairs < 0 ? -1 : (p2_pairs ? 1 : 0);
     });
 }
 

@@ -107,13 +107,6 @@ void prepare_p2_umma();
 void prepare_p1_umma();
 void launch_p2_umma(const CUtensorMap& tmA, const CUtensorMap& tmB, const P2UArgs& a,
                     cudaStream_t st);
-// SM-pair form (lds_umma_pair.cu): clusters of two CTAs over pairs of 128-SNP
-// tiles; tmB's box is half the sketch tile's rows (box_rows / 2); with a tile
-// table, tiles[p] is the pair's first tile and j1 - j0 the number of pairs.
-size_t p2_umma_pair_smem_bytes(int box_rows);
-void prepare_p2_umma_pair();
-void launch_p2_umma_pair(const CUtensorMap& tmA, const CUtensorMap& tmB, const P2UArgs& a,
-                         cudaStream_t st);
 
 }  // namespace umma
 }  // namespace lds

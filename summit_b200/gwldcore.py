@@ -630,11 +630,6 @@ def set_p2_kernel(impl: str) -> None:
     check(_lib.load().lds_set_p2_kernel({"mma": 0, "tcgen05": 1}[impl]))
 
 
-def set_p2_pairs(on: bool) -> None:
-    """Run windowed phase 2 on SM pairs (cta_group::2) for plans executed from now on."""
-    check(_lib.load().lds_set_p2_pairs(int(bool(on))))
-
-
 def set_slices(s: int) -> None:
     check(_lib.load().lds_set_slices(int(s)))
 

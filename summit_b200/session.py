@@ -262,10 +262,10 @@ class WinPlan:
         return {"weights": buf[0], "phase1": buf[1], "digits": buf[2], "phase2": buf[3]}
 
     # ---- control-variate outputs (see lds_win_plan_set_cv) ----
-    def set_tiling(self, p1_sb_per_cta: int = 0, p2_pairs: int = -1) -> None:
-        """Phase-1 super-bins per CTA (0: default) and phase 2 on SM pairs
-        (1/0; -1: the global switch); call before the first execute."""
-        check(_lib.load().lds_win_plan_set_tiling(self.handle, int(p1_sb_per_cta), int(p2_pairs)))
+    def set_tiling(self, p1_sb_per_cta: int = 0) -> None:
+        """Phase-1 super-bins per CTA (0: default); call before the first
+        execute."""
+        check(_lib.load().lds_win_plan_set_tiling(self.handle, int(p1_sb_per_cta)))
 
     def cv_annot_view(self):
         """Read-only torch view (cuda, float64, M x K) of the annotation matrix the
@@ -350,7 +350,7 @@ def windowed_ldscore(bed_rows, n_total: int, annot, window_starts, nvecs: int, s
     ``bed_rows`` in pinned memory (e.g. a ``pin_memory=True`` torch tensor's
     ``.numpy()``) for full-rate uploads.  Returns ``ldscore`` (M x K) and, with
     ``meansq``, ``meansq_accum`` and ``inv``.  ``tiling`` (``p1_sb_per_cta``,
-    ``p2_pairs``, e.g. an autotuner record's config) sets the chunks' tiling.
+    e.g. an autotuner record's config) sets the chunks' tiling.
     """
     tiling = tiling or {}
     bed_rows = np.ascontiguousarray(bed_rows, dtype=np.uint8)
@@ -370,7 +370,7 @@ def windowed_ldscore(bed_rows, n_total: int, annot, window_starts, nvecs: int, s
                                       int(ddof), _impute(impute_mode), int(impute_seed),
                                       float(eps), int(as_float), int(chunks),
                                       int(tiling.get("p1_sb_per_cta", 0)),
-                                      int(tiling.get("p2_pairs", -1)), ptr(ld), ptr(ms), ptr(inv)))
+                                      ptr(ld), ptr(ms), ptr(inv)))
     return {"ldscore": ld, "meansq_accum": ms, "inv": inv}
 
 

@@ -30,7 +30,7 @@ def test_workload_key_is_stable_and_shape_sensitive():
 def test_select_picks_fastest_and_checks_scores():
     ld = np.arange(12.0).reshape(6, 2)
     times = {4: 3.0, 8: 2.0, 16: 2.5}
-    rec = autotune.select([{"p1_sb_per_cta": s, "batch_gb": 8.0, "p2_pairs": 0} for s in times],
+    rec = autotune.select([{"p1_sb_per_cta": s, "batch_gb": 8.0} for s in times],
                           lambda c: (times[c["p1_sb_per_cta"]], ld))
     assert rec["config"]["p1_sb_per_cta"] == 8 and rec["ms"] == 2.0
     assert len(rec["trials"]) == 3
@@ -50,7 +50,7 @@ def test_tune_uses_and_refreshes_the_cache(tmp_path):
         return 10.0 / c["p1_sb_per_cta"], np.ones(3)
 
     annot = np.ones((5000, 2))
-    cands = [{"p1_sb_per_cta": s, "batch_gb": 8.0, "p2_pairs": 0} for s in (4, 16)]
+    cands = [{"p1_sb_per_cta": s, "batch_gb": 8.0} for s in (4, 16)]
     r1 = autotune.tune_windowed(FakeSession(), annot, _ws(), 50, 1000, 1, candidates=cands,
                                 cache=autotune.TuneCache(path), run=run)
     assert not r1["cached"] and r1["config"]["p1_sb_per_cta"] == 16 and len(calls) == 2
@@ -76,6 +76,6 @@ def test_cache_survives_a_corrupt_file(tmp_path):
 
 def test_default_candidates_cover_the_knobs():
     cands = autotune.default_candidates()
-    assert {c["p2_pairs"] for c in cands} == {0, 1}
+    assert {c["batch_gb"] for c in cands} == {4.0, 8.0, 16.0}
     assert len({c["p1_sb_per_cta"] for c in cands}) >= 3
     assert all(set(c) == set(autotune.DEFAULT_CONFIG) for c in cands)

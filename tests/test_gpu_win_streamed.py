@@ -90,6 +90,6 @@ def test_streamed_after_clearing_the_device_cache(small_bed):
     _lib.load().lds_clear_device_cache()
     b = windowed_ldscore(packed, n, annot, ws, 16, 50, 5, chunks=3)["ldscore"]
     c = windowed_ldscore(packed, n, annot, ws, 16, 50, 5, chunks=2,
-                         tiling={"p1_sb_per_cta": 64, "p2_pairs": 1})["ldscore"]
+                         tiling={"p1_sb_per_cta": 64})["ldscore"]
     np.testing.assert_array_equal(a, b)
     np.testing.assert_array_equal(a, c)
