@@ -710,10 +710,9 @@ void run_phase2(Context& c, Prepared& P, int64_t K, int V, int64_t j0, int64_t j
         }
         const CUtensorMap tA = make_map_2d(P.g.codes, (uint64_t)P.g.nbp, (uint64_t)P.g.M_pad,
                                            (uint64_t)P.g.nbp, 32, 128, CU_TENSOR_MAP_SWIZZLE_NONE);
-        const CUtensorMap tB =
-            make_map_2d(c.yq.p, (uint64_t)P.g.N_pad, (uint64_t)(K * nc), (uint64_t)P.g.N_pad, 128,
-                        (uint32_t)u.box_rows, CU_TENSOR_MAP_SWIZZLE_128B);
-        umma::launch_p2_umma(tA, tB, u, c.st);
+        u.yq = static_cast<const int8_t*>(c.yq.p);
+        u.yq_cols = K * nc;
+        umma::launch_p2_umma(tA, u, c.st);
         return;
     }
     P2Args a;
@@ -879,9 +878,9 @@ std::vector<double> snp_products(Context& c, const Prepared& P, int64_t j0, int6
     ck(cudaMemsetAsync(dst, 0, 4, c.st), "memset");
     const CUtensorMap tA = make_map_2d(P.g.codes, (uint64_t)P.g.nbp, (uint64_t)P.g.M_pad,
                                        (uint64_t)P.g.nbp, 32, 128, CU_TENSOR_MAP_SWIZZLE_NONE);
-    const CUtensorMap tB = make_map_2d(yq, (uint64_t)Np, (uint64_t)nc, (uint64_t)Np, 128,
-                                       (uint32_t)std::min(256, nc), CU_TENSOR_MAP_SWIZZLE_128B);
     umma::P2UArgs u;
+    u.yq = yq;
+    u.yq_cols = nc;
     u.K = 1;
     u.V = (int)V;
     u.ncolp = nc;
@@ -898,7 +897,7 @@ std::vector<double> snp_products(Context& c, const Prepared& P, int64_t j0, int6
     u.status = dst;
     u.raw_g = dg;
     u.raw_o = dO;
-    umma::launch_p2_umma(tA, tB, u, c.st);
+    umma::launch_p2_umma(tA, u, c.st);
     ck(cudaGetLastError(), "launch");
     std::vector<long long> hg((size_t)(L * V)), ho((size_t)(L * V));
     std::vector<double> hcs((size_t)V);
@@ -1738,7 +1737,6 @@ struct GwPlan {
     DevBuf y, yq, ycs, accum, mc, lscale, guards, status;
     DevBuf colsum;                   // sketch digit column sums (images with complete tiles)
     bool umma = false;
-    std::vector<CUtensorMap> tmB;    // per V-tile (sketch digit layout depends on V)
     CUtensorMap tmA;
     // One set of events per execute (up to kMaxTimed executes between reads):
     // a start event and one after each kernel of each V-tile.
@@ -1894,14 +1892,6 @@ std::unique_ptr<GwPlan> plan_create(Context& c, std::shared_ptr<Prepared> P, con
         if (P->has_complete) pl->colsum.as<int>((size_t)(K * ncolp));
         pl->tmA = make_map_2d(P->g.codes, (uint64_t)P->g.nbp, (uint64_t)P->g.M_pad,
                               (uint64_t)P->g.nbp, 32, 128, CU_TENSOR_MAP_SWIZZLE_NONE);
-        for (int V : pl->vt) {
-            const int nc = umma::ncolp_for(V);
-            const int nb = umma::p2_bins_per_cta(nc, (int)K);
-            pl->tmB.push_back(make_map_2d(yq, (uint64_t)P->g.N_pad, (uint64_t)(K * nc),
-                                          (uint64_t)P->g.N_pad, 128,
-                                          (uint32_t)std::min(256, nb * nc),
-                                          CU_TENSOR_MAP_SWIZZLE_128B));
-        }
         ck(cudaMemsetAsync(pl->status.as<unsigned>(1), 0, 4, c.st), "memset");
     } else {
         pl->yq.as<int8_t>((size_t)(pl->S * K * vpmax * P->g.N_pad));
@@ -2020,7 +2010,9 @@ void plan_enqueue_phase2(Context& c, GwPlan& pl, size_t ti, const double* y, cud
             u.snp_missing = static_cast<const uint8_t*>(P.d_missing.p);
             u.colsum = colsum;
         }
-        umma::launch_p2_umma(pl.tmA, pl.tmB[ti], u, c.st);
+        u.yq = static_cast<const int8_t*>(pl.yq.p);
+        u.yq_cols = K * nc;
+        umma::launch_p2_umma(pl.tmA, u, c.st);
         if (ev) ck(cudaEventRecord(ev[e++], c.st), "event");
         return;
     }
@@ -2499,10 +2491,9 @@ void win_enqueue(Context& c, WinPlan& pl) {
                                           colsum, c.st);
             ck(cudaEventRecordWithFlags(pl.ev[(size_t)e++], c.st, cudaEventRecordExternal), "event");
             const int nb = umma::p2_bins_per_cta(nc, (int)K);
-            const CUtensorMap tmB =
-                make_map_2d(pl.yq->p, (uint64_t)Np, (uint64_t)(b.ksup * nc), (uint64_t)Np, 128,
-                            (uint32_t)std::min(256, nb * nc), CU_TENSOR_MAP_SWIZZLE_128B);
             umma::P2UArgs u;
+            u.yq = static_cast<const int8_t*>(pl.yq->p);
+            u.yq_cols = b.ksup * nc;
             u.K = (int)K;
             u.V = V;
             u.ncolp = nc;
@@ -2533,7 +2524,7 @@ void win_enqueue(Context& c, WinPlan& pl) {
                 u.colsum = colsum;
             }
             u.tiles = static_cast<int4*>(b.tiles.p);
-            umma::launch_p2_umma(pl.tmA, tmB, u, c.st);
+            umma::launch_p2_umma(pl.tmA, u, c.st);
             ck(cudaEventRecordWithFlags(pl.ev[(size_t)e++], c.st, cudaEventRecordExternal), "event");
         }
     }
@@ -3000,7 +2991,6 @@ struct GxePair {
     DevBuf ypair;                        // N_pad x 2C FP64, rows N..N_pad zero
     int B = 0;                           // probe count the digits were made for
     DevBuf yq, ycs;
-    CUtensorMap tmB;
 };
 
 std::map<int64_t, std::unique_ptr<GxeCtx>>& gxe_table() {
@@ -3295,9 +3285,6 @@ void gxe_target_impl(Context& c, GxeCtx& g, int64_t j0, int64_t j1, GxePair& pr,
         int8_t* yq = pr.yq.as<int8_t>((size_t)(Kp * nc * Np));
         umma::launch_quantize_y4(static_cast<double*>(pr.ypair.p), N, Np, (int)Kp, (int)B, nc, yq,
                                  pr.ycs.as<double>((size_t)(Kp * B)), c.st);
-        const int nb = umma::p2_bins_per_cta(nc, (int)Kp);
-        pr.tmB = make_map_2d(yq, (uint64_t)Np, (uint64_t)(Kp * nc), (uint64_t)Np, 128,
-                             (uint32_t)std::min(256, nb * nc), CU_TENSOR_MAP_SWIZZLE_128B);
         pr.B = (int)B;
     }
     const double* dsx = dev_in(c, g.sx, sx, (size_t)(L * T), device_ptrs);
@@ -3366,7 +3353,9 @@ void gxe_target_impl(Context& c, GxeCtx& g, int64_t j0, int64_t j1, GxePair& pr,
     u.status = status;
     const CUtensorMap tmA = make_map_2d(P.g.codes, (uint64_t)P.g.nbp, (uint64_t)P.g.M_pad,
                                         (uint64_t)P.g.nbp, 32, 128, CU_TENSOR_MAP_SWIZZLE_NONE);
-    umma::launch_p2_umma(tmA, pr.tmB, u, c.st);
+    u.yq = static_cast<const int8_t*>(pr.yq.p);
+    u.yq_cols = Kp * nc;
+    umma::launch_p2_umma(tmA, u, c.st);
     }
     const size_t nacc = (size_t)(g.E * total * K);
     double* A[4];
@@ -4418,7 +4407,8 @@ LDS_API int lds_debug_xt_products_umma(const uint8_t* bed_rows, int64_t bed_row_
         const int64_t Np = P->g.N_pad;
         const int nc = umma::ncolp_for((int)V);
         std::vector<int8_t> yq((size_t)(nc * Np), 0);
-        for (int64_t q = 0; q < 4 * V; ++q) std::memcpy(&yq[(size_t)(q * Np)], y + q * n, (size_t)n);
+        for (int64_t q = 0; q < 4 * V; ++q)
+            for (int64_t i = 0; i < n; ++i) yq[(size_t)umma::digit_offset(q, i, nc)] = y[q * n + i];
         DevBuf dyq, rg, ro, st;
         int8_t* d_yq = dyq.as<int8_t>(yq.size());
         h2d(d_yq, yq.data(), yq.size(), c.st);
@@ -4428,9 +4418,9 @@ LDS_API int lds_debug_xt_products_umma(const uint8_t* bed_rows, int64_t bed_row_
         ck(cudaMemsetAsync(dst, 0, 4, c.st), "memset");
         const CUtensorMap tA = make_map_2d(P->g.codes, (uint64_t)P->g.nbp, (uint64_t)P->g.M_pad,
                                            (uint64_t)P->g.nbp, 32, 128, CU_TENSOR_MAP_SWIZZLE_NONE);
-        const CUtensorMap tB = make_map_2d(d_yq, (uint64_t)Np, (uint64_t)nc, (uint64_t)Np, 128,
-                                           (uint32_t)std::min(256, nc), CU_TENSOR_MAP_SWIZZLE_128B);
         umma::P2UArgs u;
+        u.yq = d_yq;
+        u.yq_cols = nc;
         u.K = 1;
         u.V = (int)V;
         u.ncolp = nc;
@@ -4446,7 +4436,7 @@ LDS_API int lds_debug_xt_products_umma(const uint8_t* bed_rows, int64_t bed_row_
         u.status = dst;
         u.raw_g = dg;
         u.raw_o = dO;
-        umma::launch_p2_umma(tA, tB, u, c.st);
+        umma::launch_p2_umma(tA, u, c.st);
         ck(cudaGetLastError(), "launch");
         unsigned stv = 0;
         d2h(&stv, dst, 1, c.st);

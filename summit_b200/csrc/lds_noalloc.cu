@@ -162,11 +162,9 @@ static int run(const uint8_t* d_codes, int64_t row_bytes, int64_t n, int64_t row
         g_msg = "cudaMemsetAsync of the status words failed";
         return LDS_ERR_CUDA;
     }
-    CUtensorMap tA, tB;
+    CUtensorMap tA;
     if (!map2d(&tA, d_codes, (uint64_t)row_bytes, (uint64_t)rows_total, (uint64_t)row_bytes, 32, 128,
-               CU_TENSOR_MAP_SWIZZLE_NONE) ||
-        !map2d(&tB, yq, (uint64_t)N_pad, (uint64_t)K * ncolp, (uint64_t)N_pad, 128,
-               (uint32_t)(ncolp < 256 ? ncolp : 256), CU_TENSOR_MAP_SWIZZLE_128B)) {
+               CU_TENSOR_MAP_SWIZZLE_NONE)) {
         g_msg = "cuTensorMapEncodeTiled failed";
         return LDS_ERR_CUDA;
     }
@@ -192,7 +190,9 @@ static int run(const uint8_t* d_codes, int64_t row_bytes, int64_t n, int64_t row
     u.extreme_warn = phase2_extreme_warn();
     u.drop_extreme = phase2_drop_extreme();
     u.status = status;
-    umma::launch_p2_umma(tA, tB, u, st);
+    u.yq = yq;
+    u.yq_cols = (int64_t)K * ncolp;
+    umma::launch_p2_umma(tA, u, st);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         g_msg = std::string("launch failed: ") + cudaGetErrorString(e);

@@ -15,7 +15,10 @@ namespace umma {
 // soon as the phase completes), so a wait gives up after at most about
 // kWaitLimit * kSuspendNs = 6.7 s.
 constexpr long long kWaitLimit = 1LL << 25;
-constexpr uint32_t kSuspendNs = 200;
+#ifndef LDS_SUSPEND_NS
+#define LDS_SUSPEND_NS 200
+#endif
+constexpr uint32_t kSuspendNs = LDS_SUSPEND_NS;
 
 // The iteration limit in force: one copy per translation unit and device,
 // kWaitLimit unless lds_set_wait_limit() changed it.  Each file that includes
@@ -65,6 +68,17 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
         "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes "
         "[%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
         "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// Bulk copy of `bytes` contiguous bytes (16-byte aligned, a multiple of 16)
+// into this CTA's shared memory, completing on `bar`.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes,
+                                          uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_u32(bar))
         : "memory");
 }
 

@@ -2,9 +2,11 @@
 //
 // Work[j, c] = x_j^T Y[:, c] for a tile of 128 SNPs and one annotation bin,
 // with the LD-score epilogue, as in p2_kernel (lds_kernels.cu) but with:
-//   * TMA tile copies (cp.async.bulk.tensor into the CTA's own shared memory) bringing the packed 2-bit
-//     genotype tile (128 SNPs x 128 samples = 4 KB) and the sketch digit tile
-//     (bin columns x 128 samples, SWIZZLE_128B) into a 3-stage smem ring;
+//   * a TMA tile copy (cp.async.bulk.tensor into the CTA's own shared memory)
+//     bringing the packed 2-bit genotype tile (128 SNPs x 128 samples = 4 KB),
+//     and one bulk copy (cp.async.bulk) of the sketch digit tile (bin columns x
+//     128 samples), stored contiguous and pre-swizzled (digit_offset), into
+//     shared-memory rings;
 //   * 4 decoder warps expanding packed codes into the G (value) and O
 //     (observed) int8 operand tiles in the canonical K-major SWIZZLE_128B
 //     layout the UMMA descriptors expect;
@@ -72,8 +74,7 @@ struct Layout {
 };
 
 __global__ void __launch_bounds__(kThreads, 1)
-    p2_umma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                   P2UArgs a) {
+    p2_umma_kernel(const __grid_constant__ CUtensorMap tmA, P2UArgs a) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -112,10 +113,10 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (tid == 0) {
         for (int s = 0; s < kPkStages; ++s) {
             mbar_init(&pk_full[s], 1);
-            mbar_init(&pk_empty[s], 128);
+            mbar_init(&pk_empty[s], 4);   // one arrival per decoder warp
         }
         for (int s = 0; s < kAStages; ++s) {
-            mbar_init(&a_full[s], 128);
+            mbar_init(&a_full[s], 4);     // one arrival per decoder warp
             mbar_init(&a_empty[s], 1);
         }
         for (int s = 0; s < kBStages; ++s) {
@@ -123,7 +124,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             mbar_init(&b_empty[s], 1);
         }
         mbar_init(acc_full, 1);
-        mbar_init(acc_empty, 128);
+        mbar_init(acc_empty, 4);          // one arrival per epilogue warp
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -180,8 +181,14 @@ __global__ void __launch_bounds__(kThreads, 1)
                     !mbar_wait(&b_empty[s], ((uint32_t)(it / kBStages) & 1u) ^ 1u)) { fail(2); break; }
                 if (*abort_flag) break;
                 const int g = it / a.nkt, kt = it % a.nkt;
-                mbar_expect_tx(&b_full[s], (uint32_t)(a.box_rows * kBK));
-                tma_load_2d(smem + lay.b_off(s), &tmB, kt * kBK, kb * a.ncolp + g * 256, &b_full[s]);
+                // The group's columns that exist (this CTA's bins); MMA columns
+                // past them read stale rows whose results no output uses.
+                const int live = min(min(256, cols - g * 256), nbk * a.ncolp - g * 256);
+                const uint32_t bytes = (uint32_t)live * (uint32_t)kBK;
+                mbar_expect_tx(&b_full[s], bytes);
+                bulk_load(smem + lay.b_off(s),
+                          a.yq + ((int64_t)kt * a.yq_cols + (int64_t)kb * a.ncolp + g * 256) * kBK,
+                          bytes, &b_full[s]);
             }
             for (int j = max(0, it - kBStages); j < it; ++j)
                 mbar_wait(&b_full[j % kBStages], (uint32_t)(j / kBStages) & 1u);
@@ -261,23 +268,39 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (int kt = 0; kt < a.nkt; ++kt, ++it) {
                 if (it % kDecSets != dset) continue;
                 const int sp = it % kPkStages, sa = it % kAStages;
-                if (!mbar_wait(&pk_full[sp], (uint32_t)(it / kPkStages) & 1u)) { fail(5); break; }
-                if (*abort_flag) break;
+                // Warp-uniform waits and one arrival per warp (after __syncwarp,
+                // which orders the warp's shared-memory accesses before it):
+                // 4 arrivals per stage instead of 128.
+                if (!__all_sync(0xffffffffu,
+                                mbar_wait(&pk_full[sp], (uint32_t)(it / kPkStages) & 1u))) {
+                    fail(5);
+                    break;
+                }
+                if (__any_sync(0xffffffffu, *abort_flag != 0)) break;
                 const uint4* pk = reinterpret_cast<const uint4*>(smem + lay.pk_off(sp) + r * 32);
                 const uint4 p0 = pk[0], p1 = pk[1];
-                mbar_arrive(&pk_empty[sp]);
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&pk_empty[sp]);
                 if (it >= kAStages &&
-                    !mbar_wait(&a_empty[sa], ((uint32_t)(it / kAStages) & 1u) ^ 1u)) { fail(6); break; }
+                    !__all_sync(0xffffffffu, mbar_wait(&a_empty[sa],
+                                                       ((uint32_t)(it / kAStages) & 1u) ^ 1u))) {
+                    fail(6);
+                    break;
+                }
                 uint8_t* gRow = smem + lay.a_off(sa) + (r >> 3) * 1024 + (r & 7) * 128;
                 if (complete) decode_row_sw128_g(p0, p1, gRow, r);
                 else decode_row_sw128(p0, p1, gRow, gRow + kATile, r);
                 fence_async_smem();
-                mbar_arrive(&a_full[sa]);
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&a_full[sa]);
             }
-            if (*abort_flag) break;
+            if (__any_sync(0xffffffffu, *abort_flag != 0)) break;
             if (dset != 0) continue;
             // Epilogue of column group g.
-            if (!mbar_wait(acc_full, (uint32_t)g & 1u)) { fail(7); break; }
+            if (!__all_sync(0xffffffffu, mbar_wait(acc_full, (uint32_t)g & 1u))) {
+                fail(7);
+                break;
+            }
             tc_fence_after();
             const int ncols = min(256, cols - g * 256);
             const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16);
@@ -327,7 +350,8 @@ __global__ void __launch_bounds__(kThreads, 1)
                 }
             }
             tc_fence_before();
-            mbar_arrive(acc_empty);
+            __syncwarp();
+            if (lane == 0) mbar_arrive(acc_empty);
         }
         if (dset == 0) flush();
     }
@@ -378,7 +402,7 @@ __global__ void quantize_y4_kernel(const double* __restrict__ Y, int64_t N, int6
         e = ilogb(amax) + 1;
         if (ldexp(amax, 7 - e) > 127.0) e += 1;
     }
-    int8_t* base = Yq + ((int64_t)k * ncolp + 4 * v) * N_pad;
+    const int64_t col0 = (int64_t)k * ncolp + 4 * v, cols = (int64_t)K * ncolp;
     int dsum[4] = {0, 0, 0, 0};
     for (int64_t i = threadIdx.x; i < N_pad; i += blockDim.x) {
         int8_t d[4] = {0, 0, 0, 0};
@@ -395,7 +419,7 @@ __global__ void quantize_y4_kernel(const double* __restrict__ Y, int64_t N, int6
             }
         }
         for (int s = 0; s < 4; ++s) {
-            base[(int64_t)s * N_pad + i] = d[s];
+            Yq[digit_offset(col0 + s, i, cols)] = d[s];
             dsum[s] += d[s];
         }
     }
@@ -414,14 +438,15 @@ __global__ void quantize_y4_kernel(const double* __restrict__ Y, int64_t N, int6
     }
 }
 
-// colsum[c] = sum of digit column c over its N_pad samples (one CTA per column).
-__global__ void digit_colsum_kernel(const int8_t* __restrict__ Yq, int64_t N_pad,
+// colsum[c] = sum of digit column c over its N_pad samples (one CTA per column;
+// a column's 128-byte rows, one per sample chunk, in any swizzled order).
+__global__ void digit_colsum_kernel(const int8_t* __restrict__ Yq, int64_t cols, int64_t N_pad,
                                     int* __restrict__ colsum) {
     __shared__ int part[32];
-    const int8_t* col = Yq + (int64_t)blockIdx.x * N_pad;
+    const int8_t* col = Yq + (int64_t)blockIdx.x * 128;
     int s = 0;
-    for (int64_t i = (int64_t)threadIdx.x * 16; i < N_pad; i += (int64_t)blockDim.x * 16) {
-        const int4 v = *reinterpret_cast<const int4*>(col + i);
+    for (int64_t u = threadIdx.x; u < (N_pad >> 7) * 8; u += blockDim.x) {
+        const int4 v = *reinterpret_cast<const int4*>(col + (u >> 3) * cols * 128 + (u & 7) * 16);
         const int w[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
         for (int q = 0; q < 4; ++q)
@@ -443,8 +468,8 @@ __global__ void zero_pad_cols_kernel(int8_t* Yq, int64_t N_pad, int K, int V, in
     const int k = blockIdx.y;
     const int c = 4 * V + blockIdx.x;
     if (c >= ncolp) return;
-    int8_t* base = Yq + ((int64_t)k * ncolp + c) * N_pad;
-    for (int64_t i = threadIdx.x; i < N_pad; i += blockDim.x) base[i] = 0;
+    const int64_t col = (int64_t)k * ncolp + c, cols = (int64_t)K * ncolp;
+    for (int64_t i = threadIdx.x; i < N_pad; i += blockDim.x) Yq[digit_offset(col, i, cols)] = 0;
     if (colsum && threadIdx.x == 0) colsum[(int64_t)k * ncolp + c] = 0;
 }
 
@@ -463,7 +488,7 @@ void launch_quantize_y4(const double* Y, int64_t N, int64_t N_pad, int K, int V,
 void launch_digit_colsum(const int8_t* Yq, int64_t ncols, int64_t N_pad, int* colsum,
                          cudaStream_t st) {
     if (ncols <= 0) return;
-    digit_colsum_kernel<<<(unsigned)ncols, 256, 0, st>>>(Yq, N_pad, colsum);
+    digit_colsum_kernel<<<(unsigned)ncols, 256, 0, st>>>(Yq, ncols, N_pad, colsum);
     count_launch();
 }
 
@@ -497,8 +522,7 @@ void prepare_p2_umma() {
                          (int)p2_umma_smem_bytes(256));
 }
 
-void launch_p2_umma(const CUtensorMap& tmA, const CUtensorMap& tmB, const P2UArgs& a,
-                    cudaStream_t st) {
+void launch_p2_umma(const CUtensorMap& tmA, const P2UArgs& a, cudaStream_t st) {
     const int64_t rows = a.j1 - a.j0;
     if ((!a.tiles && rows <= 0) || a.K <= 0) return;
     const size_t smem = p2_umma_smem_bytes(a.box_rows);
@@ -509,7 +533,7 @@ void launch_p2_umma(const CUtensorMap& tmA, const CUtensorMap& tmB, const P2UArg
     // With a tile table, j0 is unused and j1 - j0 carries the number of tiles.
     const int nb = a.bins_per_cta > 0 ? a.bins_per_cta : 1;
     dim3 grid((unsigned)(a.tiles ? rows : (rows + kBM - 1) / kBM), (unsigned)((a.K + nb - 1) / nb));
-    p2_umma_kernel<<<grid, kThreads, smem, st>>>(tmA, tmB, a);
+    p2_umma_kernel<<<grid, kThreads, smem, st>>>(tmA, a);
     count_launch();
 }
 

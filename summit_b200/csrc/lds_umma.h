@@ -7,8 +7,21 @@
 namespace lds {
 namespace umma {
 
-// Arguments of p2_umma_kernel.  The sketch digits live in Yq with layout
-// [K bins][ncolp columns][N_pad samples], column 4 v + t = digit t of probe v.
+// Sketch digits in phase 2's operand layout.  Column 4 v + t of bin k is digit
+// t of probe v (global column k * ncolp + 4 v + t of `cols` columns).  The
+// samples come in chunks of 128 (one phase-2 K-step): chunk kt holds every
+// column's 128-byte row, contiguously ([kt][cols][128 bytes]), and each
+// 8-row group (1 KB) is pre-swizzled as the SWIZZLE_128B K-major UMMA atom
+// expects (16-byte chunk index XOR row & 7).  A K-step's tile of any run of
+// columns starting on a multiple of 8 is then one contiguous block that a
+// single bulk copy moves into shared memory ready for the MMA.
+__host__ __device__ inline int64_t digit_offset(int64_t col, int64_t i, int64_t cols) {
+    const int s = (int)(i & 127);
+    return ((i >> 7) * cols + col) * 128 + ((((s >> 4) ^ (int)(col & 7)) << 4) | (s & 15));
+}
+
+// Arguments of p2_umma_kernel.  The sketch digits are yq (digit_offset layout
+// with yq_cols columns): per bin, ncolp columns.
 struct P2UArgs {
     int K = 0, V = 0, ncolp = 0, ngroups = 1, box_rows = 0, nkt = 0;
     int64_t M = 0, j0 = 0, j1 = 0, out_row0 = 0;
@@ -22,6 +35,8 @@ struct P2UArgs {
     double extreme_warn = 1e10;
     int drop_extreme = 1;
     unsigned int* status = nullptr;      // 0 = ok; nonzero = pipeline wait timed out
+    const int8_t* yq = nullptr;          // sketch digits (digit_offset layout)
+    int64_t yq_cols = 0;                 // columns of yq (super-bins x ncolp)
     // Verification mode: write the exact recombined products G^T y and O^T y
     // per (SNP, probe) to raw_g / raw_o ((j - out_row0) * V + v), no epilogue.
     long long* raw_g = nullptr;
@@ -68,8 +83,9 @@ struct P1UArgs {
     unsigned int* status = nullptr;
     int sb_per_cta = 1;                 // super-bins processed by one CTA (pipeline continues)
     // Digit output (windowed estimates): when yq is set the epilogue writes the
-    // sketch's 4 int8 digits in phase 2's layout (column k*ncolp + 4v + t)
-    // using the a-priori exponents in ycolscale (K*V) instead of FP64 Y.
+    // sketch's 4 int8 digits in phase 2's layout (digit_offset, column
+    // k*ncolp + 4v + t of K*ncolp) using the a-priori exponents in ycolscale
+    // (K*V) instead of FP64 Y.
     int8_t* yq = nullptr;
     const double* ycolscale = nullptr;
     const int* yshift = nullptr;        // K*V digit shifts eW - eY (from the weight kernel)
@@ -105,8 +121,7 @@ size_t p2_umma_smem_bytes(int box_rows);
 // Set the kernels' shared-memory attributes ahead of any stream capture.
 void prepare_p2_umma();
 void prepare_p1_umma();
-void launch_p2_umma(const CUtensorMap& tmA, const CUtensorMap& tmB, const P2UArgs& a,
-                    cudaStream_t st);
+void launch_p2_umma(const CUtensorMap& tmA, const P2UArgs& a, cudaStream_t st);
 
 }  // namespace umma
 }  // namespace lds

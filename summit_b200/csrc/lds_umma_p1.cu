@@ -67,12 +67,12 @@ __global__ void __launch_bounds__(p1::kThreads, 1)
     if (tid == 0) {
         for (int s = 0; s < kStages; ++s) {
             mbar_init(&full_w[s], 1);
-            mbar_init(&full_dec[s], 128);
+            mbar_init(&full_dec[s], 4);            // one arrival per decoder warp
             mbar_init(&empty[s], 1);
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(&acc_full[b], 1);
-            mbar_init(&acc_empty[b], kEpiThreads);
+            mbar_init(&acc_empty[b], kEpiThreads / 32);  // one arrival per epilogue warp
         }
         mbar_init(mma_done, 1);
         *abort_flag = 0;
@@ -198,9 +198,9 @@ __global__ void __launch_bounds__(p1::kThreads, 1)
         };
         for (int d = 0; d < kRing - 1; ++d) prefetch_one();
         int it = 0;
-        for (int k = kb0; k < kb1 && !*abort_flag; ++k) {
+        for (int k = kb0; k < kb1 && !__any_sync(0xffffffffu, *abort_flag != 0); ++k) {
             const int nkt = nkt_of(k);
-            for (int g = 0; g < a.ngroups && nkt > 0 && !*abort_flag; ++g) {
+            for (int g = 0; g < a.ngroups && nkt > 0 && !__any_sync(0xffffffffu, *abort_flag != 0); ++g) {
                 for (int kt = 0; kt < nkt; ++kt, ++it) {
                     const int s = it % kStages;
                     const uint32_t ph = (uint32_t)(it / kStages) & 1u;
@@ -209,13 +209,17 @@ __global__ void __launch_bounds__(p1::kThreads, 1)
                     const uint4* src =
                         reinterpret_cast<const uint4*>(ring + (it % kRing) * kRingSlot + t * 32);
                     const uint4 c0 = src[0], c1 = src[1];
-                    if (it >= kStages && !mbar_wait(&empty[s], ph ^ 1u)) { fail(14); break; }
-                    if (*abort_flag) break;
+                    if (it >= kStages && !__all_sync(0xffffffffu, mbar_wait(&empty[s], ph ^ 1u))) {
+                        fail(14);
+                        break;
+                    }
+                    if (__any_sync(0xffffffffu, *abort_flag != 0)) break;
                     uint8_t* st = smem + s * kStageBytes;
                     uint8_t* gRow = st + (t >> 3) * 1024 + (t & 7) * 128;
                     decode_row_sw128(c0, c1, gRow, gRow + kATile, t);
                     fence_async_smem();
-                    mbar_arrive(&full_dec[s]);
+                    __syncwarp();  // orders the warp's operand stores before its one arrival
+                    if (lane == 0) mbar_arrive(&full_dec[s]);
                 }
             }
         }
@@ -227,23 +231,26 @@ __global__ void __launch_bounds__(p1::kThreads, 1)
         const int h = (warp - 6) >> 2;           // which quarter of the 16-column chunks
         const int64_t i = i0 + q * 32 + lane;    // sample row of this thread's accumulator lane
         int au = 0;
-        for (int k = kb0; k < kb1 && !*abort_flag; ++k) {
+        for (int k = kb0; k < kb1 && !__any_sync(0xffffffffu, *abort_flag != 0); ++k) {
             const int nkt = nkt_of(k);
+            // This sample tile's block of super-bin k in phase 2's digit layout
+            // (digit_offset): ncolp rows of 128 bytes.
+            int8_t* const yblk =
+                a.yq ? a.yq + ((int64_t)blockIdx.x * a.K * a.ncolp + (int64_t)k * a.ncolp) * 128
+                     : nullptr;
             if (a.yq) {
                 // Digit padding rows 4V..ncolp of this tile read as zero in phase 2.
-                for (int idx = e; idx < (a.ncolp - 4 * a.V) * 8; idx += kEpiThreads) {
-                    const int c = 4 * a.V + (idx >> 3);
-                    *reinterpret_cast<uint4*>(a.yq + ((int64_t)k * a.ncolp + c) * a.N_pad + i0 +
-                                              (idx & 7) * 16) = make_uint4(0, 0, 0, 0);
-                }
+                for (int idx = e; idx < (a.ncolp - 4 * a.V) * 8; idx += kEpiThreads)
+                    *reinterpret_cast<uint4*>(yblk + (4 * a.V + (idx >> 3)) * 128 + (idx & 7) * 16) =
+                        make_uint4(0, 0, 0, 0);
             }
             if (nkt == 0) {
                 // Bin without members: its sketch columns are zero (the
                 // reference's untouched-bin zeroing, gw_ldscore.py:2017-2019).
                 if (a.yq) {
                     for (int idx = e; idx < 4 * a.V * 8; idx += kEpiThreads)
-                        *reinterpret_cast<uint4*>(a.yq + ((int64_t)k * a.ncolp + (idx >> 3)) * a.N_pad +
-                                                  i0 + (idx & 7) * 16) = make_uint4(0, 0, 0, 0);
+                        *reinterpret_cast<uint4*>(yblk + (idx >> 3) * 128 + (idx & 7) * 16) =
+                            make_uint4(0, 0, 0, 0);
                 } else {
                     for (int idx = e; idx < a.V * 64; idx += kEpiThreads)
                         *reinterpret_cast<uint4*>(a.Y + ((int64_t)k * a.V + (idx >> 6)) * a.N_pad +
@@ -251,7 +258,7 @@ __global__ void __launch_bounds__(p1::kThreads, 1)
                 }
                 continue;
             }
-            for (int g = 0; g < a.ngroups && !*abort_flag; ++g, ++au) {
+            for (int g = 0; g < a.ngroups && !__any_sync(0xffffffffu, *abort_flag != 0); ++g, ++au) {
                 const int b = au & 1, u = au >> 1;
                 // This group's 64 per-probe shifts (or scales), two per lane, loaded
                 // before the accumulator wait so the loads overlap the MMAs; the
@@ -269,10 +276,10 @@ __global__ void __launch_bounds__(p1::kThreads, 1)
                         if (vb < a.V) scB = a.colscale[o + vb];
                     }
                 }
-                // The warp's 32 samples of this super-bin's digit rows start here.
-                int8_t* const ywarp =
-                    a.yq ? a.yq + (int64_t)k * a.ncolp * a.N_pad + i0 + q * 32 : nullptr;
-                if (!mbar_wait(&acc_full[b], (uint32_t)u & 1u)) { fail(15); break; }
+                if (!__all_sync(0xffffffffu, mbar_wait(&acc_full[b], (uint32_t)u & 1u))) {
+                    fail(15);
+                    break;
+                }
                 tc_fence_after();
                 const int ncols = min(kAccCols, a.ncolp - g * 256);
                 const uint32_t tbase = tmem + (uint32_t)(b * kAccCols) + ((uint32_t)(q * 32) << 16);
@@ -286,11 +293,15 @@ __global__ void __launch_bounds__(p1::kThreads, 1)
                     // byte transpose within each lane quad turns the lanes' digit
                     // words (4 digits of one sample) into words of one digit for 4
                     // consecutive samples, stored straight to global memory (a warp
-                    // writes 4 digit rows x 32 samples per probe).
+                    // writes 4 digit rows x 32 samples per probe).  Lane 4a + t
+                    // stores digit row 4v + t, samples s = 32 q + 4a of the block:
+                    // 16-byte chunk s / 16 = 2q + a / 4, swizzled with the row's
+                    // low three bits, (4 v + t) & 7 = 4 (v & 1) + t.
                     const int qd = lane & 3;
                     const uint32_t selA = qd < 2 ? 0x5410u : 0x3276u;
                     const uint32_t selB = (qd & 1) ? 0x3715u : 0x6240u;
-                    int8_t* const ylane = ywarp + 4 * (lane >> 2) + (int64_t)qd * a.N_pad;
+                    const int chunk = 2 * q + (lane >> 4);
+                    int8_t* const ylane = yblk + qd * 128 + 4 * ((lane >> 2) & 3);
                     for (int c0 = 32 * h; c0 < ncols; c0 += 128) {
                         int rr[32];
                         tmem_ld32(tbase + (uint32_t)c0, rr);
@@ -327,9 +338,11 @@ __global__ void __launch_bounds__(p1::kThreads, 1)
                             // with digit t of samples 4a .. 4a + 3.
                             w = __byte_perm(w, __shfl_xor_sync(0xffffffffu, w, 2), selA);
                             w = __byte_perm(w, __shfl_xor_sync(0xffffffffu, w, 1), selB);
-                            if (p < nv)
+                            if (p < nv) {
+                                const int v = g * 64 + vl;
                                 *reinterpret_cast<uint32_t*>(
-                                    ylane + (int64_t)(4 * (g * 64 + vl)) * a.N_pad) = w;
+                                    ylane + v * 512 + ((chunk ^ (4 * (v & 1) + qd)) << 4)) = w;
+                            }
                         }
                     }
                 } else {
@@ -351,7 +364,8 @@ __global__ void __launch_bounds__(p1::kThreads, 1)
                 }
                 }
                 tc_fence_before();
-                mbar_arrive(&acc_empty[b]);
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&acc_empty[b]);
             }
         }
     }
