@@ -724,6 +724,17 @@ int lds_block_boundaries(int64_t M, int B, const double* mass, int min_snps, int
                          int64_t* ends);
 int lds_sym_solve(const double* systems, int64_t nsys, int K, double rtol, int require_full_rank,
                   double* x, int* rank, double* eigenvalues, int device_ptrs);
+/* lds_sym_solve_diag: the same solve with the diagnostics of
+ * solve_context_normal_equations / _rank_diagnostics (context/fit.py:435-513):
+ * per system x (K), rank, ascending eigenvalues (K), eigenvectors (K x K
+ * row-major, column p for the p-th eigenvalue), residual S x - b (K; S the
+ * symmetrized matrix), symmetry error max|A - A^T|, the retention tolerance,
+ * and status bits (1 asymmetry above 2e-10 scale, 4 non-finite input) that
+ * the caller turns into its errors.  Rank deficiency is reported, not an
+ * error.  Host pointers (any output may be NULL); K <= 96. */
+int lds_sym_solve_diag(const double* systems, int64_t nsys, int K, double rtol, double* x,
+                       int* rank, double* eigenvalues, double* eigenvectors, double* residual,
+                       double* symmetry_error, double* tolerance, int* status);
 int lds_jackknife_normal_equations(const double* terms, int64_t M, int K, const int64_t* starts,
                                    const int64_t* ends, int64_t B, double rtol, double* theta,
                                    double* replicates, double* se, double* cov, int device_ptrs);

@@ -97,6 +97,7 @@ SIGNATURES: dict[str, tuple] = {
     "lds_philox_rademacher": (_int, [_p, _i64, _i64, _p, _int]),
     "lds_block_boundaries": (_int, [_i64, _int, _p, _int, _p, _p]),
     "lds_sym_solve": (_int, [_p, _i64, _int, _dbl, _int, _p, _p, _p, _int]),
+    "lds_sym_solve_diag": (_int, [_p, _i64, _int, _dbl, _p, _p, _p, _p, _p, _p, _p, _p]),
     "lds_jackknife_normal_equations": (_int, [_p, _i64, _int, _p, _p, _i64, _dbl, _p, _p, _p, _p,
                                               _int]),
     "lds_gw_plan_create": (_int, [_i64, _p, _i64, _int, _int, _int, _u64, _int, _dbl, _int, _int,

@@ -5290,6 +5290,45 @@ LDS_API int lds_sym_solve(const double* systems, int64_t nsys, int K, double rto
     });
 }
 
+LDS_API int lds_sym_solve_diag(const double* systems, int64_t nsys, int K, double rtol,
+                               double* x, int* rank, double* eigenvalues, double* eigenvectors,
+                               double* residual, double* symmetry_error, double* tolerance,
+                               int* status) {
+    return guarded([&] {
+        if (!systems || nsys <= 0) fail(LDS_ERR_ARG, "no systems");
+        if (K <= 0 || K > sym_solve_max_k())
+            fail(LDS_ERR_ARG, "system size must be in [1, %d]", sym_solve_max_k());
+        if (!std::isfinite(rtol) || rtol <= 0.0) fail(LDS_ERR_ARG, "rtol must be finite and positive.");
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        ensure_device(c);
+        const size_t n = (size_t)nsys, k = (size_t)K;
+        DevBuf ds, dx, dr, de, dv, dres, da, dt, dst;
+        double* d = ds.as<double>(n * (k * k + k));
+        h2d(d, systems, n * (k * k + k), c.st);
+        SymSolveExtras ex;
+        ex.evec = dv.as<double>(n * k * k);
+        ex.resid = dres.as<double>(n * k);
+        ex.asym = da.as<double>(n);
+        ex.tol = dt.as<double>(n);
+        double* xo = dx.as<double>(n * k);
+        int* ro = dr.as<int>(n);
+        double* eo = de.as<double>(n * k);
+        int* so = dst.as<int>(n);
+        launch_sym_solve(d, nsys, K, rtol, 0, xo, ro, eo, so, c.st, ex);
+        ck(cudaGetLastError(), "launch");
+        if (x) d2h(x, xo, n * k, c.st);
+        if (rank) d2h(rank, ro, n, c.st);
+        if (eigenvalues) d2h(eigenvalues, eo, n * k, c.st);
+        if (eigenvectors) d2h(eigenvectors, ex.evec, n * k * k, c.st);
+        if (residual) d2h(residual, ex.resid, n * k, c.st);
+        if (symmetry_error) d2h(symmetry_error, ex.asym, n, c.st);
+        if (tolerance) d2h(tolerance, ex.tol, n, c.st);
+        if (status) d2h(status, so, n, c.st);
+        ck(cudaStreamSynchronize(c.st), "solve");
+    });
+}
+
 LDS_API int lds_jackknife_normal_equations(const double* terms, int64_t M, int K,
                                            const int64_t* starts, const int64_t* ends, int64_t B,
                                            double rtol, double* theta, double* replicates,

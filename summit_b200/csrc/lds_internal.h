@@ -173,8 +173,18 @@ int sym_solve_max_k();
 void launch_block_sums(const double* X, int64_t P, const int64_t* starts, const int64_t* ends,
                        int64_t B, double* out, cudaStream_t st);
 void launch_delete_one(const double* blocks, int64_t B, int64_t P, double* sys, cudaStream_t st);
+// Optional per-system outputs of the symmetric solve (device pointers, each
+// may be null): eigenvectors (K x K, column p for the p-th smallest
+// eigenvalue), residual S x - b (K), symmetry error and tolerance (1 each).
+struct SymSolveExtras {
+    double* evec = nullptr;
+    double* resid = nullptr;
+    double* asym = nullptr;
+    double* tol = nullptr;
+};
 void launch_sym_solve(const double* sys, int64_t nsys, int K, double rtol, int require_full_rank,
-                      double* x, int* rank, double* eig, int* status, cudaStream_t st);
+                      double* x, int* rank, double* eig, int* status, cudaStream_t st,
+                      const SymSolveExtras& ex = SymSolveExtras());
 void launch_jackknife_stats(const double* reps, int64_t R, int K, double* mean, double* se,
                             double* cov, cudaStream_t st);
 

@@ -44,16 +44,20 @@ __global__ void delete_one_kernel(const double* __restrict__ blocks, int64_t B, 
 // One CTA per system (row-major K x K matrix then K rhs, stride K*K + K).
 // status[s] bits: 1 asymmetric input, 2 rank deficient under require_full_rank,
 // 4 non-finite input.
+// Optional outputs (ex, any pointer may be null): eigenvectors (K x K per
+// system, column p the eigenvector of the p-th smallest eigenvalue), the solve
+// residual S x - b, the symmetry error max|A - A^T| and the retention
+// tolerance.
 __global__ void __launch_bounds__(kSolveThreads)
     sym_solve_kernel(const double* __restrict__ sys, int K, double rtol, int require_full_rank,
                      double* __restrict__ x, int* __restrict__ rank_out,
-                     double* __restrict__ eig_out, int* __restrict__ status) {
+                     double* __restrict__ eig_out, int* __restrict__ status, SymSolveExtras ex) {
     extern __shared__ double sm[];
     const int ld = K + 1;
     auto A = [&](int i, int j) -> double& { return sm[i * ld + j]; };
     auto S = [&](int i, int j) -> double& { return sm[K * ld + i * ld + j]; };
     auto V = [&](int i, int j) -> double& { return sm[2 * K * ld + i * ld + j]; };
-    __shared__ double bvec[kMaxK], lam[kMaxK], red[kSolveThreads];
+    __shared__ double bvec[kMaxK], lam[kMaxK], xs[kMaxK], red[kSolveThreads];
     __shared__ double rot[2];
     __shared__ int flag;
     const int s = blockIdx.x, t = threadIdx.x;
@@ -90,6 +94,7 @@ __global__ void __launch_bounds__(kSolveThreads)
         __syncthreads();
     }
     if (t == 0 && red[0] > 2.0e-10 * scale) atomicOr(&flag, 1);
+    if (t == 0 && ex.asym) ex.asym[s] = red[0];
     if (t < K)
         for (int j = 0; j < K; ++j) {
             S(t, j) = 0.5 * (A(t, j) + A(j, t));
@@ -166,6 +171,7 @@ __global__ void __launch_bounds__(kSolveThreads)
     const double leading = red[0];
     const double abs_tol = 100.0 * 2.220446049250313e-16 * scale;
     const double tol = fmax(abs_tol, rtol * leading);
+    if (t == 0 && ex.tol) ex.tol[s] = tol;
     __syncthreads();
     // retained Rayleigh quotients and the solution (fit.py:496-506)
     // proj[t] = v_t^T b / (v_t^T S v_t) for retained t
@@ -188,8 +194,14 @@ __global__ void __launch_bounds__(kSolveThreads)
         double xi = 0.0;
         for (int r = 0; r < K; ++r) xi += V(t, r) * red[r];
         x[(int64_t)s * K + t] = xi;
+        xs[t] = xi;
     }
     __syncthreads();
+    if (ex.resid && t < K) {
+        double r = 0.0;
+        for (int j = 0; j < K; ++j) r += S(t, j) * xs[j];
+        ex.resid[(int64_t)s * K + t] = r - bvec[t];
+    }
     red[t] = keep;
     __syncthreads();
     for (int o = kSolveThreads / 2; o; o >>= 1) {
@@ -209,6 +221,8 @@ __global__ void __launch_bounds__(kSolveThreads)
         for (int j = 0; j < K; ++j)
             if (lam[j] < lam[t] || (lam[j] == lam[t] && j < t)) ++pos;
         eig_out[(int64_t)s * K + pos] = lam[t];
+        if (ex.evec)
+            for (int i = 0; i < K; ++i) ex.evec[(int64_t)s * K * K + (int64_t)i * K + pos] = V(i, t);
     }
 }
 
@@ -255,7 +269,8 @@ void launch_delete_one(const double* blocks, int64_t B, int64_t P, double* sys, 
 }
 
 void launch_sym_solve(const double* sys, int64_t nsys, int K, double rtol, int require_full_rank,
-                      double* x, int* rank, double* eig, int* status, cudaStream_t st) {
+                      double* x, int* rank, double* eig, int* status, cudaStream_t st,
+                      const SymSolveExtras& ex) {
     if (nsys == 0) return;
     const size_t smem = (size_t)3 * K * (K + 1) * sizeof(double);
     static std::atomic<unsigned long long> attr{0};
@@ -264,7 +279,7 @@ void launch_sym_solve(const double* sys, int64_t nsys, int K, double rtol, int r
                              (int)((size_t)3 * kMaxK * (kMaxK + 1) * sizeof(double)));
     });
     sym_solve_kernel<<<(unsigned)nsys, kSolveThreads, smem, st>>>(sys, K, rtol, require_full_rank, x,
-                                                                   rank, eig, status);
+                                                                   rank, eig, status, ex);
     count_launch();
 }
 
