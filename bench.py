@@ -545,6 +545,27 @@ def ours_arm(args) -> None:
     # graph launches run kernels the launch counter does not see: count them per graph
     wplan.close()
 
+    # ---- the same estimate with exact product checks (tensor-core checksums
+    # against a CUDA-core recomputation, compared on the host) ----
+    product_checks = None
+    if not os.environ.get("LDS_SKIP_CHECKS"):
+        cplan = autotune.tuned_win_plan(sess, annot, ws, B_PROBES, BLOCK, PROBE_SEED, "rademacher",
+                                        tune_if_missing=False)
+        cplan.set_checks(True)
+        for _ in range(args.warmup):
+            cplan.execute()
+        torch.cuda.synchronize()
+        cms = timed(cplan.execute, args.steps)
+        chk = cplan.check_products()
+        same = bool(np.array_equal(cplan.results()["ldscore"], res["ldscore"]))
+        cplan.close()
+        if chk["mismatches"] or not same:
+            raise RuntimeError(f"product checks failed: {chk['mismatches']} SNPs, "
+                               f"scores identical: {same}")
+        product_checks = {"ms_per_step": round(cms, 3), "overhead": round(cms / ms - 1.0, 4),
+                          "check_kernels_ms": round(chk["check_ms"], 3), "mismatches": 0,
+                          "scores_identical": same}
+
     # ---- secondary: genome-wide form of the same workload ----
     plan = sess.plan(annot, B_PROBES, BLOCK, PROBE_SEED, "rademacher")
     for _ in range(args.warmup):
@@ -664,6 +685,8 @@ def ours_arm(args) -> None:
         }
         if hwe is not None:
             line["windowed_hwe"] = hwe
+        if product_checks is not None:
+            line["product_checks"] = product_checks
         if lvp is not None:
             line["learned_vs_plain"] = lvp
         if world == 1 and not os.environ.get("LDS_SKIP_CPU_BASELINE"):

@@ -317,6 +317,25 @@ int lds_win_plan_bin_totals(int64_t plan, double* mkw_out);
  * The LD scores do not depend on the tiling (bit for bit).  No reference
  * counterpart (it replaces the reference's CPU tiling environment knobs). */
 int lds_win_plan_set_tiling(int64_t plan, int p1_sb_per_cta);
+/* Exact integrity check of the phase-2 tensor-core products (the counterpart
+ * of the reference's ABFT / Freivalds check of its GxE GEMMs,
+ * gxeldcore.cpp:4674-4734, made exact because the products are integers).
+ * With checks on (set before the plan's first execute), every estimate also
+ * forms per SNP j two pairs of wrapping 64-bit checksums: lhs from the phase-2
+ * epilogue, sum over (bin k, probe v) of h(k, v) times the exact products
+ * G_j^T y~_kv and O_j^T y~_kv, and rhs = sum_i g_ij u(i), sum_i o_ij u(i) with
+ * u(i) = sum h(k, v) y~_kv(i), recomputed on the CUDA cores from the sketch
+ * digits and the packed codes (h odd, so any single wrong product shows).
+ * lds_win_plan_check copies both (2 x M each, [2j] G and [2j+1] O; either
+ * pointer may be NULL) and compares them on the host: mismatches = SNPs that
+ * differ, first_snp the first (-1 if none), check_ms the check kernels' time
+ * in the last estimate.  lds_check_vectors is that host comparison alone (for
+ * checksums a caller copied or stored). */
+int lds_win_plan_set_checks(int64_t plan, int on);
+int lds_win_plan_check(int64_t plan, unsigned long long* lhs, unsigned long long* rhs,
+                       int64_t* mismatches, int64_t* first_snp, double* check_ms);
+int lds_check_vectors(const unsigned long long* lhs, const unsigned long long* rhs, int64_t n_snps,
+                      int64_t* mismatches, int64_t* first_snp);
 int lds_win_plan_destroy(int64_t plan);
 
 /* Windowed + partitioned LD scores in one call from host BED rows (the

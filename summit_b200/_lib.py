@@ -54,6 +54,9 @@ SIGNATURES: dict[str, tuple] = {
     "lds_win_plan_bin_totals": (_int, [_i64, _p]),
     "lds_win_plan_cv_annot": (_int, [_i64, _p]),
     "lds_win_plan_set_tiling": (_int, [_i64, _int]),
+    "lds_win_plan_set_checks": (_int, [_i64, _int]),
+    "lds_win_plan_check": (_int, [_i64, _p, _p, _p, _p, _p]),
+    "lds_check_vectors": (_int, [_p, _p, _i64, _p, _p]),
     "lds_win_plan_destroy": (_int, [_i64]),
     "lds_win_plan_set_cv": (_int, [_i64, _p, _int, _int]),
     "lds_win_plan_tiles": (_int, [_i64, _p, _p]),

@@ -104,4 +104,9 @@ __host__ __device__ __forceinline__ uint64_t mix64(uint64_t x) {
     return x ^ (x >> 31);
 }
 
+// Odd 64-bit weight of (bin k, probe v) in the phase-2 product checksums.
+__host__ __device__ __forceinline__ uint64_t check_weight(int k, int v) {
+    return mix64(((uint64_t)(uint32_t)k << 32) | (uint64_t)(uint32_t)v) | 1ULL;
+}
+
 }  // namespace lds

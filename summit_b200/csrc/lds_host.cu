@@ -2173,8 +2173,15 @@ struct WinPlan {
     double cv_ms = 0.0;
     CUtensorMap tmA;
     std::vector<cudaEvent_t> ev;        // start, after phase 1 of each launch group, end
-    double kernel_ms[4] = {0, 0, 0, 0};
+    // weights, phase 1, digits, phase 2 and (with checks) product checks
+    double kernel_ms[5] = {0, 0, 0, 0, 0};
     int pending = 0;
+    // Product checksums (lds_win_plan_set_checks): lhs from the phase-2
+    // epilogue, rhs from the CUDA-core pass (lds_check.cu), 2 per SNP; u per
+    // window of the largest batch.
+    int check = 0;
+    DevBuf chk_lhs, chk_rhs, chk_u;
+    int ev_per() const { return check ? 5 : 4; }
     cudaGraphExec_t graph = nullptr;
     unsigned long long graph_kernels = 0;  // kernel nodes in the captured graph
     // Output slices: with `split`, probes [0, half) and [half, nvecs) of every
@@ -2403,6 +2410,10 @@ void win_enqueue(Context& c, WinPlan& pl) {
     ck(cudaMemsetAsync(pl.accum.p, 0, sizeof(double) * nout, c.st), "memset");
     if (pl.with_mc) ck(cudaMemsetAsync(pl.mc.p, 0, sizeof(double) * MK, c.st), "memset");
     ck(cudaMemsetAsync(pl.guards.p, 0, 16, c.st), "memset");
+    if (pl.check) {
+        ck(cudaMemsetAsync(pl.chk_lhs.p, 0, sizeof(unsigned long long) * 2 * (size_t)M, c.st), "memset");
+        ck(cudaMemsetAsync(pl.chk_rhs.p, 0, sizeof(unsigned long long) * 2 * (size_t)M, c.st), "memset");
+    }
     if (pl.cv_D > 0) {
         // Near-field control variate sums: inputs are static (probes, products),
         // so they run first, timed by their own event pair.
@@ -2524,8 +2535,23 @@ void win_enqueue(Context& c, WinPlan& pl) {
                 u.colsum = colsum;
             }
             u.tiles = static_cast<int4*>(b.tiles.p);
+            if (pl.check) {
+                u.chk = static_cast<unsigned long long*>(pl.chk_lhs.p);
+                u.chk_v0 = pl.voff(ti);
+            }
             umma::launch_p2_umma(pl.tmA, u, c.st);
             ck(cudaEventRecordWithFlags(pl.ev[(size_t)e++], c.st, cudaEventRecordExternal), "event");
+            if (pl.check) {
+                // the same products, recomputed on the CUDA cores before the
+                // next batch's phase 1 overwrites the sketch digits
+                auto* ub = static_cast<unsigned long long*>(pl.chk_u.p);
+                launch_check_u(static_cast<const int8_t*>(pl.yq->p), b.ksup * nc, nc, (int)K, V,
+                               pl.voff(ti), b.w1 - b.w0, Np, ub, c.st);
+                launch_check_rhs(P.g.codes, P.g.nbp, static_cast<const int4*>(b.tiles.p), b.ntiles,
+                                 (int)K, ub, Np, static_cast<unsigned long long*>(pl.chk_rhs.p),
+                                 c.st);
+                ck(cudaEventRecordWithFlags(pl.ev[(size_t)e++], c.st, cudaEventRecordExternal), "event");
+            }
         }
     }
     ck(cudaGetLastError(), "launch");
@@ -2570,7 +2596,8 @@ void win_times(WinPlan& pl) {
         float ms = 0.f;
         ck(cudaEventElapsedTime(&ms, pl.ev[i], pl.ev[i + 1]), "elapsed");
         // event order per (V-tile, batch): weights, phase 1, digits, phase 2
-        pl.kernel_ms[i % 4] += ms;
+        // and, with checks, the product check
+        pl.kernel_ms[i % (size_t)pl.ev_per()] += ms;
     }
     pl.pending = 0;
 }
@@ -4534,6 +4561,81 @@ LDS_API int lds_win_plan_set_tiling(int64_t plan, int p1_sb_per_cta) {
         if (p1_sb_per_cta < 0 || p1_sb_per_cta > 4096)
             fail(LDS_ERR_ARG, "p1_sb_per_cta must be in [0, 4096]");
         pl.p1_spc = p1_sb_per_cta;
+    });
+}
+
+// SNPs whose G or O checksum pair differs (host comparison); the first one in
+// *first (-1 if none).
+static int64_t count_check_mismatches(const unsigned long long* lhs, const unsigned long long* rhs,
+                                      int64_t n_snps, int64_t* first) {
+    int64_t bad = 0, f = -1;
+    for (int64_t j = 0; j < n_snps; ++j)
+        if (lhs[2 * j] != rhs[2 * j] || lhs[2 * j + 1] != rhs[2 * j + 1]) {
+            if (f < 0) f = j;
+            ++bad;
+        }
+    if (first) *first = f;
+    return bad;
+}
+
+LDS_API int lds_win_plan_set_checks(int64_t plan, int on) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        WinPlan& pl = win_of_handle(plan);
+        if (pl.graph) fail(LDS_ERR_ARG, "set the product checks before the plan's first execute");
+        pl.check = on ? 1 : 0;
+        if (pl.check) {
+            const size_t M = (size_t)pl.P->g.M;
+            int64_t maxw = 1;
+            for (const auto& b : pl.batches) maxw = std::max(maxw, b.w1 - b.w0);
+            pl.chk_lhs.as<unsigned long long>(2 * M);
+            pl.chk_rhs.as<unsigned long long>(2 * M);
+            pl.chk_u.as<unsigned long long>((size_t)maxw * (size_t)pl.P->g.N_pad);
+        }
+        // one more event per (V-tile, batch) closes the check interval
+        const size_t need = 1 + (size_t)pl.ev_per() * pl.vt.size() * pl.batches.size();
+        while (pl.ev.size() < need) {
+            cudaEvent_t e = nullptr;
+            ck(cudaEventCreate(&e), "event");
+            pl.ev.push_back(e);
+        }
+        while (pl.ev.size() > need) {
+            cudaEventDestroy(pl.ev.back());
+            pl.ev.pop_back();
+        }
+    });
+}
+
+LDS_API int lds_win_plan_check(int64_t plan, unsigned long long* lhs, unsigned long long* rhs,
+                               int64_t* mismatches, int64_t* first_snp, double* check_ms) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        WinPlan& pl = win_of_handle(plan);
+        if (!pl.check) fail(LDS_ERR_ARG, "product checks are off for this plan (lds_win_plan_set_checks)");
+        if (!pl.graph) fail(LDS_ERR_ARG, "no estimate of this plan has run");
+        const size_t n = 2 * (size_t)pl.P->g.M;
+        std::vector<unsigned long long> hl, hr;
+        if (!lhs) { hl.resize(n); lhs = hl.data(); }
+        if (!rhs) { hr.resize(n); rhs = hr.data(); }
+        ck(cudaStreamSynchronize(c.st), "sync");
+        win_times(pl);
+        d2h(lhs, static_cast<unsigned long long*>(pl.chk_lhs.p), n, c.st);
+        d2h(rhs, static_cast<unsigned long long*>(pl.chk_rhs.p), n, c.st);
+        ck(cudaStreamSynchronize(c.st), "checksums");
+        const int64_t bad = count_check_mismatches(lhs, rhs, (int64_t)(n / 2), first_snp);
+        if (mismatches) *mismatches = bad;
+        if (check_ms) *check_ms = pl.kernel_ms[4];
+    });
+}
+
+LDS_API int lds_check_vectors(const unsigned long long* lhs, const unsigned long long* rhs,
+                              int64_t n_snps, int64_t* mismatches, int64_t* first_snp) {
+    return guarded([&] {
+        if (n_snps < 0 || (n_snps > 0 && (!lhs || !rhs))) fail(LDS_ERR_ARG, "invalid checksum vectors");
+        const int64_t bad = count_check_mismatches(lhs, rhs, n_snps, first_snp);
+        if (mismatches) *mismatches = bad;
     });
 }
 

@@ -168,6 +168,15 @@ template <typename T> void launch_standardize_dosage(T* G, int64_t N, int64_t L,
                                                      double missing, unsigned long long* counts,
                                                      cudaStream_t st);
 
+// Phase-2 product checksums (lds_check.cu): u[wl][i] over the n_windows
+// windows of a batch (K super-bins each, V probes from global probe v0), and
+// rhs[2j], rhs[2j+1] += sum_i g_ij u(i), sum_i o_ij u(i) for the rows of each tile.
+void launch_check_u(const int8_t* yq, int64_t yq_cols, int ncolp, int K, int V, int v0,
+                    int64_t n_windows, int64_t N_pad, unsigned long long* u, cudaStream_t st);
+void launch_check_rhs(const uint8_t* codes, int64_t nbp, const int4* tiles, int64_t n_tiles, int K,
+                      const unsigned long long* u, int64_t N_pad, unsigned long long* rhs,
+                      cudaStream_t st);
+
 // Jackknife and normal-equation solves (lds_jack.cu).
 int sym_solve_max_k();
 void launch_block_sums(const double* X, int64_t P, const int64_t* starts, const int64_t* ends,

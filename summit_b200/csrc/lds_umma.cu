@@ -234,6 +234,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         const double mu = stats ? a.mean[j] : 0.0;
         const double sd = stats ? a.sdinv[j] : 0.0;
         double run2 = 0.0, run4 = 0.0, run2b = 0.0;
+        unsigned long long chk_g = 0ULL, chk_o = 0ULL;  // product checksums (a.chk)
         int cur = 0;  // bin offset (within this CTA's bins) that run2/run4 belong to
         // Add the running sums of bin k0 + cur to the outputs, with the
         // reference's guards, and restart them.
@@ -334,6 +335,11 @@ __global__ void __launch_bounds__(kThreads, 1)
                     const long long TO =
                         (((long long)ro[4 * p] * 128 + ro[4 * p + 1]) * 128 + ro[4 * p + 2]) * 128 +
                         ro[4 * p + 3];
+                    if (a.chk) {
+                        const unsigned long long h = check_weight(k0 + bo, a.chk_v0 + v);
+                        chk_g += h * (unsigned long long)TG;
+                        chk_o += h * (unsigned long long)TO;
+                    }
                     if (a.raw_g) {
                         if (j < jend) {
                             a.raw_g[(j - a.out_row0) * a.V + v] = TG;
@@ -353,7 +359,13 @@ __global__ void __launch_bounds__(kThreads, 1)
             __syncwarp();
             if (lane == 0) mbar_arrive(acc_empty);
         }
-        if (dset == 0) flush();
+        if (dset == 0) {
+            flush();
+            if (a.chk && j < jend && !*abort_flag) {
+                atomicAdd(&a.chk[2 * j], chk_g);
+                atomicAdd(&a.chk[2 * j + 1], chk_o);
+            }
+        }
     }
     tc_fence_before();
     __syncthreads();

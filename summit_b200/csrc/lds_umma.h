@@ -60,6 +60,11 @@ struct P2UArgs {
     // samples; padding samples carry zero digits).  Unused if either is null.
     const uint8_t* snp_missing = nullptr;
     const int* colsum = nullptr;
+    // Product checksums (lds_check.cu): when set, chk[2j] and chk[2j+1] gain
+    // sum over this CTA's (bin k, probe v) of check_weight(k, chk_v0 + v) times
+    // the exact products T_G and T_O of SNP row j (wrapping mod 2^64).
+    unsigned long long* chk = nullptr;
+    int chk_v0 = 0;
 };
 
 // Bins that share one CTA in phase 2: as many whole bins as fit 256 columns.

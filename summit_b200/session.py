@@ -267,6 +267,26 @@ class WinPlan:
         execute."""
         check(_lib.load().lds_win_plan_set_tiling(self.handle, int(p1_sb_per_cta)))
 
+    def set_checks(self, on: bool = True) -> None:
+        """Exact integrity checks of the phase-2 products on every estimate
+        (checksums from the tensor-core epilogue against a CUDA-core
+        recomputation); call before the first execute."""
+        check(_lib.load().lds_win_plan_set_checks(self.handle, int(bool(on))))
+
+    def check_products(self) -> dict:
+        """Checksums of the last estimate: {"mismatches", "first_snp",
+        "check_ms", "lhs", "rhs"} (lhs / rhs: M x 2 uint64, columns G and O).
+        A mismatch means some tensor-core product of that SNP was wrong."""
+        n = np.zeros(1, dtype=np.int64)
+        f = np.zeros(1, dtype=np.int64)
+        ms = np.zeros(1)
+        lhs = np.zeros((self.M, 2), dtype=np.uint64)
+        rhs = np.zeros((self.M, 2), dtype=np.uint64)
+        check(_lib.load().lds_win_plan_check(self.handle, ptr(lhs), ptr(rhs), ptr(n), ptr(f),
+                                             ptr(ms)))
+        return {"mismatches": int(n[0]), "first_snp": int(f[0]), "check_ms": float(ms[0]),
+                "lhs": lhs, "rhs": rhs}
+
     def cv_annot_view(self):
         """Read-only torch view (cuda, float64, M x K) of the annotation matrix the
         plan uploaded in set_cv; valid while the plan lives."""
