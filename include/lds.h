@@ -332,6 +332,11 @@ int lds_win_plan_set_tiling(int64_t plan, int p1_sb_per_cta);
  * in the last estimate.  lds_check_vectors is that host comparison alone (for
  * checksums a caller copied or stored). */
 int lds_win_plan_set_checks(int64_t plan, int on);
+/* The same checks on a genome-wide plan (lds_gw_plan_create; the tcgen05 path):
+ * its rows form one window. */
+int lds_gw_plan_set_checks(int64_t plan, int on);
+int lds_gw_plan_check(int64_t plan, unsigned long long* lhs, unsigned long long* rhs,
+                      int64_t* mismatches, int64_t* first_snp, double* check_ms);
 int lds_win_plan_check(int64_t plan, unsigned long long* lhs, unsigned long long* rhs,
                        int64_t* mismatches, int64_t* first_snp, double* check_ms);
 int lds_check_vectors(const unsigned long long* lhs, const unsigned long long* rhs, int64_t n_snps,
@@ -687,6 +692,35 @@ int lds_gxe_target_score_block_dense(int64_t gxe, const double* genotype, int64_
                                      int64_t total_variants, int probe_count,
                                      int environment_start, int device_ptrs);
 int lds_gxe_destroy(int64_t gxe);
+/* Generalized per-variant GxE two-pass estimator (generalized_gxe_pass1.py
+ * GeneralizedGxEPass1Executor, generalized_gxe_pass2.py
+ * GeneralizedGxEPass2Executor), on a resident image (lds_geno_create) whose
+ * standardized genotypes x_ij = s_j (g_ij - mu_j), 0 on a missing call, are
+ * the decoded blocks of the reference's genotype operator.  Host pointers.
+ * lds_geno_source_product: out (N x K*B column-major, column k*B + b) =
+ *   sum_{j in [j0, j1)} x_j sqrt(a_jk) Z[j, b] (the pass-1 base sources);
+ *   annot (L x K row-major) NULL means one unit-weight bin (K ignored).
+ *   Z is L x B column-major.
+ * lds_geno_target_product: out (L x cols column-major) = X_[j0,j1)^T Y, Y
+ *   N x cols column-major (the pass-2 cross sketches).
+ * lds_global_variant_probes: out (L x B column-major) = the reference's
+ *   global_probe_sign (generalized_gxe_variant.py:80-103) for variants
+ *   v0 .. v0+L-1 and probes p0 .. p0+B-1, namespace_key its FNV-1a key.
+ * lds_generalized_component_diagonal: numerator (K*P x N row-major, component
+ *   k*P + p, P = Q(Q+1)/2 pairs diagonal first) += sum_j a_jk kf_p f_q f_r
+ *   with f_q(i, j) = phi_q(i) x_ij - sum_r F(i, r) coef[j, q, r] (the pass-2
+ *   component-kernel diagonals, generalized_gxe_pass2.py:528-562); basis
+ *   N x Q and fixed N x R column-major, coef L x Q x R row-major (NULL when
+ *   R = 0); Q <= 6, R <= 16. */
+int lds_geno_source_product(int64_t geno, int64_t j0, int64_t j1, const double* annot, int64_t K,
+                            const double* Z, int64_t B, double* out);
+int lds_geno_target_product(int64_t geno, int64_t j0, int64_t j1, const double* Y, int64_t cols,
+                            double* out);
+int lds_global_variant_probes(uint64_t root_seed, uint64_t namespace_key, int64_t v0, int64_t L,
+                              int64_t p0, int64_t B, double* out);
+int lds_generalized_component_diagonal(int64_t geno, int64_t j0, int64_t j1, const double* annot,
+                                       int K, const double* basis, int Q, const double* fixed,
+                                       int R, const double* coef, double* numerator);
 /* Generalized per-SNP GxE packed products (GeneralizedGxELDScoreDirectContext::
  * packed_source_product / packed_target_product, generalized_gxe_variant.inc:
  * 1749-1988) on a mean-imputed resident image (lds_geno_create): with the

@@ -1,0 +1,81 @@
+"""CPU restatement of the device pieces of the generalized per-variant GxE
+estimator.  Test infrastructure only: the tests use it as the checker of
+summit_b200.generalized_gxe's host-side algebra (standing in for the device
+products) and of the device probe stream; no product path imports it.
+
+* global_probe_sign / global_probes: the reference's counter-based Rademacher
+  stream (ldscore/generalized_gxe_variant.py:60-103, 114-152);
+* source_product / target_product: the dense products of pass 1
+  (generalized_gxe_pass1.py:683-700, base += G (sqrt(a) o Z)) and pass 2
+  (generalized_gxe_pass2.py:619, G^T rhs) on a decoded standardized block;
+* component_diagonal: the pass-2 component-kernel diagonal numerators
+  (generalized_gxe_pass2.py:528-572), projected-feature form.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+MASK64 = (1 << 64) - 1
+
+
+def splitmix64(value: int) -> int:
+    value = (value + 0x9E3779B97F4A7C15) & MASK64
+    value = ((value ^ (value >> 30)) * 0xBF58476D1CE4E5B9) & MASK64
+    value = ((value ^ (value >> 27)) * 0x94D049BB133111EB) & MASK64
+    return (value ^ (value >> 31)) & MASK64
+
+
+def namespace_key(namespace: str) -> int:
+    value = 0xCBF29CE484222325
+    for byte in namespace.encode("utf-8"):
+        value ^= byte
+        value = (value * 0x100000001B3) & MASK64
+    return value
+
+
+def global_probe_sign(root_seed: int, variant: int, probe: int, key: int) -> float:
+    state = splitmix64((root_seed ^ key ^ 0x9E3779B97F4A7C15) & MASK64)
+    state ^= splitmix64((variant + 0xD2B74407B1CE6E93) & MASK64)
+    state ^= splitmix64((probe + 0xCA5A826395121157) & MASK64)
+    return 1.0 if (splitmix64(state) >> 63) else -1.0
+
+
+def global_probes(root_seed: int, variants, probes, namespace: str) -> np.ndarray:
+    key = namespace_key(namespace)
+    out = np.empty((len(variants), len(probes)), order="F")
+    for c, p in enumerate(probes):
+        for r, v in enumerate(variants):
+            out[r, c] = global_probe_sign(root_seed, int(v), int(p), key)
+    return out
+
+
+def source_product(X: np.ndarray, j0: int, j1: int, annot_blk: np.ndarray,
+                   z: np.ndarray) -> np.ndarray:
+    blk = X[:, j0:j1]
+    k_count = annot_blk.shape[1]
+    return np.asfortranarray(np.concatenate(
+        [blk @ (np.sqrt(annot_blk[:, k])[:, None] * z) for k in range(k_count)], axis=1))
+
+
+def target_product(X: np.ndarray, j0: int, j1: int, Y: np.ndarray) -> np.ndarray:
+    return np.asfortranarray(X[:, j0:j1].T @ Y)
+
+
+def component_diagonal(X: np.ndarray, j0: int, j1: int, annot_blk, basis, fixed, coef,
+                       numerator: np.ndarray) -> None:
+    blk = X[:, j0:j1]
+    q_count = basis.shape[1]
+    pairs = [(q, q) for q in range(q_count)] + [
+        (q, r) for q in range(q_count - 1) for r in range(q + 1, q_count)]
+    p_count = len(pairs)
+    feats = []
+    for q in range(q_count):
+        f = basis[:, q, None] * blk
+        if fixed.shape[1]:
+            f = f - fixed @ coef[:, q, :].T
+        feats.append(f)
+    for p, (q, r) in enumerate(pairs):
+        factor = 1.0 if q == r else 2.0
+        prod = (factor * feats[q] * feats[r]) @ annot_blk   # N x K
+        for k in range(annot_blk.shape[1]):
+            numerator[k * p_count + p] += prod[:, k]

@@ -55,8 +55,15 @@ SIGNATURES: dict[str, tuple] = {
     "lds_win_plan_cv_annot": (_int, [_i64, _p]),
     "lds_win_plan_set_tiling": (_int, [_i64, _int]),
     "lds_win_plan_set_checks": (_int, [_i64, _int]),
+    "lds_gw_plan_set_checks": (_int, [_i64, _int]),
+    "lds_gw_plan_check": (_int, [_i64, _p, _p, _p, _p, _p]),
     "lds_win_plan_check": (_int, [_i64, _p, _p, _p, _p, _p]),
     "lds_check_vectors": (_int, [_p, _p, _i64, _p, _p]),
+    "lds_geno_source_product": (_int, [_i64, _i64, _i64, _p, _i64, _p, _i64, _p]),
+    "lds_geno_target_product": (_int, [_i64, _i64, _i64, _p, _i64, _p]),
+    "lds_global_variant_probes": (_int, [_u64, _u64, _i64, _i64, _i64, _i64, _p]),
+    "lds_generalized_component_diagonal": (_int, [_i64, _i64, _i64, _p, _int, _p, _int, _p, _int,
+                                                  _p, _p]),
     "lds_win_plan_destroy": (_int, [_i64]),
     "lds_win_plan_set_cv": (_int, [_i64, _p, _int, _int]),
     "lds_win_plan_tiles": (_int, [_i64, _p, _p]),

@@ -10,7 +10,7 @@ from pathlib import Path
 PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 OUT = PKG / "liblds.so"
-SOURCES = ["lds_kernels.cu", "lds_umma.cu", "lds_umma_p1.cu", "lds_band.cu", "lds_gram.cu", "lds_gxe.cu", "lds_proj.cu", "lds_jack.cu", "lds_dense.cu", "lds_probes.cu", "lds_cv.cu", "lds_mlp.cu", "lds_check.cu", "lds_host.cu",
+SOURCES = ["lds_kernels.cu", "lds_umma.cu", "lds_umma_p1.cu", "lds_band.cu", "lds_gram.cu", "lds_gxe.cu", "lds_proj.cu", "lds_jack.cu", "lds_dense.cu", "lds_probes.cu", "lds_cv.cu", "lds_mlp.cu", "lds_check.cu", "lds_generalized.cu", "lds_host.cu",
            "lds_noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -1,0 +1,118 @@
+// Device pieces of the generalized per-variant GxE two-pass estimator
+// (ldscore/generalized_gxe_pass1.py, generalized_gxe_pass2.py): the global
+// variant x probe Rademacher stream and the component-kernel diagonals.
+// The genotype products of both passes run on the tensor-core kernels
+// (lds_umma_p1.cu, lds_umma.cu) through lds_geno_source_product /
+// lds_geno_target_product.
+#include <cstdint>
+
+#include "lds_device.cuh"
+#include "lds_internal.h"
+
+namespace lds {
+
+namespace {
+
+// splitmix64 with the increment applied first (generalized_gxe_variant.py
+// _splitmix64), and the addressable sign of global_probe_sign.
+__device__ __forceinline__ uint64_t splitmix64_step(uint64_t v) {
+    v += 0x9E3779B97F4A7C15ULL;
+    v = (v ^ (v >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    v = (v ^ (v >> 27)) * 0x94D049BB133111EBULL;
+    return v ^ (v >> 31);
+}
+
+// out[b * L + j] = sign(root, variant v0 + j, probe p0 + b) (column-major L x B).
+__global__ void global_probes_kernel(uint64_t root_state, int64_t v0, int64_t L, int64_t p0,
+                                     int64_t B, double* __restrict__ out) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= L * B) return;
+    const int64_t j = idx % L, b = idx / L;
+    uint64_t s = root_state;
+    s ^= splitmix64_step((uint64_t)(v0 + j) + 0xD2B74407B1CE6E93ULL);
+    s ^= splitmix64_step((uint64_t)(p0 + b) + 0xCA5A826395121157ULL);
+    out[idx] = (splitmix64_step(s) >> 63) ? 1.0 : -1.0;
+}
+
+constexpr int kDiagThreads = 128;
+constexpr int kDiagComp = 16;      // components per thread (registers)
+
+// num[c * N + i] += sum_j a[j, k] kf(p) f_q(i, j) f_r(i, j) for the components
+// c = k * P + p of this CTA's chunk, with the projected contextual features
+// f_q(i, j) = phi_q(i) x_ij - sum_r F(i, r) coef[j, q, r] (pass-2 feature
+// tiles, generalized_gxe_pass2.py:528-562) and x_ij the image's standardized
+// genotype (0 on a missing call).  One thread per sample.
+__global__ void __launch_bounds__(kDiagThreads)
+    component_diag_kernel(const uint8_t* __restrict__ codes, int64_t nbp,
+                          const double* __restrict__ mean, const double* __restrict__ sdinv,
+                          int64_t j0, int64_t L, int64_t N, const double* __restrict__ annot,
+                          int K, const double* __restrict__ basis, int Q,
+                          const double* __restrict__ fixed, int R,
+                          const double* __restrict__ coef, const int* __restrict__ pq,
+                          const int* __restrict__ pr, const double* __restrict__ kf, int P,
+                          double* __restrict__ num) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int c0 = blockIdx.y * kDiagComp;
+    const int C = K * P;
+    if (i >= N) return;
+    double phi[kGenMaxQ], frow[kGenMaxR], acc[kDiagComp];
+    for (int q = 0; q < Q; ++q) phi[q] = basis[(int64_t)q * N + i];
+    for (int r = 0; r < R; ++r) frow[r] = fixed[(int64_t)r * N + i];
+#pragma unroll
+    for (int t = 0; t < kDiagComp; ++t) acc[t] = 0.0;
+    const int shift = 2 * (int)(i & 3);
+    for (int64_t jl = 0; jl < L; ++jl) {
+        const int64_t j = j0 + jl;
+        const uint32_t code = (codes[j * nbp + (i >> 2)] >> shift) & 3u;
+        const double g = (double)((code >> 1) + (code == 3u));
+        const double x = code == 1u ? 0.0 : sdinv[j] * (g - mean[j]);
+        double f[kGenMaxQ];
+        for (int q = 0; q < Q; ++q) {
+            double v = phi[q] * x;
+            const double* cj = coef + (jl * Q + q) * R;
+            for (int r = 0; r < R; ++r) v -= frow[r] * cj[r];
+            f[q] = v;
+        }
+#pragma unroll
+        for (int t = 0; t < kDiagComp; ++t) {
+            const int c = c0 + t;
+            if (c >= C) break;
+            const int k = c / P, p = c - k * P;
+            const double a = annot[jl * K + k];
+            if (a != 0.0) acc[t] += a * (kf[p] * f[pq[p]] * f[pr[p]]);
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < kDiagComp; ++t) {
+        const int c = c0 + t;
+        if (c < C) num[(int64_t)c * N + i] += acc[t];
+    }
+}
+
+}  // namespace
+
+void launch_global_probes(uint64_t root_state, int64_t v0, int64_t L, int64_t p0, int64_t B,
+                          double* out, cudaStream_t st) {
+    const int64_t n = L * B;
+    if (n <= 0) return;
+    global_probes_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(root_state, v0, L, p0, B,
+                                                                      out);
+    count_launch();
+}
+
+void launch_component_diag(const uint8_t* codes, int64_t nbp, const double* mean,
+                           const double* sdinv, int64_t j0, int64_t L, int64_t N,
+                           const double* annot, int K, const double* basis, int Q,
+                           const double* fixed, int R, const double* coef, const int* pq,
+                           const int* pr, const double* kf, int P, double* num, cudaStream_t st) {
+    const int C = K * P;
+    if (N <= 0 || L <= 0 || C <= 0) return;
+    dim3 grid((unsigned)((N + kDiagThreads - 1) / kDiagThreads),
+              (unsigned)((C + kDiagComp - 1) / kDiagComp));
+    component_diag_kernel<<<grid, kDiagThreads, 0, st>>>(codes, nbp, mean, sdinv, j0, L, N, annot,
+                                                         K, basis, Q, fixed, R, coef, pq, pr, kf,
+                                                         P, num);
+    count_launch();
+}
+
+}  // namespace lds

@@ -1744,9 +1744,20 @@ struct GwPlan {
     std::vector<std::vector<cudaEvent_t>> evsets;
     int pending = 0;
     double kernel_ms[4] = {0, 0, 0, 0};  // weights, phase 1, sketch digits, phase 2
+    // Product checksums (lds_gw_plan_set_checks), as for windowed plans: lhs
+    // from the phase-2 epilogue, rhs from the CUDA-core pass; the rows form
+    // one window (a tile table of 128-SNP tiles).  chk_evsets[p][t] closes
+    // V-tile t's phase 2 before its check kernels.
+    int check = 0, executed = 0;
+    DevBuf chk_lhs, chk_rhs, chk_u, chk_tiles;
+    int64_t chk_ntiles = 0;
+    std::vector<std::vector<cudaEvent_t>> chk_evsets;
+    double check_ms = 0.0;
     int64_t snp_offset = 0;  // index of SNP 0 of this image in the whole fileset (SNP shards)
     ~GwPlan() {
         for (auto& s : evsets)
+            for (cudaEvent_t e : s) cudaEventDestroy(e);
+        for (auto& s : chk_evsets)
             for (cudaEvent_t e : s) cudaEventDestroy(e);
     }
 };
@@ -1908,6 +1919,10 @@ std::unique_ptr<GwPlan> plan_create(Context& c, std::shared_ptr<Prepared> P, con
 void plan_zero(Context& c, GwPlan& pl) {
     const int64_t M = pl.P->g.M, K = pl.K;
     ck(cudaMemsetAsync(pl.accum.p, 0, sizeof(double) * (size_t)(M * K), c.st), "memset");
+    if (pl.check) {
+        ck(cudaMemsetAsync(pl.chk_lhs.p, 0, sizeof(unsigned long long) * 2 * (size_t)M, c.st), "memset");
+        ck(cudaMemsetAsync(pl.chk_rhs.p, 0, sizeof(unsigned long long) * 2 * (size_t)M, c.st), "memset");
+    }
     if (pl.with_mc) ck(cudaMemsetAsync(pl.mc.p, 0, sizeof(double) * (size_t)(M * K), c.st), "memset");
     ck(cudaMemsetAsync(pl.guards.p, 0, 16, c.st), "memset");
 }
@@ -1973,7 +1988,7 @@ void plan_enqueue_phase1(Context& c, GwPlan& pl, size_t ti, double* y, cudaEvent
 // Phase 2 of V-tile ti from the sketch y: its digits, then
 // accum += the guarded per-SNP updates over this image's SNPs.
 void plan_enqueue_phase2(Context& c, GwPlan& pl, size_t ti, const double* y, cudaEvent_t* ev,
-                         int& e) {
+                         int& e, cudaEvent_t chk_ev = nullptr) {
     Prepared& P = *pl.P;
     const int64_t M = P.g.M, K = pl.K;
     GwPlan::Tile& t = *pl.tiles[ti];
@@ -2012,7 +2027,22 @@ void plan_enqueue_phase2(Context& c, GwPlan& pl, size_t ti, const double* y, cud
         }
         u.yq = static_cast<const int8_t*>(pl.yq.p);
         u.yq_cols = K * nc;
+        int v0 = 0;
+        for (size_t q = 0; q < ti; ++q) v0 += pl.tiles[q]->V;
+        if (pl.check) {
+            u.chk = static_cast<unsigned long long*>(pl.chk_lhs.p);
+            u.chk_v0 = v0;
+        }
         umma::launch_p2_umma(pl.tmA, u, c.st);
+        if (pl.check) {
+            if (chk_ev) ck(cudaEventRecord(chk_ev, c.st), "event");
+            auto* ub = static_cast<unsigned long long*>(pl.chk_u.p);
+            launch_check_u(static_cast<const int8_t*>(pl.yq.p), K * nc, nc, (int)K, t.V, v0, 1,
+                           P.g.N_pad, ub, c.st);
+            launch_check_rhs(P.g.codes, P.g.nbp, static_cast<const int4*>(pl.chk_tiles.p),
+                             pl.chk_ntiles, (int)K, ub, P.g.N_pad,
+                             static_cast<unsigned long long*>(pl.chk_rhs.p), c.st);
+        }
         if (ev) ck(cudaEventRecord(ev[e++], c.st), "event");
         return;
     }
@@ -2052,13 +2082,22 @@ void plan_execute(Context& c, GwPlan& pl) {
             pl.evsets.push_back(std::move(set));
         }
         ev = pl.evsets[(size_t)pl.pending].data();
+        if (pl.check) {
+            while ((int)pl.chk_evsets.size() <= pl.pending) {
+                std::vector<cudaEvent_t> set(pl.tiles.size());
+                for (auto& x : set) ck(cudaEventCreate(&x), "event");
+                pl.chk_evsets.push_back(std::move(set));
+            }
+        }
     }
+    pl.executed = 1;
     int e = 0;
     if (tm) ck(cudaEventRecord(ev[e++], c.st), "event");
     double* y = static_cast<double*>(pl.y.p);
     for (size_t ti = 0; ti < pl.tiles.size(); ++ti) {
         plan_enqueue_phase1(c, pl, ti, y, ev, e);
-        plan_enqueue_phase2(c, pl, ti, y, ev, e);
+        plan_enqueue_phase2(c, pl, ti, y, ev, e,
+                            (tm && pl.check) ? pl.chk_evsets[(size_t)pl.pending][ti] : nullptr);
     }
     if (tm) ++pl.pending;
     ck(cudaGetLastError(), "launch");
@@ -2068,6 +2107,7 @@ void plan_execute(Context& c, GwPlan& pl) {
 void plan_kernel_times(GwPlan& pl) {
     if (pl.pending == 0) return;
     for (double& x : pl.kernel_ms) x = 0.0;
+    pl.check_ms = 0.0;
     const size_t nt = pl.tiles.size();
     for (int p = 0; p < pl.pending; ++p) {
         const std::vector<cudaEvent_t>& ev = pl.evsets[(size_t)p];
@@ -2075,11 +2115,20 @@ void plan_kernel_times(GwPlan& pl) {
         for (size_t t = 0; t < nt; ++t)
             for (int k = 0; k < 4; ++k) {
                 float ms = 0.f;
-                ck(cudaEventElapsedTime(&ms, ev[4 * t + k], ev[4 * t + k + 1]), "elapsed");
+                // with checks, phase 2 ends at the check event and the check
+                // kernels run from there to the tile's last event
+                const cudaEvent_t end = (k == 3 && pl.check && pl.umma)
+                                            ? pl.chk_evsets[(size_t)p][t] : ev[4 * t + k + 1];
+                ck(cudaEventElapsedTime(&ms, ev[4 * t + k], end), "elapsed");
                 pl.kernel_ms[k] += ms;
+                if (end != ev[4 * t + k + 1]) {
+                    ck(cudaEventElapsedTime(&ms, end, ev[4 * t + k + 1]), "elapsed");
+                    pl.check_ms += ms;
+                }
             }
     }
     for (double& x : pl.kernel_ms) x /= (double)pl.pending;
+    pl.check_ms /= (double)pl.pending;
     pl.pending = 0;
 }
 
@@ -4401,6 +4450,53 @@ LDS_API int lds_gw_plan_results(int64_t plan, double* ldscore, double* meansq_ac
     });
 }
 
+static int64_t count_check_mismatches(const unsigned long long* lhs, const unsigned long long* rhs,
+                                      int64_t n_snps, int64_t* first);
+
+LDS_API int lds_gw_plan_set_checks(int64_t plan, int on) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        GwPlan& pl = plan_of(plan);
+        if (pl.executed) fail(LDS_ERR_ARG, "set the product checks before the plan's first execute");
+        if (on && !pl.umma) fail(LDS_ERR_ARG, "product checks need the tcgen05 phase-2 kernel");
+        pl.check = on ? 1 : 0;
+        if (!pl.check) return;
+        const int64_t M = pl.P->g.M;
+        pl.chk_lhs.as<unsigned long long>(2 * (size_t)M);
+        pl.chk_rhs.as<unsigned long long>(2 * (size_t)M);
+        pl.chk_u.as<unsigned long long>((size_t)pl.P->g.N_pad);
+        std::vector<int4> tiles;
+        for (int64_t j = 0; j < M; j += 128) tiles.push_back(make_int4((int)j, (int)M, 0, 0));
+        pl.chk_ntiles = (int64_t)tiles.size();
+        h2d(pl.chk_tiles.as<int4>(tiles.size()), tiles.data(), tiles.size(), c.st);
+        ck(cudaStreamSynchronize(c.st), "check tiles");
+    });
+}
+
+LDS_API int lds_gw_plan_check(int64_t plan, unsigned long long* lhs, unsigned long long* rhs,
+                              int64_t* mismatches, int64_t* first_snp, double* check_ms) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        GwPlan& pl = plan_of(plan);
+        if (!pl.check) fail(LDS_ERR_ARG, "product checks are off for this plan (lds_gw_plan_set_checks)");
+        if (!pl.executed) fail(LDS_ERR_ARG, "no estimate of this plan has run");
+        const size_t n = 2 * (size_t)pl.P->g.M;
+        std::vector<unsigned long long> hl, hr;
+        if (!lhs) { hl.resize(n); lhs = hl.data(); }
+        if (!rhs) { hr.resize(n); rhs = hr.data(); }
+        ck(cudaStreamSynchronize(c.st), "sync");
+        plan_kernel_times(pl);
+        d2h(lhs, static_cast<unsigned long long*>(pl.chk_lhs.p), n, c.st);
+        d2h(rhs, static_cast<unsigned long long*>(pl.chk_rhs.p), n, c.st);
+        ck(cudaStreamSynchronize(c.st), "checksums");
+        const int64_t bad = count_check_mismatches(lhs, rhs, (int64_t)(n / 2), first_snp);
+        if (mismatches) *mismatches = bad;
+        if (check_ms) *check_ms = pl.check_ms;
+    });
+}
+
 LDS_API int lds_gw_plan_kernel_ms(int64_t plan, double* ms4) {
     return guarded([&] {
         Context& c = ctx();
@@ -5081,6 +5177,137 @@ LDS_API int lds_generalized_target_product(int64_t geno, int64_t j0, int64_t j1,
         for (int64_t j = 0; j < L; ++j)
             for (int64_t q = 0; q < cols; ++q)
                 out[q * L + j] = -ratio[(size_t)j] * pr[(size_t)(j * cols + q)];
+    });
+}
+
+// ---------------------------------------------------------------------------
+// Products of the generalized per-variant GxE two-pass estimator
+// (generalized_gxe_pass1.py / _pass2.py) on the image's own standardized
+// genotypes x_ij = s_j (g_ij - mu_j), 0 on a missing call (the decoded blocks
+// its genotype operator returns).
+// ---------------------------------------------------------------------------
+static Prepared& product_image(int64_t geno, int64_t j0, int64_t j1, int64_t cols) {
+    auto it = geno_table().find(geno);
+    if (it == geno_table().end()) fail(LDS_ERR_ARG, "unknown genotype handle");
+    Prepared& P = *it->second;
+    if (j0 < 0 || j1 > P.g.M || j1 <= j0 || cols <= 0) fail(LDS_ERR_ARG, "genotype product is mis-sized");
+    return P;
+}
+
+LDS_API int lds_geno_source_product(int64_t geno, int64_t j0, int64_t j1, const double* annot,
+                                    int64_t K, const double* Z, int64_t B, double* out) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        ensure_device(c);
+        if (!Z || !out || (annot && K <= 0)) fail(LDS_ERR_ARG, "null or mis-sized product argument");
+        const int64_t nb = annot ? K : 1;
+        Prepared& P = product_image(geno, j0, j1, B * nb);
+        const int64_t L = j1 - j0, N = P.g.N, Np = P.g.N_pad;
+        if (annot)
+            for (int64_t q = 0; q < L * K; ++q)
+                if (!std::isfinite(annot[q]) || annot[q] < 0.0)
+                    fail(LDS_ERR_ARG, "annotations must be finite and nonnegative");
+        std::vector<double> ones((size_t)(L * nb), 1.0), unit((size_t)L, 1.0);
+        const int Vp = (int)round_up(B, kColTile);
+        const Csr cs = build_csr<double>(annot ? annot : ones.data(), unit.data(), L, nb, j0, Vp,
+                                         c.slices, kSnpStep, P.constant.data());
+        run_phase1(c, P, cs, nb, (int)B, Z, L, L, j0);
+        std::vector<double> y((size_t)(Np * nb * B));
+        d2h(y.data(), static_cast<double*>(c.y.p), y.size(), c.st);
+        ck(cudaStreamSynchronize(c.st), "genotype source product");
+        for (int64_t q = 0; q < nb * B; ++q)
+            std::memcpy(out + q * N, &y[(size_t)(q * Np)], sizeof(double) * (size_t)N);
+    });
+}
+
+LDS_API int lds_geno_target_product(int64_t geno, int64_t j0, int64_t j1, const double* Y,
+                                    int64_t cols, double* out) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        ensure_device(c);
+        if (!Y || !out) fail(LDS_ERR_ARG, "null product argument");
+        Prepared& P = product_image(geno, j0, j1, cols);
+        const int64_t L = j1 - j0, N = P.g.N;
+        const std::vector<double> Yv(Y, Y + N * cols);
+        const std::vector<double> pr = snp_products(c, P, j0, j1, Yv, cols);
+        for (int64_t j = 0; j < L; ++j)
+            for (int64_t q = 0; q < cols; ++q) out[q * L + j] = pr[(size_t)(j * cols + q)];
+    });
+}
+
+LDS_API int lds_global_variant_probes(uint64_t root_seed, uint64_t namespace_key, int64_t v0,
+                                      int64_t L, int64_t p0, int64_t B, double* out) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        ensure_device(c);
+        if (!out || L <= 0 || B <= 0 || v0 < 0 || p0 < 0) fail(LDS_ERR_ARG, "invalid probe block");
+        auto mix = [](uint64_t v) {
+            v += 0x9E3779B97F4A7C15ULL;
+            v = (v ^ (v >> 30)) * 0xBF58476D1CE4E5B9ULL;
+            v = (v ^ (v >> 27)) * 0x94D049BB133111EBULL;
+            return v ^ (v >> 31);
+        };
+        const uint64_t root_state = mix(root_seed ^ namespace_key ^ 0x9E3779B97F4A7C15ULL);
+        DevBuf d;
+        double* dp = d.as<double>((size_t)(L * B));
+        launch_global_probes(root_state, v0, L, p0, B, dp, c.st);
+        ck(cudaGetLastError(), "launch");
+        d2h(out, dp, (size_t)(L * B), c.st);
+        ck(cudaStreamSynchronize(c.st), "probes");
+    });
+}
+
+LDS_API int lds_generalized_component_diagonal(int64_t geno, int64_t j0, int64_t j1,
+                                               const double* annot, int K, const double* basis,
+                                               int Q, const double* fixed, int R,
+                                               const double* coef, double* numerator) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        ensure_device(c);
+        if (!annot || !basis || !numerator || K <= 0 || Q <= 0 || R < 0 || (R > 0 && (!fixed || !coef)))
+            fail(LDS_ERR_ARG, "invalid component-diagonal arguments");
+        if (Q > kGenMaxQ || R > kGenMaxR)
+            fail(LDS_ERR_ARG, "component diagonals support at most %d bases and %d fixed effects",
+                 kGenMaxQ, kGenMaxR);
+        Prepared& P = product_image(geno, j0, j1, 1);
+        const int64_t L = j1 - j0, N = P.g.N;
+        // pairs: diagonals first, then lexicographic off-diagonals; kernel
+        // factor 1 on the diagonal, 2 off it (context/spec.py ContextPairIndex)
+        std::vector<int> pq, pr;
+        std::vector<double> kf;
+        for (int q = 0; q < Q; ++q) { pq.push_back(q); pr.push_back(q); kf.push_back(1.0); }
+        for (int q = 0; q < Q - 1; ++q)
+            for (int r = q + 1; r < Q; ++r) { pq.push_back(q); pr.push_back(r); kf.push_back(2.0); }
+        const int Pn = (int)pq.size(), C = K * Pn;
+        DevBuf da, db, df, dc, dq, dr, dk, dn;
+        double* a = da.as<double>((size_t)(L * K));
+        double* b = db.as<double>((size_t)(N * Q));
+        double* f = df.as<double>((size_t)std::max<int64_t>(N * R, 1));
+        double* cf = dc.as<double>((size_t)std::max<int64_t>(L * Q * R, 1));
+        int* qd = dq.as<int>((size_t)Pn);
+        int* rd = dr.as<int>((size_t)Pn);
+        double* kd = dk.as<double>((size_t)Pn);
+        double* nm = dn.as<double>((size_t)(C * N));
+        h2d(a, annot, (size_t)(L * K), c.st);
+        h2d(b, basis, (size_t)(N * Q), c.st);
+        if (R > 0) {
+            h2d(f, fixed, (size_t)(N * R), c.st);
+            h2d(cf, coef, (size_t)(L * Q * R), c.st);
+        }
+        h2d(qd, pq.data(), pq.size(), c.st);
+        h2d(rd, pr.data(), pr.size(), c.st);
+        h2d(kd, kf.data(), kf.size(), c.st);
+        h2d(nm, numerator, (size_t)(C * N), c.st);
+        launch_component_diag(P.g.codes, P.g.nbp, static_cast<double*>(P.d_mean.p),
+                              static_cast<double*>(P.d_sdinv.p), j0, L, N, a, K, b, Q, f, R, cf,
+                              qd, rd, kd, Pn, nm, c.st);
+        ck(cudaGetLastError(), "launch");
+        d2h(numerator, nm, (size_t)(C * N), c.st);
+        ck(cudaStreamSynchronize(c.st), "component diagonal");
     });
 }
 

@@ -168,6 +168,20 @@ template <typename T> void launch_standardize_dosage(T* G, int64_t N, int64_t L,
                                                      double missing, unsigned long long* counts,
                                                      cudaStream_t st);
 
+// Generalized per-variant GxE estimator (lds_generalized.cu): the global
+// variant x probe sign stream (out column-major L x B; root_state = splitmix64
+// of root ^ namespace key ^ the root constant) and the component-kernel
+// diagonals for at most kGenMaxQ context bases and kGenMaxR fixed effects.
+constexpr int kGenMaxQ = 6;
+constexpr int kGenMaxR = 16;
+void launch_global_probes(uint64_t root_state, int64_t v0, int64_t L, int64_t p0, int64_t B,
+                          double* out, cudaStream_t st);
+void launch_component_diag(const uint8_t* codes, int64_t nbp, const double* mean,
+                           const double* sdinv, int64_t j0, int64_t L, int64_t N,
+                           const double* annot, int K, const double* basis, int Q,
+                           const double* fixed, int R, const double* coef, const int* pq,
+                           const int* pr, const double* kf, int P, double* num, cudaStream_t st);
+
 // Phase-2 product checksums (lds_check.cu): u[wl][i] over the n_windows
 // windows of a batch (K super-bins each, V probes from global probe v0), and
 // rhs[2j], rhs[2j+1] += sum_i g_ij u(i), sum_i o_ij u(i) for the rows of each tile.

@@ -44,6 +44,23 @@ class GwPlan:
         check(_lib.load().lds_gw_plan_kernel_ms(self.handle, ptr(buf)))
         return {"weights": buf[0], "phase1": buf[1], "digits": buf[2], "phase2": buf[3]}
 
+    def set_checks(self, on: bool = True) -> None:
+        """Exact integrity checks of the phase-2 products (as WinPlan.set_checks);
+        call before the first execute."""
+        check(_lib.load().lds_gw_plan_set_checks(self.handle, int(bool(on))))
+
+    def check_products(self) -> dict:
+        """Checksums of the last estimate (as WinPlan.check_products)."""
+        n = np.zeros(1, dtype=np.int64)
+        f = np.zeros(1, dtype=np.int64)
+        ms = np.zeros(1)
+        lhs = np.zeros((self.M, 2), dtype=np.uint64)
+        rhs = np.zeros((self.M, 2), dtype=np.uint64)
+        check(_lib.load().lds_gw_plan_check(self.handle, ptr(lhs), ptr(rhs), ptr(n), ptr(f),
+                                            ptr(ms)))
+        return {"mismatches": int(n[0]), "first_snp": int(f[0]), "check_ms": float(ms[0]),
+                "lhs": lhs, "rhs": rhs}
+
     # -- the two halves of an estimate, for callers that exchange the sketch --
     def tiles(self) -> tuple[list[int], int]:
         """Probe counts of the V-tiles and the sketch's row count N_pad."""

@@ -107,3 +107,34 @@ def test_injected_product_errors_are_found(bigger):
     plan.close()
     other.close()
     sess.close()
+
+
+@pytest.mark.parametrize("impute,vtile", [("mean", 0), ("hwe", 16)])
+def test_genome_wide_plan_checks(bigger, impute, vtile):
+    """The same checks on a genome-wide plan (its rows form one window)."""
+    from summit_b200.session import GwSession
+
+    n, m = bigger["n"], bigger["m"]
+    rng = np.random.default_rng(8)
+    annot = (rng.random((m, 3)) < 0.4).astype(float)
+    annot[:, 0] = 1.0
+    sess = GwSession(bigger["rows"], n, impute_mode=impute, impute_seed=4)
+    kw = dict(vtile=vtile) if vtile else {}
+    plain = sess.plan(annot, 40, 100, 13, "rademacher", **kw)
+    checked = sess.plan(annot, 40, 100, 13, "rademacher", **kw)
+    checked.set_checks(True)
+    plain.execute()
+    checked.execute()
+    np.testing.assert_array_equal(plain.results()["ldscore"], checked.results()["ldscore"])
+    r = checked.check_products()
+    assert r["mismatches"] == 0 and r["first_snp"] == -1
+    assert np.count_nonzero(r["lhs"]) > m
+    np.testing.assert_array_equal(r["lhs"], r["rhs"])
+    assert r["check_ms"] > 0.0
+    checked.execute()
+    assert checked.check_products()["mismatches"] == 0
+    with pytest.raises(RuntimeError, match="before the plan's first execute"):
+        checked.set_checks(False)
+    for p in (plain, checked):
+        p.close()
+    sess.close()
