@@ -953,6 +953,151 @@ def gxe_arm(args) -> None:
 
 
 # ---------------------------------------------------------------------------
+# Generalized per-variant GxE two-pass estimator (summit_b200.generalized_gxe):
+# N = 50,000 x M = 100,000, Q = 3 context bases (1, E, 0.3 E^2 + noise), R = 2
+# orthonormal fixed effects, K = 4 continuous annotations (20 % zeros),
+# B = 50 global-variant probes.  One step = pass 1 + pass 2 from the resident
+# image to host results.
+# ---------------------------------------------------------------------------
+GEN_N, GEN_M, GEN_Q, GEN_R, GEN_K, GEN_B = 50_000, 100_000, 3, 2, 4, 50
+GEN_METRIC = "geno x probe TOPS (generalized per-variant GxE two-pass estimator)"
+GEN_WORKLOAD = "generalized_gxe_two_pass_n50k_m100k_q3_r2_k4_b50"
+
+
+def gen_inputs(n: int, m: int, seed: int = 4242):
+    rng = np.random.default_rng(seed)
+    env, cov = rng.normal(size=n), rng.normal(size=n)
+    basis = np.asfortranarray(np.column_stack([np.ones(n), env, 0.3 * env ** 2 + rng.normal(size=n)]))
+    u, _s, _vt = np.linalg.svd(np.column_stack([np.ones(n), cov]), full_matrices=False)
+    annot = rng.uniform(0.1, 1.4, size=(m, GEN_K))
+    annot[rng.random((m, GEN_K)) < 0.2] = 0.0
+    annot[0] = 0.7
+    return basis, np.asfortranarray(u), annot
+
+
+def gen_ops(n: int, annot: np.ndarray, b: int, families: int) -> float:
+    """2 ops per MAC: pass 1 X (sqrt(a) o Z) over the annotation nonzeros,
+    pass 2 X^T of the K * B * families right-hand-side columns."""
+    nnz = float((annot > 0).sum())
+    m, k = annot.shape
+    return 2.0 * n * nnz * b + 2.0 * n * m * k * b * families
+
+
+def generalized_arm(args) -> None:
+    import torch
+
+    local = env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    from summit_b200 import _lib, gwldcore
+    from summit_b200 import generalized_gxe as gg
+    from summit_b200.session import GwSession
+
+    n, m = env_int("LDS_GEN_N", GEN_N), env_int("LDS_GEN_M", GEN_M)
+    bed = gwldcore.synth_bed_rows(n, m, DATA_SEED)
+    basis, fixed, annot = gen_inputs(n, m)
+    spec = gg.GlobalVariantProbeSpec(root_seed=2027, probe_offset=0, probe_count=GEN_B)
+    families = GEN_Q * GEN_Q  # fixed effects: every ordered (t, s)
+    ops = gen_ops(n, annot, GEN_B, families)
+
+    def run(sess):
+        p1, p2 = gg.two_pass(sess, basis, fixed, annot, spec)
+        return p2
+
+    sess = GwSession(bed, n)
+    p2 = run(sess)  # warm-up
+    lib = _lib.load()
+    launches0 = lib.lds_kernel_launches()
+    times = []
+    with Clocks(local) as clk:
+        for _ in range(args.steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            p2 = run(sess)
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t0)
+    launches = int(lib.lds_kernel_launches() - launches0) // max(args.steps, 1)
+    assert np.isfinite(p2.directional_ldscores).all()
+    sec = float(np.median(times))
+    # end to end: host BED rows -> resident image -> both passes -> host results
+    t0 = time.perf_counter()
+    sess2 = GwSession(bed, n)
+    run(sess2)
+    e2e_s = time.perf_counter() - t0
+    sess2.close()
+    line = {
+        "metric": GEN_METRIC, "value": round(ops / sec / 1e12, 3), "unit": "TOPS", "n_gpus": 1,
+        "steps": args.steps, "warmup": 1, "ms_per_step": round(sec * 1e3, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int8-digit exact products, f64 projection, scores and diagonals",
+        "data": "synthetic (seeded HWE/AR(1) generator; global variant x probe signs on device)",
+        "config": {"workload": GEN_WORKLOAD, "N": n, "M": m, "Q": GEN_Q, "R": GEN_R, "K": GEN_K,
+                   "B": GEN_B, "rhs_columns": GEN_K * GEN_B * families,
+                   "timing": "wall clock from the resident image to host results (host FP64 "
+                             "projection and orientation-term set-up included)"},
+        "e2e": {"value": round(ops / e2e_s / 1e12, 3), "unit": "TOPS",
+                "h2d_bytes_per_step": int(bed.nbytes),
+                "d2h_bytes_per_step": int(p2.directional_ldscores.nbytes),
+                "ms_per_step": round(e2e_s * 1e3, 1)},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    if not os.environ.get("LDS_SKIP_CPU_BASELINE"):
+        line["cpu_baseline"] = generalized_cpu_sample(bed, n, basis, fixed, annot, spec, families)
+    sess.close()
+    print(json.dumps(line), flush=True)
+
+
+def generalized_cpu_sample(bed, n, basis, fixed, annot, spec, families) -> dict:
+    """The oracle's dense FP64 restatement of both passes (NumPy / OpenBLAS,
+    all host threads) on the first S SNPs of the workload, as a genome of S
+    SNPs: decode excluded, products, projection and scores timed."""
+    from oracle import generalized_oracle as go
+    from oracle.oracle import Oracle
+    from summit_b200 import generalized_gxe as gg
+
+    s = env_int("LDS_GEN_CPU_SNPS", 2000)
+    X, _m, _i = Oracle().standardize(bed[:s], n, 0, s)
+    a = annot[:s]
+    t0 = time.perf_counter()
+    z = go.global_probes(spec.root_seed, range(s), range(spec.probe_offset,
+                                                         spec.probe_offset + spec.probe_count),
+                         spec.namespace)
+    probe_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    base = go.source_product(X, 0, s, a, z)                   # N x K*B
+    k_count, b_count, q_count = a.shape[1], spec.probe_count, basis.shape[1]
+    src = base.T.reshape(k_count, b_count, n).transpose(0, 2, 1)
+    rhs = np.empty((n, k_count * b_count * families), order="F")
+    fam = [(t, u) for t in range(q_count) for u in range(q_count)]
+    for k in range(k_count):
+        for q in range(q_count):
+            w = basis[:, q, None] * src[k]
+            ctx = w - fixed @ (fixed.T @ w)
+            for f, (t, u) in enumerate(fam):
+                if u == q:
+                    rhs[:, (np.arange(b_count) + k * b_count) * families + f] = basis[:, t, None] * ctx
+    pairs = gg.pair_order(q_count)
+    index = {pr: f for f, pr in enumerate(fam)}
+    off, f1, f2 = [0], [], []
+    for tp in pairs:
+        for sp in pairs:
+            for tl, tr in ((tp[0], tp[0]),) if tp[0] == tp[1] else ((tp[0], tp[1]), (tp[1], tp[0])):
+                for sl, sr in ((sp[0], sp[0]),) if sp[0] == sp[1] else ((sp[0], sp[1]), (sp[1], sp[0])):
+                    f1.append(index[(tr, sl)])
+                    f2.append(index[(tl, sr)])
+            off.append(len(f1))
+    go.pass2_scores(X, rhs, k_count, b_count, families, len(pairs), off, f1, f2,
+                    float(n - fixed.shape[1]), a)
+    sec = time.perf_counter() - t0
+    ops = gen_ops(n, a, b_count, families)
+    return {"value": round(ops / sec / 1e12, 6), "unit": "TOPS", "cores": cpu_threads(),
+            "kind": "port", "sample": f"first {s} SNPs as a genome of {s} SNPs (N={n}); "
+                                      f"oracle/generalized_oracle.py dense FP64 products and "
+                                      f"scores, {sec:.1f} s (probe stream {probe_s:.1f} s, "
+                                      f"decode excluded)"}
+
+
+# ---------------------------------------------------------------------------
 # Biobank-scale workload (config-5 shape): N = 400,000 x M = 800,000 (80 GB of
 # packed codes, resident in HBM, generated on the device), B = 50 +-1 probes.
 # One step = one plain genome-wide estimate (K = 1); the GxE reference build
@@ -1152,7 +1297,7 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["windowed", "gxe", "exact", "biobank"],
+    ap.add_argument("--workload", choices=["windowed", "gxe", "exact", "biobank", "generalized"],
                     default="windowed")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -1166,6 +1311,13 @@ def main() -> None:
         biobank_arm(args)
     elif args.workload == "exact":
         exact_arm(args)
+    elif args.workload == "generalized":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "workload": "generalized",
+                              "unavailable": "the generalized workload has no reference arm; "
+                                             "its cpu_baseline times the oracle port"}))
+            return
+        generalized_arm(args)
     elif args.workload == "gxe":
         if args.impl == "reference":
             sec, sample = gxe_reference_sample(GXE_N, env_int("LDS_GXE_CPU_SNPS", 400),

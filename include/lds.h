@@ -718,6 +718,20 @@ int lds_geno_target_product(int64_t geno, int64_t j0, int64_t j1, const double* 
                             double* out);
 int lds_global_variant_probes(uint64_t root_seed, uint64_t namespace_key, int64_t v0, int64_t L,
                               int64_t p0, int64_t B, double* out);
+/* lds_generalized_pass2: the per-variant pass-2 scores of all M variants in
+ * blocks of variant_block rows.  rhs (N x K*B*F column-major, column
+ * (k*B + b)*F + f: phi_t o contextual source s of annotation k, probe b, for
+ * family f = (t, s)) is uploaded and quantized once; per block the phase-2
+ * tensor-core kernel forms the exact products, and per variant j
+ *   directional[j][tp][k*P + sp] = (1/B) sum over the orientation terms
+ *   t in [term_off[tp*P + sp], term_off[tp*P + sp + 1]) of
+ *   sum_b cross_{term_f1[t]} cross_{term_f2[t]},  cross = X^T rhs / residual_rank,
+ * (directional: M x P x K*P, host) and directed (K*P x K*P) = sum_j a_jk1
+ * directional[j][p1][.] (annot M x K row-major).  K*B*F <= 25,600. */
+int lds_generalized_pass2(int64_t geno, const double* rhs, int K, int B, int F, int P,
+                          const int* term_off, const int* term_f1, const int* term_f2,
+                          double residual_rank, const double* annot, int64_t variant_block,
+                          double* directional, double* directed);
 int lds_generalized_component_diagonal(int64_t geno, int64_t j0, int64_t j1, const double* annot,
                                        int K, const double* basis, int Q, const double* fixed,
                                        int R, const double* coef, double* numerator);

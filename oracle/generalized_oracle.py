@@ -79,3 +79,24 @@ def component_diagonal(X: np.ndarray, j0: int, j1: int, annot_blk, basis, fixed,
         prod = (factor * feats[q] * feats[r]) @ annot_blk   # N x K
         for k in range(annot_blk.shape[1]):
             numerator[k * p_count + p] += prod[:, k]
+
+
+def pass2_scores(X: np.ndarray, rhs: np.ndarray, k_count: int, b_count: int, f_count: int,
+                 p_count: int, term_off, term_f1, term_f2, residual_rank: float,
+                 annot: np.ndarray):
+    """Per-variant pass-2 scores and the directed numerator from dense
+    products (generalized_gxe_pass2.py:600-693): cross = X^T rhs / rr, column
+    (k*B + b)*F + f; directional[j, tp, k*P + sp] = (1/B) sum over the terms of
+    (tp, sp) of sum_b cross[j, (k,b,f1)] cross[j, (k,b,f2)]."""
+    cross = (X.T @ rhs / residual_rank).reshape(X.shape[1], k_count, b_count, f_count)
+    m, c_count = X.shape[1], k_count * p_count
+    directional = np.zeros((m, p_count, c_count))
+    for tp in range(p_count):
+        for sp in range(p_count):
+            acc = np.zeros((m, k_count))
+            for t in range(term_off[tp * p_count + sp], term_off[tp * p_count + sp + 1]):
+                acc += np.einsum("jkb,jkb->jk", cross[:, :, :, term_f1[t]],
+                                 cross[:, :, :, term_f2[t]])
+            directional[:, tp, np.arange(k_count) * p_count + sp] = acc / b_count
+    directed = np.einsum("vk,vpc->kpc", annot, directional).reshape(c_count, c_count)
+    return directional, directed

@@ -89,7 +89,86 @@ __global__ void __launch_bounds__(kDiagThreads)
     }
 }
 
+// Pass-2 scores of one variant block, one CTA per variant row jl: the row's
+// cross sketches cross[c] = s_j cs[c] (G^T y_c - mu_j O^T y_c) / rr from the
+// exact raw digit products (column c = (k * B + b) * F + f of the
+// right-hand side, raw row stride raw_ld), then
+//   out[jl][tp][k * P + sp] = (1 / B) sum over the orientation terms (f1, f2)
+//   of (tp, sp) of sum_b cross[(k B + b) F + f1] cross[(k B + b) F + f2]
+// (generalized_gxe_pass2.py:600-676).
+__global__ void gen_rows_kernel(const long long* __restrict__ raw_g,
+                                const long long* __restrict__ raw_o, int64_t raw_ld,
+                                const double* __restrict__ cs, const double* __restrict__ mean,
+                                const double* __restrict__ sdinv, int64_t j0, double inv_rr, int K,
+                                int B, int F, int P, const int* __restrict__ term_off,
+                                const int* __restrict__ term_f1, const int* __restrict__ term_f2,
+                                double* __restrict__ out) {
+    extern __shared__ double cross[];
+    const int64_t jl = blockIdx.x, j = j0 + jl;
+    const int cols = K * B * F, C = K * P, nout = P * C;
+    const double mu = mean[j], sd = sdinv[j];
+    for (int c = threadIdx.x; c < cols; c += blockDim.x) {
+        const int64_t q = jl * raw_ld + c;
+        cross[c] = sd * cs[c] * ((double)raw_g[q] - mu * (double)raw_o[q]) * inv_rr;
+    }
+    __syncthreads();
+    for (int o = threadIdx.x; o < nout; o += blockDim.x) {
+        const int tp = o / C, c = o - tp * C, k = c / P, sp = c - k * P;
+        double acc = 0.0;
+        for (int t = term_off[tp * P + sp]; t < term_off[tp * P + sp + 1]; ++t) {
+            const double* x1 = cross + (int64_t)k * B * F + term_f1[t];
+            const double* x2 = cross + (int64_t)k * B * F + term_f2[t];
+            double s = 0.0;
+            for (int b = 0; b < B; ++b) s += x1[b * F] * x2[b * F];
+            acc += s;
+        }
+        out[jl * nout + o] = acc / (double)B;
+    }
+}
+
+// directed[c1][c2] += sum_jl a[j0 + jl][k1] rows[jl][p1][c2], c1 = k1 P + p1.
+__global__ void gen_directed_kernel(const double* __restrict__ rows, int64_t L,
+                                    const double* __restrict__ annot, int64_t j0, int K, int P,
+                                    double* __restrict__ directed) {
+    const int C = K * P;
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= C * C) return;
+    const int c1 = idx / C, c2 = idx - c1 * C, k1 = c1 / P, p1 = c1 - k1 * P;
+    double s = 0.0;
+    for (int64_t jl = 0; jl < L; ++jl)
+        s += annot[(j0 + jl) * K + k1] * rows[(jl * P + p1) * C + c2];
+    directed[idx] += s;
+}
+
 }  // namespace
+
+size_t gen_rows_smem_bytes(int cols) { return (size_t)cols * sizeof(double); }
+
+void launch_gen_rows(const long long* raw_g, const long long* raw_o, int64_t raw_ld,
+                     const double* cs, const double* mean, const double* sdinv, int64_t j0,
+                     int64_t L, double inv_rr, int K, int B, int F, int P, const int* term_off,
+                     const int* term_f1, const int* term_f2, double* out, cudaStream_t st) {
+    if (L <= 0) return;
+    const size_t smem = gen_rows_smem_bytes(K * B * F);
+    static std::atomic<unsigned long long> attr{0};
+    once_per_device(attr, [] {
+        cudaFuncSetAttribute(gen_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kGenRowsMaxSmem);
+    });
+    gen_rows_kernel<<<(unsigned)L, 256, smem, st>>>(raw_g, raw_o, raw_ld, cs, mean, sdinv, j0,
+                                                     inv_rr, K, B, F, P, term_off, term_f1,
+                                                     term_f2, out);
+    count_launch();
+}
+
+void launch_gen_directed(const double* rows, int64_t L, const double* annot, int64_t j0, int K,
+                         int P, double* directed, cudaStream_t st) {
+    const int C = K * P;
+    if (L <= 0 || C <= 0) return;
+    gen_directed_kernel<<<(unsigned)((C * C + 255) / 256), 256, 0, st>>>(rows, L, annot, j0, K, P,
+                                                                          directed);
+    count_launch();
+}
 
 void launch_global_probes(uint64_t root_state, int64_t v0, int64_t L, int64_t p0, int64_t B,
                           double* out, cudaStream_t st) {

@@ -5311,6 +5311,101 @@ LDS_API int lds_generalized_component_diagonal(int64_t geno, int64_t j0, int64_t
     });
 }
 
+LDS_API int lds_generalized_pass2(int64_t geno, const double* rhs, int K, int B, int F, int P,
+                                  const int* term_off, const int* term_f1, const int* term_f2,
+                                  double residual_rank, const double* annot,
+                                  int64_t variant_block, double* directional, double* directed) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        ensure_device(c);
+        if (!rhs || !term_off || !term_f1 || !term_f2 || !annot || !directional || !directed ||
+            K <= 0 || B <= 0 || F <= 0 || P <= 0 || variant_block <= 0 || !(residual_rank > 0.0))
+            fail(LDS_ERR_ARG, "invalid generalized pass-2 arguments");
+        const int cols = K * B * F;
+        if (gen_rows_smem_bytes(cols) > (size_t)kGenRowsMaxSmem)
+            fail(LDS_ERR_ARG, "K * B * families = %d right-hand-side columns exceeds %d", cols,
+                 (int)(kGenRowsMaxSmem / sizeof(double)));
+        if (c.slices != 4 || p2_impl() != 1)
+            fail(LDS_ERR_ARG, "generalized products need the tcgen05 kernels with 4 digits");
+        Prepared& P_ = product_image(geno, 0, 1, cols);
+        const Prepared& Pc = P_;
+        const int64_t M = Pc.g.M, N = Pc.g.N, Np = Pc.g.N_pad;
+        const int nterm = term_off[P * P];
+        for (int t = 0; t < nterm; ++t)
+            if (term_f1[t] < 0 || term_f1[t] >= F || term_f2[t] < 0 || term_f2[t] >= F)
+                fail(LDS_ERR_ARG, "orientation term family out of range");
+        // The right-hand side as K2 bins of 64 columns (zero columns pad the
+        // last), quantized to the phase-2 digits once for every block.
+        constexpr int kV2 = 64;
+        const int K2 = (cols + kV2 - 1) / kV2, nc = umma::ncolp_for(kV2);
+        const int64_t ld = (int64_t)K2 * kV2;
+        DevBuf dY, dyq, dcs, dann, dto, df1, df2, ddir, drg, dro, drows, dst;
+        double* Y = dY.as<double>((size_t)(Np * ld));
+        ck(cudaMemsetAsync(Y, 0, sizeof(double) * (size_t)(Np * ld), c.st), "memset");
+        ck(cudaMemcpy2DAsync(Y, sizeof(double) * (size_t)Np, rhs, sizeof(double) * (size_t)N,
+                             sizeof(double) * (size_t)N, (size_t)cols, cudaMemcpyHostToDevice, c.st),
+           "rhs upload");
+        int8_t* yq = dyq.as<int8_t>((size_t)((int64_t)K2 * nc * Np));
+        double* cs = dcs.as<double>((size_t)ld);
+        umma::launch_quantize_y4(Y, N, Np, K2, kV2, nc, yq, cs, c.st);
+        double* ann = dann.as<double>((size_t)(M * K));
+        h2d(ann, annot, (size_t)(M * K), c.st);
+        int* to = dto.as<int>((size_t)(P * P + 1));
+        int* f1 = df1.as<int>((size_t)std::max(nterm, 1));
+        int* f2 = df2.as<int>((size_t)std::max(nterm, 1));
+        h2d(to, term_off, (size_t)(P * P + 1), c.st);
+        h2d(f1, term_f1, (size_t)nterm, c.st);
+        h2d(f2, term_f2, (size_t)nterm, c.st);
+        const int Cc = K * P;
+        double* dd = ddir.as<double>((size_t)(Cc * Cc));
+        ck(cudaMemsetAsync(dd, 0, sizeof(double) * (size_t)(Cc * Cc), c.st), "memset");
+        unsigned* stv = dst.as<unsigned>(1);
+        ck(cudaMemsetAsync(stv, 0, 4, c.st), "memset");
+        const int64_t Lmax = std::min<int64_t>(variant_block, M);
+        long long* rg = drg.as<long long>((size_t)(Lmax * ld));
+        long long* ro = dro.as<long long>((size_t)(Lmax * ld));
+        double* rows = drows.as<double>((size_t)(Lmax * P * Cc));
+        const CUtensorMap tA = make_map_2d(Pc.g.codes, (uint64_t)Pc.g.nbp, (uint64_t)Pc.g.M_pad,
+                                           (uint64_t)Pc.g.nbp, 32, 128, CU_TENSOR_MAP_SWIZZLE_NONE);
+        for (int64_t j0 = 0; j0 < M; j0 += Lmax) {
+            const int64_t j1 = std::min(M, j0 + Lmax), L = j1 - j0;
+            umma::P2UArgs u;
+            u.yq = yq;
+            u.yq_cols = (int64_t)K2 * nc;
+            u.K = K2;
+            u.V = kV2;
+            u.ncolp = nc;
+            u.bins_per_cta = umma::p2_bins_per_cta(nc, K2);
+            u.ngroups = (u.bins_per_cta * nc + 255) / 256;
+            u.box_rows = std::min(256, u.bins_per_cta * nc);
+            u.nkt = (int)(Np / 128);
+            u.M = M;
+            u.j0 = j0;
+            u.j1 = j1;
+            u.out_row0 = j0;
+            u.colscale = cs;
+            u.mean = static_cast<double*>(Pc.d_mean.p);
+            u.sdinv = static_cast<double*>(Pc.d_sdinv.p);
+            u.status = stv;
+            u.raw_g = rg;
+            u.raw_o = ro;
+            umma::launch_p2_umma(tA, u, c.st);
+            launch_gen_rows(rg, ro, ld, cs, static_cast<double*>(Pc.d_mean.p),
+                            static_cast<double*>(Pc.d_sdinv.p), j0, L, 1.0 / residual_rank, K, B, F,
+                            P, to, f1, f2, rows, c.st);
+            launch_gen_directed(rows, L, ann, j0, K, P, dd, c.st);
+            ck(cudaGetLastError(), "launch");
+            d2h(directional + j0 * P * Cc, rows, (size_t)(L * P * Cc), c.st);
+        }
+        unsigned hst = 0;
+        d2h(directed, dd, (size_t)(Cc * Cc), c.st);
+        d2h(&hst, stv, 1, c.st);
+        ck(cudaStreamSynchronize(c.st), "generalized pass 2");
+        if (hst) fail(LDS_ERR_CUDA, "phase-2 tensor-core pipeline wait timed out (code %u)", hst);
+    });
+}
+
 LDS_API int lds_gxe_destroy(int64_t gxe) {
     return guarded([&] {
         Context& c = ctx();

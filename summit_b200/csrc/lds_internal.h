@@ -176,6 +176,17 @@ constexpr int kGenMaxQ = 6;
 constexpr int kGenMaxR = 16;
 void launch_global_probes(uint64_t root_state, int64_t v0, int64_t L, int64_t p0, int64_t B,
                           double* out, cudaStream_t st);
+// Pass-2 scores of a variant block (one CTA per row; the row's K*B*F cross
+// sketches in shared memory, at most kGenRowsMaxSmem bytes) and the directed
+// numerator accumulation.
+constexpr int kGenRowsMaxSmem = 200 * 1024;
+size_t gen_rows_smem_bytes(int cols);
+void launch_gen_rows(const long long* raw_g, const long long* raw_o, int64_t raw_ld,
+                     const double* cs, const double* mean, const double* sdinv, int64_t j0,
+                     int64_t L, double inv_rr, int K, int B, int F, int P, const int* term_off,
+                     const int* term_f1, const int* term_f2, double* out, cudaStream_t st);
+void launch_gen_directed(const double* rows, int64_t L, const double* annot, int64_t j0, int K,
+                         int P, double* directed, cudaStream_t st);
 void launch_component_diag(const uint8_t* codes, int64_t nbp, const double* mean,
                            const double* sdinv, int64_t j0, int64_t L, int64_t N,
                            const double* annot, int K, const double* basis, int Q,

@@ -342,8 +342,9 @@ __global__ void __launch_bounds__(kThreads, 1)
                     }
                     if (a.raw_g) {
                         if (j < jend) {
-                            a.raw_g[(j - a.out_row0) * a.V + v] = TG;
-                            a.raw_o[(j - a.out_row0) * a.V + v] = TO;
+                            const int64_t ro = ((j - a.out_row0) * a.K + k0 + bo) * a.V + v;
+                            a.raw_g[ro] = TG;
+                            a.raw_o[ro] = TO;
                         }
                         continue;
                     }

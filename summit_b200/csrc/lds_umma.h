@@ -38,7 +38,8 @@ struct P2UArgs {
     const int8_t* yq = nullptr;          // sketch digits (digit_offset layout)
     int64_t yq_cols = 0;                 // columns of yq (super-bins x ncolp)
     // Verification mode: write the exact recombined products G^T y and O^T y
-    // per (SNP, probe) to raw_g / raw_o ((j - out_row0) * V + v), no epilogue.
+    // per (SNP, bin, probe) to raw_g / raw_o (((j - out_row0) * K + k) * V + v),
+    // no epilogue.
     long long* raw_g = nullptr;
     long long* raw_o = nullptr;
     // Optional tile table (windowed estimates): CTA x processes rows

@@ -107,6 +107,22 @@ def _component_diagonal(session, j0: int, j1: int, annot_blk, basis, fixed, coef
         ptr(np.ascontiguousarray(coef)) if r_count else None, ptr(numerator)))
 
 
+def _pass2_scores(session, rhs, k_count, b_count, f_count, p_count, term_off, term_f1, term_f2,
+                  residual_rank, weights, block):
+    """(directional M x P x K*P, directed K*P x K*P) of all variants: the
+    right-hand side quantized once, the exact products and the per-variant
+    orientation products on the device (lds_generalized_pass2)."""
+    m, c_count = session.M, k_count * p_count
+    directional = np.empty((m, p_count, c_count))
+    directed = np.empty((c_count, c_count))
+    r = np.asfortranarray(rhs, dtype=np.float64)
+    a = np.ascontiguousarray(weights, dtype=np.float64)
+    check(_lib.load().lds_generalized_pass2(
+        session.handle, ptr(r), k_count, b_count, f_count, p_count, ptr(term_off), ptr(term_f1),
+        ptr(term_f2), float(residual_rank), ptr(a), int(block), ptr(directional), ptr(directed)))
+    return directional, directed
+
+
 def pair_order(q_count: int) -> tuple[tuple[int, int], ...]:
     """Diagonal-first unordered basis pairs (context/spec.py ContextPairIndex)."""
     return tuple((q, q) for q in range(q_count)) + tuple(
@@ -238,36 +254,35 @@ def pass2(session, pass1_result: GeneralizedPass1Result, basis, fixed_effect_bas
             rhs[:, cols] = basis[:, t, None] * sources[k, s]
     weighted_fixed = np.asfortranarray(
         (basis[:, :, None] * fixed[:, None, :]).reshape(n, q_count * r_count)) if r_count else None
-    directional = np.empty((m, p_count, c_count))
-    directed = np.zeros((c_count, c_count))
+    # Orientation terms of every (target pair, source pair): products of the
+    # cross sketches of families (t_right, s_left) and (t_left, s_right).
+    family = {}
+    for f, (u, v) in enumerate(families):
+        family[(u, v)] = f
+        if symmetric_cross:
+            family[(v, u)] = f
+    term_off, term_f1, term_f2 = [0], [], []
+    for target_pair in pairs:
+        for source_pair in pairs:
+            for tl, tr in _orientations(target_pair):
+                for sl, sr in _orientations(source_pair):
+                    term_f1.append(family[(tr, sl)])
+                    term_f2.append(family[(tl, sr)])
+            term_off.append(len(term_f1))
     diag_num = np.zeros((c_count, n))
     for j0 in range(0, m, variant_block_width):
         j1 = min(m, j0 + variant_block_width)
-        L = j1 - j0
         coef = None
         if r_count:
             cf = _target_product(session, j0, j1, weighted_fixed)
-            coef = np.ascontiguousarray(cf.reshape(L, q_count, r_count))
+            coef = np.ascontiguousarray(cf.reshape(j1 - j0, q_count, r_count))
         _component_diagonal(session, j0, j1, weights[j0:j1], basis, fixed, coef, diag_num)
-        cross_raw = _target_product(session, j0, j1, rhs)
-        unique = (cross_raw / float(residual_rank)).reshape(L, k_count, b_count, f_count)
-        cross = {}
-        for f, (u, v) in enumerate(families):
-            cross[(u, v)] = unique[:, :, :, f]          # L x K x B
-            if symmetric_cross and u != v:
-                cross[(v, u)] = cross[(u, v)]
-        lrow = np.zeros((L, p_count, c_count))
-        for tp, target_pair in enumerate(pairs):
-            for sp, source_pair in enumerate(pairs):
-                acc = np.zeros((L, k_count))
-                for tl, tr in _orientations(target_pair):
-                    for sl, sr in _orientations(source_pair):
-                        acc += np.einsum("lkb,lkb->lk", cross[(tr, sl)], cross[(tl, sr)])
-                lrow[:, tp, np.arange(k_count) * p_count + sp] = acc / float(b_count)
-        if not np.all(np.isfinite(lrow)):
-            raise RuntimeError("per-variant directional scores are non-finite")
-        directional[j0:j1] = lrow
-        directed += np.einsum("vk,vpc->kpc", weights[j0:j1], lrow).reshape(c_count, c_count)
+    directional, directed = _pass2_scores(
+        session, rhs, k_count, b_count, f_count, p_count, np.asarray(term_off, np.int32),
+        np.asarray(term_f1, np.int32), np.asarray(term_f2, np.int32), float(residual_rank),
+        weights, variant_block_width)
+    if not np.all(np.isfinite(directional)):
+        raise RuntimeError("per-variant directional scores are non-finite")
     pre_abs = float(np.max(np.abs(directed - directed.T), initial=0.0))
     pre_rel = pre_abs / max(1.0, float(np.max(np.abs(directed), initial=0.0)))
     symmetric = 0.5 * (directed + directed.T)
