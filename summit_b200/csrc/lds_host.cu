@@ -5328,9 +5328,8 @@ LDS_API int lds_generalized_pass2(int64_t geno, const double* rhs, int K, int B,
                  (int)(kGenRowsMaxSmem / sizeof(double)));
         if (c.slices != 4 || p2_impl() != 1)
             fail(LDS_ERR_ARG, "generalized products need the tcgen05 kernels with 4 digits");
-        Prepared& P_ = product_image(geno, 0, 1, cols);
-        const Prepared& Pc = P_;
-        const int64_t M = Pc.g.M, N = Pc.g.N, Np = Pc.g.N_pad;
+        const Prepared& img = product_image(geno, 0, 1, cols);
+        const int64_t M = img.g.M, N = img.g.N, Np = img.g.N_pad;
         const int nterm = term_off[P * P];
         for (int t = 0; t < nterm; ++t)
             if (term_f1[t] < 0 || term_f1[t] >= F || term_f2[t] < 0 || term_f2[t] >= F)
@@ -5366,8 +5365,8 @@ LDS_API int lds_generalized_pass2(int64_t geno, const double* rhs, int K, int B,
         long long* rg = drg.as<long long>((size_t)(Lmax * ld));
         long long* ro = dro.as<long long>((size_t)(Lmax * ld));
         double* rows = drows.as<double>((size_t)(Lmax * P * Cc));
-        const CUtensorMap tA = make_map_2d(Pc.g.codes, (uint64_t)Pc.g.nbp, (uint64_t)Pc.g.M_pad,
-                                           (uint64_t)Pc.g.nbp, 32, 128, CU_TENSOR_MAP_SWIZZLE_NONE);
+        const CUtensorMap tA = make_map_2d(img.g.codes, (uint64_t)img.g.nbp, (uint64_t)img.g.M_pad,
+                                           (uint64_t)img.g.nbp, 32, 128, CU_TENSOR_MAP_SWIZZLE_NONE);
         for (int64_t j0 = 0; j0 < M; j0 += Lmax) {
             const int64_t j1 = std::min(M, j0 + Lmax), L = j1 - j0;
             umma::P2UArgs u;
@@ -5385,14 +5384,14 @@ LDS_API int lds_generalized_pass2(int64_t geno, const double* rhs, int K, int B,
             u.j1 = j1;
             u.out_row0 = j0;
             u.colscale = cs;
-            u.mean = static_cast<double*>(Pc.d_mean.p);
-            u.sdinv = static_cast<double*>(Pc.d_sdinv.p);
+            u.mean = static_cast<double*>(img.d_mean.p);
+            u.sdinv = static_cast<double*>(img.d_sdinv.p);
             u.status = stv;
             u.raw_g = rg;
             u.raw_o = ro;
             umma::launch_p2_umma(tA, u, c.st);
-            launch_gen_rows(rg, ro, ld, cs, static_cast<double*>(Pc.d_mean.p),
-                            static_cast<double*>(Pc.d_sdinv.p), j0, L, 1.0 / residual_rank, K, B, F,
+            launch_gen_rows(rg, ro, ld, cs, static_cast<double*>(img.d_mean.p),
+                            static_cast<double*>(img.d_sdinv.p), j0, L, 1.0 / residual_rank, K, B, F,
                             P, to, f1, f2, rows, c.st);
             launch_gen_directed(rows, L, ann, j0, K, P, dd, c.st);
             ck(cudaGetLastError(), "launch");
