@@ -183,33 +183,36 @@ def pass1(session, basis, fixed_effect_basis, annotations, probe_spec: GlobalVar
         raise ValueError("variant_block_width must be positive")
     n, m = session.N, session.M
     k_count, q_count, b_count = weights.shape[1], basis.shape[1], probe_spec.probe_count
-    base = np.zeros((k_count, n, b_count))
+    # Sources are kept as B x N rows (the layout the device returns and pass 2
+    # reads); the results expose the reference's N x B views.
+    base = np.zeros((k_count, b_count, n))
     for j0 in range(0, m, variant_block_width):
         j1 = min(m, j0 + variant_block_width)
         z = global_variant_probes(probe_spec, j0, j1 - j0)
         out = _source_product(session, j0, j1, weights[j0:j1], z)
-        base += out.T.reshape(k_count, b_count, n).transpose(0, 2, 1)
-    contextual = np.empty((k_count, q_count, n, b_count))
+        base += out.T.reshape(k_count, b_count, n)
+    contextual = np.empty((k_count, q_count, b_count, n))
     max_abs = max_rel = 0.0
     for k in range(k_count):
         for q in range(q_count):
-            weighted = basis[:, q, None] * base[k]
+            weighted = base[k] * basis[:, q]
             if not fixed.shape[1]:
                 contextual[k, q] = weighted
                 continue
-            projected = weighted - fixed @ (fixed.T @ weighted)
+            projected = weighted - (weighted @ fixed) @ fixed.T
             contextual[k, q] = projected
-            leakage = fixed.T @ projected
+            leakage = projected @ fixed
             max_abs = max(max_abs, float(np.max(np.abs(leakage), initial=0.0)))
             max_rel = max(max_rel, float(np.linalg.norm(leakage)
                                          / max(1.0, float(np.linalg.norm(projected)))))
     if max_rel > projection_tolerance:
         raise RuntimeError("contextual source projection leakage exceeds its tolerance")
+    contextual = contextual.transpose(0, 1, 3, 2)
     pairs = pair_order(q_count)
     components = tuple((k, p) for k in range(k_count) for p in range(len(pairs)))
     contextual.setflags(write=False)
     return GeneralizedPass1Result(contextual, masses, pairs, components, max_abs, max_rel,
-                                  base if retain_base_sources else None)
+                                  base.transpose(0, 2, 1) if retain_base_sources else None)
 
 
 @dataclass(frozen=True)
@@ -247,11 +250,14 @@ def pass2(session, pass1_result: GeneralizedPass1Result, basis, fixed_effect_bas
                      for v in range(u if symmetric_cross else 0, q_count))
     f_count = len(families)
     # rhs column (k * B + b) * F + f = phi_t o sources[k, s][:, b] for family f = (t, s)
-    rhs = np.empty((n, k_count * b_count * f_count), order="F")
+    rows = np.swapaxes(sources, 2, 3)   # K x Q x B x N (contiguous for pass-1 results)
+    # (K, B, F, N) in C order is exactly the column-major N x K*B*F layout
+    # (column (k*B + b)*F + f), filled by contiguous B x N blocks.
+    slab = np.empty((k_count, b_count, f_count, n))
     for k in range(k_count):
         for f, (t, s) in enumerate(families):
-            cols = (np.arange(b_count) + k * b_count) * f_count + f
-            rhs[:, cols] = basis[:, t, None] * sources[k, s]
+            np.multiply(rows[k, s], basis[:, t], out=slab[k, :, f, :])
+    rhs = slab.reshape(k_count * b_count * f_count, n).T
     weighted_fixed = np.asfortranarray(
         (basis[:, :, None] * fixed[:, None, :]).reshape(n, q_count * r_count)) if r_count else None
     # Orientation terms of every (target pair, source pair): products of the
