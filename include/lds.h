@@ -331,6 +331,16 @@ int lds_win_plan_set_tiling(int64_t plan, int p1_sb_per_cta);
  * differ, first_snp the first (-1 if none), check_ms the check kernels' time
  * in the last estimate.  lds_check_vectors is that host comparison alone (for
  * checksums a caller copied or stored). */
+/* Bounds-checked build (python -m summit_b200.build --checked, which writes
+ * liblds_checked.so; no reference counterpart, it stands in for the
+ * reference's sanitizer builds, CMakeLists.txt:476-515): the tensor-core
+ * kernels check their tile, bin, sketch-column, member-row and output indices,
+ * and a failed check records its code in a device error word and skips the
+ * access instead of trapping.  lds_checked_build: 1 in that build, 0 otherwise.
+ * lds_checked_errors: the first failed check's code since the last call (0:
+ * none; always 0 in the ordinary build), then clears it. */
+int lds_checked_build(void);
+int lds_checked_errors(unsigned* code_out);
 int lds_win_plan_set_checks(int64_t plan, int on);
 /* The same checks on a genome-wide plan (lds_gw_plan_create; the tcgen05 path):
  * its rows form one window. */

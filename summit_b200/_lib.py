@@ -12,7 +12,10 @@ from pathlib import Path
 import numpy as np
 
 PKG = Path(__file__).resolve().parent
-LIB_PATH = PKG / "liblds.so"
+# SUMMIT_B200_CHECKED=1 loads the bounds-checked build (python -m
+# summit_b200.build --checked) instead.
+LIB_PATH = PKG / ("liblds_checked.so" if os.environ.get("SUMMIT_B200_CHECKED") == "1"
+                  else "liblds.so")
 
 LDS_DIST = {"rademacher": 0, "gaussian": 1, "normal": 1, "spherical": 2}
 LDS_IMPUTE = {"mean": 0, "hwe": 1}
@@ -59,6 +62,8 @@ SIGNATURES: dict[str, tuple] = {
     "lds_gw_plan_check": (_int, [_i64, _p, _p, _p, _p, _p]),
     "lds_win_plan_check": (_int, [_i64, _p, _p, _p, _p, _p]),
     "lds_check_vectors": (_int, [_p, _p, _i64, _p, _p]),
+    "lds_checked_build": (_int, []),
+    "lds_checked_errors": (_int, [_p]),
     "lds_geno_source_product": (_int, [_i64, _i64, _i64, _p, _i64, _p, _i64, _p]),
     "lds_geno_target_product": (_int, [_i64, _i64, _i64, _p, _i64, _p]),
     "lds_global_variant_probes": (_int, [_u64, _u64, _i64, _i64, _i64, _i64, _p]),

@@ -227,6 +227,7 @@ struct Context {
     int device = -1;
     cudaStream_t st = nullptr;
     cudaEvent_t ev[8];
+    unsigned* checked_err = nullptr;  // bounds-checked build: first failed index check
     std::list<std::unique_ptr<Prepared>> cache;  // most recent first
     DevBuf raw, rows_dev, hwe_q0, hwe_q01, hwe_sb, counts_dev, units_dev;
     // Image preparation stream of the streamed one-call windowed estimate
@@ -264,6 +265,13 @@ void ensure_device(Context& c) {
     ck(cudaGetDevice(&c.device), "cudaGetDevice");
     ck(cudaStreamCreateWithFlags(&c.st, cudaStreamNonBlocking), "cudaStreamCreate");
     for (auto& e : c.ev) ck(cudaEventCreate(&e), "cudaEventCreate");
+#ifdef LDS_CHECKED
+    // The bounds-checked build's device error word, published to every file's
+    // copy of the pointer.
+    ck(cudaMalloc(&c.checked_err, sizeof(unsigned)), "checked error word");
+    ck(cudaMemset(c.checked_err, 0, sizeof(unsigned)), "checked error word");
+    for (CheckedErrSetter f : checked_err_setters()) ck(f(c.checked_err), "checked error word");
+#endif
     c.ready = true;
 }
 
@@ -1975,6 +1983,7 @@ void plan_enqueue_phase1(Context& c, GwPlan& pl, size_t ti, double* y, cudaEvent
         pa.colscale = w.colscale;
         pa.Y = y;
         pa.status = static_cast<unsigned*>(pl.status.p);
+        pa.m_pad = P.g.M_pad;
         umma::launch_p1_umma(t.tmW, pa, P.g.N_pad, c.st);
     } else {
         launch_p1_weights(w, static_cast<double*>(P.d_mean.p), static_cast<double*>(P.d_sdinv.p),
@@ -2027,6 +2036,7 @@ void plan_enqueue_phase2(Context& c, GwPlan& pl, size_t ti, const double* y, cud
         }
         u.yq = static_cast<const int8_t*>(pl.yq.p);
         u.yq_cols = K * nc;
+        u.accum_elems = M * K;
         int v0 = 0;
         for (size_t q = 0; q < ti; ++q) v0 += pl.tiles[q]->V;
         if (pl.check) {
@@ -2204,6 +2214,13 @@ struct WinPlan {
         Csr csr;
         DevBuf rowind, sc, binoff, tiles;
         int64_t ntiles = 0;                // 128-SNP tiles
+        // Phase-2 CTA order per bins-per-CTA value work_nb[i]: window by
+        // window, chunks of kWorkBinChunk bin groups, the window's tiles, the
+        // chunk's bin groups (a tile's packed codes and a (window, bin)
+        // sketch stay in L2 while the CTAs that share them run).
+        std::vector<int> work_nb;
+        std::vector<std::unique_ptr<DevBuf>> work;
+        std::vector<int64_t> n_work;
     };
     std::vector<Batch> batches;
     std::vector<DevBuf> z;              // per V-tile, M x V FP64 probes
@@ -2381,11 +2398,32 @@ std::unique_ptr<WinPlan> win_plan_create(Context& c, std::shared_ptr<Prepared> P
         h2d(b.sc.as<double>(nm), scv.data(), scv.size(), c.st);
         h2d(b.binoff.as<int64_t>(cs.bin_off.size()), cs.bin_off.data(), cs.bin_off.size(), c.st);
         std::vector<int4> tiles;
-        for (int64_t w = b.w0; w < b.w1; ++w)
+        std::vector<int64_t> tile_begin;   // first tile of each window of the batch
+        for (int64_t w = b.w0; w < b.w1; ++w) {
+            tile_begin.push_back((int64_t)tiles.size());
             for (int64_t j = ws[w]; j < ws[w + 1]; j += 128)
                 tiles.push_back(make_int4((int)j, (int)ws[w + 1], (int)((w - b.w0) * K), 0));
+        }
+        tile_begin.push_back((int64_t)tiles.size());
         b.ntiles = (int64_t)tiles.size();
         h2d(b.tiles.as<int4>(tiles.size()), tiles.data(), tiles.size(), c.st);
+        constexpr int kWorkBinChunk = 4;
+        for (int V : pl->vt) {
+            const int nb = umma::p2_bins_per_cta(umma::ncolp_for(V), (int)K);
+            if (std::find(b.work_nb.begin(), b.work_nb.end(), nb) != b.work_nb.end()) continue;
+            const int groups = (int)((K + nb - 1) / nb);
+            std::vector<int2> order;
+            for (size_t w = 0; w + 1 < tile_begin.size(); ++w)
+                for (int g0 = 0; g0 < groups; g0 += kWorkBinChunk)
+                    for (int64_t t = tile_begin[w]; t < tile_begin[w + 1]; ++t)
+                        for (int g = g0; g < std::min(groups, g0 + kWorkBinChunk); ++g)
+                            order.push_back(make_int2((int)t, g));
+            auto buf = std::make_unique<DevBuf>();
+            h2d(buf->as<int2>(order.size()), order.data(), order.size(), c.st);
+            b.work_nb.push_back(nb);
+            b.work.push_back(std::move(buf));
+            b.n_work.push_back((int64_t)order.size());
+        }
         ck(cudaStreamSynchronize(c.st), "window batch upload");
         max_ksup = std::max(max_ksup, b.ksup);
         max_wq = std::max(max_wq, b.ksup * 2 * ncmax * b.lmax);
@@ -2541,6 +2579,7 @@ void win_enqueue(Context& c, WinPlan& pl) {
             pa.yq = static_cast<int8_t*>(pl.yq->p);
             pa.ycolscale = static_cast<double*>(pl.ycs.p);
             pa.yshift = static_cast<int*>(pl.yshift.p);
+            pa.m_pad = P.g.M_pad;
             umma::launch_p1_umma(tmW, pa, Np, c.st);
             ck(cudaEventRecordWithFlags(pl.ev[(size_t)e++], c.st, cudaEventRecordExternal), "event");
             // (sketch digits were written by phase 1's epilogue; their column
@@ -2583,7 +2622,17 @@ void win_enqueue(Context& c, WinPlan& pl) {
                 u.snp_missing = static_cast<const uint8_t*>(P.d_missing.p);
                 u.colsum = colsum;
             }
+            u.accum_elems = (int64_t)MK;
             u.tiles = static_cast<int4*>(b.tiles.p);
+            static const bool grid_order = [] {
+                const char* e = std::getenv("LDS_P2_GRID_ORDER");
+                return e && std::atoi(e) != 0;
+            }();
+            for (size_t q = 0; q < b.work_nb.size() && !grid_order; ++q)
+                if (b.work_nb[q] == nb) {
+                    u.work = static_cast<const int2*>(b.work[q]->p);
+                    u.n_work = b.n_work[q];
+                }
             if (pl.check) {
                 u.chk = static_cast<unsigned long long*>(pl.chk_lhs.p);
                 u.chk_v0 = pl.voff(ti);
@@ -3507,6 +3556,11 @@ static std::vector<WaitLimitSetter>& wait_limit_setters() {
     return v;
 }
 void register_wait_limit_setter(WaitLimitSetter f) { wait_limit_setters().push_back(f); }
+std::vector<CheckedErrSetter>& checked_err_setters() {
+    static std::vector<CheckedErrSetter> v;
+    return v;
+}
+void register_checked_err_setter(CheckedErrSetter f) { checked_err_setters().push_back(f); }
 cudaError_t set_wait_limit_all(long long iters) {
     cudaError_t first = cudaSuccess;
     for (WaitLimitSetter f : wait_limit_setters()) {
@@ -3579,6 +3633,27 @@ LDS_API int lds_set_wait_limit(long long iters) {
 }
 
 LDS_API long long lds_get_wait_limit(void) { return g_wait_limit.load(); }
+
+LDS_API int lds_checked_build(void) {
+#ifdef LDS_CHECKED
+    return 1;
+#else
+    return 0;
+#endif
+}
+
+LDS_API int lds_checked_errors(unsigned* code_out) {
+    Context& c = ctx();
+    std::lock_guard<std::mutex> lk(c.mu);
+    return guarded([&] {
+        if (!code_out) fail(LDS_ERR_ARG, "null output");
+        *code_out = 0;
+        if (!c.ready || !c.checked_err) return;
+        ck(cudaStreamSynchronize(c.st), "sync");
+        ck(cudaMemcpy(code_out, c.checked_err, sizeof(unsigned), cudaMemcpyDeviceToHost), "read");
+        ck(cudaMemset(c.checked_err, 0, sizeof(unsigned)), "clear");
+    });
+}
 
 LDS_API int lds_selftest_wait_timeout(unsigned* status_out) {
     Context& c = ctx();

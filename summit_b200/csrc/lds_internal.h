@@ -4,6 +4,7 @@
 #include <atomic>
 #include <cstdint>
 #include <string>
+#include <vector>
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -352,6 +353,11 @@ using WaitLimitSetter = cudaError_t (*)(long long);
 void register_wait_limit_setter(WaitLimitSetter f);
 // Calls every registered setter; returns the first error.
 cudaError_t set_wait_limit_all(long long iters);
+// Bounds-checked builds (-DLDS_CHECKED): setters of the per-file device
+// pointers to the error word that failed index checks write (lds_tc.cuh).
+using CheckedErrSetter = cudaError_t (*)(unsigned*);
+void register_checked_err_setter(CheckedErrSetter f);
+std::vector<CheckedErrSetter>& checked_err_setters();
 // Self-test of the bounded wait (lds_umma.cu): one thread waits on an
 // mbarrier that nothing arrives at; *status_dev = 1 when the wait ran out,
 // 2 if it (wrongly) completed.

@@ -174,6 +174,27 @@ __device__ __forceinline__ void decode_row_sw128(uint4 p0, uint4 p1, uint8_t* gR
     }
 }
 
+// Index checks of the bounds-checked build (-DLDS_CHECKED): a failed check
+// records its code in the library's device error word (first failure wins)
+// and evaluates false, and the caller skips the access instead of trapping.
+// In ordinary builds in_range is true and the checks compile away.
+#ifdef LDS_CHECKED
+static __constant__ unsigned* c_checked_err = nullptr;
+__device__ __forceinline__ bool in_range(bool ok, unsigned code) {
+    if (!ok && c_checked_err) atomicCAS(c_checked_err, 0u, code);
+    return ok;
+}
+static inline cudaError_t set_checked_err_here(unsigned* p) {
+    return cudaMemcpyToSymbol(c_checked_err, &p, sizeof p);
+}
+struct CheckedErrRegistrar {
+    CheckedErrRegistrar() { register_checked_err_setter(&set_checked_err_here); }
+};
+static CheckedErrRegistrar g_checked_err_registrar;
+#else
+__device__ __forceinline__ bool in_range(bool, unsigned) { return true; }
+#endif
+
 // Registers set_wait_limit_here of the including file with the library, so
 // that lds_set_wait_limit reaches every copy of c_wait_limit.
 struct WaitLimitRegistrar {

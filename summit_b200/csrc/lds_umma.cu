@@ -94,13 +94,16 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     // This CTA's bins: k0 .. k0 + nbk - 1, sharing each decoded genotype tile;
     // their sketch columns are consecutive (bin-major), one TMA box for all.
-    const int k0 = blockIdx.y * a.bins_per_cta;
+    // (tile, bin group) of this CTA: the grid's (x, y), or entry x of the work
+    // order when one is given.
+    const int2 wk = a.work ? a.work[blockIdx.x] : make_int2((int)blockIdx.x, (int)blockIdx.y);
+    const int k0 = wk.y * a.bins_per_cta;
     const int nbk = min(a.bins_per_cta, a.K - k0);
     const int cols = a.bins_per_cta * a.ncolp;
     int64_t jt0, jend;
     int sb = 0;  // super-bin base of this tile's window
     if (a.tiles) {
-        const int4 t = a.tiles[blockIdx.x];
+        const int4 t = a.tiles[wk.x];
         jt0 = t.x;
         jend = t.y;
         sb = t.z;
@@ -109,6 +112,13 @@ __global__ void __launch_bounds__(kThreads, 1)
         jend = a.j1;
     }
     const int kb = sb + k0;  // first super-bin of this CTA
+    // Bounds-checked build: this CTA's tile, bins and sketch columns, before
+    // any barrier or tensor memory is touched (a failing CTA only returns).
+    if (!in_range(!a.tiles || (wk.x >= 0 && (int64_t)wk.x < a.j1), 0x2001u) ||
+        !in_range(wk.y >= 0 && k0 < a.K, 0x2002u) ||
+        !in_range(jt0 >= 0 && jend <= a.M, 0x2003u) ||
+        !in_range(a.yq_cols == 0 || ((int64_t)kb + nbk) * a.ncolp <= a.yq_cols, 0x2004u))
+        return;
 
     if (tid == 0) {
         for (int s = 0; s < kPkStages; ++s) {
@@ -253,6 +263,8 @@ __global__ void __launch_bounds__(kThreads, 1)
                 if (!(nonfinite || (extreme && a.drop_extreme))) {
                     if (upd < 0.0) upd = 0.0;
                     const int64_t o = (j - a.out_row0) * a.K + k0 + cur;
+                    if (!in_range(a.accum_elems == 0 || (o >= 0 && o < a.accum_elems), 0x2005u))
+                        return;
                     if (a.accum2) {
                         a.accum[o] += run2 * ls;
                         a.accum2[o] += run2b * ls;
@@ -546,6 +558,7 @@ void launch_p2_umma(const CUtensorMap& tmA, const P2UArgs& a, cudaStream_t st) {
     // With a tile table, j0 is unused and j1 - j0 carries the number of tiles.
     const int nb = a.bins_per_cta > 0 ? a.bins_per_cta : 1;
     dim3 grid((unsigned)(a.tiles ? rows : (rows + kBM - 1) / kBM), (unsigned)((a.K + nb - 1) / nb));
+    if (a.work) grid = dim3((unsigned)a.n_work, 1);
     p2_umma_kernel<<<grid, kThreads, smem, st>>>(tmA, a);
     count_launch();
 }

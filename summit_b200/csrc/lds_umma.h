@@ -66,6 +66,14 @@ struct P2UArgs {
     // the exact products T_G and T_O of SNP row j (wrapping mod 2^64).
     unsigned long long* chk = nullptr;
     int chk_v0 = 0;
+    // Optional CTA order (tile-table mode): CTA x processes tile work[x].x with
+    // bin group work[x].y (n_work entries, the grid), instead of tile
+    // blockIdx.x and bin group blockIdx.y.
+    const int2* work = nullptr;
+    int64_t n_work = 0;
+    // Extent of accum / accum2 / mc in elements, read by the bounds-checked
+    // build's output checks (0: unchecked).
+    int64_t accum_elems = 0;
 };
 
 // Bins that share one CTA in phase 2: as many whole bins as fit 256 columns.
@@ -95,6 +103,7 @@ struct P1UArgs {
     int8_t* yq = nullptr;
     const double* ycolscale = nullptr;
     const int* yshift = nullptr;        // K*V digit shifts eW - eY (from the weight kernel)
+    int64_t m_pad = 0;                  // image rows, for the bounds-checked build (0: unchecked)
 };
 
 struct P1UWeights {

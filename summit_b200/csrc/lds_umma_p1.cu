@@ -176,7 +176,9 @@ __global__ void __launch_bounds__(p1::kThreads, 1)
         auto cursor_row = [&]() -> int64_t {  // rowind of the cursor's step, or -1 past the end
             while (pk < kb1 && nkt_of(pk) == 0) { ++pk; pg = 0; pkt = 0; }
             if (pk >= kb1) return -1;
-            const int64_t row = a.rowind[a.bin_off[pk] + (int64_t)pkt * kBK + t];
+            int64_t row = a.rowind[a.bin_off[pk] + (int64_t)pkt * kBK + t];
+            // bounds-checked build: a member row outside the image is not gathered
+            if (!in_range(a.m_pad == 0 || (row >= 0 && row < a.m_pad), 0x1001u)) row = -2;
             if (++pkt == nkt_of(pk)) {
                 pkt = 0;
                 if (++pg == a.ngroups) { pg = 0; ++pk; }

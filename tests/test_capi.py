@@ -65,3 +65,21 @@ def test_wait_limit_argument_check_without_gpu():
     assert lib.lds_set_wait_limit(0) == -1
     assert "wait limit" in lib.lds_last_error().decode()
     assert lib.lds_get_wait_limit() == 1 << 25
+
+
+def test_checked_build_reports_itself_and_exports_every_symbol():
+    """The bounds-checked build (liblds_checked.so) and the ordinary one say
+    which they are; the checked one exports the same entries."""
+    from summit_b200 import _lib
+
+    plain = ctypes.CDLL(str(_lib.PKG / "liblds.so"))
+    plain.lds_checked_build.restype = ctypes.c_int
+    assert plain.lds_checked_build() == 0
+    path = _lib.PKG / "liblds_checked.so"
+    if not path.exists():
+        pytest.skip("bounds-checked build not built (python -m summit_b200.build --checked)")
+    checked = ctypes.CDLL(str(path))
+    checked.lds_checked_build.restype = ctypes.c_int
+    assert checked.lds_checked_build() == 1
+    missing = [s for s in sorted(_declared()) if not hasattr(checked, s)]
+    assert not missing, f"declared but not exported by the checked build: {missing}"
