@@ -1757,6 +1757,11 @@ struct GwPlan {
     // one window (a tile table of 128-SNP tiles).  chk_evsets[p][t] closes
     // V-tile t's phase 2 before its check kernels.
     int check = 0, executed = 0;
+    // Phase-2 CTA order per bins-per-CTA value (as for windowed batches: chunks
+    // of 4 bin groups, all row tiles, the chunk's bin groups).
+    std::vector<int> work_nb;
+    std::vector<std::unique_ptr<DevBuf>> work;
+    std::vector<int64_t> n_work;
     DevBuf chk_lhs, chk_rhs, chk_u, chk_tiles;
     int64_t chk_ntiles = 0;
     std::vector<std::vector<cudaEvent_t>> chk_evsets;
@@ -1912,6 +1917,23 @@ std::unique_ptr<GwPlan> plan_create(Context& c, std::shared_ptr<Prepared> P, con
         pl->tmA = make_map_2d(P->g.codes, (uint64_t)P->g.nbp, (uint64_t)P->g.M_pad,
                               (uint64_t)P->g.nbp, 32, 128, CU_TENSOR_MAP_SWIZZLE_NONE);
         ck(cudaMemsetAsync(pl->status.as<unsigned>(1), 0, 4, c.st), "memset");
+        // phase-2 CTA orders, one per bins-per-CTA value of the V-tiles
+        for (const auto& t : pl->tiles) {
+            const int nb = umma::p2_bins_per_cta(umma::ncolp_for(t->V), (int)K);
+            if (std::find(pl->work_nb.begin(), pl->work_nb.end(), nb) != pl->work_nb.end()) continue;
+            const int64_t tiles = (M + 127) / 128;
+            const int groups = (int)((K + nb - 1) / nb);
+            std::vector<int2> order;
+            for (int g0 = 0; g0 < groups; g0 += 4)
+                for (int64_t tl = 0; tl < tiles; ++tl)
+                    for (int g = g0; g < std::min(groups, g0 + 4); ++g)
+                        order.push_back(make_int2((int)tl, g));
+            auto buf = std::make_unique<DevBuf>();
+            h2d(buf->as<int2>(order.size()), order.data(), order.size(), c.st);
+            pl->work_nb.push_back(nb);
+            pl->work.push_back(std::move(buf));
+            pl->n_work.push_back((int64_t)order.size());
+        }
     } else {
         pl->yq.as<int8_t>((size_t)(pl->S * K * vpmax * P->g.N_pad));
         pl->ycs.as<double>((size_t)(K * vpmax));
@@ -2037,6 +2059,15 @@ void plan_enqueue_phase2(Context& c, GwPlan& pl, size_t ti, const double* y, cud
         u.yq = static_cast<const int8_t*>(pl.yq.p);
         u.yq_cols = K * nc;
         u.accum_elems = M * K;
+        static const bool grid_order = [] {
+            const char* e = std::getenv("LDS_P2_GRID_ORDER");
+            return e && std::atoi(e) != 0;
+        }();
+        for (size_t q = 0; q < pl.work_nb.size() && !grid_order; ++q)
+            if (pl.work_nb[q] == u.bins_per_cta) {
+                u.work = static_cast<const int2*>(pl.work[q]->p);
+                u.n_work = pl.n_work[q];
+            }
         int v0 = 0;
         for (size_t q = 0; q < ti; ++q) v0 += pl.tiles[q]->V;
         if (pl.check) {

@@ -108,7 +108,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         jend = t.y;
         sb = t.z;
     } else {
-        jt0 = a.j0 + (int64_t)blockIdx.x * kBM;
+        jt0 = a.j0 + (int64_t)wk.x * kBM;
         jend = a.j1;
     }
     const int kb = sb + k0;  // first super-bin of this CTA

@@ -66,9 +66,10 @@ struct P2UArgs {
     // the exact products T_G and T_O of SNP row j (wrapping mod 2^64).
     unsigned long long* chk = nullptr;
     int chk_v0 = 0;
-    // Optional CTA order (tile-table mode): CTA x processes tile work[x].x with
-    // bin group work[x].y (n_work entries, the grid), instead of tile
-    // blockIdx.x and bin group blockIdx.y.
+    // Optional CTA order: CTA x processes tile work[x].x (an entry of the tile
+    // table, or rows j0 + 128 work[x].x without one) with bin group
+    // work[x].y (n_work entries, the grid), instead of tile blockIdx.x and bin
+    // group blockIdx.y.
     const int2* work = nullptr;
     int64_t n_work = 0;
     // Extent of accum / accum2 / mc in elements, read by the bounds-checked
