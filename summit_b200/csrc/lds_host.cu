@@ -17,6 +17,7 @@
 #include <limits>
 #include <list>
 #include <map>
+#include <tuple>
 #include <memory>
 #include <mutex>
 #include <random>
@@ -3140,6 +3141,9 @@ struct GxeCtx {
     DevBuf probes, annot, sx, sw, panel, y, wq, wcs, rowind, sc, binoff, coef, coef2, denom;
     DevBuf sacc, acc4, guards, status, flag;
     DevBuf dgeno, dw, ones_L;            // dense-block path
+    // Phase-2 CTA orders (chunks of 4 bin groups, the block's row tiles, the
+    // chunk's groups) keyed by (row tiles, bins per CTA, groups).
+    std::map<std::tuple<int64_t, int, int>, std::pair<std::unique_ptr<DevBuf>, int64_t>> p2_work;
 };
 
 struct GxePair {
@@ -3511,6 +3515,27 @@ void gxe_target_impl(Context& c, GxeCtx& g, int64_t j0, int64_t j1, GxePair& pr,
                                         (uint64_t)P.g.nbp, 32, 128, CU_TENSOR_MAP_SWIZZLE_NONE);
     u.yq = static_cast<const int8_t*>(pr.yq.p);
     u.yq_cols = Kp * nc;
+    static const bool grid_order = [] {
+        const char* e = std::getenv("LDS_P2_GRID_ORDER");
+        return e && std::atoi(e) != 0;
+    }();
+    if (!grid_order) {
+        const int64_t tiles = (L + 127) / 128;
+        const int groups = (int)((Kp + nb - 1) / nb);
+        auto& entry = g.p2_work[std::make_tuple(tiles, nb, groups)];
+        if (!entry.first) {
+            std::vector<int2> order;
+            for (int g0 = 0; g0 < groups; g0 += 4)
+                for (int64_t tl = 0; tl < tiles; ++tl)
+                    for (int q = g0; q < std::min(groups, g0 + 4); ++q)
+                        order.push_back(make_int2((int)tl, q));
+            entry.first = std::make_unique<DevBuf>();
+            h2d(entry.first->as<int2>(order.size()), order.data(), order.size(), c.st);
+            entry.second = (int64_t)order.size();
+        }
+        u.work = static_cast<const int2*>(entry.first->p);
+        u.n_work = entry.second;
+    }
     umma::launch_p2_umma(tmA, u, c.st);
     }
     const size_t nacc = (size_t)(g.E * total * K);
