@@ -518,11 +518,12 @@ def ours_arm(args) -> None:
 
     # ---- tiling of the windowed plans: the project's autotuner, timed on this
     # device before the measured region (phase-1 split, window batching,
-    # phase-2 tile shape; every candidate's scores must agree bit for bit) ----
+    # phase-2 CTA order; every candidate's scores must agree bit for bit) ----
     from summit_b200 import autotune
 
     cands = ([{"p1_sb_per_cta": s, "batch_gb": 8.0} for s in (8, 16, 32, 64, 128)] +
-             [{"p1_sb_per_cta": 64, "batch_gb": b} for b in (4.0, 16.0)])
+             [{"p1_sb_per_cta": 64, "batch_gb": b} for b in (4.0, 16.0)] +
+             [{"p1_sb_per_cta": 128, "batch_gb": 8.0, "p2_bin_chunk": c} for c in (0, 2, 8)])
     t_tune = time.perf_counter()
     tune = autotune.tune_windowed(sess, annot, ws, B_PROBES, BLOCK, PROBE_SEED, "rademacher",
                                   candidates=cands, reps=1)

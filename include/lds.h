@@ -317,6 +317,13 @@ int lds_win_plan_bin_totals(int64_t plan, double* mkw_out);
  * The LD scores do not depend on the tiling (bit for bit).  No reference
  * counterpart (it replaces the reference's CPU tiling environment knobs). */
 int lds_win_plan_set_tiling(int64_t plan, int p1_sb_per_cta);
+/* Phase-2 CTA order of a windowed plan, set before its first execute (the
+ * autotuner's knob; no reference counterpart): window by window, chunks of
+ * bin_chunk bin groups, the window's 128-SNP tiles, the chunk's bin groups,
+ * so that the CTAs that run together share a tile's packed codes and a
+ * (window, bin) sketch in L2 (default 4; 0: grid order, bins slowest).  The
+ * scores do not depend on it (bit for bit). */
+int lds_win_plan_set_p2_order(int64_t plan, int bin_chunk);
 /* Exact integrity check of the phase-2 tensor-core products (the counterpart
  * of the reference's ABFT / Freivalds check of its GxE GEMMs,
  * gxeldcore.cpp:4674-4734, made exact because the products are integers).

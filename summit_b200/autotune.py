@@ -9,7 +9,11 @@ device work of a windowed estimate are chosen by timing them on the device:
   split across CTAs (super-bins per CTA: longer per-CTA pipelines against
   more CTAs to balance);
 * ``batch_gb``: how the windows are split into launches (the sketch digits of
-  one batch stay under this many GB).
+  one batch stay under this many GB);
+* ``p2_bin_chunk``: the phase-2 CTA order (window by window, chunks of this
+  many bin groups, the window's tiles, the chunk's groups; 0 is the grid's
+  order), which sets how many CTAs share a tile's packed codes and a
+  (window, bin) sketch in L2.
 
 The LD scores do not depend on any of them, and the tuner checks that: every
 candidate's scores must equal the first candidate's bit for bit.  A
@@ -30,13 +34,19 @@ from typing import Callable, Iterable
 
 import numpy as np
 
-DEFAULT_CONFIG = {"p1_sb_per_cta": 8, "batch_gb": 8.0}
+DEFAULT_CONFIG = {"p1_sb_per_cta": 8, "batch_gb": 8.0, "p2_bin_chunk": 4}
 
 
 def default_candidates() -> list[dict]:
-    """Phase-1 split x window batching."""
-    return [{"p1_sb_per_cta": s, "batch_gb": b}
-            for s in (8, 16, 32, 64, 128) for b in (4.0, 8.0, 16.0)]
+    """Phase-1 split x window batching, then the phase-2 order."""
+    return ([{"p1_sb_per_cta": s, "batch_gb": b, "p2_bin_chunk": 4}
+             for s in (8, 16, 32, 64, 128) for b in (4.0, 8.0, 16.0)] +
+            [{"p1_sb_per_cta": 64, "batch_gb": 8.0, "p2_bin_chunk": c} for c in (0, 2, 8)])
+
+
+def _apply(plan, cand: dict) -> None:
+    plan.set_tiling(int(cand["p1_sb_per_cta"]))
+    plan.set_p2_order(int(cand.get("p2_bin_chunk", DEFAULT_CONFIG["p2_bin_chunk"])))
 
 
 def cache_path() -> Path:
@@ -115,7 +125,7 @@ def _plan_runner(session, annot, window_starts, nvecs, step, seed, rand_dist, re
         plan = WinPlan(session, annot, window_starts, nvecs, step, seed, rand_dist,
                        batch_gb=float(cand["batch_gb"]))
         try:
-            plan.set_tiling(int(cand["p1_sb_per_cta"]))
+            _apply(plan, cand)
             plan.execute()  # captures the graph
             ld = plan.results(meansq=False)["ldscore"]
             best = math.inf
@@ -186,5 +196,5 @@ def tuned_win_plan(session, annot, window_starts, nvecs: int, step: int, seed: i
     cfg = dict(DEFAULT_CONFIG, **(rec["config"] if rec else {}))
     plan = WinPlan(session, annot, window_starts, nvecs, step, seed, rand_dist,
                    batch_gb=float(cfg["batch_gb"]), **plan_kw)
-    plan.set_tiling(int(cfg["p1_sb_per_cta"]))
+    _apply(plan, cfg)
     return plan

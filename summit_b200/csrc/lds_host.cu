@@ -2253,6 +2253,7 @@ struct WinPlan {
         std::vector<int> work_nb;
         std::vector<std::unique_ptr<DevBuf>> work;
         std::vector<int64_t> n_work;
+        std::vector<int64_t> tile_begin;   // first tile of each window, and the tile count
     };
     std::vector<Batch> batches;
     std::vector<DevBuf> z;              // per V-tile, M x V FP64 probes
@@ -2311,6 +2312,33 @@ std::shared_ptr<DevBuf> shared_workspace(Context& c, int slot, size_t bytes) {
         w->get(bytes);
     }
     return w;
+}
+
+// Phase-2 CTA orders of a window batch, one per bins-per-CTA value of the
+// V-tiles: window by window, chunks of `chunk` bin groups, the window's
+// tiles, the chunk's bin groups (chunk 0: no order, the grid's).
+void build_win_work(Context& c, WinPlan::Batch& b, const std::vector<int>& vt, int64_t K,
+                    int chunk) {
+    b.work_nb.clear();
+    b.work.clear();
+    b.n_work.clear();
+    if (chunk <= 0) return;
+    for (int V : vt) {
+        const int nb = umma::p2_bins_per_cta(umma::ncolp_for(V), (int)K);
+        if (std::find(b.work_nb.begin(), b.work_nb.end(), nb) != b.work_nb.end()) continue;
+        const int groups = (int)((K + nb - 1) / nb);
+        std::vector<int2> order;
+        for (size_t w = 0; w + 1 < b.tile_begin.size(); ++w)
+            for (int g0 = 0; g0 < groups; g0 += chunk)
+                for (int64_t t = b.tile_begin[w]; t < b.tile_begin[w + 1]; ++t)
+                    for (int g = g0; g < std::min(groups, g0 + chunk); ++g)
+                        order.push_back(make_int2((int)t, g));
+        auto buf = std::make_unique<DevBuf>();
+        h2d(buf->as<int2>(order.size()), order.data(), order.size(), c.st);
+        b.work_nb.push_back(nb);
+        b.work.push_back(std::move(buf));
+        b.n_work.push_back((int64_t)order.size());
+    }
 }
 
 std::map<int64_t, std::unique_ptr<WinPlan>>& win_table() {
@@ -2439,23 +2467,8 @@ std::unique_ptr<WinPlan> win_plan_create(Context& c, std::shared_ptr<Prepared> P
         tile_begin.push_back((int64_t)tiles.size());
         b.ntiles = (int64_t)tiles.size();
         h2d(b.tiles.as<int4>(tiles.size()), tiles.data(), tiles.size(), c.st);
-        constexpr int kWorkBinChunk = 4;
-        for (int V : pl->vt) {
-            const int nb = umma::p2_bins_per_cta(umma::ncolp_for(V), (int)K);
-            if (std::find(b.work_nb.begin(), b.work_nb.end(), nb) != b.work_nb.end()) continue;
-            const int groups = (int)((K + nb - 1) / nb);
-            std::vector<int2> order;
-            for (size_t w = 0; w + 1 < tile_begin.size(); ++w)
-                for (int g0 = 0; g0 < groups; g0 += kWorkBinChunk)
-                    for (int64_t t = tile_begin[w]; t < tile_begin[w + 1]; ++t)
-                        for (int g = g0; g < std::min(groups, g0 + kWorkBinChunk); ++g)
-                            order.push_back(make_int2((int)t, g));
-            auto buf = std::make_unique<DevBuf>();
-            h2d(buf->as<int2>(order.size()), order.data(), order.size(), c.st);
-            b.work_nb.push_back(nb);
-            b.work.push_back(std::move(buf));
-            b.n_work.push_back((int64_t)order.size());
-        }
+        b.tile_begin = std::move(tile_begin);
+        build_win_work(c, b, pl->vt, K, 4);
         ck(cudaStreamSynchronize(c.st), "window batch upload");
         max_ksup = std::max(max_ksup, b.ksup);
         max_wq = std::max(max_wq, b.ksup * 2 * ncmax * b.lmax);
@@ -3141,9 +3154,6 @@ struct GxeCtx {
     DevBuf probes, annot, sx, sw, panel, y, wq, wcs, rowind, sc, binoff, coef, coef2, denom;
     DevBuf sacc, acc4, guards, status, flag;
     DevBuf dgeno, dw, ones_L;            // dense-block path
-    // Phase-2 CTA orders (chunks of 4 bin groups, the block's row tiles, the
-    // chunk's groups) keyed by (row tiles, bins per CTA, groups).
-    std::map<std::tuple<int64_t, int, int>, std::pair<std::unique_ptr<DevBuf>, int64_t>> p2_work;
 };
 
 struct GxePair {
@@ -3515,27 +3525,6 @@ void gxe_target_impl(Context& c, GxeCtx& g, int64_t j0, int64_t j1, GxePair& pr,
                                         (uint64_t)P.g.nbp, 32, 128, CU_TENSOR_MAP_SWIZZLE_NONE);
     u.yq = static_cast<const int8_t*>(pr.yq.p);
     u.yq_cols = Kp * nc;
-    static const bool grid_order = [] {
-        const char* e = std::getenv("LDS_P2_GRID_ORDER");
-        return e && std::atoi(e) != 0;
-    }();
-    if (!grid_order) {
-        const int64_t tiles = (L + 127) / 128;
-        const int groups = (int)((Kp + nb - 1) / nb);
-        auto& entry = g.p2_work[std::make_tuple(tiles, nb, groups)];
-        if (!entry.first) {
-            std::vector<int2> order;
-            for (int g0 = 0; g0 < groups; g0 += 4)
-                for (int64_t tl = 0; tl < tiles; ++tl)
-                    for (int q = g0; q < std::min(groups, g0 + 4); ++q)
-                        order.push_back(make_int2((int)tl, q));
-            entry.first = std::make_unique<DevBuf>();
-            h2d(entry.first->as<int2>(order.size()), order.data(), order.size(), c.st);
-            entry.second = (int64_t)order.size();
-        }
-        u.work = static_cast<const int2*>(entry.first->p);
-        u.n_work = entry.second;
-    }
     umma::launch_p2_umma(tmA, u, c.st);
     }
     const size_t nacc = (size_t)(g.E * total * K);
@@ -4803,6 +4792,18 @@ static int64_t count_check_mismatches(const unsigned long long* lhs, const unsig
         }
     if (first) *first = f;
     return bad;
+}
+
+LDS_API int lds_win_plan_set_p2_order(int64_t plan, int bin_chunk) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        WinPlan& pl = win_of_handle(plan);
+        if (pl.graph) fail(LDS_ERR_ARG, "set the phase-2 order before the plan's first execute");
+        if (bin_chunk < 0 || bin_chunk > 4096) fail(LDS_ERR_ARG, "bin_chunk must be in [0, 4096]");
+        for (auto& b : pl.batches) build_win_work(c, b, pl.vt, pl.K, bin_chunk);
+        ck(cudaStreamSynchronize(c.st), "phase-2 order");
+    });
 }
 
 LDS_API int lds_win_plan_set_checks(int64_t plan, int on) {

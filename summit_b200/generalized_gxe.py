@@ -173,7 +173,7 @@ class GeneralizedPass1Result:
 
 
 def pass1(session, basis, fixed_effect_basis, annotations, probe_spec: GlobalVariantProbeSpec, *,
-          variant_block_width: int = 8192, projection_tolerance: float = 2.0e-11,
+          variant_block_width: int = 65536, projection_tolerance: float = 2.0e-11,
           retain_base_sources: bool = False) -> GeneralizedPass1Result:
     """Global contextual sources (GeneralizedGxEPass1Executor.execute)."""
     basis, fixed, weights, masses = _validate(session, basis, fixed_effect_basis, annotations)
@@ -230,7 +230,7 @@ class GeneralizedPass2Result:
 
 
 def pass2(session, pass1_result: GeneralizedPass1Result, basis, fixed_effect_basis, annotations,
-          *, variant_block_width: int = 8192) -> GeneralizedPass2Result:
+          *, variant_block_width: int = 65536) -> GeneralizedPass2Result:
     """Per-variant directional scores (GeneralizedGxEPass2Executor.execute)."""
     basis, fixed, weights, masses = _validate(session, basis, fixed_effect_basis, annotations)
     sources = pass1_result.contextual_sources
@@ -308,7 +308,7 @@ def pass2(session, pass1_result: GeneralizedPass1Result, basis, fixed_effect_bas
 
 
 def two_pass(session, basis, fixed_effect_basis, annotations, probe_spec: GlobalVariantProbeSpec,
-             *, variant_block_width: int = 8192, projection_tolerance: float = 2.0e-11):
+             *, variant_block_width: int = 65536, projection_tolerance: float = 2.0e-11):
     """Both passes; returns (pass-1 result, pass-2 result)."""
     p1 = pass1(session, basis, fixed_effect_basis, annotations, probe_spec,
                variant_block_width=variant_block_width,

@@ -284,6 +284,11 @@ class WinPlan:
         execute."""
         check(_lib.load().lds_win_plan_set_tiling(self.handle, int(p1_sb_per_cta)))
 
+    def set_p2_order(self, bin_chunk: int = 4) -> None:
+        """Phase-2 CTA order: chunks of bin_chunk bin groups per window (0:
+        grid order); call before the first execute."""
+        check(_lib.load().lds_win_plan_set_p2_order(self.handle, int(bin_chunk)))
+
     def set_checks(self, on: bool = True) -> None:
         """Exact integrity checks of the phase-2 products on every estimate
         (checksums from the tensor-core epilogue against a CUDA-core
