@@ -324,6 +324,13 @@ int lds_win_plan_set_tiling(int64_t plan, int p1_sb_per_cta);
  * (window, bin) sketch in L2 (default 4; 0: grid order, bins slowest).  The
  * scores do not depend on it (bit for bit). */
 int lds_win_plan_set_p2_order(int64_t plan, int bin_chunk);
+/* Bins per phase-2 CTA of a windowed plan, set before its first execute (the
+ * autotuner's knob; no reference counterpart).  A CTA walks its bins' sketch
+ * columns in MMA groups of up to 256, a bin possibly straddling two groups;
+ * 0 (default) takes the smallest count with the fewest groups per 128-SNP
+ * tile (6 for K = 24 bins of 50 probes: 20 groups of 256 columns instead of
+ * 24 of 208).  The scores do not depend on it (bit for bit). */
+int lds_win_plan_set_p2_bins(int64_t plan, int bins_per_cta);
 /* Exact integrity check of the phase-2 tensor-core products (the counterpart
  * of the reference's ABFT / Freivalds check of its GxE GEMMs,
  * gxeldcore.cpp:4674-4734, made exact because the products are integers).

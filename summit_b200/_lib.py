@@ -58,6 +58,7 @@ SIGNATURES: dict[str, tuple] = {
     "lds_win_plan_cv_annot": (_int, [_i64, _p]),
     "lds_win_plan_set_tiling": (_int, [_i64, _int]),
     "lds_win_plan_set_p2_order": (_int, [_i64, _int]),
+    "lds_win_plan_set_p2_bins": (_int, [_i64, _int]),
     "lds_win_plan_set_checks": (_int, [_i64, _int]),
     "lds_gw_plan_set_checks": (_int, [_i64, _int]),
     "lds_gw_plan_check": (_int, [_i64, _p, _p, _p, _p, _p]),

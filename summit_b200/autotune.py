@@ -13,7 +13,9 @@ device work of a windowed estimate are chosen by timing them on the device:
 * ``p2_bin_chunk``: the phase-2 CTA order (window by window, chunks of this
   many bin groups, the window's tiles, the chunk's groups; 0 is the grid's
   order), which sets how many CTAs share a tile's packed codes and a
-  (window, bin) sketch in L2.
+  (window, bin) sketch in L2;
+* ``p2_bins``: bins per phase-2 CTA (0: the fewest 256-column MMA groups per
+  SNP tile; 1: one bin per CTA).
 
 The LD scores do not depend on any of them, and the tuner checks that: every
 candidate's scores must equal the first candidate's bit for bit.  A
@@ -34,19 +36,22 @@ from typing import Callable, Iterable
 
 import numpy as np
 
-DEFAULT_CONFIG = {"p1_sb_per_cta": 8, "batch_gb": 8.0, "p2_bin_chunk": 4}
+DEFAULT_CONFIG = {"p1_sb_per_cta": 8, "batch_gb": 8.0, "p2_bin_chunk": 4, "p2_bins": 0}
 
 
 def default_candidates() -> list[dict]:
-    """Phase-1 split x window batching, then the phase-2 order."""
-    return ([{"p1_sb_per_cta": s, "batch_gb": b, "p2_bin_chunk": 4}
+    """Phase-1 split x window batching, then the phase-2 order and CTA shape."""
+    return ([{"p1_sb_per_cta": s, "batch_gb": b, "p2_bin_chunk": 4, "p2_bins": 0}
              for s in (8, 16, 32, 64, 128) for b in (4.0, 8.0, 16.0)] +
-            [{"p1_sb_per_cta": 64, "batch_gb": 8.0, "p2_bin_chunk": c} for c in (0, 2, 8)])
+            [{"p1_sb_per_cta": 64, "batch_gb": 8.0, "p2_bin_chunk": c, "p2_bins": 0}
+             for c in (0, 2, 8)] +
+            [{"p1_sb_per_cta": 64, "batch_gb": 8.0, "p2_bin_chunk": 2, "p2_bins": 1}])
 
 
 def _apply(plan, cand: dict) -> None:
     plan.set_tiling(int(cand["p1_sb_per_cta"]))
     plan.set_p2_order(int(cand.get("p2_bin_chunk", DEFAULT_CONFIG["p2_bin_chunk"])))
+    plan.set_p2_bins(int(cand.get("p2_bins", DEFAULT_CONFIG["p2_bins"])))
 
 
 def cache_path() -> Path:

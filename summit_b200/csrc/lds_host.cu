@@ -1920,14 +1920,17 @@ std::unique_ptr<GwPlan> plan_create(Context& c, std::shared_ptr<Prepared> P, con
         ck(cudaMemsetAsync(pl->status.as<unsigned>(1), 0, 4, c.st), "memset");
         // phase-2 CTA orders, one per bins-per-CTA value of the V-tiles
         for (const auto& t : pl->tiles) {
-            const int nb = umma::p2_bins_per_cta(umma::ncolp_for(t->V), (int)K);
+            const int nb = umma::p2_bins_per_cta_grouped(umma::ncolp_for(t->V), (int)K);
             if (std::find(pl->work_nb.begin(), pl->work_nb.end(), nb) != pl->work_nb.end()) continue;
             const int64_t tiles = (M + 127) / 128;
             const int groups = (int)((K + nb - 1) / nb);
+            // chunks of about 4 bins, so that the sketch columns the running
+            // CTAs share stay in L2 (4 bins x 208 columns x 50k samples: 42 MB)
+            const int chunk = std::max(1, 4 / nb);
             std::vector<int2> order;
-            for (int g0 = 0; g0 < groups; g0 += 4)
+            for (int g0 = 0; g0 < groups; g0 += chunk)
                 for (int64_t tl = 0; tl < tiles; ++tl)
-                    for (int g = g0; g < std::min(groups, g0 + 4); ++g)
+                    for (int g = g0; g < std::min(groups, g0 + chunk); ++g)
                         order.push_back(make_int2((int)tl, g));
             auto buf = std::make_unique<DevBuf>();
             h2d(buf->as<int2>(order.size()), order.data(), order.size(), c.st);
@@ -2035,7 +2038,7 @@ void plan_enqueue_phase2(Context& c, GwPlan& pl, size_t ti, const double* y, cud
         u.K = (int)K;
         u.V = t.V;
         u.ncolp = nc;
-        u.bins_per_cta = umma::p2_bins_per_cta(nc, (int)K);
+        u.bins_per_cta = umma::p2_bins_per_cta_grouped(nc, (int)K);
         u.ngroups = (u.bins_per_cta * nc + 255) / 256;
         u.box_rows = std::min(256, u.bins_per_cta * nc);
         u.nkt = (int)(P.g.N_pad / 128);
@@ -2266,6 +2269,14 @@ struct WinPlan {
     // Tiling chosen for this plan (lds_win_plan_set_tiling): phase-1 super-bins
     // per CTA (0: default).
     int p1_spc = 0;
+    // Phase-2 CTA shape and order (lds_win_plan_set_p2_bins / _set_p2_order):
+    // bins per CTA (0: p2_bins_per_cta_grouped) and bin groups per chunk of
+    // the window-major work order (0: grid order).
+    int p2_nb = 0, p2_chunk = 4;
+    int p2_bins(int ncolp) const {
+        return p2_nb > 0 ? (int)std::min<int64_t>(p2_nb, K)
+                         : umma::p2_bins_per_cta_grouped(ncolp, (int)K);
+    }
     DevBuf annot_d, winof_d, sqrt_ls, xx, band_cnt, cvC, cvMu;
     DevBuf mkw_d, ld_d, ms_d;           // finalize inputs and outputs
     cudaEvent_t cv_ev[2] = {nullptr, nullptr};
@@ -2317,14 +2328,15 @@ std::shared_ptr<DevBuf> shared_workspace(Context& c, int slot, size_t bytes) {
 // Phase-2 CTA orders of a window batch, one per bins-per-CTA value of the
 // V-tiles: window by window, chunks of `chunk` bin groups, the window's
 // tiles, the chunk's bin groups (chunk 0: no order, the grid's).
-void build_win_work(Context& c, WinPlan::Batch& b, const std::vector<int>& vt, int64_t K,
-                    int chunk) {
+void build_win_work(Context& c, const WinPlan& pl, WinPlan::Batch& b) {
+    const int64_t K = pl.K;
+    const int chunk = pl.p2_chunk;
     b.work_nb.clear();
     b.work.clear();
     b.n_work.clear();
     if (chunk <= 0) return;
-    for (int V : vt) {
-        const int nb = umma::p2_bins_per_cta(umma::ncolp_for(V), (int)K);
+    for (int V : pl.vt) {
+        const int nb = pl.p2_bins(umma::ncolp_for(V));
         if (std::find(b.work_nb.begin(), b.work_nb.end(), nb) != b.work_nb.end()) continue;
         const int groups = (int)((K + nb - 1) / nb);
         std::vector<int2> order;
@@ -2468,7 +2480,7 @@ std::unique_ptr<WinPlan> win_plan_create(Context& c, std::shared_ptr<Prepared> P
         b.ntiles = (int64_t)tiles.size();
         h2d(b.tiles.as<int4>(tiles.size()), tiles.data(), tiles.size(), c.st);
         b.tile_begin = std::move(tile_begin);
-        build_win_work(c, b, pl->vt, K, 4);
+        build_win_work(c, *pl, b);
         ck(cudaStreamSynchronize(c.st), "window batch upload");
         max_ksup = std::max(max_ksup, b.ksup);
         max_wq = std::max(max_wq, b.ksup * 2 * ncmax * b.lmax);
@@ -2634,7 +2646,7 @@ void win_enqueue(Context& c, WinPlan& pl) {
                 umma::launch_digit_colsum(static_cast<const int8_t*>(pl.yq->p), b.ksup * nc, Np,
                                           colsum, c.st);
             ck(cudaEventRecordWithFlags(pl.ev[(size_t)e++], c.st, cudaEventRecordExternal), "event");
-            const int nb = umma::p2_bins_per_cta(nc, (int)K);
+            const int nb = pl.p2_bins(nc);
             umma::P2UArgs u;
             u.yq = static_cast<const int8_t*>(pl.yq->p);
             u.yq_cols = b.ksup * nc;
@@ -4801,8 +4813,23 @@ LDS_API int lds_win_plan_set_p2_order(int64_t plan, int bin_chunk) {
         WinPlan& pl = win_of_handle(plan);
         if (pl.graph) fail(LDS_ERR_ARG, "set the phase-2 order before the plan's first execute");
         if (bin_chunk < 0 || bin_chunk > 4096) fail(LDS_ERR_ARG, "bin_chunk must be in [0, 4096]");
-        for (auto& b : pl.batches) build_win_work(c, b, pl.vt, pl.K, bin_chunk);
+        pl.p2_chunk = bin_chunk;
+        for (auto& b : pl.batches) build_win_work(c, pl, b);
         ck(cudaStreamSynchronize(c.st), "phase-2 order");
+    });
+}
+
+LDS_API int lds_win_plan_set_p2_bins(int64_t plan, int bins_per_cta) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        WinPlan& pl = win_of_handle(plan);
+        if (pl.graph) fail(LDS_ERR_ARG, "set the phase-2 bins per CTA before the plan's first execute");
+        if (bins_per_cta < 0 || bins_per_cta > 4096)
+            fail(LDS_ERR_ARG, "bins_per_cta must be in [0, 4096]");
+        pl.p2_nb = bins_per_cta;
+        for (auto& b : pl.batches) build_win_work(c, pl, b);
+        ck(cudaStreamSynchronize(c.st), "phase-2 bins per CTA");
     });
 }
 

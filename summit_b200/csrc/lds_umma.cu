@@ -161,7 +161,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         *abort_flag = 1;
     };
 
-    const int ngroups = a.ngroups;
+    // Column groups of this CTA's bins (the last CTA of a tile may hold fewer
+    // bins than bins_per_cta).
+    const int ngroups = min(a.ngroups, (nbk * a.ncolp + 255) / 256);
     const int total = ngroups * a.nkt;
     if (warp == 0) {
         // ---------------- packed-code producer (runs up to 8 stages ahead) ----------------
@@ -221,11 +223,23 @@ __global__ void __launch_bounds__(kThreads, 1)
                     const uint64_t dG = sw128_desc(smem + lay.a_off(sa));
                     const uint64_t dO = sw128_desc(smem + lay.a_off(sa) + kATile);
                     const uint64_t dB = sw128_desc(smem + lay.b_off(sb));
+                    if (complete) {
+                        // No O plane: the G products alternate between two
+                        // accumulators (even K-substeps at column 0, odd ones
+                        // in the O accumulator's columns), summed by the
+                        // epilogue; back-to-back MMAs into one accumulator
+                        // run at about half the rate of two interleaved ones.
 #pragma unroll
-                    for (int kk = 0; kk < kBK / 32; ++kk) {
-                        const uint32_t acc = (kt | kk) ? 1u : 0u;
-                        umma_i8(tmem, dG + 2 * kk, dB + 2 * kk, idesc, acc);
-                        if (!complete) umma_i8(tmem + kOCol, dO + 2 * kk, dB + 2 * kk, idesc, acc);
+                        for (int kk = 0; kk < kBK / 32; ++kk)
+                            umma_i8(tmem + ((kk & 1) ? kOCol : 0u), dG + 2 * kk, dB + 2 * kk, idesc,
+                                    (kt > 0 || kk >= 2) ? 1u : 0u);
+                    } else {
+#pragma unroll
+                        for (int kk = 0; kk < kBK / 32; ++kk) {
+                            const uint32_t acc = (kt | kk) ? 1u : 0u;
+                            umma_i8(tmem, dG + 2 * kk, dB + 2 * kk, idesc, acc);
+                            umma_i8(tmem + kOCol, dO + 2 * kk, dB + 2 * kk, idesc, acc);
+                        }
                     }
                     umma_commit(&a_empty[sa]);
                     umma_commit(&b_empty[sb]);
@@ -320,17 +334,19 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (int c0 = 0; c0 < ncols; c0 += 32) {
                 int rg[32], ro[32];
                 tmem_ld32(tbase + (uint32_t)c0, rg);
+                tmem_ld32(tbase + kOCol + (uint32_t)c0, ro);
+                tmem_wait_ld();
                 if (complete) {
-                    // every call observed: O^T y = the digit columns' sums
-                    // (columns past this CTA's bins belong to no output)
+                    // the G products' second accumulator, then every call
+                    // observed: O^T y = the digit columns' sums (columns past
+                    // this CTA's bins belong to no output)
+#pragma unroll
+                    for (int q = 0; q < 32; ++q) rg[q] += ro[q];
                     const int live = min(ncols, nbk * a.ncolp - g * 256) - c0;
                     const int* cs = a.colsum + (int64_t)kb * a.ncolp + g * 256 + c0;
 #pragma unroll
                     for (int q = 0; q < 32; ++q) ro[q] = q < live ? cs[q] : 0;
-                } else {
-                    tmem_ld32(tbase + kOCol + (uint32_t)c0, ro);
                 }
-                tmem_wait_ld();
 #pragma unroll
                 for (int p = 0; p < 8; ++p) {
                     const int gc = g * 256 + c0 + 4 * p;   // column within this CTA's bins

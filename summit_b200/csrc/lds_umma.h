@@ -1,5 +1,6 @@
 // tcgen05 (UMMA) phase-2 kernel interface.
 #pragma once
+#include <climits>
 #include <cstdint>
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -82,6 +83,27 @@ inline int p2_bins_per_cta(int ncolp, int K) {
     if (ncolp > 128) return 1;
     const int nb = 256 / ncolp;
     return nb < K ? nb : K;
+}
+
+// Bins per CTA for the plans that run phase 2 from a work order: the CTA
+// walks its bins' columns in MMA groups of up to 256 (a bin may straddle two
+// groups), so a tile costs ceil(K / nb) CTAs x ceil(nb * ncolp / 256) groups.
+// The smallest nb with the fewest groups per tile: for 208-column bins and
+// K = 24, nb = 6 (20 groups of 256 columns instead of 24 of 208; an MMA's
+// cost is nearly the same at N = 208 and N = 256).
+inline int p2_bins_per_cta_grouped(int ncolp, int K) {
+    if (ncolp <= 128) return p2_bins_per_cta(ncolp, K);
+    int best = 1;
+    int64_t best_groups = INT64_MAX;
+    for (int nb = 1; nb <= K; ++nb) {
+        const int64_t groups =
+            (int64_t)((K + nb - 1) / nb) * (((int64_t)nb * ncolp + 255) / 256);
+        if (groups < best_groups) {
+            best_groups = groups;
+            best = nb;
+        }
+    }
+    return best;
 }
 
 // Phase-1 tcgen05 kernel arguments.  Member lists of bin k occupy

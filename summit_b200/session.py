@@ -289,6 +289,11 @@ class WinPlan:
         grid order); call before the first execute."""
         check(_lib.load().lds_win_plan_set_p2_order(self.handle, int(bin_chunk)))
 
+    def set_p2_bins(self, bins_per_cta: int = 0) -> None:
+        """Bins per phase-2 CTA (0: the fewest 256-column MMA groups per SNP
+        tile); call before the first execute."""
+        check(_lib.load().lds_win_plan_set_p2_bins(self.handle, int(bins_per_cta)))
+
     def set_checks(self, on: bool = True) -> None:
         """Exact integrity checks of the phase-2 products on every estimate
         (checksums from the tensor-core epilogue against a CUDA-core

@@ -79,3 +79,4 @@ def test_default_candidates_cover_the_knobs():
     assert {c["batch_gb"] for c in cands} == {4.0, 8.0, 16.0}
     assert len({c["p1_sb_per_cta"] for c in cands}) >= 3
     assert all(set(c) == set(autotune.DEFAULT_CONFIG) for c in cands)
+    assert {c["p2_bins"] for c in cands} == {0, 1}
