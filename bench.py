@@ -523,7 +523,7 @@ def ours_arm(args) -> None:
 
     cands = ([{"p1_sb_per_cta": s, "batch_gb": 8.0} for s in (8, 16, 32, 64, 128)] +
              [{"p1_sb_per_cta": 64, "batch_gb": b} for b in (4.0, 16.0)] +
-             [{"p1_sb_per_cta": 128, "batch_gb": 8.0, "p2_bin_chunk": c} for c in (0, 1, 2)] +
+             [{"p1_sb_per_cta": 128, "batch_gb": 8.0, "p2_bin_chunk": c} for c in (0, 12, 24)] +
              [{"p1_sb_per_cta": 128, "batch_gb": 8.0, "p2_bin_chunk": 2, "p2_bins": 1}])
     t_tune = time.perf_counter()
     tune = autotune.tune_windowed(sess, annot, ws, B_PROBES, BLOCK, PROBE_SEED, "rademacher",

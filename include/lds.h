@@ -319,10 +319,11 @@ int lds_win_plan_bin_totals(int64_t plan, double* mkw_out);
 int lds_win_plan_set_tiling(int64_t plan, int p1_sb_per_cta);
 /* Phase-2 CTA order of a windowed plan, set before its first execute (the
  * autotuner's knob; no reference counterpart): window by window, chunks of
- * bin_chunk bin groups, the window's 128-SNP tiles, the chunk's bin groups,
- * so that the CTAs that run together share a tile's packed codes and a
- * (window, bin) sketch in L2 (default 4; 0: grid order, bins slowest).  The
- * scores do not depend on it (bit for bit). */
+ * about bin_chunk bins (whole bin groups of lds_win_plan_set_p2_bins, at
+ * least one), the window's 128-SNP tiles, the chunk's bin groups, so that the
+ * CTAs that run together share a tile's packed codes and a (window, bin)
+ * sketch in L2 (default 4; 0: grid order, bins slowest).  The scores do not
+ * depend on it (bit for bit). */
 int lds_win_plan_set_p2_order(int64_t plan, int bin_chunk);
 /* Bins per phase-2 CTA of a windowed plan, set before its first execute (the
  * autotuner's knob; no reference counterpart).  A CTA walks its bins' sketch

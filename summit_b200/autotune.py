@@ -10,10 +10,10 @@ device work of a windowed estimate are chosen by timing them on the device:
   more CTAs to balance);
 * ``batch_gb``: how the windows are split into launches (the sketch digits of
   one batch stay under this many GB);
-* ``p2_bin_chunk``: the phase-2 CTA order (window by window, chunks of this
-  many bin groups, the window's tiles, the chunk's groups; 0 is the grid's
-  order), which sets how many CTAs share a tile's packed codes and a
-  (window, bin) sketch in L2;
+* ``p2_bin_chunk``: the phase-2 CTA order (window by window, chunks of about
+  this many bins in whole CTA bin groups, the window's tiles, the chunk's
+  groups; 0 is the grid's order), which sets how many CTAs share a tile's
+  packed codes and a (window, bin) sketch in L2;
 * ``p2_bins``: bins per phase-2 CTA (0: the fewest 256-column MMA groups per
   SNP tile; 1: one bin per CTA).
 
@@ -44,7 +44,7 @@ def default_candidates() -> list[dict]:
     return ([{"p1_sb_per_cta": s, "batch_gb": b, "p2_bin_chunk": 4, "p2_bins": 0}
              for s in (8, 16, 32, 64, 128) for b in (4.0, 8.0, 16.0)] +
             [{"p1_sb_per_cta": 64, "batch_gb": 8.0, "p2_bin_chunk": c, "p2_bins": 0}
-             for c in (0, 2, 8)] +
+             for c in (0, 12, 24)] +
             [{"p1_sb_per_cta": 64, "batch_gb": 8.0, "p2_bin_chunk": 2, "p2_bins": 1}])
 
 

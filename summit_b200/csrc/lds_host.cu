@@ -2270,8 +2270,8 @@ struct WinPlan {
     // per CTA (0: default).
     int p1_spc = 0;
     // Phase-2 CTA shape and order (lds_win_plan_set_p2_bins / _set_p2_order):
-    // bins per CTA (0: p2_bins_per_cta_grouped) and bin groups per chunk of
-    // the window-major work order (0: grid order).
+    // bins per CTA (0: p2_bins_per_cta_grouped) and bins per chunk of the
+    // window-major work order (0: grid order).
     int p2_nb = 0, p2_chunk = 4;
     int p2_bins(int ncolp) const {
         return p2_nb > 0 ? (int)std::min<int64_t>(p2_nb, K)
@@ -2326,19 +2326,20 @@ std::shared_ptr<DevBuf> shared_workspace(Context& c, int slot, size_t bytes) {
 }
 
 // Phase-2 CTA orders of a window batch, one per bins-per-CTA value of the
-// V-tiles: window by window, chunks of `chunk` bin groups, the window's
-// tiles, the chunk's bin groups (chunk 0: no order, the grid's).
+// V-tiles: window by window, chunks of about p2_chunk bins (whole CTA bin
+// groups, at least one), the window's tiles, the chunk's bin groups
+// (p2_chunk 0: no order, the grid's).
 void build_win_work(Context& c, const WinPlan& pl, WinPlan::Batch& b) {
     const int64_t K = pl.K;
-    const int chunk = pl.p2_chunk;
     b.work_nb.clear();
     b.work.clear();
     b.n_work.clear();
-    if (chunk <= 0) return;
+    if (pl.p2_chunk <= 0) return;
     for (int V : pl.vt) {
         const int nb = pl.p2_bins(umma::ncolp_for(V));
         if (std::find(b.work_nb.begin(), b.work_nb.end(), nb) != b.work_nb.end()) continue;
         const int groups = (int)((K + nb - 1) / nb);
+        const int chunk = std::max(1, pl.p2_chunk / nb);
         std::vector<int2> order;
         for (size_t w = 0; w + 1 < b.tile_begin.size(); ++w)
             for (int g0 = 0; g0 < groups; g0 += chunk)

@@ -285,8 +285,9 @@ class WinPlan:
         check(_lib.load().lds_win_plan_set_tiling(self.handle, int(p1_sb_per_cta)))
 
     def set_p2_order(self, bin_chunk: int = 4) -> None:
-        """Phase-2 CTA order: chunks of bin_chunk bin groups per window (0:
-        grid order); call before the first execute."""
+        """Phase-2 CTA order: chunks of about bin_chunk bins per window (whole
+        bin groups, at least one; 0: grid order); call before the first
+        execute."""
         check(_lib.load().lds_win_plan_set_p2_order(self.handle, int(bin_chunk)))
 
     def set_p2_bins(self, bins_per_cta: int = 0) -> None:
