@@ -943,6 +943,19 @@ def gxe_arm(args) -> None:
         "gpu_launches": launches,
         "clocks": clk.summary(),
     }
+    if not os.environ.get("LDS_SKIP_CHECKS"):
+        # the same build with the target's exact product checks (outside the
+        # timed region): overhead, mismatches, accumulators unchanged
+        gxc = GxeReference(sess, *[d[k] for k in keys], annotation_bins=K, product_checks=True)
+        resc = gxc.run(probes, annot, scale, scale)
+        rc = gxc.last_check()
+        same = all(torch.equal(resc[k], res[k])
+                   for k in ("accum_xx", "accum_xw", "accum_wx", "accum_ww"))
+        line["product_checks"] = {
+            "target_ms": round(resc["timings"]["target"], 1),
+            "unchecked_target_ms": round(res["timings"]["target"], 1),
+            "rows": rc["rows"], "mismatches": rc["mismatches"], "scores_identical": bool(same)}
+        gxc.close()
     if rank == 0 and world == 1 and not os.environ.get("LDS_SKIP_CPU_BASELINE"):
         threads = cpu_threads()
         snps = env_int("LDS_GXE_CPU_SNPS", 400)

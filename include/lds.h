@@ -791,6 +791,24 @@ int lds_gxe_target_score_block(int64_t gxe, int64_t j0, int64_t j1, int64_t pair
 int lds_gxe_normalize_scores(double* accum_xx, double* accum_xw, double* accum_wx,
                              double* accum_ww, int64_t rows, int64_t K, int probe_count,
                              int device_ptrs);
+/* Exact integrity check of the GxE target's tensor-core products (the
+ * counterpart of the reference's ABFT / Freivalds check of its GxE GEMMs,
+ * gxeldcore.cpp:4674-4734, made exact because the products are integers; the
+ * reference re-checks flagged columns under a floating-point bound and fails
+ * on a material error).  With checks on (contexts on a resident image only),
+ * every lds_gxe_target_score_block call also forms, per SNP, the checksums
+ * sum_{k,v} h(k, v) T(j, k, v) of its products in the kernel's epilogue and
+ * sum_i g_ij u(i) from the packed codes on the CUDA cores (G and O planes,
+ * mod 2^64, h an odd weight per (group, probe)), compares them on the host
+ * and returns LDS_ERR_INTERNAL if any SNP disagrees (the accumulators then
+ * hold that call's suspect products). */
+int lds_gxe_set_checks(int64_t gxe, int on);
+/* The last checked target call: its checksums (2 x rows each, [G, O] per
+ * SNP; either pointer may be null), first SNP, row count, mismatching SNPs
+ * and the first of them (-1 if none). */
+int lds_gxe_last_check(int64_t gxe, unsigned long long* lhs, unsigned long long* rhs,
+                       int64_t* first_row, int64_t* rows, int64_t* mismatches,
+                       int64_t* first_snp);
 int lds_philox_rademacher(const uint64_t* keys, int64_t probes, int64_t rows, double* out,
                           int device_ptrs);
 

@@ -99,6 +99,8 @@ SIGNATURES: dict[str, tuple] = {
     "lds_compute_maf_bed": (_int, [_str, _str, _int, _int, _p, _i64, _p]),
     "lds_gxe_create": (_int, [_i64, _i64, _p, _i64, _p, _p, _i64, _p, _p, _p, _p, _int, _p]),
     "lds_gxe_destroy": (_int, [_i64]),
+    "lds_gxe_set_checks": (_int, [_i64, _int]),
+    "lds_gxe_last_check": (_int, [_i64, _p, _p, _p, _p, _p, _p]),
     "lds_gxe_create_dense": (_int, [_i64, _i64, _p, _i64, _p, _p, _i64, _p, _p, _p, _p, _int,
                                     _p]),
     "lds_gxe_source_block_dense": (_int, [_i64, _p, _i64, _p, _i64, _p, _int, _p, _p, _i64, _int,

@@ -3167,6 +3167,13 @@ struct GxeCtx {
     DevBuf probes, annot, sx, sw, panel, y, wq, wcs, rowind, sc, binoff, coef, coef2, denom;
     DevBuf sacc, acc4, guards, status, flag;
     DevBuf dgeno, dw, ones_L;            // dense-block path
+    // Exact checks of the target's phase-2 products (lds_gxe_set_checks):
+    // per-SNP checksums from the tensor-core epilogue (lhs) and from the
+    // CUDA-core recomputation (rhs), and the last target call's result.
+    int check = 0;
+    DevBuf chk_lhs, chk_rhs, chk_u, chk_tiles;
+    std::vector<unsigned long long> chk_hl, chk_hr;
+    int64_t chk_j0 = 0, chk_rows = 0, chk_bad = 0, chk_first = -1;
 };
 
 struct GxePair {
@@ -3450,6 +3457,20 @@ std::unique_ptr<GxePair> gxe_pair_impl(Context& c, const GxeCtx& g, const double
 }
 
 // target_score_block (gxeldcore.cpp:11731-11936).
+// SNPs whose G or O checksum pair differs (host comparison); the first one in
+// *first (-1 if none).
+static int64_t count_check_mismatches(const unsigned long long* lhs, const unsigned long long* rhs,
+                                      int64_t n_snps, int64_t* first) {
+    int64_t bad = 0, f = -1;
+    for (int64_t j = 0; j < n_snps; ++j)
+        if (lhs[2 * j] != rhs[2 * j] || lhs[2 * j + 1] != rhs[2 * j + 1]) {
+            if (f < 0) f = j;
+            ++bad;
+        }
+    if (first) *first = f;
+    return bad;
+}
+
 void gxe_target_impl(Context& c, GxeCtx& g, int64_t j0, int64_t j1, GxePair& pr, const double* sx,
                      const double* sw, int64_t T, double* axx, double* axw, double* awx, double* aww,
                      int64_t block_start, int64_t total, int probe_count, int env_start,
@@ -3473,6 +3494,8 @@ void gxe_target_impl(Context& c, GxeCtx& g, int64_t j0, int64_t j1, GxePair& pr,
     const double* dsx = dev_in(c, g.sx, sx, (size_t)(L * T), device_ptrs);
     const double* dsw = dev_in(c, g.sw, sw, (size_t)(L * T), device_ptrs);
     unsigned* flag = g.flag.as<unsigned>(1);
+    const bool checked = g.check && !dense;
+    std::vector<int4> chk_tiles;  // rows of the check's CUDA-core pass (alive until the sync)
     ck(cudaMemsetAsync(flag, 0, 4, c.st), "memset");
     launch_gxe_check(dsx, 0, dsx, dsw, L * T, dsx, 0, flag, c.st);
     unsigned fv = 0;
@@ -3538,7 +3561,36 @@ void gxe_target_impl(Context& c, GxeCtx& g, int64_t j0, int64_t j1, GxePair& pr,
                                         (uint64_t)P.g.nbp, 32, 128, CU_TENSOR_MAP_SWIZZLE_NONE);
     u.yq = static_cast<const int8_t*>(pr.yq.p);
     u.yq_cols = Kp * nc;
+    unsigned long long *chk_lhs = nullptr, *chk_rhs = nullptr;
+    if (checked) {
+        // checksums indexed by SNP (the kernel writes 2 j, 2 j + 1)
+        chk_lhs = g.chk_lhs.as<unsigned long long>((size_t)(2 * P.g.M));
+        chk_rhs = g.chk_rhs.as<unsigned long long>((size_t)(2 * P.g.M));
+        ck(cudaMemsetAsync(chk_lhs + 2 * j0, 0, sizeof(unsigned long long) * 2 * (size_t)L, c.st),
+           "memset");
+        ck(cudaMemsetAsync(chk_rhs + 2 * j0, 0, sizeof(unsigned long long) * 2 * (size_t)L, c.st),
+           "memset");
+        u.chk = chk_lhs;
+        u.chk_v0 = 0;
+    }
     umma::launch_p2_umma(tmA, u, c.st);
+    if (checked) {
+        // the same products on the CUDA cores: u(i) = sum_{k,v} h(k, v) y~_kv(i)
+        // over the pair's digits, then sum_i g_ij u(i) and o_ij u(i) per SNP
+        auto* ub = g.chk_u.as<unsigned long long>((size_t)Np);
+        launch_check_u(static_cast<const int8_t*>(pr.yq.p), Kp * nc, nc, (int)Kp, (int)B, 0, 1, Np,
+                       ub, c.st);
+        for (int64_t j = j0; j < j1; j += 128)
+            chk_tiles.push_back(make_int4((int)j, (int)j1, 0, 0));
+        int4* dt = g.chk_tiles.as<int4>(chk_tiles.size());
+        h2d(dt, chk_tiles.data(), chk_tiles.size(), c.st);
+        launch_check_rhs(P.g.codes, P.g.nbp, dt, (int64_t)chk_tiles.size(), (int)Kp, ub, Np, chk_rhs,
+                         c.st);
+        g.chk_hl.resize(2 * (size_t)L);
+        g.chk_hr.resize(2 * (size_t)L);
+        d2h(g.chk_hl.data(), chk_lhs + 2 * j0, 2 * (size_t)L, c.st);
+        d2h(g.chk_hr.data(), chk_rhs + 2 * j0, 2 * (size_t)L, c.st);
+    }
     }
     const size_t nacc = (size_t)(g.E * total * K);
     double* A[4];
@@ -3567,6 +3619,17 @@ void gxe_target_impl(Context& c, GxeCtx& g, int64_t j0, int64_t j1, GxePair& pr,
     }
     ck(cudaStreamSynchronize(c.st), "gxe target");
     if (stv) fail(LDS_ERR_CUDA, "GxE target tensor-core pipeline wait timed out (code %u)", stv);
+    if (checked) {
+        int64_t first = -1;
+        g.chk_j0 = j0;
+        g.chk_rows = L;
+        g.chk_bad = count_check_mismatches(g.chk_hl.data(), g.chk_hr.data(), L, &first);
+        g.chk_first = first < 0 ? -1 : j0 + first;
+        if (g.chk_bad)
+            fail(LDS_ERR_INTERNAL,
+                 "GxE target product check failed: %lld SNPs disagree (first SNP %lld)",
+                 (long long)g.chk_bad, (long long)g.chk_first);
+    }
 }
 
 void gw_ldscore_impl(const uint8_t* bed_rows, int64_t row_bytes, int64_t n_total, int64_t M,
@@ -4583,9 +4646,6 @@ LDS_API int lds_gw_plan_results(int64_t plan, double* ldscore, double* meansq_ac
     });
 }
 
-static int64_t count_check_mismatches(const unsigned long long* lhs, const unsigned long long* rhs,
-                                      int64_t n_snps, int64_t* first);
-
 LDS_API int lds_gw_plan_set_checks(int64_t plan, int on) {
     return guarded([&] {
         Context& c = ctx();
@@ -4791,20 +4851,6 @@ LDS_API int lds_win_plan_set_tiling(int64_t plan, int p1_sb_per_cta) {
             fail(LDS_ERR_ARG, "p1_sb_per_cta must be in [0, 4096]");
         pl.p1_spc = p1_sb_per_cta;
     });
-}
-
-// SNPs whose G or O checksum pair differs (host comparison); the first one in
-// *first (-1 if none).
-static int64_t count_check_mismatches(const unsigned long long* lhs, const unsigned long long* rhs,
-                                      int64_t n_snps, int64_t* first) {
-    int64_t bad = 0, f = -1;
-    for (int64_t j = 0; j < n_snps; ++j)
-        if (lhs[2 * j] != rhs[2 * j] || lhs[2 * j + 1] != rhs[2 * j + 1]) {
-            if (f < 0) f = j;
-            ++bad;
-        }
-    if (first) *first = f;
-    return bad;
 }
 
 LDS_API int lds_win_plan_set_p2_order(int64_t plan, int bin_chunk) {
@@ -5571,6 +5617,37 @@ LDS_API int lds_gxe_destroy(int64_t gxe) {
         std::lock_guard<std::mutex> lk(c.mu);
         if (c.ready) ck(cudaStreamSynchronize(c.st), "sync");
         gxe_table().erase(gxe);
+    });
+}
+
+LDS_API int lds_gxe_set_checks(int64_t gxe, int on) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        GxeCtx& g = gxe_of(gxe);
+        if (on && !g.P) fail(LDS_ERR_ARG, "product checks need a resident genotype image");
+        g.check = on ? 1 : 0;
+        g.chk_rows = g.chk_bad = 0;
+        g.chk_first = -1;
+    });
+}
+
+LDS_API int lds_gxe_last_check(int64_t gxe, unsigned long long* lhs, unsigned long long* rhs,
+                               int64_t* first_row, int64_t* rows, int64_t* mismatches,
+                               int64_t* first_snp) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        const GxeCtx& g = gxe_of(gxe);
+        if (!g.check) fail(LDS_ERR_ARG, "product checks are off for this context (lds_gxe_set_checks)");
+        if (lhs && g.chk_rows)
+            std::memcpy(lhs, g.chk_hl.data(), sizeof(unsigned long long) * 2 * (size_t)g.chk_rows);
+        if (rhs && g.chk_rows)
+            std::memcpy(rhs, g.chk_hr.data(), sizeof(unsigned long long) * 2 * (size_t)g.chk_rows);
+        if (first_row) *first_row = g.chk_j0;
+        if (rows) *rows = g.chk_rows;
+        if (mismatches) *mismatches = g.chk_bad;
+        if (first_snp) *first_snp = g.chk_first;
     });
 }
 

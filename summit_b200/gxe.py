@@ -27,13 +27,17 @@ def _dp(t):
 class GxeReference:
     def __init__(self, session, environments, feature_basis, power_indices, power_offsets, ranks,
                  gram_values, gram_offsets, e2_gram_values, common_basis, directions,
-                 annotation_bins: int = 1, ddof: int = 1):
+                 annotation_bins: int = 1, ddof: int = 1, product_checks: bool = False):
         self.session = session
         self.kernel = MultiEnvironmentKernel(environments, feature_basis, power_indices,
                                              power_offsets, ranks, gram_values, gram_offsets,
                                              e2_gram_values, common_basis, directions, ddof,
                                              annotation_bins, 1)
         self.h = self.kernel._ctx(session)
+        if product_checks:
+            # exact checksums of the target's tensor-core products, compared
+            # on the host after every target call (a mismatch raises)
+            check(_lib.load().lds_gxe_set_checks(self.h, 1))
         self.E = self.kernel._E
         self.K = int(annotation_bins)
         self.env = np.asfortranarray(environments, dtype=np.float64)
@@ -88,6 +92,24 @@ class GxeReference:
         self.timings["total"] = ev[0].elapsed_time(ev[4])
         return {"accum_xx": accs[0], "accum_xw": accs[1], "accum_wx": accs[2],
                 "accum_ww": accs[3], "leakages": leak, "timings": dict(self.timings)}
+
+    def last_check(self, vectors: bool = False) -> dict:
+        """The last target call's product check: rows checked, mismatching
+        SNPs and the first of them, and with ``vectors`` the per-SNP checksum
+        pairs (rows x 2 each: tensor-core epilogue, CUDA-core recomputation)."""
+        lib = _lib.load()
+        first_row, rows, bad, first = (C.c_int64(0) for _ in range(4))
+        check(lib.lds_gxe_last_check(self.h, None, None, C.byref(first_row), C.byref(rows),
+                                     C.byref(bad), C.byref(first)))
+        out = {"first_row": first_row.value, "rows": rows.value, "mismatches": bad.value,
+               "first_snp": first.value}
+        if vectors:
+            lhs = np.zeros((rows.value, 2), dtype=np.uint64)
+            rhs = np.zeros((rows.value, 2), dtype=np.uint64)
+            check(lib.lds_gxe_last_check(self.h, lhs.ctypes.data_as(C.c_void_p),
+                                         rhs.ctypes.data_as(C.c_void_p), None, None, None, None))
+            out["lhs"], out["rhs"] = lhs, rhs
+        return out
 
     def close(self):
         self.kernel = None

@@ -138,3 +138,63 @@ def test_genome_wide_plan_checks(bigger, impute, vtile):
     for p in (plain, checked):
         p.close()
     sess.close()
+
+
+def test_gxe_target_checks(oracle):
+    """GxE reference build with the target's product checks on: the same
+    accumulators as without them, every SNP's checksum pair equal, and a
+    product error planted in a copy of the checksums is found."""
+    import torch
+
+    from oracle.gxe_oracle import design, rademacher_block
+    from summit_b200 import _lib
+    from summit_b200._lib import check, ptr
+    from summit_b200.gxe import GxeReference
+    from summit_b200.session import GwSession
+
+    n, m, E, K, B, T = 600, 900, 3, 2, 8, 3
+    rows = oracle.synth_bed_rows(n, m, 21)
+    d = design(n, E, seed=4, categorical=1)
+    rng = np.random.default_rng(6)
+    probes = rademacher_block(5, 0, m, range(B))
+    ann = rng.random((m, K)) + 0.05
+    sx = 0.5 + rng.random((m, T))
+    sw = 0.5 + rng.random((m, T))
+    names = ("accum_xx", "accum_xw", "accum_wx", "accum_ww")
+
+    def cm(a):
+        return torch.from_numpy(np.ascontiguousarray(a.T)).cuda().T
+
+    g = GwSession(rows, n)
+    out = {}
+    for checked in (False, True):
+        ref = GxeReference(g, d["environments"], d["feature_basis"], d["power_indices"],
+                           d["power_offsets"], d["ranks"], d["gram_values"], d["gram_offsets"],
+                           d["e2_gram_values"], d["common_basis"], d["directions"], K,
+                           product_checks=checked)
+        res = ref.run(cm(probes), cm(ann), cm(sx), cm(sw), 0)
+        out[checked] = {k: res[k].cpu().numpy() for k in names}
+        if checked:
+            r = ref.last_check(vectors=True)
+            assert r["rows"] == m and r["first_row"] == 0
+            assert r["mismatches"] == 0 and r["first_snp"] == -1
+            assert np.count_nonzero(r["lhs"]) > m
+            np.testing.assert_array_equal(r["lhs"], r["rhs"])
+        else:
+            with pytest.raises(RuntimeError, match="product checks are off"):
+                ref.last_check()
+        ref.close()
+    g.close()
+    for k in names:
+        np.testing.assert_array_equal(out[True][k], out[False][k], err_msg=k)
+
+    def verify(lhs, rhs):
+        bad, first = np.zeros(1, np.int64), np.zeros(1, np.int64)
+        check(_lib.load().lds_check_vectors(ptr(np.ascontiguousarray(lhs)),
+                                            ptr(np.ascontiguousarray(rhs)), m, ptr(bad),
+                                            ptr(first)))
+        return int(bad[0]), int(first[0])
+
+    lhs = r["lhs"].copy()
+    lhs[311, 1] = np.uint64((int(lhs[311, 1]) + 5 * 0x9E3779B97F4A7C15) % (1 << 64))
+    assert verify(lhs, r["rhs"]) == (1, 311)
