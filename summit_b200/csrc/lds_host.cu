@@ -3535,7 +3535,9 @@ void gxe_target_impl(Context& c, GxeCtx& g, int64_t j0, int64_t j1, GxePair& pr,
                                  nullptr, gd, std::numeric_limits<double>::infinity(), 0, c.st);
     } else {
     const Prepared& P = *g.P;
-    const int nb = umma::p2_bins_per_cta(nc, (int)Kp);
+    // several groups per CTA in 256-column MMA groups (16 groups of 400
+    // columns at B = 100: 50 MMA groups per SNP tile instead of 64)
+    const int nb = umma::p2_bins_per_cta_grouped(nc, (int)Kp);
     umma::P2UArgs u;
     u.K = (int)Kp;
     u.V = (int)B;
