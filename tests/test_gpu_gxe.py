@@ -43,8 +43,11 @@ def test_philox_rademacher_matches_numpy():
                                       rademacher_block(91, 1000, rows, range(11)))
 
 
-@pytest.mark.parametrize("T,env_start,K,is_sqrt", [(3, 0, 1, False), (2, 1, 2, True)])
-def test_gxe_products_match_reference(oracle, refgxe, small_bed, T, env_start, K, is_sqrt):
+# B = 40 gives 160 digit columns per group: the target's CTAs then take 8
+# groups each, walked in 256-column MMA groups that split groups.
+@pytest.mark.parametrize("T,env_start,K,is_sqrt,B", [(3, 0, 1, False, 6), (2, 1, 2, True, 6),
+                                                    (2, 0, 2, False, 40)])
+def test_gxe_products_match_reference(oracle, refgxe, small_bed, T, env_start, K, is_sqrt, B):
     from oracle.gxe_oracle import design, rademacher_block
     from summit_b200.session import GwSession
 
@@ -55,7 +58,6 @@ def test_gxe_products_match_reference(oracle, refgxe, small_bed, T, env_start, K
     ref, gpu = _kernels(refgxe, d, K)
     sess = GwSession(packed, n)
     rng = np.random.default_rng(8)
-    B = 6
     cols = T * 2 * K * B
     blocks = [(0, 150), (150, 151), (151, m)]  # includes a one-SNP block
     target_r = np.asfortranarray(rng.normal(size=(n, cols)))
