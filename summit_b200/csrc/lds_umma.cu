@@ -347,8 +347,17 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
                     for (int q = 0; q < 32; ++q) ro[q] = q < live ? cs[q] : 0;
                 }
+                // Checksum weights of the chunk's 8 probes: lane p hashes
+                // probe p's, the loop below broadcasts them.
+                unsigned long long hl = 0ULL;
+                if (a.chk) {
+                    const int gcl = g * 256 + c0 + 4 * (lane & 7);
+                    const int bol = gcl / a.ncolp;
+                    hl = check_weight(k0 + bol, a.chk_v0 + ((gcl - bol * a.ncolp) >> 2));
+                }
 #pragma unroll
                 for (int p = 0; p < 8; ++p) {
+                    const unsigned long long h = a.chk ? __shfl_sync(0xffffffffu, hl, p) : 0ULL;
                     const int gc = g * 256 + c0 + 4 * p;   // column within this CTA's bins
                     const int bo = gc / a.ncolp;            // bin offset (warp-uniform)
                     const int v = (gc - bo * a.ncolp) >> 2;
@@ -364,7 +373,6 @@ __global__ void __launch_bounds__(kThreads, 1)
                         (((long long)ro[4 * p] * 128 + ro[4 * p + 1]) * 128 + ro[4 * p + 2]) * 128 +
                         ro[4 * p + 3];
                     if (a.chk) {
-                        const unsigned long long h = check_weight(k0 + bo, a.chk_v0 + v);
                         chk_g += h * (unsigned long long)TG;
                         chk_o += h * (unsigned long long)TO;
                     }
