@@ -757,6 +757,18 @@ int lds_generalized_pass2(int64_t geno, const double* rhs, int K, int B, int F, 
                           const int* term_off, const int* term_f1, const int* term_f2,
                           double residual_rank, const double* annot, int64_t variant_block,
                           double* directional, double* directed);
+/* lds_generalized_pass2 with the right-hand side formed on the device from
+ * the contextual sources: sources holds K*Q*B rows of N samples (row
+ * (k*Q + s)*B + b: source s of annotation k, probe b; the (K, Q, B, N) array
+ * of GeneralizedGxEPass1Executor's sources), basis is N x Q row-major, and
+ * family f = (fam_t[f], fam_s[f]) gives column (k*B + b)*F + f =
+ * basis[:, t] o sources[k, s][b].  Only the sources and the basis cross PCIe
+ * (K*Q*B*N + N*Q doubles instead of K*B*F*N). */
+int lds_generalized_pass2_sources(int64_t geno, const double* sources, int Q, const double* basis,
+                                  const int* fam_t, const int* fam_s, int K, int B, int F, int P,
+                                  const int* term_off, const int* term_f1, const int* term_f2,
+                                  double residual_rank, const double* annot,
+                                  int64_t variant_block, double* directional, double* directed);
 int lds_generalized_component_diagonal(int64_t geno, int64_t j0, int64_t j1, const double* annot,
                                        int K, const double* basis, int Q, const double* fixed,
                                        int R, const double* coef, double* numerator);

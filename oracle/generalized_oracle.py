@@ -81,6 +81,20 @@ def component_diagonal(X: np.ndarray, j0: int, j1: int, annot_blk, basis, fixed,
             numerator[k * p_count + p] += prod[:, k]
 
 
+def assemble_rhs(rows: np.ndarray, basis: np.ndarray, fam_t, fam_s) -> np.ndarray:
+    """Pass 2's right-hand side (generalized_gxe_pass2.py:401-415): N x K*B*F,
+    column (k*B + b)*F + f = basis[:, t] * sources[k, s][b] for family
+    f = (fam_t[f], fam_s[f]); rows is the (K, Q, B, N) source array."""
+    k_count, _, b_count, n = rows.shape
+    f_count = len(fam_t)
+    rhs = np.empty((n, k_count * b_count * f_count))
+    for k in range(k_count):
+        for b in range(b_count):
+            for f in range(f_count):
+                rhs[:, (k * b_count + b) * f_count + f] = basis[:, fam_t[f]] * rows[k, fam_s[f], b]
+    return rhs
+
+
 def pass2_scores(X: np.ndarray, rhs: np.ndarray, k_count: int, b_count: int, f_count: int,
                  p_count: int, term_off, term_f1, term_f2, residual_rank: float,
                  annot: np.ndarray):

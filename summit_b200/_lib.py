@@ -73,6 +73,8 @@ SIGNATURES: dict[str, tuple] = {
                                                   _p, _p]),
     "lds_generalized_pass2": (_int, [_i64, _p, _int, _int, _int, _int, _p, _p, _p, _dbl, _p, _i64,
                                      _p, _p]),
+    "lds_generalized_pass2_sources": (_int, [_i64, _p, _int, _p, _p, _p, _int, _int, _int, _int,
+                                             _p, _p, _p, _dbl, _p, _i64, _p, _p]),
     "lds_win_plan_destroy": (_int, [_i64]),
     "lds_win_plan_set_cv": (_int, [_i64, _p, _int, _int]),
     "lds_win_plan_tiles": (_int, [_i64, _p, _p]),

@@ -4,6 +4,7 @@
 // The genotype products of both passes run on the tensor-core kernels
 // (lds_umma_p1.cu, lds_umma.cu) through lds_geno_source_product /
 // lds_geno_target_product.
+#include <algorithm>
 #include <cstdint>
 
 #include "lds_device.cuh"
@@ -140,7 +141,40 @@ __global__ void gen_directed_kernel(const double* __restrict__ rows, int64_t L,
     directed[idx] += s;
 }
 
+// Pass 2's right-hand side from the contextual sources
+// (GeneralizedGxEPass2Executor's family columns, generalized_gxe_pass2.py):
+// column (k B + b) F + f = phi_t o sources[k, s][:, b] for family f = (t, s).
+// S holds the sources as K Q B rows of N_pad samples, basis is N x Q
+// row-major; Y gets one column of N_pad samples per (k, b, f), rows N and
+// beyond left as they are (zero).
+__global__ void gen_assemble_rhs_kernel(const double* __restrict__ S, int64_t Np,
+                                        const double* __restrict__ basis, int Q,
+                                        const int* __restrict__ fam_t,
+                                        const int* __restrict__ fam_s, int B, int F, int64_t N,
+                                        double* __restrict__ Y) {
+    const int col = blockIdx.y;
+    const int f = col % F, kb = col / F;
+    const int b = kb % B, k = kb / B;
+    const int t = fam_t[f], s = fam_s[f];
+    const double* src = S + ((int64_t)(k * Q + s) * B + b) * Np;
+    double* dst = Y + (int64_t)col * Np;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < N;
+         n += (int64_t)gridDim.x * blockDim.x)
+        dst[n] = src[n] * basis[n * Q + t];
+}
+
 }  // namespace
+
+void launch_gen_assemble_rhs(const double* S, int64_t Np, const double* basis, int Q,
+                             const int* fam_t, const int* fam_s, int K, int B, int F, int64_t N,
+                             double* Y, cudaStream_t st) {
+    const int cols = K * B * F;
+    if (cols <= 0 || N <= 0) return;
+    const unsigned bx = (unsigned)std::min<int64_t>((N + 255) / 256, 64);
+    gen_assemble_rhs_kernel<<<dim3(bx, (unsigned)cols), 256, 0, st>>>(S, Np, basis, Q, fam_t, fam_s,
+                                                                     B, F, N, Y);
+    count_launch();
+}
 
 size_t gen_rows_smem_bytes(int cols) { return (size_t)cols * sizeof(double); }
 

@@ -5519,15 +5519,17 @@ LDS_API int lds_generalized_component_diagonal(int64_t geno, int64_t j0, int64_t
     });
 }
 
-LDS_API int lds_generalized_pass2(int64_t geno, const double* rhs, int K, int B, int F, int P,
-                                  const int* term_off, const int* term_f1, const int* term_f2,
-                                  double residual_rank, const double* annot,
-                                  int64_t variant_block, double* directional, double* directed) {
-    return guarded([&] {
-        Context& c = ctx();
-        std::lock_guard<std::mutex> lk(c.mu);
+// Pass 2 of the generalized estimator on the device; `fill` writes the
+// right-hand side's K B F columns (N_pad samples each, rows past N zero) into
+// the zeroed FP64 workspace Y.
+static void gen_pass2_run(Context& c, int64_t geno,
+                          const std::function<void(double* Y, int64_t N, int64_t Np)>& fill,
+                          int K, int B, int F, int P, const int* term_off, const int* term_f1,
+                          const int* term_f2, double residual_rank, const double* annot,
+                          int64_t variant_block, double* directional, double* directed) {
+    {
         ensure_device(c);
-        if (!rhs || !term_off || !term_f1 || !term_f2 || !annot || !directional || !directed ||
+        if (!term_off || !term_f1 || !term_f2 || !annot || !directional || !directed ||
             K <= 0 || B <= 0 || F <= 0 || P <= 0 || variant_block <= 0 || !(residual_rank > 0.0))
             fail(LDS_ERR_ARG, "invalid generalized pass-2 arguments");
         const int cols = K * B * F;
@@ -5550,9 +5552,7 @@ LDS_API int lds_generalized_pass2(int64_t geno, const double* rhs, int K, int B,
         DevBuf dY, dyq, dcs, dann, dto, df1, df2, ddir, drg, dro, drows, dst;
         double* Y = dY.as<double>((size_t)(Np * ld));
         ck(cudaMemsetAsync(Y, 0, sizeof(double) * (size_t)(Np * ld), c.st), "memset");
-        ck(cudaMemcpy2DAsync(Y, sizeof(double) * (size_t)Np, rhs, sizeof(double) * (size_t)N,
-                             sizeof(double) * (size_t)N, (size_t)cols, cudaMemcpyHostToDevice, c.st),
-           "rhs upload");
+        fill(Y, N, Np);
         int8_t* yq = dyq.as<int8_t>((size_t)((int64_t)K2 * nc * Np));
         double* cs = dcs.as<double>((size_t)ld);
         umma::launch_quantize_y4(Y, N, Np, K2, kV2, nc, yq, cs, c.st);
@@ -5610,6 +5610,68 @@ LDS_API int lds_generalized_pass2(int64_t geno, const double* rhs, int K, int B,
         d2h(&hst, stv, 1, c.st);
         ck(cudaStreamSynchronize(c.st), "generalized pass 2");
         if (hst) fail(LDS_ERR_CUDA, "phase-2 tensor-core pipeline wait timed out (code %u)", hst);
+    }
+}
+
+LDS_API int lds_generalized_pass2(int64_t geno, const double* rhs, int K, int B, int F, int P,
+                                  const int* term_off, const int* term_f1, const int* term_f2,
+                                  double residual_rank, const double* annot,
+                                  int64_t variant_block, double* directional, double* directed) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        if (!rhs) fail(LDS_ERR_ARG, "invalid generalized pass-2 arguments");
+        const int cols = K * B * F;
+        gen_pass2_run(
+            c, geno,
+            [&](double* Y, int64_t N, int64_t Np) {
+                ck(cudaMemcpy2DAsync(Y, sizeof(double) * (size_t)Np, rhs, sizeof(double) * (size_t)N,
+                                     sizeof(double) * (size_t)N, (size_t)cols,
+                                     cudaMemcpyHostToDevice, c.st),
+                   "rhs upload");
+            },
+            K, B, F, P, term_off, term_f1, term_f2, residual_rank, annot, variant_block,
+            directional, directed);
+    });
+}
+
+LDS_API int lds_generalized_pass2_sources(int64_t geno, const double* sources, int Q,
+                                          const double* basis, const int* fam_t,
+                                          const int* fam_s, int K, int B, int F, int P,
+                                          const int* term_off, const int* term_f1,
+                                          const int* term_f2, double residual_rank,
+                                          const double* annot, int64_t variant_block,
+                                          double* directional, double* directed) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        if (!sources || !basis || !fam_t || !fam_s || Q <= 0 || F <= 0)
+            fail(LDS_ERR_ARG, "invalid generalized pass-2 arguments");
+        for (int f = 0; f < F; ++f)
+            if (fam_t[f] < 0 || fam_t[f] >= Q || fam_s[f] < 0 || fam_s[f] >= Q)
+                fail(LDS_ERR_ARG, "family basis index out of range");
+        DevBuf dS, dbasis, dft, dfs;
+        gen_pass2_run(
+            c, geno,
+            [&](double* Y, int64_t N, int64_t Np) {
+                // the sources (K Q B rows of N samples) and the basis cross
+                // PCIe; the K B F family columns are formed on the device
+                const int64_t rows = (int64_t)K * Q * B;
+                double* S = dS.as<double>((size_t)(rows * Np));
+                ck(cudaMemcpy2DAsync(S, sizeof(double) * (size_t)Np, sources,
+                                     sizeof(double) * (size_t)N, sizeof(double) * (size_t)N,
+                                     (size_t)rows, cudaMemcpyHostToDevice, c.st),
+                   "sources upload");
+                double* bs = dbasis.as<double>((size_t)(N * Q));
+                h2d(bs, basis, (size_t)(N * Q), c.st);
+                int* ft = dft.as<int>((size_t)F);
+                int* fs = dfs.as<int>((size_t)F);
+                h2d(ft, fam_t, (size_t)F, c.st);
+                h2d(fs, fam_s, (size_t)F, c.st);
+                launch_gen_assemble_rhs(S, Np, bs, Q, ft, fs, K, B, F, N, Y, c.st);
+            },
+            K, B, F, P, term_off, term_f1, term_f2, residual_rank, annot, variant_block,
+            directional, directed);
     });
 }
 

@@ -123,6 +123,26 @@ def _pass2_scores(session, rhs, k_count, b_count, f_count, p_count, term_off, te
     return directional, directed
 
 
+def _pass2_scores_sources(session, rows, basis, fam_t, fam_s, k_count, b_count, p_count,
+                          term_off, term_f1, term_f2, residual_rank, weights, block):
+    """_pass2_scores with the right-hand side formed on the device from the
+    sources (K x Q x B x N rows) and the basis (lds_generalized_pass2_sources):
+    only they cross PCIe, not the K*B*F columns."""
+    m, c_count = session.M, k_count * p_count
+    directional = np.empty((m, p_count, c_count))
+    directed = np.empty((c_count, c_count))
+    src = np.ascontiguousarray(rows, dtype=np.float64)
+    bas = np.ascontiguousarray(basis, dtype=np.float64)
+    ft = np.ascontiguousarray(fam_t, dtype=np.int32)
+    fs = np.ascontiguousarray(fam_s, dtype=np.int32)
+    a = np.ascontiguousarray(weights, dtype=np.float64)
+    check(_lib.load().lds_generalized_pass2_sources(
+        session.handle, ptr(src), int(bas.shape[1]), ptr(bas), ptr(ft), ptr(fs), k_count, b_count,
+        len(ft), p_count, ptr(term_off), ptr(term_f1), ptr(term_f2), float(residual_rank), ptr(a),
+        int(block), ptr(directional), ptr(directed)))
+    return directional, directed
+
+
 def pair_order(q_count: int) -> tuple[tuple[int, int], ...]:
     """Diagonal-first unordered basis pairs (context/spec.py ContextPairIndex)."""
     return tuple((q, q) for q in range(q_count)) + tuple(
@@ -249,15 +269,11 @@ def pass2(session, pass1_result: GeneralizedPass1Result, basis, fixed_effect_bas
     families = tuple((u, v) for u in range(q_count)
                      for v in range(u if symmetric_cross else 0, q_count))
     f_count = len(families)
-    # rhs column (k * B + b) * F + f = phi_t o sources[k, s][:, b] for family f = (t, s)
-    rows = np.swapaxes(sources, 2, 3)   # K x Q x B x N (contiguous for pass-1 results)
-    # (K, B, F, N) in C order is exactly the column-major N x K*B*F layout
-    # (column (k*B + b)*F + f), filled by contiguous B x N blocks.
-    slab = np.empty((k_count, b_count, f_count, n))
-    for k in range(k_count):
-        for f, (t, s) in enumerate(families):
-            np.multiply(rows[k, s], basis[:, t], out=slab[k, :, f, :])
-    rhs = slab.reshape(k_count * b_count * f_count, n).T
+    # rhs column (k * B + b) * F + f = phi_t o sources[k, s][:, b] for family
+    # f = (t, s), formed on the device from the K x Q x B x N source rows
+    rows = np.swapaxes(sources, 2, 3)   # contiguous for pass-1 results
+    fam_t = np.array([t for t, _ in families], dtype=np.int32)
+    fam_s = np.array([s for _, s in families], dtype=np.int32)
     weighted_fixed = np.asfortranarray(
         (basis[:, :, None] * fixed[:, None, :]).reshape(n, q_count * r_count)) if r_count else None
     # Orientation terms of every (target pair, source pair): products of the
@@ -283,10 +299,10 @@ def pass2(session, pass1_result: GeneralizedPass1Result, basis, fixed_effect_bas
             cf = _target_product(session, j0, j1, weighted_fixed)
             coef = np.ascontiguousarray(cf.reshape(j1 - j0, q_count, r_count))
         _component_diagonal(session, j0, j1, weights[j0:j1], basis, fixed, coef, diag_num)
-    directional, directed = _pass2_scores(
-        session, rhs, k_count, b_count, f_count, p_count, np.asarray(term_off, np.int32),
-        np.asarray(term_f1, np.int32), np.asarray(term_f2, np.int32), float(residual_rank),
-        weights, variant_block_width)
+    directional, directed = _pass2_scores_sources(
+        session, rows, basis, fam_t, fam_s, k_count, b_count, p_count,
+        np.asarray(term_off, np.int32), np.asarray(term_f1, np.int32),
+        np.asarray(term_f2, np.int32), float(residual_rank), weights, variant_block_width)
     if not np.all(np.isfinite(directional)):
         raise RuntimeError("per-variant directional scores are non-finite")
     pre_abs = float(np.max(np.abs(directed - directed.T), initial=0.0))

@@ -50,9 +50,10 @@ def test_driver_algebra_matches_reference(monkeypatch, decoded, case, width):
     monkeypatch.setattr(gg, "_target_product", lambda s, a, b, Y: go.target_product(X, a, b, Y))
     monkeypatch.setattr(gg, "_component_diagonal",
                         lambda s, a, b, ab, ba, fx, cf, num: go.component_diagonal(X, a, b, ab, ba, fx, cf, num))
-    monkeypatch.setattr(gg, "_pass2_scores",
-                        lambda s, rhs, k, b, f, p, to, f1, f2, rr, a, blk: go.pass2_scores(
-                            X, rhs, k, b, f, p, to, f1, f2, rr, a))
+    monkeypatch.setattr(gg, "_pass2_scores_sources",
+                        lambda s, rows, bas, ft, fs, k, b, p, to, f1, f2, rr, a, blk: go.pass2_scores(
+                            X, go.assemble_rhs(rows, bas, ft, fs), k, b, len(ft), p, to, f1, f2,
+                            rr, a))
     monkeypatch.setattr(gg, "global_variant_probes",
                         lambda spec, v0, cnt: go.global_probes(spec.root_seed, range(v0, v0 + cnt),
                                                                range(spec.probe_offset, spec.probe_offset + spec.probe_count),

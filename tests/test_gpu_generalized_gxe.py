@@ -80,6 +80,39 @@ def test_device_products_match_dense_products(session, decoded):
         assert np.abs(num - ref).max() <= 1e-12 * np.abs(ref).max()
 
 
+def test_device_rhs_assembly_matches_host_rhs(session, decoded):
+    """Pass-2 scores from the sources (right-hand side formed on the device)
+    equal the scores from the host-assembled right-hand side bit for bit."""
+    from oracle import generalized_oracle as go
+    from summit_b200 import generalized_gxe as gg
+
+    n, m = decoded.shape
+    rng = np.random.default_rng(12)
+    K, Q, B, P = 2, 3, 5, 6
+    rows = rng.normal(size=(K, Q, B, n))
+    basis = rng.normal(size=(n, Q))
+    fam = [(t, s) for t in range(Q) for s in range(Q)]
+    ft = np.array([t for t, _ in fam], np.int32)
+    fs = np.array([s for _, s in fam], np.int32)
+    pairs = gg.pair_order(Q)
+    term_off, term_f1, term_f2 = [0], [], []
+    for tp in pairs:
+        for sp in pairs:
+            for tl, tr in gg._orientations(tp):
+                for sl, sr in gg._orientations(sp):
+                    term_f1.append(tr * Q + sl)
+                    term_f2.append(tl * Q + sr)
+            term_off.append(len(term_f1))
+    to, f1, f2 = (np.asarray(x, np.int32) for x in (term_off, term_f1, term_f2))
+    annot = rng.uniform(0.0, 1.0, size=(m, K))
+    rhs = go.assemble_rhs(rows, basis, ft, fs)
+    want = gg._pass2_scores(session, rhs, K, B, len(fam), P, to, f1, f2, float(n - 1), annot, 97)
+    got = gg._pass2_scores_sources(session, rows, basis, ft, fs, K, B, P, to, f1, f2,
+                                   float(n - 1), annot, 97)
+    np.testing.assert_array_equal(got[0], want[0])
+    np.testing.assert_array_equal(got[1], want[1])
+
+
 @pytest.mark.parametrize("case", CASES)
 def test_two_pass_matches_reference_executors(session, case):
     from summit_b200 import generalized_gxe as gg
