@@ -757,6 +757,17 @@ int lds_generalized_pass2(int64_t geno, const double* rhs, int K, int B, int F, 
                           const int* term_off, const int* term_f1, const int* term_f2,
                           double residual_rank, const double* annot, int64_t variant_block,
                           double* directional, double* directed);
+/* Pass 1's projection of the contextual sources off the fixed effects
+ * (GeneralizedGxEPass1Executor, generalized_gxe_pass1.py:718-757): base holds
+ * K*B rows of N samples ((K, B, N): base source of annotation k, probe b),
+ * basis N x Q and fixed N x R row-major (R <= 16, R = 0: no projection).
+ * contextual (K*Q*B rows of N: row (k*Q + q)*B + b) = w - fixed fixed^T w with
+ * w = basis[:, q] o base[k, b], in FP64 on the device.  max_abs / max_rel get
+ * the reference's leakage measures: the largest |fixed^T p| entry and, over
+ * (k, q), ||fixed^T P||_F / max(1, ||P||_F). */
+int lds_generalized_project(const double* base, const double* basis, const double* fixed, int K,
+                            int Q, int B, int R, int64_t N, double* contextual, double* max_abs,
+                            double* max_rel);
 /* lds_generalized_pass2 with the right-hand side formed on the device from
  * the contextual sources: sources holds K*Q*B rows of N samples (row
  * (k*Q + s)*B + b: source s of annotation k, probe b; the (K, Q, B, N) array

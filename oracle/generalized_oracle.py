@@ -81,6 +81,30 @@ def component_diagonal(X: np.ndarray, j0: int, j1: int, annot_blk, basis, fixed,
             numerator[k * p_count + p] += prod[:, k]
 
 
+def project_sources(base: np.ndarray, basis: np.ndarray, fixed: np.ndarray):
+    """Pass 1's projection (generalized_gxe_pass1.py:718-757): contextual
+    sources (K, Q, B, N) = w - fixed (fixed^T w) with w = basis[:, q] * base[k]
+    (base (K, B, N)), and the maximum absolute and relative leakage of
+    fixed^T p (zero without fixed effects)."""
+    k_count, b_count, n = base.shape
+    q_count = basis.shape[1]
+    contextual = np.empty((k_count, q_count, b_count, n))
+    max_abs = max_rel = 0.0
+    for k in range(k_count):
+        for q in range(q_count):
+            weighted = base[k] * basis[:, q]
+            if not fixed.shape[1]:
+                contextual[k, q] = weighted
+                continue
+            projected = weighted - (weighted @ fixed) @ fixed.T
+            contextual[k, q] = projected
+            leakage = projected @ fixed
+            max_abs = max(max_abs, float(np.max(np.abs(leakage), initial=0.0)))
+            max_rel = max(max_rel, float(np.linalg.norm(leakage)
+                                         / max(1.0, float(np.linalg.norm(projected)))))
+    return contextual, max_abs, max_rel
+
+
 def assemble_rhs(rows: np.ndarray, basis: np.ndarray, fam_t, fam_s) -> np.ndarray:
     """Pass 2's right-hand side (generalized_gxe_pass2.py:401-415): N x K*B*F,
     column (k*B + b)*F + f = basis[:, t] * sources[k, s][b] for family

@@ -73,6 +73,7 @@ SIGNATURES: dict[str, tuple] = {
                                                   _p, _p]),
     "lds_generalized_pass2": (_int, [_i64, _p, _int, _int, _int, _int, _p, _p, _p, _dbl, _p, _i64,
                                      _p, _p]),
+    "lds_generalized_project": (_int, [_p, _p, _p, _int, _int, _int, _int, _i64, _p, _p, _p]),
     "lds_generalized_pass2_sources": (_int, [_i64, _p, _int, _p, _p, _p, _int, _int, _int, _int,
                                              _p, _p, _p, _dbl, _p, _i64, _p, _p]),
     "lds_win_plan_destroy": (_int, [_i64]),

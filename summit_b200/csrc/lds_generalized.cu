@@ -163,7 +163,90 @@ __global__ void gen_assemble_rhs_kernel(const double* __restrict__ S, int64_t Np
         dst[n] = src[n] * basis[n * Q + t];
 }
 
+// Pass 1's projection of the contextual sources off the fixed effects
+// (GeneralizedGxEPass1Executor, generalized_gxe_pass1.py:718-757), one CTA per
+// (annotation k, basis coordinate q, probe b): with w = basis[:, q] o
+// base[k, b], coef = fixed^T w, the row is p = w - fixed coef, written to out;
+// leak = fixed^T p (R values) and p^T p are reduced in a fixed order for the
+// host's leakage check.  base is K B rows of N samples, basis N x Q and fixed
+// N x R row-major.
+constexpr int kProjThreads = 256;
+
+// Sums v[0..n) over the CTA (warp trees, then warps in order); the totals
+// land in tot[0..n) for every thread.
+template <int kMax>
+__device__ __forceinline__ void block_sum(double (&v)[kMax], int n, double (*red)[kMax],
+                                          double* tot) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int r = 0; r < kMax; ++r) {
+        if (r >= n) break;
+        double x = v[r];
+        for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) red[w][r] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < n) {
+        double t = 0.0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i][threadIdx.x];
+        tot[threadIdx.x] = t;
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kProjThreads)
+    gen_project_kernel(const double* __restrict__ base, const double* __restrict__ basis, int Q,
+                       const double* __restrict__ fixed, int R, int B, int64_t N,
+                       double* __restrict__ out, double* __restrict__ leak,
+                       double* __restrict__ pn2) {
+    constexpr int kM = kGenMaxR + 1;
+    __shared__ double red[kProjThreads / 32][kM];
+    __shared__ double coef[kM];
+    const int row = blockIdx.x;  // (k Q + q) B + b
+    const int b = row % B, kq = row / B, q = kq % Q, k = kq / Q;
+    const double* src = base + ((int64_t)k * B + b) * N;
+    double* dst = out + (int64_t)row * N;
+    double acc[kM];
+#pragma unroll
+    for (int r = 0; r < kM; ++r) acc[r] = 0.0;
+    for (int64_t n = threadIdx.x; n < N; n += blockDim.x) {
+        const double w = src[n] * basis[n * Q + q];
+#pragma unroll
+        for (int r = 0; r < kGenMaxR; ++r)
+            if (r < R) acc[r] += w * fixed[n * R + r];
+    }
+    block_sum<kM>(acc, R, red, coef);
+#pragma unroll
+    for (int r = 0; r < kM; ++r) acc[r] = 0.0;  // leak[0..R), p^T p at R
+    for (int64_t n = threadIdx.x; n < N; n += blockDim.x) {
+        const double w = src[n] * basis[n * Q + q];
+        double fc = 0.0;
+#pragma unroll
+        for (int r = 0; r < kGenMaxR; ++r)
+            if (r < R) fc += fixed[n * R + r] * coef[r];
+        const double p = w - fc;
+        dst[n] = p;
+#pragma unroll
+        for (int r = 0; r < kGenMaxR; ++r)
+            if (r < R) acc[r] += p * fixed[n * R + r];
+        acc[R < kGenMaxR ? R : kGenMaxR] += p * p;
+    }
+    block_sum<kM>(acc, R + 1, red, coef);
+    if (threadIdx.x < R) leak[(int64_t)row * R + threadIdx.x] = coef[threadIdx.x];
+    if (threadIdx.x == 0) pn2[row] = coef[R];
+}
+
 }  // namespace
+
+void launch_gen_project(const double* base, const double* basis, int Q, const double* fixed,
+                        int R, int K, int B, int64_t N, double* out, double* leak, double* pn2,
+                        cudaStream_t st) {
+    const int rows = K * Q * B;
+    if (rows <= 0 || N <= 0) return;
+    gen_project_kernel<<<(unsigned)rows, kProjThreads, 0, st>>>(base, basis, Q, fixed, R, B, N, out,
+                                                               leak, pn2);
+    count_launch();
+}
 
 void launch_gen_assemble_rhs(const double* S, int64_t Np, const double* basis, int Q,
                              const int* fam_t, const int* fam_s, int K, int B, int F, int64_t N,

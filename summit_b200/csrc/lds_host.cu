@@ -5635,6 +5635,59 @@ LDS_API int lds_generalized_pass2(int64_t geno, const double* rhs, int K, int B,
     });
 }
 
+LDS_API int lds_generalized_project(const double* base, const double* basis, const double* fixed,
+                                    int K, int Q, int B, int R, int64_t N, double* contextual,
+                                    double* max_abs, double* max_rel) {
+    return guarded([&] {
+        Context& c = ctx();
+        std::lock_guard<std::mutex> lk(c.mu);
+        ensure_device(c);
+        if (!base || !basis || (R > 0 && !fixed) || !contextual || K <= 0 || Q <= 0 || B <= 0 ||
+            R < 0 || R > kGenMaxR || N <= 0)
+            fail(LDS_ERR_ARG, "invalid generalized projection arguments");
+        const int64_t rows = (int64_t)K * Q * B;
+        DevBuf dbase, dbasis, dfixed, dout, dleak, dpn;
+        double* db = dbase.as<double>((size_t)((int64_t)K * B * N));
+        h2d(db, base, (size_t)((int64_t)K * B * N), c.st);
+        double* dq = dbasis.as<double>((size_t)(N * Q));
+        h2d(dq, basis, (size_t)(N * Q), c.st);
+        double* df = nullptr;
+        if (R > 0) {
+            df = dfixed.as<double>((size_t)(N * R));
+            h2d(df, fixed, (size_t)(N * R), c.st);
+        }
+        double* o = dout.as<double>((size_t)(rows * N));
+        double* lk2 = dleak.as<double>((size_t)std::max<int64_t>(rows * R, 1));
+        double* pn = dpn.as<double>((size_t)rows);
+        launch_gen_project(db, dq, Q, df, R, K, B, N, o, lk2, pn, c.st);
+        ck(cudaGetLastError(), "launch");
+        std::vector<double> hl((size_t)(rows * R)), hp((size_t)rows);
+        d2h(contextual, o, (size_t)(rows * N), c.st);
+        if (R > 0) d2h(hl.data(), lk2, hl.size(), c.st);
+        d2h(hp.data(), pn, hp.size(), c.st);
+        ck(cudaStreamSynchronize(c.st), "generalized projection");
+        // the reference's leakage measures: the largest |fixed^T p| entry, and
+        // per (k, q) ||fixed^T P||_F / max(1, ||P||_F); zero without fixed effects
+        double mabs = 0.0, mrel = 0.0;
+        if (R > 0)
+            for (int64_t kq = 0; kq < (int64_t)K * Q; ++kq) {
+                double l2 = 0.0, p2 = 0.0;
+                for (int b = 0; b < B; ++b) {
+                    const int64_t row = kq * B + b;
+                    p2 += hp[(size_t)row];
+                    for (int r = 0; r < R; ++r) {
+                        const double v = hl[(size_t)(row * R + r)];
+                        mabs = std::max(mabs, std::fabs(v));
+                        l2 += v * v;
+                    }
+                }
+                mrel = std::max(mrel, std::sqrt(l2) / std::max(1.0, std::sqrt(p2)));
+            }
+        if (max_abs) *max_abs = mabs;
+        if (max_rel) *max_rel = mrel;
+    });
+}
+
 LDS_API int lds_generalized_pass2_sources(int64_t geno, const double* sources, int Q,
                                           const double* basis, const int* fam_t,
                                           const int* fam_s, int K, int B, int F, int P,

@@ -182,6 +182,9 @@ void launch_global_probes(uint64_t root_state, int64_t v0, int64_t L, int64_t p0
 // numerator accumulation.
 constexpr int kGenRowsMaxSmem = 200 * 1024;
 size_t gen_rows_smem_bytes(int cols);
+void launch_gen_project(const double* base, const double* basis, int Q, const double* fixed,
+                        int R, int K, int B, int64_t N, double* out, double* leak, double* pn2,
+                        cudaStream_t st);
 void launch_gen_assemble_rhs(const double* S, int64_t Np, const double* basis, int Q,
                              const int* fam_t, const int* fam_s, int K, int B, int F, int64_t N,
                              double* Y, cudaStream_t st);

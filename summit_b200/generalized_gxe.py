@@ -21,6 +21,7 @@ factor 1 on the diagonal and 2 off it; components are annotation-major
 """
 from __future__ import annotations
 
+import ctypes as C
 from dataclasses import dataclass
 
 import numpy as np
@@ -123,6 +124,23 @@ def _pass2_scores(session, rhs, k_count, b_count, f_count, p_count, term_off, te
     return directional, directed
 
 
+def _project_sources(base, basis, fixed):
+    """Pass 1's projection on the device (lds_generalized_project): the
+    contextual sources (K x Q x B x N) of the base sources (K x B x N), and the
+    maximum absolute and relative leakage."""
+    k_count, b_count, n = base.shape
+    q_count, r_count = basis.shape[1], fixed.shape[1]
+    out = np.empty((k_count, q_count, b_count, n))
+    b_ = np.ascontiguousarray(base, dtype=np.float64)
+    q_ = np.ascontiguousarray(basis, dtype=np.float64)
+    f_ = np.ascontiguousarray(fixed, dtype=np.float64) if r_count else None
+    mabs, mrel = C.c_double(0.0), C.c_double(0.0)
+    check(_lib.load().lds_generalized_project(
+        ptr(b_), ptr(q_), ptr(f_) if r_count else None, k_count, q_count, b_count, r_count, n,
+        ptr(out), C.byref(mabs), C.byref(mrel)))
+    return out, mabs.value, mrel.value
+
+
 def _pass2_scores_sources(session, rows, basis, fam_t, fam_s, k_count, b_count, p_count,
                           term_off, term_f1, term_f2, residual_rank, weights, block):
     """_pass2_scores with the right-hand side formed on the device from the
@@ -211,20 +229,7 @@ def pass1(session, basis, fixed_effect_basis, annotations, probe_spec: GlobalVar
         z = global_variant_probes(probe_spec, j0, j1 - j0)
         out = _source_product(session, j0, j1, weights[j0:j1], z)
         base += out.T.reshape(k_count, b_count, n)
-    contextual = np.empty((k_count, q_count, b_count, n))
-    max_abs = max_rel = 0.0
-    for k in range(k_count):
-        for q in range(q_count):
-            weighted = base[k] * basis[:, q]
-            if not fixed.shape[1]:
-                contextual[k, q] = weighted
-                continue
-            projected = weighted - (weighted @ fixed) @ fixed.T
-            contextual[k, q] = projected
-            leakage = projected @ fixed
-            max_abs = max(max_abs, float(np.max(np.abs(leakage), initial=0.0)))
-            max_rel = max(max_rel, float(np.linalg.norm(leakage)
-                                         / max(1.0, float(np.linalg.norm(projected)))))
+    contextual, max_abs, max_rel = _project_sources(base, basis, fixed)
     if max_rel > projection_tolerance:
         raise RuntimeError("contextual source projection leakage exceeds its tolerance")
     contextual = contextual.transpose(0, 1, 3, 2)

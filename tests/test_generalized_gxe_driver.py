@@ -50,6 +50,7 @@ def test_driver_algebra_matches_reference(monkeypatch, decoded, case, width):
     monkeypatch.setattr(gg, "_target_product", lambda s, a, b, Y: go.target_product(X, a, b, Y))
     monkeypatch.setattr(gg, "_component_diagonal",
                         lambda s, a, b, ab, ba, fx, cf, num: go.component_diagonal(X, a, b, ab, ba, fx, cf, num))
+    monkeypatch.setattr(gg, "_project_sources", go.project_sources)
     monkeypatch.setattr(gg, "_pass2_scores_sources",
                         lambda s, rows, bas, ft, fs, k, b, p, to, f1, f2, rr, a, blk: go.pass2_scores(
                             X, go.assemble_rhs(rows, bas, ft, fs), k, b, len(ft), p, to, f1, f2,

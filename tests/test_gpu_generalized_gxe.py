@@ -127,3 +127,27 @@ def test_two_pass_matches_reference_executors(session, case):
                 "genetic_gram", "component_kernel_diagonal", "same_person"):
         assert_rel_elementwise(getattr(p2, key), GOLD[f"{case}/{key}"], 1e-6, key,
                                atol_frac=1e-7)
+
+
+@pytest.mark.parametrize("r", [0, 2, 5])
+def test_device_projection_matches_numpy(r):
+    """Pass 1's projection on the device against the NumPy restatement: the
+    contextual sources to 1e-12 of their scale, the leakage measures tiny on
+    both sides (orthonormal fixed effects)."""
+    from oracle import generalized_oracle as go
+    from summit_b200 import generalized_gxe as gg
+
+    rng = np.random.default_rng(20 + r)
+    K, Q, B, n = 3, 4, 7, 5003
+    base = rng.normal(size=(K, B, n))
+    basis = rng.normal(size=(n, Q))
+    fixed = np.linalg.qr(rng.normal(size=(n, max(r, 1))))[0][:, :r]
+    got, gabs, grel = gg._project_sources(base, basis, fixed)
+    want, wabs, wrel = go.project_sources(base, basis, fixed)
+    assert got.shape == want.shape == (K, Q, B, n)
+    assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max()
+    if r:
+        assert 0.0 < gabs < 1e-10 and 0.0 <= grel < 1e-12 and wrel < 1e-12
+    else:
+        np.testing.assert_array_equal(got, want)
+        assert gabs == grel == 0.0
