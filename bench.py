@@ -1047,8 +1047,9 @@ def generalized_arm(args) -> None:
         "data": "synthetic (seeded HWE/AR(1) generator; global variant x probe signs on device)",
         "config": {"workload": GEN_WORKLOAD, "N": n, "M": m, "Q": GEN_Q, "R": GEN_R, "K": GEN_K,
                    "B": GEN_B, "rhs_columns": GEN_K * GEN_B * families,
-                   "timing": "wall clock from the resident image to host results (host FP64 "
-                             "projection and orientation-term set-up included)"},
+                   "timing": "wall clock from the resident image to host results (host "
+                             "orientation-term set-up and PCIe transfers between the steps "
+                             "included)"},
         "e2e": {"value": round(ops / e2e_s / 1e12, 3), "unit": "TOPS",
                 "h2d_bytes_per_step": int(bed.nbytes),
                 "d2h_bytes_per_step": int(p2.directional_ldscores.nbytes),
