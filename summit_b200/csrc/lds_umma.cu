@@ -1,19 +1,23 @@
 // Phase 2 on 5th-generation tensor cores (tcgen05, sm_100a).
 //
-// Work[j, c] = x_j^T Y[:, c] for a tile of 128 SNPs and one annotation bin,
-// with the LD-score epilogue, as in p2_kernel (lds_kernels.cu) but with:
+// Work[j, c] = x_j^T Y[:, c] for a tile of 128 SNPs and the CTA's annotation
+// bins, with the LD-score epilogue, as in p2_kernel (lds_kernels.cu) but with:
 //   * a TMA tile copy (cp.async.bulk.tensor into the CTA's own shared memory)
 //     bringing the packed 2-bit genotype tile (128 SNPs x 128 samples = 4 KB),
-//     and one bulk copy (cp.async.bulk) of the sketch digit tile (bin columns x
-//     128 samples), stored contiguous and pre-swizzled (digit_offset), into
-//     shared-memory rings;
-//   * 4 decoder warps expanding packed codes into the G (value) and O
-//     (observed) int8 operand tiles in the canonical K-major SWIZZLE_128B
-//     layout the UMMA descriptors expect;
-//   * one thread issuing tcgen05.mma.kind::i8 (M=128, N=bin columns, K=32)
-//     into two TMEM accumulators (G at column 0, O at column 256);
-//   * the decoder warps reading the accumulators back with tcgen05.ld for the
-//     exact digit recombination and the squared-sum epilogue.
+//     and one bulk copy (cp.async.bulk) of the sketch digit tile (up to 256
+//     columns x 128 samples), stored contiguous and pre-swizzled
+//     (digit_offset), into shared-memory rings;
+//   * two sets of 4 decoder warps expanding packed codes into the G (value)
+//     and O (observed) int8 operand tiles in the canonical K-major
+//     SWIZZLE_128B layout the UMMA descriptors expect;
+//   * one thread issuing tcgen05.mma.kind::i8 (M=128, N<=256, K=32) into two
+//     TMEM accumulators (G at column 0, O at column 256; on tiles without a
+//     missing call, two alternating G accumulators);
+//   * the first decoder set reading the accumulators back with tcgen05.ld for
+//     the exact digit recombination and the squared-sum epilogue.
+// The CTA's bins' columns are walked in MMA groups of up to 256, a bin
+// possibly straddling two groups: an MMA costs about the same at N = 64 and
+// N = 256, so full groups do the most work per instruction.
 // Digits of each probe column sit next to each other (column = 4 v + t), so
 // one 32-column TMEM load holds 8 probes x 4 digits.
 //
