@@ -202,9 +202,13 @@ __global__ void __launch_bounds__(kThreads, 1)
                 const int live = min(min(256, cols - g * 256), nbk * a.ncolp - g * 256);
                 const uint32_t bytes = (uint32_t)live * (uint32_t)kBK;
                 mbar_expect_tx(&b_full[s], bytes);
-                bulk_load(smem + lay.b_off(s),
-                          a.yq + ((int64_t)kt * a.yq_cols + (int64_t)kb * a.ncolp + g * 256) * kBK,
-                          bytes, &b_full[s]);
+                // two copies of whole 16-row pieces (2 KB multiples): phase 2
+                // measured ~2 % faster than with one copy of up to 32 KB
+                const int8_t* src =
+                    a.yq + ((int64_t)kt * a.yq_cols + (int64_t)kb * a.ncolp + g * 256) * kBK;
+                const uint32_t first = (uint32_t)(live / 32) * 16u * (uint32_t)kBK;
+                if (first) bulk_load(smem + lay.b_off(s), src, first, &b_full[s]);
+                bulk_load(smem + lay.b_off(s) + first, src + first, bytes - first, &b_full[s]);
             }
             for (int j = max(0, it - kBStages); j < it; ++j)
                 mbar_wait(&b_full[j % kBStages], (uint32_t)(j / kBStages) & 1u);
